@@ -1,0 +1,326 @@
+"""Benchmark of the B200 DG SN sweep (one JSON line on rank 0).
+
+A step is one transport sweep over the whole workload: every (cell, angle,
+group) of the 196,608-tet S8 G=8 Kuhn-cube workload (32^3 hexes x 6 tets,
++-0.05h jitter, lognormal sigma_t, downscatter, box source) updated once,
+phi_out = D L^-1 (Q + M S phi_in).  `value` is the mixed-precision (FP32)
+sweep's updates/s with inputs resident in HBM; the FP64 sweep is reported
+beside it, with the phi error of the mixed-precision solve against the FP64
+solve.  `e2e` is the drop-in SweeperAbstract::sweep(psi, source) through the
+C ABI with host buffers (psi-sized source in, psi out, copies timed).
+
+Multi-GPU: the sweep does not shard across GPUs here (one mesh partition per
+GPU by design); --gpus N runs N independent replicas, one per rank, and
+reports the sum of their throughputs with the max-over-ranks time.
+
+--impl reference times the reference's own CPU sweep (SweeperTraverse::sweep
+compiled from its sources, oracle/_ref/ref_dump.x) on the host cores.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sweep cell*dir*grp updates/s (mixed-precision FP32 sweep, FP64 refinement)"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--workload", default="kuhn32_s8_g8")
+    p.add_argument("--no-solve", action="store_true", help="skip the solve-error check")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return p.parse_args()
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes(nc, A, G, n_in, s):
+    """Per sweep: s*G*sum_(c,a)(4 + 3 n_in) + Nc*4*G*(8+8) + Nc*208 bytes.
+    psi write (4 nodal values) and upwind reads (3 per incoming interior face)
+    in the sweep precision, FP64 phi in and out, per-cell geometry and tables."""
+    return s * G * (4 * nc * A + 3 * n_in) + nc * 4 * G * 16 + nc * 208
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def build_problem(name):
+    from tycho2_b200 import problems
+    w = dict(problems.WORKLOADS[name])
+    mesh, st, ss, mat, q = problems.make_problem(**w)
+    return w, mesh, st, ss, mat, q
+
+
+def cpu_baseline(w, mesh, st, q, steps=1, warmup=0):
+    """Times the reference's own CPU sweep (oracle/_ref) if present, else the
+    oracle restatement, on all host cores; one full sweep of the workload."""
+    ncpu = os.cpu_count() or 1
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_dump.x")
+    nc, A, G = mesh.n_cells, 2 * w["sn"] ** 2, w["groups"]
+    with tempfile.TemporaryDirectory() as d:
+        pm = os.path.join(d, "m.pmesh")
+        mesh.write_pmesh(pm)
+        if os.path.exists(ref):
+            np.ascontiguousarray(st).tofile(os.path.join(d, "st.f64"))
+            np.ascontiguousarray(q).tofile(os.path.join(d, "q.f64"))
+            env = dict(os.environ, OMP_NUM_THREADS=str(min(ncpu, A)))
+            r = subprocess.run([ref, "bench", pm, str(w["sn"]), str(G), os.path.join(d, "st.f64"),
+                                os.path.join(d, "q.f64"), str(steps), str(warmup)],
+                               capture_output=True, text=True, env=env, timeout=1800)
+            line = [ln for ln in r.stdout.splitlines() if ln.startswith("REFBENCH ")]
+            if r.returncode != 0 or not line:
+                raise RuntimeError("reference bench failed: %s" % r.stderr[-500:])
+            res = json.loads(line[0][len("REFBENCH "):])
+            return {"value": nc * A * G / res["seconds_per_sweep"], "unit": "updates/s",
+                    "cores": res["threads"], "kind": "reference",
+                    "sample": "%d full sweep(s) of the workload, SweeperTraverse::sweep" % steps,
+                    "seconds_per_sweep": res["seconds_per_sweep"]}
+        from oracle.oracle import Oracle, OracleMesh
+        o = Oracle(OracleMesh(pm), w["sn"], G)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            o.sweep(st, src_iso=np.ascontiguousarray(q))
+        dt = (time.perf_counter() - t0) / steps
+        return {"value": nc * A * G / dt, "unit": "updates/s", "cores": ncpu, "kind": "port",
+                "sample": "%d full sweep(s) of the workload, oracle restatement" % steps,
+                "seconds_per_sweep": dt}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w, mesh, st, ss, mat, q = build_problem(args.workload)
+    nc, A, G = mesh.n_cells, 2 * w["sn"] ** 2, w["groups"]
+    steps = max(1, min(args.steps, 3))
+    res = cpu_baseline(w, mesh, st, q, steps=steps, warmup=min(args.warmup, 1))
+    v = res["value"]
+    line = {"metric": METRIC, "value": v, "unit": "updates/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": res["seconds_per_sweep"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.workload, "cells": nc, "angles": A, "groups": G},
+            "cpu_baseline": res,
+            "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    import tycho2_b200 as ty
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = local if world > 1 else 0
+
+    w, mesh, st, ss, mat, q = build_problem(args.workload)
+    nc, A, G = mesh.n_cells, 2 * w["sn"] ** 2, w["groups"]
+    updates = nc * A * G
+    sw = ty.SweeperCuda(mesh, w["sn"], G, fp32=True, device=dev)
+    sw.set_cross_sections(st, ss, mat)
+    sw.set_source(q, "isotropic")
+    info = sw.schedule_info()
+
+    # Untimed warm-up (graph capture of both precisions), then K timed steps
+    # of each precision.  psi (6.4 GB FP64 / 3.2 GB FP32) is far larger than
+    # L2; a 256 MB buffer is also written between steps.
+    sw.time_sweeps(1, max(args.warmup, 3))
+    sw.time_sweeps(0, max(args.warmup, 3))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    with Clocks(dev) as clk:
+        barrier()
+        t0 = time.perf_counter()
+        ms32, lvl32 = sw.time_sweeps(1, args.steps, True)
+        barrier()
+        wall32 = time.perf_counter() - t0
+        ms64, lvl64 = sw.time_sweeps(0, args.steps, True)
+        barrier()
+    clocks = clk.summary()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms32, lvl32, ms64, lvl64 = (max_over_ranks(x) for x in (ms32, lvl32, ms64, lvl64))
+    value = world * updates / (ms32 * 1e-3)
+    fp64_value = world * updates / (ms64 * 1e-3)
+
+    peak, peak_kind = hbm_peak()
+    b32 = algorithmic_bytes(nc, A, G, info["n_incoming_interior"], 4)
+    b64 = algorithmic_bytes(nc, A, G, info["n_incoming_interior"], 8)
+    ach32 = b32 / (lvl32 * 1e-3) / 1e9
+    ach64 = b64 / (lvl64 * 1e-3) / 1e9
+
+    # Solve-level check: mixed precision vs FP64 GMRES on the same problem.
+    solve = None
+    if not args.no_solve:
+        tol = w.get("tol", 1e-10)
+        phi64, _, s64 = sw.solve("gmres", iter_max=500, err_max=tol, restart=w.get("restart", 20),
+                                 want_psi=False)
+        phim, _, sm = sw.solve("mixed", iter_max=500, err_max=tol, restart=w.get("restart", 20),
+                               want_psi=False)
+        err = float(np.abs(phim - phi64).sum() / np.abs(phi64).sum())
+        solve = {"phi_rel_err_l1_mixed_vs_fp64": err, "fp64_gmres_seconds": s64["seconds"],
+                 "mixed_seconds": sm["seconds"], "fp64_sweeps": s64["sweeps_fp64"],
+                 "mixed_sweeps_fp32": sm["sweeps_fp32"], "mixed_sweeps_fp64": sm["sweeps_fp64"],
+                 "fp64_residual": s64["final_error"], "mixed_residual": sm["final_error"],
+                 "tol": tol, "speedup": s64["seconds"] / sm["seconds"]}
+
+    # End to end through the drop-in sweep with host buffers.
+    e2e = None
+    if not args.no_e2e:
+        npsi = nc * A * 4 * G
+        src_t = torch.empty(npsi, dtype=torch.float64, pin_memory=True)
+        psi_t = torch.empty(npsi, dtype=torch.float64, pin_memory=True)
+        src = src_t.numpy().reshape(sw.psi_shape)
+        src[:] = q[:, None, :, :]
+        psi = psi_t.numpy().reshape(sw.psi_shape)
+        sw.sweep(psi, src)
+        n_e2e = max(1, min(args.steps, 3))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(n_e2e):
+            sw.sweep(psi, src)
+        barrier()
+        dt = max_over_ranks((time.perf_counter() - t0) / n_e2e)
+        e2e = {"value": world * updates / dt, "unit": "updates/s", "h2d_bytes_per_step": npsi * 8,
+               "d2h_bytes_per_step": npsi * 8, "path": "tycho_sweeper_sweep (FP64, host buffers)",
+               "seconds_per_step": dt}
+        del src_t, psi_t
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(w, mesh, st, q, steps=1)
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "error": str(e)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms32,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "cells": nc, "angles": A, "groups": G,
+                       "levels": info["n_levels"], "parallelism": "replicas" if world > 1 else "1 gpu",
+                       "l2": "psi > L2 and a 256 MB flush between steps"},
+            "fp64": {"value": fp64_value, "ms_per_step": ms64, "dtype": "f64"},
+            "mixed_vs_fp64_sweep_speedup": value / fp64_value,
+            "solve": solve,
+            "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
+                         "frac": ach32 / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "sweep_level_kernel<float>", "bytes_per_sweep": b32,
+                         "kernel_ms_per_sweep": lvl32,
+                         "fp64": {"achieved": ach64, "frac": ach64 / peak, "bytes_per_sweep": b64,
+                                  "kernel_ms_per_sweep": lvl64}},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps * 2 * (info["n_levels"] + 2),
+            "clocks": clocks,
+            "wall_check_s": wall32,
+        }
+        print(json.dumps(line), flush=True)
+    sw.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

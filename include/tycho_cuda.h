@@ -1,0 +1,197 @@
+/*
+ * tycho_cuda.h -- C ABI of the B200-native DG SN sweep.
+ *
+ * A drop-in for the transport sweep of lanl/tycho2: the reference's
+ * SweeperAbstract (src/SweeperAbstract.hh:47-70) is implemented on top of
+ * these calls (tycho2_b200/csrc/SweeperCuda.hh), so SourceIteration and the
+ * Krylov driver call the GPU sweep unchanged.  Plain pointers and sizes only;
+ * host arrays use the reference's layouts:
+ *
+ *   psi / angular source   ((cell*A + angle)*4 + vertex)*G + group
+ *                          (PsiData, src/PsiData.hh:155-163)
+ *   phi / isotropic source (cell*4 + vertex)*G + group
+ *                          (PhiData, src/PsiData.hh:363-370)
+ *   per-face tables        [cell][face][...] row-major, face k opposite
+ *                          cell vertex k (src/TychoMeshIO.cc:128-145)
+ *
+ * Every entry point returns a tycho_status; tycho_last_error() gives the
+ * message of the calling thread's last failure.  The reference aborts on
+ * the same conditions through Insist (src/Assert.hh:62); the C++ adapter
+ * maps a nonzero status back onto Insist.  There is no CPU fallback: without
+ * a usable CUDA device the sweeper entry points fail with TYCHO_ERR_CUDA.
+ *
+ * Threading: a handle is used from one host thread at a time; distinct
+ * handles are independent.
+ */
+#ifndef TYCHO_CUDA_H
+#define TYCHO_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tycho_status {
+    TYCHO_OK = 0,
+    TYCHO_ERR_ARG = 1,
+    TYCHO_ERR_IO = 2,
+    TYCHO_ERR_FORMAT = 3,
+    TYCHO_ERR_CUDA = 4,
+    TYCHO_ERR_OOM = 5,
+    TYCHO_ERR_CYCLE = 6,
+    TYCHO_ERR_NOT_CONVERGED = 7,
+    TYCHO_ERR_TIMEOUT = 8,
+    TYCHO_ERR_BUSY = 9,
+    TYCHO_ERR_MISSING = 10
+} tycho_status;
+
+/* Arithmetic of the sweep (psi, face fluxes, 4x4 solves). */
+typedef enum tycho_precision { TYCHO_FP64 = 0, TYCHO_FP32 = 1 } tycho_precision;
+
+/* Outer solver of tycho_sweeper_solve. */
+typedef enum tycho_method {
+    TYCHO_SOURCE_ITERATION = 0, /* SourceIteration::fixedPoint (src/SourceIteration.cc:127-207) */
+    TYCHO_GMRES = 1,            /* SourceIteration::krylov (src/SourceIteration.cc:216-285) */
+    TYCHO_MIXED_GMRES = 2       /* FP32-sweep GMRES inside FP64 iterative refinement */
+} tycho_method;
+
+/* Local 4x4 solve (deck key GaussElim, src/Global.hh:99-105). */
+typedef enum tycho_gauss_elim { TYCHO_GAUSS_ORIGINAL = 0, TYCHO_GAUSS_NOPIVOT = 1 } tycho_gauss_elim;
+
+typedef struct tycho_mesh tycho_mesh;       /* host-side mesh (ingest + tables) */
+typedef struct tycho_sweeper tycho_sweeper; /* device-resident sweep instance */
+
+const char *tycho_status_string(int status);
+/* Copies the calling thread's last error message; returns its length. */
+size_t tycho_last_error(char *buf, size_t len);
+int tycho_version(void);
+
+/* ---- mesh ingest: replaces TychoMesh::TychoMesh (src/TychoMesh.cc:193-260)
+        and TychoMesh::readTychoMesh (src/TychoMeshIO.cc:153-333) ---------- */
+
+/* Reads a one-partition .pmesh (src/ParallelMesh.hh:43-81). */
+int tycho_mesh_read_pmesh(const char *path, tycho_mesh **out);
+/* Reads a .smesh (src/SerialMesh.hh:43-68) as one partition, as the
+   reference's util/PartitionColumns 1 1 would convert it. */
+int tycho_mesh_read_smesh(const char *path, tycho_mesh **out);
+/* Kuhn-split cube: n^3 hexes x 6 tets on [0,length]^3, interior vertices
+   jittered by U(-jitter*h, jitter*h) per coordinate (seeded). */
+int tycho_mesh_kuhn_cube(uint32_t n, double jitter, uint64_t seed, double length,
+                         tycho_mesh **out);
+int tycho_mesh_write_smesh(const tycho_mesh *mesh, const char *path);
+int tycho_mesh_write_pmesh(const tycho_mesh *mesh, const char *path);
+int tycho_mesh_info(const tycho_mesh *mesh, uint64_t *n_cells, uint64_t *n_nodes,
+                    uint64_t *n_sides);
+/* Copies TychoMesh tables out; any pointer may be NULL.  Sizes: adj_cell,
+   cell_nodes [n*4]; neighbor_vrtx, face_to_cell [n*12]; cell_to_face [n*16]
+   (UINT64_MAX at [c][f][f]); volume [n]; area [n*4]; normal [n*12];
+   cell_gid [n]; coords [n_nodes*3].  Boundary = UINT64_MAX. */
+int tycho_mesh_tables(const tycho_mesh *mesh, uint64_t *adj_cell, uint64_t *neighbor_vrtx,
+                      uint64_t *face_to_cell, uint64_t *cell_to_face, uint64_t *cell_nodes,
+                      double *volume, double *area, double *normal, uint64_t *cell_gid,
+                      double *coords);
+void tycho_mesh_free(tycho_mesh *mesh);
+
+/* Host-side levelling of a mesh for one quadrature, no device needed.
+   (angle, cell) order, any output may be NULL: t-levels of the wavefront
+   schedule, dependency counts as the GraphTraverser constructor sets them
+   (src/GraphTraverser.cc:442-458) and b-levels as Priorities' BLevelData
+   computes them (src/Priorities.cc:59-164).  n_levels receives the number
+   of wavefront levels.  TYCHO_ERR_CYCLE if some direction is cyclic. */
+int tycho_mesh_levels(const tycho_mesh *mesh, int sn_order, uint32_t *tlevel, uint32_t *deps,
+                      uint32_t *blevel, uint32_t *n_levels);
+
+/* ---- quadrature: Quadrature::Quadrature (src/Quadrature.cc:150-244) ----- */
+
+/* Fills the 2*sn^2 directions and weights; returns the count or -1. */
+int tycho_quadrature(int sn_order, double *xi, double *eta, double *mu, double *wt);
+
+/* ---- sweeper: SweeperAbstract (src/SweeperAbstract.hh:47-70) ----------- */
+
+typedef struct tycho_sweeper_opts {
+    int sn_order;   /* deck key snOrder */
+    int n_groups;   /* deck key nGroups */
+    int gauss_elim; /* tycho_gauss_elim, deck key GaussElim */
+    int device;     /* CUDA device ordinal */
+    int fp32;       /* nonzero: also prepare the FP32 sweep (mixed precision) */
+    int tpi64;      /* threads per (cell,angle) item of the FP64 sweep, 0 = auto */
+    int tpi32;      /* same for the FP32 sweep, 0 = auto */
+} tycho_sweeper_opts;
+
+/* Builds the device-resident instance: uploads the mesh tables, levels every
+   (cell, angle) pair into wavefronts (replaces the GraphTraverser constructor
+   and Priorities, src/GraphTraverser.cc:416-459, src/Priorities.cc:396-435)
+   and allocates psi.  Fails with TYCHO_ERR_CYCLE on a cyclic direction. */
+int tycho_sweeper_create(const tycho_mesh *mesh, const tycho_sweeper_opts *opts,
+                         tycho_sweeper **out);
+void tycho_sweeper_destroy(tycho_sweeper *sw);
+
+/* Cross sections (Problem::createCrossSections, src/Problem.cc:149-172):
+   sigma_t[c], sigma_s[c] per cell.  scatter == NULL: within-group
+   scattering sigma_s[c]/(4 pi) phi_g (src/Util.cc:118-130); otherwise the
+   G x G matrix scatter[g*G + g'] scales sigma_s[c] for g' -> g. */
+int tycho_sweeper_set_cross_sections(tycho_sweeper *sw, const double *sigma_t,
+                                     const double *sigma_s, const double *scatter);
+
+/* Fixed source Q (Problem::getSource, src/Problem.cc:140-143).
+   kind 0: angular, psi layout (as the reference's PsiData source);
+   kind 1: isotropic, phi layout.  q == NULL clears it. */
+int tycho_sweeper_set_source(tycho_sweeper *sw, int kind, const double *q);
+
+/* The drop-in SweeperAbstract::sweep(psi, source): psi = L^{-1} source for
+   an angular source in psi layout, vacuum boundaries.  Host buffers; the
+   copies in and out are part of the call. */
+int tycho_sweeper_sweep(tycho_sweeper *sw, const double *source, double *psi);
+
+typedef struct tycho_solve_opts {
+    int method;        /* tycho_method */
+    int iter_max;      /* SI steps / Krylov iterations (deck key iterMax) */
+    double err_max;    /* SI: L1 relative change; Krylov: relative residual (errMax) */
+    int restart;       /* GMRES restart length */
+    double inner_tol;  /* mixed: relative tolerance of each FP32 correction solve */
+    int refine_max;    /* mixed: maximum FP64 refinement steps */
+} tycho_solve_opts;
+
+typedef struct tycho_solve_stats {
+    int iterations;        /* SI steps or total Krylov iterations */
+    int sweeps_fp64;       /* FP64 sweeps performed */
+    int sweeps_fp32;       /* FP32 sweeps performed */
+    int refinements;       /* mixed: FP64 refinement steps */
+    double final_error;    /* SI: last L1 relative change; Krylov: relative residual */
+    double seconds;        /* device time of the solve */
+} tycho_solve_stats;
+
+/* SweeperAbstract::solve (src/SweeperTraverse.cc:65-74): psi starts at 0 and
+   the chosen outer iteration runs on the device.  phi_out / psi_out (host,
+   may be NULL) receive the result; psi stays resident on the device. */
+int tycho_sweeper_solve(tycho_sweeper *sw, const tycho_solve_opts *opts, double *phi_out,
+                        double *psi_out, tycho_solve_stats *stats);
+
+/* Writes the resident psi in the reference's .psi format
+   (PsiData::writeToFile, src/PsiData.cc:62-106). */
+int tycho_sweeper_write_psi(tycho_sweeper *sw, const char *path);
+
+/* Schedule facts: levels (max over angles), items (cells x angles) and the
+   number of incoming interior faces summed over items. */
+int tycho_sweeper_schedule_info(const tycho_sweeper *sw, uint32_t *n_levels, uint64_t *n_items,
+                                uint64_t *n_incoming_interior);
+/* Integer tables for parity, (angle, cell) order, any pointer may be NULL:
+   t-levels of the wavefront schedule, the GraphTraverser constructor's
+   dependency counts and Priorities' b-levels. */
+int tycho_sweeper_levels(const tycho_sweeper *sw, uint32_t *tlevel, uint32_t *deps,
+                         uint32_t *blevel);
+
+/* Device timing of n back-to-back operator applications
+   phi_out = D L^{-1} (M S phi_in + Q) in the given precision, on the
+   sweeper's stream with CUDA events (inputs resident).  ms[0] = mean time
+   of one application, ms[1] = mean time of its wavefront kernels alone. */
+int tycho_sweeper_time_sweeps(tycho_sweeper *sw, int precision, int n, int flush_l2,
+                              double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,104 @@
+"""Regenerates the golden fixtures in this directory from the reference.
+
+Needs the tycho2 source tree (default /root/reference, or $TYCHO2_REF) and the
+reference built from it by `make -C oracle ref` (oracle/_ref).  Writes:
+
+  gold.psi, cube-208.smesh   the reference's own regression vector and mesh
+                             (test/regression/gold.psi, util/cube-208.smesh),
+                             copied byte for byte
+  kuhn3_ref.npz              what the reference computes on a jittered Kuhn
+                             cube (3^3 hexes x 6 tets on [0,100]^3, written by
+                             this project's generator and converted by the
+                             reference's PartitionColumns 1 1):
+                               pmesh_sha256       the converted mesh file
+                               s{4,8}_{adj,nbr,f2c,c2f,deps,blev}  integer tables
+                               s4_vol, s4_area, s4_odn             geometry (f64)
+                               sweep_* : one SweeperTraverse::sweep of a seeded
+                                         angular source, S4, G=3
+                               si_*    : SourceIteration::fixedPoint with the
+                                         hat source, per-cell sigma, S4, G=2
+
+Run:  python tests/golden/make_golden.py
+"""
+import hashlib
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+REF = os.environ.get("TYCHO2_REF", "/root/reference")
+REF_BIN = os.path.join(ROOT, "oracle", "_ref")
+
+
+def run(*args, cwd=None):
+    subprocess.run(list(args), check=True, cwd=cwd, stdout=subprocess.DEVNULL)
+
+
+def kuhn3_fixture(tmp):
+    import tycho2_b200 as ty
+    from tycho2_b200 import problems
+
+    mesh = ty.TychoMesh.kuhn_cube(3, 0.05, 2024, 100.0)
+    smesh = os.path.join(tmp, "k3.smesh")
+    pmesh = os.path.join(tmp, "k3.pmesh")
+    mesh.write_smesh(smesh)
+    run(os.path.join(REF_BIN, "PartitionColumns.x"), "1", "1", smesh, pmesh)
+    out = {"pmesh_sha256": np.frombuffer(hashlib.sha256(open(pmesh, "rb").read()).digest(), np.uint8)}
+    nc = mesh.n_cells
+    for sn in (4, 8):
+        pre = os.path.join(tmp, "s%d_" % sn)
+        run(os.path.join(REF_BIN, "ref_dump.x"), "tables", pmesh, str(sn), pre)
+        for k in ("adj", "nbr", "f2c", "c2f", "deps", "blev"):
+            out["s%d_%s" % (sn, k)] = np.fromfile(pre + k + ".u64", np.uint64)
+        if sn == 4:
+            for k in ("vol", "area", "odn"):
+                out["s4_" + k] = np.fromfile(pre + k + ".f64", np.float64)
+    # One sweep of a seeded angular source.
+    rng = np.random.default_rng(7)
+    A, G = 32, 3
+    sig_t = rng.uniform(0.5, 3.0, nc)
+    src = rng.uniform(0.0, 1.0, (nc, A, 4, G))
+    f_st, f_src, f_psi = (os.path.join(tmp, n) for n in ("st.f64", "src.f64", "psi.f64"))
+    sig_t.tofile(f_st)
+    src.tofile(f_src)
+    run(os.path.join(REF_BIN, "ref_dump.x"), "sweep", pmesh, "4", str(G), f_st, f_src, f_psi)
+    out["sweep_sigma_t"] = sig_t
+    out["sweep_source"] = src
+    out["sweep_psi"] = np.fromfile(f_psi, np.float64).reshape(nc, A, 4, G)
+    # Source iteration with the hat source and per-cell cross sections.
+    G = 2
+    sig_t = rng.uniform(1.0, 4.0, nc)
+    sig_s = sig_t * rng.uniform(0.2, 0.8, nc)
+    quad = ty.Quadrature(4)
+    hat = problems.hat_source(mesh, quad, sig_t, sig_s, G)
+    f_ss = os.path.join(tmp, "ss.f64")
+    sig_t.tofile(f_st)
+    sig_s.tofile(f_ss)
+    hat.tofile(f_src)
+    run(os.path.join(REF_BIN, "ref_dump.x"), "si", pmesh, "4", str(G), f_st, f_ss, f_src, "100",
+        "1e-12", f_psi)
+    out["si_sigma_t"] = sig_t
+    out["si_sigma_s"] = sig_s
+    out["si_psi"] = np.fromfile(f_psi, np.float64).reshape(nc, A, 4, G)
+    np.savez_compressed(os.path.join(HERE, "kuhn3_ref.npz"), **out)
+
+
+def main():
+    if not os.path.isdir(REF):
+        sys.exit("reference tree not found: %s" % REF)
+    run("make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", "oracle", "REF=" + REF)
+    shutil.copyfile(os.path.join(REF, "test", "regression", "gold.psi"), os.path.join(HERE, "gold.psi"))
+    shutil.copyfile(os.path.join(REF, "util", "cube-208.smesh"), os.path.join(HERE, "cube-208.smesh"))
+    with tempfile.TemporaryDirectory() as tmp:
+        kuhn3_fixture(tmp)
+
+
+if __name__ == "__main__":
+    main()

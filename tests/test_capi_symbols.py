@@ -1,0 +1,39 @@
+"""The C ABI library loads, exports every function include/tycho_cuda.h
+declares, and refuses to sweep without a GPU (there is no CPU fallback)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT, gpu_available
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, "include", "tycho_cuda.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(tycho_\w+)\s*\(", text)))
+
+
+def test_header_declares_the_abi():
+    names = declared_functions()
+    for required in ("tycho_sweeper_create", "tycho_sweeper_sweep", "tycho_sweeper_solve",
+                     "tycho_mesh_read_pmesh", "tycho_quadrature"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol(built):
+    from tycho2_b200._capi import LIB_PATH, SIGNATURES
+    lib = ctypes.CDLL(LIB_PATH)
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+        assert name in SIGNATURES, "binding missing for %s" % name
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU failure mode")
+def test_sweeper_fails_loudly_without_gpu(built):
+    import tycho2_b200 as ty
+    mesh = ty.TychoMesh.kuhn_cube(2)
+    with pytest.raises(ty.TychoError) as e:
+        ty.SweeperCuda(mesh, 4, 1)
+    assert e.value.status == 4 and "no CPU fallback" in str(e.value)

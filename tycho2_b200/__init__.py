@@ -1,0 +1,11 @@
+"""tycho2_b200: a B200-native drop-in for lanl/tycho2's DG SN transport sweep.
+
+The sweep, the scalar-flux reduction and the outer solvers run as sm_100a
+CUDA kernels in libtycho_b200.so (C ABI: include/tycho_cuda.h); this package
+is the host-side mirror of the reference's interface over that ABI.
+"""
+from ._capi import TychoError, lib  # noqa: F401
+from .sweeper import Quadrature, SweeperCuda, TychoMesh  # noqa: F401
+from . import problems  # noqa: F401
+
+__all__ = ["TychoError", "TychoMesh", "Quadrature", "SweeperCuda", "problems", "lib"]

@@ -1,0 +1,109 @@
+"""ctypes binding of the C ABI in include/tycho_cuda.h (libtycho_b200.so).
+
+The library is built in-tree by tycho2_b200/csrc/Makefile (see
+__graft_entry__.build()).  Loading fails loudly when it is missing: there is
+no CPU fallback for the sweep.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libtycho_b200.so")
+
+TYCHO_OK = 0
+STATUS_NAMES = {
+    0: "TYCHO_OK", 1: "TYCHO_ERR_ARG", 2: "TYCHO_ERR_IO", 3: "TYCHO_ERR_FORMAT",
+    4: "TYCHO_ERR_CUDA", 5: "TYCHO_ERR_OOM", 6: "TYCHO_ERR_CYCLE",
+    7: "TYCHO_ERR_NOT_CONVERGED", 8: "TYCHO_ERR_TIMEOUT", 9: "TYCHO_ERR_BUSY",
+    10: "TYCHO_ERR_MISSING",
+}
+
+# Every function the header declares, with (restype, argtypes).
+_P = C.c_void_p
+_PP = C.POINTER(C.c_void_p)
+_U64P = C.POINTER(C.c_uint64)
+_U32P = C.POINTER(C.c_uint32)
+
+
+class SweeperOpts(C.Structure):
+    _fields_ = [("sn_order", C.c_int), ("n_groups", C.c_int), ("gauss_elim", C.c_int),
+                ("device", C.c_int), ("fp32", C.c_int), ("tpi64", C.c_int), ("tpi32", C.c_int)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("method", C.c_int), ("iter_max", C.c_int), ("err_max", C.c_double),
+                ("restart", C.c_int), ("inner_tol", C.c_double), ("refine_max", C.c_int)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("sweeps_fp64", C.c_int), ("sweeps_fp32", C.c_int),
+                ("refinements", C.c_int), ("final_error", C.c_double), ("seconds", C.c_double)]
+
+
+SIGNATURES = {
+    "tycho_status_string": (C.c_char_p, [C.c_int]),
+    "tycho_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "tycho_version": (C.c_int, []),
+    "tycho_mesh_read_pmesh": (C.c_int, [C.c_char_p, _PP]),
+    "tycho_mesh_read_smesh": (C.c_int, [C.c_char_p, _PP]),
+    "tycho_mesh_kuhn_cube": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, C.c_double, _PP]),
+    "tycho_mesh_write_smesh": (C.c_int, [_P, C.c_char_p]),
+    "tycho_mesh_write_pmesh": (C.c_int, [_P, C.c_char_p]),
+    "tycho_mesh_info": (C.c_int, [_P, _U64P, _U64P, _U64P]),
+    "tycho_mesh_tables": (C.c_int, [_P] + [_P] * 10),
+    "tycho_mesh_free": (None, [_P]),
+    "tycho_mesh_levels": (C.c_int, [_P, C.c_int, _P, _P, _P, _U32P]),
+    "tycho_quadrature": (C.c_int, [C.c_int, _P, _P, _P, _P]),
+    "tycho_sweeper_create": (C.c_int, [_P, C.POINTER(SweeperOpts), _PP]),
+    "tycho_sweeper_destroy": (None, [_P]),
+    "tycho_sweeper_set_cross_sections": (C.c_int, [_P, _P, _P, _P]),
+    "tycho_sweeper_set_source": (C.c_int, [_P, C.c_int, _P]),
+    "tycho_sweeper_sweep": (C.c_int, [_P, _P, _P]),
+    "tycho_sweeper_solve": (C.c_int, [_P, C.POINTER(SolveOpts), _P, _P, C.POINTER(SolveStats)]),
+    "tycho_sweeper_write_psi": (C.c_int, [_P, C.c_char_p]),
+    "tycho_sweeper_schedule_info": (C.c_int, [_P, _U32P, _U64P, _U64P]),
+    "tycho_sweeper_levels": (C.c_int, [_P, _P, _P, _P]),
+    "tycho_sweeper_time_sweeps": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P]),
+}
+
+_lib = None
+
+
+class TychoError(RuntimeError):
+    """A nonzero tycho_status, with the library's message."""
+
+    def __init__(self, status, message):
+        self.status = status
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), message))
+
+
+def lib():
+    """Loads libtycho_b200.so once; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libtycho_b200.so is not built (%s); run __graft_entry__.build()" % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != TYCHO_OK:
+        buf = C.create_string_buffer(1024)
+        lib().tycho_last_error(buf, 1024)
+        raise TychoError(status, buf.value.decode(errors="replace"))
+
+
+def ptr(a):
+    """Raw pointer of a C-contiguous numpy array (None passes NULL)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.c_void_p)

@@ -1,0 +1,346 @@
+// extern "C" entry points declared in include/tycho_cuda.h.
+#include "../../include/tycho_cuda.h"
+
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "mesh.hpp"
+#include "schedule.hpp"
+#include "status.hpp"
+#include "sweeper.hpp"
+
+struct tycho_mesh {
+    tycho::MeshRecords rec;
+    tycho::MeshTables tab;
+};
+
+struct tycho_sweeper {
+    tycho::Sweeper sw;
+};
+
+namespace tycho {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+const std::string &last_error() { return g_last_error; }
+
+}  // namespace tycho
+
+namespace {
+
+int finish(int status, const std::string &err)
+{
+    if (status != tycho::kOk) tycho::set_last_error(err.empty() ? tycho_status_string(status) : err);
+    return status;
+}
+
+template <typename F>
+int guarded(F &&f)
+{
+    try {
+        return f();
+    } catch (const std::bad_alloc &) {
+        tycho::set_last_error("host allocation failed");
+        return tycho::kErrOom;
+    } catch (const std::exception &e) {
+        tycho::set_last_error(e.what());
+        return tycho::kErrArg;
+    }
+}
+
+int mesh_from_records(tycho_mesh *m, tycho_mesh **out)
+{
+    std::string err;
+    int st = tycho::build_tables(m->rec, m->tab, err);
+    if (st != tycho::kOk) {
+        delete m;
+        return finish(st, err);
+    }
+    *out = m;
+    return tycho::kOk;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *tycho_status_string(int s)
+{
+    switch (s) {
+    case TYCHO_OK: return "ok";
+    case TYCHO_ERR_ARG: return "invalid argument";
+    case TYCHO_ERR_IO: return "I/O error";
+    case TYCHO_ERR_FORMAT: return "malformed input";
+    case TYCHO_ERR_CUDA: return "CUDA error";
+    case TYCHO_ERR_OOM: return "out of memory";
+    case TYCHO_ERR_CYCLE: return "cyclic sweep dependency";
+    case TYCHO_ERR_NOT_CONVERGED: return "not converged";
+    case TYCHO_ERR_TIMEOUT: return "device wait timed out";
+    case TYCHO_ERR_BUSY: return "admission refused";
+    case TYCHO_ERR_MISSING: return "required input not set";
+    default: return "unknown status";
+    }
+}
+
+size_t tycho_last_error(char *buf, size_t len)
+{
+    const std::string &e = tycho::last_error();
+    if (buf && len) {
+        size_t n = e.size() < len - 1 ? e.size() : len - 1;
+        std::memcpy(buf, e.data(), n);
+        buf[n] = 0;
+    }
+    return e.size();
+}
+
+int tycho_version(void) { return 1; }
+
+int tycho_mesh_read_pmesh(const char *path, tycho_mesh **out)
+{
+    if (!path || !out) return finish(TYCHO_ERR_ARG, "null argument");
+    return guarded([&] {
+        auto *m = new tycho_mesh;
+        std::string err;
+        int st = tycho::read_pmesh(path, m->rec, err);
+        if (st != tycho::kOk) { delete m; return finish(st, err); }
+        return mesh_from_records(m, out);
+    });
+}
+
+int tycho_mesh_read_smesh(const char *path, tycho_mesh **out)
+{
+    if (!path || !out) return finish(TYCHO_ERR_ARG, "null argument");
+    return guarded([&] {
+        auto *m = new tycho_mesh;
+        std::string err;
+        int st = tycho::read_smesh(path, m->rec, err);
+        if (st != tycho::kOk) { delete m; return finish(st, err); }
+        return mesh_from_records(m, out);
+    });
+}
+
+int tycho_mesh_kuhn_cube(uint32_t n, double jitter, uint64_t seed, double length, tycho_mesh **out)
+{
+    if (!out || n == 0 || !(jitter >= 0.0 && jitter < 0.25) || !(length > 0.0))
+        return finish(TYCHO_ERR_ARG, "kuhn cube: need n >= 1, 0 <= jitter < 0.25, length > 0");
+    return guarded([&] {
+        auto *m = new tycho_mesh;
+        tycho::kuhn_cube(n, jitter, seed, length, m->rec);
+        return mesh_from_records(m, out);
+    });
+}
+
+int tycho_mesh_write_smesh(const tycho_mesh *m, const char *path)
+{
+    if (!m || !path) return finish(TYCHO_ERR_ARG, "null argument");
+    std::string err;
+    return finish(tycho::write_smesh(path, m->rec, err), err);
+}
+
+int tycho_mesh_write_pmesh(const tycho_mesh *m, const char *path)
+{
+    if (!m || !path) return finish(TYCHO_ERR_ARG, "null argument");
+    std::string err;
+    return finish(tycho::write_pmesh(path, m->rec, err), err);
+}
+
+int tycho_mesh_info(const tycho_mesh *m, uint64_t *nc, uint64_t *nn, uint64_t *ns)
+{
+    if (!m) return finish(TYCHO_ERR_ARG, "null mesh");
+    if (nc) *nc = m->tab.n_cells;
+    if (nn) *nn = m->tab.n_nodes;
+    if (ns) *ns = m->tab.n_sides;
+    return TYCHO_OK;
+}
+
+int tycho_mesh_tables(const tycho_mesh *m, uint64_t *adj_cell, uint64_t *neighbor_vrtx,
+                      uint64_t *face_to_cell, uint64_t *cell_to_face, uint64_t *cell_nodes,
+                      double *volume, double *area, double *normal, uint64_t *cell_gid,
+                      double *coords)
+{
+    if (!m) return finish(TYCHO_ERR_ARG, "null mesh");
+    const auto &t = m->tab;
+    auto cp = [](auto *dst, const auto &v) {
+        if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(adj_cell, t.adj_cell);
+    cp(neighbor_vrtx, t.neighbor_vrtx);
+    cp(face_to_cell, t.face_to_cell);
+    cp(cell_to_face, t.cell_to_face);
+    cp(cell_nodes, t.cell_nodes);
+    cp(volume, t.volume);
+    cp(area, t.area);
+    cp(normal, t.normal);
+    cp(cell_gid, t.cell_gid);
+    cp(coords, t.coords);
+    return TYCHO_OK;
+}
+
+void tycho_mesh_free(tycho_mesh *m) { delete m; }
+
+int tycho_mesh_levels(const tycho_mesh *m, int sn, uint32_t *tlevel, uint32_t *deps, uint32_t *blevel,
+                      uint32_t *n_levels)
+{
+    if (!m) return finish(TYCHO_ERR_ARG, "null mesh");
+    return guarded([&] {
+        tycho::Quadrature q;
+        tycho::Schedule s;
+        std::string err;
+        int st = tycho::make_quadrature(sn, q, err);
+        if (st == tycho::kOk) st = tycho::build_schedule(m->tab, q, s, err);
+        if (st != tycho::kOk) return finish(st, err);
+        if (n_levels) *n_levels = s.n_levels;
+        if (tlevel) std::memcpy(tlevel, s.tlevel.data(), s.tlevel.size() * 4);
+        if (deps) {
+            std::vector<uint32_t> d;
+            tycho::dependency_counts(m->tab, q, d);
+            std::memcpy(deps, d.data(), d.size() * 4);
+        }
+        if (blevel) {
+            std::vector<uint32_t> b;
+            tycho::b_levels(m->tab, q, s, b);
+            std::memcpy(blevel, b.data(), b.size() * 4);
+        }
+        return (int)TYCHO_OK;
+    });
+}
+
+int tycho_quadrature(int sn, double *xi, double *eta, double *mu, double *wt)
+{
+    tycho::Quadrature q;
+    std::string err;
+    if (tycho::make_quadrature(sn, q, err) != tycho::kOk) {
+        tycho::set_last_error(err);
+        return -1;
+    }
+    size_t b = sizeof(double) * q.n_angles;
+    if (xi) std::memcpy(xi, q.xi.data(), b);
+    if (eta) std::memcpy(eta, q.eta.data(), b);
+    if (mu) std::memcpy(mu, q.mu.data(), b);
+    if (wt) std::memcpy(wt, q.wt.data(), b);
+    return q.n_angles;
+}
+
+int tycho_sweeper_create(const tycho_mesh *mesh, const tycho_sweeper_opts *opts, tycho_sweeper **out)
+{
+    if (!mesh || !opts || !out) return finish(TYCHO_ERR_ARG, "null argument");
+    return guarded([&] {
+        auto *h = new tycho_sweeper;
+        tycho::SweeperOptions o;
+        o.sn_order = opts->sn_order;
+        o.n_groups = opts->n_groups;
+        o.device = opts->device;
+        o.fp32 = opts->fp32 != 0;
+        o.tpi64 = opts->tpi64;
+        o.tpi32 = opts->tpi32;
+        std::string err;
+        if (opts->gauss_elim != TYCHO_GAUSS_NOPIVOT && opts->gauss_elim != TYCHO_GAUSS_ORIGINAL) {
+            delete h;
+            return finish(TYCHO_ERR_ARG, "GaussElim must be Original or NoPivot");
+        }
+        int st = h->sw.init(mesh->tab, o, err);
+        if (st != tycho::kOk) { delete h; return finish(st, err); }
+        *out = h;
+        return (int)TYCHO_OK;
+    });
+}
+
+void tycho_sweeper_destroy(tycho_sweeper *h) { delete h; }
+
+int tycho_sweeper_set_cross_sections(tycho_sweeper *h, const double *sigma_t, const double *sigma_s,
+                                     const double *scatter)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    std::string err;
+    return finish(h->sw.set_cross_sections(sigma_t, sigma_s, scatter, err), err);
+}
+
+int tycho_sweeper_set_source(tycho_sweeper *h, int kind, const double *q)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    std::string err;
+    return finish(h->sw.set_source(kind, q, err), err);
+}
+
+int tycho_sweeper_sweep(tycho_sweeper *h, const double *source, double *psi)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    std::string err;
+    return guarded([&] { return finish(h->sw.sweep_host(source, psi, err), err); });
+}
+
+int tycho_sweeper_solve(tycho_sweeper *h, const tycho_solve_opts *opts, double *phi_out,
+                        double *psi_out, tycho_solve_stats *stats)
+{
+    if (!h || !opts) return finish(TYCHO_ERR_ARG, "null argument");
+    return guarded([&] {
+        tycho::SolveOptions o;
+        o.method = opts->method;
+        o.iter_max = opts->iter_max;
+        o.err_max = opts->err_max;
+        o.restart = opts->restart > 0 ? opts->restart : 20;
+        o.inner_tol = opts->inner_tol > 0 ? opts->inner_tol : 1e-5;
+        o.refine_max = opts->refine_max > 0 ? opts->refine_max : 10;
+        tycho::SolveStats st;
+        std::string err;
+        int s = h->sw.solve(o, phi_out, psi_out, st, err);
+        if (stats) {
+            stats->iterations = st.iterations;
+            stats->sweeps_fp64 = st.sweeps_fp64;
+            stats->sweeps_fp32 = st.sweeps_fp32;
+            stats->refinements = st.refinements;
+            stats->final_error = st.final_error;
+            stats->seconds = st.seconds;
+        }
+        return finish(s, err);
+    });
+}
+
+int tycho_sweeper_write_psi(tycho_sweeper *h, const char *path)
+{
+    if (!h || !path) return finish(TYCHO_ERR_ARG, "null argument");
+    std::string err;
+    return guarded([&] { return finish(h->sw.write_psi(path, err), err); });
+}
+
+int tycho_sweeper_schedule_info(const tycho_sweeper *h, uint32_t *n_levels, uint64_t *n_items,
+                                uint64_t *n_incoming)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    const auto &s = h->sw.schedule();
+    if (n_levels) *n_levels = s.n_levels;
+    if (n_items) *n_items = s.items.size();
+    if (n_incoming) *n_incoming = s.n_incoming_interior;
+    return TYCHO_OK;
+}
+
+int tycho_sweeper_levels(const tycho_sweeper *h, uint32_t *tlevel, uint32_t *deps, uint32_t *blevel)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    return guarded([&] {
+        const auto &sw = h->sw;
+        if (tlevel) std::memcpy(tlevel, sw.schedule().tlevel.data(), sw.schedule().tlevel.size() * 4);
+        if (deps) {
+            std::vector<uint32_t> d;
+            tycho::dependency_counts(sw.tables(), sw.quadrature(), d);
+            std::memcpy(deps, d.data(), d.size() * 4);
+        }
+        if (blevel) {
+            std::vector<uint32_t> b;
+            tycho::b_levels(sw.tables(), sw.quadrature(), sw.schedule(), b);
+            std::memcpy(blevel, b.data(), b.size() * 4);
+        }
+        return (int)TYCHO_OK;
+    });
+}
+
+int tycho_sweeper_time_sweeps(tycho_sweeper *h, int precision, int n, int flush_l2, double *ms)
+{
+    if (!h || !ms) return finish(TYCHO_ERR_ARG, "null argument");
+    std::string err;
+    return guarded([&] { return finish(h->sw.time_sweeps(precision, n, flush_l2 != 0, ms, err), err); });
+}
+
+}  // extern "C"

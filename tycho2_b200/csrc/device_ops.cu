@@ -1,0 +1,270 @@
+// Streaming kernels around the wavefront sweep, and deterministic vector
+// kernels for the outer solvers.  This translation unit is compiled with
+// -fmad=false: the FP64 wavefront kernel, the per-item face terms, the
+// scalar flux and the scattering source keep the reference's rounding.
+#include "device_ops.hpp"
+#include "sweep_kernels.cuh"
+
+namespace tycho {
+
+template cudaError_t launch_level<double>(int, const LevelArgs &, uint64_t, uint64_t, cudaStream_t);
+
+namespace {
+
+constexpr double kFourPi = 4.0 * 3.14159265358979323846;
+
+__global__ void item_abar_kernel(const uint32_t *__restrict__ items, uint64_t n, uint32_t A,
+                                 const double *__restrict__ normal, const double *__restrict__ area,
+                                 const double *__restrict__ omega, double4 *abar64, float4 *abar32)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t ca = items[i];
+    const uint32_t c = ca / A, a = ca - c * A;
+    const double xi = omega[a], eta = omega[A + a], mu = omega[2 * A + a];
+    double ab[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        const double *nrm = normal + ((size_t)c * 4 + f) * 3;
+        // TychoMesh.cc:219-221 then Transport.cc:694-701
+        const double odn = xi * nrm[0] + eta * nrm[1] + mu * nrm[2];
+        ab[f] = area[(size_t)c * 4 + f] * odn;
+    }
+    abar64[i] = make_double4(ab[0], ab[1], ab[2], ab[3]);
+    if (abar32) abar32[i] = make_float4((float)ab[0], (float)ab[1], (float)ab[2], (float)ab[3]);
+}
+
+template <typename Real>
+__global__ void psi_to_phi_kernel(const Real *__restrict__ psi, const double *__restrict__ w,
+                                  double *__restrict__ phi, uint64_t nc, uint32_t A, uint32_t G)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t row = (uint64_t)4 * G;
+    if (i >= nc * row) return;
+    const uint64_t c = i / row;
+    const uint64_t vg = i - c * row;
+    const Real *p = psi + c * A * row + vg;
+    double s = 0.0;
+    for (uint32_t a = 0; a < A; ++a) s += (double)p[(size_t)a * row] * w[a];
+    phi[i] = s;
+}
+
+__global__ void scatter_source_kernel(const double *__restrict__ phi, const double *__restrict__ q,
+                                      const double *__restrict__ sigma_s,
+                                      const double *__restrict__ scat, double *__restrict__ iso,
+                                      float *__restrict__ iso32, uint64_t nc, uint32_t G)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t row = (uint64_t)4 * G;
+    if (i >= nc * row) return;
+    const uint64_t c = i / row;
+    double s;
+    if (phi) {
+        if (!scat) {
+            s = sigma_s[c] / kFourPi * phi[i];  // Util.cc:126-128
+        } else {
+            const uint32_t g = (uint32_t)(i % G);
+            const double *pv = phi + (i - g);
+            s = 0.0;
+            for (uint32_t gp = 0; gp < G; ++gp) {
+                const double k = scat[g * G + gp];
+                if (k == 0.0) continue;
+                s += sigma_s[c] * k / kFourPi * pv[gp];
+            }
+        }
+        if (q) s = q[i] + s;
+    } else {
+        s = q ? q[i] : 0.0;
+    }
+    iso[i] = s;
+    if (iso32) iso32[i] = (float)s;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int K>
+__global__ void __launch_bounds__(256)
+multi_dot_kernel(const double *__restrict__ w, const double *__restrict__ V, size_t ld, int k,
+                 int j0, uint64_t n, double *__restrict__ partials)
+{
+    double acc[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc[j] = 0.0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const double wi = w[i];
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            if (j0 + j < k) acc[j] = __fma_rn(wi, V[(size_t)(j0 + j) * ld + i], acc[j]);
+    }
+    __shared__ double sh[8][K];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const double v = warp_sum(acc[j]);
+        if (lane == 0) sh[warp][j] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < K && j0 + (int)threadIdx.x < k) {
+        double s = 0.0;
+        for (int q = 0; q < 8; ++q) s += sh[q][threadIdx.x];
+        partials[(size_t)blockIdx.x * 64 + j0 + threadIdx.x] = s;
+    }
+}
+
+__global__ void l1_kernel(const double *__restrict__ x, const double *__restrict__ y, uint64_t n,
+                          double *__restrict__ partials)
+{
+    double d = 0.0, m = 0.0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const double xi = x[i];
+        d += fabs(y ? xi - y[i] : xi);
+        m += fabs(xi);
+    }
+    __shared__ double sh[8][2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    d = warp_sum(d);
+    m = warp_sum(m);
+    if (lane == 0) { sh[warp][0] = d; sh[warp][1] = m; }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double s = 0.0;
+        for (int q = 0; q < 8; ++q) s += sh[q][threadIdx.x];
+        partials[(size_t)blockIdx.x * 64 + threadIdx.x] = s;
+    }
+}
+
+__global__ void reduce_partials_kernel(const double *__restrict__ partials, int nblocks, int k,
+                                       double *__restrict__ out)
+{
+    const int j = threadIdx.x;
+    if (j >= k) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partials[(size_t)b * 64 + j];
+    out[j] = s;
+}
+
+__global__ void multi_axpy_kernel(double *__restrict__ w, const double *__restrict__ V, size_t ld,
+                                  const double *__restrict__ h, int k, uint64_t n)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = w[i];
+    for (int j = 0; j < k; ++j) s = __fma_rn(-h[j], V[(size_t)j * ld + i], s);
+    w[i] = s;
+}
+
+__global__ void axpby_kernel(double alpha, const double *__restrict__ x, double beta,
+                             double *__restrict__ y, uint64_t n)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = __fma_rn(alpha, x[i], beta * y[i]);
+}
+
+__global__ void sub_from_kernel(const double *__restrict__ x, double *__restrict__ y, uint64_t n)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = x[i] - y[i];
+}
+
+inline unsigned blocks_for(uint64_t n, unsigned t = 256) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+cudaError_t launch_item_abar(const uint32_t *items, uint64_t n, uint32_t A, const double *normal,
+                             const double *area, const double *omega, double4 *abar64,
+                             float4 *abar32, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    item_abar_kernel<<<blocks_for(n), 256, 0, s>>>(items, n, A, normal, area, omega, abar64, abar32);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_psi_to_phi(const void *psi, bool psi_fp32, const double *w, double *phi,
+                              uint64_t nc, uint32_t A, uint32_t G, cudaStream_t s)
+{
+    const uint64_t n = nc * 4 * G;
+    if (n == 0) return cudaSuccess;
+    if (psi_fp32)
+        psi_to_phi_kernel<float><<<blocks_for(n), 256, 0, s>>>((const float *)psi, w, phi, nc, A, G);
+    else
+        psi_to_phi_kernel<double><<<blocks_for(n), 256, 0, s>>>((const double *)psi, w, phi, nc, A, G);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_source(const double *phi_in, const double *q_fixed, const double *sigma_s,
+                                  const double *scatter, double *iso, float *iso32, uint64_t nc,
+                                  uint32_t G, cudaStream_t s)
+{
+    const uint64_t n = nc * 4 * G;
+    if (n == 0) return cudaSuccess;
+    scatter_source_kernel<<<blocks_for(n), 256, 0, s>>>(phi_in, q_fixed, sigma_s, scatter, iso, iso32, nc, G);
+    return cudaGetLastError();
+}
+
+cudaError_t reducer_init(Reducer &r)
+{
+    cudaError_t e = cudaMalloc(&r.partials, sizeof(double) * kReduceBlocks * 64);
+    if (e == cudaSuccess) e = cudaMalloc(&r.result, sizeof(double) * 64);
+    if (e == cudaSuccess) e = cudaMallocHost(&r.host, sizeof(double) * 64);
+    return e;
+}
+
+void reducer_free(Reducer &r)
+{
+    if (r.partials) cudaFree(r.partials);
+    if (r.result) cudaFree(r.result);
+    if (r.host) cudaFreeHost(r.host);
+    r = Reducer();
+}
+
+cudaError_t multi_dot(const double *w, const double *V, size_t ld, int k, uint64_t n, Reducer &r,
+                      cudaStream_t s)
+{
+    if (k < 1 || k > 64) return cudaErrorInvalidValue;
+    for (int j0 = 0; j0 < k; j0 += 16)
+        multi_dot_kernel<16><<<kReduceBlocks, 256, 0, s>>>(w, V, ld, k, j0, n, r.partials);
+    reduce_partials_kernel<<<1, 64, 0, s>>>(r.partials, kReduceBlocks, k, r.result);
+    cudaError_t e = cudaMemcpyAsync(r.host, r.result, sizeof(double) * k, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);
+}
+
+cudaError_t l1_pair(const double *x, const double *y, uint64_t n, Reducer &r, cudaStream_t s)
+{
+    l1_kernel<<<kReduceBlocks, 256, 0, s>>>(x, y, n, r.partials);
+    reduce_partials_kernel<<<1, 64, 0, s>>>(r.partials, kReduceBlocks, 2, r.result);
+    cudaError_t e = cudaMemcpyAsync(r.host, r.result, sizeof(double) * 2, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);
+}
+
+cudaError_t multi_axpy(double *w, const double *V, size_t ld, const double *h, int k, uint64_t n,
+                       cudaStream_t s)
+{
+    if (n == 0 || k == 0) return cudaSuccess;
+    multi_axpy_kernel<<<blocks_for(n), 256, 0, s>>>(w, V, ld, h, k, n);
+    return cudaGetLastError();
+}
+
+cudaError_t axpby(double alpha, const double *x, double beta, double *y, uint64_t n, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    axpby_kernel<<<blocks_for(n), 256, 0, s>>>(alpha, x, beta, y, n);
+    return cudaGetLastError();
+}
+
+cudaError_t sub_from(const double *x, double *y, uint64_t n, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    sub_from_kernel<<<blocks_for(n), 256, 0, s>>>(x, y, n);
+    return cudaGetLastError();
+}
+
+}  // namespace tycho

@@ -1,0 +1,28 @@
+// Host-safe declarations of the wavefront launch (no device code): the
+// per-level argument block and the launcher, instantiated for double (in
+// device_ops.cu, FMA contraction off) and float (sweep_f32.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tycho {
+
+struct LevelArgs {
+    const uint32_t *items;   // cell*A + angle, level-sorted
+    const void *abar;        // Real4 per item: face area * omega.n, faces 0..3
+    const int4 *adj;         // per cell: neighbour across face f, -1 on the boundary
+    const uint32_t *nbrmap;  // per cell: 2 bits per (face f, vertex j): neighbour's vertex at j
+    const void *cellk;       // Real[3] per cell: V/20, sigma_t V/20, 2 sigma_t V/20
+    const void *iso;         // Real, phi layout: isotropic total source (nullable)
+    const double *qang;      // angular source, psi layout, FP64 only (nullable)
+    void *psi;               // Real, psi layout
+    uint32_t A, G;
+};
+
+// Launches the wavefront kernel over items [begin, end) with `tpi` threads
+// per item (1, 2, 4, 8 or 16).
+template <typename Real>
+cudaError_t launch_level(int tpi, const LevelArgs &p, uint64_t begin, uint64_t end, cudaStream_t s);
+
+}  // namespace tycho

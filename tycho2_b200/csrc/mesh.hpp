@@ -1,0 +1,66 @@
+// Host-side mesh ingest for the B200 sweep.
+//
+// Reads tycho2's one-partition .pmesh files (format: src/ParallelMesh.hh:43-81
+// in the reference) and derives the same per-cell tables that the reference's
+// TychoMesh builds (src/TychoMeshIO.cc:153-333, src/TychoMesh.cc:193-260),
+// bit for bit.  Also writes .smesh/.pmesh and generates the Kuhn-split cube
+// meshes used by the benchmark problems.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace tycho {
+
+constexpr uint64_t kNone = UINT64_MAX;  // boundary marker (TychoMesh::BOUNDARY_FACE)
+
+// Raw mesh records, shared by the .smesh and .pmesh formats.
+struct MeshRecords {
+    uint64_t n_cells = 0, n_faces = 0, n_nodes = 0;
+    std::vector<uint64_t> cell_faces;   // (c,4) bounding faces, file order
+    std::vector<uint64_t> cell_nodes;   // (c,4)
+    std::vector<uint64_t> cell_material;
+    std::vector<uint64_t> cell_gid;     // global id (identity for one partition)
+    std::vector<uint64_t> face_cells;   // (f,2), second = kNone on the boundary
+    std::vector<uint64_t> face_nodes;   // (f,3)
+    std::vector<uint64_t> face_btype;   // 0 mesh boundary, 1 partition boundary, 2 interior
+    std::vector<double> coords;         // (node,3)
+};
+
+// The TychoMesh tables the sweep needs, all row-major [cell][face][...].
+struct MeshTables {
+    uint64_t n_cells = 0, n_nodes = 0, n_sides = 0;
+    std::vector<uint64_t> adj_cell;        // (c,4)    kNone on the boundary
+    std::vector<uint64_t> adj_face;        // (c,4)
+    std::vector<uint64_t> side;            // (c,4)    kNone when interior
+    std::vector<uint64_t> face_to_cell;    // (c,4,3)  faceToCellVrtx
+    std::vector<uint64_t> cell_to_face;    // (c,4,4)  cellToFaceVrtx, kNone at [c][f][f]
+    std::vector<uint64_t> neighbor_vrtx;   // (c,4,3)
+    std::vector<uint64_t> cell_nodes;      // (c,4)
+    std::vector<uint64_t> cell_gid;        // c -> global cell id (.psi order)
+    std::vector<uint64_t> cell_material;
+    std::vector<double> coords;            // (node,3)
+    std::vector<double> volume;            // c
+    std::vector<double> area;              // (c,4)
+    std::vector<double> normal;            // (c,4,3) outward unit normals
+};
+
+// Status codes shared with the C ABI (see include/tycho_cuda.h).
+int read_smesh(const std::string &path, MeshRecords &out, std::string &err);
+int write_smesh(const std::string &path, const MeshRecords &m, std::string &err);
+int read_pmesh(const std::string &path, MeshRecords &out, std::string &err);
+int write_pmesh(const std::string &path, const MeshRecords &m, std::string &err);
+
+// Adds the partition-0 fields (global ids, boundary types) that a one-partition
+// .pmesh carries, as the reference's PartitionColumns 1 1 would.
+void make_single_partition(MeshRecords &m);
+
+// Unit-cube-like mesh: n^3 hexes of side length/n, each split into 6 Kuhn tets
+// around its (0,0,0)-(1,1,1) diagonal; interior vertices moved by
+// U(-jitter*h, +jitter*h) per coordinate from a seeded generator.
+void kuhn_cube(uint32_t n, double jitter, uint64_t seed, double length, MeshRecords &out);
+
+int build_tables(const MeshRecords &m, MeshTables &t, std::string &err);
+
+}  // namespace tycho

@@ -1,0 +1,53 @@
+// Quadrature and the wavefront schedule of the sweep.
+//
+// The reference walks each direction's cell dependency graph dynamically with
+// per-thread priority queues (src/GraphTraverser.cc:467-759).  Here every
+// (cell, angle) pair is levelled once: its t-level is the length of the
+// longest upwind chain that ends at it, so all pairs of one level depend only
+// on pairs of lower levels and can be updated together.  Items of a level are
+// stored contiguously, in increasing (cell*A + angle) order, which is the psi
+// row order, so neighbouring items write neighbouring psi rows.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "mesh.hpp"
+
+namespace tycho {
+
+struct Quadrature {
+    int sn_order = 0;
+    int n_angles = 0;
+    std::vector<double> xi, eta, mu, wt;
+};
+
+// Product Gauss-Legendre x Chebyshev set (src/Quadrature.cc:150-244).
+int make_quadrature(int sn_order, Quadrature &q, std::string &err);
+
+struct Schedule {
+    uint32_t n_levels = 0;
+    std::vector<uint64_t> level_offset;  // n_levels + 1 offsets into items
+    std::vector<uint32_t> items;         // cell*A + angle, grouped by level
+    std::vector<uint32_t> tlevel;        // (angle, cell)
+    uint64_t n_incoming_interior = 0;    // sum over items of incoming interior faces
+};
+
+// omega.n with the reference's operation order (src/TychoMesh.cc:212-223).
+inline double omega_dot_n(const Quadrature &q, int a, const double *n)
+{
+    return q.xi[a] * n[0] + q.eta[a] * n[1] + q.mu[a] * n[2];
+}
+
+// Levels every (cell, angle) pair.  Fails with kErrCycle if some direction's
+// graph has a cycle (the reference would spin forever on such a mesh).
+int build_schedule(const MeshTables &t, const Quadrature &q, Schedule &s, std::string &err);
+
+// Dependency counts as the GraphTraverser constructor sets them
+// (src/GraphTraverser.cc:442-458) and b-levels as Priorities' BLevelData
+// computes them (src/Priorities.cc:59-164); (angle, cell) order.
+void dependency_counts(const MeshTables &t, const Quadrature &q, std::vector<uint32_t> &deps);
+void b_levels(const MeshTables &t, const Quadrature &q, const Schedule &s, std::vector<uint32_t> &blev);
+
+}  // namespace tycho

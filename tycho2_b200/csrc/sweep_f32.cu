@@ -1,0 +1,10 @@
+// FP32 instantiation of the wavefront kernel (mixed-precision sweeps).
+// Compiled with FMA contraction on: this path is checked against the FP64
+// sweep by tolerance, not bit for bit.
+#include "sweep_kernels.cuh"
+
+namespace tycho {
+
+template cudaError_t launch_level<float>(int, const LevelArgs &, uint64_t, uint64_t, cudaStream_t);
+
+}  // namespace tycho

@@ -1,0 +1,517 @@
+// Device-resident sweep instance and its outer solvers.
+//
+// Reference call structure mirrored here:
+//   SweeperTraverse::sweep            -> Sweeper::apply / Sweeper::sweep_host
+//   SourceIteration::fixedPoint       -> Sweeper::solve, method 0
+//   SourceIteration::krylov (+PETSc)  -> Sweeper::solve, method 1 (own GMRES)
+//   FP32-sweep GMRES in FP64 iterative refinement -> method 2
+// (src/SweeperTraverse.cc:65-89, src/SourceIteration.cc:76-285).
+#include "sweeper.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "status.hpp"
+
+namespace tycho {
+
+#define TY_CUDA(expr)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (expr);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            err = std::string(#expr) + ": " + cudaGetErrorString(e_);                  \
+            return e_ == cudaErrorMemoryAllocation ? kErrOom : kErrCuda;               \
+        }                                                                              \
+    } while (0)
+
+#define TY_CHECK(expr)                  \
+    do {                                \
+        int s_ = (expr);                \
+        if (s_ != kOk) return s_;       \
+    } while (0)
+
+namespace {
+
+template <typename T>
+cudaError_t upload(T *&dst, const T *src, size_t n, cudaStream_t s)
+{
+    cudaError_t e = cudaMalloc(&dst, sizeof(T) * std::max<size_t>(n, 1));
+    if (e != cudaSuccess) return e;
+    if (n) e = cudaMemcpyAsync(dst, src, sizeof(T) * n, cudaMemcpyHostToDevice, s);
+    return e;
+}
+
+int auto_tpi(int G, bool fp32)
+{
+    if (fp32) return G >= 16 ? 8 : (G >= 8 ? 4 : (G >= 4 ? 2 : 1));
+    return G >= 16 ? 4 : (G >= 8 ? 2 : 1);
+}
+
+}  // namespace
+
+Sweeper::~Sweeper()
+{
+    if (device_ >= 0) cudaSetDevice(device_);
+    for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+    void *bufs[] = {d_items_, d_abar64_, d_abar32_, d_adj_, d_nbrmap_, d_cellk64_, d_cellk32_,
+                    d_w_, d_sigs_, d_scat_, d_qiso_, d_qang_, d_src_, d_iso_, d_iso32_, d_psi_,
+                    d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    reducer_free(red_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err)
+{
+    if (o.n_groups < 1 || o.n_groups > 64) { err = "nGroups must be in 1..64"; return kErrArg; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        err = "no CUDA device: the B200 sweep has no CPU fallback";
+        return kErrCuda;
+    }
+    if (o.device < 0 || o.device >= ndev) { err = "bad device ordinal"; return kErrArg; }
+    device_ = o.device;
+    TY_CUDA(cudaSetDevice(device_));
+    TY_CHECK(make_quadrature(o.sn_order, quad_, err));
+    tables_ = t;
+    nc_ = t.n_cells;
+    A_ = quad_.n_angles;
+    G_ = o.n_groups;
+    fp32_ = o.fp32;
+    tpi64_ = o.tpi64 ? o.tpi64 : auto_tpi(G_, false);
+    tpi32_ = o.tpi32 ? o.tpi32 : auto_tpi(G_, true);
+    for (int tp : {tpi64_, tpi32_})
+        if (tp != 1 && tp != 2 && tp != 4 && tp != 8 && tp != 16) {
+            err = "threads per item must be 1, 2, 4, 8 or 16";
+            return kErrArg;
+        }
+    TY_CHECK(build_schedule(tables_, quad_, sched_, err));
+    TY_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+
+    // Per-cell topology: neighbours and, per (face, local vertex), the
+    // neighbour's vertex index (neighborVrtx o cellToFaceVrtx).
+    std::vector<int4> adj(nc_);
+    std::vector<uint32_t> nmap(nc_, 0);
+    for (uint64_t c = 0; c < nc_; ++c) {
+        int a4[4];
+        for (int f = 0; f < 4; ++f) {
+            uint64_t n = t.adj_cell[c * 4 + f];
+            a4[f] = n == kNone ? -1 : (int)n;
+            if (n == kNone) continue;
+            for (int j = 0; j < 4; ++j) {
+                if (j == f) continue;
+                uint64_t fv = t.cell_to_face[(c * 4 + f) * 4 + j];
+                uint64_t nv = t.neighbor_vrtx[(c * 4 + f) * 3 + fv];
+                nmap[c] |= (uint32_t)(nv & 3u) << ((f * 4 + j) * 2);
+            }
+        }
+        adj[c] = make_int4(a4[0], a4[1], a4[2], a4[3]);
+    }
+    if (nc_ >= (1ull << 31)) { err = "too many cells"; return kErrArg; }
+    const uint64_t nitems = sched_.items.size();
+    TY_CUDA(upload(d_items_, sched_.items.data(), nitems, stream_));
+    TY_CUDA(upload(d_adj_, adj.data(), nc_, stream_));
+    TY_CUDA(upload(d_nbrmap_, nmap.data(), nc_, stream_));
+    TY_CUDA(upload(d_w_, quad_.wt.data(), (size_t)A_, stream_));
+    {
+        std::vector<double> omega(3 * (size_t)A_);
+        std::copy(quad_.xi.begin(), quad_.xi.end(), omega.begin());
+        std::copy(quad_.eta.begin(), quad_.eta.end(), omega.begin() + A_);
+        std::copy(quad_.mu.begin(), quad_.mu.end(), omega.begin() + 2 * A_);
+        double *d_omega = nullptr, *d_normal = nullptr, *d_area = nullptr;
+        TY_CUDA(upload(d_omega, omega.data(), omega.size(), stream_));
+        TY_CUDA(upload(d_normal, t.normal.data(), t.normal.size(), stream_));
+        TY_CUDA(upload(d_area, t.area.data(), t.area.size(), stream_));
+        TY_CUDA(cudaMalloc(&d_abar64_, sizeof(double4) * std::max<uint64_t>(nitems, 1)));
+        if (fp32_) TY_CUDA(cudaMalloc(&d_abar32_, sizeof(float4) * std::max<uint64_t>(nitems, 1)));
+        TY_CUDA(launch_item_abar(d_items_, nitems, A_, d_normal, d_area, d_omega, d_abar64_,
+                                 d_abar32_, stream_));
+        TY_CUDA(cudaStreamSynchronize(stream_));
+        cudaFree(d_omega); cudaFree(d_normal); cudaFree(d_area);
+    }
+    const size_t nphi = phi_size(), npsi = psi_size();
+    TY_CUDA(cudaMalloc(&d_psi_, sizeof(double) * std::max<size_t>(npsi, 1)));
+    TY_CUDA(cudaMemsetAsync(d_psi_, 0, sizeof(double) * npsi, stream_));
+    TY_CUDA(cudaMalloc(&d_iso_, sizeof(double) * nphi));
+    if (fp32_) TY_CUDA(cudaMalloc(&d_iso32_, sizeof(float) * nphi));
+    TY_CUDA(cudaMalloc(&d_phi_, sizeof(double) * nphi));
+    TY_CUDA(cudaMalloc(&d_r_, sizeof(double) * nphi));
+    TY_CUDA(cudaMalloc(&d_tmp_, sizeof(double) * nphi));
+    TY_CUDA(cudaMemsetAsync(d_phi_, 0, sizeof(double) * nphi, stream_));
+    TY_CUDA(cudaMalloc(&d_cellk64_, sizeof(double) * 3 * nc_));
+    if (fp32_) TY_CUDA(cudaMalloc(&d_cellk32_, sizeof(float) * 3 * nc_));
+    TY_CUDA(cudaMalloc(&d_sigs_, sizeof(double) * nc_));
+    TY_CUDA(reducer_init(red_));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    return kOk;
+}
+
+int Sweeper::set_cross_sections(const double *sigma_t, const double *sigma_s, const double *scatter,
+                                std::string &err)
+{
+    if (!sigma_t || !sigma_s) { err = "sigma_t and sigma_s are required"; return kErrArg; }
+    TY_CUDA(cudaSetDevice(device_));
+    std::vector<double> k64(3 * nc_);
+    std::vector<float> k32(3 * nc_);
+    for (uint64_t c = 0; c < nc_; ++c) {
+        const double volume = tables_.volume[c], sigma = sigma_t[c];
+        if (!(sigma >= 0.0) || !std::isfinite(sigma)) { err = "sigma_t must be finite and >= 0"; return kErrArg; }
+        // Transport.cc:66-69 and :84-102 with the reference's grouping.
+        k64[3 * c + 0] = volume / 20.0;
+        k64[3 * c + 1] = 1.0 * sigma * volume / 20.0;
+        k64[3 * c + 2] = 2.0 * sigma * volume / 20.0;
+        for (int i = 0; i < 3; ++i) k32[3 * c + i] = (float)k64[3 * c + i];
+    }
+    TY_CUDA(cudaMemcpyAsync(d_cellk64_, k64.data(), sizeof(double) * k64.size(), cudaMemcpyHostToDevice, stream_));
+    if (d_cellk32_)
+        TY_CUDA(cudaMemcpyAsync(d_cellk32_, k32.data(), sizeof(float) * k32.size(), cudaMemcpyHostToDevice, stream_));
+    TY_CUDA(cudaMemcpyAsync(d_sigs_, sigma_s, sizeof(double) * nc_, cudaMemcpyHostToDevice, stream_));
+    if (scatter) {
+        if (!d_scat_) TY_CUDA(cudaMalloc(&d_scat_, sizeof(double) * G_ * G_));
+        TY_CUDA(cudaMemcpyAsync(d_scat_, scatter, sizeof(double) * G_ * G_, cudaMemcpyHostToDevice, stream_));
+    } else if (d_scat_) {
+        cudaFree(d_scat_);
+        d_scat_ = nullptr;
+    }
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    have_xs_ = true;
+    return kOk;
+}
+
+int Sweeper::set_source(int kind, const double *q, std::string &err)
+{
+    TY_CUDA(cudaSetDevice(device_));
+    if (kind != 0 && kind != 1) { err = "source kind must be 0 (angular) or 1 (isotropic)"; return kErrArg; }
+    double *&dst = kind == 0 ? d_qang_ : d_qiso_;
+    const size_t n = kind == 0 ? psi_size() : phi_size();
+    if (!q) {
+        if (dst) cudaFree(dst);
+        dst = nullptr;
+        return kOk;
+    }
+    if (!dst) TY_CUDA(cudaMalloc(&dst, sizeof(double) * n));
+    TY_CUDA(cudaMemcpyAsync(dst, q, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    return kOk;
+}
+
+int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg, cudaEvent_t end,
+                    std::string &err)
+{
+    auto key = std::make_tuple(prec, has_iso, qang);
+    auto it = graphs_.find(key);
+    if (it == graphs_.end()) {
+        LevelArgs p;
+        p.items = d_items_;
+        p.abar = prec ? (const void *)d_abar32_ : (const void *)d_abar64_;
+        p.adj = d_adj_;
+        p.nbrmap = d_nbrmap_;
+        p.cellk = prec ? (const void *)d_cellk32_ : (const void *)d_cellk64_;
+        p.iso = has_iso ? (prec ? (const void *)d_iso32_ : (const void *)d_iso_) : nullptr;
+        p.qang = qang;
+        p.psi = d_psi_;
+        p.A = (uint32_t)A_;
+        p.G = (uint32_t)G_;
+        cudaGraph_t graph;
+        TY_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        cudaError_t le = cudaSuccess;
+        for (uint32_t l = 0; l < sched_.n_levels && le == cudaSuccess; ++l) {
+            const uint64_t b = sched_.level_offset[l], e = sched_.level_offset[l + 1];
+            le = prec ? launch_level<float>(tpi32_, p, b, e, stream_)
+                      : launch_level<double>(tpi64_, p, b, e, stream_);
+        }
+        cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
+        TY_CUDA(le);
+        TY_CUDA(ce);
+        cudaGraphExec_t exec;
+        cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        TY_CUDA(ie);
+        it = graphs_.emplace(key, exec).first;
+    }
+    if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
+    TY_CUDA(cudaGraphLaunch(it->second, stream_));
+    if (end) TY_CUDA(cudaEventRecord(end, stream_));
+    return kOk;
+}
+
+static thread_local cudaEvent_t tl_level_beg = nullptr, tl_level_end = nullptr;
+
+int Sweeper::apply(int prec, const double *phi_in, bool with_fixed, double *phi_out,
+                   const double *qang_override, std::string &err)
+{
+    if (!have_xs_) { err = "cross sections not set"; return kErrMissing; }
+    if (prec == 1 && !fp32_) { err = "sweeper was created without the FP32 sweep"; return kErrArg; }
+    const double *qang = qang_override ? qang_override : (with_fixed ? d_qang_ : nullptr);
+    if (prec == 1 && qang) { err = "the FP32 sweep takes isotropic sources only"; return kErrArg; }
+    const double *qfix = with_fixed ? d_qiso_ : nullptr;
+    const bool has_iso = phi_in != nullptr || qfix != nullptr;
+    if (has_iso)
+        TY_CUDA(launch_scatter_source(phi_in, qfix, d_sigs_, d_scat_, d_iso_, prec ? d_iso32_ : nullptr,
+                                      nc_, (uint32_t)G_, stream_));
+    TY_CHECK(levels(prec, has_iso, qang, tl_level_beg, tl_level_end, err));
+    if (phi_out) TY_CUDA(launch_psi_to_phi(d_psi_, prec == 1, d_w_, phi_out, nc_, (uint32_t)A_, (uint32_t)G_, stream_));
+    last_psi_prec_ = prec;
+    return kOk;
+}
+
+int Sweeper::sweep_host(const double *source, double *psi, std::string &err)
+{
+    if (!source || !psi) { err = "source and psi are required"; return kErrArg; }
+    TY_CUDA(cudaSetDevice(device_));
+    const size_t n = psi_size();
+    if (!d_src_) TY_CUDA(cudaMalloc(&d_src_, sizeof(double) * n));
+    TY_CUDA(cudaMemcpyAsync(d_src_, source, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
+    TY_CHECK(apply(0, nullptr, false, nullptr, d_src_, err));
+    TY_CUDA(cudaMemcpyAsync(psi, d_psi_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    return kOk;
+}
+
+int Sweeper::ensure_krylov(int m, std::string &err)
+{
+    if (m < 1 || m > 60) { err = "GMRES restart must be in 1..60"; return kErrArg; }
+    if (krylov_m_ >= m) return kOk;
+    if (d_V_) cudaFree(d_V_);
+    d_V_ = nullptr;
+    TY_CUDA(cudaMalloc(&d_V_, sizeof(double) * phi_size() * (m + 1)));
+    if (!d_h_) TY_CUDA(cudaMalloc(&d_h_, sizeof(double) * 64));
+    krylov_m_ = m;
+    return kOk;
+}
+
+// Restarted GMRES(m) on (I - K) x = b, K = D L^{-1} M S swept in `prec`,
+// x starting at 0.  Classical Gram-Schmidt applied twice, Givens rotations
+// on the host, stop when the residual estimate <= rtol ||b||; the true
+// residual is recomputed at each restart.
+int Sweeper::gmres(int prec, const double *b, double *x, int m, double rtol, int iter_max, int &its,
+                   double &rnorm, SolveStats &st, std::string &err)
+{
+    TY_CHECK(ensure_krylov(m, err));
+    const uint64_t n = phi_size();
+    double *V = d_V_;
+    its = 0;
+    TY_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream_));
+    TY_CUDA(multi_dot(b, b, n, 1, n, red_, stream_));
+    const double bnorm = std::sqrt(red_.host[0]);
+    rnorm = bnorm;
+    if (bnorm == 0.0) return kOk;
+    TY_CUDA(cudaMemcpyAsync(V, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+    double beta = bnorm;
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    for (;;) {
+        if (beta <= rtol * bnorm || its >= iter_max) { rnorm = beta; break; }
+        TY_CUDA(axpby(1.0 / beta, V, 0.0, V, n, stream_));
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int k = 0;
+        bool converged = false;
+        double est = beta;
+        for (; k < m && its < iter_max;) {
+            double *vk = V + (size_t)k * n, *w = V + (size_t)(k + 1) * n;
+            TY_CHECK(apply(prec, vk, false, w, nullptr, err));
+            (prec ? st.sweeps_fp32 : st.sweeps_fp64)++;
+            TY_CUDA(sub_from(vk, w, n, stream_));
+            for (int j = 0; j <= k; ++j) H[(size_t)j * m + k] = 0.0;
+            for (int pass = 0; pass < 2; ++pass) {
+                TY_CUDA(multi_dot(w, V, n, k + 1, n, red_, stream_));
+                for (int j = 0; j <= k; ++j) H[(size_t)j * m + k] += red_.host[j];
+                TY_CUDA(multi_axpy(w, V, n, red_.result, k + 1, n, stream_));
+            }
+            TY_CUDA(multi_dot(w, w, n, 1, n, red_, stream_));
+            const double hn = std::sqrt(red_.host[0]);
+            H[(size_t)(k + 1) * m + k] = hn;
+            if (hn > 0.0) TY_CUDA(axpby(1.0 / hn, w, 0.0, w, n, stream_));
+            for (int j = 0; j < k; ++j) {
+                const double h0 = H[(size_t)j * m + k], h1 = H[(size_t)(j + 1) * m + k];
+                H[(size_t)j * m + k] = cs[j] * h0 + sn[j] * h1;
+                H[(size_t)(j + 1) * m + k] = -sn[j] * h0 + cs[j] * h1;
+            }
+            const double hk = H[(size_t)k * m + k];
+            const double den = std::hypot(hk, hn);
+            cs[k] = den > 0 ? hk / den : 1.0;
+            sn[k] = den > 0 ? hn / den : 0.0;
+            H[(size_t)k * m + k] = den;
+            g[k + 1] = -sn[k] * g[k];
+            g[k] = cs[k] * g[k];
+            est = std::fabs(g[k + 1]);
+            ++its;
+            ++k;
+            if (est <= rtol * bnorm || hn == 0.0) { converged = true; break; }
+        }
+        for (int i = k - 1; i >= 0; --i) {
+            double s = g[i];
+            for (int j = i + 1; j < k; ++j) s -= H[(size_t)i * m + j] * y[j];
+            y[i] = s / H[(size_t)i * m + i];
+        }
+        std::vector<double> negy(k);
+        for (int j = 0; j < k; ++j) negy[j] = -y[j];
+        TY_CUDA(cudaMemcpyAsync(d_h_, negy.data(), sizeof(double) * k, cudaMemcpyHostToDevice, stream_));
+        TY_CUDA(multi_axpy(x, V, n, d_h_, k, n, stream_));
+        if (converged || its >= iter_max) {
+            rnorm = est;
+            TY_CUDA(cudaStreamSynchronize(stream_));
+            break;
+        }
+        // True residual r = b - (x - K x) into V_0.
+        TY_CHECK(apply(prec, x, false, V, nullptr, err));
+        (prec ? st.sweeps_fp32 : st.sweeps_fp64)++;
+        TY_CUDA(sub_from(x, V, n, stream_));
+        TY_CUDA(sub_from(b, V, n, stream_));
+        TY_CUDA(multi_dot(V, V, n, 1, n, red_, stream_));
+        beta = std::sqrt(red_.host[0]);
+    }
+    return kOk;
+}
+
+int Sweeper::solve(const SolveOptions &o, double *phi_out, double *psi_out, SolveStats &st,
+                   std::string &err)
+{
+    TY_CUDA(cudaSetDevice(device_));
+    st = SolveStats();
+    const uint64_t n = phi_size();
+    cudaEvent_t e0, e1;
+    TY_CUDA(cudaEventCreate(&e0));
+    TY_CUDA(cudaEventCreate(&e1));
+    TY_CUDA(cudaEventRecord(e0, stream_));
+    double *result = nullptr;  // phi consistent with the resident psi
+    int status = kOk;
+    if (o.method == 0) {
+        // SourceIteration::fixedPoint: L1 relative change of phi.
+        TY_CUDA(cudaMemsetAsync(d_phi_, 0, sizeof(double) * n, stream_));
+        int iter = 0;
+        double error = 1.0;
+        while (iter < o.iter_max && error > o.err_max) {
+            TY_CUDA(cudaMemcpyAsync(d_tmp_, d_phi_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+            TY_CHECK(apply(0, d_tmp_, true, d_phi_, nullptr, err));
+            st.sweeps_fp64++;
+            TY_CUDA(l1_pair(d_phi_, d_tmp_, n, red_, stream_));
+            error = red_.host[0] / red_.host[1];
+            ++iter;
+        }
+        st.iterations = iter;
+        st.final_error = error;
+        result = d_phi_;
+    } else if (o.method == 1) {
+        // SourceIteration::krylov: b = D L^{-1} Q, GMRES, psi = L^{-1}(MS phi + Q).
+        TY_CHECK(apply(0, nullptr, true, d_r_, nullptr, err));
+        st.sweeps_fp64++;
+        int its = 0;
+        double rn = 0;
+        TY_CHECK(gmres(0, d_r_, d_phi_, o.restart, o.err_max, o.iter_max, its, rn, st, err));
+        TY_CUDA(multi_dot(d_r_, d_r_, n, 1, n, red_, stream_));
+        const double bnorm = std::sqrt(red_.host[0]);
+        TY_CHECK(apply(0, d_phi_, true, d_tmp_, nullptr, err));
+        st.sweeps_fp64++;
+        st.iterations = its;
+        st.final_error = bnorm > 0 ? rn / bnorm : 0.0;
+        result = d_tmp_;
+    } else if (o.method == 2) {
+        // FP64 iterative refinement: r = T(phi) - phi with one FP64 sweep,
+        // correction (I - K32) delta = r by FP32-sweep GMRES, phi += delta.
+        if (!fp32_) { err = "mixed precision needs a sweeper created with fp32"; return kErrArg; }
+        if (d_qang_) { err = "mixed precision takes an isotropic fixed source"; return kErrArg; }
+        TY_CUDA(cudaMemsetAsync(d_phi_, 0, sizeof(double) * n, stream_));
+        double bnorm = 0.0, rnorm = 0.0;
+        int ref = 0;
+        for (;;) {
+            TY_CHECK(apply(0, d_phi_, true, d_tmp_, nullptr, err));
+            st.sweeps_fp64++;
+            TY_CUDA(cudaMemcpyAsync(d_r_, d_tmp_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+            TY_CUDA(axpby(-1.0, d_phi_, 1.0, d_r_, n, stream_));
+            TY_CUDA(multi_dot(d_r_, d_r_, n, 1, n, red_, stream_));
+            rnorm = std::sqrt(red_.host[0]);
+            if (ref == 0) bnorm = rnorm;
+            if (rnorm <= o.err_max * bnorm || ref >= o.refine_max || st.iterations >= o.iter_max) break;
+            int its = 0;
+            double rn = 0;
+            TY_CHECK(gmres(1, d_r_, d_tmp_, o.restart, o.inner_tol, o.iter_max - st.iterations, its, rn, st, err));
+            st.iterations += its;
+            TY_CUDA(axpby(1.0, d_tmp_, 1.0, d_phi_, n, stream_));
+            ++ref;
+        }
+        // psi is the FP64 sweep of the last residual; its phi is T(phi) (d_tmp_).
+        st.refinements = ref;
+        st.final_error = bnorm > 0 ? rnorm / bnorm : 0.0;
+        result = d_tmp_;
+    } else {
+        err = "unknown method";
+        return kErrArg;
+    }
+    TY_CUDA(cudaEventRecord(e1, stream_));
+    TY_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    st.seconds = ms * 1e-3;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (result != d_phi_) TY_CUDA(cudaMemcpyAsync(d_phi_, result, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+    if (phi_out) TY_CUDA(cudaMemcpyAsync(phi_out, d_phi_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
+    if (psi_out) TY_CUDA(cudaMemcpyAsync(psi_out, d_psi_, sizeof(double) * psi_size(), cudaMemcpyDeviceToHost, stream_));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    if (status == kErrNotConverged) err = "iteration limit reached before the tolerance";
+    return status;
+}
+
+int Sweeper::write_psi(const std::string &path, std::string &err)
+{
+    if (last_psi_prec_ != 0) { err = "no FP64 psi resident (run a solve or an FP64 sweep first)"; return kErrMissing; }
+    TY_CUDA(cudaSetDevice(device_));
+    std::vector<double> psi(psi_size());
+    TY_CUDA(cudaMemcpyAsync(psi.data(), d_psi_, sizeof(double) * psi.size(), cudaMemcpyDeviceToHost, stream_));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    FILE *fp = std::fopen(path.c_str(), "wb");
+    if (!fp) { err = "cannot open " + path; return kErrIO; }
+    // PsiData::writeToFile (src/PsiData.cc:62-106): 32-byte name, version 1,
+    // cells, angles, groups, then psi cell by cell at global offsets.
+    char name[32] = "Tycho 2 Psi Output";
+    uint64_t hdr[4] = {1, nc_, (uint64_t)A_, (uint64_t)G_};
+    bool ok = std::fwrite(name, 1, 32, fp) == 32 && std::fwrite(hdr, 8, 4, fp) == 4;
+    const size_t per = (size_t)A_ * 4 * G_;
+    for (uint64_t c = 0; c < nc_ && ok; ++c) {
+        ok = std::fseek(fp, (long)(64 + tables_.cell_gid[c] * per * 8), SEEK_SET) == 0 &&
+             std::fwrite(&psi[c * per], 8, per, fp) == per;
+    }
+    std::fclose(fp);
+    if (!ok) { err = "write failed: " + path; return kErrIO; }
+    return kOk;
+}
+
+int Sweeper::time_sweeps(int prec, int n, bool flush_l2, double *ms, std::string &err)
+{
+    TY_CUDA(cudaSetDevice(device_));
+    if (n < 1) { err = "n must be >= 1"; return kErrArg; }
+    const size_t flush_bytes = 256ull << 20;  // > 126 MB L2
+    if (flush_l2 && !d_flush_) TY_CUDA(cudaMalloc(&d_flush_, flush_bytes));
+    cudaEvent_t e0, e1, l0, l1;
+    TY_CUDA(cudaEventCreate(&e0));
+    TY_CUDA(cudaEventCreate(&e1));
+    TY_CUDA(cudaEventCreate(&l0));
+    TY_CUDA(cudaEventCreate(&l1));
+    double tot = 0, lvl = 0;
+    int status = kOk;
+    for (int i = 0; i < n && status == kOk; ++i) {
+        if (flush_l2) TY_CUDA(cudaMemsetAsync(d_flush_, i & 0xff, flush_bytes, stream_));
+        TY_CUDA(cudaEventRecord(e0, stream_));
+        tl_level_beg = l0;
+        tl_level_end = l1;
+        status = apply(prec, d_phi_, true, d_r_, nullptr, err);
+        tl_level_beg = tl_level_end = nullptr;
+        TY_CUDA(cudaEventRecord(e1, stream_));
+        TY_CUDA(cudaEventSynchronize(e1));
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, e0, e1);
+        cudaEventElapsedTime(&b, l0, l1);
+        tot += a;
+        lvl += b;
+    }
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(l0); cudaEventDestroy(l1);
+    ms[0] = tot / n;
+    ms[1] = lvl / n;
+    return status;
+}
+
+}  // namespace tycho

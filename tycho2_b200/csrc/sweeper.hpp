@@ -1,0 +1,113 @@
+// Device-resident sweep instance: mesh tables, wavefront schedule, psi and
+// the outer solvers (source iteration, GMRES, mixed-precision refinement).
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "device_ops.hpp"
+#include "mesh.hpp"
+#include "schedule.hpp"
+
+namespace tycho {
+
+struct SweeperOptions {
+    int sn_order = 4;
+    int n_groups = 1;
+    int device = 0;
+    bool fp32 = false;
+    int tpi64 = 0;  // 0 = auto
+    int tpi32 = 0;
+};
+
+struct SolveOptions {
+    int method = 0;  // 0 SI, 1 GMRES, 2 mixed
+    int iter_max = 100;
+    double err_max = 1e-10;
+    int restart = 20;
+    double inner_tol = 1e-5;
+    int refine_max = 10;
+};
+
+struct SolveStats {
+    int iterations = 0, sweeps_fp64 = 0, sweeps_fp32 = 0, refinements = 0;
+    double final_error = 0.0, seconds = 0.0;
+};
+
+class Sweeper {
+public:
+    ~Sweeper();
+    int init(const MeshTables &t, const SweeperOptions &o, std::string &err);
+
+    int set_cross_sections(const double *sigma_t, const double *sigma_s, const double *scatter,
+                           std::string &err);
+    int set_source(int kind, const double *q, std::string &err);
+    int sweep_host(const double *source, double *psi, std::string &err);
+    int solve(const SolveOptions &o, double *phi_out, double *psi_out, SolveStats &st,
+              std::string &err);
+    int write_psi(const std::string &path, std::string &err);
+    int time_sweeps(int precision, int n, bool flush_l2, double *ms, std::string &err);
+
+    // One operator application, on the device:
+    //   phi_out = D L^{-1} ( [Q] + M S phi_in )     (phi_in / phi_out nullable)
+    // prec 0 = FP64, 1 = FP32.  qang overrides the angular fixed source.
+    int apply(int prec, const double *phi_in, bool with_fixed, double *phi_out,
+              const double *qang_override, std::string &err);
+
+    const MeshTables &tables() const { return tables_; }
+    const Quadrature &quadrature() const { return quad_; }
+    const Schedule &schedule() const { return sched_; }
+    uint64_t n_cells() const { return nc_; }
+    int n_angles() const { return A_; }
+    int n_groups() const { return G_; }
+    uint64_t phi_size() const { return nc_ * 4 * (uint64_t)G_; }
+    uint64_t psi_size() const { return nc_ * (uint64_t)A_ * 4 * G_; }
+    cudaStream_t stream() const { return stream_; }
+    int tpi(int prec) const { return prec ? tpi32_ : tpi64_; }
+
+private:
+    int levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg, cudaEvent_t end,
+               std::string &err);
+    int gmres(int prec, const double *b, double *x, int restart, double rtol, int iter_max,
+              int &its, double &rnorm, SolveStats &st, std::string &err);
+    int ensure_krylov(int restart, std::string &err);
+
+    MeshTables tables_;
+    Quadrature quad_;
+    Schedule sched_;
+    uint64_t nc_ = 0;
+    int A_ = 0, G_ = 0, device_ = 0, tpi64_ = 1, tpi32_ = 1;
+    bool fp32_ = false, have_xs_ = false;
+    int last_psi_prec_ = -1;
+
+    cudaStream_t stream_ = nullptr;
+    uint32_t *d_items_ = nullptr;
+    double4 *d_abar64_ = nullptr;
+    float4 *d_abar32_ = nullptr;
+    int4 *d_adj_ = nullptr;
+    uint32_t *d_nbrmap_ = nullptr;
+    double *d_cellk64_ = nullptr;
+    float *d_cellk32_ = nullptr;
+    double *d_w_ = nullptr;
+    double *d_sigs_ = nullptr;
+    double *d_scat_ = nullptr;
+    double *d_qiso_ = nullptr;
+    double *d_qang_ = nullptr;
+    double *d_src_ = nullptr;     // staging for sweep_host's source
+    double *d_iso_ = nullptr;
+    float *d_iso32_ = nullptr;
+    void *d_psi_ = nullptr;
+    double *d_phi_ = nullptr, *d_r_ = nullptr, *d_tmp_ = nullptr;
+    double *d_V_ = nullptr, *d_h_ = nullptr;
+    int krylov_m_ = 0;
+    void *d_flush_ = nullptr;
+    Reducer red_;
+    std::map<std::tuple<int, bool, const double *>, cudaGraphExec_t> graphs_;
+};
+
+}  // namespace tycho

@@ -1,0 +1,91 @@
+"""Problem definitions (the reference's Problem namespace, src/Problem.cc)
+and the benchmark workloads.
+
+hat_source / hat_l2_error restate Problem::hatSource / hatL2Error
+(src/Problem.cc:47-134) for meshes on [0,100]^3.  The benchmark family
+(`workload`) extends the reference's two-material problem with per-cell
+lognormal sigma_t, a lower-triangular downscatter matrix and a box source,
+all drawn from seeded generators; q is the angular source density, the
+reference's convention (src/Problem.cc:73-75).
+"""
+import numpy as np
+
+CUBE_SIZE = 100.0
+
+
+def hat_source(mesh, quad, sigma_t, sigma_s, n_groups):
+    """Problem::hatSource (src/Problem.cc:47-82), psi layout."""
+    t = mesh.tables()
+    xyz = t["coords"][t["cell_nodes"].astype(np.int64)] - CUBE_SIZE / 2.0  # (c, v, 3)
+    x, y, z = xyz[..., 0][:, None, :], xyz[..., 1][:, None, :], xyz[..., 2][:, None, :]
+    xi, eta, mu = quad.xi[None, :, None], quad.eta[None, :, None], quad.mu[None, :, None]
+    r = np.sqrt(x * x + y * y + z * z)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        val = (-x / (30.0 * r) * xi - y / (30.0 * r) * eta - z / (30.0 * r) * mu
+               + (sigma_t - sigma_s)[:, None, None] * (1.0 - r / 30.0))
+    val = np.where(r <= 30.0, val, 0.0)
+    return np.ascontiguousarray(np.repeat(val[..., None], n_groups, axis=3))
+
+
+def hat_l2_error(mesh, psi):
+    """Problem::hatL2Error (src/Problem.cc:91-134)."""
+    t = mesh.tables()
+    xyz = (t["coords"][t["cell_nodes"].astype(np.int64)] - CUBE_SIZE / 2.0).mean(axis=1)
+    c = np.sqrt((xyz ** 2).sum(axis=1))
+    act = np.where(c <= 30.0, 1.0 - c / 30.0, 0.0)
+    val = psi.mean(axis=2)  # (c, a, g)
+    diff = val - act[:, None, None]
+    return float(np.sqrt((diff ** 2).sum() / (val ** 2).sum()))
+
+
+def downscatter_matrix(n_groups, ratio):
+    """Lower-triangular g' -> g matrix, row g split equally over g' <= g so
+    that each row sums to `ratio` (sigma_s = sigma_t * matrix)."""
+    m = np.zeros((n_groups, n_groups))
+    for g in range(n_groups):
+        m[g, : g + 1] = ratio / (g + 1)
+    return m
+
+
+# The workloads the benchmark and the parity tests run.
+WORKLOADS = {
+    # 8^3 hexes x 6 = 3,072 tets, S4, G=1, sigma_t=1, sigma_s=0.5, q=1, SI to 1e-10.
+    "kuhn8_s4_g1": dict(n=8, jitter=0.0, sn=4, groups=1, sigma="uniform", sigma_t=1.0,
+                        ratio=0.5, scatter="within", source="all", method="si", tol=1e-10),
+    # 32^3 x 6 = 196,608 tets, +-0.05h jitter, S8, G=8, lognormal(0,0.5) sigma_t,
+    # downscatter rows 0.6 sigma_t, q=1 in the central 1/8, GMRES(20) to 1e-10.
+    "kuhn32_s8_g8": dict(n=32, jitter=0.05, sn=8, groups=8, sigma="lognormal", lognormal_s=0.5,
+                         ratio=0.6, scatter="down", source="box", method="gmres", tol=1e-10,
+                         restart=20),
+    # 64^3 x 6 = 1,572,864 tets, S8, G=16, lognormal(0,1), ratio 0.99, GMRES(30).
+    "kuhn64_s8_g16": dict(n=64, jitter=0.05, sn=8, groups=16, sigma="lognormal", lognormal_s=1.0,
+                          ratio=0.99, scatter="down", source="box", method="mixed", tol=1e-10,
+                          restart=30),
+}
+
+
+def make_problem(n, jitter, sn, groups, sigma="uniform", sigma_t=1.0, lognormal_s=0.5,
+                 ratio=0.5, scatter="within", source="all", seed=1234, length=1.0, **_):
+    """Builds (mesh, sigma_t, sigma_s, scatter_matrix or None, q_iso)."""
+    from .sweeper import TychoMesh
+    mesh = TychoMesh.kuhn_cube(n, jitter, seed, length)
+    rng = np.random.default_rng(seed + 1)
+    nc = mesh.n_cells
+    if sigma == "uniform":
+        st = np.full(nc, float(sigma_t))
+    else:
+        st = np.exp(rng.normal(0.0, lognormal_s, nc))
+    if scatter == "within":
+        ss = ratio * st
+        mat = None
+    else:
+        ss = st.copy()
+        mat = downscatter_matrix(groups, ratio)
+    q = np.zeros((nc, 4, groups))
+    if source == "all":
+        q[:] = 1.0
+    else:
+        cen = mesh.centroids() / length
+        inside = np.all((cen >= 0.25) & (cen <= 0.75), axis=1)
+        q[inside] = 1.0
+    return mesh, st, ss, mat, q

@@ -1,0 +1,216 @@
+"""Host-side mirror of tycho2's sweeper interface over the C ABI.
+
+Names follow the reference so that callers read the same:
+  TychoMesh        src/TychoMesh.hh      (tables from .pmesh/.smesh or a Kuhn cube)
+  Quadrature       src/Quadrature.hh     (getXi/getEta/getMu/getWt)
+  SweeperCuda      src/SweeperAbstract.hh (sweep, solve, getPsi, writePsiToFile)
+Every call goes to libtycho_b200.so; errors raise TychoError with the
+library's status and message (the reference aborts through Insist).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import check, lib, ptr
+
+NONE = np.uint64(0xFFFFFFFFFFFFFFFF)  # TychoMesh::BOUNDARY_FACE
+
+GAUSS_ELIM = {"Original": 0, "NoPivot": 1}
+METHODS = {"si": 0, "gmres": 1, "mixed": 2}
+
+
+class TychoMesh:
+    """TychoMesh (src/TychoMesh.hh:52-159) built by the C++ host ingest."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+        nc, nn, ns = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(lib().tycho_mesh_info(self._h, C.byref(nc), C.byref(nn), C.byref(ns)))
+        self.n_cells, self.n_nodes, self.n_sides = nc.value, nn.value, ns.value
+        self._tables = None
+
+    @classmethod
+    def read_pmesh(cls, path):
+        h = C.c_void_p()
+        check(lib().tycho_mesh_read_pmesh(str(path).encode(), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def read_smesh(cls, path):
+        h = C.c_void_p()
+        check(lib().tycho_mesh_read_smesh(str(path).encode(), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def kuhn_cube(cls, n, jitter=0.0, seed=0, length=1.0):
+        h = C.c_void_p()
+        check(lib().tycho_mesh_kuhn_cube(n, jitter, seed, length, C.byref(h)))
+        return cls(h.value)
+
+    def write_smesh(self, path):
+        check(lib().tycho_mesh_write_smesh(self._h, str(path).encode()))
+
+    def write_pmesh(self, path):
+        check(lib().tycho_mesh_write_pmesh(self._h, str(path).encode()))
+
+    def tables(self):
+        """dict of the TychoMesh tables as numpy arrays, [cell][face][...]."""
+        if self._tables is None:
+            n, nn = self.n_cells, self.n_nodes
+            t = {
+                "adj_cell": np.empty((n, 4), np.uint64),
+                "neighbor_vrtx": np.empty((n, 4, 3), np.uint64),
+                "face_to_cell": np.empty((n, 4, 3), np.uint64),
+                "cell_to_face": np.empty((n, 4, 4), np.uint64),
+                "cell_nodes": np.empty((n, 4), np.uint64),
+                "volume": np.empty(n, np.float64),
+                "area": np.empty((n, 4), np.float64),
+                "normal": np.empty((n, 4, 3), np.float64),
+                "cell_gid": np.empty(n, np.uint64),
+                "coords": np.empty((nn, 3), np.float64),
+            }
+            check(lib().tycho_mesh_tables(
+                self._h, *(ptr(t[k]) for k in ("adj_cell", "neighbor_vrtx", "face_to_cell",
+                                               "cell_to_face", "cell_nodes", "volume", "area",
+                                               "normal", "cell_gid", "coords"))))
+            self._tables = t
+        return self._tables
+
+    def levels(self, sn_order):
+        """(tlevel, deps, blevel) in (angle, cell) order and the level count."""
+        A = 2 * sn_order * sn_order
+        t = np.empty((A, self.n_cells), np.uint32)
+        d = np.empty((A, self.n_cells), np.uint32)
+        b = np.empty((A, self.n_cells), np.uint32)
+        nl = C.c_uint32()
+        check(lib().tycho_mesh_levels(self._h, sn_order, ptr(t), ptr(d), ptr(b), C.byref(nl)))
+        return t, d, b, nl.value
+
+    def centroids(self):
+        t = self.tables()
+        return t["coords"][t["cell_nodes"].astype(np.int64)].mean(axis=1)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _capi._lib is not None:
+            _capi._lib.tycho_mesh_free(h)
+            self._h = None
+
+
+class Quadrature:
+    """Quadrature (src/Quadrature.hh:45-64): 2 N^2 directions."""
+
+    def __init__(self, sn_order):
+        A = 2 * sn_order * sn_order
+        self.xi, self.eta, self.mu, self.wt = (np.empty(A) for _ in range(4))
+        n = lib().tycho_quadrature(sn_order, ptr(self.xi), ptr(self.eta), ptr(self.mu), ptr(self.wt))
+        if n != A:
+            raise _capi.TychoError(1, "Quadrature order not supported: %d" % sn_order)
+        self.sn_order, self.n_angles = sn_order, A
+
+    def getXi(self, a):
+        return self.xi[a]
+
+    def getEta(self, a):
+        return self.eta[a]
+
+    def getMu(self, a):
+        return self.mu[a]
+
+    def getWt(self, a):
+        return self.wt[a]
+
+
+class SweeperCuda:
+    """SweeperAbstract (src/SweeperAbstract.hh:47-70) on the B200 sweep.
+
+    sweep(psi, source) fills psi = L^-1 source in place (host arrays in the
+    PsiData layout); solve() runs SourceIteration / Krylov / mixed-precision
+    refinement on the device and keeps psi resident.
+    """
+
+    def __init__(self, mesh, sn_order, n_groups, gauss_elim="NoPivot", fp32=False, device=0,
+                 tpi64=0, tpi32=0):
+        if gauss_elim not in GAUSS_ELIM:
+            raise ValueError("GaussElim must be one of %s" % sorted(GAUSS_ELIM))
+        self.mesh = mesh
+        self.n_groups = n_groups
+        self.quadrature = Quadrature(sn_order)
+        self.n_angles = self.quadrature.n_angles
+        opts = _capi.SweeperOpts(sn_order, n_groups, GAUSS_ELIM[gauss_elim], device, int(fp32),
+                                 tpi64, tpi32)
+        h = C.c_void_p()
+        check(lib().tycho_sweeper_create(mesh._h, C.byref(opts), C.byref(h)))
+        self._h = h
+        self.stats = None
+
+    # sizes of the reference containers
+    @property
+    def psi_shape(self):
+        return (self.mesh.n_cells, self.n_angles, 4, self.n_groups)
+
+    @property
+    def phi_shape(self):
+        return (self.mesh.n_cells, 4, self.n_groups)
+
+    def set_cross_sections(self, sigma_t, sigma_s, scatter=None):
+        st = np.ascontiguousarray(sigma_t, np.float64)
+        ss = np.ascontiguousarray(sigma_s, np.float64)
+        sc = None if scatter is None else np.ascontiguousarray(scatter, np.float64)
+        assert st.shape == (self.mesh.n_cells,) and ss.shape == (self.mesh.n_cells,)
+        if sc is not None:
+            assert sc.shape == (self.n_groups, self.n_groups)
+        check(lib().tycho_sweeper_set_cross_sections(self._h, ptr(st), ptr(ss), ptr(sc)))
+        self._xs = (st, ss, sc)
+
+    def set_source(self, q, kind="angular"):
+        """Fixed source Q: 'angular' in the psi layout, 'isotropic' in phi's."""
+        k = {"angular": 0, "isotropic": 1}[kind]
+        if q is None:
+            check(lib().tycho_sweeper_set_source(self._h, k, None))
+            return
+        arr = np.ascontiguousarray(q, np.float64)
+        assert arr.size == np.prod(self.psi_shape if k == 0 else self.phi_shape)
+        check(lib().tycho_sweeper_set_source(self._h, k, ptr(arr)))
+
+    def sweep(self, psi, source, zeroPsiBound=False):
+        """SweeperAbstract::sweep: psi = L^-1 source (vacuum boundaries)."""
+        del zeroPsiBound  # one partition: no partition-boundary psi exists
+        src = np.ascontiguousarray(source, np.float64)
+        assert psi.dtype == np.float64 and psi.flags["C_CONTIGUOUS"] and psi.size == src.size
+        check(lib().tycho_sweeper_sweep(self._h, ptr(src), ptr(psi)))
+        return psi
+
+    def solve(self, method="si", iter_max=100, err_max=1e-10, restart=20, inner_tol=1e-5,
+              refine_max=10, want_psi=True):
+        """SweeperAbstract::solve; returns (phi, psi or None, stats dict)."""
+        o = _capi.SolveOpts(METHODS[method], iter_max, err_max, restart, inner_tol, refine_max)
+        phi = np.empty(self.phi_shape)
+        psi = np.empty(self.psi_shape) if want_psi else None
+        st = _capi.SolveStats()
+        status = lib().tycho_sweeper_solve(self._h, C.byref(o), ptr(phi), ptr(psi), C.byref(st))
+        self.stats = {k: getattr(st, k) for k, _ in _capi.SolveStats._fields_}
+        check(status)
+        return phi, psi, self.stats
+
+    def writePsiToFile(self, filename):
+        check(lib().tycho_sweeper_write_psi(self._h, str(filename).encode()))
+
+    def schedule_info(self):
+        nl, ni, nin = C.c_uint32(), C.c_uint64(), C.c_uint64()
+        check(lib().tycho_sweeper_schedule_info(self._h, C.byref(nl), C.byref(ni), C.byref(nin)))
+        return {"n_levels": nl.value, "n_items": ni.value, "n_incoming_interior": nin.value}
+
+    def time_sweeps(self, precision, n, flush_l2=True):
+        ms = np.zeros(2)
+        check(lib().tycho_sweeper_time_sweeps(self._h, precision, n, int(flush_l2), ptr(ms)))
+        return float(ms[0]), float(ms[1])
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value and _capi._lib is not None:
+            _capi._lib.tycho_sweeper_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
