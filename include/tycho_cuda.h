@@ -80,6 +80,17 @@ int tycho_mesh_read_smesh(const char *path, tycho_mesh **out);
    jittered by U(-jitter*h, jitter*h) per coordinate (seeded). */
 int tycho_mesh_kuhn_cube(uint32_t n, double jitter, uint64_t seed, double length,
                          tycho_mesh **out);
+/* From an already-loaded reference TychoMesh, through its getters
+   (src/TychoMesh.hh:70-116): cell_nodes [n*4] (getCellNode), coords
+   [n_nodes*3] (getNodeCoord), adj_cell [n*4] (getAdjCell, UINT64_MAX on the
+   boundary), face_to_cell [n*12] (getFaceToCellVrtx), cell_gid [n]
+   (getLGCell, may be NULL).  Volumes, areas, normals, cellToFaceVrtx and
+   neighborVrtx are derived as TychoMesh derives them.  Such a mesh has no
+   face records, so it cannot be written back as .smesh/.pmesh. */
+int tycho_mesh_from_arrays(uint64_t n_cells, uint64_t n_nodes, const uint64_t *cell_nodes,
+                           const double *coords, const uint64_t *adj_cell,
+                           const uint64_t *face_to_cell, const uint64_t *cell_gid,
+                           tycho_mesh **out);
 int tycho_mesh_write_smesh(const tycho_mesh *mesh, const char *path);
 int tycho_mesh_write_pmesh(const tycho_mesh *mesh, const char *path);
 int tycho_mesh_info(const tycho_mesh *mesh, uint64_t *n_cells, uint64_t *n_nodes,
@@ -118,6 +129,8 @@ typedef struct tycho_sweeper_opts {
     int fp32;       /* nonzero: also prepare the FP32 sweep (mixed precision) */
     int tpi64;      /* threads per (cell,angle) item of the FP64 sweep, 0 = auto */
     int tpi32;      /* same for the FP32 sweep, 0 = auto */
+    int schedule;   /* 0 = auto (dataflow), 1 = one launch per wavefront level,
+                       2 = one persistent dataflow launch per sweep */
 } tycho_sweeper_opts;
 
 /* Builds the device-resident instance: uploads the mesh tables, levels every
@@ -182,6 +195,16 @@ int tycho_sweeper_schedule_info(const tycho_sweeper *sw, uint32_t *n_levels, uin
    dependency counts and Priorities' b-levels. */
 int tycho_sweeper_levels(const tycho_sweeper *sw, uint32_t *tlevel, uint32_t *deps,
                          uint32_t *blevel);
+
+/* Autotuner: times every launch shape of the given precision's sweep --
+   schedule (1 = one launch per level, 2 = persistent dataflow) x threads per
+   (cell, angle) item (1..16, i.e. the group tiling) -- with `reps` operator
+   applications each on this instance's own problem, keeps the fastest and
+   reports it.  Cross sections must be set. */
+int tycho_sweeper_autotune(tycho_sweeper *sw, int precision, int reps, int *best_tpi,
+                           int *best_schedule, double *best_ms);
+/* Sets the launch shape explicitly (schedule 1 or 2, tpi 1..16). */
+int tycho_sweeper_configure(tycho_sweeper *sw, int precision, int schedule, int tpi);
 
 /* Device timing of n back-to-back operator applications
    phi_out = D L^{-1} (M S phi_in + Q) in the given precision, on the

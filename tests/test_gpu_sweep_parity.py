@@ -22,28 +22,31 @@ def test_fp64_sweep_bit_exact_vs_reference_fixture(built, kuhn3_ref):
     import tycho2_b200 as ty
     r = kuhn3_ref
     mesh = ty.TychoMesh.kuhn_cube(3, 0.05, 2024, 100.0)
-    for tpi in (1, 2):
-        sw = make(mesh, 4, 3, tpi64=tpi)
+    for tpi, schedule in ((1, "levels"), (2, "levels"), (1, "dataflow"), (4, "dataflow")):
+        sw = make(mesh, 4, 3, tpi64=tpi, schedule=schedule)
         sw.set_cross_sections(r["sweep_sigma_t"], np.zeros(mesh.n_cells))
         psi = np.empty(sw.psi_shape)
         sw.sweep(psi, r["sweep_source"])
         assert bits_equal(psi, r["sweep_psi"]), "tpi=%d" % tpi
 
 
+@pytest.mark.parametrize("schedule", ["levels", "dataflow"])
 @pytest.mark.parametrize("n,jitter,sn,G,tpi", [
     (4, 0.05, 4, 1, 1), (5, 0.05, 8, 2, 2), (3, 0.0, 2, 3, 1), (6, 0.05, 6, 4, 4),
     (4, 0.07, 8, 8, 8), (2, 0.05, 4, 16, 16), (7, 0.05, 4, 5, 2), (1, 0.0, 4, 1, 1)])
-def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi):
+def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi, schedule):
     from oracle.oracle import Oracle
     mesh, om = kuhn(workdir, n, jitter, seed=5)
     o = Oracle(om, sn, G)
     rng = np.random.default_rng(n * 100 + G)
     st = rng.lognormal(0.0, 0.5, mesh.n_cells)
     src = rng.uniform(-0.2, 1.0, o.psi_shape)
-    sw = make(mesh, sn, G, tpi64=tpi)
+    sw = make(mesh, sn, G, tpi64=tpi, schedule=schedule)
     sw.set_cross_sections(st, np.zeros(mesh.n_cells))
     psi = np.empty(sw.psi_shape)
     sw.sweep(psi, src)
+    assert bits_equal(psi, o.sweep(st, src_ang=src))
+    sw.sweep(psi, src)  # a second sweep (next completion epoch) is identical
     assert bits_equal(psi, o.sweep(st, src_ang=src))
 
 
@@ -227,3 +230,22 @@ def test_missing_inputs_are_errors(built, workdir):
     # caller reads the last relative change.
     phi, psi, stats = sw.solve("si", iter_max=2, err_max=1e-30)
     assert stats["iterations"] == 2 and stats["final_error"] > 1e-30
+
+
+def test_autotune_keeps_results_bit_exact(built, workdir):
+    """Whatever launch shape the autotuner picks, the FP64 sweep is unchanged."""
+    from oracle.oracle import Oracle
+    mesh, om = kuhn(workdir, 6, 0.05, seed=12)
+    G = 4
+    o = Oracle(om, 8, G)
+    rng = np.random.default_rng(12)
+    st = rng.lognormal(0.0, 0.5, mesh.n_cells)
+    src = rng.uniform(0.0, 1.0, o.psi_shape)
+    sw = make(mesh, 8, G, fp32=True)
+    sw.set_cross_sections(st, np.zeros(mesh.n_cells))
+    best64 = sw.autotune(0, reps=2)
+    best32 = sw.autotune(1, reps=2)
+    assert best64["tpi"] in (1, 2, 4, 8, 16) and best32["schedule"] in ("levels", "dataflow")
+    psi = np.empty(sw.psi_shape)
+    sw.sweep(psi, src)
+    assert bits_equal(psi, o.sweep(st, src_ang=src))

@@ -61,6 +61,27 @@ def test_tables_and_levels_match_oracle(built, workdir, n, jitter, sn):
     assert np.array_equal(blev, oblev)
 
 
+def test_mesh_from_reference_getters(built):
+    """tycho_mesh_from_arrays (the SweeperCuda adapter's entry) rebuilds the
+    same tables from what TychoMesh's getters expose."""
+    import tycho2_b200 as ty
+    mesh = ty.TychoMesh.kuhn_cube(4, 0.06, 9, 3.0)
+    t = mesh.tables()
+    m2 = ty.TychoMesh.from_arrays(t["cell_nodes"], t["coords"], t["adj_cell"], t["face_to_cell"],
+                                  t["cell_gid"])
+    t2 = m2.tables()
+    for k in t:
+        assert bits_equal(t[k], t2[k]) if t[k].dtype == np.float64 else np.array_equal(t[k], t2[k]), k
+    assert m2.n_sides == mesh.n_sides
+    assert np.array_equal(m2.levels(8)[0], mesh.levels(8)[0])
+    with pytest.raises(ty.TychoError):
+        m2.write_pmesh("/nonexistent/never_written.pmesh")
+    bad = t["face_to_cell"].copy()
+    bad[0, 0, 0] = 0  # face 0 cannot contain vertex 0
+    with pytest.raises(ty.TychoError):
+        ty.TychoMesh.from_arrays(t["cell_nodes"], t["coords"], t["adj_cell"], bad)
+
+
 def test_s6_ties_are_not_dependencies(built):
     """S6 has a 45-degree azimuth, so xi == eta and faces of normal (1,-1,0)/sqrt2
     between unjittered nodes have omega.n == 0 exactly.  The reference counts

@@ -29,7 +29,8 @@ _U32P = C.POINTER(C.c_uint32)
 
 class SweeperOpts(C.Structure):
     _fields_ = [("sn_order", C.c_int), ("n_groups", C.c_int), ("gauss_elim", C.c_int),
-                ("device", C.c_int), ("fp32", C.c_int), ("tpi64", C.c_int), ("tpi32", C.c_int)]
+                ("device", C.c_int), ("fp32", C.c_int), ("tpi64", C.c_int), ("tpi32", C.c_int),
+                ("schedule", C.c_int)]
 
 
 class SolveOpts(C.Structure):
@@ -49,6 +50,7 @@ SIGNATURES = {
     "tycho_mesh_read_pmesh": (C.c_int, [C.c_char_p, _PP]),
     "tycho_mesh_read_smesh": (C.c_int, [C.c_char_p, _PP]),
     "tycho_mesh_kuhn_cube": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, C.c_double, _PP]),
+    "tycho_mesh_from_arrays": (C.c_int, [C.c_uint64, C.c_uint64, _P, _P, _P, _P, _P, _PP]),
     "tycho_mesh_write_smesh": (C.c_int, [_P, C.c_char_p]),
     "tycho_mesh_write_pmesh": (C.c_int, [_P, C.c_char_p]),
     "tycho_mesh_info": (C.c_int, [_P, _U64P, _U64P, _U64P]),
@@ -66,6 +68,9 @@ SIGNATURES = {
     "tycho_sweeper_schedule_info": (C.c_int, [_P, _U32P, _U64P, _U64P]),
     "tycho_sweeper_levels": (C.c_int, [_P, _P, _P, _P]),
     "tycho_sweeper_time_sweeps": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P]),
+    "tycho_sweeper_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "tycho_sweeper_configure": (C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
 }
 
 _lib = None

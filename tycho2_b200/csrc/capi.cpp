@@ -132,9 +132,27 @@ int tycho_mesh_kuhn_cube(uint32_t n, double jitter, uint64_t seed, double length
     });
 }
 
+int tycho_mesh_from_arrays(uint64_t n_cells, uint64_t n_nodes, const uint64_t *cell_nodes,
+                           const double *coords, const uint64_t *adj_cell,
+                           const uint64_t *face_to_cell, const uint64_t *cell_gid, tycho_mesh **out)
+{
+    if (!out || !cell_nodes || !coords || !adj_cell || !face_to_cell || n_cells == 0)
+        return finish(TYCHO_ERR_ARG, "null argument");
+    return guarded([&] {
+        auto *m = new tycho_mesh;
+        std::string err;
+        int st = tycho::tables_from_arrays(n_cells, n_nodes, cell_nodes, coords, adj_cell,
+                                           face_to_cell, cell_gid, m->tab, err);
+        if (st != tycho::kOk) { delete m; return finish(st, err); }
+        *out = m;
+        return (int)TYCHO_OK;
+    });
+}
+
 int tycho_mesh_write_smesh(const tycho_mesh *m, const char *path)
 {
     if (!m || !path) return finish(TYCHO_ERR_ARG, "null argument");
+    if (m->rec.n_cells == 0) return finish(TYCHO_ERR_ARG, "mesh has no face records to write");
     std::string err;
     return finish(tycho::write_smesh(path, m->rec, err), err);
 }
@@ -142,6 +160,7 @@ int tycho_mesh_write_smesh(const tycho_mesh *m, const char *path)
 int tycho_mesh_write_pmesh(const tycho_mesh *m, const char *path)
 {
     if (!m || !path) return finish(TYCHO_ERR_ARG, "null argument");
+    if (m->rec.n_cells == 0) return finish(TYCHO_ERR_ARG, "mesh has no face records to write");
     std::string err;
     return finish(tycho::write_pmesh(path, m->rec, err), err);
 }
@@ -235,6 +254,11 @@ int tycho_sweeper_create(const tycho_mesh *mesh, const tycho_sweeper_opts *opts,
         o.fp32 = opts->fp32 != 0;
         o.tpi64 = opts->tpi64;
         o.tpi32 = opts->tpi32;
+        o.schedule = opts->schedule;
+        if (o.schedule < 0 || o.schedule > 2) {
+            delete h;
+            return finish(TYCHO_ERR_ARG, "schedule must be 0, 1 or 2");
+        }
         std::string err;
         if (opts->gauss_elim != TYCHO_GAUSS_NOPIVOT && opts->gauss_elim != TYCHO_GAUSS_ORIGINAL) {
             delete h;
@@ -311,7 +335,7 @@ int tycho_sweeper_schedule_info(const tycho_sweeper *h, uint32_t *n_levels, uint
     if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
     const auto &s = h->sw.schedule();
     if (n_levels) *n_levels = s.n_levels;
-    if (n_items) *n_items = s.items.size();
+    if (n_items) *n_items = s.n_items;
     if (n_incoming) *n_incoming = s.n_incoming_interior;
     return TYCHO_OK;
 }
@@ -334,6 +358,24 @@ int tycho_sweeper_levels(const tycho_sweeper *h, uint32_t *tlevel, uint32_t *dep
         }
         return (int)TYCHO_OK;
     });
+}
+
+int tycho_sweeper_autotune(tycho_sweeper *h, int precision, int reps, int *best_tpi, int *best_schedule,
+                           double *best_ms)
+{
+    if (!h || reps < 1) return finish(TYCHO_ERR_ARG, "null sweeper or reps < 1");
+    std::string err;
+    return guarded([&] {
+        return finish(h->sw.autotune(precision, reps, best_tpi, best_schedule, best_ms, err), err);
+    });
+}
+
+int tycho_sweeper_configure(tycho_sweeper *h, int precision, int schedule, int tpi)
+{
+    if (!h || (schedule != 1 && schedule != 2) || (precision != 0 && precision != 1))
+        return finish(TYCHO_ERR_ARG, "bad sweeper, precision or schedule");
+    std::string err;
+    return finish(h->sw.configure(precision, tpi, schedule == 2, err), err);
 }
 
 int tycho_sweeper_time_sweeps(tycho_sweeper *h, int precision, int n, int flush_l2, double *ms)

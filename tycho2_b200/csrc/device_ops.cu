@@ -8,6 +8,8 @@
 namespace tycho {
 
 template cudaError_t launch_level<double>(int, const LevelArgs &, uint64_t, uint64_t, cudaStream_t);
+template cudaError_t launch_dataflow<double>(int, const LevelArgs &, const DataflowArgs &, unsigned, cudaStream_t);
+template cudaError_t dataflow_blocks_per_sm<double>(int, int *);
 
 namespace {
 
@@ -20,6 +22,11 @@ __global__ void item_abar_kernel(const uint32_t *__restrict__ items, uint64_t n,
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t ca = items[i];
+    if (ca == kSentinel) {  // level padding: never read by the sweep
+        abar64[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (abar32) abar32[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
     const uint32_t c = ca / A, a = ca - c * A;
     const double xi = omega[a], eta = omega[A + a], mu = omega[2 * A + a];
     double ab[4];
@@ -173,6 +180,12 @@ __global__ void sub_from_kernel(const double *__restrict__ x, double *__restrict
     if (i < n) y[i] = x[i] - y[i];
 }
 
+__global__ void bump_epoch_kernel(uint32_t *epoch)
+{
+    const uint32_t v = *epoch + 1u;
+    *epoch = v == 0u ? 1u : v;
+}
+
 inline unsigned blocks_for(uint64_t n, unsigned t = 256) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -205,6 +218,12 @@ cudaError_t launch_scatter_source(const double *phi_in, const double *q_fixed, c
     const uint64_t n = nc * 4 * G;
     if (n == 0) return cudaSuccess;
     scatter_source_kernel<<<blocks_for(n), 256, 0, s>>>(phi_in, q_fixed, sigma_s, scatter, iso, iso32, nc, G);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bump_epoch(uint32_t *epoch, cudaStream_t s)
+{
+    bump_epoch_kernel<<<1, 1, 0, s>>>(epoch);
     return cudaGetLastError();
 }
 

@@ -25,6 +25,9 @@ cudaError_t launch_scatter_source(const double *phi_in, const double *q_fixed, c
                                   const double *scatter, double *iso, float *iso32, uint64_t nc,
                                   uint32_t G, cudaStream_t s);
 
+// epoch = epoch + 1, skipping 0 (the value a fresh completion array holds).
+cudaError_t launch_bump_epoch(uint32_t *epoch, cudaStream_t s);
+
 // Deterministic reductions: a fixed grid writes per-block partials that one
 // block sums in a fixed order, so results do not depend on scheduling.
 constexpr int kReduceBlocks = 592;  // 4 per SM on 148 SMs

@@ -20,9 +20,28 @@ struct LevelArgs {
     uint32_t A, G;
 };
 
+// Per-sweep state of the persistent (dataflow) schedule.
+struct DataflowArgs {
+    uint32_t *done;       // per cell*A + angle: epoch of the sweep that finished it
+    uint32_t *err;        // [0] error code (0 = none), [1] item, [2] face
+    uint32_t *abort;      // raised on the first failure; every warp drains
+    const uint32_t *epoch;  // device word: this sweep's epoch (never 0)
+    uint64_t n_items;     // padded item count, a multiple of 32
+    uint32_t spin_limit;  // polls of one upwind flag before giving up
+};
+constexpr uint32_t kErrTimeoutCode = 1;
+
 // Launches the wavefront kernel over items [begin, end) with `tpi` threads
 // per item (1, 2, 4, 8 or 16).
 template <typename Real>
 cudaError_t launch_level(int tpi, const LevelArgs &p, uint64_t begin, uint64_t end, cudaStream_t s);
+
+// The whole sweep as one cooperative launch of `grid` 256-thread blocks
+// (at most the co-resident count from dataflow_blocks_per_sm).
+template <typename Real>
+cudaError_t launch_dataflow(int tpi, const LevelArgs &p, const DataflowArgs &df, unsigned grid,
+                            cudaStream_t s);
+template <typename Real>
+cudaError_t dataflow_blocks_per_sm(int tpi, int *blocks);
 
 }  // namespace tycho

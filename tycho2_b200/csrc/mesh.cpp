@@ -333,12 +333,18 @@ int build_tables(const MeshRecords &m, MeshTables &t, std::string &err)
                     }
         }
 
+    return finish_tables(t, err);
+}
+
+int finish_tables(MeshTables &t, std::string &err)
+{
+    const uint64_t nc = t.n_cells;
     // Geometry with the reference's operation order (src/TychoMesh.cc:67-187).
     t.volume.resize(nc); t.area.resize(nc * 4); t.normal.resize(nc * 12);
     for (uint64_t c = 0; c < nc; ++c) {
         double cp[4][3];
         for (int v = 0; v < 4; ++v)
-            for (int d = 0; d < 3; ++d) cp[v][d] = m.coords[m.cell_nodes[c * 4 + v] * 3 + d];
+            for (int d = 0; d < 3; ++d) cp[v][d] = t.coords[t.cell_nodes[c * 4 + v] * 3 + d];
         {
             double a[3], b[3], cc[3], x[3];
             for (int d = 0; d < 3; ++d) {
@@ -379,14 +385,49 @@ int build_tables(const MeshRecords &m, MeshTables &t, std::string &err)
             for (int k = 0; k < 3; ++k) {
                 uint64_t adj = t.adj_cell[c * 4 + f];
                 if (adj == kNone) { t.neighbor_vrtx[(c * 4 + f) * 3 + k] = kNone; continue; }
-                uint64_t node = m.cell_nodes[c * 4 + t.face_to_cell[(c * 4 + f) * 3 + k]];
+                uint64_t node = t.cell_nodes[c * 4 + t.face_to_cell[(c * 4 + f) * 3 + k]];
                 uint64_t nv = kNone;
                 for (uint64_t v = 0; v < 4; ++v)
-                    if (m.cell_nodes[adj * 4 + v] == node) { nv = v; break; }
+                    if (t.cell_nodes[adj * 4 + v] == node) { nv = v; break; }
                 if (nv == kNone) { err = "neighbour does not share a face node"; return kErrFormat; }
                 t.neighbor_vrtx[(c * 4 + f) * 3 + k] = nv;
             }
     return kOk;
+}
+
+int tables_from_arrays(uint64_t n_cells, uint64_t n_nodes, const uint64_t *cell_nodes,
+                       const double *coords, const uint64_t *adj_cell,
+                       const uint64_t *face_to_cell, const uint64_t *cell_gid, MeshTables &t,
+                       std::string &err)
+{
+    t = MeshTables();
+    t.n_cells = n_cells;
+    t.n_nodes = n_nodes;
+    t.cell_nodes.assign(cell_nodes, cell_nodes + n_cells * 4);
+    t.coords.assign(coords, coords + n_nodes * 3);
+    t.adj_cell.assign(adj_cell, adj_cell + n_cells * 4);
+    t.face_to_cell.assign(face_to_cell, face_to_cell + n_cells * 12);
+    t.cell_material.assign(n_cells, 1);
+    if (cell_gid) t.cell_gid.assign(cell_gid, cell_gid + n_cells);
+    else { t.cell_gid.resize(n_cells); for (uint64_t c = 0; c < n_cells; ++c) t.cell_gid[c] = c; }
+    t.adj_face.assign(n_cells * 4, kNone);
+    t.side.resize(n_cells * 4);
+    t.cell_to_face.assign(n_cells * 16, kNone);
+    for (uint64_t c = 0; c < n_cells; ++c) {
+        for (int v = 0; v < 4; ++v)
+            if (t.cell_nodes[c * 4 + v] >= n_nodes) { err = "cell node out of range"; return kErrFormat; }
+        for (int f = 0; f < 4; ++f) {
+            const uint64_t adj = t.adj_cell[c * 4 + f];
+            if (adj != kNone && adj >= n_cells) { err = "neighbour out of range"; return kErrFormat; }
+            t.side[c * 4 + f] = adj == kNone ? t.n_sides++ : kNone;
+            for (int k = 0; k < 3; ++k) {
+                const uint64_t v = t.face_to_cell[(c * 4 + f) * 3 + k];
+                if (v > 3 || (int)v == f) { err = "bad face-to-cell vertex"; return kErrFormat; }
+                t.cell_to_face[(c * 4 + f) * 4 + v] = k;
+            }
+        }
+    }
+    return finish_tables(t, err);
 }
 
 }  // namespace tycho

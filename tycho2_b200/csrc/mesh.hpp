@@ -63,4 +63,15 @@ void kuhn_cube(uint32_t n, double jitter, uint64_t seed, double length, MeshReco
 
 int build_tables(const MeshRecords &m, MeshTables &t, std::string &err);
 
+// Geometry (volumes, areas, outward normals) and neighbour vertices from
+// cell_nodes, coords, face_to_cell and adj_cell already in `t`.
+int finish_tables(MeshTables &t, std::string &err);
+
+// The tables from what a reference TychoMesh exposes through its getters
+// (getCellNode, getNodeCoord, getAdjCell, getFaceToCellVrtx, getLGCell).
+int tables_from_arrays(uint64_t n_cells, uint64_t n_nodes, const uint64_t *cell_nodes,
+                       const double *coords, const uint64_t *adj_cell,
+                       const uint64_t *face_to_cell, const uint64_t *cell_gid, MeshTables &t,
+                       std::string &err);
+
 }  // namespace tycho

@@ -134,11 +134,17 @@ int build_schedule(const MeshTables &t, const Quadrature &q, Schedule &s, std::s
     std::vector<uint64_t> count(s.n_levels + 1, 0);
     for (uint64_t c = 0; c < nc; ++c)
         for (int a = 0; a < A; ++a) count[s.tlevel[(size_t)a * nc + c] + 1]++;
+    // Each level is padded to a multiple of kLevelPad with sentinel items, so
+    // that a warp's chunk of the persistent schedule never spans two levels.
     s.level_offset.resize(s.n_levels + 1);
     s.level_offset[0] = 0;
-    for (uint32_t l = 0; l < s.n_levels; ++l) s.level_offset[l + 1] = s.level_offset[l] + count[l + 1];
+    for (uint32_t l = 0; l < s.n_levels; ++l) {
+        const uint64_t padded = (count[l + 1] + kLevelPad - 1) / kLevelPad * kLevelPad;
+        s.level_offset[l + 1] = s.level_offset[l] + padded;
+    }
+    s.n_items = (uint64_t)A * nc;
     std::vector<uint64_t> pos(s.level_offset.begin(), s.level_offset.end() - 1);
-    s.items.resize((size_t)A * nc);
+    s.items.assign(s.level_offset[s.n_levels], kSentinelItem);
     for (uint64_t c = 0; c < nc; ++c)
         for (int a = 0; a < A; ++a) {
             uint32_t l = s.tlevel[(size_t)a * nc + c];
@@ -159,6 +165,7 @@ void b_levels(const MeshTables &t, const Quadrature &q, const Schedule &s, std::
         #pragma omp parallel for schedule(static)
         for (uint64_t i = b; i < e; ++i) {
             uint32_t ca = s.items[i];
+            if (ca == kSentinelItem) continue;
             uint64_t c = ca / A;
             int a = (int)(ca - c * A);
             unsigned m = incoming_mask(t, q, c, a);

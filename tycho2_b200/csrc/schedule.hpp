@@ -26,10 +26,15 @@ struct Quadrature {
 // Product Gauss-Legendre x Chebyshev set (src/Quadrature.cc:150-244).
 int make_quadrature(int sn_order, Quadrature &q, std::string &err);
 
+constexpr uint32_t kSentinelItem = 0xFFFFFFFFu;  // level padding
+constexpr uint64_t kLevelPad = 32;
+
 struct Schedule {
     uint32_t n_levels = 0;
+    uint64_t n_items = 0;                // cells x angles (without padding)
     std::vector<uint64_t> level_offset;  // n_levels + 1 offsets into items
-    std::vector<uint32_t> items;         // cell*A + angle, grouped by level
+    std::vector<uint32_t> items;         // cell*A + angle, grouped by level,
+                                         // each level padded to kLevelPad
     std::vector<uint32_t> tlevel;        // (angle, cell)
     uint64_t n_incoming_interior = 0;    // sum over items of incoming interior faces
 };

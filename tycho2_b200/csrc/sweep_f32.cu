@@ -6,5 +6,7 @@
 namespace tycho {
 
 template cudaError_t launch_level<float>(int, const LevelArgs &, uint64_t, uint64_t, cudaStream_t);
+template cudaError_t launch_dataflow<float>(int, const LevelArgs &, const DataflowArgs &, unsigned, cudaStream_t);
+template cudaError_t dataflow_blocks_per_sm<float>(int, int *);
 
 }  // namespace tycho

@@ -1,8 +1,8 @@
 // Wavefront kernels of the DG SN sweep (sm_100a).
 //
-// One launch updates every (cell, angle) item of one wavefront level, for all
-// energy groups.  Per item the 4x4 streaming+collision matrix depends only on
-// (cell, angle) -- the reference rebuilds and re-eliminates it for every group
+// Every (cell, angle) item updates all energy groups of that pair.  Per item
+// the 4x4 streaming+collision matrix depends only on (cell, angle) -- the
+// reference rebuilds and re-eliminates it for every group
 // (src/Transport.cc:687-733) -- so here it is assembled and LU-factored once
 // in registers and the G right-hand sides are pushed through the same
 // elimination.  The arithmetic, including the order of every addition, is the
@@ -13,7 +13,15 @@
 // same steps in single precision for the mixed-precision solver.
 //
 // TPI threads cooperate on one item; thread `sub` handles groups sub,
-// sub+TPI, ...  so a warp's loads of one upwind vertex row are contiguous.
+// sub+TPI, ...  so the TPI lanes' loads of one upwind vertex row are
+// contiguous (TPI*sizeof(Real) >= 32 B fills a DRAM sector).
+//
+// Two schedules drive the same item update:
+//   sweep_level_kernel     one launch per wavefront level (level-synchronous);
+//   sweep_dataflow_kernel  one persistent cooperative launch per sweep: warps
+//                          take level-ordered 32-item chunks round-robin and
+//                          wait, with a bounded spin, only for the upwind items
+//                          they read, through per-item completion epochs.
 #pragma once
 
 #include <cstdint>
@@ -27,36 +35,38 @@ template <typename Real> struct Vec4Of;
 template <> struct Vec4Of<double> { using type = double4; };
 template <> struct Vec4Of<float> { using type = float4; };
 
+constexpr uint32_t kSentinel = 0xFFFFFFFFu;  // padding item of a level
 
+// The group-independent part of one item's update.
+template <typename Real>
+struct ItemFactor {
+    uint32_t c, a;
+    int adj[4];
+    uint32_t nmap;
+    Real ab[4], t1[4], t2[4], vs20;
+    Real r0, u01, u02, u03, l1, l2, l3, r1, u12, u13, a21, a31, r2, u23, b32, c33;
+};
 
-template <typename Real, int TPI>
-__global__ void __launch_bounds__(256)
-sweep_level_kernel(const LevelArgs p, const uint64_t begin, const uint64_t end)
+template <typename Real>
+__device__ __forceinline__ void item_setup(const LevelArgs &p, uint64_t it, uint32_t ca, ItemFactor<Real> &F)
 {
     using R4 = typename Vec4Of<Real>::type;
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t it = begin + t / TPI;
-    if (it >= end) return;
-    const int sub = (int)(t % TPI);
-
-    const uint32_t A = p.A, G = p.G;
-    const uint32_t ca = __ldg(p.items + it);
-    const uint32_t c = ca / A;
-    const uint32_t a = ca - c * A;
+    F.c = ca / p.A;
+    F.a = ca - F.c * p.A;
     const R4 ab4 = reinterpret_cast<const R4 *>(p.abar)[it];
-    const Real ab[4] = {ab4.x, ab4.y, ab4.z, ab4.w};
-    const int4 adj4 = __ldg(p.adj + c);
-    const int adj[4] = {adj4.x, adj4.y, adj4.z, adj4.w};
-    const uint32_t nmap = __ldg(p.nbrmap + c);
-    const Real *ck = reinterpret_cast<const Real *>(p.cellk) + 3 * (size_t)c;
-    const Real vs20 = ck[0], d1 = ck[1], d2 = ck[2];
+    F.ab[0] = ab4.x; F.ab[1] = ab4.y; F.ab[2] = ab4.z; F.ab[3] = ab4.w;
+    const int4 adj4 = __ldg(p.adj + F.c);
+    F.adj[0] = adj4.x; F.adj[1] = adj4.y; F.adj[2] = adj4.z; F.adj[3] = adj4.w;
+    F.nmap = __ldg(p.nbrmap + F.c);
+    const Real *ck = reinterpret_cast<const Real *>(p.cellk) + 3 * (size_t)F.c;
+    F.vs20 = ck[0];
+    const Real d1 = ck[1], d2 = ck[2];
 
     // Face terms A_f/12 and 2 A_f/12 with A_f = area * omega.n.
-    Real t1[4], t2[4];
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-        t1[f] = ab[f] / Real(12);
-        t2[f] = Real(2) * ab[f] / Real(12);
+        F.t1[f] = F.ab[f] / Real(12);
+        F.t2[f] = Real(2) * F.ab[f] / Real(12);
     }
     // Streaming + collision (volume integrals), then outgoing-face terms in
     // increasing face order.
@@ -64,38 +74,55 @@ sweep_level_kernel(const LevelArgs p, const uint64_t begin, const uint64_t end)
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) M[i][j] = t1[i] + (i == j ? d2 : d1);
+        for (int j = 0; j < 4; ++j) M[i][j] = F.t1[i] + (i == j ? d2 : d1);
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-        if (ab[f] > Real(0)) {
+        if (F.ab[f] > Real(0)) {
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
-                    if (i != f && j != f) M[i][j] += (i == j ? t2[f] : t1[f]);
+                    if (i != f && j != f) M[i][j] += (i == j ? F.t2[f] : F.t1[f]);
         }
     }
     // LU without pivoting: the elimination steps of gaussElim4 NoPivot that
     // touch only the matrix.
-    const Real r0 = Real(1) / M[0][0];
-    const Real u01 = M[0][1] * r0, u02 = M[0][2] * r0, u03 = M[0][3] * r0;
-    const Real l1 = M[1][0], l2 = M[2][0], l3 = M[3][0];
-    const Real a11 = M[1][1] - u01 * l1, a12 = M[1][2] - u02 * l1, a13 = M[1][3] - u03 * l1;
-    const Real a21 = M[2][1] - u01 * l2, a22 = M[2][2] - u02 * l2, a23 = M[2][3] - u03 * l2;
-    const Real a31 = M[3][1] - u01 * l3, a32 = M[3][2] - u02 * l3, a33 = M[3][3] - u03 * l3;
-    const Real r1 = Real(1) / a11;
-    const Real u12 = a12 * r1, u13 = a13 * r1;
-    const Real b22 = a22 - u12 * a21, b23 = a23 - u13 * a21;
-    const Real b32 = a32 - u12 * a31, b33 = a33 - u13 * a31;
-    const Real r2 = Real(1) / b22;
-    const Real u23 = b23 * r2;
-    const Real c33 = b33 - u23 * b32;
+    F.r0 = Real(1) / M[0][0];
+    F.u01 = M[0][1] * F.r0; F.u02 = M[0][2] * F.r0; F.u03 = M[0][3] * F.r0;
+    F.l1 = M[1][0]; F.l2 = M[2][0]; F.l3 = M[3][0];
+    const Real a11 = M[1][1] - F.u01 * F.l1, a12 = M[1][2] - F.u02 * F.l1, a13 = M[1][3] - F.u03 * F.l1;
+    const Real a21 = M[2][1] - F.u01 * F.l2, a22 = M[2][2] - F.u02 * F.l2, a23 = M[2][3] - F.u03 * F.l2;
+    const Real a31 = M[3][1] - F.u01 * F.l3, a32 = M[3][2] - F.u02 * F.l3, a33 = M[3][3] - F.u03 * F.l3;
+    F.a21 = a21; F.a31 = a31;
+    F.r1 = Real(1) / a11;
+    F.u12 = a12 * F.r1; F.u13 = a13 * F.r1;
+    const Real b22 = a22 - F.u12 * a21, b23 = a23 - F.u13 * a21;
+    F.b32 = a32 - F.u12 * a31;
+    const Real b33 = a33 - F.u13 * a31;
+    F.r2 = Real(1) / b22;
+    F.u23 = b23 * F.r2;
+    F.c33 = b33 - F.u23 * F.b32;
+}
 
+// Loads an upwind psi value; L2_ONLY bypasses L1, which another SM's recent
+// write may have left stale (the dataflow schedule reads values written in
+// the same launch).
+template <typename Real, bool L2_ONLY>
+__device__ __forceinline__ Real load_upwind(const Real *p)
+{
+    if (L2_ONLY) return __ldcg(p);
+    return *p;
+}
+
+template <typename Real, int TPI, bool L2_ONLY>
+__device__ __forceinline__ void item_groups(const LevelArgs &p, uint32_t ca, int sub, const ItemFactor<Real> &F)
+{
+    const uint32_t A = p.A, G = p.G;
     const size_t rowG = (size_t)4 * G;
     const Real *__restrict__ psi_in = reinterpret_cast<const Real *>(p.psi);
     Real *__restrict__ psi_out = reinterpret_cast<Real *>(p.psi) + (size_t)ca * rowG;
     const Real *__restrict__ iso = reinterpret_cast<const Real *>(p.iso);
-    const Real *iso_c = iso ? iso + (size_t)c * rowG : nullptr;
+    const Real *iso_c = iso ? iso + (size_t)F.c * rowG : nullptr;
     const double *qang_ca = p.qang ? p.qang + (size_t)ca * rowG : nullptr;
 
     for (uint32_t g = sub; g < G; g += TPI) {
@@ -108,22 +135,22 @@ sweep_level_kernel(const LevelArgs p, const uint64_t begin, const uint64_t end)
             else q[v] = Real(0);
         }
         Real b[4];
-        b[0] = vs20 * (Real(2) * q[0] + q[1] + q[2] + q[3]);
-        b[1] = vs20 * (q[0] + Real(2) * q[1] + q[2] + q[3]);
-        b[2] = vs20 * (q[0] + q[1] + Real(2) * q[2] + q[3]);
-        b[3] = vs20 * (q[0] + q[1] + q[2] + Real(2) * q[3]);
+        b[0] = F.vs20 * (Real(2) * q[0] + q[1] + q[2] + q[3]);
+        b[1] = F.vs20 * (q[0] + Real(2) * q[1] + q[2] + q[3]);
+        b[2] = F.vs20 * (q[0] + q[1] + Real(2) * q[2] + q[3]);
+        b[3] = F.vs20 * (q[0] + q[1] + q[2] + Real(2) * q[3]);
         // Upwind faces, increasing face order; vacuum (0) on the boundary.
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-            if (ab[f] < Real(0)) {
+            if (F.ab[f] < Real(0)) {
                 Real pn[4];
-                const int nb = adj[f];
-                const Real *nrow = psi_in + ((size_t)(nb < 0 ? 0 : nb) * A + a) * rowG + g;
+                const int nb = F.adj[f];
+                const Real *nrow = psi_in + ((size_t)(nb < 0 ? 0 : nb) * A + F.a) * rowG + g;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     if (j == f) { pn[j] = Real(0); continue; }
-                    const uint32_t nv = (nmap >> ((f * 4 + j) * 2)) & 3u;
-                    pn[j] = nb >= 0 ? nrow[nv * G] : Real(0);
+                    const uint32_t nv = (F.nmap >> ((f * 4 + j) * 2)) & 3u;
+                    pn[j] = nb >= 0 ? load_upwind<Real, L2_ONLY>(nrow + nv * G) : Real(0);
                 }
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
@@ -131,27 +158,113 @@ sweep_level_kernel(const LevelArgs p, const uint64_t begin, const uint64_t end)
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         if (j == f) continue;
-                        b[i] -= (i == j ? t2[f] : t1[f]) * pn[j];
+                        b[i] -= (i == j ? F.t2[f] : F.t1[f]) * pn[j];
                     }
                 }
             }
         }
         // The right-hand-side steps of gaussElim4 NoPivot.
-        b[0] = b[0] * r0;
-        b[1] = b[1] - b[0] * l1;
-        b[2] = b[2] - b[0] * l2;
-        b[3] = b[3] - b[0] * l3;
-        b[1] = b[1] * r1;
-        b[2] = b[2] - b[1] * a21;
-        b[3] = b[3] - b[1] * a31;
-        b[2] = b[2] * r2;
-        b[3] = b[3] - b[2] * b32;
-        b[3] = b[3] / c33;
-        b[2] = b[2] - u23 * b[3];
-        b[1] = b[1] - u13 * b[3] - u12 * b[2];
-        b[0] = b[0] - u03 * b[3] - u02 * b[2] - u01 * b[1];
+        b[0] = b[0] * F.r0;
+        b[1] = b[1] - b[0] * F.l1;
+        b[2] = b[2] - b[0] * F.l2;
+        b[3] = b[3] - b[0] * F.l3;
+        b[1] = b[1] * F.r1;
+        b[2] = b[2] - b[1] * F.a21;
+        b[3] = b[3] - b[1] * F.a31;
+        b[2] = b[2] * F.r2;
+        b[3] = b[3] - b[2] * F.b32;
+        b[3] = b[3] / F.c33;
+        b[2] = b[2] - F.u23 * b[3];
+        b[1] = b[1] - F.u13 * b[3] - F.u12 * b[2];
+        b[0] = b[0] - F.u03 * b[3] - F.u02 * b[2] - F.u01 * b[1];
 #pragma unroll
         for (int v = 0; v < 4; ++v) psi_out[v * G + g] = b[v];
+    }
+}
+
+template <typename Real, int TPI>
+__global__ void __launch_bounds__(256)
+sweep_level_kernel(const LevelArgs p, const uint64_t begin, const uint64_t end)
+{
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t it = begin + t / TPI;
+    if (it >= end) return;
+    const uint32_t ca = __ldg(p.items + it);
+    if (ca == kSentinel) return;
+    ItemFactor<Real> F;
+    item_setup(p, it, ca, F);
+    item_groups<Real, TPI, false>(p, ca, (int)(t % TPI), F);
+}
+
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(uint32_t *p, uint32_t v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Waits until done[idx] == epoch.  Gives up after df.spin_limit polls: records
+// the item and face in df.err (first failure wins), raises df.abort, and
+// returns false; every warp then drains without computing.
+__device__ __forceinline__ bool wait_done(const DataflowArgs &df, uint32_t epoch, uint32_t idx,
+                                          uint32_t ca, int f)
+{
+    const uint32_t *flag = df.done + idx;
+    if (ld_acquire_gpu(flag) == epoch) return true;
+    unsigned backoff = 32;
+    for (uint32_t spin = 0; spin < df.spin_limit; ++spin) {
+        if (*(volatile const uint32_t *)df.abort) return false;
+        __nanosleep(backoff);
+        if (backoff < 1024) backoff <<= 1;
+        if (ld_acquire_gpu(flag) == epoch) return true;
+    }
+    if (atomicCAS(df.err, 0u, (uint32_t)kErrTimeoutCode) == 0u) {
+        df.err[1] = ca;
+        df.err[2] = (uint32_t)f;
+    }
+    atomicExch(df.abort, 1u);
+    return false;
+}
+
+// One persistent launch per sweep.  Items are padded per level to multiples
+// of 32, so a warp's 32/TPI-item chunk never spans two levels: an item only
+// waits for items of lower levels, which belong to chunks of lower index.
+// Warps take chunks round-robin in increasing order and every warp is
+// resident (cooperative launch), so the lowest unfinished chunk can always
+// make progress.
+template <typename Real, int TPI>
+__global__ void __launch_bounds__(256)
+sweep_dataflow_kernel(const LevelArgs p, const DataflowArgs df)
+{
+    constexpr uint32_t IPW = 32 / TPI;  // items per warp chunk
+    const uint32_t lane = threadIdx.x & 31u;
+    const int sub = (int)(lane % TPI);
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint64_t nchunks = df.n_items / IPW;
+    const uint32_t epoch = *df.epoch;
+    for (uint64_t chunk = warp; chunk < nchunks; chunk += nwarps) {
+        if (*(volatile const uint32_t *)df.abort) break;
+        const uint64_t it = chunk * IPW + lane / TPI;
+        const uint32_t ca = __ldg(p.items + it);
+        bool ok = true;
+        if (ca != kSentinel) {
+            ItemFactor<Real> F;
+            item_setup(p, it, ca, F);
+#pragma unroll
+            for (int f = 0; f < 4; ++f)
+                if (ok && F.ab[f] < Real(0) && F.adj[f] >= 0)
+                    ok = wait_done(df, epoch, (uint32_t)F.adj[f] * p.A + F.a, ca, f);
+            if (ok) item_groups<Real, TPI, true>(p, ca, sub, F);
+        }
+        __threadfence();
+        __syncwarp();
+        if (ca != kSentinel && sub == 0 && ok) st_release_gpu(df.done + ca, epoch);
     }
 }
 
@@ -171,6 +284,45 @@ cudaError_t launch_level(int tpi, const LevelArgs &p, uint64_t begin, uint64_t e
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+template <typename Real>
+static const void *dataflow_fn(int tpi)
+{
+    switch (tpi) {
+    case 1: return (const void *)sweep_dataflow_kernel<Real, 1>;
+    case 2: return (const void *)sweep_dataflow_kernel<Real, 2>;
+    case 4: return (const void *)sweep_dataflow_kernel<Real, 4>;
+    case 8: return (const void *)sweep_dataflow_kernel<Real, 8>;
+    case 16: return (const void *)sweep_dataflow_kernel<Real, 16>;
+    default: return nullptr;
+    }
+}
+
+template <typename Real>
+cudaError_t dataflow_blocks_per_sm(int tpi, int *blocks)
+{
+    const void *fn = dataflow_fn<Real>(tpi);
+    if (!fn) return cudaErrorInvalidValue;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, fn, 256, 0);
+}
+
+template <typename Real>
+cudaError_t launch_dataflow(int tpi, const LevelArgs &p, const DataflowArgs &df, unsigned grid, cudaStream_t s)
+{
+    const void *fn = dataflow_fn<Real>(tpi);
+    if (!fn || grid == 0) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void *args[] = {(void *)&p, (void *)&df};
+    return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 }  // namespace tycho

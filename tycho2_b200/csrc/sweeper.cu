@@ -57,7 +57,7 @@ Sweeper::~Sweeper()
     for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
     void *bufs[] = {d_items_, d_abar64_, d_abar32_, d_adj_, d_nbrmap_, d_cellk64_, d_cellk32_,
                     d_w_, d_sigs_, d_scat_, d_qiso_, d_qang_, d_src_, d_iso_, d_iso32_, d_psi_,
-                    d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_};
+                    d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_, d_done_, d_ctl_};
     for (void *b : bufs)
         if (b) cudaFree(b);
     reducer_free(red_);
@@ -83,11 +83,6 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     fp32_ = o.fp32;
     tpi64_ = o.tpi64 ? o.tpi64 : auto_tpi(G_, false);
     tpi32_ = o.tpi32 ? o.tpi32 : auto_tpi(G_, true);
-    for (int tp : {tpi64_, tpi32_})
-        if (tp != 1 && tp != 2 && tp != 4 && tp != 8 && tp != 16) {
-            err = "threads per item must be 1, 2, 4, 8 or 16";
-            return kErrArg;
-        }
     TY_CHECK(build_schedule(tables_, quad_, sched_, err));
     TY_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
 
@@ -145,8 +140,81 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     if (fp32_) TY_CUDA(cudaMalloc(&d_cellk32_, sizeof(float) * 3 * nc_));
     TY_CUDA(cudaMalloc(&d_sigs_, sizeof(double) * nc_));
     TY_CUDA(reducer_init(red_));
+
+    // Dataflow schedule: completion epochs per item and a control block;
+    // grid = every block that can be co-resident (cooperative launch).
+    TY_CUDA(cudaMalloc(&d_done_, sizeof(uint32_t) * (size_t)nc_ * A_));
+    TY_CUDA(cudaMemsetAsync(d_done_, 0, sizeof(uint32_t) * (size_t)nc_ * A_, stream_));
+    TY_CUDA(cudaMalloc(&d_ctl_, sizeof(uint32_t) * 8));
+    TY_CUDA(cudaMemsetAsync(d_ctl_, 0, sizeof(uint32_t) * 8, stream_));
+    const bool dataflow = o.schedule != 1;
+    TY_CHECK(configure(0, tpi64_, dataflow, err));
+    TY_CHECK(configure(1, tpi32_, dataflow, err));
     TY_CUDA(cudaStreamSynchronize(stream_));
     return kOk;
+}
+
+int Sweeper::configure(int prec, int tpi, bool dataflow, std::string &err)
+{
+    if (tpi != 1 && tpi != 2 && tpi != 4 && tpi != 8 && tpi != 16) {
+        err = "threads per item must be 1, 2, 4, 8 or 16";
+        return kErrArg;
+    }
+    int sms = 0, per_sm = 0;
+    TY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+    TY_CUDA(prec ? dataflow_blocks_per_sm<float>(tpi, &per_sm) : dataflow_blocks_per_sm<double>(tpi, &per_sm));
+    if (per_sm < 1) { err = "dataflow kernel does not fit on an SM"; return kErrCuda; }
+    (prec ? tpi32_ : tpi64_) = tpi;
+    (prec ? dataflow32_ : dataflow64_) = dataflow;
+    (prec ? grid32_ : grid64_) = (unsigned)(sms * per_sm);
+    // cached level graphs were captured for the previous launch shape
+    for (auto it = graphs_.begin(); it != graphs_.end();) {
+        if (std::get<0>(it->first) == prec) {
+            cudaGraphExecDestroy(it->second);
+            it = graphs_.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    return kOk;
+}
+
+// Times every (schedule, threads-per-item) candidate on this instance's own
+// problem with a few operator applications and keeps the fastest.
+int Sweeper::autotune(int prec, int reps, int *best_tpi, int *best_sched, double *best_ms, std::string &err)
+{
+    if (prec == 1 && !fp32_) { err = "sweeper was created without the FP32 sweep"; return kErrArg; }
+    if (!have_xs_) { err = "cross sections not set"; return kErrMissing; }
+    double best = 1e300;
+    int btpi = tpi(prec), bdf = (prec ? dataflow32_ : dataflow64_) ? 2 : 1;
+    for (int sched = 1; sched <= 2; ++sched)
+        for (int t : {1, 2, 4, 8, 16}) {
+            if (t > 2 * G_ && t > 1) continue;  // lanes with no group to update
+            TY_CHECK(configure(prec, t, sched == 2, err));
+            double ms[2];
+            TY_CHECK(time_sweeps(prec, 1, false, ms, err));  // warm-up (and graph capture)
+            TY_CHECK(time_sweeps(prec, reps, false, ms, err));
+            if (ms[0] < best) { best = ms[0]; btpi = t; bdf = sched; }
+        }
+    TY_CHECK(configure(prec, btpi, bdf == 2, err));
+    if (best_tpi) *best_tpi = btpi;
+    if (best_sched) *best_sched = bdf;
+    if (best_ms) *best_ms = best;
+    return kOk;
+}
+
+int Sweeper::check_device_error(std::string &err)
+{
+    if (!d_ctl_) return kOk;
+    uint32_t ctl[4];
+    TY_CUDA(cudaMemcpyAsync(ctl, d_ctl_, sizeof ctl, cudaMemcpyDeviceToHost, stream_));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    if (ctl[0] == 0) return kOk;
+    err = "sweep wait timed out at item " + std::to_string(ctl[1]) + " face " + std::to_string(ctl[2]) +
+          " (upwind item never completed)";
+    TY_CUDA(cudaMemsetAsync(d_ctl_, 0, sizeof(uint32_t) * 4, stream_));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    return kErrTimeout;
 }
 
 int Sweeper::set_cross_sections(const double *sigma_t, const double *sigma_s, const double *scatter,
@@ -201,6 +269,32 @@ int Sweeper::set_source(int kind, const double *q, std::string &err)
 int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg, cudaEvent_t end,
                     std::string &err)
 {
+    if (prec ? dataflow32_ : dataflow64_) {
+        LevelArgs p;
+        p.items = d_items_;
+        p.abar = prec ? (const void *)d_abar32_ : (const void *)d_abar64_;
+        p.adj = d_adj_;
+        p.nbrmap = d_nbrmap_;
+        p.cellk = prec ? (const void *)d_cellk32_ : (const void *)d_cellk64_;
+        p.iso = has_iso ? (prec ? (const void *)d_iso32_ : (const void *)d_iso_) : nullptr;
+        p.qang = qang;
+        p.psi = d_psi_;
+        p.A = (uint32_t)A_;
+        p.G = (uint32_t)G_;
+        DataflowArgs df;
+        df.done = d_done_;
+        df.err = d_ctl_;
+        df.abort = d_ctl_ + 3;
+        df.epoch = d_ctl_ + 4;
+        df.n_items = sched_.items.size();
+        df.spin_limit = 1u << 22;  // ~4 s of polling with backoff
+        TY_CUDA(launch_bump_epoch(d_ctl_ + 4, stream_));
+        if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
+        TY_CUDA(prec ? launch_dataflow<float>(tpi32_, p, df, grid32_, stream_)
+                     : launch_dataflow<double>(tpi64_, p, df, grid64_, stream_));
+        if (end) TY_CUDA(cudaEventRecord(end, stream_));
+        return kOk;
+    }
     auto key = std::make_tuple(prec, has_iso, qang);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
@@ -268,7 +362,7 @@ int Sweeper::sweep_host(const double *source, double *psi, std::string &err)
     TY_CHECK(apply(0, nullptr, false, nullptr, d_src_, err));
     TY_CUDA(cudaMemcpyAsync(psi, d_psi_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
     TY_CUDA(cudaStreamSynchronize(stream_));
-    return kOk;
+    return check_device_error(err);
 }
 
 int Sweeper::ensure_krylov(int m, std::string &err)
@@ -452,7 +546,7 @@ int Sweeper::solve(const SolveOptions &o, double *phi_out, double *psi_out, Solv
     if (phi_out) TY_CUDA(cudaMemcpyAsync(phi_out, d_phi_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
     if (psi_out) TY_CUDA(cudaMemcpyAsync(psi_out, d_psi_, sizeof(double) * psi_size(), cudaMemcpyDeviceToHost, stream_));
     TY_CUDA(cudaStreamSynchronize(stream_));
-    if (status == kErrNotConverged) err = "iteration limit reached before the tolerance";
+    if (status == kOk) status = check_device_error(err);
     return status;
 }
 
@@ -509,6 +603,7 @@ int Sweeper::time_sweeps(int prec, int n, bool flush_l2, double *ms, std::string
         lvl += b;
     }
     cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(l0); cudaEventDestroy(l1);
+    if (status == kOk) status = check_device_error(err);
     ms[0] = tot / n;
     ms[1] = lvl / n;
     return status;

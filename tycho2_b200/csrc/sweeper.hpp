@@ -23,6 +23,7 @@ struct SweeperOptions {
     bool fp32 = false;
     int tpi64 = 0;  // 0 = auto
     int tpi32 = 0;
+    int schedule = 0;  // 0 auto (dataflow), 1 level-synchronous, 2 dataflow
 };
 
 struct SolveOptions {
@@ -52,6 +53,10 @@ public:
               std::string &err);
     int write_psi(const std::string &path, std::string &err);
     int time_sweeps(int precision, int n, bool flush_l2, double *ms, std::string &err);
+    // Launch shape of one precision: threads per item and schedule.
+    int configure(int prec, int tpi, bool dataflow, std::string &err);
+    int autotune(int prec, int reps, int *best_tpi, int *best_sched, double *best_ms, std::string &err);
+    bool dataflow(int prec) const { return prec ? dataflow32_ : dataflow64_; }
 
     // One operator application, on the device:
     //   phi_out = D L^{-1} ( [Q] + M S phi_in )     (phi_in / phi_out nullable)
@@ -73,6 +78,8 @@ public:
 private:
     int levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg, cudaEvent_t end,
                std::string &err);
+    // Reads (and clears) the dataflow schedule's device error word.
+    int check_device_error(std::string &err);
     int gmres(int prec, const double *b, double *x, int restart, double rtol, int iter_max,
               int &its, double &rnorm, SolveStats &st, std::string &err);
     int ensure_krylov(int restart, std::string &err);
@@ -108,6 +115,11 @@ private:
     void *d_flush_ = nullptr;
     Reducer red_;
     std::map<std::tuple<int, bool, const double *>, cudaGraphExec_t> graphs_;
+    // dataflow schedule
+    bool dataflow64_ = true, dataflow32_ = true;
+    unsigned grid64_ = 0, grid32_ = 0;
+    uint32_t *d_done_ = nullptr;   // per item: epoch of completion
+    uint32_t *d_ctl_ = nullptr;    // [0..2] error, [3] abort, [4] epoch
 };
 
 }  // namespace tycho

@@ -48,6 +48,19 @@ class TychoMesh:
         check(lib().tycho_mesh_kuhn_cube(n, jitter, seed, length, C.byref(h)))
         return cls(h.value)
 
+    @classmethod
+    def from_arrays(cls, cell_nodes, coords, adj_cell, face_to_cell, cell_gid=None):
+        """From the arrays a reference TychoMesh exposes through its getters."""
+        cn = np.ascontiguousarray(cell_nodes, np.uint64)
+        xyz = np.ascontiguousarray(coords, np.float64)
+        adj = np.ascontiguousarray(adj_cell, np.uint64)
+        f2c = np.ascontiguousarray(face_to_cell, np.uint64)
+        gid = None if cell_gid is None else np.ascontiguousarray(cell_gid, np.uint64)
+        h = C.c_void_p()
+        check(lib().tycho_mesh_from_arrays(cn.shape[0], xyz.shape[0], ptr(cn), ptr(xyz), ptr(adj),
+                                           ptr(f2c), ptr(gid), C.byref(h)))
+        return cls(h.value)
+
     def write_smesh(self, path):
         check(lib().tycho_mesh_write_smesh(self._h, str(path).encode()))
 
@@ -130,8 +143,10 @@ class SweeperCuda:
     refinement on the device and keeps psi resident.
     """
 
+    SCHEDULES = {"auto": 0, "levels": 1, "dataflow": 2}
+
     def __init__(self, mesh, sn_order, n_groups, gauss_elim="NoPivot", fp32=False, device=0,
-                 tpi64=0, tpi32=0):
+                 tpi64=0, tpi32=0, schedule="auto"):
         if gauss_elim not in GAUSS_ELIM:
             raise ValueError("GaussElim must be one of %s" % sorted(GAUSS_ELIM))
         self.mesh = mesh
@@ -139,7 +154,7 @@ class SweeperCuda:
         self.quadrature = Quadrature(sn_order)
         self.n_angles = self.quadrature.n_angles
         opts = _capi.SweeperOpts(sn_order, n_groups, GAUSS_ELIM[gauss_elim], device, int(fp32),
-                                 tpi64, tpi32)
+                                 tpi64, tpi32, self.SCHEDULES[schedule])
         h = C.c_void_p()
         check(lib().tycho_sweeper_create(mesh._h, C.byref(opts), C.byref(h)))
         self._h = h
@@ -206,6 +221,16 @@ class SweeperCuda:
         ms = np.zeros(2)
         check(lib().tycho_sweeper_time_sweeps(self._h, precision, n, int(flush_l2), ptr(ms)))
         return float(ms[0]), float(ms[1])
+
+    def autotune(self, precision, reps=3):
+        """Picks the fastest (schedule, threads-per-item) for one precision."""
+        t, s, ms = C.c_int(), C.c_int(), C.c_double()
+        check(lib().tycho_sweeper_autotune(self._h, precision, reps, C.byref(t), C.byref(s),
+                                           C.byref(ms)))
+        return {"tpi": t.value, "schedule": {1: "levels", 2: "dataflow"}[s.value], "ms": ms.value}
+
+    def configure(self, precision, schedule, tpi):
+        check(lib().tycho_sweeper_configure(self._h, precision, self.SCHEDULES[schedule], tpi))
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value and _capi._lib is not None:
