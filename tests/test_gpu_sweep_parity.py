@@ -222,12 +222,13 @@ def test_missing_inputs_are_errors(built, workdir):
     with pytest.raises(ty.TychoError) as e:
         sw.solve("si")
     assert e.value.status == 10
-    sw.set_cross_sections(np.ones(mesh.n_cells), np.zeros(mesh.n_cells))
+    sw.set_cross_sections(np.ones(mesh.n_cells), np.full(mesh.n_cells, 0.5))
     with pytest.raises(ty.TychoError) as e:
         sw.solve("mixed")  # created without the FP32 sweep
     assert e.value.status == 1
     # Like SourceIteration::fixedPoint, hitting iterMax is not an error: the
     # caller reads the last relative change.
+    sw.set_source(np.ones(sw.phi_shape), "isotropic")
     phi, psi, stats = sw.solve("si", iter_max=2, err_max=1e-30)
     assert stats["iterations"] == 2 and stats["final_error"] > 1e-30
 
