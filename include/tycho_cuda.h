@@ -206,6 +206,29 @@ int tycho_sweeper_autotune(tycho_sweeper *sw, int precision, int reps, int *best
 /* Sets the launch shape explicitly (schedule 1 or 2, tpi 1..16). */
 int tycho_sweeper_configure(tycho_sweeper *sw, int precision, int schedule, int tpi);
 
+/* A sweep that allocates nothing.  No counterpart in the reference.
+   For callers that cannot allocate device memory when they sweep: code under
+   CUDA stream capture (cudaMalloc is refused during a global-mode capture), a
+   host framework that owns all device memory through its own pool and
+   budget, or a time-critical loop that cannot afford cudaMalloc's implicit
+   synchronization.  psi = L^{-1} iso for an isotropic source on the caller's
+   own device buffers, in the sweep precision (0: double, 1: float):
+     iso  phi layout (cell*4 + vertex)*G + group, may be NULL (zero source);
+     psi  psi layout, written.
+   The persistent dataflow kernel's scratch (per-item completion flags and
+   control words) lives in one file-scope device array of 64 MiB + 256 B,
+   which every GPU that loads this library holds until the process exits, so
+   at most 16,777,216 cells x angles are accepted (larger: TYCHO_ERR_ARG).
+   The first call on a device looks up that array's device address; make it
+   before any stream capture.  All calls share the array and each leaves its
+   flags behind (a per-call epoch makes them stale; the error and abort words
+   are cleared at the start of every call), so calls that overlap on the GPU
+   race.  The call runs on `stream` (a cudaStream_t, NULL = legacy default
+   stream), synchronizes it and returns TYCHO_ERR_TIMEOUT if a bounded wait
+   gave up.  The sweeper's own buffers and results are not touched. */
+int tycho_sweeper_sweep_noalloc(tycho_sweeper *sw, int precision, const void *iso, void *psi,
+                                void *stream);
+
 /* Device timing of n back-to-back operator applications
    phi_out = D L^{-1} (M S phi_in + Q) in the given precision, on the
    sweeper's stream with CUDA events (inputs resident).  ms[0] = mean time

@@ -71,6 +71,7 @@ SIGNATURES = {
     "tycho_sweeper_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_int),
                                          C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "tycho_sweeper_configure": (C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
+    "tycho_sweeper_sweep_noalloc": (C.c_int, [_P, C.c_int, _P, _P, _P]),
 }
 
 _lib = None

@@ -378,6 +378,13 @@ int tycho_sweeper_configure(tycho_sweeper *h, int precision, int schedule, int t
     return finish(h->sw.configure(precision, tpi, schedule == 2, err), err);
 }
 
+int tycho_sweeper_sweep_noalloc(tycho_sweeper *h, int precision, const void *iso, void *psi, void *stream)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    std::string err;
+    return finish(tycho::sweep_noalloc(h->sw, precision, iso, psi, stream, err), err);
+}
+
 int tycho_sweeper_time_sweeps(tycho_sweeper *h, int precision, int n, int flush_l2, double *ms)
 {
     if (!h || !ms) return finish(TYCHO_ERR_ARG, "null argument");

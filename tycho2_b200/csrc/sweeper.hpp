@@ -64,6 +64,14 @@ public:
     int apply(int prec, const double *phi_in, bool with_fixed, double *phi_out,
               const double *qang_override, std::string &err);
 
+    // One persistent-dataflow sweep psi = L^{-1} iso on caller-owned device
+    // buffers (iso: phi layout, may be null; psi: psi layout; both in the
+    // sweep precision), with caller-provided completion flags (n_items words)
+    // and control words (ctl[0..2] error, [3] abort, [4] epoch).  Allocates
+    // nothing; synchronizes `s` and reports a timed-out wait.
+    int sweep_external(int prec, const void *iso, void *psi, uint32_t *done, uint32_t *ctl,
+                       cudaStream_t s, std::string &err);
+
     const MeshTables &tables() const { return tables_; }
     const Quadrature &quadrature() const { return quad_; }
     const Schedule &schedule() const { return sched_; }
@@ -74,6 +82,7 @@ public:
     uint64_t psi_size() const { return nc_ * (uint64_t)A_ * 4 * G_; }
     cudaStream_t stream() const { return stream_; }
     int tpi(int prec) const { return prec ? tpi32_ : tpi64_; }
+    int device() const { return device_; }
 
 private:
     int levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg, cudaEvent_t end,
@@ -121,5 +130,10 @@ private:
     uint32_t *d_done_ = nullptr;   // per item: epoch of completion
     uint32_t *d_ctl_ = nullptr;    // [0..2] error, [3] abort, [4] epoch
 };
+
+// The no-alloc sweep (tycho_sweeper_sweep_noalloc, sweep_noalloc.cu): scratch
+// in a fixed file-scope device array instead of allocated memory.
+int sweep_noalloc(Sweeper &sw, int precision, const void *iso, void *psi, void *stream,
+                  std::string &err);
 
 }  // namespace tycho
