@@ -196,15 +196,27 @@ int tycho_sweeper_schedule_info(const tycho_sweeper *sw, uint32_t *n_levels, uin
 int tycho_sweeper_levels(const tycho_sweeper *sw, uint32_t *tlevel, uint32_t *deps,
                          uint32_t *blevel);
 
-/* Autotuner: times every launch shape of the given precision's sweep --
-   schedule (1 = one launch per level, 2 = persistent dataflow) x threads per
-   (cell, angle) item (1..16, i.e. the group tiling) -- with `reps` operator
-   applications each on this instance's own problem, keeps the fastest and
-   reports it.  Cross sections must be set. */
-int tycho_sweeper_autotune(tycho_sweeper *sw, int precision, int reps, int *best_tpi,
-                           int *best_schedule, double *best_ms);
-/* Sets the launch shape explicitly (schedule 1 or 2, tpi 1..16). */
-int tycho_sweeper_configure(tycho_sweeper *sw, int precision, int schedule, int tpi);
+/* Launch shape of one precision's sweep:
+     schedule 1 = one launch per wavefront level, 2 = persistent dataflow;
+     variant  0 = item-parallel: knob lanes per (cell, angle) item, each lane
+                  a strided subset of the groups (group tiling; 1..16),
+              1 = warp tiles: 32 items per warp, factors in shared memory,
+                  knob warps per block (1, 2, 4). */
+typedef struct tycho_launch_shape {
+    int schedule;
+    int variant;
+    int knob;
+} tycho_launch_shape;
+
+/* Autotuner: times every launch shape of the given precision's sweep with
+   `reps` operator applications each on this instance's own problem, keeps
+   the fastest and reports it.  Cross sections must be set. */
+int tycho_sweeper_autotune(tycho_sweeper *sw, int precision, int reps, tycho_launch_shape *best,
+                           double *best_ms);
+/* Sets the launch shape explicitly. */
+int tycho_sweeper_configure(tycho_sweeper *sw, int precision, const tycho_launch_shape *shape);
+/* Reads the current launch shape. */
+int tycho_sweeper_get_shape(const tycho_sweeper *sw, int precision, tycho_launch_shape *shape);
 
 /* A sweep that allocates nothing.  No counterpart in the reference.
    For callers that cannot allocate device memory when they sweep: code under

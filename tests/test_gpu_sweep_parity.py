@@ -22,26 +22,31 @@ def test_fp64_sweep_bit_exact_vs_reference_fixture(built, kuhn3_ref):
     import tycho2_b200 as ty
     r = kuhn3_ref
     mesh = ty.TychoMesh.kuhn_cube(3, 0.05, 2024, 100.0)
-    for tpi, schedule in ((1, "levels"), (2, "levels"), (1, "dataflow"), (4, "dataflow")):
-        sw = make(mesh, 4, 3, tpi64=tpi, schedule=schedule)
+    for shape in (("levels", "items", 1), ("levels", "items", 2), ("dataflow", "items", 4),
+                  ("levels", "tiles", 4), ("dataflow", "tiles", 1), ("dataflow", "tiles", 2)):
+        sw = make(mesh, 4, 3)
+        sw.configure(0, *shape)
         sw.set_cross_sections(r["sweep_sigma_t"], np.zeros(mesh.n_cells))
         psi = np.empty(sw.psi_shape)
         sw.sweep(psi, r["sweep_source"])
-        assert bits_equal(psi, r["sweep_psi"]), "tpi=%d" % tpi
+        assert bits_equal(psi, r["sweep_psi"]), shape
 
 
 @pytest.mark.parametrize("schedule", ["levels", "dataflow"])
+@pytest.mark.parametrize("variant", ["items", "tiles"])
 @pytest.mark.parametrize("n,jitter,sn,G,tpi", [
     (4, 0.05, 4, 1, 1), (5, 0.05, 8, 2, 2), (3, 0.0, 2, 3, 1), (6, 0.05, 6, 4, 4),
-    (4, 0.07, 8, 8, 8), (2, 0.05, 4, 16, 16), (7, 0.05, 4, 5, 2), (1, 0.0, 4, 1, 1)])
-def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi, schedule):
+    (4, 0.07, 8, 8, 8), (2, 0.05, 4, 16, 16), (7, 0.05, 4, 5, 2), (1, 0.0, 4, 1, 1),
+    (3, 0.05, 4, 64, 4), (2, 0.05, 4, 33, 1)])
+def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi, variant, schedule):
     from oracle.oracle import Oracle
     mesh, om = kuhn(workdir, n, jitter, seed=5)
     o = Oracle(om, sn, G)
     rng = np.random.default_rng(n * 100 + G)
     st = rng.lognormal(0.0, 0.5, mesh.n_cells)
     src = rng.uniform(-0.2, 1.0, o.psi_shape)
-    sw = make(mesh, sn, G, tpi64=tpi, schedule=schedule)
+    sw = make(mesh, sn, G)
+    sw.configure(0, schedule, variant, tpi if variant == "items" else min(tpi, 4))
     sw.set_cross_sections(st, np.zeros(mesh.n_cells))
     psi = np.empty(sw.psi_shape)
     sw.sweep(psi, src)
@@ -157,17 +162,18 @@ def test_fp32_sweep_within_tolerance(built, workdir):
     st = rng.lognormal(0.0, 0.5, mesh.n_cells)
     mat = problems.downscatter_matrix(G, 0.6)
     q = rng.uniform(0.0, 1.0, o.phi_shape)
-    psi_o = o.sweep(st, src_iso=np.ascontiguousarray(q))
-    for tpi in (1, 4, 8):
-        sw = make(mesh, 8, G, fp32=True, tpi32=tpi)
+    psi_ref, phi_ref, _, _ = o.krylov(st, st, mat, q_iso=q, restart=20, iter_max=200, rtol=1e-11)
+    for shape in (("levels", "items", 1), ("levels", "items", 8), ("dataflow", "items", 4),
+                  ("levels", "tiles", 2), ("dataflow", "tiles", 4)):
+        sw = make(mesh, 8, G, fp32=True)
+        sw.configure(1, *shape)
         sw.set_cross_sections(st, st, mat)
         sw.set_source(q, "isotropic")
-        # one FP32 mixed solve step exercises the FP32 operator; compare the
-        # FP32 operator directly through a converged mixed solve instead:
+        # The FP32 operator inside FP64 refinement: converged phi within 1e-8.
         phi, psi, stats = sw.solve("mixed", iter_max=200, err_max=1e-11, restart=20)
-        psi_ref, phi_ref, _, _ = o.krylov(st, st, mat, q_iso=q, restart=20, iter_max=200, rtol=1e-11)
-        assert rel_l1(phi, phi_ref) <= 1e-8, tpi
+        assert rel_l1(phi, phi_ref) <= 1e-8, shape
         assert stats["sweeps_fp32"] > stats["sweeps_fp64"]
+        sw.close()
 
 
 def test_mixed_vs_fp64_gmres_and_si(built, workdir):
@@ -246,7 +252,8 @@ def test_autotune_keeps_results_bit_exact(built, workdir):
     sw.set_cross_sections(st, np.zeros(mesh.n_cells))
     best64 = sw.autotune(0, reps=2)
     best32 = sw.autotune(1, reps=2)
-    assert best64["tpi"] in (1, 2, 4, 8, 16) and best32["schedule"] in ("levels", "dataflow")
+    assert best64["variant"] in ("items", "tiles") and best32["schedule"] in ("levels", "dataflow")
+    assert sw.shape(0) == {k: best64[k] for k in ("schedule", "variant", "knob")}
     psi = np.empty(sw.psi_shape)
     sw.sweep(psi, src)
     assert bits_equal(psi, o.sweep(st, src_ang=src))

@@ -38,6 +38,10 @@ class SolveOpts(C.Structure):
                 ("restart", C.c_int), ("inner_tol", C.c_double), ("refine_max", C.c_int)]
 
 
+class LaunchShape(C.Structure):
+    _fields_ = [("schedule", C.c_int), ("variant", C.c_int), ("knob", C.c_int)]
+
+
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("sweeps_fp64", C.c_int), ("sweeps_fp32", C.c_int),
                 ("refinements", C.c_int), ("final_error", C.c_double), ("seconds", C.c_double)]
@@ -68,9 +72,10 @@ SIGNATURES = {
     "tycho_sweeper_schedule_info": (C.c_int, [_P, _U32P, _U64P, _U64P]),
     "tycho_sweeper_levels": (C.c_int, [_P, _P, _P, _P]),
     "tycho_sweeper_time_sweeps": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P]),
-    "tycho_sweeper_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_int),
-                                         C.POINTER(C.c_int), C.POINTER(C.c_double)]),
-    "tycho_sweeper_configure": (C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
+    "tycho_sweeper_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(LaunchShape),
+                                         C.POINTER(C.c_double)]),
+    "tycho_sweeper_configure": (C.c_int, [_P, C.c_int, C.POINTER(LaunchShape)]),
+    "tycho_sweeper_get_shape": (C.c_int, [_P, C.c_int, C.POINTER(LaunchShape)]),
     "tycho_sweeper_sweep_noalloc": (C.c_int, [_P, C.c_int, _P, _P, _P]),
 }
 

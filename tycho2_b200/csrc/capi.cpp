@@ -360,22 +360,41 @@ int tycho_sweeper_levels(const tycho_sweeper *h, uint32_t *tlevel, uint32_t *dep
     });
 }
 
-int tycho_sweeper_autotune(tycho_sweeper *h, int precision, int reps, int *best_tpi, int *best_schedule,
+int tycho_sweeper_autotune(tycho_sweeper *h, int precision, int reps, tycho_launch_shape *best,
                            double *best_ms)
 {
-    if (!h || reps < 1) return finish(TYCHO_ERR_ARG, "null sweeper or reps < 1");
+    if (!h || reps < 1 || (precision != 0 && precision != 1))
+        return finish(TYCHO_ERR_ARG, "null sweeper, reps < 1 or bad precision");
     std::string err;
     return guarded([&] {
-        return finish(h->sw.autotune(precision, reps, best_tpi, best_schedule, best_ms, err), err);
+        tycho::LaunchShape sh;
+        int s = h->sw.autotune(precision, reps, &sh, best_ms, err);
+        if (s == tycho::kOk && best) {
+            best->schedule = sh.schedule;
+            best->variant = sh.variant;
+            best->knob = sh.knob;
+        }
+        return finish(s, err);
     });
 }
 
-int tycho_sweeper_configure(tycho_sweeper *h, int precision, int schedule, int tpi)
+int tycho_sweeper_configure(tycho_sweeper *h, int precision, const tycho_launch_shape *shape)
 {
-    if (!h || (schedule != 1 && schedule != 2) || (precision != 0 && precision != 1))
-        return finish(TYCHO_ERR_ARG, "bad sweeper, precision or schedule");
+    if (!h || !shape || (precision != 0 && precision != 1))
+        return finish(TYCHO_ERR_ARG, "bad sweeper, precision or shape");
     std::string err;
-    return finish(h->sw.configure(precision, tpi, schedule == 2, err), err);
+    return finish(h->sw.configure(precision, shape->schedule, shape->variant, shape->knob, err), err);
+}
+
+int tycho_sweeper_get_shape(const tycho_sweeper *h, int precision, tycho_launch_shape *shape)
+{
+    if (!h || !shape || (precision != 0 && precision != 1))
+        return finish(TYCHO_ERR_ARG, "bad sweeper, precision or shape");
+    const tycho::LaunchShape &sh = h->sw.shape(precision);
+    shape->schedule = sh.schedule;
+    shape->variant = sh.variant;
+    shape->knob = sh.knob;
+    return TYCHO_OK;
 }
 
 int tycho_sweeper_sweep_noalloc(tycho_sweeper *h, int precision, const void *iso, void *psi, void *stream)

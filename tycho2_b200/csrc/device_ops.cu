@@ -4,12 +4,16 @@
 // scalar flux and the scattering source keep the reference's rounding.
 #include "device_ops.hpp"
 #include "sweep_kernels.cuh"
+#include "sweep_tiles.cuh"
 
 namespace tycho {
 
 template cudaError_t launch_level<double>(int, const LevelArgs &, uint64_t, uint64_t, cudaStream_t);
 template cudaError_t launch_dataflow<double>(int, const LevelArgs &, const DataflowArgs &, unsigned, cudaStream_t);
 template cudaError_t dataflow_blocks_per_sm<double>(int, int *);
+template cudaError_t launch_level_tile<double>(int, const LevelArgs &, uint64_t, uint64_t, cudaStream_t);
+template cudaError_t launch_dataflow_tile<double>(int, const LevelArgs &, const DataflowArgs &, unsigned, cudaStream_t);
+template cudaError_t tile_dataflow_blocks_per_sm<double>(int, int *);
 
 namespace {
 

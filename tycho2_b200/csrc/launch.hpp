@@ -18,6 +18,7 @@ struct LevelArgs {
     const double *qang;      // angular source, psi layout, FP64 only (nullable)
     void *psi;               // Real, psi layout
     uint32_t A, G;
+    uint32_t gmagic;         // ceil(2^32 / G): pair -> item in the warp-tile variant (0 when G == 1)
 };
 
 // Per-sweep state of the persistent (dataflow) schedule.
@@ -43,5 +44,15 @@ cudaError_t launch_dataflow(int tpi, const LevelArgs &p, const DataflowArgs &df,
                             cudaStream_t s);
 template <typename Real>
 cudaError_t dataflow_blocks_per_sm(int tpi, int *blocks);
+
+// Warp-tile variant (sweep_tiles.cuh): 32 items per warp, `wpb` warps per
+// block (1, 2 or 4); same contracts as the launchers above.
+template <typename Real>
+cudaError_t launch_level_tile(int wpb, const LevelArgs &p, uint64_t begin, uint64_t end, cudaStream_t s);
+template <typename Real>
+cudaError_t launch_dataflow_tile(int wpb, const LevelArgs &p, const DataflowArgs &df, unsigned grid,
+                                 cudaStream_t s);
+template <typename Real>
+cudaError_t tile_dataflow_blocks_per_sm(int wpb, int *blocks);
 
 }  // namespace tycho

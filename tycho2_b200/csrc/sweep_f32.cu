@@ -2,11 +2,15 @@
 // Compiled with FMA contraction on: this path is checked against the FP64
 // sweep by tolerance, not bit for bit.
 #include "sweep_kernels.cuh"
+#include "sweep_tiles.cuh"
 
 namespace tycho {
 
 template cudaError_t launch_level<float>(int, const LevelArgs &, uint64_t, uint64_t, cudaStream_t);
 template cudaError_t launch_dataflow<float>(int, const LevelArgs &, const DataflowArgs &, unsigned, cudaStream_t);
 template cudaError_t dataflow_blocks_per_sm<float>(int, int *);
+template cudaError_t launch_level_tile<float>(int, const LevelArgs &, uint64_t, uint64_t, cudaStream_t);
+template cudaError_t launch_dataflow_tile<float>(int, const LevelArgs &, const DataflowArgs &, unsigned, cudaStream_t);
+template cudaError_t tile_dataflow_blocks_per_sm<float>(int, int *);
 
 }  // namespace tycho

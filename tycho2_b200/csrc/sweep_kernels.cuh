@@ -25,6 +25,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "launch.hpp"
@@ -47,6 +48,22 @@ struct ItemFactor {
     Real r0, u01, u02, u03, l1, l2, l3, r1, u12, u13, a21, a31, r2, u23, b32, c33;
 };
 
+// FP64 keeps the reference's IEEE divisions (bit-identical results); FP32,
+// checked by tolerance, uses reciprocals.
+template <typename Real>
+__device__ __forceinline__ Real div_ref(Real x, Real y)
+{
+    if constexpr (std::is_same<Real, float>::value) return x * __frcp_rn(y);
+    else return x / y;
+}
+
+template <typename Real>
+__device__ __forceinline__ Real over12(Real x)
+{
+    if constexpr (std::is_same<Real, float>::value) return x * (1.0f / 12.0f);
+    else return x / 12.0;
+}
+
 template <typename Real>
 __device__ __forceinline__ void item_setup(const LevelArgs &p, uint64_t it, uint32_t ca, ItemFactor<Real> &F)
 {
@@ -65,8 +82,8 @@ __device__ __forceinline__ void item_setup(const LevelArgs &p, uint64_t it, uint
     // Face terms A_f/12 and 2 A_f/12 with A_f = area * omega.n.
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-        F.t1[f] = F.ab[f] / Real(12);
-        F.t2[f] = Real(2) * F.ab[f] / Real(12);
+        F.t1[f] = over12(F.ab[f]);
+        F.t2[f] = over12(Real(2) * F.ab[f]);
     }
     // Streaming + collision (volume integrals), then outgoing-face terms in
     // increasing face order.
@@ -87,19 +104,19 @@ __device__ __forceinline__ void item_setup(const LevelArgs &p, uint64_t it, uint
     }
     // LU without pivoting: the elimination steps of gaussElim4 NoPivot that
     // touch only the matrix.
-    F.r0 = Real(1) / M[0][0];
+    F.r0 = div_ref(Real(1), M[0][0]);
     F.u01 = M[0][1] * F.r0; F.u02 = M[0][2] * F.r0; F.u03 = M[0][3] * F.r0;
     F.l1 = M[1][0]; F.l2 = M[2][0]; F.l3 = M[3][0];
     const Real a11 = M[1][1] - F.u01 * F.l1, a12 = M[1][2] - F.u02 * F.l1, a13 = M[1][3] - F.u03 * F.l1;
     const Real a21 = M[2][1] - F.u01 * F.l2, a22 = M[2][2] - F.u02 * F.l2, a23 = M[2][3] - F.u03 * F.l2;
     const Real a31 = M[3][1] - F.u01 * F.l3, a32 = M[3][2] - F.u02 * F.l3, a33 = M[3][3] - F.u03 * F.l3;
     F.a21 = a21; F.a31 = a31;
-    F.r1 = Real(1) / a11;
+    F.r1 = div_ref(Real(1), a11);
     F.u12 = a12 * F.r1; F.u13 = a13 * F.r1;
     const Real b22 = a22 - F.u12 * a21, b23 = a23 - F.u13 * a21;
     F.b32 = a32 - F.u12 * a31;
     const Real b33 = a33 - F.u13 * a31;
-    F.r2 = Real(1) / b22;
+    F.r2 = div_ref(Real(1), b22);
     F.u23 = b23 * F.r2;
     F.c33 = b33 - F.u23 * F.b32;
 }
@@ -173,7 +190,7 @@ __device__ __forceinline__ void item_groups(const LevelArgs &p, uint32_t ca, int
         b[3] = b[3] - b[1] * F.a31;
         b[2] = b[2] * F.r2;
         b[3] = b[3] - b[2] * F.b32;
-        b[3] = b[3] / F.c33;
+        b[3] = div_ref(b[3], F.c33);
         b[2] = b[2] - F.u23 * b[3];
         b[1] = b[1] - F.u13 * b[3] - F.u12 * b[2];
         b[0] = b[0] - F.u03 * b[3] - F.u02 * b[2] - F.u01 * b[1];

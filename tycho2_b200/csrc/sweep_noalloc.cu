@@ -82,17 +82,7 @@ int Sweeper::sweep_external(int prec, const void *iso, void *psi, uint32_t *done
     if (prec == 1 && !fp32_) { err = "sweeper was created without the FP32 sweep"; return kErrArg; }
     if (!have_xs_) { err = "cross sections not set"; return kErrMissing; }
     if (!psi) { err = "psi buffer is required"; return kErrArg; }
-    LevelArgs p;
-    p.items = d_items_;
-    p.abar = prec ? (const void *)d_abar32_ : (const void *)d_abar64_;
-    p.adj = d_adj_;
-    p.nbrmap = d_nbrmap_;
-    p.cellk = prec ? (const void *)d_cellk32_ : (const void *)d_cellk64_;
-    p.iso = iso;
-    p.qang = nullptr;
-    p.psi = psi;
-    p.A = (uint32_t)A_;
-    p.G = (uint32_t)G_;
+    const LevelArgs p = level_args(prec, iso, nullptr, psi);
     DataflowArgs df;
     df.done = done;
     df.err = ctl;
@@ -105,11 +95,14 @@ int Sweeper::sweep_external(int prec, const void *iso, void *psi, uint32_t *done
         noalloc_begin_kernel<<<1, 1, 0, s>>>(ctl);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess)
-        e = prec ? launch_dataflow<float>(tpi32_, p, df, grid32_, s)
-                 : launch_dataflow<double>(tpi64_, p, df, grid64_, s);
+    if (e != cudaSuccess) {
+        err = std::string("no-alloc sweep: ") + cudaGetErrorString(e);
+        return kErrCuda;
+    }
+    const int st = launch_dataflow_shape(prec, p, df, s, err);
+    if (st != kOk) return st;
     uint32_t word[3] = {0, 0, 0};
-    if (e == cudaSuccess) e = cudaMemcpyAsync(word, ctl, sizeof word, cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(word, ctl, sizeof word, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         err = std::string("no-alloc sweep: ") + cudaGetErrorString(e);

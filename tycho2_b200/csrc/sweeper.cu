@@ -43,10 +43,9 @@ cudaError_t upload(T *&dst, const T *src, size_t n, cudaStream_t s)
     return e;
 }
 
-int auto_tpi(int G, bool fp32)
+uint32_t group_magic(uint32_t G)
 {
-    if (fp32) return G >= 16 ? 8 : (G >= 8 ? 4 : (G >= 4 ? 2 : 1));
-    return G >= 16 ? 4 : (G >= 8 ? 2 : 1);
+    return G == 1 ? 0u : (uint32_t)(((1ull << 32) + G - 1) / G);
 }
 
 }  // namespace
@@ -81,8 +80,6 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     A_ = quad_.n_angles;
     G_ = o.n_groups;
     fp32_ = o.fp32;
-    tpi64_ = o.tpi64 ? o.tpi64 : auto_tpi(G_, false);
-    tpi32_ = o.tpi32 ? o.tpi32 : auto_tpi(G_, true);
     TY_CHECK(build_schedule(tables_, quad_, sched_, err));
     TY_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
 
@@ -147,26 +144,41 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     TY_CUDA(cudaMemsetAsync(d_done_, 0, sizeof(uint32_t) * (size_t)nc_ * A_, stream_));
     TY_CUDA(cudaMalloc(&d_ctl_, sizeof(uint32_t) * 8));
     TY_CUDA(cudaMemsetAsync(d_ctl_, 0, sizeof(uint32_t) * 8, stream_));
-    const bool dataflow = o.schedule != 1;
-    TY_CHECK(configure(0, tpi64_, dataflow, err));
-    TY_CHECK(configure(1, tpi32_, dataflow, err));
+    // Default launch shape: warp tiles (4 warps per block) on the persistent
+    // dataflow schedule; explicit threads-per-item selects the item-parallel
+    // variant.  The autotuner can replace either.
+    const int sched = o.schedule == 1 ? 1 : 2;
+    TY_CHECK(configure(0, sched, o.tpi64 ? 0 : 1, o.tpi64 ? o.tpi64 : 4, err));
+    TY_CHECK(configure(1, sched, o.tpi32 ? 0 : 1, o.tpi32 ? o.tpi32 : 4, err));
     TY_CUDA(cudaStreamSynchronize(stream_));
     return kOk;
 }
 
-int Sweeper::configure(int prec, int tpi, bool dataflow, std::string &err)
+int Sweeper::configure(int prec, int schedule, int variant, int knob, std::string &err)
 {
-    if (tpi != 1 && tpi != 2 && tpi != 4 && tpi != 8 && tpi != 16) {
-        err = "threads per item must be 1, 2, 4, 8 or 16";
+    if (schedule != 1 && schedule != 2) { err = "schedule must be 1 (levels) or 2 (dataflow)"; return kErrArg; }
+    if (variant == 0 && knob != 1 && knob != 2 && knob != 4 && knob != 8 && knob != 16) {
+        err = "item-parallel variant: threads per item must be 1, 2, 4, 8 or 16";
         return kErrArg;
     }
+    if (variant == 1 && knob != 1 && knob != 2 && knob != 4) {
+        err = "warp-tile variant: warps per block must be 1, 2 or 4";
+        return kErrArg;
+    }
+    if (variant != 0 && variant != 1) { err = "variant must be 0 (item-parallel) or 1 (warp tiles)"; return kErrArg; }
     int sms = 0, per_sm = 0;
     TY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
-    TY_CUDA(prec ? dataflow_blocks_per_sm<float>(tpi, &per_sm) : dataflow_blocks_per_sm<double>(tpi, &per_sm));
+    if (variant == 0)
+        TY_CUDA(prec ? dataflow_blocks_per_sm<float>(knob, &per_sm) : dataflow_blocks_per_sm<double>(knob, &per_sm));
+    else
+        TY_CUDA(prec ? tile_dataflow_blocks_per_sm<float>(knob, &per_sm)
+                     : tile_dataflow_blocks_per_sm<double>(knob, &per_sm));
     if (per_sm < 1) { err = "dataflow kernel does not fit on an SM"; return kErrCuda; }
-    (prec ? tpi32_ : tpi64_) = tpi;
-    (prec ? dataflow32_ : dataflow64_) = dataflow;
-    (prec ? grid32_ : grid64_) = (unsigned)(sms * per_sm);
+    LaunchShape &sh = shape_[prec ? 1 : 0];
+    sh.schedule = schedule;
+    sh.variant = variant;
+    sh.knob = knob;
+    sh.grid = (unsigned)(sms * per_sm);
     // cached level graphs were captured for the previous launch shape
     for (auto it = graphs_.begin(); it != graphs_.end();) {
         if (std::get<0>(it->first) == prec) {
@@ -179,28 +191,61 @@ int Sweeper::configure(int prec, int tpi, bool dataflow, std::string &err)
     return kOk;
 }
 
-// Times every (schedule, threads-per-item) candidate on this instance's own
-// problem with a few operator applications and keeps the fastest.
-int Sweeper::autotune(int prec, int reps, int *best_tpi, int *best_sched, double *best_ms, std::string &err)
+// Times every launch shape -- schedule x variant x (threads per item or warps
+// per block) -- on this instance's own problem and keeps the fastest.
+int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_ms, std::string &err)
 {
     if (prec == 1 && !fp32_) { err = "sweeper was created without the FP32 sweep"; return kErrArg; }
     if (!have_xs_) { err = "cross sections not set"; return kErrMissing; }
     double best = 1e300;
-    int btpi = tpi(prec), bdf = (prec ? dataflow32_ : dataflow64_) ? 2 : 1;
+    LaunchShape keep = shape_[prec ? 1 : 0];
     for (int sched = 1; sched <= 2; ++sched)
-        for (int t : {1, 2, 4, 8, 16}) {
-            if (t > 2 * G_ && t > 1) continue;  // lanes with no group to update
-            TY_CHECK(configure(prec, t, sched == 2, err));
-            double ms[2];
-            TY_CHECK(time_sweeps(prec, 1, false, ms, err));  // warm-up (and graph capture)
-            TY_CHECK(time_sweeps(prec, reps, false, ms, err));
-            if (ms[0] < best) { best = ms[0]; btpi = t; bdf = sched; }
-        }
-    TY_CHECK(configure(prec, btpi, bdf == 2, err));
-    if (best_tpi) *best_tpi = btpi;
-    if (best_sched) *best_sched = bdf;
+        for (int variant = 0; variant <= 1; ++variant)
+            for (int knob : {1, 2, 4, 8, 16}) {
+                if (variant == 0 && knob > 2 * G_ && knob > 1) continue;  // lanes with no group
+                if (variant == 1 && knob > 4) continue;
+                TY_CHECK(configure(prec, sched, variant, knob, err));
+                double ms[2];
+                TY_CHECK(time_sweeps(prec, 1, false, ms, err));  // warm-up (and graph capture)
+                TY_CHECK(time_sweeps(prec, reps, false, ms, err));
+                if (ms[0] < best) { best = ms[0]; keep = shape_[prec ? 1 : 0]; }
+            }
+    TY_CHECK(configure(prec, keep.schedule, keep.variant, keep.knob, err));
+    if (best_shape) *best_shape = shape_[prec ? 1 : 0];
     if (best_ms) *best_ms = best;
     return kOk;
+}
+
+int Sweeper::launch_dataflow_shape(int prec, const LevelArgs &p, const DataflowArgs &df, cudaStream_t s,
+                                   std::string &err)
+{
+    const LaunchShape &sh = shape_[prec ? 1 : 0];
+    cudaError_t e;
+    if (sh.variant == 0)
+        e = prec ? launch_dataflow<float>(sh.knob, p, df, sh.grid, s)
+                 : launch_dataflow<double>(sh.knob, p, df, sh.grid, s);
+    else
+        e = prec ? launch_dataflow_tile<float>(sh.knob, p, df, sh.grid, s)
+                 : launch_dataflow_tile<double>(sh.knob, p, df, sh.grid, s);
+    TY_CUDA(e);
+    return kOk;
+}
+
+LevelArgs Sweeper::level_args(int prec, const void *iso, const double *qang, void *psi) const
+{
+    LevelArgs p;
+    p.items = d_items_;
+    p.abar = prec ? (const void *)d_abar32_ : (const void *)d_abar64_;
+    p.adj = d_adj_;
+    p.nbrmap = d_nbrmap_;
+    p.cellk = prec ? (const void *)d_cellk32_ : (const void *)d_cellk64_;
+    p.iso = iso;
+    p.qang = qang;
+    p.psi = psi;
+    p.A = (uint32_t)A_;
+    p.G = (uint32_t)G_;
+    p.gmagic = group_magic((uint32_t)G_);
+    return p;
 }
 
 int Sweeper::check_device_error(std::string &err)
@@ -269,18 +314,10 @@ int Sweeper::set_source(int kind, const double *q, std::string &err)
 int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg, cudaEvent_t end,
                     std::string &err)
 {
-    if (prec ? dataflow32_ : dataflow64_) {
-        LevelArgs p;
-        p.items = d_items_;
-        p.abar = prec ? (const void *)d_abar32_ : (const void *)d_abar64_;
-        p.adj = d_adj_;
-        p.nbrmap = d_nbrmap_;
-        p.cellk = prec ? (const void *)d_cellk32_ : (const void *)d_cellk64_;
-        p.iso = has_iso ? (prec ? (const void *)d_iso32_ : (const void *)d_iso_) : nullptr;
-        p.qang = qang;
-        p.psi = d_psi_;
-        p.A = (uint32_t)A_;
-        p.G = (uint32_t)G_;
+    const void *iso = has_iso ? (prec ? (const void *)d_iso32_ : (const void *)d_iso_) : nullptr;
+    const LaunchShape &sh = shape_[prec ? 1 : 0];
+    if (sh.schedule == 2) {
+        const LevelArgs p = level_args(prec, iso, qang, d_psi_);
         DataflowArgs df;
         df.done = d_done_;
         df.err = d_ctl_;
@@ -290,32 +327,25 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         df.spin_limit = 1u << 22;  // ~4 s of polling with backoff
         TY_CUDA(launch_bump_epoch(d_ctl_ + 4, stream_));
         if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
-        TY_CUDA(prec ? launch_dataflow<float>(tpi32_, p, df, grid32_, stream_)
-                     : launch_dataflow<double>(tpi64_, p, df, grid64_, stream_));
+        TY_CHECK(launch_dataflow_shape(prec, p, df, stream_, err));
         if (end) TY_CUDA(cudaEventRecord(end, stream_));
         return kOk;
     }
     auto key = std::make_tuple(prec, has_iso, qang);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
-        LevelArgs p;
-        p.items = d_items_;
-        p.abar = prec ? (const void *)d_abar32_ : (const void *)d_abar64_;
-        p.adj = d_adj_;
-        p.nbrmap = d_nbrmap_;
-        p.cellk = prec ? (const void *)d_cellk32_ : (const void *)d_cellk64_;
-        p.iso = has_iso ? (prec ? (const void *)d_iso32_ : (const void *)d_iso_) : nullptr;
-        p.qang = qang;
-        p.psi = d_psi_;
-        p.A = (uint32_t)A_;
-        p.G = (uint32_t)G_;
+        const LevelArgs p = level_args(prec, iso, qang, d_psi_);
         cudaGraph_t graph;
         TY_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         cudaError_t le = cudaSuccess;
         for (uint32_t l = 0; l < sched_.n_levels && le == cudaSuccess; ++l) {
             const uint64_t b = sched_.level_offset[l], e = sched_.level_offset[l + 1];
-            le = prec ? launch_level<float>(tpi32_, p, b, e, stream_)
-                      : launch_level<double>(tpi64_, p, b, e, stream_);
+            if (sh.variant == 0)
+                le = prec ? launch_level<float>(sh.knob, p, b, e, stream_)
+                          : launch_level<double>(sh.knob, p, b, e, stream_);
+            else
+                le = prec ? launch_level_tile<float>(sh.knob, p, b, e, stream_)
+                          : launch_level_tile<double>(sh.knob, p, b, e, stream_);
         }
         cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
         TY_CUDA(le);

@@ -26,6 +26,15 @@ struct SweeperOptions {
     int schedule = 0;  // 0 auto (dataflow), 1 level-synchronous, 2 dataflow
 };
 
+// Launch shape of one precision's sweep.
+struct LaunchShape {
+    int schedule = 2;   // 1 one launch per wavefront level, 2 persistent dataflow
+    int variant = 1;    // 0 item-parallel (knob = threads per item),
+                        // 1 warp tiles (knob = warps per block)
+    int knob = 4;
+    unsigned grid = 0;  // dataflow: co-resident blocks
+};
+
 struct SolveOptions {
     int method = 0;  // 0 SI, 1 GMRES, 2 mixed
     int iter_max = 100;
@@ -53,10 +62,9 @@ public:
               std::string &err);
     int write_psi(const std::string &path, std::string &err);
     int time_sweeps(int precision, int n, bool flush_l2, double *ms, std::string &err);
-    // Launch shape of one precision: threads per item and schedule.
-    int configure(int prec, int tpi, bool dataflow, std::string &err);
-    int autotune(int prec, int reps, int *best_tpi, int *best_sched, double *best_ms, std::string &err);
-    bool dataflow(int prec) const { return prec ? dataflow32_ : dataflow64_; }
+    int configure(int prec, int schedule, int variant, int knob, std::string &err);
+    int autotune(int prec, int reps, LaunchShape *best, double *best_ms, std::string &err);
+    const LaunchShape &shape(int prec) const { return shape_[prec ? 1 : 0]; }
 
     // One operator application, on the device:
     //   phi_out = D L^{-1} ( [Q] + M S phi_in )     (phi_in / phi_out nullable)
@@ -81,7 +89,6 @@ public:
     uint64_t phi_size() const { return nc_ * 4 * (uint64_t)G_; }
     uint64_t psi_size() const { return nc_ * (uint64_t)A_ * 4 * G_; }
     cudaStream_t stream() const { return stream_; }
-    int tpi(int prec) const { return prec ? tpi32_ : tpi64_; }
     int device() const { return device_; }
 
 private:
@@ -89,6 +96,9 @@ private:
                std::string &err);
     // Reads (and clears) the dataflow schedule's device error word.
     int check_device_error(std::string &err);
+    LevelArgs level_args(int prec, const void *iso, const double *qang, void *psi) const;
+    int launch_dataflow_shape(int prec, const LevelArgs &p, const DataflowArgs &df, cudaStream_t s,
+                              std::string &err);
     int gmres(int prec, const double *b, double *x, int restart, double rtol, int iter_max,
               int &its, double &rnorm, SolveStats &st, std::string &err);
     int ensure_krylov(int restart, std::string &err);
@@ -97,7 +107,7 @@ private:
     Quadrature quad_;
     Schedule sched_;
     uint64_t nc_ = 0;
-    int A_ = 0, G_ = 0, device_ = 0, tpi64_ = 1, tpi32_ = 1;
+    int A_ = 0, G_ = 0, device_ = 0;
     bool fp32_ = false, have_xs_ = false;
     int last_psi_prec_ = -1;
 
@@ -125,8 +135,7 @@ private:
     Reducer red_;
     std::map<std::tuple<int, bool, const double *>, cudaGraphExec_t> graphs_;
     // dataflow schedule
-    bool dataflow64_ = true, dataflow32_ = true;
-    unsigned grid64_ = 0, grid32_ = 0;
+    LaunchShape shape_[2];  // [0] FP64, [1] FP32
     uint32_t *d_done_ = nullptr;   // per item: epoch of completion
     uint32_t *d_ctl_ = nullptr;    // [0..2] error, [3] abort, [4] epoch
 };

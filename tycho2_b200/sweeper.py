@@ -222,15 +222,31 @@ class SweeperCuda:
         check(lib().tycho_sweeper_time_sweeps(self._h, precision, n, int(flush_l2), ptr(ms)))
         return float(ms[0]), float(ms[1])
 
-    def autotune(self, precision, reps=3):
-        """Picks the fastest (schedule, threads-per-item) for one precision."""
-        t, s, ms = C.c_int(), C.c_int(), C.c_double()
-        check(lib().tycho_sweeper_autotune(self._h, precision, reps, C.byref(t), C.byref(s),
-                                           C.byref(ms)))
-        return {"tpi": t.value, "schedule": {1: "levels", 2: "dataflow"}[s.value], "ms": ms.value}
+    VARIANTS = {"items": 0, "tiles": 1}
 
-    def configure(self, precision, schedule, tpi):
-        check(lib().tycho_sweeper_configure(self._h, precision, self.SCHEDULES[schedule], tpi))
+    @staticmethod
+    def _shape_dict(sh):
+        return {"schedule": {1: "levels", 2: "dataflow"}[sh.schedule],
+                "variant": {0: "items", 1: "tiles"}[sh.variant], "knob": sh.knob}
+
+    def autotune(self, precision, reps=3):
+        """Picks the fastest launch shape (schedule, variant, knob) for one precision."""
+        sh, ms = _capi.LaunchShape(), C.c_double()
+        check(lib().tycho_sweeper_autotune(self._h, precision, reps, C.byref(sh), C.byref(ms)))
+        d = self._shape_dict(sh)
+        d["ms"] = ms.value
+        return d
+
+    def configure(self, precision, schedule, variant, knob):
+        """schedule 'levels'|'dataflow'; variant 'items' (knob = lanes per item)
+        or 'tiles' (knob = warps per block)."""
+        sh = _capi.LaunchShape(self.SCHEDULES[schedule], self.VARIANTS[variant], knob)
+        check(lib().tycho_sweeper_configure(self._h, precision, C.byref(sh)))
+
+    def shape(self, precision):
+        sh = _capi.LaunchShape()
+        check(lib().tycho_sweeper_get_shape(self._h, precision, C.byref(sh)))
+        return self._shape_dict(sh)
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value and _capi._lib is not None:
