@@ -201,7 +201,10 @@ int tycho_sweeper_levels(const tycho_sweeper *sw, uint32_t *tlevel, uint32_t *de
      variant  0 = item-parallel: knob lanes per (cell, angle) item, each lane
                   a strided subset of the groups (group tiling; 1..16),
               1 = warp tiles: 32 items per warp, factors in shared memory,
-                  knob warps per block (1, 2, 4). */
+                  knob warps per block (1, 2, 4),
+              2 = records: the per-item factors precomputed once per
+                  cross-section set (128 B per item in FP32, 256 B in FP64),
+                  pairs loaded several at a time; knob warps per block (1, 2, 4). */
 typedef struct tycho_launch_shape {
     int schedule;
     int variant;

@@ -23,7 +23,8 @@ def test_fp64_sweep_bit_exact_vs_reference_fixture(built, kuhn3_ref):
     r = kuhn3_ref
     mesh = ty.TychoMesh.kuhn_cube(3, 0.05, 2024, 100.0)
     for shape in (("levels", "items", 1), ("levels", "items", 2), ("dataflow", "items", 4),
-                  ("levels", "tiles", 4), ("dataflow", "tiles", 1), ("dataflow", "tiles", 2)):
+                  ("levels", "tiles", 4), ("dataflow", "tiles", 1), ("dataflow", "tiles", 2),
+                  ("levels", "records", 4), ("dataflow", "records", 1), ("dataflow", "records", 4)):
         sw = make(mesh, 4, 3)
         sw.configure(0, *shape)
         sw.set_cross_sections(r["sweep_sigma_t"], np.zeros(mesh.n_cells))
@@ -33,7 +34,7 @@ def test_fp64_sweep_bit_exact_vs_reference_fixture(built, kuhn3_ref):
 
 
 @pytest.mark.parametrize("schedule", ["levels", "dataflow"])
-@pytest.mark.parametrize("variant", ["items", "tiles"])
+@pytest.mark.parametrize("variant", ["items", "tiles", "records"])
 @pytest.mark.parametrize("n,jitter,sn,G,tpi", [
     (4, 0.05, 4, 1, 1), (5, 0.05, 8, 2, 2), (3, 0.0, 2, 3, 1), (6, 0.05, 6, 4, 4),
     (4, 0.07, 8, 8, 8), (2, 0.05, 4, 16, 16), (7, 0.05, 4, 5, 2), (1, 0.0, 4, 1, 1),
@@ -164,7 +165,8 @@ def test_fp32_sweep_within_tolerance(built, workdir):
     q = rng.uniform(0.0, 1.0, o.phi_shape)
     psi_ref, phi_ref, _, _ = o.krylov(st, st, mat, q_iso=q, restart=20, iter_max=200, rtol=1e-11)
     for shape in (("levels", "items", 1), ("levels", "items", 8), ("dataflow", "items", 4),
-                  ("levels", "tiles", 2), ("dataflow", "tiles", 4)):
+                  ("levels", "tiles", 2), ("dataflow", "tiles", 4), ("levels", "records", 2),
+                  ("dataflow", "records", 4)):
         sw = make(mesh, 8, G, fp32=True)
         sw.configure(1, *shape)
         sw.set_cross_sections(st, st, mat)

@@ -5,6 +5,7 @@
 #include "device_ops.hpp"
 #include "sweep_kernels.cuh"
 #include "sweep_tiles.cuh"
+#include "sweep_records.cuh"
 
 namespace tycho {
 
@@ -14,6 +15,11 @@ template cudaError_t dataflow_blocks_per_sm<double>(int, int *);
 template cudaError_t launch_level_tile<double>(int, const LevelArgs &, uint64_t, uint64_t, cudaStream_t);
 template cudaError_t launch_dataflow_tile<double>(int, const LevelArgs &, const DataflowArgs &, unsigned, cudaStream_t);
 template cudaError_t tile_dataflow_blocks_per_sm<double>(int, int *);
+template cudaError_t launch_item_records<double>(const LevelArgs &, uint64_t, void *, cudaStream_t);
+template cudaError_t launch_level_record<double>(int, const LevelArgs &, const void *, uint64_t, uint64_t, cudaStream_t);
+template cudaError_t launch_dataflow_record<double>(int, const LevelArgs &, const void *, const DataflowArgs &, unsigned,
+                                               cudaStream_t);
+template cudaError_t record_dataflow_blocks_per_sm<double>(int, int *);
 
 namespace {
 

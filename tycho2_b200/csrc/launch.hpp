@@ -55,4 +55,18 @@ cudaError_t launch_dataflow_tile(int wpb, const LevelArgs &p, const DataflowArgs
 template <typename Real>
 cudaError_t tile_dataflow_blocks_per_sm(int wpb, int *blocks);
 
+// Record variant (sweep_records.cuh): per-item factors precomputed once per
+// cross-section set into `rec` (128 B per item for float, 256 B for double).
+constexpr size_t record_bytes(bool fp32) { return fp32 ? 128 : 256; }
+template <typename Real>
+cudaError_t launch_item_records(const LevelArgs &p, uint64_t n, void *rec, cudaStream_t s);
+template <typename Real>
+cudaError_t launch_level_record(int wpb, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
+                                cudaStream_t s);
+template <typename Real>
+cudaError_t launch_dataflow_record(int wpb, const LevelArgs &p, const void *rec, const DataflowArgs &df,
+                                   unsigned grid, cudaStream_t s);
+template <typename Real>
+cudaError_t record_dataflow_blocks_per_sm(int wpb, int *blocks);
+
 }  // namespace tycho

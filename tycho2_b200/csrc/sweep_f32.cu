@@ -3,6 +3,7 @@
 // sweep by tolerance, not bit for bit.
 #include "sweep_kernels.cuh"
 #include "sweep_tiles.cuh"
+#include "sweep_records.cuh"
 
 namespace tycho {
 
@@ -12,5 +13,10 @@ template cudaError_t dataflow_blocks_per_sm<float>(int, int *);
 template cudaError_t launch_level_tile<float>(int, const LevelArgs &, uint64_t, uint64_t, cudaStream_t);
 template cudaError_t launch_dataflow_tile<float>(int, const LevelArgs &, const DataflowArgs &, unsigned, cudaStream_t);
 template cudaError_t tile_dataflow_blocks_per_sm<float>(int, int *);
+template cudaError_t launch_item_records<float>(const LevelArgs &, uint64_t, void *, cudaStream_t);
+template cudaError_t launch_level_record<float>(int, const LevelArgs &, const void *, uint64_t, uint64_t, cudaStream_t);
+template cudaError_t launch_dataflow_record<float>(int, const LevelArgs &, const void *, const DataflowArgs &, unsigned,
+                                               cudaStream_t);
+template cudaError_t record_dataflow_blocks_per_sm<float>(int, int *);
 
 }  // namespace tycho

@@ -56,7 +56,7 @@ Sweeper::~Sweeper()
     for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
     void *bufs[] = {d_items_, d_abar64_, d_abar32_, d_adj_, d_nbrmap_, d_cellk64_, d_cellk32_,
                     d_w_, d_sigs_, d_scat_, d_qiso_, d_qang_, d_src_, d_iso_, d_iso32_, d_psi_,
-                    d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_, d_done_, d_ctl_};
+                    d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_, d_done_, d_ctl_, d_rec_[0], d_rec_[1]};
     for (void *b : bufs)
         if (b) cudaFree(b);
     reducer_free(red_);
@@ -165,14 +165,25 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
         err = "warp-tile variant: warps per block must be 1, 2 or 4";
         return kErrArg;
     }
-    if (variant != 0 && variant != 1) { err = "variant must be 0 (item-parallel) or 1 (warp tiles)"; return kErrArg; }
+    if (variant == 2 && knob != 1 && knob != 2 && knob != 4) {
+        err = "record variant: warps per block must be 1, 2 or 4";
+        return kErrArg;
+    }
+    if (variant < 0 || variant > 2) {
+        err = "variant must be 0 (item-parallel), 1 (warp tiles) or 2 (precomputed records)";
+        return kErrArg;
+    }
+    if (variant == 2) TY_CHECK(ensure_records(prec, false, err));
     int sms = 0, per_sm = 0;
     TY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
     if (variant == 0)
         TY_CUDA(prec ? dataflow_blocks_per_sm<float>(knob, &per_sm) : dataflow_blocks_per_sm<double>(knob, &per_sm));
-    else
+    else if (variant == 1)
         TY_CUDA(prec ? tile_dataflow_blocks_per_sm<float>(knob, &per_sm)
                      : tile_dataflow_blocks_per_sm<double>(knob, &per_sm));
+    else
+        TY_CUDA(prec ? record_dataflow_blocks_per_sm<float>(knob, &per_sm)
+                     : record_dataflow_blocks_per_sm<double>(knob, &per_sm));
     if (per_sm < 1) { err = "dataflow kernel does not fit on an SM"; return kErrCuda; }
     LaunchShape &sh = shape_[prec ? 1 : 0];
     sh.schedule = schedule;
@@ -200,11 +211,13 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
     double best = 1e300;
     LaunchShape keep = shape_[prec ? 1 : 0];
     for (int sched = 1; sched <= 2; ++sched)
-        for (int variant = 0; variant <= 1; ++variant)
+        for (int variant = 0; variant <= 2; ++variant)
             for (int knob : {1, 2, 4, 8, 16}) {
                 if (variant == 0 && knob > 2 * G_ && knob > 1) continue;  // lanes with no group
-                if (variant == 1 && knob > 4) continue;
-                TY_CHECK(configure(prec, sched, variant, knob, err));
+                if (variant >= 1 && knob > 4) continue;
+                const int cs = configure(prec, sched, variant, knob, err);
+                if (cs == kErrOom) continue;  // records do not fit next to psi
+                TY_CHECK(cs);
                 double ms[2];
                 TY_CHECK(time_sweeps(prec, 1, false, ms, err));  // warm-up (and graph capture)
                 TY_CHECK(time_sweeps(prec, reps, false, ms, err));
@@ -224,9 +237,14 @@ int Sweeper::launch_dataflow_shape(int prec, const LevelArgs &p, const DataflowA
     if (sh.variant == 0)
         e = prec ? launch_dataflow<float>(sh.knob, p, df, sh.grid, s)
                  : launch_dataflow<double>(sh.knob, p, df, sh.grid, s);
-    else
+    else if (sh.variant == 1)
         e = prec ? launch_dataflow_tile<float>(sh.knob, p, df, sh.grid, s)
                  : launch_dataflow_tile<double>(sh.knob, p, df, sh.grid, s);
+    else {
+        TY_CHECK(ensure_records(prec, true, err));
+        e = prec ? launch_dataflow_record<float>(sh.knob, p, d_rec_[1], df, sh.grid, s)
+                 : launch_dataflow_record<double>(sh.knob, p, d_rec_[0], df, sh.grid, s);
+    }
     TY_CUDA(e);
     return kOk;
 }
@@ -246,6 +264,32 @@ LevelArgs Sweeper::level_args(int prec, const void *iso, const double *qang, voi
     p.G = (uint32_t)G_;
     p.gmagic = group_magic((uint32_t)G_);
     return p;
+}
+
+// Allocates (once) and fills (once per cross-section set) the per-item
+// records of the record variant for one precision.
+int Sweeper::ensure_records(int prec, bool need_filled, std::string &err)
+{
+    const int k = prec ? 1 : 0;
+    if (!d_rec_[k]) {
+        const size_t bytes = record_bytes(prec == 1) * sched_.items.size();
+        cudaError_t e = cudaMalloc(&d_rec_[k], bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            d_rec_[k] = nullptr;
+            err = "records (" + std::to_string(bytes >> 20) + " MiB) do not fit: " + cudaGetErrorString(e);
+            return e == cudaErrorMemoryAllocation ? kErrOom : kErrCuda;
+        }
+        rec_valid_[k] = false;
+    }
+    if (!rec_valid_[k] && have_xs_) {
+        const LevelArgs p = level_args(prec, nullptr, nullptr, d_psi_);
+        TY_CUDA(prec ? launch_item_records<float>(p, sched_.items.size(), d_rec_[k], stream_)
+                     : launch_item_records<double>(p, sched_.items.size(), d_rec_[k], stream_));
+        rec_valid_[k] = true;
+    }
+    if (need_filled && !rec_valid_[k]) { err = "cross sections not set"; return kErrMissing; }
+    return kOk;
 }
 
 int Sweeper::check_device_error(std::string &err)
@@ -291,6 +335,9 @@ int Sweeper::set_cross_sections(const double *sigma_t, const double *sigma_s, co
     }
     TY_CUDA(cudaStreamSynchronize(stream_));
     have_xs_ = true;
+    rec_valid_[0] = rec_valid_[1] = false;
+    for (int k = 0; k < 2; ++k)
+        if (shape_[k].variant == 2 && (k == 0 || fp32_)) TY_CHECK(ensure_records(k, true, err));
     return kOk;
 }
 
@@ -331,6 +378,7 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         if (end) TY_CUDA(cudaEventRecord(end, stream_));
         return kOk;
     }
+    if (sh.variant == 2) TY_CHECK(ensure_records(prec, true, err));
     auto key = std::make_tuple(prec, has_iso, qang);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
@@ -343,9 +391,12 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
             if (sh.variant == 0)
                 le = prec ? launch_level<float>(sh.knob, p, b, e, stream_)
                           : launch_level<double>(sh.knob, p, b, e, stream_);
-            else
+            else if (sh.variant == 1)
                 le = prec ? launch_level_tile<float>(sh.knob, p, b, e, stream_)
                           : launch_level_tile<double>(sh.knob, p, b, e, stream_);
+            else
+                le = prec ? launch_level_record<float>(sh.knob, p, d_rec_[1], b, e, stream_)
+                          : launch_level_record<double>(sh.knob, p, d_rec_[0], b, e, stream_);
         }
         cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
         TY_CUDA(le);

@@ -30,7 +30,8 @@ struct SweeperOptions {
 struct LaunchShape {
     int schedule = 2;   // 1 one launch per wavefront level, 2 persistent dataflow
     int variant = 1;    // 0 item-parallel (knob = threads per item),
-                        // 1 warp tiles (knob = warps per block)
+                        // 1 warp tiles (knob = warps per block),
+                        // 2 precomputed per-item records (knob = warps per block)
     int knob = 4;
     unsigned grid = 0;  // dataflow: co-resident blocks
 };
@@ -102,6 +103,9 @@ private:
     int gmres(int prec, const double *b, double *x, int restart, double rtol, int iter_max,
               int &its, double &rnorm, SolveStats &st, std::string &err);
     int ensure_krylov(int restart, std::string &err);
+    // Allocates the record array of one precision; need_filled also requires
+    // (and computes, when stale) its contents for the current cross sections.
+    int ensure_records(int prec, bool need_filled, std::string &err);
 
     MeshTables tables_;
     Quadrature quad_;
@@ -138,6 +142,9 @@ private:
     LaunchShape shape_[2];  // [0] FP64, [1] FP32
     uint32_t *d_done_ = nullptr;   // per item: epoch of completion
     uint32_t *d_ctl_ = nullptr;    // [0..2] error, [3] abort, [4] epoch
+    // record variant: per-item factors, [0] FP64, [1] FP32
+    void *d_rec_[2] = {nullptr, nullptr};
+    bool rec_valid_[2] = {false, false};
 };
 
 // The no-alloc sweep (tycho_sweeper_sweep_noalloc, sweep_noalloc.cu): scratch

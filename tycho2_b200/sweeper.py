@@ -222,12 +222,12 @@ class SweeperCuda:
         check(lib().tycho_sweeper_time_sweeps(self._h, precision, n, int(flush_l2), ptr(ms)))
         return float(ms[0]), float(ms[1])
 
-    VARIANTS = {"items": 0, "tiles": 1}
+    VARIANTS = {"items": 0, "tiles": 1, "records": 2}
 
     @staticmethod
     def _shape_dict(sh):
         return {"schedule": {1: "levels", 2: "dataflow"}[sh.schedule],
-                "variant": {0: "items", 1: "tiles"}[sh.variant], "knob": sh.knob}
+                "variant": {0: "items", 1: "tiles", 2: "records"}[sh.variant], "knob": sh.knob}
 
     def autotune(self, precision, reps=3):
         """Picks the fastest launch shape (schedule, variant, knob) for one precision."""
@@ -238,8 +238,8 @@ class SweeperCuda:
         return d
 
     def configure(self, precision, schedule, variant, knob):
-        """schedule 'levels'|'dataflow'; variant 'items' (knob = lanes per item)
-        or 'tiles' (knob = warps per block)."""
+        """schedule 'levels'|'dataflow'; variant 'items' (knob = lanes per item),
+        'tiles' or 'records' (knob = warps per block)."""
         sh = _capi.LaunchShape(self.SCHEDULES[schedule], self.VARIANTS[variant], knob)
         check(lib().tycho_sweeper_configure(self._h, precision, C.byref(sh)))
 
