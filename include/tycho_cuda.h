@@ -204,7 +204,7 @@ int tycho_sweeper_levels(const tycho_sweeper *sw, uint32_t *tlevel, uint32_t *de
                   knob warps per block (1, 2, 4),
               2 = records: the per-item factors precomputed once per
                   cross-section set (128 B per item in FP32, 256 B in FP64),
-                  pairs loaded several at a time; knob warps per block (1, 2, 4). */
+                  pairs loaded several at a time; knob items per warp (8, 16, 32). */
 typedef struct tycho_launch_shape {
     int schedule;
     int variant;

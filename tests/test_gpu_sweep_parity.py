@@ -24,7 +24,7 @@ def test_fp64_sweep_bit_exact_vs_reference_fixture(built, kuhn3_ref):
     mesh = ty.TychoMesh.kuhn_cube(3, 0.05, 2024, 100.0)
     for shape in (("levels", "items", 1), ("levels", "items", 2), ("dataflow", "items", 4),
                   ("levels", "tiles", 4), ("dataflow", "tiles", 1), ("dataflow", "tiles", 2),
-                  ("levels", "records", 4), ("dataflow", "records", 1), ("dataflow", "records", 4)):
+                  ("levels", "records", 8), ("dataflow", "records", 16), ("dataflow", "records", 32)):
         sw = make(mesh, 4, 3)
         sw.configure(0, *shape)
         sw.set_cross_sections(r["sweep_sigma_t"], np.zeros(mesh.n_cells))
@@ -47,7 +47,8 @@ def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi, v
     st = rng.lognormal(0.0, 0.5, mesh.n_cells)
     src = rng.uniform(-0.2, 1.0, o.psi_shape)
     sw = make(mesh, sn, G)
-    sw.configure(0, schedule, variant, tpi if variant == "items" else min(tpi, 4))
+    knob = {"items": tpi, "tiles": min(tpi, 4), "records": 8 if tpi <= 2 else (16 if tpi <= 4 else 32)}
+    sw.configure(0, schedule, variant, knob[variant])
     sw.set_cross_sections(st, np.zeros(mesh.n_cells))
     psi = np.empty(sw.psi_shape)
     sw.sweep(psi, src)
@@ -165,8 +166,8 @@ def test_fp32_sweep_within_tolerance(built, workdir):
     q = rng.uniform(0.0, 1.0, o.phi_shape)
     psi_ref, phi_ref, _, _ = o.krylov(st, st, mat, q_iso=q, restart=20, iter_max=200, rtol=1e-11)
     for shape in (("levels", "items", 1), ("levels", "items", 8), ("dataflow", "items", 4),
-                  ("levels", "tiles", 2), ("dataflow", "tiles", 4), ("levels", "records", 2),
-                  ("dataflow", "records", 4)):
+                  ("levels", "tiles", 2), ("dataflow", "tiles", 4), ("levels", "records", 16),
+                  ("dataflow", "records", 32)):
         sw = make(mesh, 8, G, fp32=True)
         sw.configure(1, *shape)
         sw.set_cross_sections(st, st, mat)

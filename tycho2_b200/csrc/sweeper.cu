@@ -165,8 +165,8 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
         err = "warp-tile variant: warps per block must be 1, 2 or 4";
         return kErrArg;
     }
-    if (variant == 2 && knob != 1 && knob != 2 && knob != 4) {
-        err = "record variant: warps per block must be 1, 2 or 4";
+    if (variant == 2 && knob != 8 && knob != 16 && knob != 32) {
+        err = "record variant: items per warp must be 8, 16 or 32";
         return kErrArg;
     }
     if (variant < 0 || variant > 2) {
@@ -212,9 +212,10 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
     LaunchShape keep = shape_[prec ? 1 : 0];
     for (int sched = 1; sched <= 2; ++sched)
         for (int variant = 0; variant <= 2; ++variant)
-            for (int knob : {1, 2, 4, 8, 16}) {
-                if (variant == 0 && knob > 2 * G_ && knob > 1) continue;  // lanes with no group
-                if (variant >= 1 && knob > 4) continue;
+            for (int knob : {1, 2, 4, 8, 16, 32}) {
+                if (variant == 0 && ((knob > 2 * G_ && knob > 1) || knob > 16)) continue;  // idle lanes
+                if (variant == 1 && knob > 4) continue;
+                if (variant == 2 && knob < 8) continue;
                 const int cs = configure(prec, sched, variant, knob, err);
                 if (cs == kErrOom) continue;  // records do not fit next to psi
                 TY_CHECK(cs);

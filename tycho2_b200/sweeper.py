@@ -239,7 +239,7 @@ class SweeperCuda:
 
     def configure(self, precision, schedule, variant, knob):
         """schedule 'levels'|'dataflow'; variant 'items' (knob = lanes per item),
-        'tiles' or 'records' (knob = warps per block)."""
+        'tiles' (knob = warps per block) or 'records' (knob = items per warp)."""
         sh = _capi.LaunchShape(self.SCHEDULES[schedule], self.VARIANTS[variant], knob)
         check(lib().tycho_sweeper_configure(self._h, precision, C.byref(sh)))
 
