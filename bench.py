@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--no-solve", action="store_true", help="skip the solve-error check")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--shape", default="auto",
+                   help="launch shape 'schedule,variant,knob' for both precisions, or auto (autotuner)")
     return p.parse_args()
 
 
@@ -181,18 +183,51 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+KERNELS = {
+    (1, "items"): "sweep_level_kernel<{r},{k}>", (1, "tiles"): "sweep_tile_level_kernel<{r},{k}>",
+    (1, "records"): "sweep_record_level_kernel<{r},{k},{vg}>",
+    (2, "items"): "sweep_dataflow_kernel<{r},{k}>", (2, "tiles"): "sweep_tile_dataflow_kernel<{r},{k}>",
+    (2, "records"): "sweep_record_dataflow_kernel<{r},{k},{vg}>",
+    (3, "records"): "sweep_record_persist_kernel<{r},{k},{vg}>",
+}
+SCHED = {"levels": 1, "dataflow": 2, "persist": 3}
+
+
+def kernel_name(shape, fp32, G):
+    vg = (4 if G % 4 == 0 else 2 if G % 2 == 0 else 1) if fp32 else (2 if G % 2 == 0 else 1)
+    return KERNELS[(SCHED[shape["schedule"]], shape["variant"])].format(
+        r="float" if fp32 else "double", k=shape["knob"], vg=vg)
+
+
+def launches_per_sweep(shape, n_levels):
+    """Kernels of one operator application: scatter-source, the sweep, psi->phi."""
+    sweep = {"levels": n_levels, "dataflow": 2, "persist": 1}[shape["schedule"]]
+    return sweep + 2
+
+
+def profiled_traffic(workload, kernel):
+    """DRAM bytes of one sweep (dram__bytes_read.sum + dram__bytes_write.sum over
+    the sweep's launches) from the ncu summary table in profiles/, if that
+    kernel was captured on this workload; else None."""
+    path = os.path.join(ROOT, "profiles", "sweep_traffic.md")
+    try:
+        with open(path) as f:
+            for ln in f:
+                cells = [c.strip() for c in ln.strip().strip("|").split("|")]
+                if len(cells) >= 3 and cells[0] == workload and cells[1] == "`%s`" % kernel:
+                    return float(cells[2])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def run_b200(args):
     import torch
-    import torch.distributed as dist
     import tycho2_b200 as ty
+    from tycho2_b200.replicas import ReplicaGroup
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
-    dev = local if world > 1 else 0
+    grp = ReplicaGroup()
+    world, rank, dev = grp.world, grp.rank, grp.device
 
     w, mesh, st, ss, mat, q = build_problem(args.workload)
     nc, A, G = mesh.n_cells, 2 * w["sn"] ** 2, w["groups"]
@@ -202,43 +237,45 @@ def run_b200(args):
     sw.set_source(q, "isotropic")
     info = sw.schedule_info()
 
+    # Launch shapes: the autotuner's pick per precision (or a fixed shape).
+    if args.shape == "auto":
+        tuned = {1: sw.autotune(1, 3), 0: sw.autotune(0, 3)}
+    else:
+        s, v, k = args.shape.split(",")
+        for prec in (1, 0):
+            sw.configure(prec, s, v, int(k))
+        tuned = {1: sw.shape(1), 0: sw.shape(0)}
+    shape32, shape64 = sw.shape(1), sw.shape(0)
+
     # Untimed warm-up (graph capture of both precisions), then K timed steps
     # of each precision.  psi (6.4 GB FP64 / 3.2 GB FP32) is far larger than
     # L2; a 256 MB buffer is also written between steps.
-    sw.time_sweeps(1, max(args.warmup, 3))
-    sw.time_sweeps(0, max(args.warmup, 3))
-
-    def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
+    warm = max(args.warmup, 3)
+    sw.time_sweeps(1, warm)
+    sw.time_sweeps(0, warm)
 
     with Clocks(dev) as clk:
-        barrier()
+        grp.barrier()
+        torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
         t0 = time.perf_counter()
         ms32, lvl32 = sw.time_sweeps(1, args.steps, True)
-        barrier()
+        grp.barrier()
         wall32 = time.perf_counter() - t0
         ms64, lvl64 = sw.time_sweeps(0, args.steps, True)
-        barrier()
+        grp.barrier()
+        torch.cuda.profiler.stop()
     clocks = clk.summary()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    ms32, lvl32, ms64, lvl64 = (max_over_ranks(x) for x in (ms32, lvl32, ms64, lvl64))
-    value = world * updates / (ms32 * 1e-3)
-    fp64_value = world * updates / (ms64 * 1e-3)
+    ms32, lvl32, ms64, lvl64 = (grp.max(x) for x in (ms32, lvl32, ms64, lvl64))
+    value = grp.sum(updates) / (ms32 * 1e-3)
+    fp64_value = grp.sum(updates) / (ms64 * 1e-3)
 
     peak, peak_kind = hbm_peak()
     b32 = algorithmic_bytes(nc, A, G, info["n_incoming_interior"], 4)
     b64 = algorithmic_bytes(nc, A, G, info["n_incoming_interior"], 8)
     ach32 = b32 / (lvl32 * 1e-3) / 1e9
     ach64 = b64 / (lvl64 * 1e-3) / 1e9
+    k32, k64 = kernel_name(shape32, True, G), kernel_name(shape64, False, G)
 
     # Solve-level check: mixed precision vs FP64 GMRES on the same problem.
     solve = None
@@ -266,13 +303,13 @@ def run_b200(args):
         psi = psi_t.numpy().reshape(sw.psi_shape)
         sw.sweep(psi, src)
         n_e2e = max(1, min(args.steps, 3))
-        barrier()
+        grp.barrier()
         t0 = time.perf_counter()
         for _ in range(n_e2e):
             sw.sweep(psi, src)
-        barrier()
-        dt = max_over_ranks((time.perf_counter() - t0) / n_e2e)
-        e2e = {"value": world * updates / dt, "unit": "updates/s", "h2d_bytes_per_step": npsi * 8,
+        grp.barrier()
+        dt = grp.max((time.perf_counter() - t0) / n_e2e)
+        e2e = {"value": grp.sum(updates) / dt, "unit": "updates/s", "h2d_bytes_per_step": npsi * 8,
                "d2h_bytes_per_step": npsi * 8, "path": "tycho_sweeper_sweep (FP64, host buffers)",
                "seconds_per_step": dt}
         del src_t, psi_t
@@ -285,33 +322,39 @@ def run_b200(args):
             cpu = {"value": None, "error": str(e)[:200]}
 
     if rank == 0:
+        t32 = profiled_traffic(args.workload, k32)
+        t64 = profiled_traffic(args.workload, k64)
         line = {
             "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms32,
+            "steps": args.steps, "warmup": warm, "ms_per_step": ms32,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload, "cells": nc, "angles": A, "groups": G,
                        "levels": info["n_levels"], "parallelism": "replicas" if world > 1 else "1 gpu",
-                       "l2": "psi > L2 and a 256 MB flush between steps"},
+                       "l2": "psi > L2 and a 256 MB flush between steps",
+                       "shape_fp32": shape32, "shape_fp64": shape64,
+                       "autotune_ms": ({"fp32": tuned[1]["ms"], "fp64": tuned[0]["ms"]}
+                                       if args.shape == "auto" else None)},
             "fp64": {"value": fp64_value, "ms_per_step": ms64, "dtype": "f64"},
             "mixed_vs_fp64_sweep_speedup": value / fp64_value,
             "solve": solve,
             "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
-                         "frac": ach32 / peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "sweep_level_kernel<float>", "bytes_per_sweep": b32,
-                         "kernel_ms_per_sweep": lvl32,
-                         "fp64": {"achieved": ach64, "frac": ach64 / peak, "bytes_per_sweep": b64,
-                                  "kernel_ms_per_sweep": lvl64}},
+                         "frac": ach32 / peak, "traffic": t32, "peak_kind": peak_kind,
+                         "kernel": k32, "bytes_per_sweep": b32, "kernel_ms_per_sweep": lvl32,
+                         "per": "one sweep (all of its launches)",
+                         "fp64": {"kernel": k64, "achieved": ach64, "frac": ach64 / peak,
+                                  "bytes_per_sweep": b64, "kernel_ms_per_sweep": lvl64,
+                                  "traffic": t64}},
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": args.steps * 2 * (info["n_levels"] + 2),
+            "gpu_launches": args.steps * (launches_per_sweep(shape32, info["n_levels"])
+                                          + launches_per_sweep(shape64, info["n_levels"])),
             "clocks": clocks,
             "wall_check_s": wall32,
         }
         print(json.dumps(line), flush=True)
     sw.close()
-    if world > 1:
-        dist.destroy_process_group()
+    grp.close()
 
 
 def main():

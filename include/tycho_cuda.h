@@ -197,18 +197,25 @@ int tycho_sweeper_levels(const tycho_sweeper *sw, uint32_t *tlevel, uint32_t *de
                          uint32_t *blevel);
 
 /* Launch shape of one precision's sweep:
-     schedule 1 = one launch per wavefront level, 2 = persistent dataflow;
+     schedule 1 = one launch per wavefront level, 2 = persistent dataflow,
+              3 = persistent levels: one cooperative launch walking the
+                  levels with a bounded grid barrier between them (variant 2
+                  only; FP64 knob 8 or 16);
      variant  0 = item-parallel: knob lanes per (cell, angle) item, each lane
                   a strided subset of the groups (group tiling; 1..16),
               1 = warp tiles: 32 items per warp, factors in shared memory,
                   knob warps per block (1, 2, 4),
               2 = records: the per-item factors precomputed once per
                   cross-section set (128 B per item in FP32, 256 B in FP64),
-                  pairs loaded several at a time; knob items per warp (8, 16, 32). */
+                  pairs loaded several at a time; knob items per warp (8, 16, 32);
+     vector   records only: groups per vector access of a psi row (1, 2, or
+              4 in FP32; must divide nGroups); 0 = the widest that divides
+              nGroups (4 or 2 in FP32, 2 in FP64). */
 typedef struct tycho_launch_shape {
     int schedule;
     int variant;
     int knob;
+    int vector;
 } tycho_launch_shape;
 
 /* Autotuner: times every launch shape of the given precision's sweep with

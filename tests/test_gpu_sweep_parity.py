@@ -24,7 +24,8 @@ def test_fp64_sweep_bit_exact_vs_reference_fixture(built, kuhn3_ref):
     mesh = ty.TychoMesh.kuhn_cube(3, 0.05, 2024, 100.0)
     for shape in (("levels", "items", 1), ("levels", "items", 2), ("dataflow", "items", 4),
                   ("levels", "tiles", 4), ("dataflow", "tiles", 1), ("dataflow", "tiles", 2),
-                  ("levels", "records", 8), ("dataflow", "records", 16), ("dataflow", "records", 32)):
+                  ("levels", "records", 8), ("dataflow", "records", 16), ("dataflow", "records", 32),
+                  ("persist", "records", 8), ("persist", "records", 16)):
         sw = make(mesh, 4, 3)
         sw.configure(0, *shape)
         sw.set_cross_sections(r["sweep_sigma_t"], np.zeros(mesh.n_cells))
@@ -33,13 +34,15 @@ def test_fp64_sweep_bit_exact_vs_reference_fixture(built, kuhn3_ref):
         assert bits_equal(psi, r["sweep_psi"]), shape
 
 
-@pytest.mark.parametrize("schedule", ["levels", "dataflow"])
-@pytest.mark.parametrize("variant", ["items", "tiles", "records"])
+@pytest.mark.parametrize("schedule,variant,vector", [
+    ("levels", "items", 0), ("levels", "tiles", 0), ("levels", "records", 0), ("levels", "records", 1),
+    ("dataflow", "items", 0), ("dataflow", "tiles", 0), ("dataflow", "records", 0),
+    ("persist", "records", 0), ("persist", "records", 1)])
 @pytest.mark.parametrize("n,jitter,sn,G,tpi", [
     (4, 0.05, 4, 1, 1), (5, 0.05, 8, 2, 2), (3, 0.0, 2, 3, 1), (6, 0.05, 6, 4, 4),
     (4, 0.07, 8, 8, 8), (2, 0.05, 4, 16, 16), (7, 0.05, 4, 5, 2), (1, 0.0, 4, 1, 1),
     (3, 0.05, 4, 64, 4), (2, 0.05, 4, 33, 1)])
-def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi, variant, schedule):
+def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi, variant, schedule, vector):
     from oracle.oracle import Oracle
     mesh, om = kuhn(workdir, n, jitter, seed=5)
     o = Oracle(om, sn, G)
@@ -48,7 +51,9 @@ def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi, v
     src = rng.uniform(-0.2, 1.0, o.psi_shape)
     sw = make(mesh, sn, G)
     knob = {"items": tpi, "tiles": min(tpi, 4), "records": 8 if tpi <= 2 else (16 if tpi <= 4 else 32)}
-    sw.configure(0, schedule, variant, knob[variant])
+    if schedule == "persist":
+        knob["records"] = min(knob["records"], 16)  # two 32-item FP64 tiles exceed shared memory
+    sw.configure(0, schedule, variant, knob[variant], vector)
     sw.set_cross_sections(st, np.zeros(mesh.n_cells))
     psi = np.empty(sw.psi_shape)
     sw.sweep(psi, src)
@@ -167,7 +172,8 @@ def test_fp32_sweep_within_tolerance(built, workdir):
     psi_ref, phi_ref, _, _ = o.krylov(st, st, mat, q_iso=q, restart=20, iter_max=200, rtol=1e-11)
     for shape in (("levels", "items", 1), ("levels", "items", 8), ("dataflow", "items", 4),
                   ("levels", "tiles", 2), ("dataflow", "tiles", 4), ("levels", "records", 16),
-                  ("dataflow", "records", 32)):
+                  ("dataflow", "records", 32), ("persist", "records", 8), ("persist", "records", 32),
+                  ("levels", "records", 16, 1), ("levels", "records", 16, 2)):
         sw = make(mesh, 8, G, fp32=True)
         sw.configure(1, *shape)
         sw.set_cross_sections(st, st, mat)
@@ -255,8 +261,8 @@ def test_autotune_keeps_results_bit_exact(built, workdir):
     sw.set_cross_sections(st, np.zeros(mesh.n_cells))
     best64 = sw.autotune(0, reps=2)
     best32 = sw.autotune(1, reps=2)
-    assert best64["variant"] in ("items", "tiles") and best32["schedule"] in ("levels", "dataflow")
-    assert sw.shape(0) == {k: best64[k] for k in ("schedule", "variant", "knob")}
+    assert best64["variant"] in ("items", "tiles", "records") and best32["schedule"] in ("levels", "dataflow", "persist")
+    assert sw.shape(0) == {k: best64[k] for k in ("schedule", "variant", "knob", "vector")}
     psi = np.empty(sw.psi_shape)
     sw.sweep(psi, src)
     assert bits_equal(psi, o.sweep(st, src_ang=src))

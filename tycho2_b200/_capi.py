@@ -39,7 +39,7 @@ class SolveOpts(C.Structure):
 
 
 class LaunchShape(C.Structure):
-    _fields_ = [("schedule", C.c_int), ("variant", C.c_int), ("knob", C.c_int)]
+    _fields_ = [("schedule", C.c_int), ("variant", C.c_int), ("knob", C.c_int), ("vector", C.c_int)]
 
 
 class SolveStats(C.Structure):

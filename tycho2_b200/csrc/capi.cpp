@@ -373,6 +373,7 @@ int tycho_sweeper_autotune(tycho_sweeper *h, int precision, int reps, tycho_laun
             best->schedule = sh.schedule;
             best->variant = sh.variant;
             best->knob = sh.knob;
+            best->vector = sh.vg;
         }
         return finish(s, err);
     });
@@ -383,7 +384,8 @@ int tycho_sweeper_configure(tycho_sweeper *h, int precision, const tycho_launch_
     if (!h || !shape || (precision != 0 && precision != 1))
         return finish(TYCHO_ERR_ARG, "bad sweeper, precision or shape");
     std::string err;
-    return finish(h->sw.configure(precision, shape->schedule, shape->variant, shape->knob, err), err);
+    return finish(h->sw.configure(precision, shape->schedule, shape->variant, shape->knob, err, shape->vector),
+                  err);
 }
 
 int tycho_sweeper_get_shape(const tycho_sweeper *h, int precision, tycho_launch_shape *shape)
@@ -394,6 +396,7 @@ int tycho_sweeper_get_shape(const tycho_sweeper *h, int precision, tycho_launch_
     shape->schedule = sh.schedule;
     shape->variant = sh.variant;
     shape->knob = sh.knob;
+    shape->vector = sh.vg;
     return TYCHO_OK;
 }
 

@@ -19,7 +19,15 @@ struct LevelArgs {
     void *psi;               // Real, psi layout
     uint32_t A, G;
     uint32_t gmagic;         // ceil(2^32 / G): pair -> item in the warp-tile variant (0 when G == 1)
+    uint32_t vg;             // record variant: groups per vector access (divides G)
+    uint32_t vmagic;         // ceil(2^32 / (G / vg)): task -> item (0 when G == vg)
 };
+
+// Record variant's group vector width: 16-byte accesses where G allows.
+constexpr uint32_t record_vg(bool fp32, uint32_t G)
+{
+    return fp32 ? (G % 4 == 0 ? 4 : (G % 2 == 0 ? 2 : 1)) : (G % 2 == 0 ? 2 : 1);
+}
 
 // Per-sweep state of the persistent (dataflow) schedule.
 struct DataflowArgs {
@@ -67,6 +75,14 @@ template <typename Real>
 cudaError_t launch_dataflow_record(int wpb, const LevelArgs &p, const void *rec, const DataflowArgs &df,
                                    unsigned grid, cudaStream_t s);
 template <typename Real>
-cudaError_t record_dataflow_blocks_per_sm(int wpb, int *blocks);
+cudaError_t record_dataflow_blocks_per_sm(int ipw, int vg, int *blocks);
+// Persistent levels: one cooperative launch, a bounded grid barrier between
+// levels (level_off: device copy of the n_levels + 1 level offsets).
+template <typename Real>
+cudaError_t launch_persist_record(int ipw, const LevelArgs &p, const void *rec, const uint64_t *level_off,
+                                  uint32_t n_levels, unsigned long long *barrier, const DataflowArgs &df,
+                                  unsigned grid, cudaStream_t s);
+template <typename Real>
+cudaError_t record_persist_blocks_per_sm(int ipw, int vg, int *blocks);
 
 }  // namespace tycho

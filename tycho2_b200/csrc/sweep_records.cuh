@@ -17,8 +17,9 @@
 // A warp takes IPW consecutive items; lane i < IPW copies record i into a
 // field-major (structure-of-arrays) tile in shared memory, so that lanes
 // reading one field of different items hit different banks.  The warp then
-// walks the IPW*G (item, group) pairs, pair p = lane + 32k -> item p / G,
-// group p % G, UNROLL pairs per lane at a time with all their loads issued
+// walks the IPW*G (item, group) pairs in tasks of VG consecutive groups
+// (vector loads and stores of psi rows), task t = lane + 32k -> item
+// t / (G/VG), several tasks per lane at a time with all their loads issued
 // before any arithmetic.
 //
 // Level schedule kernels use programmatic dependent launch: a level lets the
@@ -94,23 +95,50 @@ __device__ __forceinline__ void tile_fill(RecordTile<Real, IPW> &T, const ItemRe
     for (int k = 0; k < 7; ++k) T.u[k][lane] = ur[k];
 }
 
-template <typename Real, bool L2_ONLY>
-__device__ __forceinline__ Real load_psi(const Real *p)
+// VG consecutive groups of one psi/phi row move as one vector access (the
+// group index is fastest in both layouts; the host picks VG dividing G).
+template <typename Real, int VG> struct GVec;
+template <> struct GVec<float, 1> { using T = float; };
+template <> struct GVec<float, 2> { using T = float2; };
+template <> struct GVec<float, 4> { using T = float4; };
+template <> struct GVec<double, 1> { using T = double; };
+template <> struct GVec<double, 2> { using T = double2; };
+
+__device__ __forceinline__ void gv_unpack(float v, float (&o)[1]) { o[0] = v; }
+__device__ __forceinline__ void gv_unpack(float2 v, float (&o)[2]) { o[0] = v.x; o[1] = v.y; }
+__device__ __forceinline__ void gv_unpack(float4 v, float (&o)[4]) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
+__device__ __forceinline__ void gv_unpack(double v, double (&o)[1]) { o[0] = v; }
+__device__ __forceinline__ void gv_unpack(double2 v, double (&o)[2]) { o[0] = v.x; o[1] = v.y; }
+__device__ __forceinline__ void gv_store(float *p, const float (&o)[1]) { *p = o[0]; }
+__device__ __forceinline__ void gv_store(float *p, const float (&o)[2]) { *reinterpret_cast<float2 *>(p) = make_float2(o[0], o[1]); }
+__device__ __forceinline__ void gv_store(float *p, const float (&o)[4])
 {
-    if (L2_ONLY) return __ldcg(p);
-    return *p;
+    *reinterpret_cast<float4 *>(p) = make_float4(o[0], o[1], o[2], o[3]);
+}
+__device__ __forceinline__ void gv_store(double *p, const double (&o)[1]) { *p = o[0]; }
+__device__ __forceinline__ void gv_store(double *p, const double (&o)[2]) { *reinterpret_cast<double2 *>(p) = make_double2(o[0], o[1]); }
+
+// L2_ONLY: upwind rows written by other SMs during this launch (dataflow and
+// persistent schedules) are read around L1.
+template <typename Real, int VG, bool L2_ONLY>
+__device__ __forceinline__ void gv_load(const Real *p, Real (&o)[VG])
+{
+    using V = typename GVec<Real, VG>::T;
+    const V *vp = reinterpret_cast<const V *>(p);
+    if constexpr (L2_ONLY) gv_unpack(__ldcg(vp), o);
+    else gv_unpack(*vp, o);
 }
 
-// All the inputs of one (item, group) pair, loaded before any arithmetic.
-template <typename Real>
+// All the inputs of one (item, VG groups) task, loaded before any arithmetic.
+template <typename Real, int VG>
 struct PairIn {
-    Real q[4];
-    Real pn[4][3];  // [face][the three cell vertices j != f, increasing]
+    Real q[4][VG];
+    Real pn[4][3][VG];  // [face][the three cell vertices j != f, increasing][group]
 };
 
-template <typename Real, int IPW, bool L2_ONLY>
+template <typename Real, int IPW, int VG, bool L2_ONLY>
 __device__ __forceinline__ void pair_load(const LevelArgs &p, const RecordTile<Real, IPW> &T, uint32_t i,
-                                          uint32_t g, PairIn<Real> &in)
+                                          uint32_t g, PairIn<Real, VG> &in)
 {
     const uint32_t G = p.G;
     const size_t rowG = (size_t)4 * G;
@@ -121,14 +149,21 @@ __device__ __forceinline__ void pair_load(const LevelArgs &p, const RecordTile<R
         const double *qa = p.qang + (size_t)T.u[1][i] * rowG + g;
         const Real *ic = iso ? iso + (size_t)c * rowG + g : nullptr;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) in.q[v] = ic ? (Real)qa[v * G] + ic[v * G] : (Real)qa[v * G];
+        for (int v = 0; v < 4; ++v) {
+            Real icv[VG];
+            if (ic) gv_load<Real, VG, false>(ic + v * G, icv);
+#pragma unroll
+            for (int k = 0; k < VG; ++k) in.q[v][k] = ic ? (Real)qa[v * G + k] + icv[k] : (Real)qa[v * G + k];
+        }
     } else if (iso) {
         const Real *ic = iso + (size_t)c * rowG + g;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) in.q[v] = ic[v * G];
+        for (int v = 0; v < 4; ++v) gv_load<Real, VG, false>(ic + v * G, in.q[v]);
     } else {
 #pragma unroll
-        for (int v = 0; v < 4; ++v) in.q[v] = Real(0);
+        for (int v = 0; v < 4; ++v)
+#pragma unroll
+            for (int k = 0; k < VG; ++k) in.q[v][k] = Real(0);
     }
     const uint32_t nmap = T.u[2][i];
 #pragma unroll
@@ -140,78 +175,102 @@ __device__ __forceinline__ void pair_load(const LevelArgs &p, const RecordTile<R
         for (int k = 0; k < 3; ++k) {
             const int j = k < f ? k : k + 1;
             const uint32_t nv = (nmap >> ((f * 4 + j) * 2)) & 3u;
-            in.pn[f][k] = live ? load_psi<Real, L2_ONLY>(nrow + nv * G) : Real(0);
-        }
-    }
-}
-
-template <typename Real, int IPW>
-__device__ __forceinline__ void pair_solve_store(const LevelArgs &p, const RecordTile<Real, IPW> &T, uint32_t i,
-                                                 uint32_t g, const PairIn<Real> &in)
-{
-    const Real *q = in.q;
-    const Real vs20 = T.f[4][i];
-    Real b[4];
-    b[0] = vs20 * (Real(2) * q[0] + q[1] + q[2] + q[3]);
-    b[1] = vs20 * (q[0] + Real(2) * q[1] + q[2] + q[3]);
-    b[2] = vs20 * (q[0] + q[1] + Real(2) * q[2] + q[3]);
-    b[3] = vs20 * (q[0] + q[1] + q[2] + Real(2) * q[3]);
-    // Upwind faces in increasing order; for face f, rows i != f in increasing
-    // order, each subtracting its three terms j != f in increasing order.
+            if (live) {
+                gv_load<Real, VG, L2_ONLY>(nrow + nv * G, in.pn[f][k]);
+            } else {
 #pragma unroll
-    for (int f = 0; f < 4; ++f) {
-        const Real t1 = T.f[f][i];
-        if (t1 < Real(0)) {
-            const Real t2 = Real(2) * t1;
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                if (r == f) continue;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const int j = k < f ? k : k + 1;
-                    b[r] -= (r == j ? t2 : t1) * in.pn[f][k];
-                }
+                for (int e = 0; e < VG; ++e) in.pn[f][k][e] = Real(0);
             }
         }
     }
-    b[0] = b[0] * T.f[5][i];
-    b[1] = b[1] - b[0] * T.f[9][i];
-    b[2] = b[2] - b[0] * T.f[10][i];
-    b[3] = b[3] - b[0] * T.f[11][i];
-    b[1] = b[1] * T.f[12][i];
-    b[2] = b[2] - b[1] * T.f[15][i];
-    b[3] = b[3] - b[1] * T.f[16][i];
-    b[2] = b[2] * T.f[17][i];
-    b[3] = b[3] - b[2] * T.f[19][i];
-    b[3] = div_ref(b[3], T.f[20][i]);
-    b[2] = b[2] - T.f[18][i] * b[3];
-    b[1] = b[1] - T.f[14][i] * b[3] - T.f[13][i] * b[2];
-    b[0] = b[0] - T.f[8][i] * b[3] - T.f[7][i] * b[2] - T.f[6][i] * b[1];
-    Real *__restrict__ out = reinterpret_cast<Real *>(p.psi) + (size_t)T.u[1][i] * 4 * p.G + g;
-#pragma unroll
-    for (int v = 0; v < 4; ++v) out[v * p.G] = b[v];
 }
 
-template <typename Real, int IPW, int UNROLL, bool L2_ONLY>
+// The per-group arithmetic of one task, group by group in the reference's
+// operation order (the factors come from shared memory once per task).
+template <typename Real, int IPW, int VG>
+__device__ __forceinline__ void pair_solve_store(const LevelArgs &p, const RecordTile<Real, IPW> &T, uint32_t i,
+                                                 uint32_t g, const PairIn<Real, VG> &in)
+{
+    Real res[4][VG];
+#pragma unroll
+    for (int e = 0; e < VG; ++e) {
+        const Real q[4] = {in.q[0][e], in.q[1][e], in.q[2][e], in.q[3][e]};
+        const Real vs20 = T.f[4][i];
+        Real b[4];
+        b[0] = vs20 * (Real(2) * q[0] + q[1] + q[2] + q[3]);
+        b[1] = vs20 * (q[0] + Real(2) * q[1] + q[2] + q[3]);
+        b[2] = vs20 * (q[0] + q[1] + Real(2) * q[2] + q[3]);
+        b[3] = vs20 * (q[0] + q[1] + q[2] + Real(2) * q[3]);
+        // Upwind faces in increasing order; for face f, rows r != f in
+        // increasing order, each subtracting its three terms j != f in
+        // increasing order.
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            const Real t1 = T.f[f][i];
+            if (t1 < Real(0)) {
+                const Real t2 = Real(2) * t1;
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    if (r == f) continue;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const int j = k < f ? k : k + 1;
+                        b[r] -= (r == j ? t2 : t1) * in.pn[f][k][e];
+                    }
+                }
+            }
+        }
+        b[0] = b[0] * T.f[5][i];
+        b[1] = b[1] - b[0] * T.f[9][i];
+        b[2] = b[2] - b[0] * T.f[10][i];
+        b[3] = b[3] - b[0] * T.f[11][i];
+        b[1] = b[1] * T.f[12][i];
+        b[2] = b[2] - b[1] * T.f[15][i];
+        b[3] = b[3] - b[1] * T.f[16][i];
+        b[2] = b[2] * T.f[17][i];
+        b[3] = b[3] - b[2] * T.f[19][i];
+        b[3] = div_ref(b[3], T.f[20][i]);
+        b[2] = b[2] - T.f[18][i] * b[3];
+        b[1] = b[1] - T.f[14][i] * b[3] - T.f[13][i] * b[2];
+        b[0] = b[0] - T.f[8][i] * b[3] - T.f[7][i] * b[2] - T.f[6][i] * b[1];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) res[v][e] = b[v];
+    }
+    Real *__restrict__ out = reinterpret_cast<Real *>(p.psi) + (size_t)T.u[1][i] * 4 * p.G + g;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) gv_store(out + v * p.G, res[v]);
+}
+
+// Tasks per lane in flight: fewer as the vector width grows (registers).
+template <typename Real, int IPW, int VG>
+__host__ __device__ constexpr int record_unroll()
+{
+    return VG == 1 ? (IPW == 32 ? 4 : 2) : (VG == 2 && sizeof(Real) == 4 ? 2 : 1);
+}
+
+// The warp walks the IPW * (G / VG) tasks of a tile: task t -> item
+// t / (G / VG), groups VG * (t % (G / VG)) and the next VG - 1.
+template <typename Real, int IPW, int VG, bool L2_ONLY>
 __device__ __forceinline__ void record_pairs(const LevelArgs &p, const RecordTile<Real, IPW> &T, uint32_t lane)
 {
-    const uint32_t G = p.G, npairs = (uint32_t)IPW * G;
-    for (uint32_t q0 = lane; q0 < npairs; q0 += 32u * UNROLL) {
-        PairIn<Real> in[UNROLL];
+    constexpr int UNROLL = record_unroll<Real, IPW, VG>();
+    const uint32_t gpv = p.G / VG, ntask = (uint32_t)IPW * gpv;
+    for (uint32_t q0 = lane; q0 < ntask; q0 += 32u * UNROLL) {
+        PairIn<Real, VG> in[UNROLL];
         uint32_t item[UNROLL], grp[UNROLL];
         bool live[UNROLL];
 #pragma unroll
         for (int u = 0; u < UNROLL; ++u) {
             const uint32_t q = q0 + 32u * u;
-            const uint32_t it = G == 1u ? q : __umulhi(q, p.gmagic);
+            const uint32_t it = gpv == 1u ? q : __umulhi(q, p.vmagic);
             item[u] = it < (uint32_t)IPW ? it : 0u;
-            grp[u] = q - it * G;
-            live[u] = q < npairs && T.u[0][item[u]] != kSentinel;
-            if (live[u]) pair_load<Real, IPW, L2_ONLY>(p, T, item[u], grp[u], in[u]);
+            grp[u] = (q - it * gpv) * VG;
+            live[u] = q < ntask && T.u[0][item[u]] != kSentinel;
+            if (live[u]) pair_load<Real, IPW, VG, L2_ONLY>(p, T, item[u], grp[u], in[u]);
         }
 #pragma unroll
         for (int u = 0; u < UNROLL; ++u)
-            if (live[u]) pair_solve_store(p, T, item[u], grp[u], in[u]);
+            if (live[u]) pair_solve_store<Real, IPW, VG>(p, T, item[u], grp[u], in[u]);
     }
 }
 
@@ -226,7 +285,7 @@ __device__ __forceinline__ void pdl_wait_prerequisites()
 }
 
 // Level schedule: 4 warps per block, IPW items per warp.
-template <typename Real, int IPW, int UNROLL>
+template <typename Real, int IPW, int VG>
 __global__ void __launch_bounds__(128)
 sweep_record_level_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict__ rec, const uint64_t begin,
                           const uint64_t end)
@@ -240,13 +299,13 @@ sweep_record_level_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict_
     pdl_wait_prerequisites();
     if (!any) return;
     __syncwarp();
-    record_pairs<Real, IPW, UNROLL, false>(p, tiles[w], lane);
+    record_pairs<Real, IPW, VG, false>(p, tiles[w], lane);
 }
 
 // Dataflow schedule: persistent warps take IPW-item chunks round-robin; lane
 // i < IPW stages record i and waits for its upwind items, the warp sweeps the
 // chunk's pairs, fences, and lane i publishes item i's epoch.
-template <typename Real, int IPW, int UNROLL>
+template <typename Real, int IPW, int VG>
 __global__ void __launch_bounds__(128)
 sweep_record_dataflow_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict__ rec, const DataflowArgs df)
 {
@@ -273,11 +332,159 @@ sweep_record_dataflow_kernel(const LevelArgs p, const ItemRecord<Real> *__restri
             if (!ok) T.u[0][lane] = kSentinel;
         }
         __syncwarp();
-        record_pairs<Real, IPW, UNROLL, true>(p, T, lane);
+        record_pairs<Real, IPW, VG, true>(p, T, lane);
         __threadfence();
         __syncwarp();
         if (ok) st_release_gpu(df.done + ca, epoch);
     }
+}
+
+// Block-level barrier across the whole (co-resident) grid with a bounded
+// wait: thread 0 of every block adds one arrival to *count and waits until
+// it reaches `target`; gives up after spin_limit polls (records the level in
+// err, raises abort) so that no wait can hang the device.
+__device__ __forceinline__ bool grid_barrier(unsigned long long *count, unsigned long long target,
+                                             const DataflowArgs &df, uint32_t level)
+{
+    __shared__ int ok_s;
+    __syncthreads();  // the block's psi stores happen before thread 0's fence
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        __threadfence();
+        atomicAdd(count, 1ull);
+        unsigned backoff = 32;
+        uint32_t spin = 0;
+        for (;;) {
+            unsigned long long v;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(count) : "memory");
+            if (v >= target) break;
+            if (*(volatile const uint32_t *)df.abort || ++spin > df.spin_limit) {
+                if (atomicCAS(df.err, 0u, (uint32_t)kErrTimeoutCode) == 0u) {
+                    df.err[1] = level;
+                    df.err[2] = 4u;  // face 4: a level barrier, not an upwind face
+                }
+                atomicExch(df.abort, 1u);
+                ok = 0;
+                break;
+            }
+            __nanosleep(backoff);
+            if (backoff < 256) backoff <<= 1;
+        }
+        __threadfence();
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+// Persistent levels: one cooperative launch per sweep; all warps take the
+// chunks of level L (warp w: chunks w, w + W, ...), then every block meets at
+// a barrier before level L+1.  The records of a warp's first chunk of the
+// next level are staged before the barrier (they do not depend on psi).
+template <typename Real, int IPW, int VG>
+__global__ void __launch_bounds__(128)
+sweep_record_persist_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict__ rec,
+                            const uint64_t *__restrict__ level_off, const uint32_t n_levels,
+                            unsigned long long *barrier, const DataflowArgs df)
+{
+    __shared__ RecordTile<Real, IPW> tiles[4][2];
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    const uint64_t warp = (uint64_t)blockIdx.x * 4 + w;
+    const uint64_t nwarps = (uint64_t)gridDim.x * 4;
+    int cur = 0;
+    // stage the first chunk of level 0
+    if (warp * IPW < level_off[1] - level_off[0]) tile_fill<Real, IPW>(tiles[w][cur], rec + level_off[0] + warp * IPW + lane, lane, true);
+    for (uint32_t L = 0; L < n_levels; ++L) {
+        const uint64_t b = level_off[L], nch = (level_off[L + 1] - b) / IPW;
+        for (uint64_t ch = warp, k = 0; ch < nch; ch += nwarps, ++k) {
+            if (k > 0) tile_fill<Real, IPW>(tiles[w][cur], rec + b + ch * IPW + lane, lane, true);
+            __syncwarp();
+            record_pairs<Real, IPW, VG, true>(p, tiles[w][cur], lane);
+            __syncwarp();
+        }
+        if (L + 1 < n_levels) {
+            const uint64_t nb = level_off[L + 1];
+            if (warp * IPW < level_off[L + 2] - nb)
+                tile_fill<Real, IPW>(tiles[w][cur ^ 1], rec + nb + warp * IPW + lane, lane, true);
+            if (!grid_barrier(barrier, (unsigned long long)(L + 1) * gridDim.x, df, L)) return;
+            cur ^= 1;
+        }
+    }
+}
+
+// Kernel selection by items per warp and group vector width.  The double
+// variants stop at VG = 2 (one 16-byte access); two 32-item double tiles per
+// warp (persistent levels) exceed static shared memory.
+template <typename Real, int IPW, int VG>
+struct LevelK {
+    static const void *fn() { return (const void *)sweep_record_level_kernel<Real, IPW, VG>; }
+};
+template <typename Real, int IPW, int VG>
+struct DataflowK {
+    static const void *fn() { return (const void *)sweep_record_dataflow_kernel<Real, IPW, VG>; }
+};
+template <typename Real, int IPW, int VG>
+struct PersistK {
+    static const void *fn()
+    {
+        if constexpr (sizeof(Real) == 8 && IPW == 32) return nullptr;
+        else return (const void *)sweep_record_persist_kernel<Real, IPW, VG>;
+    }
+};
+
+template <typename Real, template <typename, int, int> class K, int IPW>
+static const void *record_fn_vg(int vg)
+{
+    switch (vg) {
+    case 1: return K<Real, IPW, 1>::fn();
+    case 2: return K<Real, IPW, 2>::fn();
+    case 4:
+        if constexpr (sizeof(Real) == 4) return K<Real, IPW, 4>::fn();
+        else return nullptr;
+    default: return nullptr;
+    }
+}
+
+template <typename Real, template <typename, int, int> class K>
+static const void *record_fn(int ipw, int vg)
+{
+    switch (ipw) {
+    case 8: return record_fn_vg<Real, K, 8>(vg);
+    case 16: return record_fn_vg<Real, K, 16>(vg);
+    case 32: return record_fn_vg<Real, K, 32>(vg);
+    default: return nullptr;
+    }
+}
+
+template <typename Real>
+cudaError_t record_persist_blocks_per_sm(int ipw, int vg, int *blocks)
+{
+    const void *fn = record_fn<Real, PersistK>(ipw, vg);
+    if (!fn) return cudaErrorInvalidValue;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, fn, 128, 0);
+}
+
+template <typename Real>
+cudaError_t launch_persist_record(int ipw, const LevelArgs &p, const void *rec, const uint64_t *level_off,
+                                  uint32_t n_levels, unsigned long long *barrier, const DataflowArgs &df,
+                                  unsigned grid, cudaStream_t s)
+{
+    const void *fn = record_fn<Real, PersistK>(ipw, (int)p.vg);
+    if (!fn || grid == 0) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(barrier, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(128);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const ItemRecord<Real> *r = (const ItemRecord<Real> *)rec;
+    void *args[] = {(void *)&p, (void *)&r, (void *)&level_off, (void *)&n_levels, (void *)&barrier, (void *)&df};
+    return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 template <typename Real>
@@ -288,14 +495,17 @@ cudaError_t launch_item_records(const LevelArgs &p, uint64_t n, void *out, cudaS
     return cudaGetLastError();
 }
 
-template <typename Real, int IPW>
-static cudaError_t launch_level_record_ipw(const LevelArgs &p, const ItemRecord<Real> *r, uint64_t begin,
-                                           uint64_t end, cudaStream_t s)
+// knob = items per warp (8, 16 or 32); one launch over items [begin, end).
+template <typename Real>
+cudaError_t launch_level_record(int ipw, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
+                                cudaStream_t s)
 {
-    const uint64_t warps = (end - begin + IPW - 1) / IPW;
-    const unsigned blocks = (unsigned)((warps + 3) / 4);
+    if (end <= begin) return cudaSuccess;
+    const void *fn = record_fn<Real, LevelK>(ipw, (int)p.vg);
+    if (!fn) return cudaErrorInvalidValue;
+    const uint64_t warps = (end - begin + ipw - 1) / ipw;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(blocks);
+    cfg.gridDim = dim3((unsigned)((warps + 3) / 4));
     cfg.blockDim = dim3(128);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -303,40 +513,15 @@ static cudaError_t launch_level_record_ipw(const LevelArgs &p, const ItemRecord<
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    constexpr int U = IPW == 32 ? 4 : 2;
-    return cudaLaunchKernelEx(&cfg, sweep_record_level_kernel<Real, IPW, U>, p, r, begin, end);
-}
-
-// knob = items per warp (8, 16 or 32).
-template <typename Real>
-cudaError_t launch_level_record(int ipw, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
-                                cudaStream_t s)
-{
-    if (end <= begin) return cudaSuccess;
     const ItemRecord<Real> *r = (const ItemRecord<Real> *)rec;
-    switch (ipw) {
-    case 8: return launch_level_record_ipw<Real, 8>(p, r, begin, end, s);
-    case 16: return launch_level_record_ipw<Real, 16>(p, r, begin, end, s);
-    case 32: return launch_level_record_ipw<Real, 32>(p, r, begin, end, s);
-    default: return cudaErrorInvalidValue;
-    }
+    void *args[] = {(void *)&p, (void *)&r, (void *)&begin, (void *)&end};
+    return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 template <typename Real>
-static const void *record_dataflow_fn(int ipw)
+cudaError_t record_dataflow_blocks_per_sm(int ipw, int vg, int *blocks)
 {
-    switch (ipw) {
-    case 8: return (const void *)sweep_record_dataflow_kernel<Real, 8, 2>;
-    case 16: return (const void *)sweep_record_dataflow_kernel<Real, 16, 2>;
-    case 32: return (const void *)sweep_record_dataflow_kernel<Real, 32, 4>;
-    default: return nullptr;
-    }
-}
-
-template <typename Real>
-cudaError_t record_dataflow_blocks_per_sm(int ipw, int *blocks)
-{
-    const void *fn = record_dataflow_fn<Real>(ipw);
+    const void *fn = record_fn<Real, DataflowK>(ipw, vg);
     if (!fn) return cudaErrorInvalidValue;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, fn, 128, 0);
 }
@@ -345,7 +530,7 @@ template <typename Real>
 cudaError_t launch_dataflow_record(int ipw, const LevelArgs &p, const void *rec, const DataflowArgs &df,
                                    unsigned grid, cudaStream_t s)
 {
-    const void *fn = record_dataflow_fn<Real>(ipw);
+    const void *fn = record_fn<Real, DataflowK>(ipw, (int)p.vg);
     if (!fn || grid == 0) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);

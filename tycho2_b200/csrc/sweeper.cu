@@ -56,7 +56,8 @@ Sweeper::~Sweeper()
     for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
     void *bufs[] = {d_items_, d_abar64_, d_abar32_, d_adj_, d_nbrmap_, d_cellk64_, d_cellk32_,
                     d_w_, d_sigs_, d_scat_, d_qiso_, d_qang_, d_src_, d_iso_, d_iso32_, d_psi_,
-                    d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_, d_done_, d_ctl_, d_rec_[0], d_rec_[1]};
+                    d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_, d_done_, d_ctl_, d_rec_[0], d_rec_[1],
+                    d_level_off_, d_barrier_};
     for (void *b : bufs)
         if (b) cudaFree(b);
     reducer_free(red_);
@@ -144,6 +145,8 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     TY_CUDA(cudaMemsetAsync(d_done_, 0, sizeof(uint32_t) * (size_t)nc_ * A_, stream_));
     TY_CUDA(cudaMalloc(&d_ctl_, sizeof(uint32_t) * 8));
     TY_CUDA(cudaMemsetAsync(d_ctl_, 0, sizeof(uint32_t) * 8, stream_));
+    TY_CUDA(upload(d_level_off_, sched_.level_offset.data(), sched_.level_offset.size(), stream_));
+    TY_CUDA(cudaMalloc(&d_barrier_, sizeof(unsigned long long)));
     // Default launch shape: warp tiles (4 warps per block) on the persistent
     // dataflow schedule; explicit threads-per-item selects the item-parallel
     // variant.  The autotuner can replace either.
@@ -154,9 +157,22 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     return kOk;
 }
 
-int Sweeper::configure(int prec, int schedule, int variant, int knob, std::string &err)
+int Sweeper::configure(int prec, int schedule, int variant, int knob, std::string &err, int vg)
 {
-    if (schedule != 1 && schedule != 2) { err = "schedule must be 1 (levels) or 2 (dataflow)"; return kErrArg; }
+    if (vg == 0) vg = (int)record_vg(prec != 0, (uint32_t)G_);
+    if (vg != 1 && vg != 2 && !(vg == 4 && prec == 1)) {
+        err = "group vector width must be 1 or 2 (FP64), 1, 2 or 4 (FP32)";
+        return kErrArg;
+    }
+    if (G_ % vg != 0) { err = "group vector width must divide the number of groups"; return kErrArg; }
+    if (schedule < 1 || schedule > 3) {
+        err = "schedule must be 1 (levels), 2 (dataflow) or 3 (persistent levels)";
+        return kErrArg;
+    }
+    if (schedule == 3 && variant != 2) {
+        err = "the persistent-levels schedule runs the record variant only";
+        return kErrArg;
+    }
     if (variant == 0 && knob != 1 && knob != 2 && knob != 4 && knob != 8 && knob != 16) {
         err = "item-parallel variant: threads per item must be 1, 2, 4, 8 or 16";
         return kErrArg;
@@ -167,6 +183,10 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
     }
     if (variant == 2 && knob != 8 && knob != 16 && knob != 32) {
         err = "record variant: items per warp must be 8, 16 or 32";
+        return kErrArg;
+    }
+    if (schedule == 3 && prec == 0 && knob == 32) {
+        err = "persistent levels in FP64: items per warp must be 8 or 16";
         return kErrArg;
     }
     if (variant < 0 || variant > 2) {
@@ -182,14 +202,22 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
         TY_CUDA(prec ? tile_dataflow_blocks_per_sm<float>(knob, &per_sm)
                      : tile_dataflow_blocks_per_sm<double>(knob, &per_sm));
     else
-        TY_CUDA(prec ? record_dataflow_blocks_per_sm<float>(knob, &per_sm)
-                     : record_dataflow_blocks_per_sm<double>(knob, &per_sm));
+        TY_CUDA(prec ? record_dataflow_blocks_per_sm<float>(knob, vg, &per_sm)
+                     : record_dataflow_blocks_per_sm<double>(knob, vg, &per_sm));
     if (per_sm < 1) { err = "dataflow kernel does not fit on an SM"; return kErrCuda; }
+    int persist_per_sm = 0;
+    if (schedule == 3) {
+        TY_CUDA(prec ? record_persist_blocks_per_sm<float>(knob, vg, &persist_per_sm)
+                     : record_persist_blocks_per_sm<double>(knob, vg, &persist_per_sm));
+        if (persist_per_sm < 1) { err = "persistent-levels kernel does not fit on an SM"; return kErrCuda; }
+    }
     LaunchShape &sh = shape_[prec ? 1 : 0];
     sh.schedule = schedule;
     sh.variant = variant;
     sh.knob = knob;
+    sh.vg = variant == 2 ? vg : 1;
     sh.grid = (unsigned)(sms * per_sm);
+    sh.persist_grid = (unsigned)(sms * persist_per_sm);
     // cached level graphs were captured for the previous launch shape
     for (auto it = graphs_.begin(); it != graphs_.end();) {
         if (std::get<0>(it->first) == prec) {
@@ -210,21 +238,25 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
     if (!have_xs_) { err = "cross sections not set"; return kErrMissing; }
     double best = 1e300;
     LaunchShape keep = shape_[prec ? 1 : 0];
-    for (int sched = 1; sched <= 2; ++sched)
+    for (int sched = 1; sched <= 3; ++sched)
         for (int variant = 0; variant <= 2; ++variant)
             for (int knob : {1, 2, 4, 8, 16, 32}) {
                 if (variant == 0 && ((knob > 2 * G_ && knob > 1) || knob > 16)) continue;  // idle lanes
                 if (variant == 1 && knob > 4) continue;
                 if (variant == 2 && knob < 8) continue;
-                const int cs = configure(prec, sched, variant, knob, err);
-                if (cs == kErrOom) continue;  // records do not fit next to psi
-                TY_CHECK(cs);
-                double ms[2];
-                TY_CHECK(time_sweeps(prec, 1, false, ms, err));  // warm-up (and graph capture)
-                TY_CHECK(time_sweeps(prec, reps, false, ms, err));
-                if (ms[0] < best) { best = ms[0]; keep = shape_[prec ? 1 : 0]; }
+                if (sched == 3 && (variant != 2 || (prec == 0 && knob == 32))) continue;
+                for (int vg : {1, 2, 4}) {
+                    if (vg > 1 && (variant != 2 || G_ % vg != 0 || (vg == 4 && prec == 0))) continue;
+                    const int cs = configure(prec, sched, variant, knob, err, vg);
+                    if (cs == kErrOom) continue;  // records do not fit next to psi
+                    TY_CHECK(cs);
+                    double ms[2];
+                    TY_CHECK(time_sweeps(prec, 1, false, ms, err));  // warm-up (and graph capture)
+                    TY_CHECK(time_sweeps(prec, reps, false, ms, err));
+                    if (ms[0] < best) { best = ms[0]; keep = shape_[prec ? 1 : 0]; }
+                }
             }
-    TY_CHECK(configure(prec, keep.schedule, keep.variant, keep.knob, err));
+    TY_CHECK(configure(prec, keep.schedule, keep.variant, keep.knob, err, keep.vg));
     if (best_shape) *best_shape = shape_[prec ? 1 : 0];
     if (best_ms) *best_ms = best;
     return kOk;
@@ -264,6 +296,8 @@ LevelArgs Sweeper::level_args(int prec, const void *iso, const double *qang, voi
     p.A = (uint32_t)A_;
     p.G = (uint32_t)G_;
     p.gmagic = group_magic((uint32_t)G_);
+    p.vg = (uint32_t)shape_[prec ? 1 : 0].vg;
+    p.vmagic = group_magic((uint32_t)G_ / p.vg);
     return p;
 }
 
@@ -364,6 +398,24 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
 {
     const void *iso = has_iso ? (prec ? (const void *)d_iso32_ : (const void *)d_iso_) : nullptr;
     const LaunchShape &sh = shape_[prec ? 1 : 0];
+    if (sh.schedule == 3) {
+        TY_CHECK(ensure_records(prec, true, err));
+        const LevelArgs p = level_args(prec, iso, qang, d_psi_);
+        DataflowArgs df;
+        df.done = d_done_;
+        df.err = d_ctl_;
+        df.abort = d_ctl_ + 3;
+        df.epoch = d_ctl_ + 4;
+        df.n_items = sched_.items.size();
+        df.spin_limit = 1u << 22;
+        if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
+        TY_CUDA(prec ? launch_persist_record<float>(sh.knob, p, d_rec_[1], d_level_off_, sched_.n_levels,
+                                                    d_barrier_, df, sh.persist_grid, stream_)
+                     : launch_persist_record<double>(sh.knob, p, d_rec_[0], d_level_off_, sched_.n_levels,
+                                                     d_barrier_, df, sh.persist_grid, stream_));
+        if (end) TY_CUDA(cudaEventRecord(end, stream_));
+        return kOk;
+    }
     if (sh.schedule == 2) {
         const LevelArgs p = level_args(prec, iso, qang, d_psi_);
         DataflowArgs df;

@@ -28,12 +28,15 @@ struct SweeperOptions {
 
 // Launch shape of one precision's sweep.
 struct LaunchShape {
-    int schedule = 2;   // 1 one launch per wavefront level, 2 persistent dataflow
+    int schedule = 2;   // 1 one launch per wavefront level, 2 persistent dataflow,
+                        // 3 persistent levels (record variant only)
     int variant = 1;    // 0 item-parallel (knob = threads per item),
                         // 1 warp tiles (knob = warps per block),
-                        // 2 precomputed per-item records (knob = warps per block)
+                        // 2 precomputed per-item records (knob = items per warp)
     int knob = 4;
-    unsigned grid = 0;  // dataflow: co-resident blocks
+    int vg = 1;                 // records: groups per vector access of a psi row
+    unsigned grid = 0;          // dataflow kernel of this variant: co-resident blocks
+    unsigned persist_grid = 0;  // persistent-levels kernel: co-resident blocks
 };
 
 struct SolveOptions {
@@ -63,7 +66,8 @@ public:
               std::string &err);
     int write_psi(const std::string &path, std::string &err);
     int time_sweeps(int precision, int n, bool flush_l2, double *ms, std::string &err);
-    int configure(int prec, int schedule, int variant, int knob, std::string &err);
+    // vg: record variant's groups per vector access (0 = widest dividing G).
+    int configure(int prec, int schedule, int variant, int knob, std::string &err, int vg = 0);
     int autotune(int prec, int reps, LaunchShape *best, double *best_ms, std::string &err);
     const LaunchShape &shape(int prec) const { return shape_[prec ? 1 : 0]; }
 
@@ -145,6 +149,9 @@ private:
     // record variant: per-item factors, [0] FP64, [1] FP32
     void *d_rec_[2] = {nullptr, nullptr};
     bool rec_valid_[2] = {false, false};
+    // persistent-levels schedule: level offsets and the grid barrier counter
+    uint64_t *d_level_off_ = nullptr;
+    unsigned long long *d_barrier_ = nullptr;
 };
 
 // The no-alloc sweep (tycho_sweeper_sweep_noalloc, sweep_noalloc.cu): scratch

@@ -57,6 +57,11 @@ WORKLOADS = {
     "kuhn32_s8_g8": dict(n=32, jitter=0.05, sn=8, groups=8, sigma="lognormal", lognormal_s=0.5,
                          ratio=0.6, scatter="down", source="box", method="gmres", tol=1e-10,
                          restart=20),
+    # The 32^3 problem at 24^3 x 6 = 82,944 tets (psi 1.4 GB in FP32, over
+    # ten times L2): the size for multi-pass profiler captures.
+    "kuhn24_s8_g8": dict(n=24, jitter=0.05, sn=8, groups=8, sigma="lognormal", lognormal_s=0.5,
+                         ratio=0.6, scatter="down", source="box", method="gmres", tol=1e-10,
+                         restart=20),
     # 64^3 x 6 = 1,572,864 tets, S8, G=16, lognormal(0,1), ratio 0.99, GMRES(30).
     "kuhn64_s8_g16": dict(n=64, jitter=0.05, sn=8, groups=16, sigma="lognormal", lognormal_s=1.0,
                           ratio=0.99, scatter="down", source="box", method="mixed", tol=1e-10,

@@ -143,7 +143,7 @@ class SweeperCuda:
     refinement on the device and keeps psi resident.
     """
 
-    SCHEDULES = {"auto": 0, "levels": 1, "dataflow": 2}
+    SCHEDULES = {"auto": 0, "levels": 1, "dataflow": 2, "persist": 3}
 
     def __init__(self, mesh, sn_order, n_groups, gauss_elim="NoPivot", fp32=False, device=0,
                  tpi64=0, tpi32=0, schedule="auto"):
@@ -226,8 +226,9 @@ class SweeperCuda:
 
     @staticmethod
     def _shape_dict(sh):
-        return {"schedule": {1: "levels", 2: "dataflow"}[sh.schedule],
-                "variant": {0: "items", 1: "tiles", 2: "records"}[sh.variant], "knob": sh.knob}
+        return {"schedule": {1: "levels", 2: "dataflow", 3: "persist"}[sh.schedule],
+                "variant": {0: "items", 1: "tiles", 2: "records"}[sh.variant], "knob": sh.knob,
+                "vector": sh.vector}
 
     def autotune(self, precision, reps=3):
         """Picks the fastest launch shape (schedule, variant, knob) for one precision."""
@@ -237,10 +238,11 @@ class SweeperCuda:
         d["ms"] = ms.value
         return d
 
-    def configure(self, precision, schedule, variant, knob):
-        """schedule 'levels'|'dataflow'; variant 'items' (knob = lanes per item),
-        'tiles' (knob = warps per block) or 'records' (knob = items per warp)."""
-        sh = _capi.LaunchShape(self.SCHEDULES[schedule], self.VARIANTS[variant], knob)
+    def configure(self, precision, schedule, variant, knob, vector=0):
+        """schedule 'levels'|'dataflow'|'persist' (records only); variant 'items' (knob = lanes per item),
+        'tiles' (knob = warps per block) or 'records' (knob = items per warp; vector = groups per
+        psi-row access, 0 = widest dividing nGroups)."""
+        sh = _capi.LaunchShape(self.SCHEDULES[schedule], self.VARIANTS[variant], knob, vector)
         check(lib().tycho_sweeper_configure(self._h, precision, C.byref(sh)))
 
     def shape(self, precision):
