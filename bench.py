@@ -193,10 +193,9 @@ KERNELS = {
 SCHED = {"levels": 1, "dataflow": 2, "persist": 3}
 
 
-def kernel_name(shape, fp32, G):
-    vg = (4 if G % 4 == 0 else 2 if G % 2 == 0 else 1) if fp32 else (2 if G % 2 == 0 else 1)
+def kernel_name(shape, fp32):
     return KERNELS[(SCHED[shape["schedule"]], shape["variant"])].format(
-        r="float" if fp32 else "double", k=shape["knob"], vg=vg)
+        r="float" if fp32 else "double", k=shape["knob"], vg=shape["vector"])
 
 
 def launches_per_sweep(shape, n_levels):
@@ -275,7 +274,7 @@ def run_b200(args):
     b64 = algorithmic_bytes(nc, A, G, info["n_incoming_interior"], 8)
     ach32 = b32 / (lvl32 * 1e-3) / 1e9
     ach64 = b64 / (lvl64 * 1e-3) / 1e9
-    k32, k64 = kernel_name(shape32, True, G), kernel_name(shape64, False, G)
+    k32, k64 = kernel_name(shape32, True), kernel_name(shape64, False)
 
     # Solve-level check: mixed precision vs FP64 GMRES on the same problem.
     solve = None

@@ -258,6 +258,50 @@ int tycho_sweeper_sweep_noalloc(tycho_sweeper *sw, int precision, const void *is
 int tycho_sweeper_time_sweeps(tycho_sweeper *sw, int precision, int n, int flush_l2,
                               double *ms);
 
+/* ---- batched solves: many independent instances on one GPU ------------
+   No counterpart in the reference, which solves one problem per process.
+   Members are sweepers (cross sections and isotropic fixed source set) on
+   the batch's device, of any size, group count and SN order.  Every step
+   runs one FP64 pass over the members in source iteration or at an outer
+   refinement step and one FP32 pass over the members in their inner
+   correction solve; each pass is one CUDA graph whose wavefront launches
+   take their work from a device list over (member, level) built by the
+   pass's first kernel.  A member's arithmetic and reductions do not depend
+   on the other members: its result is bit-identical alone and in any mix. */
+
+typedef struct tycho_batch tycho_batch;
+
+typedef struct tycho_batch_opts {
+    int method;       /* TYCHO_SOURCE_ITERATION (FP64 throughout) or
+                         TYCHO_MIXED_GMRES's batched form: FP32-sweep source
+                         iteration on the correction inside FP64 refinement */
+    int iter_max;     /* sweeps of the solve (FP32 inner sweeps included) */
+    double err_max;   /* stop: L1 relative change of phi over one FP64 sweep
+                         (SourceIteration.cc:167-175) */
+    double inner_tol; /* mixed: inner stop, L1 relative change of the correction */
+    int inner_max;    /* mixed: inner sweeps per refinement */
+    int refine_max;   /* mixed: refinements */
+} tycho_batch_opts;
+
+/* ipw32 / ipw64: items per warp of the FP32 / FP64 wavefront kernels (8, 16, 32). */
+int tycho_batch_create(int device, int ipw32, int ipw64, tycho_batch **out);
+void tycho_batch_destroy(tycho_batch *b);
+/* Adds a member (the sweeper must outlive its membership); its solve starts
+   from phi = 0 at the next step.  *id identifies it. */
+int tycho_batch_add(tycho_batch *b, tycho_sweeper *sw, const tycho_batch_opts *opts, int *id);
+int tycho_batch_remove(tycho_batch *b, int id);
+/* One step of every running member; *n_running = members still running. */
+int tycho_batch_step(tycho_batch *b, int *n_running);
+/* Steps until every member is done. */
+int tycho_batch_run(tycho_batch *b);
+/* A member's statistics and (phi != NULL) its phi, phi layout.  *done is 1
+   once it has converged or hit a limit.  The member's sweeper keeps the FP64
+   psi of its last sweep (tycho_sweeper_write_psi). */
+int tycho_batch_result(tycho_batch *b, int id, double *phi, tycho_solve_stats *stats, int *done);
+/* Device time of all passes so far (ms) and pass counts, [0] FP64, [1] FP32,
+   and the cell x angle x group updates swept in each. */
+int tycho_batch_timing(const tycho_batch *b, double *ms, int *passes, double *updates);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,122 @@
+"""Batched solves of uneven instances (mesh size, group count, SN order).
+
+Parity: a member's FP64 source iteration reproduces the oracle's
+SourceIteration::fixedPoint restatement; the mixed-precision solve lands
+within 1e-8 (relative L1) of it; and every member's result is bit-identical
+alone and inside the mix (its arithmetic and reductions never touch another
+member's data).
+"""
+import numpy as np
+import pytest
+
+from conftest import bits_equal, rel_l1
+from helpers import kuhn
+
+pytestmark = pytest.mark.gpu
+
+# (n, jitter, sn, G, scattering ratio, downscatter)
+CASES = [(3, 0.05, 4, 1, 0.5, False), (4, 0.05, 6, 2, 0.8, True), (2, 0.05, 8, 4, 0.3, True),
+         (5, 0.05, 4, 8, 0.9, True), (3, 0.05, 8, 3, 0.6, False)]
+
+
+def _problem(workdir, case, seed):
+    import tycho2_b200 as ty
+    from tycho2_b200 import problems
+    n, jitter, sn, G, ratio, down = case
+    mesh, om = kuhn(workdir, n, jitter, seed=seed)
+    rng = np.random.default_rng(seed)
+    st = rng.lognormal(0.0, 0.5, mesh.n_cells)
+    if down:  # sigma_s(g' -> g) = sigma_t * matrix, rows summing to the ratio
+        ss, mat = st, problems.downscatter_matrix(G, ratio)
+    else:
+        ss, mat = ratio * st, None
+    q = np.ones((mesh.n_cells, 4, G))
+    sw = ty.SweeperCuda(mesh, sn, G, fp32=True)
+    sw.set_cross_sections(st, ss, mat)
+    sw.set_source(q, "isotropic")
+    return sw, om, (st, ss, mat, q)
+
+
+def _solve(sws, method, **kw):
+    import tycho2_b200 as ty
+    b = ty.BatchSolver()
+    ids = [b.add(sw, method, **kw) for sw in sws]
+    b.run()
+    out = [b.result(i) for i in ids]
+    for i in ids:
+        b.remove(i)
+    b.close()
+    return out
+
+
+def test_batch_si_matches_oracle_source_iteration(built, workdir):
+    from oracle.oracle import Oracle
+    probs = [_problem(workdir, c, 40 + k) for k, c in enumerate(CASES)]
+    res = _solve([p[0] for p in probs], "si", err_max=1e-10, iter_max=400)
+    for (sw, om, (st, ss, mat, q)), case, (phi, stats, done) in zip(probs, CASES, res):
+        o = Oracle(om, case[2], case[3])
+        _, phi_ref, it_ref, _ = o.source_iteration(st, ss, mat, q_iso=q, iter_max=400, err_max=1e-10)
+        assert done and stats["sweeps_fp32"] == 0
+        if stats["iterations"] == it_ref:
+            # same sweeps, same scatter and psi->phi arithmetic: the same bits
+            assert bits_equal(phi, phi_ref), case
+        else:  # the stopping test sits on the threshold; one extra iteration apart
+            assert abs(stats["iterations"] - it_ref) == 1 and rel_l1(phi, phi_ref) <= 1e-9, case
+
+
+def test_batch_mixed_within_1e8_of_fp64(built, workdir):
+    probs = [_problem(workdir, c, 60 + k) for k, c in enumerate(CASES)]
+    sws = [p[0] for p in probs]
+    si = _solve(sws, "si", err_max=1e-12, iter_max=2000)
+    mixed = _solve(sws, "mixed", err_max=1e-12, iter_max=4000)
+    for case, (phi64, s64, _), (phim, sm, done) in zip(CASES, si, mixed):
+        assert done
+        assert rel_l1(phim, phi64) <= 1e-8, (case, rel_l1(phim, phi64))
+        assert sm["sweeps_fp32"] > sm["sweeps_fp64"] and sm["refinements"] >= 1
+
+
+@pytest.mark.parametrize("method", ["si", "mixed"])
+def test_batch_member_bit_identical_alone_and_in_mix(built, workdir, method):
+    probs = [_problem(workdir, c, 80 + k) for k, c in enumerate(CASES)]
+    sws = [p[0] for p in probs]
+    alone = [_solve([sw], method, err_max=1e-10)[0] for sw in sws]
+    mixed = _solve(sws, method, err_max=1e-10)
+    for case, (pa, sa, _), (pm, smx, _) in zip(CASES, alone, mixed):
+        assert bits_equal(pa, pm), case
+        assert sa == smx, case
+    # and again in another order, with a repeated solve of the same members
+    rev = _solve(sws[::-1], method, err_max=1e-10)[::-1]
+    for case, (pa, _, _), (pr, _, _) in zip(CASES, alone, rev):
+        assert bits_equal(pa, pr), case
+
+
+def test_batch_psi_is_the_last_fp64_sweep(built, workdir):
+    """After a batched solve the member's resident psi is its last FP64
+    sweep, consistent with the returned phi for source iteration."""
+    import tycho2_b200 as ty
+    sw, om, (st, ss, mat, q) = _problem(workdir, CASES[1], 99)
+    (phi, stats, done), = _solve([sw], "si", err_max=1e-10)
+    path = str(workdir / "batch.psi")
+    sw.writePsiToFile(path)
+    raw = np.fromfile(path, np.float64)
+    psi = raw[raw.size - np.prod(sw.psi_shape):].reshape(sw.psi_shape)
+    w = ty.Quadrature(CASES[1][2]).wt
+    phi_from_psi = np.einsum("cavg,a->cvg", psi, w)
+    assert rel_l1(phi_from_psi, phi) <= 1e-13
+
+
+def test_batch_errors(built, workdir):
+    import tycho2_b200 as ty
+    sw, _, _ = _problem(workdir, CASES[0], 7)
+    b = ty.BatchSolver()
+    b.add(sw, "si")
+    with pytest.raises(ty.TychoError):
+        b.add(sw, "si")  # already a member
+    with pytest.raises(ty.TychoError):
+        b.remove(12345)
+    mesh, _ = kuhn(workdir, 2, 0.0, seed=3)
+    plain = ty.SweeperCuda(mesh, 4, 1)  # no FP32 sweep
+    plain.set_cross_sections(np.ones(mesh.n_cells), np.zeros(mesh.n_cells))
+    with pytest.raises(ty.TychoError):
+        b.add(plain, "mixed")
+    b.close()

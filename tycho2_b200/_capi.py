@@ -42,6 +42,11 @@ class LaunchShape(C.Structure):
     _fields_ = [("schedule", C.c_int), ("variant", C.c_int), ("knob", C.c_int), ("vector", C.c_int)]
 
 
+class BatchOpts(C.Structure):
+    _fields_ = [("method", C.c_int), ("iter_max", C.c_int), ("err_max", C.c_double),
+                ("inner_tol", C.c_double), ("inner_max", C.c_int), ("refine_max", C.c_int)]
+
+
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("sweeps_fp64", C.c_int), ("sweeps_fp32", C.c_int),
                 ("refinements", C.c_int), ("final_error", C.c_double), ("seconds", C.c_double)]
@@ -77,6 +82,14 @@ SIGNATURES = {
     "tycho_sweeper_configure": (C.c_int, [_P, C.c_int, C.POINTER(LaunchShape)]),
     "tycho_sweeper_get_shape": (C.c_int, [_P, C.c_int, C.POINTER(LaunchShape)]),
     "tycho_sweeper_sweep_noalloc": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "tycho_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, _PP]),
+    "tycho_batch_destroy": (None, [_P]),
+    "tycho_batch_add": (C.c_int, [_P, _P, C.POINTER(BatchOpts), C.POINTER(C.c_int)]),
+    "tycho_batch_remove": (C.c_int, [_P, C.c_int]),
+    "tycho_batch_step": (C.c_int, [_P, C.POINTER(C.c_int)]),
+    "tycho_batch_run": (C.c_int, [_P]),
+    "tycho_batch_result": (C.c_int, [_P, C.c_int, _P, C.POINTER(SolveStats), C.POINTER(C.c_int)]),
+    "tycho_batch_timing": (C.c_int, [_P, _P, _P, _P]),
 }
 
 _lib = None

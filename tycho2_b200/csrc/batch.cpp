@@ -1,0 +1,405 @@
+// Batched solves: host side (member state machines, slot tables, pass graphs).
+#include "batch.hpp"
+
+#include <algorithm>
+#include <cmath>
+
+#include "status.hpp"
+
+namespace tycho {
+
+#define TB_CUDA(expr)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (expr);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            err = std::string(#expr) + ": " + cudaGetErrorString(e_);                  \
+            return e_ == cudaErrorMemoryAllocation ? kErrOom : kErrCuda;               \
+        }                                                                              \
+    } while (0)
+
+#define TB_CHECK(expr)            \
+    do {                          \
+        int s_ = (expr);          \
+        if (s_ != kOk) return s_; \
+    } while (0)
+
+namespace {
+
+constexpr unsigned kStreamGrid = 148 * 8;     // blocks of the grid-stride streaming kernels
+constexpr unsigned kLevelGridCap = 148 * 16;  // level kernels loop beyond this
+
+uint32_t magic(uint32_t d) { return d == 1 ? 0u : (uint32_t)(((1ull << 32) + d - 1) / d); }
+
+template <typename T>
+void free_dev(T *&p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+}  // namespace
+
+Batch::~Batch()
+{
+    cudaSetDevice(device_);
+    for (auto &g : graph_)
+        if (g) cudaGraphExecDestroy(g);
+    for (auto &m : members_) {
+        free_dev(m.r);
+        free_dev(m.d);
+        free_dev(m.k);
+    }
+    for (int p = 0; p < 2; ++p) {
+        free_dev(d_slots_[p]);
+        if (h_slots_[p]) cudaFreeHost(h_slots_[p]);
+    }
+    if (h_norms_) cudaFreeHost(h_norms_);
+    free_dev(plan_.segs);
+    free_dev(plan_.level_nseg);
+    free_dev(plan_.level_nchunk);
+    free_dev(plan_.act);
+    free_dev(plan_.chunk_prefix);
+    free_dev(plan_.n_act);
+    free_dev(plan_.partials);
+    free_dev(plan_.norms);
+    for (auto &e : ev_)
+        if (e) cudaEventDestroy(e);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Batch::init(int device, int ipw32, int ipw64, std::string &err)
+{
+    for (int ipw : {ipw32, ipw64})
+        if (ipw != 8 && ipw != 16 && ipw != 32) { err = "items per warp must be 8, 16 or 32"; return kErrArg; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        err = "no CUDA device: the batched sweep has no CPU fallback";
+        return kErrCuda;
+    }
+    if (device < 0 || device >= ndev) { err = "bad device ordinal"; return kErrArg; }
+    device_ = device;
+    ipw_[0] = ipw64;
+    ipw_[1] = ipw32;
+    TB_CUDA(cudaSetDevice(device_));
+    TB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    for (auto &e : ev_) TB_CUDA(cudaEventCreate(&e));
+    return kOk;
+}
+
+void Batch::invalidate()
+{
+    for (auto &g : graph_)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+int Batch::add(Sweeper *sw, const BatchOptions &o, int &id, std::string &err)
+{
+    if (!sw) { err = "null sweeper"; return kErrArg; }
+    if (sw->device() != device_) { err = "sweeper lives on another device than the batch"; return kErrArg; }
+    if (o.method != 0 && o.method != 2) { err = "batch method must be 0 (source iteration) or 2 (mixed)"; return kErrArg; }
+    if (o.iter_max < 1 || o.err_max < 0 || o.inner_tol <= 0 || o.inner_max < 1 || o.refine_max < 0) {
+        err = "bad batch solve options";
+        return kErrArg;
+    }
+    for (const auto &m : members_)
+        if (m.sw == sw) { err = "sweeper is already in the batch"; return kErrArg; }
+    TB_CUDA(cudaSetDevice(device_));
+    Member m;
+    m.sw = sw;
+    m.o = o;
+    TB_CHECK(sw->device_view(0, m.v[0], err));
+    if (o.method == 2) {
+        TB_CHECK(sw->device_view(1, m.v[1], err));
+        const size_t n = sw->phi_size();
+        TB_CUDA(cudaMalloc(&m.r, sizeof(double) * n));
+        TB_CUDA(cudaMalloc(&m.d, sizeof(double) * n));
+        TB_CUDA(cudaMalloc(&m.k, sizeof(double) * n));
+        m.state = kRunOuter;
+    } else {
+        m.v[1] = m.v[0];
+        m.state = kRunSI;
+    }
+    m.cur = m.v[0].phi;
+    m.nxt = m.v[0].tmp;
+    TB_CUDA(cudaMemsetAsync(m.v[0].phi, 0, sizeof(double) * sw->phi_size(), stream_));
+    m.updates = sw->n_cells() * (uint64_t)sw->n_angles() * (uint64_t)sw->n_groups();
+    m.id = next_id_++;
+    id = m.id;
+    members_.push_back(m);
+    invalidate();
+    return kOk;
+}
+
+int Batch::remove(int id, std::string &err)
+{
+    for (size_t i = 0; i < members_.size(); ++i)
+        if (members_[i].id == id) {
+            TB_CUDA(cudaSetDevice(device_));
+            TB_CUDA(cudaStreamSynchronize(stream_));
+            free_dev(members_[i].r);
+            free_dev(members_[i].d);
+            free_dev(members_[i].k);
+            members_.erase(members_.begin() + (long)i);
+            invalidate();
+            return kOk;
+        }
+    err = "no batch member with that id";
+    return kErrArg;
+}
+
+int Batch::ensure_capacity(std::string &err)
+{
+    const size_t n = members_.size();
+    uint32_t lv = 0;
+    size_t chunks = 0;
+    for (const auto &m : members_) {
+        lv = std::max(lv, m.v[0].n_levels);
+        chunks += (m.sw->phi_size() + kBatchChunk - 1) / kBatchChunk;
+    }
+    max_levels_ = lv;
+    if (n > cap_slots_ || lv > cap_levels_) {
+        const size_t cs = std::max(n, cap_slots_ * 2 > 16 ? cap_slots_ * 2 : (size_t)16);
+        const size_t cl = std::max((size_t)lv, cap_levels_);
+        for (int p = 0; p < 2; ++p) {
+            free_dev(d_slots_[p]);
+            if (h_slots_[p]) cudaFreeHost(h_slots_[p]);
+            h_slots_[p] = nullptr;
+            TB_CUDA(cudaMalloc(&d_slots_[p], sizeof(BatchSlot) * cs));
+            TB_CUDA(cudaMallocHost(&h_slots_[p], sizeof(BatchSlot) * cs));
+        }
+        if (h_norms_) cudaFreeHost(h_norms_);
+        h_norms_ = nullptr;
+        TB_CUDA(cudaMallocHost(&h_norms_, sizeof(double) * 2 * cs));
+        free_dev(plan_.segs);
+        free_dev(plan_.level_nseg);
+        free_dev(plan_.level_nchunk);
+        free_dev(plan_.act);
+        free_dev(plan_.chunk_prefix);
+        free_dev(plan_.n_act);
+        free_dev(plan_.norms);
+        const size_t lc = std::max<size_t>(cl, 1) * kBatchClasses;
+        TB_CUDA(cudaMalloc(&plan_.segs, sizeof(BatchSeg) * cs * lc));
+        TB_CUDA(cudaMalloc(&plan_.level_nseg, sizeof(uint32_t) * lc));
+        TB_CUDA(cudaMalloc(&plan_.level_nchunk, sizeof(uint32_t) * lc));
+        TB_CUDA(cudaMalloc(&plan_.act, sizeof(uint32_t) * cs));
+        TB_CUDA(cudaMalloc(&plan_.chunk_prefix, sizeof(uint32_t) * (cs + 1)));
+        TB_CUDA(cudaMalloc(&plan_.n_act, sizeof(uint32_t)));
+        TB_CUDA(cudaMalloc(&plan_.norms, sizeof(double) * 2 * cs));
+        TB_CUDA(cudaMemsetAsync(plan_.norms, 0, sizeof(double) * 2 * cs, stream_));
+        plan_.seg_stride = (uint32_t)cs;
+        cap_slots_ = cs;
+        cap_levels_ = cl;
+        invalidate();  // the graphs hold the old buffers
+    }
+    if (chunks > cap_chunks_) {
+        free_dev(plan_.partials);
+        const size_t cc = std::max(chunks, cap_chunks_ * 2);
+        TB_CUDA(cudaMalloc(&plan_.partials, sizeof(double) * 2 * cc));
+        cap_chunks_ = cc;
+        invalidate();
+    }
+    return kOk;
+}
+
+void Batch::fill_slot(int prec, const Member &m, BatchSlot &s) const
+{
+    const Sweeper::DeviceView &v = m.v[prec];
+    s = BatchSlot();
+    s.rec = v.rec;
+    s.psi = v.psi;
+    s.iso = m.v[0].iso;
+    s.iso32 = prec ? v.iso32 : nullptr;
+    s.sigma_s = v.sigs;
+    s.scat = v.scat;
+    s.w = v.w;
+    s.level_off = v.level_off;
+    s.nc = m.sw->n_cells();
+    s.A = (uint32_t)m.sw->n_angles();
+    s.G = (uint32_t)m.sw->n_groups();
+    s.vg = v.vg;
+    s.vmagic = magic(s.G / s.vg);
+    s.n_levels = v.n_levels;
+    s.active = 0;
+    if (prec == 0 && m.state == kRunSI) {
+        s.active = 1;
+        s.op = kOpSI;
+        s.phi_in = m.cur;
+        s.q_fixed = v.qiso;
+        s.phi_out = m.nxt;
+    } else if (prec == 0 && m.state == kRunOuter) {
+        s.active = 1;
+        s.op = kOpOuter;
+        s.phi = v.phi;
+        s.phi_in = v.phi;
+        s.q_fixed = v.qiso;
+        s.phi_out = v.tmp;
+        s.vec_r = m.r;
+        s.vec_d = m.d;
+        s.accept = m.accept ? 1u : 0u;
+    } else if (prec == 1 && m.state == kRunInner) {
+        s.active = 1;
+        s.op = kOpInner;
+        s.phi_in = m.d;
+        s.q_fixed = nullptr;
+        s.phi_out = m.k;
+        s.vec_r = m.r;
+        s.vec_d = m.d;
+    }
+}
+
+int Batch::build_graph(int prec, std::string &err)
+{
+    const int ipw = ipw_[prec];
+    const uint32_t n = (uint32_t)members_.size();
+    // Blocks per level and class: enough for every member's chunks at once
+    // (fewer when some are idle; the kernel's warps then exit at once).
+    std::vector<BatchCuts> cuts(max_levels_);
+    for (uint32_t L = 0; L < max_levels_; ++L) {
+        uint64_t chunks[kBatchClasses] = {0, 0, 0};
+        for (const auto &m : members_) {
+            const auto &lo = m.sw->schedule().level_offset;
+            if (L < m.v[0].n_levels) chunks[m.v[prec].vg == 4 ? 2 : m.v[prec].vg == 2 ? 1 : 0] += (lo[L + 1] - lo[L]) / ipw;
+        }
+        cuts[L].c[0] = 0;
+        for (uint32_t c = 0; c < kBatchClasses; ++c)
+            cuts[L].c[c + 1] = cuts[L].c[c] + (unsigned)std::min<uint64_t>((chunks[c] + 3) / 4, kLevelGridCap);
+    }
+    cudaGraph_t g;
+    TB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = launch_batch_plan(ipw, d_slots_[prec], n, max_levels_, plan_, stream_);
+    if (e == cudaSuccess && prec == 0) e = launch_batch_accept(d_slots_[prec], plan_, kStreamGrid, stream_);
+    if (e == cudaSuccess) e = launch_batch_scatter(d_slots_[prec], plan_, kStreamGrid, stream_);
+    for (uint32_t L = 0; L < max_levels_ && e == cudaSuccess; ++L)
+        e = prec ? launch_batch_level<float>(ipw, d_slots_[prec], plan_, L, cuts[L], stream_)
+                 : launch_batch_level<double>(ipw, d_slots_[prec], plan_, L, cuts[L], stream_);
+    if (e == cudaSuccess) e = launch_batch_psi_to_phi(prec == 1, d_slots_[prec], plan_, kStreamGrid, stream_);
+    if (e == cudaSuccess) e = launch_batch_post(d_slots_[prec], plan_, kStreamGrid, stream_);
+    if (e == cudaSuccess) e = launch_batch_finish(d_slots_[prec], plan_, 64, stream_);
+    cudaError_t ce = cudaStreamEndCapture(stream_, &g);
+    TB_CUDA(e);
+    TB_CUDA(ce);
+    cudaError_t ie = cudaGraphInstantiate(&graph_[prec], g, 0);
+    cudaGraphDestroy(g);
+    TB_CUDA(ie);
+    return kOk;
+}
+
+int Batch::pass(int prec, std::string &err)
+{
+    const size_t n = members_.size();
+    bool any = false;
+    for (size_t j = 0; j < n; ++j) {
+        fill_slot(prec, members_[j], h_slots_[prec][j]);
+        any = any || h_slots_[prec][j].active;
+    }
+    if (!any) return kOk;
+    if (!graph_[prec]) TB_CHECK(build_graph(prec, err));
+    TB_CUDA(cudaMemcpyAsync(d_slots_[prec], h_slots_[prec], sizeof(BatchSlot) * n, cudaMemcpyHostToDevice, stream_));
+    TB_CUDA(cudaEventRecord(ev_[2 * prec], stream_));
+    TB_CUDA(cudaGraphLaunch(graph_[prec], stream_));
+    TB_CUDA(cudaEventRecord(ev_[2 * prec + 1], stream_));
+    passes_[prec]++;
+    for (size_t j = 0; j < n; ++j)
+        if (h_slots_[prec][j].active) updates_[prec] += (double)members_[j].updates;
+    return kOk;
+}
+
+int Batch::step(int &n_running, std::string &err)
+{
+    n_running = 0;
+    for (const auto &m : members_) n_running += m.state != kDone;
+    if (n_running == 0) return kOk;
+    TB_CUDA(cudaSetDevice(device_));
+    TB_CHECK(ensure_capacity(err));
+    const int before[2] = {passes_[0], passes_[1]};
+    TB_CHECK(pass(0, err));
+    TB_CHECK(pass(1, err));
+    const size_t n = members_.size();
+    TB_CUDA(cudaMemcpyAsync(h_norms_, plan_.norms, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    for (int p = 0; p < 2; ++p)
+        if (passes_[p] > before[p]) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev_[2 * p], ev_[2 * p + 1]);
+            ms_[p] += ms;
+        }
+    n_running = 0;
+    for (size_t j = 0; j < n; ++j) {
+        Member &m = members_[j];
+        if (m.state == kDone) continue;
+        const double d = h_norms_[2 * j], mm = h_norms_[2 * j + 1];
+        const double e = mm > 0 ? d / mm : 0.0;
+        m.st.steps++;
+        if (m.state == kRunSI) {
+            std::swap(m.cur, m.nxt);
+            m.st.sweeps_fp64++;
+            m.st.iterations++;
+            m.st.final_error = e;
+            if (e <= m.o.err_max || m.st.iterations >= m.o.iter_max) m.state = kDone;
+        } else if (m.state == kRunOuter) {
+            m.accept = false;
+            m.st.sweeps_fp64++;
+            m.st.final_error = e;
+            if (e <= m.o.err_max || m.st.refinements >= m.o.refine_max || m.st.iterations >= m.o.iter_max) {
+                m.state = kDone;
+            } else {
+                m.state = kRunInner;
+                m.inner_its = 0;
+            }
+        } else {
+            m.st.sweeps_fp32++;
+            m.st.iterations++;
+            m.inner_its++;
+            if (e <= m.o.inner_tol || m.inner_its >= m.o.inner_max || m.st.iterations >= m.o.iter_max) {
+                m.state = kRunOuter;
+                m.accept = true;
+                m.st.refinements++;
+            }
+        }
+        if (m.state == kDone) {
+            m.st.done = 1;
+            m.sw->note_psi_precision(0);
+        } else {
+            ++n_running;
+        }
+    }
+    return kOk;
+}
+
+int Batch::run(std::string &err)
+{
+    int running = 1;
+    while (running > 0) TB_CHECK(step(running, err));
+    return kOk;
+}
+
+int Batch::result(int id, double *phi_host, BatchMemberStats &st, std::string &err)
+{
+    for (const auto &m : members_)
+        if (m.id == id) {
+            st = m.st;
+            if (phi_host) {
+                const double *src = m.o.method == 0 ? m.cur : m.v[0].tmp;
+                TB_CUDA(cudaSetDevice(device_));
+                TB_CUDA(cudaMemcpyAsync(phi_host, src, sizeof(double) * m.sw->phi_size(), cudaMemcpyDeviceToHost,
+                                        stream_));
+                TB_CUDA(cudaStreamSynchronize(stream_));
+            }
+            return kOk;
+        }
+    err = "no batch member with that id";
+    return kErrArg;
+}
+
+void Batch::timing(double ms[2], int passes[2]) const
+{
+    ms[0] = ms_[0];
+    ms[1] = ms_[1];
+    passes[0] = passes_[0];
+    passes[1] = passes_[1];
+}
+
+}  // namespace tycho

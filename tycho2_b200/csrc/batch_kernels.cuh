@@ -1,0 +1,199 @@
+// Batched sweep of many independent instances (uneven mesh size, group
+// count and SN order) in one set of launches.  There is no counterpart in
+// the reference, which sweeps one problem per process.
+//
+// Each pass (one operator application of every active member, in one
+// precision) is one CUDA graph:
+//   plan        device work list over (member, wavefront level): per level,
+//               the active members' record ranges as segments with chunk
+//               prefixes; per member, its phi chunks
+//   accept      phi += delta for members that finished an inner solve
+//   scatter     iso = [Q] + M S phi_in                   (per phi element)
+//   level L     one launch per global level L = 0..max levels - 1: every
+//               warp takes IPW-item chunks of the level's work list, finds
+//               its member by binary search over the segments, and runs the
+//               record kernel's per-(item, group) arithmetic for that member
+//   psi->phi    phi_out = sum_a w_a psi
+//   post        per member operation (SI change, residual, inner update)
+//               with per-chunk partial L1 sums
+//   finish      per member: its partials in chunk order -> two norms
+// Chunks are member-local (kChunk phi elements of one member), so every
+// member's arithmetic and reductions are the same alone and in any mix.
+#pragma once
+
+#include "batch_types.hpp"
+#include "sweep_records.cuh"
+#include "stream_ops.cuh"
+
+namespace tycho {
+
+constexpr int kBatchPlanThreads = 256;
+
+__host__ __device__ __forceinline__ uint32_t batch_class(uint32_t vg) { return vg == 4 ? 2u : vg == 2 ? 1u : 0u; }
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *total)
+{
+    __shared__ uint32_t warp_tot[kBatchPlanThreads / 32];
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    uint32_t base = 0, all = 0;
+    for (uint32_t k = 0; k < kBatchPlanThreads / 32; ++k) {
+        if (k < w) base += warp_tot[k];
+        all += warp_tot[k];
+    }
+    __syncthreads();
+    *total = all;
+    return base + x - v;
+}
+
+// Grid: max levels + 1 blocks of kBatchPlanThreads.  Block L < max levels
+// builds level L's segments, one list per vector-width class (members of a
+// class run the same kernel body); the last block lists the active members
+// and their phi chunk prefix.
+template <int IPW>
+__global__ void __launch_bounds__(kBatchPlanThreads)
+batch_plan_kernel(const BatchSlot *__restrict__ slots, uint32_t n_slots, uint32_t max_levels, BatchPlan pl)
+{
+    const uint32_t L = blockIdx.x;
+    if (L < max_levels) {
+        for (uint32_t cls = 0; cls < kBatchClasses; ++cls) {
+            uint32_t chunk_run = 0, seg_run = 0;
+            BatchSeg *segs = pl.segs + ((size_t)L * kBatchClasses + cls) * pl.seg_stride;
+            for (uint32_t base = 0; base < n_slots; base += kBatchPlanThreads) {
+                const uint32_t j = base + threadIdx.x;
+                uint32_t nch = 0;
+                uint64_t lo = 0;
+                if (j < n_slots && slots[j].active && L < slots[j].n_levels && batch_class(slots[j].vg) == cls) {
+                    lo = slots[j].level_off[L];
+                    nch = (uint32_t)((slots[j].level_off[L + 1] - lo) / IPW);
+                }
+                uint32_t tot_c, tot_s;
+                const uint32_t ex_c = block_exclusive_scan(nch, &tot_c);
+                const uint32_t ex_s = block_exclusive_scan(nch ? 1u : 0u, &tot_s);
+                if (nch) {
+                    BatchSeg sg;
+                    sg.item_begin = lo;
+                    sg.slot = j;
+                    sg.chunk_begin = chunk_run + ex_c;
+                    segs[seg_run + ex_s] = sg;
+                }
+                chunk_run += tot_c;
+                seg_run += tot_s;
+            }
+            if (threadIdx.x == 0) {
+                pl.level_nchunk[L * kBatchClasses + cls] = chunk_run;
+                pl.level_nseg[L * kBatchClasses + cls] = seg_run;
+            }
+        }
+        return;
+    }
+    uint32_t chunk_run = 0, act_run = 0;
+    for (uint32_t base = 0; base < n_slots; base += kBatchPlanThreads) {
+        const uint32_t j = base + threadIdx.x;
+        uint32_t nch = 0, on = 0;
+        if (j < n_slots && slots[j].active) {
+            on = 1;
+            const uint64_t n = slots[j].nc * 4 * slots[j].G;
+            nch = (uint32_t)((n + kBatchChunk - 1) / kBatchChunk);
+        }
+        uint32_t tot_c, tot_a;
+        const uint32_t ex_c = block_exclusive_scan(nch, &tot_c);
+        const uint32_t ex_a = block_exclusive_scan(on, &tot_a);
+        if (on) {
+            pl.act[act_run + ex_a] = j;
+            pl.chunk_prefix[act_run + ex_a] = chunk_run + ex_c;
+        }
+        chunk_run += tot_c;
+        act_run += tot_a;
+    }
+    if (threadIdx.x == 0) {
+        pl.chunk_prefix[act_run] = chunk_run;
+        *pl.n_act = act_run;
+    }
+}
+
+// Largest k in [0, n) with key(k) <= x (key(0) <= x is given).
+template <typename KeyFn>
+__device__ __forceinline__ uint32_t upper_index(uint32_t n, uint32_t x, KeyFn key)
+{
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (key(mid) <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <typename Real>
+__device__ __forceinline__ LevelArgs slot_args(const BatchSlot &s)
+{
+    LevelArgs p = {};
+    p.iso = s.iso32 ? (const void *)s.iso32 : (const void *)s.iso;
+    p.qang = nullptr;
+    p.psi = s.psi;
+    p.G = s.G;
+    p.vg = s.vg;
+    p.vmagic = s.vmagic;
+    return p;
+}
+
+// The chunks of one class at one level, taken by this block's warps with a
+// stride of the class's block count.  The first chunk's records are staged
+// before waiting on the previous level (programmatic dependent launch).
+template <typename Real, int IPW, int VG>
+__device__ __forceinline__ void batch_class_body(const BatchSlot *__restrict__ slots, const BatchPlan &pl,
+                                                 uint32_t L, uint32_t cls, uint32_t blk, uint32_t nblk,
+                                                 RecordTile<Real, IPW> &T, bool &waited)
+{
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    const uint32_t nchunk = pl.level_nchunk[L * kBatchClasses + cls];
+    const uint32_t nseg = pl.level_nseg[L * kBatchClasses + cls];
+    const BatchSeg *__restrict__ segs = pl.segs + ((size_t)L * kBatchClasses + cls) * pl.seg_stride;
+    for (uint32_t ch = blk * 4u + w; ch < nchunk; ch += nblk * 4u) {
+        const uint32_t k = upper_index(nseg, ch, [&](uint32_t m) { return segs[m].chunk_begin; });
+        const BatchSeg sg = segs[k];
+        const BatchSlot &s = slots[sg.slot];
+        const ItemRecord<Real> *rec = (const ItemRecord<Real> *)s.rec;
+        tile_fill<Real, IPW>(T, rec + sg.item_begin + (uint64_t)(ch - sg.chunk_begin) * IPW + lane, lane, true);
+        if (!waited) {
+            pdl_wait_prerequisites();
+            waited = true;
+        }
+        __syncwarp();
+        record_pairs<Real, IPW, VG, false>(slot_args<Real>(s), T, lane);
+        __syncwarp();
+    }
+}
+
+// One global level of the batched sweep, 4 warps per block, IPW items per
+// chunk.  Blocks [cut[c], cut[c+1]) serve vector-width class c (1, 2, 4
+// groups per access), so each block runs one kernel body.  The work list was
+// built by the plan kernel, which completed before the first level started.
+template <typename Real, int IPW>
+__global__ void __launch_bounds__(128)
+batch_level_kernel(const BatchSlot *__restrict__ slots, BatchPlan pl, uint32_t L, BatchCuts cut)
+{
+    __shared__ RecordTile<Real, IPW> tiles[4];
+    pdl_launch_dependents();
+    RecordTile<Real, IPW> &T = tiles[threadIdx.x >> 5];
+    bool waited = false;
+    const uint32_t b = blockIdx.x;
+    if (b < cut.c[1]) {
+        batch_class_body<Real, IPW, 1>(slots, pl, L, 0, b, cut.c[1], T, waited);
+    } else if (b < cut.c[2]) {
+        batch_class_body<Real, IPW, 2>(slots, pl, L, 1, b - cut.c[1], cut.c[2] - cut.c[1], T, waited);
+    } else if constexpr (sizeof(Real) == 4) {
+        batch_class_body<Real, IPW, 4>(slots, pl, L, 2, b - cut.c[2], cut.c[3] - cut.c[2], T, waited);
+    }
+    if (!waited) pdl_wait_prerequisites();
+}
+
+}  // namespace tycho

@@ -9,6 +9,7 @@
 #include "mesh.hpp"
 #include "schedule.hpp"
 #include "status.hpp"
+#include "batch.hpp"
 #include "sweeper.hpp"
 
 struct tycho_mesh {
@@ -18,6 +19,10 @@ struct tycho_mesh {
 
 struct tycho_sweeper {
     tycho::Sweeper sw;
+};
+
+struct tycho_batch {
+    tycho::Batch b;
 };
 
 namespace tycho {
@@ -412,6 +417,97 @@ int tycho_sweeper_time_sweeps(tycho_sweeper *h, int precision, int n, int flush_
     if (!h || !ms) return finish(TYCHO_ERR_ARG, "null argument");
     std::string err;
     return guarded([&] { return finish(h->sw.time_sweeps(precision, n, flush_l2 != 0, ms, err), err); });
+}
+
+int tycho_batch_create(int device, int ipw32, int ipw64, tycho_batch **out)
+{
+    if (!out) return finish(TYCHO_ERR_ARG, "null output");
+    *out = nullptr;
+    std::string err;
+    return guarded([&] {
+        auto *b = new tycho_batch();
+        int s = b->b.init(device, ipw32, ipw64, err);
+        if (s != tycho::kOk) {
+            delete b;
+            return finish(s, err);
+        }
+        *out = b;
+        return (int)TYCHO_OK;
+    });
+}
+
+void tycho_batch_destroy(tycho_batch *b) { delete b; }
+
+int tycho_batch_add(tycho_batch *b, tycho_sweeper *sw, const tycho_batch_opts *o, int *id)
+{
+    if (!b || !sw || !o || !id) return finish(TYCHO_ERR_ARG, "null argument");
+    tycho::BatchOptions bo;
+    bo.method = o->method;
+    bo.iter_max = o->iter_max;
+    bo.err_max = o->err_max;
+    bo.inner_tol = o->inner_tol;
+    bo.inner_max = o->inner_max;
+    bo.refine_max = o->refine_max;
+    std::string err;
+    return guarded([&] { return finish(b->b.add(&sw->sw, bo, *id, err), err); });
+}
+
+int tycho_batch_remove(tycho_batch *b, int id)
+{
+    if (!b) return finish(TYCHO_ERR_ARG, "null batch");
+    std::string err;
+    return guarded([&] { return finish(b->b.remove(id, err), err); });
+}
+
+int tycho_batch_step(tycho_batch *b, int *n_running)
+{
+    if (!b || !n_running) return finish(TYCHO_ERR_ARG, "null argument");
+    std::string err;
+    return guarded([&] { return finish(b->b.step(*n_running, err), err); });
+}
+
+int tycho_batch_run(tycho_batch *b)
+{
+    if (!b) return finish(TYCHO_ERR_ARG, "null batch");
+    std::string err;
+    return guarded([&] { return finish(b->b.run(err), err); });
+}
+
+int tycho_batch_result(tycho_batch *b, int id, double *phi, tycho_solve_stats *stats, int *done)
+{
+    if (!b) return finish(TYCHO_ERR_ARG, "null batch");
+    std::string err;
+    return guarded([&] {
+        tycho::BatchMemberStats st;
+        int s = b->b.result(id, phi, st, err);
+        if (s == tycho::kOk) {
+            if (stats) {
+                stats->iterations = st.iterations;
+                stats->sweeps_fp64 = st.sweeps_fp64;
+                stats->sweeps_fp32 = st.sweeps_fp32;
+                stats->refinements = st.refinements;
+                stats->final_error = st.final_error;
+                stats->seconds = 0.0;
+            }
+            if (done) *done = st.done;
+        }
+        return finish(s, err);
+    });
+}
+
+int tycho_batch_timing(const tycho_batch *b, double *ms, int *passes, double *updates)
+{
+    if (!b) return finish(TYCHO_ERR_ARG, "null batch");
+    double m[2], u[2];
+    int p[2];
+    b->b.timing(m, p);
+    b->b.updates(u);
+    for (int i = 0; i < 2; ++i) {
+        if (ms) ms[i] = m[i];
+        if (passes) passes[i] = p[i];
+        if (updates) updates[i] = u[i];
+    }
+    return TYCHO_OK;
 }
 
 }  // extern "C"

@@ -6,6 +6,7 @@
 #include "sweep_kernels.cuh"
 #include "sweep_tiles.cuh"
 #include "sweep_records.cuh"
+#include "stream_ops.cuh"
 
 namespace tycho {
 
@@ -25,8 +26,6 @@ template cudaError_t launch_persist_record<double>(int, const LevelArgs &, const
 template cudaError_t record_persist_blocks_per_sm<double>(int, int, int *);
 
 namespace {
-
-constexpr double kFourPi = 4.0 * 3.14159265358979323846;
 
 __global__ void item_abar_kernel(const uint32_t *__restrict__ items, uint64_t n, uint32_t A,
                                  const double *__restrict__ normal, const double *__restrict__ area,
@@ -59,14 +58,8 @@ __global__ void psi_to_phi_kernel(const Real *__restrict__ psi, const double *__
                                   double *__restrict__ phi, uint64_t nc, uint32_t A, uint32_t G)
 {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t row = (uint64_t)4 * G;
-    if (i >= nc * row) return;
-    const uint64_t c = i / row;
-    const uint64_t vg = i - c * row;
-    const Real *p = psi + c * A * row + vg;
-    double s = 0.0;
-    for (uint32_t a = 0; a < A; ++a) s += (double)p[(size_t)a * row] * w[a];
-    phi[i] = s;
+    if (i >= nc * 4 * G) return;
+    phi[i] = psi_to_phi_elem(psi, w, i, A, G);
 }
 
 __global__ void scatter_source_kernel(const double *__restrict__ phi, const double *__restrict__ q,
@@ -75,36 +68,10 @@ __global__ void scatter_source_kernel(const double *__restrict__ phi, const doub
                                       float *__restrict__ iso32, uint64_t nc, uint32_t G)
 {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t row = (uint64_t)4 * G;
-    if (i >= nc * row) return;
-    const uint64_t c = i / row;
-    double s;
-    if (phi) {
-        if (!scat) {
-            s = sigma_s[c] / kFourPi * phi[i];  // Util.cc:126-128
-        } else {
-            const uint32_t g = (uint32_t)(i % G);
-            const double *pv = phi + (i - g);
-            s = 0.0;
-            for (uint32_t gp = 0; gp < G; ++gp) {
-                const double k = scat[g * G + gp];
-                if (k == 0.0) continue;
-                s += sigma_s[c] * k / kFourPi * pv[gp];
-            }
-        }
-        if (q) s = q[i] + s;
-    } else {
-        s = q ? q[i] : 0.0;
-    }
+    if (i >= nc * 4 * G) return;
+    const double s = scatter_elem(phi, q, sigma_s, scat, i, G);
     iso[i] = s;
     if (iso32) iso32[i] = (float)s;
-}
-
-__device__ __forceinline__ double warp_sum(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
 }
 
 template <int K>

@@ -301,6 +301,29 @@ LevelArgs Sweeper::level_args(int prec, const void *iso, const double *qang, voi
     return p;
 }
 
+int Sweeper::device_view(int prec, DeviceView &v, std::string &err)
+{
+    if (prec == 1 && !fp32_) { err = "sweeper was created without the FP32 sweep"; return kErrArg; }
+    if (!have_xs_) { err = "cross sections not set"; return kErrMissing; }
+    TY_CUDA(cudaSetDevice(device_));
+    TY_CHECK(ensure_records(prec, true, err));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    v.rec = d_rec_[prec ? 1 : 0];
+    v.psi = d_psi_;
+    v.iso = d_iso_;
+    v.iso32 = d_iso32_;
+    v.qiso = d_qiso_;
+    v.sigs = d_sigs_;
+    v.scat = d_scat_;
+    v.w = d_w_;
+    v.phi = d_phi_;
+    v.tmp = d_tmp_;
+    v.level_off = d_level_off_;
+    v.n_levels = sched_.n_levels;
+    v.vg = record_vg(prec != 0, (uint32_t)G_);
+    return kOk;
+}
+
 // Allocates (once) and fills (once per cross-section set) the per-item
 // records of the record variant for one precision.
 int Sweeper::ensure_records(int prec, bool need_filled, std::string &err)

@@ -85,6 +85,23 @@ public:
     int sweep_external(int prec, const void *iso, void *psi, uint32_t *done, uint32_t *ctl,
                        cudaStream_t s, std::string &err);
 
+    // Device state read by the batch driver (batch.cpp); computes the
+    // records of `prec` when stale and waits for the instance's stream.
+    struct DeviceView {
+        const void *rec;
+        void *psi;
+        double *iso;
+        float *iso32;
+        const double *qiso, *sigs, *scat, *w;
+        double *phi, *tmp;
+        const uint64_t *level_off;
+        uint32_t n_levels, vg;
+    };
+    int device_view(int prec, DeviceView &v, std::string &err);
+    // The resident psi was written by a sweep of this precision elsewhere.
+    void note_psi_precision(int prec) { last_psi_prec_ = prec; }
+    uint64_t n_items() const { return sched_.items.size(); }
+
     const MeshTables &tables() const { return tables_; }
     const Quadrature &quadrature() const { return quad_; }
     const Schedule &schedule() const { return sched_; }

@@ -257,3 +257,66 @@ class SweeperCuda:
 
     def __del__(self):
         self.close()
+
+
+class BatchSolver:
+    """Many independent sweepers solved together on one GPU (tycho_batch_*).
+
+    method "si": FP64 source iteration (the reference's fixed point);
+    "mixed": FP32-sweep source iteration on the correction inside FP64
+    refinement.  Each member's result is bit-identical alone and in any mix.
+    """
+
+    BATCH_METHODS = {"si": 0, "mixed": 2}
+
+    def __init__(self, device=0, ipw32=16, ipw64=16):
+        h = C.c_void_p()
+        check(lib().tycho_batch_create(device, ipw32, ipw64, C.byref(h)))
+        self._h = h
+        self._members = {}
+
+    def add(self, sweeper, method="mixed", iter_max=1000, err_max=1e-10, inner_tol=1e-4,
+            inner_max=200, refine_max=30):
+        o = _capi.BatchOpts(self.BATCH_METHODS[method], iter_max, err_max, inner_tol, inner_max,
+                            refine_max)
+        mid = C.c_int()
+        check(lib().tycho_batch_add(self._h, sweeper._h, C.byref(o), C.byref(mid)))
+        self._members[mid.value] = sweeper
+        return mid.value
+
+    def remove(self, mid):
+        check(lib().tycho_batch_remove(self._h, mid))
+        self._members.pop(mid, None)
+
+    def step(self):
+        n = C.c_int()
+        check(lib().tycho_batch_step(self._h, C.byref(n)))
+        return n.value
+
+    def run(self):
+        check(lib().tycho_batch_run(self._h))
+
+    def result(self, mid, want_phi=True):
+        """(phi or None, stats dict, done)."""
+        sw = self._members[mid]
+        phi = np.empty(sw.phi_shape) if want_phi else None
+        st, done = _capi.SolveStats(), C.c_int()
+        check(lib().tycho_batch_result(self._h, mid, ptr(phi), C.byref(st), C.byref(done)))
+        stats = {k: getattr(st, k) for k, _ in _capi.SolveStats._fields_ if k != "seconds"}
+        return phi, stats, bool(done.value)
+
+    def timing(self):
+        ms, passes, upd = np.zeros(2), np.zeros(2, np.int32), np.zeros(2)
+        check(lib().tycho_batch_timing(self._h, ptr(ms), ptr(passes), ptr(upd)))
+        return {"fp64_ms": float(ms[0]), "fp32_ms": float(ms[1]), "fp64_passes": int(passes[0]),
+                "fp32_passes": int(passes[1]), "fp64_updates": float(upd[0]),
+                "fp32_updates": float(upd[1])}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value and _capi._lib is not None:
+            _capi._lib.tycho_batch_destroy(self._h)
+        self._h = None
+        self._members = {}
+
+    def __del__(self):
+        self.close()
