@@ -189,6 +189,7 @@ KERNELS = {
     (2, "items"): "sweep_dataflow_kernel<{r},{k}>", (2, "tiles"): "sweep_tile_dataflow_kernel<{r},{k}>",
     (2, "records"): "sweep_record_dataflow_kernel<{r},{k},{vg}>",
     (3, "records"): "sweep_record_persist_kernel<{r},{k},{vg}>",
+    (1, "direct"): "sweep_direct_level_kernel<{r},{vg},{k}>",
 }
 SCHED = {"levels": 1, "dataflow": 2, "persist": 3}
 

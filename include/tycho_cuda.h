@@ -207,8 +207,12 @@ int tycho_sweeper_levels(const tycho_sweeper *sw, uint32_t *tlevel, uint32_t *de
                   knob warps per block (1, 2, 4),
               2 = records: the per-item factors precomputed once per
                   cross-section set (128 B per item in FP32, 256 B in FP64),
-                  pairs loaded several at a time; knob items per warp (8, 16, 32);
-     vector   records only: groups per vector access of a psi row (1, 2, or
+                  pairs loaded several at a time; knob items per warp (8, 16, 32),
+              3 = direct records: the same records loaded straight into
+                  registers, one thread per (item, group vector), the source
+                  read before the wait on the previous level; level schedule
+                  only, knob threads per block (64, 128, 256);
+     vector   records (2, 3): groups per vector access of a psi row (1, 2, or
               4 in FP32; must divide nGroups); 0 = the widest that divides
               nGroups (4 or 2 in FP32, 2 in FP64). */
 typedef struct tycho_launch_shape {
@@ -301,6 +305,54 @@ int tycho_batch_result(tycho_batch *b, int id, double *phi, tycho_solve_stats *s
 /* Device time of all passes so far (ms) and pass counts, [0] FP64, [1] FP32,
    and the cell x angle x group updates swept in each. */
 int tycho_batch_timing(const tycho_batch *b, double *ms, int *passes, double *updates);
+
+/* ---- solve service: continuous batching under a device-memory budget -----
+   Requests (mesh, SN order, groups, cross sections, isotropic source) are
+   submitted with an arrival time; tycho_server_run serves them in arrival
+   order: a request is admitted when its footprint (tycho_footprint_bytes)
+   fits the budget next to the requests already resident, host threads build
+   its device-resident sweeper (schedule, records, psi), and it joins the
+   running batch at the next step; when its solve finishes, phi is copied to
+   the caller's buffer, the request leaves the batch and its memory is freed.
+   A request's result is bit-identical to the same request served alone. */
+
+/* Device bytes a resident request holds (upper estimate, before building).
+   mixed != 0: the mixed-precision service (FP32 sweep state as well). */
+uint64_t tycho_footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, int mixed);
+
+typedef struct tycho_server tycho_server;
+
+typedef struct tycho_server_opts {
+    int device;
+    double budget_bytes;    /* device memory the resident requests may hold */
+    int setup_threads;      /* host threads building sweepers */
+    int ipw32, ipw64;       /* batched level kernels: items per warp (8, 16, 32) */
+    tycho_batch_opts solve; /* method TYCHO_SOURCE_ITERATION or TYCHO_MIXED_GMRES */
+} tycho_server_opts;
+
+typedef struct tycho_request_info {
+    int state;        /* 0 queued, 1 building, 2 built, 3 in the batch, 4 done, 5 failed */
+    int status;       /* tycho_status of a failed request */
+    double arrival;   /* seconds after tycho_server_run started */
+    double admitted;  /* -1 if never */
+    double built;
+    double finished;
+    uint64_t footprint;
+    tycho_solve_stats stats;
+} tycho_request_info;
+
+int tycho_server_create(const tycho_server_opts *opts, tycho_server **out);
+void tycho_server_destroy(tycho_server *s);
+/* Copies the request's inputs; phi_out (phi layout) must stay valid until
+   tycho_server_run returns.  scatter and q_iso may be NULL. */
+int tycho_server_submit(tycho_server *s, const tycho_mesh *mesh, int sn_order, int n_groups,
+                        const double *sigma_t, const double *sigma_s, const double *scatter,
+                        const double *q_iso, double arrival, double *phi_out, int *id);
+/* Serves every submitted request; returns when all are done or failed. */
+int tycho_server_run(tycho_server *s);
+int tycho_server_request(const tycho_server *s, int id, tycho_request_info *info);
+int tycho_server_stats(const tycho_server *s, double *peak_bytes, int *peak_active, int *steps,
+                       double *makespan);
 
 #ifdef __cplusplus
 }

@@ -37,3 +37,16 @@ def test_sweeper_fails_loudly_without_gpu(built):
     with pytest.raises(ty.TychoError) as e:
         ty.SweeperCuda(mesh, 4, 1)
     assert e.value.status == 4 and "no CPU fallback" in str(e.value)
+
+
+def test_footprint_estimate_covers_psi_and_records():
+    """Admission estimate (no device needed): at least psi (FP64) plus the
+    per-item records of both precisions, growing with cells, groups, order."""
+    import tycho2_b200 as ty
+    for nc, sn, G in [(384, 4, 1), (82944, 8, 8), (663552, 8, 8)]:
+        A = 2 * sn * sn
+        b = ty.footprint_bytes(nc, sn, G, True)
+        assert b >= nc * A * (4 * G * 8 + 256 + 128)
+        assert ty.footprint_bytes(nc, sn, G, False) < b
+        assert ty.footprint_bytes(2 * nc, sn, G, True) > b
+        assert ty.footprint_bytes(nc, sn, 2 * G, True) > b

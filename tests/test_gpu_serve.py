@@ -1,0 +1,73 @@
+"""Solve service: admission by footprint, continuous batching, and the same
+result for a request served alone and in a mix of overlapping arrivals."""
+import numpy as np
+import pytest
+
+from conftest import bits_equal, rel_l1
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(count, seed):
+    from tycho2_b200 import problems
+    params = problems.batch_instances(count, seed=seed, n_range=(2, 6))
+    out = []
+    for p in params:
+        mesh, st, ss, mat, q = problems.make_problem(**p)
+        out.append((p, mesh, st, ss, mat, q))
+    return out
+
+
+def _serve(reqs, method, arrivals, budget=150e9, threads=2):
+    import tycho2_b200 as ty
+    srv = ty.SolveServer(method=method, budget_bytes=budget, setup_threads=threads, err_max=1e-10)
+    ids = [srv.submit(mesh, p["sn"], p["groups"], st, ss, mat, q, arrival=t)
+           for (p, mesh, st, ss, mat, q), t in zip(reqs, arrivals)]
+    srv.run()
+    res = [(srv.phi(i).copy(), srv.info(i)) for i in ids]
+    stats = srv.stats()
+    srv.close()
+    return res, stats
+
+
+@pytest.mark.parametrize("method", ["mixed", "si"])
+def test_served_result_same_alone_and_in_mix(built, method):
+    reqs = _requests(6, seed=11)
+    alone = [_serve([r], method, [0.0])[0][0] for r in reqs]
+    rng = np.random.default_rng(3)
+    arrivals = np.cumsum(rng.exponential(0.01, len(reqs)))  # overlapping arrivals
+    mixed, stats = _serve(reqs, method, arrivals)
+    assert stats["peak_active"] >= 2  # the requests did share the GPU
+    for (pa, ia), (pm, im) in zip(alone, mixed):
+        assert ia["state"] == "done" and im["state"] == "done"
+        assert bits_equal(pa, pm)
+        assert im["arrival"] <= im["admitted"] <= im["built"] <= im["finished"]
+
+
+def test_served_solution_matches_fp64_solve(built):
+    """The mixed service's phi is within 1e-8 of the FP64 service's."""
+    reqs = _requests(4, seed=5)
+    a = [0.0, 0.0, 0.005, 0.01]
+    mixed, _ = _serve(reqs, "mixed", a)
+    fp64, _ = _serve(reqs, "si", a)
+    for (pm, im), (p64, i64) in zip(mixed, fp64):
+        assert rel_l1(pm, p64) <= 1e-8
+        assert im["stats"]["sweeps_fp32"] > 0 and i64["stats"]["sweeps_fp32"] == 0
+
+
+def test_admission_respects_the_budget(built):
+    import tycho2_b200 as ty
+    reqs = _requests(5, seed=21)
+    fps = [ty.footprint_bytes(r[1].n_cells, r[0]["sn"], r[0]["groups"], True) for r in reqs]
+    budget = max(fps) * 1.2  # one request at a time for the largest, a few small ones together
+    res, stats = _serve(reqs, "mixed", [0.0] * len(reqs), budget=budget)
+    assert stats["peak_bytes"] <= budget
+    assert all(i["state"] == "done" for _, i in res)
+    # a request larger than the whole budget fails; the others are served
+    res2, _ = _serve(reqs[:2], "mixed", [0.0, 0.0], budget=min(fps[:2]) * 1.01)
+    states = sorted(i["state"] for _, i in res2)
+    big = int(np.argmax(fps[:2]))
+    if fps[0] != fps[1]:
+        assert res2[big][1]["state"] == "failed" and res2[1 - big][1]["state"] == "done"
+    else:
+        assert states == ["done", "done"]

@@ -5,7 +5,8 @@ CUDA kernels in libtycho_b200.so (C ABI: include/tycho_cuda.h); this package
 is the host-side mirror of the reference's interface over that ABI.
 """
 from ._capi import TychoError, lib  # noqa: F401
-from .sweeper import BatchSolver, Quadrature, SweeperCuda, TychoMesh  # noqa: F401
+from .sweeper import BatchSolver, Quadrature, SolveServer, SweeperCuda, TychoMesh, footprint_bytes  # noqa: F401
 from . import problems  # noqa: F401
 
-__all__ = ["TychoError", "TychoMesh", "Quadrature", "SweeperCuda", "BatchSolver", "problems", "lib"]
+__all__ = ["TychoError", "TychoMesh", "Quadrature", "SweeperCuda", "BatchSolver", "SolveServer",
+           "footprint_bytes", "problems", "lib"]

@@ -47,6 +47,11 @@ class BatchOpts(C.Structure):
                 ("inner_tol", C.c_double), ("inner_max", C.c_int), ("refine_max", C.c_int)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("budget_bytes", C.c_double), ("setup_threads", C.c_int),
+                ("ipw32", C.c_int), ("ipw64", C.c_int), ("solve", BatchOpts)]
+
+
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("sweeps_fp64", C.c_int), ("sweeps_fp32", C.c_int),
                 ("refinements", C.c_int), ("final_error", C.c_double), ("seconds", C.c_double)]
@@ -91,6 +96,23 @@ SIGNATURES = {
     "tycho_batch_result": (C.c_int, [_P, C.c_int, _P, C.POINTER(SolveStats), C.POINTER(C.c_int)]),
     "tycho_batch_timing": (C.c_int, [_P, _P, _P, _P]),
 }
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("status", C.c_int), ("arrival", C.c_double),
+                ("admitted", C.c_double), ("built", C.c_double), ("finished", C.c_double),
+                ("footprint", C.c_uint64), ("stats", SolveStats)]
+
+
+SIGNATURES.update({
+    "tycho_footprint_bytes": (C.c_uint64, [C.c_uint64, C.c_int, C.c_int, C.c_int]),
+    "tycho_server_create": (C.c_int, [C.POINTER(ServerOpts), _PP]),
+    "tycho_server_destroy": (None, [_P]),
+    "tycho_server_submit": (C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P, _P, _P, C.c_double, _P,
+                                      C.POINTER(C.c_int)]),
+    "tycho_server_run": (C.c_int, [_P]),
+    "tycho_server_request": (C.c_int, [_P, C.c_int, C.POINTER(RequestInfo)]),
+    "tycho_server_stats": (C.c_int, [_P, _P, C.POINTER(C.c_int), C.POINTER(C.c_int), _P]),
+})
 
 _lib = None
 

@@ -10,6 +10,7 @@
 #include "schedule.hpp"
 #include "status.hpp"
 #include "batch.hpp"
+#include "server.hpp"
 #include "sweeper.hpp"
 
 struct tycho_mesh {
@@ -23,6 +24,10 @@ struct tycho_sweeper {
 
 struct tycho_batch {
     tycho::Batch b;
+};
+
+struct tycho_server {
+    tycho::Server s;
 };
 
 namespace tycho {
@@ -507,6 +512,97 @@ int tycho_batch_timing(const tycho_batch *b, double *ms, int *passes, double *up
         if (passes) passes[i] = p[i];
         if (updates) updates[i] = u[i];
     }
+    return TYCHO_OK;
+}
+
+uint64_t tycho_footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, int mixed)
+{
+    return tycho::footprint_bytes(n_cells, sn_order, n_groups, mixed != 0);
+}
+
+int tycho_server_create(const tycho_server_opts *o, tycho_server **out)
+{
+    if (!o || !out) return finish(TYCHO_ERR_ARG, "null argument");
+    *out = nullptr;
+    std::string err;
+    return guarded([&] {
+        tycho::ServerOptions so;
+        so.device = o->device;
+        so.budget_bytes = o->budget_bytes;
+        so.setup_threads = o->setup_threads;
+        so.ipw32 = o->ipw32;
+        so.ipw64 = o->ipw64;
+        so.solve.method = o->solve.method;
+        so.solve.iter_max = o->solve.iter_max;
+        so.solve.err_max = o->solve.err_max;
+        so.solve.inner_tol = o->solve.inner_tol;
+        so.solve.inner_max = o->solve.inner_max;
+        so.solve.refine_max = o->solve.refine_max;
+        auto *h = new tycho_server();
+        int s = h->s.init(so, err);
+        if (s != tycho::kOk) {
+            delete h;
+            return finish(s, err);
+        }
+        *out = h;
+        return (int)TYCHO_OK;
+    });
+}
+
+void tycho_server_destroy(tycho_server *s) { delete s; }
+
+int tycho_server_submit(tycho_server *s, const tycho_mesh *mesh, int sn_order, int n_groups,
+                        const double *sigma_t, const double *sigma_s, const double *scatter,
+                        const double *q_iso, double arrival, double *phi_out, int *id)
+{
+    if (!s || !mesh || !id) return finish(TYCHO_ERR_ARG, "null argument");
+    if (sn_order < 2 || sn_order > 32 || sn_order % 2) return finish(TYCHO_ERR_ARG, "bad SN order");
+    std::string err;
+    return guarded([&] {
+        return finish(s->s.submit(mesh->tab, sn_order, n_groups, sigma_t, sigma_s, scatter, q_iso, arrival,
+                                  phi_out, *id, err),
+                      err);
+    });
+}
+
+int tycho_server_run(tycho_server *s)
+{
+    if (!s) return finish(TYCHO_ERR_ARG, "null server");
+    std::string err;
+    return guarded([&] { return finish(s->s.run(err), err); });
+}
+
+int tycho_server_request(const tycho_server *s, int id, tycho_request_info *info)
+{
+    if (!s || !info) return finish(TYCHO_ERR_ARG, "null argument");
+    const tycho::Server::Request *r = s->s.request(id);
+    if (!r) return finish(TYCHO_ERR_ARG, "no request with that id");
+    info->state = r->state;
+    info->status = r->status;
+    info->arrival = r->arrival;
+    info->admitted = r->t_admit;
+    info->built = r->t_built;
+    info->finished = r->t_done;
+    info->footprint = r->footprint;
+    info->stats.iterations = r->stats.iterations;
+    info->stats.sweeps_fp64 = r->stats.sweeps_fp64;
+    info->stats.sweeps_fp32 = r->stats.sweeps_fp32;
+    info->stats.refinements = r->stats.refinements;
+    info->stats.final_error = r->stats.final_error;
+    info->stats.seconds = r->t_done >= 0 ? r->t_done - r->arrival : -1.0;
+    return TYCHO_OK;
+}
+
+int tycho_server_stats(const tycho_server *s, double *peak_bytes, int *peak_active, int *steps, double *makespan)
+{
+    if (!s) return finish(TYCHO_ERR_ARG, "null server");
+    double pb, ms;
+    int pa, st;
+    s->s.stats(pb, pa, st, ms);
+    if (peak_bytes) *peak_bytes = pb;
+    if (peak_active) *peak_active = pa;
+    if (steps) *steps = st;
+    if (makespan) *makespan = ms;
     return TYCHO_OK;
 }
 

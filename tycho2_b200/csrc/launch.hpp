@@ -76,6 +76,11 @@ cudaError_t launch_dataflow_record(int wpb, const LevelArgs &p, const void *rec,
                                    unsigned grid, cudaStream_t s);
 template <typename Real>
 cudaError_t record_dataflow_blocks_per_sm(int ipw, int vg, int *blocks);
+// Direct record variant (level schedule only): one thread per (item, group
+// vector), `bs` threads per block (64, 128 or 256).
+template <typename Real>
+cudaError_t launch_direct_level(int bs, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
+                                cudaStream_t s);
 // Persistent levels: one cooperative launch, a bounded grid barrier between
 // levels (level_off: device copy of the n_levels + 1 level offsets).
 template <typename Real>

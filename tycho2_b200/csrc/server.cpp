@@ -1,0 +1,233 @@
+// Solve service: admission by footprint, host-side builds, continuous batching.
+#include "server.hpp"
+
+#include <algorithm>
+#include <chrono>
+
+#include "status.hpp"
+
+namespace tycho {
+
+uint64_t footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, bool fp32)
+{
+    const uint64_t A = 2ull * sn_order * sn_order;
+    // level padding adds at most 31 items per level; levels stay below 16 n
+    // for Kuhn cubes, far below 5% of the items
+    const uint64_t items = n_cells * A + n_cells * A / 20 + 4096;
+    const uint64_t G = (uint64_t)n_groups, phi = n_cells * 4 * G * 8;
+    uint64_t b = items * 4 * G * 8;                 // psi (FP64-sized; the FP32 sweep shares it)
+    b += items * (32 + (fp32 ? 16 : 0));            // per-item face terms
+    b += items * (4 + 4);                           // item list, completion epochs
+    b += items * (256 + (fp32 ? 128 : 0));          // records
+    b += n_cells * (16 + 4 + 24 + 12 + 8 + 8 + 8);  // adjacency, maps, cell terms, sigma, levels
+    b += phi * (7 + (fp32 ? 4 : 0));                // phi, iso, r, tmp, (FP32 iso, batch r/d/k)
+    return b + (b >> 5) + (8ull << 20);             // allocator rounding
+}
+
+Server::~Server()
+{
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        stop_ = true;
+    }
+    cv_work_.notify_all();
+    for (auto &t : workers_) t.join();
+}
+
+int Server::init(const ServerOptions &o, std::string &err)
+{
+    if (o.budget_bytes <= 0 || o.setup_threads < 1 || o.setup_threads > 64) {
+        err = "bad server options (budget > 0, 1..64 setup threads)";
+        return kErrArg;
+    }
+    if (o.solve.method != 0 && o.solve.method != 2) { err = "server method must be 0 or 2"; return kErrArg; }
+    o_ = o;
+    return batch_.init(o.device, o.ipw32, o.ipw64, err);
+}
+
+double Server::now() const
+{
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count() - t0_;
+}
+
+int Server::submit(const MeshTables &t, int sn, int G, const double *sigma_t, const double *sigma_s,
+                   const double *scatter, const double *q_iso, double arrival, double *phi_out, int &id,
+                   std::string &err)
+{
+    if (!sigma_t || !sigma_s || !phi_out || G < 1 || G > 64 || arrival < 0) {
+        err = "bad request (cross sections, phi buffer, 1..64 groups, arrival >= 0)";
+        return kErrArg;
+    }
+    auto r = std::make_unique<Request>();
+    r->id = (int)reqs_.size() + 1;
+    r->tables = t;
+    r->sn = sn;
+    r->G = G;
+    const size_t nc = t.n_cells;
+    r->sigma_t.assign(sigma_t, sigma_t + nc);
+    r->sigma_s.assign(sigma_s, sigma_s + nc);
+    if (scatter) r->scatter.assign(scatter, scatter + (size_t)G * G);
+    if (q_iso) r->q.assign(q_iso, q_iso + nc * 4 * (size_t)G);
+    r->arrival = arrival;
+    r->phi_out = phi_out;
+    r->footprint = footprint_bytes(nc, sn, G, o_.solve.method == 2);
+    id = r->id;
+    reqs_.push_back(std::move(r));
+    return kOk;
+}
+
+const Server::Request *Server::request(int id) const
+{
+    if (id < 1 || id > (int)reqs_.size()) return nullptr;
+    return reqs_[id - 1].get();
+}
+
+void Server::stats(double &peak_bytes, int &peak_active, int &steps, double &makespan) const
+{
+    peak_bytes = peak_bytes_;
+    peak_active = peak_active_;
+    steps = steps_;
+    makespan = makespan_;
+}
+
+// Builds a request's sweeper: schedule, uploads, cross sections, source and
+// the records of every precision the solve sweeps in.
+void Server::worker()
+{
+    for (;;) {
+        Request *r = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_work_.wait(lk, [&] { return stop_ || !build_q_.empty(); });
+            if (stop_ && build_q_.empty()) return;
+            r = build_q_.front();
+            build_q_.pop_front();
+        }
+        std::string err;
+        auto sw = std::make_unique<Sweeper>();
+        SweeperOptions so;
+        so.sn_order = r->sn;
+        so.n_groups = r->G;
+        so.device = o_.device;
+        so.fp32 = o_.solve.method == 2;
+        int s = sw->init(r->tables, so, err);
+        if (s == kOk)
+            s = sw->set_cross_sections(r->sigma_t.data(), r->sigma_s.data(),
+                                       r->scatter.empty() ? nullptr : r->scatter.data(), err);
+        if (s == kOk && !r->q.empty()) s = sw->set_source(1, r->q.data(), err);
+        Sweeper::DeviceView v;
+        if (s == kOk) s = sw->device_view(0, v, err);
+        if (s == kOk && so.fp32) s = sw->device_view(1, v, err);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            r->status = s;
+            r->error = err;
+            if (s == kOk) r->sw = std::move(sw);
+            r->t_built = now();
+            built_.push_back(r);
+        }
+        cv_built_.notify_all();
+    }
+}
+
+int Server::run(std::string &err)
+{
+    using namespace std::chrono;
+    t0_ = 0;
+    t0_ = now();
+    if (workers_.empty())
+        for (int i = 0; i < o_.setup_threads; ++i) workers_.emplace_back([this] { worker(); });
+    std::vector<Request *> order;
+    for (auto &r : reqs_)
+        if (r->state == 0) order.push_back(r.get());
+    std::stable_sort(order.begin(), order.end(), [](Request *a, Request *b) { return a->arrival < b->arrival; });
+    size_t next = 0;  // next request to admit, in arrival order
+    double reserved = 0;
+    int pending = (int)order.size(), in_batch = 0, building = 0;
+    while (pending > 0) {
+        // admission in arrival order: first come, first served, no overtaking
+        const double t = now();
+        while (next < order.size() && order[next]->arrival <= t) {
+            Request *r = order[next];
+            if ((double)r->footprint > o_.budget_bytes) {
+                r->state = 5;
+                r->status = kErrOom;
+                r->error = "request footprint exceeds the server budget";
+                r->t_done = t;
+                --pending;
+                ++next;
+                continue;
+            }
+            if (reserved + (double)r->footprint > o_.budget_bytes) break;
+            reserved += (double)r->footprint;
+            peak_bytes_ = std::max(peak_bytes_, reserved);
+            r->state = 1;
+            r->t_admit = t;
+            ++building;
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                build_q_.push_back(r);
+            }
+            cv_work_.notify_one();
+            ++next;
+        }
+        // built requests join the batch
+        std::vector<Request *> ready;
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            if (in_batch == 0 && built_.empty()) {
+                // idle GPU: wait for a build or the next arrival
+                const double wait = next < order.size() && order[next]->arrival > t ? order[next]->arrival - t : 0.05;
+                if (building > 0 || wait > 0)
+                    cv_built_.wait_for(lk, duration<double>(std::min(wait > 0 ? wait : 0.05, 0.05)),
+                                       [&] { return !built_.empty(); });
+            }
+            ready.swap(built_);
+        }
+        for (Request *r : ready) {
+            --building;
+            if (r->status != kOk) {
+                r->state = 5;
+                r->t_done = now();
+                reserved -= (double)r->footprint;
+                --pending;
+                continue;
+            }
+            int s = batch_.add(r->sw.get(), o_.solve, r->member, err);
+            if (s != kOk) return s;
+            r->state = 3;
+            ++in_batch;
+        }
+        peak_active_ = std::max(peak_active_, in_batch);
+        if (in_batch == 0) continue;
+        int running = 0;
+        int s = batch_.step(running, err);
+        if (s != kOk) return s;
+        ++steps_;
+        // finished members leave the batch and free their memory
+        for (auto &rp : reqs_) {
+            Request *r = rp.get();
+            if (r->state != 3) continue;
+            BatchMemberStats st;
+            s = batch_.result(r->member, nullptr, st, err);
+            if (s != kOk) return s;
+            if (!st.done) continue;
+            s = batch_.result(r->member, r->phi_out, st, err);
+            if (s != kOk) return s;
+            r->stats = st;
+            s = batch_.remove(r->member, err);
+            if (s != kOk) return s;
+            r->sw.reset();
+            r->state = 4;
+            r->t_done = now();
+            reserved -= (double)r->footprint;
+            --in_batch;
+            --pending;
+        }
+    }
+    makespan_ = now();
+    return kOk;
+}
+
+}  // namespace tycho

@@ -129,6 +129,41 @@ __device__ __forceinline__ void gv_load(const Real *p, Real (&o)[VG])
     else gv_unpack(*vp, o);
 }
 
+// Read access to one item's record: item i of a shared-memory tile, or a
+// record held in registers (the direct variant).
+template <typename Real, int IPW>
+struct TileView {
+    const RecordTile<Real, IPW> &T;
+    uint32_t i;
+    __device__ __forceinline__ Real f(int k) const { return T.f[k][i]; }
+    __device__ __forceinline__ uint32_t u(int k) const { return T.u[k][i]; }
+};
+
+template <typename Real>
+struct RegRecord {
+    Real fv[21];
+    uint32_t uv[7];
+    __device__ __forceinline__ Real f(int k) const { return fv[k]; }
+    __device__ __forceinline__ uint32_t u(int k) const { return uv[k]; }
+};
+
+// One record from global memory straight into registers (read-only path).
+template <typename Real>
+__device__ __forceinline__ void load_record(const ItemRecord<Real> *__restrict__ src, RegRecord<Real> &r)
+{
+    constexpr int N = (21 * sizeof(Real) + 28 + 15) / 16;
+    uint4 v[N];
+    const uint4 *s = reinterpret_cast<const uint4 *>(src);
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = __ldg(s + i);
+    const Real *fr = reinterpret_cast<const Real *>(v);
+    const uint32_t *ur = reinterpret_cast<const uint32_t *>(reinterpret_cast<const char *>(v) + 21 * sizeof(Real));
+#pragma unroll
+    for (int k = 0; k < 21; ++k) r.fv[k] = fr[k];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) r.uv[k] = ur[k];
+}
+
 // All the inputs of one (item, VG groups) task, loaded before any arithmetic.
 template <typename Real, int VG>
 struct PairIn {
@@ -136,17 +171,17 @@ struct PairIn {
     Real pn[4][3][VG];  // [face][the three cell vertices j != f, increasing][group]
 };
 
-template <typename Real, int IPW, int VG, bool L2_ONLY>
-__device__ __forceinline__ void pair_load(const LevelArgs &p, const RecordTile<Real, IPW> &T, uint32_t i,
-                                          uint32_t g, PairIn<Real, VG> &in)
+// Source of one task (fixed angular source, FP64 only, plus the isotropic
+// total source; either may be absent).
+template <typename Real, int VG, typename View>
+__device__ __forceinline__ void pair_load_source(const LevelArgs &p, const View &R, uint32_t g, PairIn<Real, VG> &in)
 {
     const uint32_t G = p.G;
     const size_t rowG = (size_t)4 * G;
-    const uint32_t c = T.u[0][i];
-    const Real *__restrict__ psi = reinterpret_cast<const Real *>(p.psi);
+    const uint32_t c = R.u(0);
     const Real *__restrict__ iso = reinterpret_cast<const Real *>(p.iso);
     if (p.qang) {
-        const double *qa = p.qang + (size_t)T.u[1][i] * rowG + g;
+        const double *qa = p.qang + (size_t)R.u(1) * rowG + g;
         const Real *ic = iso ? iso + (size_t)c * rowG + g : nullptr;
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
@@ -165,11 +200,21 @@ __device__ __forceinline__ void pair_load(const LevelArgs &p, const RecordTile<R
 #pragma unroll
             for (int k = 0; k < VG; ++k) in.q[v][k] = Real(0);
     }
-    const uint32_t nmap = T.u[2][i];
+}
+
+// Upwind values of one task: for each incoming interior face, the
+// neighbour's psi at the three face vertices.
+template <typename Real, int VG, bool L2_ONLY, typename View>
+__device__ __forceinline__ void pair_load_upwind(const LevelArgs &p, const View &R, uint32_t g, PairIn<Real, VG> &in)
+{
+    const uint32_t G = p.G;
+    const size_t rowG = (size_t)4 * G;
+    const Real *__restrict__ psi = reinterpret_cast<const Real *>(p.psi);
+    const uint32_t nmap = R.u(2);
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-        const uint32_t row = T.u[3 + f][i];
-        const bool live = T.f[f][i] < Real(0) && row != kNoRow;
+        const uint32_t row = R.u(3 + f);
+        const bool live = R.f(f) < Real(0) && row != kNoRow;
         const Real *nrow = psi + (size_t)(live ? row : 0u) * rowG + g;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -185,17 +230,26 @@ __device__ __forceinline__ void pair_load(const LevelArgs &p, const RecordTile<R
     }
 }
 
+template <typename Real, int IPW, int VG, bool L2_ONLY>
+__device__ __forceinline__ void pair_load(const LevelArgs &p, const RecordTile<Real, IPW> &T, uint32_t i,
+                                          uint32_t g, PairIn<Real, VG> &in)
+{
+    const TileView<Real, IPW> R{T, i};
+    pair_load_source<Real, VG>(p, R, g, in);
+    pair_load_upwind<Real, VG, L2_ONLY>(p, R, g, in);
+}
+
 // The per-group arithmetic of one task, group by group in the reference's
-// operation order (the factors come from shared memory once per task).
-template <typename Real, int IPW, int VG>
-__device__ __forceinline__ void pair_solve_store(const LevelArgs &p, const RecordTile<Real, IPW> &T, uint32_t i,
-                                                 uint32_t g, const PairIn<Real, VG> &in)
+// operation order (the factors are read once per task).
+template <typename Real, int VG, typename View>
+__device__ __forceinline__ void pair_solve_store_v(const LevelArgs &p, const View &R, uint32_t g,
+                                                   const PairIn<Real, VG> &in)
 {
     Real res[4][VG];
 #pragma unroll
     for (int e = 0; e < VG; ++e) {
         const Real q[4] = {in.q[0][e], in.q[1][e], in.q[2][e], in.q[3][e]};
-        const Real vs20 = T.f[4][i];
+        const Real vs20 = R.f(4);
         Real b[4];
         b[0] = vs20 * (Real(2) * q[0] + q[1] + q[2] + q[3]);
         b[1] = vs20 * (q[0] + Real(2) * q[1] + q[2] + q[3]);
@@ -206,7 +260,7 @@ __device__ __forceinline__ void pair_solve_store(const LevelArgs &p, const Recor
         // increasing order.
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-            const Real t1 = T.f[f][i];
+            const Real t1 = R.f(f);
             if (t1 < Real(0)) {
                 const Real t2 = Real(2) * t1;
 #pragma unroll
@@ -220,25 +274,32 @@ __device__ __forceinline__ void pair_solve_store(const LevelArgs &p, const Recor
                 }
             }
         }
-        b[0] = b[0] * T.f[5][i];
-        b[1] = b[1] - b[0] * T.f[9][i];
-        b[2] = b[2] - b[0] * T.f[10][i];
-        b[3] = b[3] - b[0] * T.f[11][i];
-        b[1] = b[1] * T.f[12][i];
-        b[2] = b[2] - b[1] * T.f[15][i];
-        b[3] = b[3] - b[1] * T.f[16][i];
-        b[2] = b[2] * T.f[17][i];
-        b[3] = b[3] - b[2] * T.f[19][i];
-        b[3] = div_ref(b[3], T.f[20][i]);
-        b[2] = b[2] - T.f[18][i] * b[3];
-        b[1] = b[1] - T.f[14][i] * b[3] - T.f[13][i] * b[2];
-        b[0] = b[0] - T.f[8][i] * b[3] - T.f[7][i] * b[2] - T.f[6][i] * b[1];
+        b[0] = b[0] * R.f(5);
+        b[1] = b[1] - b[0] * R.f(9);
+        b[2] = b[2] - b[0] * R.f(10);
+        b[3] = b[3] - b[0] * R.f(11);
+        b[1] = b[1] * R.f(12);
+        b[2] = b[2] - b[1] * R.f(15);
+        b[3] = b[3] - b[1] * R.f(16);
+        b[2] = b[2] * R.f(17);
+        b[3] = b[3] - b[2] * R.f(19);
+        b[3] = div_ref(b[3], R.f(20));
+        b[2] = b[2] - R.f(18) * b[3];
+        b[1] = b[1] - R.f(14) * b[3] - R.f(13) * b[2];
+        b[0] = b[0] - R.f(8) * b[3] - R.f(7) * b[2] - R.f(6) * b[1];
 #pragma unroll
         for (int v = 0; v < 4; ++v) res[v][e] = b[v];
     }
-    Real *__restrict__ out = reinterpret_cast<Real *>(p.psi) + (size_t)T.u[1][i] * 4 * p.G + g;
+    Real *__restrict__ out = reinterpret_cast<Real *>(p.psi) + (size_t)R.u(1) * 4 * p.G + g;
 #pragma unroll
     for (int v = 0; v < 4; ++v) gv_store(out + v * p.G, res[v]);
+}
+
+template <typename Real, int IPW, int VG>
+__device__ __forceinline__ void pair_solve_store(const LevelArgs &p, const RecordTile<Real, IPW> &T, uint32_t i,
+                                                 uint32_t g, const PairIn<Real, VG> &in)
+{
+    pair_solve_store_v<Real, VG>(p, TileView<Real, IPW>{T, i}, g, in);
 }
 
 // Tasks per lane in flight: fewer as the vector width grows (registers).
@@ -300,6 +361,38 @@ sweep_record_level_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict_
     if (!any) return;
     __syncwarp();
     record_pairs<Real, IPW, VG, false>(p, tiles[w], lane);
+}
+
+// Direct variant (level schedule only): one thread per (item, VG groups)
+// task with the item's record loaded straight into registers -- the lanes of
+// one item read the same 128/256 bytes and L1 serves the repeats -- and its
+// source loaded before the wait on the previous level; only the upwind rows
+// are read after it.  No shared memory.  Tasks of a level: item t / (G/VG),
+// groups VG * (t % (G/VG)) and on (the host keeps a level's task count
+// below 2^26 so that the multiply-high division is exact).
+template <typename Real, int VG, int BS>
+__global__ void __launch_bounds__(BS)
+sweep_direct_level_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict__ rec, const uint64_t begin,
+                          const uint64_t end)
+{
+    pdl_launch_dependents();
+    const uint32_t gpv = p.G / VG;
+    const uint32_t t = blockIdx.x * (uint32_t)BS + threadIdx.x;
+    const uint32_t itl = gpv == 1u ? t : __umulhi(t, p.vmagic);
+    const uint32_t g = (t - itl * gpv) * VG;
+    const uint64_t it = begin + itl;
+    bool live = it < end;
+    RegRecord<Real> R;
+    PairIn<Real, VG> in;
+    if (live) {
+        load_record(rec + it, R);
+        live = R.u(0) != kSentinel;
+    }
+    if (live) pair_load_source<Real, VG>(p, R, g, in);
+    pdl_wait_prerequisites();
+    if (!live) return;
+    pair_load_upwind<Real, VG, false>(p, R, g, in);
+    pair_solve_store_v<Real, VG>(p, R, g, in);
 }
 
 // Dataflow schedule: persistent warps take IPW-item chunks round-robin; lane
@@ -493,6 +586,46 @@ cudaError_t launch_item_records(const LevelArgs &p, uint64_t n, void *out, cudaS
     if (n == 0) return cudaSuccess;
     item_record_kernel<Real><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(p, n, (ItemRecord<Real> *)out);
     return cudaGetLastError();
+}
+
+template <typename Real, int BS>
+static const void *direct_fn_vg(int vg)
+{
+    switch (vg) {
+    case 1: return (const void *)sweep_direct_level_kernel<Real, 1, BS>;
+    case 2: return (const void *)sweep_direct_level_kernel<Real, 2, BS>;
+    case 4:
+        if constexpr (sizeof(Real) == 4) return (const void *)sweep_direct_level_kernel<Real, 4, BS>;
+        else return nullptr;
+    default: return nullptr;
+    }
+}
+
+// Direct variant: knob = threads per block (64, 128 or 256).
+template <typename Real>
+cudaError_t launch_direct_level(int bs, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
+                                cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    const uint64_t tasks = (end - begin) * (p.G / p.vg);
+    if (tasks >= (1ull << 26)) return cudaErrorInvalidValue;
+    const void *fn = bs == 64    ? direct_fn_vg<Real, 64>((int)p.vg)
+                     : bs == 128 ? direct_fn_vg<Real, 128>((int)p.vg)
+                     : bs == 256 ? direct_fn_vg<Real, 256>((int)p.vg)
+                                 : nullptr;
+    if (!fn) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((tasks + bs - 1) / bs));
+    cfg.blockDim = dim3(bs);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const ItemRecord<Real> *r = (const ItemRecord<Real> *)rec;
+    void *args[] = {(void *)&p, (void *)&r, (void *)&begin, (void *)&end};
+    return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 // knob = items per warp (8, 16 or 32); one launch over items [begin, end).

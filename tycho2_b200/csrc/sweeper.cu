@@ -189,11 +189,15 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
         err = "persistent levels in FP64: items per warp must be 8 or 16";
         return kErrArg;
     }
-    if (variant < 0 || variant > 2) {
-        err = "variant must be 0 (item-parallel), 1 (warp tiles) or 2 (precomputed records)";
+    if (variant == 3 && (schedule != 1 || (knob != 64 && knob != 128 && knob != 256))) {
+        err = "direct record variant: level schedule only, 64, 128 or 256 threads per block";
         return kErrArg;
     }
-    if (variant == 2) TY_CHECK(ensure_records(prec, false, err));
+    if (variant < 0 || variant > 3) {
+        err = "variant must be 0 (item-parallel), 1 (warp tiles), 2 (records) or 3 (direct records)";
+        return kErrArg;
+    }
+    if (variant >= 2) TY_CHECK(ensure_records(prec, false, err));
     int sms = 0, per_sm = 0;
     TY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
     if (variant == 0)
@@ -201,9 +205,9 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
     else if (variant == 1)
         TY_CUDA(prec ? tile_dataflow_blocks_per_sm<float>(knob, &per_sm)
                      : tile_dataflow_blocks_per_sm<double>(knob, &per_sm));
-    else
-        TY_CUDA(prec ? record_dataflow_blocks_per_sm<float>(knob, vg, &per_sm)
-                     : record_dataflow_blocks_per_sm<double>(knob, vg, &per_sm));
+    else  // records; the direct variant's no-alloc sweep runs the 16-item record dataflow kernel
+        TY_CUDA(prec ? record_dataflow_blocks_per_sm<float>(variant == 3 ? 16 : knob, vg, &per_sm)
+                     : record_dataflow_blocks_per_sm<double>(variant == 3 ? 16 : knob, vg, &per_sm));
     if (per_sm < 1) { err = "dataflow kernel does not fit on an SM"; return kErrCuda; }
     int persist_per_sm = 0;
     if (schedule == 3) {
@@ -215,7 +219,7 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
     sh.schedule = schedule;
     sh.variant = variant;
     sh.knob = knob;
-    sh.vg = variant == 2 ? vg : 1;
+    sh.vg = variant >= 2 ? vg : 1;
     sh.grid = (unsigned)(sms * per_sm);
     sh.persist_grid = (unsigned)(sms * persist_per_sm);
     // cached level graphs were captured for the previous launch shape
@@ -239,14 +243,15 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
     double best = 1e300;
     LaunchShape keep = shape_[prec ? 1 : 0];
     for (int sched = 1; sched <= 3; ++sched)
-        for (int variant = 0; variant <= 2; ++variant)
-            for (int knob : {1, 2, 4, 8, 16, 32}) {
+        for (int variant = 0; variant <= 3; ++variant)
+            for (int knob : {1, 2, 4, 8, 16, 32, 64, 128, 256}) {
                 if (variant == 0 && ((knob > 2 * G_ && knob > 1) || knob > 16)) continue;  // idle lanes
                 if (variant == 1 && knob > 4) continue;
-                if (variant == 2 && knob < 8) continue;
+                if (variant == 2 && (knob < 8 || knob > 32)) continue;
+                if (variant == 3 && (knob < 64 || sched != 1)) continue;
                 if (sched == 3 && (variant != 2 || (prec == 0 && knob == 32))) continue;
                 for (int vg : {1, 2, 4}) {
-                    if (vg > 1 && (variant != 2 || G_ % vg != 0 || (vg == 4 && prec == 0))) continue;
+                    if (vg > 1 && (variant < 2 || G_ % vg != 0 || (vg == 4 && prec == 0))) continue;
                     const int cs = configure(prec, sched, variant, knob, err, vg);
                     if (cs == kErrOom) continue;  // records do not fit next to psi
                     TY_CHECK(cs);
@@ -275,8 +280,9 @@ int Sweeper::launch_dataflow_shape(int prec, const LevelArgs &p, const DataflowA
                  : launch_dataflow_tile<double>(sh.knob, p, df, sh.grid, s);
     else {
         TY_CHECK(ensure_records(prec, true, err));
-        e = prec ? launch_dataflow_record<float>(sh.knob, p, d_rec_[1], df, sh.grid, s)
-                 : launch_dataflow_record<double>(sh.knob, p, d_rec_[0], df, sh.grid, s);
+        const int ipw = sh.variant == 3 ? 16 : sh.knob;
+        e = prec ? launch_dataflow_record<float>(ipw, p, d_rec_[1], df, sh.grid, s)
+                 : launch_dataflow_record<double>(ipw, p, d_rec_[0], df, sh.grid, s);
     }
     TY_CUDA(e);
     return kOk;
@@ -454,7 +460,7 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         if (end) TY_CUDA(cudaEventRecord(end, stream_));
         return kOk;
     }
-    if (sh.variant == 2) TY_CHECK(ensure_records(prec, true, err));
+    if (sh.variant >= 2) TY_CHECK(ensure_records(prec, true, err));
     auto key = std::make_tuple(prec, has_iso, qang);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
@@ -470,9 +476,12 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
             else if (sh.variant == 1)
                 le = prec ? launch_level_tile<float>(sh.knob, p, b, e, stream_)
                           : launch_level_tile<double>(sh.knob, p, b, e, stream_);
-            else
+            else if (sh.variant == 2)
                 le = prec ? launch_level_record<float>(sh.knob, p, d_rec_[1], b, e, stream_)
                           : launch_level_record<double>(sh.knob, p, d_rec_[0], b, e, stream_);
+            else
+                le = prec ? launch_direct_level<float>(sh.knob, p, d_rec_[1], b, e, stream_)
+                          : launch_direct_level<double>(sh.knob, p, d_rec_[0], b, e, stream_);
         }
         cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
         TY_CUDA(le);

@@ -94,3 +94,40 @@ def make_problem(n, jitter, sn, groups, sigma="uniform", sigma_t=1.0, lognormal_
         inside = np.all((cen >= 0.25) & (cen <= 0.75), axis=1)
         q[inside] = 1.0
     return mesh, st, ss, mat, q
+
+
+def batch_instances(count=256, seed=4321, n_range=(4, 24), groups=(1, 2, 4, 8), sn_orders=(4, 6, 8),
+                    ratio_range=(0.3, 0.95), lognormal_s=0.5, jitter=0.05):
+    """Parameters of `count` independent uneven problems: n ~ U{n_range},
+    G ~ U{groups}, S ~ U{sn_orders}, sigma_t ~ lognormal(0, lognormal_s) per
+    cell, scattering ratio c ~ U[ratio_range] (downscatter rows summing to c
+    for G > 1, within-group for G = 1), isotropic q = 1 everywhere, interior
+    vertices jittered by +-jitter*h -- all seeded.  Returns a list of dicts
+    for make_problem (each with its own seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        G = int(rng.choice(groups))
+        out.append(dict(n=int(rng.integers(n_range[0], n_range[1] + 1)), jitter=jitter,
+                        sn=int(rng.choice(sn_orders)), groups=G, sigma="lognormal",
+                        lognormal_s=lognormal_s, ratio=float(rng.uniform(*ratio_range)),
+                        scatter="within" if G == 1 else "down", source="all",
+                        seed=int(seed * 1000 + k)))
+    return out
+
+
+def footprint_bytes(n_cells, n_angles, groups, fp32=True, records=True):
+    """Device memory of one resident instance (tycho::Sweeper plus its batch
+    vectors): psi (FP64-sized, shared by the FP32 sweep), per-item face terms,
+    schedule, completion flags and records, per-cell tables, phi-sized
+    vectors."""
+    items = n_cells * n_angles  # padding to 32 per level adds a little
+    phi = n_cells * 4 * groups * 8
+    b = items * 4 * groups * 8            # psi
+    b += items * (32 + (16 if fp32 else 0))  # item face terms
+    b += items * (4 + 4)                  # item list, completion flags
+    if records:
+        b += items * (256 + (128 if fp32 else 0))
+    b += n_cells * (16 + 4 + 24 + 12 + 8 + 8)  # adjacency, maps, cell terms, sigma
+    b += phi * (6 + (3 if fp32 else 0))   # phi, iso, r, tmp (+ FP32 iso, batch r/d/k)
+    return int(b * 1.03)

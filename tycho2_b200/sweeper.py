@@ -222,12 +222,12 @@ class SweeperCuda:
         check(lib().tycho_sweeper_time_sweeps(self._h, precision, n, int(flush_l2), ptr(ms)))
         return float(ms[0]), float(ms[1])
 
-    VARIANTS = {"items": 0, "tiles": 1, "records": 2}
+    VARIANTS = {"items": 0, "tiles": 1, "records": 2, "direct": 3}
 
     @staticmethod
     def _shape_dict(sh):
         return {"schedule": {1: "levels", 2: "dataflow", 3: "persist"}[sh.schedule],
-                "variant": {0: "items", 1: "tiles", 2: "records"}[sh.variant], "knob": sh.knob,
+                "variant": {0: "items", 1: "tiles", 2: "records", 3: "direct"}[sh.variant], "knob": sh.knob,
                 "vector": sh.vector}
 
     def autotune(self, precision, reps=3):
@@ -240,8 +240,9 @@ class SweeperCuda:
 
     def configure(self, precision, schedule, variant, knob, vector=0):
         """schedule 'levels'|'dataflow'|'persist' (records only); variant 'items' (knob = lanes per item),
-        'tiles' (knob = warps per block) or 'records' (knob = items per warp; vector = groups per
-        psi-row access, 0 = widest dividing nGroups)."""
+        'tiles' (knob = warps per block), 'records' (knob = items per warp) or 'direct' (records
+        in registers, level schedule, knob = threads per block); vector = records' groups per
+        psi-row access, 0 = widest dividing nGroups."""
         sh = _capi.LaunchShape(self.SCHEDULES[schedule], self.VARIANTS[variant], knob, vector)
         check(lib().tycho_sweeper_configure(self._h, precision, C.byref(sh)))
 
@@ -317,6 +318,72 @@ class BatchSolver:
             _capi._lib.tycho_batch_destroy(self._h)
         self._h = None
         self._members = {}
+
+    def __del__(self):
+        self.close()
+
+
+def footprint_bytes(n_cells, sn_order, n_groups, mixed=True):
+    """Device bytes one resident solve request holds (tycho_footprint_bytes)."""
+    return int(lib().tycho_footprint_bytes(n_cells, sn_order, n_groups, int(mixed)))
+
+
+class SolveServer:
+    """Solve service on one GPU (tycho_server_*): requests with arrival times
+    are admitted by device-memory footprint against `budget_bytes`, built by
+    host threads and solved by continuous batching."""
+
+    STATES = {0: "queued", 1: "building", 2: "built", 3: "in batch", 4: "done", 5: "failed"}
+
+    def __init__(self, method="mixed", budget_bytes=150e9, device=0, setup_threads=2, ipw32=16,
+                 ipw64=16, iter_max=3000, err_max=1e-10, inner_tol=1e-4, inner_max=200, refine_max=30):
+        solve = _capi.BatchOpts(BatchSolver.BATCH_METHODS[method], iter_max, err_max, inner_tol,
+                                inner_max, refine_max)
+        o = _capi.ServerOpts(device, float(budget_bytes), setup_threads, ipw32, ipw64, solve)
+        h = C.c_void_p()
+        check(lib().tycho_server_create(C.byref(o), C.byref(h)))
+        self._h = h
+        self.method = method
+        self._out = {}
+        self._keep = []
+
+    def submit(self, mesh, sn_order, n_groups, sigma_t, sigma_s, scatter=None, q_iso=None, arrival=0.0):
+        """Queues a request; returns its id.  phi is available after run()."""
+        phi = np.empty((mesh.n_cells, 4, n_groups))
+        arrs = [np.ascontiguousarray(a, np.float64) if a is not None else None
+                for a in (sigma_t, sigma_s, scatter, q_iso)]
+        rid = C.c_int()
+        check(lib().tycho_server_submit(self._h, mesh._h, sn_order, n_groups, *(ptr(a) for a in arrs),
+                                        float(arrival), ptr(phi), C.byref(rid)))
+        self._out[rid.value] = phi
+        self._keep.append(mesh)
+        return rid.value
+
+    def run(self):
+        check(lib().tycho_server_run(self._h))
+
+    def phi(self, rid):
+        return self._out[rid]
+
+    def info(self, rid):
+        i = _capi.RequestInfo()
+        check(lib().tycho_server_request(self._h, rid, C.byref(i)))
+        d = {k: getattr(i, k) for k, _ in _capi.RequestInfo._fields_ if k != "stats"}
+        d["state"] = self.STATES.get(d["state"], d["state"])
+        d["stats"] = {k: getattr(i.stats, k) for k, _ in _capi.SolveStats._fields_}
+        d["latency"] = d["finished"] - d["arrival"] if d["finished"] >= 0 else None
+        return d
+
+    def stats(self):
+        pb, ms = C.c_double(), C.c_double()
+        pa, st = C.c_int(), C.c_int()
+        check(lib().tycho_server_stats(self._h, C.byref(pb), C.byref(pa), C.byref(st), C.byref(ms)))
+        return {"peak_bytes": pb.value, "peak_active": pa.value, "steps": st.value, "makespan": ms.value}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value and _capi._lib is not None:
+            _capi._lib.tycho_server_destroy(self._h)
+        self._h = None
 
     def __del__(self):
         self.close()
