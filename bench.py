@@ -9,6 +9,14 @@ beside it, with the phi error of the mixed-precision solve against the FP64
 solve.  `e2e` is the drop-in SweeperAbstract::sweep(psi, source) through the
 C ABI with host buffers (psi-sized source in, psi out, copies timed).
 
+Two more legs ride on the same line (skip with --no-batch / --no-serve):
+`batch`, 256 uneven independent instances solved together (FP64 source
+iteration vs FP32-sweep iteration inside FP64 refinement, one batched pass
+per step), and `serve`, Poisson-arriving solve requests (the batch size
+distribution plus 5% large 48^3-hex S8 G=8 ones) admitted by device-memory
+footprint against 150 GB with continuous batching: p50/p99 latency and
+solves/s of the mixed and the FP64 service.
+
 Multi-GPU: the sweep does not shard across GPUs here (one mesh partition per
 GPU by design); --gpus N runs N independent replicas, one per rank, and
 reports the sum of their throughputs with the max-over-ranks time.
@@ -45,6 +53,11 @@ def parse():
     p.add_argument("--no-solve", action="store_true", help="skip the solve-error check")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-batch", action="store_true", help="skip the batched-instances leg")
+    p.add_argument("--batch-instances", type=int, default=256)
+    p.add_argument("--no-serve", action="store_true", help="skip the served-solves leg")
+    p.add_argument("--serve-requests", type=int, default=40)
+    p.add_argument("--serve-rate", type=float, default=10.0, help="Poisson arrivals per second")
     p.add_argument("--shape", default="auto",
                    help="launch shape 'schedule,variant,knob' for both precisions, or auto (autotuner)")
     return p.parse_args()
@@ -190,6 +203,7 @@ KERNELS = {
     (2, "records"): "sweep_record_dataflow_kernel<{r},{k},{vg}>",
     (3, "records"): "sweep_record_persist_kernel<{r},{k},{vg}>",
     (1, "direct"): "sweep_direct_level_kernel<{r},{vg},{k}>",
+    (1, "compact"): "sweep_direct_level_kernel<{r},{vg},{k},compact>",
 }
 SCHED = {"levels": 1, "dataflow": 2, "persist": 3}
 
@@ -219,6 +233,99 @@ def profiled_traffic(workload, kernel):
     except (OSError, ValueError):
         pass
     return None
+
+
+def run_batch_leg(grp, dev, count, seed=4321):
+    """Batched uneven instances: `count` problems (n ~ U{4..24}, G ~ U{1,2,4,8},
+    S ~ U{4,6,8}, sigma_t ~ lognormal(0, 0.5), c ~ U[0.3, 0.95], q = 1, all
+    seeded) solved together, FP64 source iteration vs FP32-sweep source
+    iteration inside FP64 refinement, both to 1e-10 relative change."""
+    import tycho2_b200 as ty
+    from tycho2_b200 import problems
+    t0 = time.perf_counter()
+    sws, upd = [], 0
+    for p in problems.batch_instances(count, seed=seed + 7919 * grp.rank):
+        mesh, st, ss, mat, q = problems.make_problem(**p)
+        sw = ty.SweeperCuda(mesh, p["sn"], p["groups"], fp32=True, device=dev)
+        sw.set_cross_sections(st, ss, mat)
+        sw.set_source(q, "isotropic")
+        sws.append(sw)
+        upd += mesh.n_cells * 2 * p["sn"] ** 2 * p["groups"]
+    setup = time.perf_counter() - t0
+    out, phis = {}, {}
+    for method in ("si", "mixed"):
+        b = ty.BatchSolver(device=dev)
+        ids = [b.add(sw, method, err_max=1e-10, iter_max=5000) for sw in sws]
+        grp.barrier()
+        t = time.perf_counter()
+        steps = 0
+        while b.step() > 0:
+            steps += 1
+        wall = grp.max(time.perf_counter() - t)
+        tm = b.timing()
+        res = [b.result(i) for i in ids]
+        phis[method] = [r[0] for r in res]
+        swept = tm["fp64_updates"] + tm["fp32_updates"]
+        out[method] = {
+            "solve_wall_s": wall, "steps": steps, "updates_swept": swept,
+            "solve_updates_per_s": grp.sum(swept) / wall,
+            "fp64_pass_updates_per_s": tm["fp64_updates"] / (tm["fp64_ms"] * 1e-3) if tm["fp64_ms"] else None,
+            "fp32_pass_updates_per_s": tm["fp32_updates"] / (tm["fp32_ms"] * 1e-3) if tm["fp32_ms"] else None,
+            "sweeps_fp64": sum(r[1]["sweeps_fp64"] for r in res),
+            "sweeps_fp32": sum(r[1]["sweeps_fp32"] for r in res),
+            "all_converged": all(r[1]["final_error"] <= 1e-10 for r in res)}
+        b.close()
+    err = [float(np.abs(m - f).sum() / np.abs(f).sum()) for m, f in zip(phis["mixed"], phis["si"])]
+    for sw in sws:
+        sw.close()
+    return {"instances": count * grp.world, "updates_per_sweep": upd, "setup_s": setup,
+            "kernel": "batch_direct_level_kernel (compact records)",
+            "fp64_si": out["si"], "mixed": out["mixed"],
+            "phi_rel_err_l1_max_mixed_vs_fp64": grp.max(max(err)),
+            "mixed_vs_fp64_solve_speedup": out["si"]["solve_wall_s"] / out["mixed"]["solve_wall_s"],
+            "mixed_vs_fp64_pass_speedup": (out["mixed"]["fp32_pass_updates_per_s"]
+                                           / out["si"]["fp64_pass_updates_per_s"])}
+
+
+def run_serve_leg(grp, dev, count, rate, seed=99):
+    """Served solves: `count` requests drawn like the batch instances plus 5%
+    large ones (48^3 hexes x 6 tets, G=8, S8), Poisson arrivals at `rate` per
+    second, admitted by footprint against 150 GB, mixed vs FP64 service."""
+    import tycho2_b200 as ty
+    from tycho2_b200 import problems
+    rng = np.random.default_rng(seed + grp.rank)
+    params = problems.batch_instances(count, seed=seed + 31 * grp.rank)
+    for k in range(count):
+        if rng.random() < 0.05:
+            params[k] = dict(n=48, jitter=0.05, sn=8, groups=8, sigma="lognormal", lognormal_s=0.5,
+                             ratio=0.6, scatter="down", source="all", seed=5000 + k)
+    probs = [problems.make_problem(**p) for p in params]
+    gaps = rng.exponential(1.0 / rate, count)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    out = {"requests": count * grp.world, "large": int(sum(p["n"] == 48 for p in params)),
+           "rate_per_s": rate * grp.world, "budget_gb": 150.0}
+    phis = {}
+    for method, key in (("mixed", "mixed"), ("si", "fp64")):
+        srv = ty.SolveServer(method=method, budget_bytes=150e9, device=dev, setup_threads=4, err_max=1e-10)
+        ids = [srv.submit(m, p["sn"], p["groups"], st, ss, mat, q, arrival=float(a))
+               for p, (m, st, ss, mat, q), a in zip(params, probs, arrivals)]
+        grp.barrier()
+        srv.run()
+        info = [srv.info(i) for i in ids]
+        done = [i for i in info if i["state"] == "done"]
+        lat = np.array([i["latency"] for i in done])
+        st_ = srv.stats()
+        phis[key] = [srv.phi(i).copy() for i in ids]
+        out[key] = {"done": len(done), "p50_latency_s": grp.max(float(np.percentile(lat, 50))),
+                    "p99_latency_s": grp.max(float(np.percentile(lat, 99))),
+                    "solves_per_s": grp.sum(len(done)) / grp.max(st_["makespan"]),
+                    "build_p50_s": float(np.percentile([i["built"] - i["admitted"] for i in done], 50)),
+                    "peak_resident_gb": st_["peak_bytes"] / 1e9, "peak_in_batch": st_["peak_active"],
+                    "batch_steps": st_["steps"]}
+        srv.close()
+    out["phi_rel_err_l1_max_mixed_vs_fp64"] = grp.max(max(
+        float(np.abs(a - b).sum() / np.abs(b).sum()) for a, b in zip(phis["mixed"], phis["fp64"])))
+    return out
 
 
 def run_b200(args):
@@ -314,6 +421,18 @@ def run_b200(args):
                "seconds_per_step": dt}
         del src_t, psi_t
 
+    batch = serve = None
+    if not args.no_batch:
+        try:
+            batch = run_batch_leg(grp, dev, args.batch_instances)
+        except Exception as e:  # reported, never fatal to the headline line
+            batch = {"error": str(e)[:300]}
+    if not args.no_serve:
+        try:
+            serve = run_serve_leg(grp, dev, args.serve_requests, args.serve_rate)
+        except Exception as e:
+            serve = {"error": str(e)[:300]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -347,6 +466,8 @@ def run_b200(args):
                                   "traffic": t64}},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "batch": batch,
+            "serve": serve,
             "gpu_launches": args.steps * (launches_per_sweep(shape32, info["n_levels"])
                                           + launches_per_sweep(shape64, info["n_levels"])),
             "clocks": clocks,

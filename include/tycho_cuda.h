@@ -211,7 +211,11 @@ int tycho_sweeper_levels(const tycho_sweeper *sw, uint32_t *tlevel, uint32_t *de
               3 = direct records: the same records loaded straight into
                   registers, one thread per (item, group vector), the source
                   read before the wait on the previous level; level schedule
-                  only, knob threads per block (64, 128, 256);
+                  only, knob threads per block (64, 128, 256),
+              4 = direct compact records: 64 B (FP32) / 96 B (FP64) per item
+                  holding the matrix inputs (face terms, sigma_t V/20, V/20)
+                  and topology; the factors are rebuilt in registers with the
+                  same arithmetic; level schedule, knob as for 3;
      vector   records (2, 3): groups per vector access of a psi row (1, 2, or
               4 in FP32; must divide nGroups); 0 = the widest that divides
               nGroups (4 or 2 in FP32, 2 in FP64). */
@@ -287,7 +291,9 @@ typedef struct tycho_batch_opts {
     int refine_max;   /* mixed: refinements */
 } tycho_batch_opts;
 
-/* ipw32 / ipw64: items per warp of the FP32 / FP64 wavefront kernels (8, 16, 32). */
+/* ipw32 / ipw64: items per warp of the FP32 / FP64 wavefront kernels (8, 16,
+   32: records staged in shared memory), or 0: records loaded straight into
+   registers, one thread per (item, group vector). */
 int tycho_batch_create(int device, int ipw32, int ipw64, tycho_batch **out);
 void tycho_batch_destroy(tycho_batch *b);
 /* Adds a member (the sweeper must outlive its membership); its solve starts
@@ -317,8 +323,10 @@ int tycho_batch_timing(const tycho_batch *b, double *ms, int *passes, double *up
    A request's result is bit-identical to the same request served alone. */
 
 /* Device bytes a resident request holds (upper estimate, before building).
-   mixed != 0: the mixed-precision service (FP32 sweep state as well). */
-uint64_t tycho_footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, int mixed);
+   mixed != 0: the mixed-precision service (FP32 sweep state as well);
+   compact != 0: the service's batch runs the direct kernels (ipw 0) on
+   compact records. */
+uint64_t tycho_footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, int mixed, int compact);
 
 typedef struct tycho_server tycho_server;
 
@@ -326,7 +334,7 @@ typedef struct tycho_server_opts {
     int device;
     double budget_bytes;    /* device memory the resident requests may hold */
     int setup_threads;      /* host threads building sweepers */
-    int ipw32, ipw64;       /* batched level kernels: items per warp (8, 16, 32) */
+    int ipw32, ipw64;       /* batched level kernels: items per warp (8, 16, 32; 0 = direct) */
     tycho_batch_opts solve; /* method TYCHO_SOURCE_ITERATION or TYCHO_MIXED_GMRES */
 } tycho_server_opts;
 

@@ -45,8 +45,10 @@ def test_footprint_estimate_covers_psi_and_records():
     import tycho2_b200 as ty
     for nc, sn, G in [(384, 4, 1), (82944, 8, 8), (663552, 8, 8)]:
         A = 2 * sn * sn
-        b = ty.footprint_bytes(nc, sn, G, True)
+        b = ty.footprint_bytes(nc, sn, G, True, False)
         assert b >= nc * A * (4 * G * 8 + 256 + 128)
-        assert ty.footprint_bytes(nc, sn, G, False) < b
-        assert ty.footprint_bytes(2 * nc, sn, G, True) > b
-        assert ty.footprint_bytes(nc, sn, 2 * G, True) > b
+        assert ty.footprint_bytes(nc, sn, G, True, True) >= nc * A * (4 * G * 8 + 96 + 64)
+        assert ty.footprint_bytes(nc, sn, G, True, True) < b
+        assert ty.footprint_bytes(nc, sn, G, False, False) < b
+        assert ty.footprint_bytes(2 * nc, sn, G, True, False) > b
+        assert ty.footprint_bytes(nc, sn, 2 * G, True, False) > b

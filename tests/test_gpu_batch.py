@@ -37,9 +37,9 @@ def _problem(workdir, case, seed):
     return sw, om, (st, ss, mat, q)
 
 
-def _solve(sws, method, **kw):
+def _solve(sws, method, ipw=16, **kw):
     import tycho2_b200 as ty
-    b = ty.BatchSolver()
+    b = ty.BatchSolver(ipw32=ipw, ipw64=ipw)
     ids = [b.add(sw, method, **kw) for sw in sws]
     b.run()
     out = [b.result(i) for i in ids]
@@ -49,10 +49,11 @@ def _solve(sws, method, **kw):
     return out
 
 
-def test_batch_si_matches_oracle_source_iteration(built, workdir):
+@pytest.mark.parametrize("ipw", [16, 0])
+def test_batch_si_matches_oracle_source_iteration(built, workdir, ipw):
     from oracle.oracle import Oracle
     probs = [_problem(workdir, c, 40 + k) for k, c in enumerate(CASES)]
-    res = _solve([p[0] for p in probs], "si", err_max=1e-10, iter_max=400)
+    res = _solve([p[0] for p in probs], "si", ipw=ipw, err_max=1e-10, iter_max=400)
     for (sw, om, (st, ss, mat, q)), case, (phi, stats, done) in zip(probs, CASES, res):
         o = Oracle(om, case[2], case[3])
         _, phi_ref, it_ref, _ = o.source_iteration(st, ss, mat, q_iso=q, iter_max=400, err_max=1e-10)
@@ -64,28 +65,29 @@ def test_batch_si_matches_oracle_source_iteration(built, workdir):
             assert abs(stats["iterations"] - it_ref) == 1 and rel_l1(phi, phi_ref) <= 1e-9, case
 
 
-def test_batch_mixed_within_1e8_of_fp64(built, workdir):
+@pytest.mark.parametrize("ipw", [16, 0])
+def test_batch_mixed_within_1e8_of_fp64(built, workdir, ipw):
     probs = [_problem(workdir, c, 60 + k) for k, c in enumerate(CASES)]
     sws = [p[0] for p in probs]
-    si = _solve(sws, "si", err_max=1e-12, iter_max=2000)
-    mixed = _solve(sws, "mixed", err_max=1e-12, iter_max=4000)
+    si = _solve(sws, "si", ipw=ipw, err_max=1e-12, iter_max=2000)
+    mixed = _solve(sws, "mixed", ipw=ipw, err_max=1e-12, iter_max=4000)
     for case, (phi64, s64, _), (phim, sm, done) in zip(CASES, si, mixed):
         assert done
         assert rel_l1(phim, phi64) <= 1e-8, (case, rel_l1(phim, phi64))
         assert sm["sweeps_fp32"] > sm["sweeps_fp64"] and sm["refinements"] >= 1
 
 
-@pytest.mark.parametrize("method", ["si", "mixed"])
-def test_batch_member_bit_identical_alone_and_in_mix(built, workdir, method):
+@pytest.mark.parametrize("method,ipw", [("si", 16), ("mixed", 16), ("si", 0), ("mixed", 0)])
+def test_batch_member_bit_identical_alone_and_in_mix(built, workdir, method, ipw):
     probs = [_problem(workdir, c, 80 + k) for k, c in enumerate(CASES)]
     sws = [p[0] for p in probs]
-    alone = [_solve([sw], method, err_max=1e-10)[0] for sw in sws]
-    mixed = _solve(sws, method, err_max=1e-10)
+    alone = [_solve([sw], method, ipw=ipw, err_max=1e-10)[0] for sw in sws]
+    mixed = _solve(sws, method, ipw=ipw, err_max=1e-10)
     for case, (pa, sa, _), (pm, smx, _) in zip(CASES, alone, mixed):
         assert bits_equal(pa, pm), case
         assert sa == smx, case
     # and again in another order, with a repeated solve of the same members
-    rev = _solve(sws[::-1], method, err_max=1e-10)[::-1]
+    rev = _solve(sws[::-1], method, ipw=ipw, err_max=1e-10)[::-1]
     for case, (pa, _, _), (pr, _, _) in zip(CASES, alone, rev):
         assert bits_equal(pa, pr), case
 

@@ -25,7 +25,8 @@ def test_fp64_sweep_bit_exact_vs_reference_fixture(built, kuhn3_ref):
     for shape in (("levels", "items", 1), ("levels", "items", 2), ("dataflow", "items", 4),
                   ("levels", "tiles", 4), ("dataflow", "tiles", 1), ("dataflow", "tiles", 2),
                   ("levels", "records", 8), ("dataflow", "records", 16), ("dataflow", "records", 32),
-                  ("persist", "records", 8), ("persist", "records", 16), ("levels", "direct", 256)):
+                  ("persist", "records", 8), ("persist", "records", 16), ("levels", "direct", 256),
+                  ("levels", "compact", 128)):
         sw = make(mesh, 4, 3)
         sw.configure(0, *shape)
         sw.set_cross_sections(r["sweep_sigma_t"], np.zeros(mesh.n_cells))
@@ -37,7 +38,8 @@ def test_fp64_sweep_bit_exact_vs_reference_fixture(built, kuhn3_ref):
 @pytest.mark.parametrize("schedule,variant,vector", [
     ("levels", "items", 0), ("levels", "tiles", 0), ("levels", "records", 0), ("levels", "records", 1),
     ("dataflow", "items", 0), ("dataflow", "tiles", 0), ("dataflow", "records", 0),
-    ("persist", "records", 0), ("persist", "records", 1), ("levels", "direct", 0), ("levels", "direct", 1)])
+    ("persist", "records", 0), ("persist", "records", 1), ("levels", "direct", 0), ("levels", "direct", 1),
+    ("levels", "compact", 0), ("levels", "compact", 1)])
 @pytest.mark.parametrize("n,jitter,sn,G,tpi", [
     (4, 0.05, 4, 1, 1), (5, 0.05, 8, 2, 2), (3, 0.0, 2, 3, 1), (6, 0.05, 6, 4, 4),
     (4, 0.07, 8, 8, 8), (2, 0.05, 4, 16, 16), (7, 0.05, 4, 5, 2), (1, 0.0, 4, 1, 1),
@@ -52,6 +54,7 @@ def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi, v
     sw = make(mesh, sn, G)
     knob = {"items": tpi, "tiles": min(tpi, 4), "records": 8 if tpi <= 2 else (16 if tpi <= 4 else 32),
             "direct": 64 * min(tpi, 4) if tpi != 4 else 128}
+    knob["compact"] = knob["direct"]
     if schedule == "persist":
         knob["records"] = min(knob["records"], 16)  # two 32-item FP64 tiles exceed shared memory
     sw.configure(0, schedule, variant, knob[variant], vector)
@@ -175,7 +178,7 @@ def test_fp32_sweep_within_tolerance(built, workdir):
                   ("levels", "tiles", 2), ("dataflow", "tiles", 4), ("levels", "records", 16),
                   ("dataflow", "records", 32), ("persist", "records", 8), ("persist", "records", 32),
                   ("levels", "records", 16, 1), ("levels", "records", 16, 2), ("levels", "direct", 128),
-                  ("levels", "direct", 64, 1)):
+                  ("levels", "direct", 64, 1), ("levels", "compact", 64), ("levels", "compact", 128, 2)):
         sw = make(mesh, 8, G, fp32=True)
         sw.configure(1, *shape)
         sw.set_cross_sections(st, st, mat)
@@ -263,7 +266,7 @@ def test_autotune_keeps_results_bit_exact(built, workdir):
     sw.set_cross_sections(st, np.zeros(mesh.n_cells))
     best64 = sw.autotune(0, reps=2)
     best32 = sw.autotune(1, reps=2)
-    assert best64["variant"] in ("items", "tiles", "records", "direct") and best32["schedule"] in ("levels", "dataflow", "persist")
+    assert best64["variant"] in ("items", "tiles", "records", "direct", "compact") and best32["schedule"] in ("levels", "dataflow", "persist")
     assert sw.shape(0) == {k: best64[k] for k in ("schedule", "variant", "knob", "vector")}
     psi = np.empty(sw.psi_shape)
     sw.sweep(psi, src)

@@ -104,7 +104,7 @@ class RequestInfo(C.Structure):
 
 
 SIGNATURES.update({
-    "tycho_footprint_bytes": (C.c_uint64, [C.c_uint64, C.c_int, C.c_int, C.c_int]),
+    "tycho_footprint_bytes": (C.c_uint64, [C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int]),
     "tycho_server_create": (C.c_int, [C.POINTER(ServerOpts), _PP]),
     "tycho_server_destroy": (None, [_P]),
     "tycho_server_submit": (C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P, _P, _P, C.c_double, _P,

@@ -70,7 +70,10 @@ Batch::~Batch()
 int Batch::init(int device, int ipw32, int ipw64, std::string &err)
 {
     for (int ipw : {ipw32, ipw64})
-        if (ipw != 8 && ipw != 16 && ipw != 32) { err = "items per warp must be 8, 16 or 32"; return kErrArg; }
+        if (ipw != 0 && ipw != 8 && ipw != 16 && ipw != 32) {
+            err = "items per warp must be 8, 16 or 32 (0: direct kernel)";
+            return kErrArg;
+        }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         err = "no CUDA device: the batched sweep has no CPU fallback";
@@ -110,9 +113,9 @@ int Batch::add(Sweeper *sw, const BatchOptions &o, int &id, std::string &err)
     Member m;
     m.sw = sw;
     m.o = o;
-    TB_CHECK(sw->device_view(0, m.v[0], err));
+    TB_CHECK(sw->device_view(0, m.v[0], err, ipw_[0] == 0));
     if (o.method == 2) {
-        TB_CHECK(sw->device_view(1, m.v[1], err));
+        TB_CHECK(sw->device_view(1, m.v[1], err, ipw_[1] == 0));
         const size_t n = sw->phi_size();
         TB_CUDA(cudaMalloc(&m.r, sizeof(double) * n));
         TB_CUDA(cudaMalloc(&m.d, sizeof(double) * n));
@@ -261,7 +264,11 @@ int Batch::build_graph(int prec, std::string &err)
         uint64_t chunks[kBatchClasses] = {0, 0, 0};
         for (const auto &m : members_) {
             const auto &lo = m.sw->schedule().level_offset;
-            if (L < m.v[0].n_levels) chunks[m.v[prec].vg == 4 ? 2 : m.v[prec].vg == 2 ? 1 : 0] += (lo[L + 1] - lo[L]) / ipw;
+            if (L >= m.v[0].n_levels) continue;
+            const uint64_t items = lo[L + 1] - lo[L];
+            const uint32_t vg = m.v[prec].vg;
+            chunks[vg == 4 ? 2 : vg == 2 ? 1 : 0] +=
+                ipw ? items / ipw : items / 32 * ((uint64_t)m.sw->n_groups() / vg);
         }
         cuts[L].c[0] = 0;
         for (uint32_t c = 0; c < kBatchClasses; ++c)
@@ -269,7 +276,9 @@ int Batch::build_graph(int prec, std::string &err)
     }
     cudaGraph_t g;
     TB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = launch_batch_plan(ipw, d_slots_[prec], n, max_levels_, plan_, stream_);
+    const uint32_t rec_bytes =
+        (uint32_t)(ipw ? record_bytes(prec == 1) : compact_record_bytes(prec == 1));
+    cudaError_t e = launch_batch_plan(ipw, d_slots_[prec], n, max_levels_, rec_bytes, plan_, stream_);
     if (e == cudaSuccess && prec == 0) e = launch_batch_accept(d_slots_[prec], plan_, kStreamGrid, stream_);
     if (e == cudaSuccess) e = launch_batch_scatter(d_slots_[prec], plan_, kStreamGrid, stream_);
     for (uint32_t L = 0; L < max_levels_ && e == cudaSuccess; ++L)

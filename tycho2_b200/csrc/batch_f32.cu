@@ -11,7 +11,8 @@ template <>
 cudaError_t launch_batch_level<float>(int ipw, const BatchSlot *slots, const BatchPlan &pl, uint32_t level,
                                       const BatchCuts &cut, cudaStream_t s)
 {
-    const void *fn = ipw == 8    ? (const void *)batch_level_kernel<float, 8>
+    const void *fn = ipw == 0    ? (const void *)batch_direct_level_kernel<float>
+                     : ipw == 8  ? (const void *)batch_level_kernel<float, 8>
                      : ipw == 16 ? (const void *)batch_level_kernel<float, 16>
                      : ipw == 32 ? (const void *)batch_level_kernel<float, 32>
                                  : nullptr;

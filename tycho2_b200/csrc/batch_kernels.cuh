@@ -59,7 +59,8 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *t
 // and their phi chunk prefix.
 template <int IPW>
 __global__ void __launch_bounds__(kBatchPlanThreads)
-batch_plan_kernel(const BatchSlot *__restrict__ slots, uint32_t n_slots, uint32_t max_levels, BatchPlan pl)
+batch_plan_kernel(const BatchSlot *__restrict__ slots, uint32_t n_slots, uint32_t max_levels, uint32_t rec_bytes,
+                  BatchPlan pl)
 {
     const uint32_t L = blockIdx.x;
     if (L < max_levels) {
@@ -72,16 +73,24 @@ batch_plan_kernel(const BatchSlot *__restrict__ slots, uint32_t n_slots, uint32_
                 uint64_t lo = 0;
                 if (j < n_slots && slots[j].active && L < slots[j].n_levels && batch_class(slots[j].vg) == cls) {
                     lo = slots[j].level_off[L];
-                    nch = (uint32_t)((slots[j].level_off[L + 1] - lo) / IPW);
+                    const uint64_t items = slots[j].level_off[L + 1] - lo;
+                    // IPW items per chunk; IPW == 0 (direct kernel): 32 (item, group vector) tasks
+                    nch = IPW ? (uint32_t)(items / IPW) : (uint32_t)(items / 32 * (slots[j].G / slots[j].vg));
                 }
                 uint32_t tot_c, tot_s;
                 const uint32_t ex_c = block_exclusive_scan(nch, &tot_c);
                 const uint32_t ex_s = block_exclusive_scan(nch ? 1u : 0u, &tot_s);
                 if (nch) {
+                    const BatchSlot &sl = slots[j];
                     BatchSeg sg;
+                    sg.rec = (const char *)sl.rec + lo * rec_bytes;
+                    sg.psi = sl.psi;
+                    sg.iso = sl.iso32 ? (const void *)sl.iso32 : (const void *)sl.iso;
                     sg.item_begin = lo;
                     sg.slot = j;
                     sg.chunk_begin = chunk_run + ex_c;
+                    sg.G = sl.G;
+                    sg.vmagic = sl.vmagic;
                     segs[seg_run + ex_s] = sg;
                 }
                 chunk_run += tot_c;
@@ -171,6 +180,75 @@ __device__ __forceinline__ void batch_class_body(const BatchSlot *__restrict__ s
         record_pairs<Real, IPW, VG, false>(slot_args<Real>(s), T, lane);
         __syncwarp();
     }
+}
+
+// Direct form (compact records rebuilt into registers): chunk = 32 (item,
+// group vector) tasks of one member at one level (a level's item count is a
+// multiple of 32, so chunks never straddle members), one task per lane.  The
+// block stages its class's segments of the level in shared memory before the
+// wait on the previous level (up to kBatchSegSmem of them; more are searched
+// in global memory), so a warp's member lookup is a shared-memory search.
+constexpr uint32_t kBatchSegSmem = 256;
+
+template <typename Real, int VG>
+__device__ __forceinline__ void batch_direct_body(const BatchPlan &pl, uint32_t L, uint32_t cls, uint32_t blk,
+                                                  uint32_t nblk, BatchSeg *sseg, bool &waited)
+{
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    const uint32_t nchunk = pl.level_nchunk[L * kBatchClasses + cls];
+    const uint32_t nseg = pl.level_nseg[L * kBatchClasses + cls];
+    const BatchSeg *gsegs = pl.segs + ((size_t)L * kBatchClasses + cls) * pl.seg_stride;
+    const bool staged = nseg <= kBatchSegSmem;
+    if (staged)
+        for (uint32_t i = threadIdx.x; i < nseg; i += blockDim.x) sseg[i] = gsegs[i];
+    __syncthreads();
+    const BatchSeg *segs = staged ? sseg : gsegs;
+    for (uint32_t ch = blk * 4u + w; ch < nchunk; ch += nblk * 4u) {
+        const uint32_t k = upper_index(nseg, ch, [&](uint32_t m) { return segs[m].chunk_begin; });
+        const BatchSeg &sg = segs[k];
+        LevelArgs p = {};
+        p.psi = sg.psi;
+        p.iso = sg.iso;
+        p.G = sg.G;
+        p.vg = VG;
+        p.vmagic = sg.vmagic;
+        const uint32_t gpv = p.G / VG;
+        const uint32_t task = (ch - sg.chunk_begin) * 32u + lane;
+        const uint32_t itl = gpv == 1u ? task : __umulhi(task, p.vmagic);
+        const uint32_t g = (task - itl * gpv) * VG;
+        RegRecord<Real> R;
+        load_record((const CompactRecord<Real> *)sg.rec + itl, R);
+        const bool live = R.u(0) != kSentinel;
+        PairIn<Real, VG> in;
+        if (live) pair_load_source<Real, VG>(p, R, g, in);
+        if (!waited) {
+            pdl_wait_prerequisites();
+            waited = true;
+        }
+        if (live) {
+            pair_load_upwind<Real, VG, false>(p, R, g, in);
+            pair_solve_store_any<Real, VG>(p, R, g, in);
+        }
+    }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(128)
+batch_direct_level_kernel(const BatchSlot *__restrict__ slots, BatchPlan pl, uint32_t L, BatchCuts cut)
+{
+    __shared__ BatchSeg sseg[kBatchSegSmem];
+    pdl_launch_dependents();
+    bool waited = false;
+    const uint32_t b = blockIdx.x;
+    if (b < cut.c[1]) {
+        batch_direct_body<Real, 1>(pl, L, 0, b, cut.c[1], sseg, waited);
+    } else if (b < cut.c[2]) {
+        batch_direct_body<Real, 2>(pl, L, 1, b - cut.c[1], cut.c[2] - cut.c[1], sseg, waited);
+    } else if constexpr (sizeof(Real) == 4) {
+        batch_direct_body<Real, 4>(pl, L, 2, b - cut.c[2], cut.c[3] - cut.c[2], sseg, waited);
+    }
+    if (!waited) pdl_wait_prerequisites();
+    (void)slots;
 }
 
 // One global level of the batched sweep, 4 warps per block, IPW items per

@@ -149,7 +149,8 @@ template <>
 cudaError_t launch_batch_level<double>(int ipw, const BatchSlot *slots, const BatchPlan &pl, uint32_t level,
                                        const BatchCuts &cut, cudaStream_t s)
 {
-    const void *fn = ipw == 8    ? (const void *)batch_level_kernel<double, 8>
+    const void *fn = ipw == 0    ? (const void *)batch_direct_level_kernel<double>
+                     : ipw == 8  ? (const void *)batch_level_kernel<double, 8>
                      : ipw == 16 ? (const void *)batch_level_kernel<double, 16>
                      : ipw == 32 ? (const void *)batch_level_kernel<double, 32>
                                  : nullptr;
@@ -158,13 +159,14 @@ cudaError_t launch_batch_level<double>(int ipw, const BatchSlot *slots, const Ba
 }
 
 cudaError_t launch_batch_plan(int ipw, const BatchSlot *slots, uint32_t n_slots, uint32_t max_levels,
-                              const BatchPlan &pl, cudaStream_t s)
+                              uint32_t rec_bytes, const BatchPlan &pl, cudaStream_t s)
 {
     const dim3 grid(max_levels + 1), block(kBatchPlanThreads);
     switch (ipw) {
-    case 8: batch_plan_kernel<8><<<grid, block, 0, s>>>(slots, n_slots, max_levels, pl); break;
-    case 16: batch_plan_kernel<16><<<grid, block, 0, s>>>(slots, n_slots, max_levels, pl); break;
-    case 32: batch_plan_kernel<32><<<grid, block, 0, s>>>(slots, n_slots, max_levels, pl); break;
+    case 0: batch_plan_kernel<0><<<grid, block, 0, s>>>(slots, n_slots, max_levels, rec_bytes, pl); break;
+    case 8: batch_plan_kernel<8><<<grid, block, 0, s>>>(slots, n_slots, max_levels, rec_bytes, pl); break;
+    case 16: batch_plan_kernel<16><<<grid, block, 0, s>>>(slots, n_slots, max_levels, rec_bytes, pl); break;
+    case 32: batch_plan_kernel<32><<<grid, block, 0, s>>>(slots, n_slots, max_levels, rec_bytes, pl); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -32,10 +32,17 @@ struct alignas(16) BatchSlot {
     uint32_t A, G, vg, vmagic, n_levels, op, active, accept;
 };
 
-struct BatchSeg {
-    uint64_t item_begin;   // first record of the member's level
+// One member's items at one level, with what a warp needs to sweep them
+// (resolved by the plan kernel, so a warp reads one segment and nothing else).
+struct alignas(16) BatchSeg {
+    const void *rec;       // the member's record of the level's first item
+    void *psi;             // the member's psi (pass precision)
+    const void *iso;       // the member's total source (pass precision)
+    uint64_t item_begin;   // first item of the member's level
     uint32_t slot;
     uint32_t chunk_begin;  // first chunk of this segment within the level
+    uint32_t G;
+    uint32_t vmagic;
 };
 
 // Members are split by vector width (groups per psi-row access): class 0
@@ -62,8 +69,9 @@ struct BatchPlan {
 // Launchers (batch_ops.cu: double and the streaming kernels, compiled with
 // -fmad=false; batch_f32.cu: the float level kernel).  `grid` is the block
 // count of the grid-stride kernels.
+// rec_bytes: size of one record of the pass's kernel (full or compact).
 cudaError_t launch_batch_plan(int ipw, const BatchSlot *slots, uint32_t n_slots, uint32_t max_levels,
-                              const BatchPlan &pl, cudaStream_t s);
+                              uint32_t rec_bytes, const BatchPlan &pl, cudaStream_t s);
 cudaError_t launch_batch_accept(const BatchSlot *slots, const BatchPlan &pl, unsigned grid, cudaStream_t s);
 cudaError_t launch_batch_scatter(const BatchSlot *slots, const BatchPlan &pl, unsigned grid, cudaStream_t s);
 cudaError_t launch_batch_psi_to_phi(bool fp32, const BatchSlot *slots, const BatchPlan &pl, unsigned grid,

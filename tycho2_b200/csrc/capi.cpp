@@ -515,9 +515,9 @@ int tycho_batch_timing(const tycho_batch *b, double *ms, int *passes, double *up
     return TYCHO_OK;
 }
 
-uint64_t tycho_footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, int mixed)
+uint64_t tycho_footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, int mixed, int compact)
 {
-    return tycho::footprint_bytes(n_cells, sn_order, n_groups, mixed != 0);
+    return tycho::footprint_bytes(n_cells, sn_order, n_groups, mixed != 0, compact != 0);
 }
 
 int tycho_server_create(const tycho_server_opts *o, tycho_server **out)

@@ -80,7 +80,12 @@ cudaError_t record_dataflow_blocks_per_sm(int ipw, int vg, int *blocks);
 // vector), `bs` threads per block (64, 128 or 256).
 template <typename Real>
 cudaError_t launch_direct_level(int bs, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
-                                cudaStream_t s);
+                                cudaStream_t s, bool compact);
+// Compact records (64 B per item for float, 96 B for double): the inputs of
+// each item's matrix, from which the direct kernels rebuild its factors.
+constexpr size_t compact_record_bytes(bool fp32) { return fp32 ? 64 : 96; }
+template <typename Real>
+cudaError_t launch_compact_records(const LevelArgs &p, uint64_t n, void *rec, cudaStream_t s);
 // Persistent levels: one cooperative launch, a bounded grid barrier between
 // levels (level_off: device copy of the n_levels + 1 level offsets).
 template <typename Real>

@@ -8,7 +8,7 @@
 
 namespace tycho {
 
-uint64_t footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, bool fp32)
+uint64_t footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, bool fp32, bool compact)
 {
     const uint64_t A = 2ull * sn_order * sn_order;
     // level padding adds at most 31 items per level; levels stay below 16 n
@@ -18,7 +18,7 @@ uint64_t footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, bool fp32
     uint64_t b = items * 4 * G * 8;                 // psi (FP64-sized; the FP32 sweep shares it)
     b += items * (32 + (fp32 ? 16 : 0));            // per-item face terms
     b += items * (4 + 4);                           // item list, completion epochs
-    b += items * (256 + (fp32 ? 128 : 0));          // records
+    b += items * (compact ? 96 + (fp32 ? 64 : 0) : 256 + (fp32 ? 128 : 0));  // records
     b += n_cells * (16 + 4 + 24 + 12 + 8 + 8 + 8);  // adjacency, maps, cell terms, sigma, levels
     b += phi * (7 + (fp32 ? 4 : 0));                // phi, iso, r, tmp, (FP32 iso, batch r/d/k)
     return b + (b >> 5) + (8ull << 20);             // allocator rounding
@@ -71,7 +71,7 @@ int Server::submit(const MeshTables &t, int sn, int G, const double *sigma_t, co
     if (q_iso) r->q.assign(q_iso, q_iso + nc * 4 * (size_t)G);
     r->arrival = arrival;
     r->phi_out = phi_out;
-    r->footprint = footprint_bytes(nc, sn, G, o_.solve.method == 2);
+    r->footprint = footprint_bytes(nc, sn, G, o_.solve.method == 2, o_.ipw32 == 0 && o_.ipw64 == 0);
     id = r->id;
     reqs_.push_back(std::move(r));
     return kOk;
@@ -117,8 +117,8 @@ void Server::worker()
                                        r->scatter.empty() ? nullptr : r->scatter.data(), err);
         if (s == kOk && !r->q.empty()) s = sw->set_source(1, r->q.data(), err);
         Sweeper::DeviceView v;
-        if (s == kOk) s = sw->device_view(0, v, err);
-        if (s == kOk && so.fp32) s = sw->device_view(1, v, err);
+        if (s == kOk) s = sw->device_view(0, v, err, o_.ipw64 == 0);
+        if (s == kOk && so.fp32) s = sw->device_view(1, v, err, o_.ipw32 == 0);
         {
             std::lock_guard<std::mutex> lk(mu_);
             r->status = s;

@@ -25,13 +25,14 @@ struct ServerOptions {
     int device = 0;
     double budget_bytes = 150e9;  // device memory the resident requests may hold
     int setup_threads = 2;        // host threads building sweepers
-    int ipw32 = 16, ipw64 = 16;   // batch level kernels: items per warp
+    int ipw32 = 0, ipw64 = 0;     // batch level kernels: items per warp (0 = direct, compact records)
     BatchOptions solve;           // method 0 FP64 source iteration, 2 mixed
 };
 
 // Device bytes one resident request holds (sweeper + batch vectors), an
-// upper estimate made before anything is allocated.
-uint64_t footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, bool fp32);
+// upper estimate made before anything is allocated; compact: the batch runs
+// the direct kernels on compact records.
+uint64_t footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, bool fp32, bool compact);
 
 class Server {
 public:

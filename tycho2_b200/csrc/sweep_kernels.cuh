@@ -65,6 +65,9 @@ __device__ __forceinline__ Real over12(Real x)
 }
 
 template <typename Real>
+__device__ __forceinline__ void item_lu(ItemFactor<Real> &F, Real d1, Real d2, const bool (&out)[4]);
+
+template <typename Real>
 __device__ __forceinline__ void item_setup(const LevelArgs &p, uint64_t it, uint32_t ca, ItemFactor<Real> &F)
 {
     using R4 = typename Vec4Of<Real>::type;
@@ -80,11 +83,22 @@ __device__ __forceinline__ void item_setup(const LevelArgs &p, uint64_t it, uint
     const Real d1 = ck[1], d2 = ck[2];
 
     // Face terms A_f/12 and 2 A_f/12 with A_f = area * omega.n.
+    bool out[4];
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
         F.t1[f] = over12(F.ab[f]);
         F.t2[f] = over12(Real(2) * F.ab[f]);
+        out[f] = F.ab[f] > Real(0);
     }
+    item_lu(F, d1, d2, out);
+}
+
+// The matrix of one (cell, angle) item from its face terms t1, t2 and the
+// volume terms d1 = sigma_t V/20, d2 = 2 sigma_t V/20 (out[f]: face f is
+// outgoing), and its LU factors.
+template <typename Real>
+__device__ __forceinline__ void item_lu(ItemFactor<Real> &F, Real d1, Real d2, const bool (&out)[4])
+{
     // Streaming + collision (volume integrals), then outgoing-face terms in
     // increasing face order.
     Real M[4][4];
@@ -94,7 +108,7 @@ __device__ __forceinline__ void item_setup(const LevelArgs &p, uint64_t it, uint
         for (int j = 0; j < 4; ++j) M[i][j] = F.t1[i] + (i == j ? d2 : d1);
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-        if (F.ab[f] > Real(0)) {
+        if (out[f]) {
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll

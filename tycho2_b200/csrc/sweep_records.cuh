@@ -69,6 +69,47 @@ __global__ void item_record_kernel(const LevelArgs p, uint64_t n, ItemRecord<Rea
     out[it] = r;
 }
 
+// Compact record (64 B float, 96 B double): the inputs of the item's matrix
+// instead of its factors -- t1[f] = A_f/12 (f[0..3]), vs20 = V/20 (f[4]),
+// d1 = sigma_t V/20 (f[5]), d2 = 2 sigma_t V/20 (f[6]) -- and the same
+// topology words as ItemRecord.  The loader rebuilds the LU factors with
+// item_lu (the arithmetic of item_setup: t2 = 2 t1 exactly, a face is
+// outgoing iff t1 > 0), so FP64 results stay bit-identical.
+template <typename Real>
+struct alignas(16) CompactRecord {
+    Real f[7];
+    uint32_t u[7];
+    uint32_t pad[(sizeof(Real) == 8 ? 24 : 16) - 7 * (sizeof(Real) / 4) - 7];
+};
+static_assert(sizeof(CompactRecord<float>) == 64, "float compact record is 64 bytes");
+static_assert(sizeof(CompactRecord<double>) == 96, "double compact record is 96 bytes");
+
+template <typename Real>
+__global__ void compact_record_kernel(const LevelArgs p, uint64_t n, CompactRecord<Real> *out)
+{
+    const uint64_t it = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= n) return;
+    const uint32_t ca = p.items[it];
+    CompactRecord<Real> r;
+    if (ca == kSentinel) {
+        for (int i = 0; i < 7; ++i) r.f[i] = Real(0);
+        r.u[0] = kSentinel; r.u[1] = 0; r.u[2] = 0;
+        for (int f = 0; f < 4; ++f) r.u[3 + f] = kNoRow;
+    } else {
+        ItemFactor<Real> F;
+        item_setup(p, it, ca, F);
+        const Real *ck = reinterpret_cast<const Real *>(p.cellk) + 3 * (size_t)F.c;
+        for (int f = 0; f < 4; ++f) r.f[f] = F.t1[f];
+        r.f[4] = F.vs20;
+        r.f[5] = ck[1];
+        r.f[6] = ck[2];
+        r.u[0] = F.c; r.u[1] = ca; r.u[2] = F.nmap;
+        for (int f = 0; f < 4; ++f) r.u[3 + f] = F.adj[f] < 0 ? kNoRow : (uint32_t)F.adj[f] * p.A + F.a;
+    }
+    for (unsigned i = 0; i < sizeof(r.pad) / 4; ++i) r.pad[i] = 0;
+    out[it] = r;
+}
+
 // Field-major tile of IPW records in shared memory.
 template <typename Real, int IPW>
 struct RecordTile {
@@ -162,6 +203,37 @@ __device__ __forceinline__ void load_record(const ItemRecord<Real> *__restrict__
     for (int k = 0; k < 21; ++k) r.fv[k] = fr[k];
 #pragma unroll
     for (int k = 0; k < 7; ++k) r.uv[k] = ur[k];
+}
+
+// A compact record into registers, with the factors rebuilt.
+template <typename Real>
+__device__ __forceinline__ void load_record(const CompactRecord<Real> *__restrict__ src, RegRecord<Real> &r)
+{
+    constexpr int N = sizeof(CompactRecord<Real>) / 16;
+    uint4 v[N];
+    const uint4 *s = reinterpret_cast<const uint4 *>(src);
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = __ldg(s + i);
+    const Real *fr = reinterpret_cast<const Real *>(v);
+    const uint32_t *ur = reinterpret_cast<const uint32_t *>(reinterpret_cast<const char *>(v) + 7 * sizeof(Real));
+#pragma unroll
+    for (int k = 0; k < 7; ++k) r.uv[k] = ur[k];
+    if (r.uv[0] == kSentinel) return;
+    ItemFactor<Real> F;
+    bool out[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        F.t1[f] = fr[f];
+        F.t2[f] = Real(2) * fr[f];
+        out[f] = fr[f] > Real(0);
+    }
+    item_lu(F, fr[5], fr[6], out);
+#pragma unroll
+    for (int f = 0; f < 4; ++f) r.fv[f] = F.t1[f];
+    r.fv[4] = fr[4]; r.fv[5] = F.r0; r.fv[6] = F.u01; r.fv[7] = F.u02; r.fv[8] = F.u03;
+    r.fv[9] = F.l1; r.fv[10] = F.l2; r.fv[11] = F.l3; r.fv[12] = F.r1; r.fv[13] = F.u12;
+    r.fv[14] = F.u13; r.fv[15] = F.a21; r.fv[16] = F.a31; r.fv[17] = F.r2; r.fv[18] = F.u23;
+    r.fv[19] = F.b32; r.fv[20] = F.c33;
 }
 
 // All the inputs of one (item, VG groups) task, loaded before any arithmetic.
@@ -295,6 +367,79 @@ __device__ __forceinline__ void pair_solve_store_v(const LevelArgs &p, const Vie
     for (int v = 0; v < 4; ++v) gv_store(out + v * p.G, res[v]);
 }
 
+// FP32 with an even group vector: the same arithmetic on pairs of groups
+// with Blackwell's packed FP32x2 add / multiply / fused multiply-add (half
+// the arithmetic instructions).  The source sum is reassociated as
+// vs20 * ((q0 + q1) + (q2 + q3) + q_v); FP32 results are checked by
+// tolerance, the FP64 path above keeps the reference's order.
+template <int VG, typename View>
+__device__ __forceinline__ void pair_solve_store_f32x2(const LevelArgs &p, const View &R, uint32_t g,
+                                                       const PairIn<float, VG> &in)
+{
+    static_assert(VG % 2 == 0, "pairs of groups");
+    float res[4][VG];
+    const float vs = R.f(4);
+    const float2 vs2 = make_float2(vs, vs);
+#pragma unroll
+    for (int e = 0; e < VG; e += 2) {
+        float2 q[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) q[v] = make_float2(in.q[v][e], in.q[v][e + 1]);
+        const float2 s = __fadd2_rn(__fadd2_rn(q[0], q[1]), __fadd2_rn(q[2], q[3]));
+        float2 b[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) b[v] = __fmul2_rn(vs2, __fadd2_rn(s, q[v]));
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            const float t1 = R.f(f);
+            if (t1 < 0.0f) {
+                const float2 m1 = make_float2(-t1, -t1), m2 = make_float2(-2.0f * t1, -2.0f * t1);
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    if (r == f) continue;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const int j = k < f ? k : k + 1;
+                        const float2 pn = make_float2(in.pn[f][k][e], in.pn[f][k][e + 1]);
+                        b[r] = __ffma2_rn(r == j ? m2 : m1, pn, b[r]);
+                    }
+                }
+            }
+        }
+        auto sp = [](float x) { return make_float2(x, x); };
+        b[0] = __fmul2_rn(b[0], sp(R.f(5)));
+        b[1] = __ffma2_rn(sp(-R.f(9)), b[0], b[1]);
+        b[2] = __ffma2_rn(sp(-R.f(10)), b[0], b[2]);
+        b[3] = __ffma2_rn(sp(-R.f(11)), b[0], b[3]);
+        b[1] = __fmul2_rn(b[1], sp(R.f(12)));
+        b[2] = __ffma2_rn(sp(-R.f(15)), b[1], b[2]);
+        b[3] = __ffma2_rn(sp(-R.f(16)), b[1], b[3]);
+        b[2] = __fmul2_rn(b[2], sp(R.f(17)));
+        b[3] = __ffma2_rn(sp(-R.f(19)), b[2], b[3]);
+        b[3] = __fmul2_rn(b[3], sp(__frcp_rn(R.f(20))));
+        b[2] = __ffma2_rn(sp(-R.f(18)), b[3], b[2]);
+        b[1] = __ffma2_rn(sp(-R.f(13)), b[2], __ffma2_rn(sp(-R.f(14)), b[3], b[1]));
+        b[0] = __ffma2_rn(sp(-R.f(6)), b[1], __ffma2_rn(sp(-R.f(7)), b[2], __ffma2_rn(sp(-R.f(8)), b[3], b[0])));
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            res[v][e] = b[v].x;
+            res[v][e + 1] = b[v].y;
+        }
+    }
+    float *__restrict__ out = reinterpret_cast<float *>(p.psi) + (size_t)R.u(1) * 4 * p.G + g;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) gv_store(out + v * p.G, res[v]);
+}
+
+// The arithmetic of one task: packed FP32x2 where it applies.
+template <typename Real, int VG, typename View>
+__device__ __forceinline__ void pair_solve_store_any(const LevelArgs &p, const View &R, uint32_t g,
+                                                     const PairIn<Real, VG> &in)
+{
+    if constexpr (std::is_same<Real, float>::value && VG % 2 == 0) pair_solve_store_f32x2<VG>(p, R, g, in);
+    else pair_solve_store_v<Real, VG>(p, R, g, in);
+}
+
 template <typename Real, int IPW, int VG>
 __device__ __forceinline__ void pair_solve_store(const LevelArgs &p, const RecordTile<Real, IPW> &T, uint32_t i,
                                                  uint32_t g, const PairIn<Real, VG> &in)
@@ -370,10 +515,9 @@ sweep_record_level_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict_
 // are read after it.  No shared memory.  Tasks of a level: item t / (G/VG),
 // groups VG * (t % (G/VG)) and on (the host keeps a level's task count
 // below 2^26 so that the multiply-high division is exact).
-template <typename Real, int VG, int BS>
+template <typename Real, int VG, int BS, typename Rec>
 __global__ void __launch_bounds__(BS)
-sweep_direct_level_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict__ rec, const uint64_t begin,
-                          const uint64_t end)
+sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const uint64_t begin, const uint64_t end)
 {
     pdl_launch_dependents();
     const uint32_t gpv = p.G / VG;
@@ -392,7 +536,7 @@ sweep_direct_level_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict_
     pdl_wait_prerequisites();
     if (!live) return;
     pair_load_upwind<Real, VG, false>(p, R, g, in);
-    pair_solve_store_v<Real, VG>(p, R, g, in);
+    pair_solve_store_any<Real, VG>(p, R, g, in);
 }
 
 // Dataflow schedule: persistent warps take IPW-item chunks round-robin; lane
@@ -588,31 +732,39 @@ cudaError_t launch_item_records(const LevelArgs &p, uint64_t n, void *out, cudaS
     return cudaGetLastError();
 }
 
-template <typename Real, int BS>
+template <typename Real, int BS, typename Rec>
 static const void *direct_fn_vg(int vg)
 {
     switch (vg) {
-    case 1: return (const void *)sweep_direct_level_kernel<Real, 1, BS>;
-    case 2: return (const void *)sweep_direct_level_kernel<Real, 2, BS>;
+    case 1: return (const void *)sweep_direct_level_kernel<Real, 1, BS, Rec>;
+    case 2: return (const void *)sweep_direct_level_kernel<Real, 2, BS, Rec>;
     case 4:
-        if constexpr (sizeof(Real) == 4) return (const void *)sweep_direct_level_kernel<Real, 4, BS>;
+        if constexpr (sizeof(Real) == 4) return (const void *)sweep_direct_level_kernel<Real, 4, BS, Rec>;
         else return nullptr;
     default: return nullptr;
     }
 }
 
-// Direct variant: knob = threads per block (64, 128 or 256).
+template <typename Real, typename Rec>
+static const void *direct_fn(int bs, int vg)
+{
+    return bs == 64 ? direct_fn_vg<Real, 64, Rec>(vg)
+           : bs == 128 ? direct_fn_vg<Real, 128, Rec>(vg)
+           : bs == 256 ? direct_fn_vg<Real, 256, Rec>(vg)
+                       : nullptr;
+}
+
+// Direct variant: knob = threads per block (64, 128 or 256); compact picks
+// the compact record format.
 template <typename Real>
 cudaError_t launch_direct_level(int bs, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
-                                cudaStream_t s)
+                                cudaStream_t s, bool compact)
 {
     if (end <= begin) return cudaSuccess;
     const uint64_t tasks = (end - begin) * (p.G / p.vg);
     if (tasks >= (1ull << 26)) return cudaErrorInvalidValue;
-    const void *fn = bs == 64    ? direct_fn_vg<Real, 64>((int)p.vg)
-                     : bs == 128 ? direct_fn_vg<Real, 128>((int)p.vg)
-                     : bs == 256 ? direct_fn_vg<Real, 256>((int)p.vg)
-                                 : nullptr;
+    const void *fn = compact ? direct_fn<Real, CompactRecord<Real>>(bs, (int)p.vg)
+                             : direct_fn<Real, ItemRecord<Real>>(bs, (int)p.vg);
     if (!fn) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)((tasks + bs - 1) / bs));
@@ -623,9 +775,17 @@ cudaError_t launch_direct_level(int bs, const LevelArgs &p, const void *rec, uin
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const ItemRecord<Real> *r = (const ItemRecord<Real> *)rec;
+    const void *r = rec;
     void *args[] = {(void *)&p, (void *)&r, (void *)&begin, (void *)&end};
     return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+template <typename Real>
+cudaError_t launch_compact_records(const LevelArgs &p, uint64_t n, void *out, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    compact_record_kernel<Real><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(p, n, (CompactRecord<Real> *)out);
+    return cudaGetLastError();
 }
 
 // knob = items per warp (8, 16 or 32); one launch over items [begin, end).

@@ -57,7 +57,7 @@ Sweeper::~Sweeper()
     void *bufs[] = {d_items_, d_abar64_, d_abar32_, d_adj_, d_nbrmap_, d_cellk64_, d_cellk32_,
                     d_w_, d_sigs_, d_scat_, d_qiso_, d_qang_, d_src_, d_iso_, d_iso32_, d_psi_,
                     d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_, d_done_, d_ctl_, d_rec_[0], d_rec_[1],
-                    d_level_off_, d_barrier_};
+                    d_level_off_, d_barrier_, d_crec_[0], d_crec_[1]};
     for (void *b : bufs)
         if (b) cudaFree(b);
     reducer_free(red_);
@@ -189,22 +189,23 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
         err = "persistent levels in FP64: items per warp must be 8 or 16";
         return kErrArg;
     }
-    if (variant == 3 && (schedule != 1 || (knob != 64 && knob != 128 && knob != 256))) {
-        err = "direct record variant: level schedule only, 64, 128 or 256 threads per block";
+    if (variant >= 3 && (schedule != 1 || (knob != 64 && knob != 128 && knob != 256))) {
+        err = "direct record variants: level schedule only, 64, 128 or 256 threads per block";
         return kErrArg;
     }
-    if (variant < 0 || variant > 3) {
-        err = "variant must be 0 (item-parallel), 1 (warp tiles), 2 (records) or 3 (direct records)";
+    if (variant < 0 || variant > 4) {
+        err = "variant must be 0 (item-parallel), 1 (warp tiles), 2 (records), 3 (direct records) or 4 "
+              "(direct compact records)";
         return kErrArg;
     }
-    if (variant >= 2) TY_CHECK(ensure_records(prec, false, err));
+    if (variant >= 2) TY_CHECK(ensure_records(prec, false, err, variant == 4));
     int sms = 0, per_sm = 0;
     TY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
     if (variant == 0)
         TY_CUDA(prec ? dataflow_blocks_per_sm<float>(knob, &per_sm) : dataflow_blocks_per_sm<double>(knob, &per_sm));
-    else if (variant == 1)
-        TY_CUDA(prec ? tile_dataflow_blocks_per_sm<float>(knob, &per_sm)
-                     : tile_dataflow_blocks_per_sm<double>(knob, &per_sm));
+    else if (variant == 1 || variant == 4)  // compact: the no-alloc sweep runs the 4-warp tile kernel
+        TY_CUDA(prec ? tile_dataflow_blocks_per_sm<float>(variant == 4 ? 4 : knob, &per_sm)
+                     : tile_dataflow_blocks_per_sm<double>(variant == 4 ? 4 : knob, &per_sm));
     else  // records; the direct variant's no-alloc sweep runs the 16-item record dataflow kernel
         TY_CUDA(prec ? record_dataflow_blocks_per_sm<float>(variant == 3 ? 16 : knob, vg, &per_sm)
                      : record_dataflow_blocks_per_sm<double>(variant == 3 ? 16 : knob, vg, &per_sm));
@@ -243,12 +244,12 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
     double best = 1e300;
     LaunchShape keep = shape_[prec ? 1 : 0];
     for (int sched = 1; sched <= 3; ++sched)
-        for (int variant = 0; variant <= 3; ++variant)
+        for (int variant = 0; variant <= 4; ++variant)
             for (int knob : {1, 2, 4, 8, 16, 32, 64, 128, 256}) {
                 if (variant == 0 && ((knob > 2 * G_ && knob > 1) || knob > 16)) continue;  // idle lanes
                 if (variant == 1 && knob > 4) continue;
                 if (variant == 2 && (knob < 8 || knob > 32)) continue;
-                if (variant == 3 && (knob < 64 || sched != 1)) continue;
+                if (variant >= 3 && (knob < 64 || sched != 1)) continue;
                 if (sched == 3 && (variant != 2 || (prec == 0 && knob == 32))) continue;
                 for (int vg : {1, 2, 4}) {
                     if (vg > 1 && (variant < 2 || G_ % vg != 0 || (vg == 4 && prec == 0))) continue;
@@ -275,9 +276,9 @@ int Sweeper::launch_dataflow_shape(int prec, const LevelArgs &p, const DataflowA
     if (sh.variant == 0)
         e = prec ? launch_dataflow<float>(sh.knob, p, df, sh.grid, s)
                  : launch_dataflow<double>(sh.knob, p, df, sh.grid, s);
-    else if (sh.variant == 1)
-        e = prec ? launch_dataflow_tile<float>(sh.knob, p, df, sh.grid, s)
-                 : launch_dataflow_tile<double>(sh.knob, p, df, sh.grid, s);
+    else if (sh.variant == 1 || sh.variant == 4)
+        e = prec ? launch_dataflow_tile<float>(sh.variant == 4 ? 4 : sh.knob, p, df, sh.grid, s)
+                 : launch_dataflow_tile<double>(sh.variant == 4 ? 4 : sh.knob, p, df, sh.grid, s);
     else {
         TY_CHECK(ensure_records(prec, true, err));
         const int ipw = sh.variant == 3 ? 16 : sh.knob;
@@ -307,14 +308,14 @@ LevelArgs Sweeper::level_args(int prec, const void *iso, const double *qang, voi
     return p;
 }
 
-int Sweeper::device_view(int prec, DeviceView &v, std::string &err)
+int Sweeper::device_view(int prec, DeviceView &v, std::string &err, bool compact)
 {
     if (prec == 1 && !fp32_) { err = "sweeper was created without the FP32 sweep"; return kErrArg; }
     if (!have_xs_) { err = "cross sections not set"; return kErrMissing; }
     TY_CUDA(cudaSetDevice(device_));
-    TY_CHECK(ensure_records(prec, true, err));
+    TY_CHECK(ensure_records(prec, true, err, compact));
     TY_CUDA(cudaStreamSynchronize(stream_));
-    v.rec = d_rec_[prec ? 1 : 0];
+    v.rec = compact ? d_crec_[prec ? 1 : 0] : d_rec_[prec ? 1 : 0];
     v.psi = d_psi_;
     v.iso = d_iso_;
     v.iso32 = d_iso32_;
@@ -332,27 +333,36 @@ int Sweeper::device_view(int prec, DeviceView &v, std::string &err)
 
 // Allocates (once) and fills (once per cross-section set) the per-item
 // records of the record variant for one precision.
-int Sweeper::ensure_records(int prec, bool need_filled, std::string &err)
+int Sweeper::ensure_records(int prec, bool need_filled, std::string &err, bool compact)
 {
     const int k = prec ? 1 : 0;
-    if (!d_rec_[k]) {
-        const size_t bytes = record_bytes(prec == 1) * sched_.items.size();
-        cudaError_t e = cudaMalloc(&d_rec_[k], bytes);
+    void *&buf = compact ? d_crec_[k] : d_rec_[k];
+    bool &valid = compact ? crec_valid_[k] : rec_valid_[k];
+    if (!buf) {
+        const size_t bytes =
+            (compact ? compact_record_bytes(prec == 1) : record_bytes(prec == 1)) * sched_.items.size();
+        cudaError_t e = cudaMalloc(&buf, bytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
-            d_rec_[k] = nullptr;
-            err = "records (" + std::to_string(bytes >> 20) + " MiB) do not fit: " + cudaGetErrorString(e);
+            buf = nullptr;
+            err = std::string(compact ? "compact records (" : "records (") + std::to_string(bytes >> 20) +
+                  " MiB) do not fit: " + cudaGetErrorString(e);
             return e == cudaErrorMemoryAllocation ? kErrOom : kErrCuda;
         }
-        rec_valid_[k] = false;
+        valid = false;
     }
-    if (!rec_valid_[k] && have_xs_) {
+    if (!valid && have_xs_) {
         const LevelArgs p = level_args(prec, nullptr, nullptr, d_psi_);
-        TY_CUDA(prec ? launch_item_records<float>(p, sched_.items.size(), d_rec_[k], stream_)
-                     : launch_item_records<double>(p, sched_.items.size(), d_rec_[k], stream_));
-        rec_valid_[k] = true;
+        const uint64_t n = sched_.items.size();
+        if (compact)
+            TY_CUDA(prec ? launch_compact_records<float>(p, n, buf, stream_)
+                         : launch_compact_records<double>(p, n, buf, stream_));
+        else
+            TY_CUDA(prec ? launch_item_records<float>(p, n, buf, stream_)
+                         : launch_item_records<double>(p, n, buf, stream_));
+        valid = true;
     }
-    if (need_filled && !rec_valid_[k]) { err = "cross sections not set"; return kErrMissing; }
+    if (need_filled && !valid) { err = "cross sections not set"; return kErrMissing; }
     return kOk;
 }
 
@@ -400,6 +410,7 @@ int Sweeper::set_cross_sections(const double *sigma_t, const double *sigma_s, co
     TY_CUDA(cudaStreamSynchronize(stream_));
     have_xs_ = true;
     rec_valid_[0] = rec_valid_[1] = false;
+    crec_valid_[0] = crec_valid_[1] = false;
     for (int k = 0; k < 2; ++k)
         if (shape_[k].variant == 2 && (k == 0 || fp32_)) TY_CHECK(ensure_records(k, true, err));
     return kOk;
@@ -460,7 +471,7 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         if (end) TY_CUDA(cudaEventRecord(end, stream_));
         return kOk;
     }
-    if (sh.variant >= 2) TY_CHECK(ensure_records(prec, true, err));
+    if (sh.variant >= 2) TY_CHECK(ensure_records(prec, true, err, sh.variant == 4));
     auto key = std::make_tuple(prec, has_iso, qang);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
@@ -479,9 +490,12 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
             else if (sh.variant == 2)
                 le = prec ? launch_level_record<float>(sh.knob, p, d_rec_[1], b, e, stream_)
                           : launch_level_record<double>(sh.knob, p, d_rec_[0], b, e, stream_);
+            else if (sh.variant == 3)
+                le = prec ? launch_direct_level<float>(sh.knob, p, d_rec_[1], b, e, stream_, false)
+                          : launch_direct_level<double>(sh.knob, p, d_rec_[0], b, e, stream_, false);
             else
-                le = prec ? launch_direct_level<float>(sh.knob, p, d_rec_[1], b, e, stream_)
-                          : launch_direct_level<double>(sh.knob, p, d_rec_[0], b, e, stream_);
+                le = prec ? launch_direct_level<float>(sh.knob, p, d_crec_[1], b, e, stream_, true)
+                          : launch_direct_level<double>(sh.knob, p, d_crec_[0], b, e, stream_, true);
         }
         cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
         TY_CUDA(le);

@@ -32,7 +32,9 @@ struct LaunchShape {
                         // 3 persistent levels (record variant only)
     int variant = 1;    // 0 item-parallel (knob = threads per item),
                         // 1 warp tiles (knob = warps per block),
-                        // 2 precomputed per-item records (knob = items per warp)
+                        // 2 precomputed per-item records (knob = items per warp),
+                        // 3 records in registers, 4 compact records in registers
+                        //   (knob = threads per block; level schedule)
     int knob = 4;
     int vg = 1;                 // records: groups per vector access of a psi row
     unsigned grid = 0;          // dataflow kernel of this variant: co-resident blocks
@@ -86,9 +88,10 @@ public:
                        cudaStream_t s, std::string &err);
 
     // Device state read by the batch driver (batch.cpp); computes the
-    // records of `prec` when stale and waits for the instance's stream.
+    // records of `prec` (compact or full) when stale and waits for the
+    // instance's stream.
     struct DeviceView {
-        const void *rec;
+        const void *rec;  // CompactRecord<Real> (compact) or ItemRecord<Real>
         void *psi;
         double *iso;
         float *iso32;
@@ -97,7 +100,7 @@ public:
         const uint64_t *level_off;
         uint32_t n_levels, vg;
     };
-    int device_view(int prec, DeviceView &v, std::string &err);
+    int device_view(int prec, DeviceView &v, std::string &err, bool compact);
     // The resident psi was written by a sweep of this precision elsewhere.
     void note_psi_precision(int prec) { last_psi_prec_ = prec; }
     uint64_t n_items() const { return sched_.items.size(); }
@@ -126,7 +129,7 @@ private:
     int ensure_krylov(int restart, std::string &err);
     // Allocates the record array of one precision; need_filled also requires
     // (and computes, when stale) its contents for the current cross sections.
-    int ensure_records(int prec, bool need_filled, std::string &err);
+    int ensure_records(int prec, bool need_filled, std::string &err, bool compact = false);
 
     MeshTables tables_;
     Quadrature quad_;
@@ -166,6 +169,9 @@ private:
     // record variant: per-item factors, [0] FP64, [1] FP32
     void *d_rec_[2] = {nullptr, nullptr};
     bool rec_valid_[2] = {false, false};
+    // compact records (direct compact variant and the batch driver)
+    void *d_crec_[2] = {nullptr, nullptr};
+    bool crec_valid_[2] = {false, false};
     // persistent-levels schedule: level offsets and the grid barrier counter
     uint64_t *d_level_off_ = nullptr;
     unsigned long long *d_barrier_ = nullptr;

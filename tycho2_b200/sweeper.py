@@ -222,12 +222,13 @@ class SweeperCuda:
         check(lib().tycho_sweeper_time_sweeps(self._h, precision, n, int(flush_l2), ptr(ms)))
         return float(ms[0]), float(ms[1])
 
-    VARIANTS = {"items": 0, "tiles": 1, "records": 2, "direct": 3}
+    VARIANTS = {"items": 0, "tiles": 1, "records": 2, "direct": 3, "compact": 4}
 
     @staticmethod
     def _shape_dict(sh):
         return {"schedule": {1: "levels", 2: "dataflow", 3: "persist"}[sh.schedule],
-                "variant": {0: "items", 1: "tiles", 2: "records", 3: "direct"}[sh.variant], "knob": sh.knob,
+                "variant": {0: "items", 1: "tiles", 2: "records", 3: "direct", 4: "compact"}[sh.variant],
+                "knob": sh.knob,
                 "vector": sh.vector}
 
     def autotune(self, precision, reps=3):
@@ -270,7 +271,7 @@ class BatchSolver:
 
     BATCH_METHODS = {"si": 0, "mixed": 2}
 
-    def __init__(self, device=0, ipw32=16, ipw64=16):
+    def __init__(self, device=0, ipw32=0, ipw64=0):
         h = C.c_void_p()
         check(lib().tycho_batch_create(device, ipw32, ipw64, C.byref(h)))
         self._h = h
@@ -323,9 +324,9 @@ class BatchSolver:
         self.close()
 
 
-def footprint_bytes(n_cells, sn_order, n_groups, mixed=True):
+def footprint_bytes(n_cells, sn_order, n_groups, mixed=True, compact=True):
     """Device bytes one resident solve request holds (tycho_footprint_bytes)."""
-    return int(lib().tycho_footprint_bytes(n_cells, sn_order, n_groups, int(mixed)))
+    return int(lib().tycho_footprint_bytes(n_cells, sn_order, n_groups, int(mixed), int(compact)))
 
 
 class SolveServer:
@@ -335,8 +336,8 @@ class SolveServer:
 
     STATES = {0: "queued", 1: "building", 2: "built", 3: "in batch", 4: "done", 5: "failed"}
 
-    def __init__(self, method="mixed", budget_bytes=150e9, device=0, setup_threads=2, ipw32=16,
-                 ipw64=16, iter_max=3000, err_max=1e-10, inner_tol=1e-4, inner_max=200, refine_max=30):
+    def __init__(self, method="mixed", budget_bytes=150e9, device=0, setup_threads=2, ipw32=0,
+                 ipw64=0, iter_max=3000, err_max=1e-10, inner_tol=1e-4, inner_max=200, refine_max=30):
         solve = _capi.BatchOpts(BatchSolver.BATCH_METHODS[method], iter_max, err_max, inner_tol,
                                 inner_max, refine_max)
         o = _capi.ServerOpts(device, float(budget_bytes), setup_threads, ipw32, ipw64, solve)
