@@ -255,7 +255,7 @@ def run_batch_leg(grp, dev, count, seed=4321):
     out, phis = {}, {}
     for method in ("si", "mixed"):
         b = ty.BatchSolver(device=dev)
-        ids = [b.add(sw, method, err_max=1e-10, iter_max=5000) for sw in sws]
+        ids = [b.add(sw, method, err_max=1e-10, iter_max=5000, inner_tol=1e-5) for sw in sws]
         grp.barrier()
         t = time.perf_counter()
         steps = 0
@@ -306,7 +306,8 @@ def run_serve_leg(grp, dev, count, rate, seed=99):
            "rate_per_s": rate * grp.world, "budget_gb": 150.0}
     phis = {}
     for method, key in (("mixed", "mixed"), ("si", "fp64")):
-        srv = ty.SolveServer(method=method, budget_bytes=150e9, device=dev, setup_threads=4, err_max=1e-10)
+        srv = ty.SolveServer(method=method, budget_bytes=150e9, device=dev, setup_threads=4, err_max=1e-10,
+                             inner_tol=1e-5)
         ids = [srv.submit(m, p["sn"], p["groups"], st, ss, mat, q, arrival=float(a))
                for p, (m, st, ss, mat, q), a in zip(params, probs, arrivals)]
         grp.barrier()
@@ -421,6 +422,8 @@ def run_b200(args):
                "seconds_per_step": dt}
         del src_t, psi_t
 
+    # the batch and serve legs need the device memory of this instance
+    sw.close()
     batch = serve = None
     if not args.no_batch:
         try:
@@ -474,7 +477,6 @@ def run_b200(args):
             "wall_check_s": wall32,
         }
         print(json.dumps(line), flush=True)
-    sw.close()
     grp.close()
 
 

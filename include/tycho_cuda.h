@@ -129,7 +129,8 @@ typedef struct tycho_sweeper_opts {
     int fp32;       /* nonzero: also prepare the FP32 sweep (mixed precision) */
     int tpi64;      /* threads per (cell,angle) item of the FP64 sweep, 0 = auto */
     int tpi32;      /* same for the FP32 sweep, 0 = auto */
-    int schedule;   /* 0 = auto (dataflow), 1 = one launch per wavefront level,
+    int schedule;   /* 0 = auto (one launch per level, compact records in
+                       registers), 1 = one launch per wavefront level,
                        2 = one persistent dataflow launch per sweep */
 } tycho_sweeper_opts;
 

@@ -207,6 +207,38 @@ int Batch::ensure_capacity(std::string &err)
     return kOk;
 }
 
+void Batch::assign_shifts()
+{
+    std::vector<double> work(max_levels_, 0.0);
+    std::vector<size_t> order(members_.size());
+    std::vector<double> total(members_.size(), 0.0);
+    for (size_t i = 0; i < members_.size(); ++i) {
+        order[i] = i;
+        const auto &lo = members_[i].sw->schedule().level_offset;
+        total[i] = (double)(lo.back() - lo.front()) * members_[i].sw->n_groups();
+    }
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return total[a] > total[b]; });
+    for (size_t i : order) {
+        Member &m = members_[i];
+        const auto &lo = m.sw->schedule().level_offset;
+        const uint32_t n = m.v[0].n_levels;
+        const double G = (double)m.sw->n_groups();
+        uint32_t best_o = 0;
+        double best = 1e300;
+        for (uint32_t o = 0; o + n <= max_levels_; ++o) {
+            double peak = 0.0;
+            for (uint32_t l = 0; l < n && peak < best; ++l)
+                peak = std::max(peak, work[o + l] + (double)(lo[l + 1] - lo[l]) * G);
+            if (peak < best) {
+                best = peak;
+                best_o = o;
+            }
+        }
+        m.shift = best_o;
+        for (uint32_t l = 0; l < n; ++l) work[best_o + l] += (double)(lo[l + 1] - lo[l]) * G;
+    }
+}
+
 void Batch::fill_slot(int prec, const Member &m, BatchSlot &s) const
 {
     const Sweeper::DeviceView &v = m.v[prec];
@@ -225,6 +257,7 @@ void Batch::fill_slot(int prec, const Member &m, BatchSlot &s) const
     s.vg = v.vg;
     s.vmagic = magic(s.G / s.vg);
     s.n_levels = v.n_levels;
+    s.level_shift = m.shift;
     s.active = 0;
     if (prec == 0 && m.state == kRunSI) {
         s.active = 1;
@@ -255,6 +288,7 @@ void Batch::fill_slot(int prec, const Member &m, BatchSlot &s) const
 
 int Batch::build_graph(int prec, std::string &err)
 {
+    if (!graph_[0] && !graph_[1]) assign_shifts();  // the member set changed
     const int ipw = ipw_[prec];
     const uint32_t n = (uint32_t)members_.size();
     // Blocks per level and class: enough for every member's chunks at once
@@ -264,8 +298,8 @@ int Batch::build_graph(int prec, std::string &err)
         uint64_t chunks[kBatchClasses] = {0, 0, 0};
         for (const auto &m : members_) {
             const auto &lo = m.sw->schedule().level_offset;
-            if (L >= m.v[0].n_levels) continue;
-            const uint64_t items = lo[L + 1] - lo[L];
+            if (L < m.shift || L - m.shift >= m.v[0].n_levels) continue;
+            const uint64_t items = lo[L - m.shift + 1] - lo[L - m.shift];
             const uint32_t vg = m.v[prec].vg;
             chunks[vg == 4 ? 2 : vg == 2 ? 1 : 0] +=
                 ipw ? items / ipw : items / 32 * ((uint64_t)m.sw->n_groups() / vg);
@@ -300,12 +334,12 @@ int Batch::pass(int prec, std::string &err)
 {
     const size_t n = members_.size();
     bool any = false;
-    for (size_t j = 0; j < n; ++j) {
-        fill_slot(prec, members_[j], h_slots_[prec][j]);
-        any = any || h_slots_[prec][j].active;
-    }
+    for (const auto &m : members_)
+        any = any || (prec == 0 ? m.state == kRunSI || m.state == kRunOuter : m.state == kRunInner);
     if (!any) return kOk;
+    // the graph (and with it the members' level shifts) before the slot table
     if (!graph_[prec]) TB_CHECK(build_graph(prec, err));
+    for (size_t j = 0; j < n; ++j) fill_slot(prec, members_[j], h_slots_[prec][j]);
     TB_CUDA(cudaMemcpyAsync(d_slots_[prec], h_slots_[prec], sizeof(BatchSlot) * n, cudaMemcpyHostToDevice, stream_));
     TB_CUDA(cudaEventRecord(ev_[2 * prec], stream_));
     TB_CUDA(cudaGraphLaunch(graph_[prec], stream_));

@@ -27,7 +27,7 @@ struct BatchOptions {
     int method = 2;           // 0 FP64 source iteration, 2 mixed (FP32 inner SI, FP64 refinement)
     int iter_max = 1000;      // sweeps of the solve (inner FP32 sweeps count for mixed)
     double err_max = 1e-10;   // L1 relative change of phi (SourceIteration.cc:167-175)
-    double inner_tol = 1e-4;  // inner FP32 iteration: L1 relative change of the correction
+    double inner_tol = 1e-5;  // inner FP32 iteration: L1 relative change of the correction
     int inner_max = 200;
     int refine_max = 30;
 };
@@ -71,7 +71,12 @@ private:
         bool accept = false;
         int inner_its = 0;
         uint64_t updates = 0;                             // per sweep
+        uint32_t shift = 0;                               // global level of the member's level 0
     };
+    // Staggers the members' level ranges over the global levels so that the
+    // work per global level is even (small members fill the levels where
+    // only the deepest ones have work).
+    void assign_shifts();
     int pass(int prec, std::string &err);
     int build_graph(int prec, std::string &err);
     void fill_slot(int prec, const Member &m, BatchSlot &s) const;

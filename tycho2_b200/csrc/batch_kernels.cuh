@@ -71,9 +71,11 @@ batch_plan_kernel(const BatchSlot *__restrict__ slots, uint32_t n_slots, uint32_
                 const uint32_t j = base + threadIdx.x;
                 uint32_t nch = 0;
                 uint64_t lo = 0;
-                if (j < n_slots && slots[j].active && L < slots[j].n_levels && batch_class(slots[j].vg) == cls) {
-                    lo = slots[j].level_off[L];
-                    const uint64_t items = slots[j].level_off[L + 1] - lo;
+                const uint32_t sh = j < n_slots ? slots[j].level_shift : 0u;
+                if (j < n_slots && slots[j].active && L >= sh && L - sh < slots[j].n_levels &&
+                    batch_class(slots[j].vg) == cls) {
+                    lo = slots[j].level_off[L - sh];
+                    const uint64_t items = slots[j].level_off[L - sh + 1] - lo;
                     // IPW items per chunk; IPW == 0 (direct kernel): 32 (item, group vector) tasks
                     nch = IPW ? (uint32_t)(items / IPW) : (uint32_t)(items / 32 * (slots[j].G / slots[j].vg));
                 }

@@ -30,6 +30,7 @@ struct alignas(16) BatchSlot {
     const uint64_t *level_off;  // member's level offsets (n_levels + 1)
     uint64_t nc;
     uint32_t A, G, vg, vmagic, n_levels, op, active, accept;
+    uint32_t level_shift;  // the member's level l runs at global level level_shift + l
 };
 
 // One member's items at one level, with what a warp needs to sweep them

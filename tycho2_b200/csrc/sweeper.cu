@@ -147,18 +147,23 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     TY_CUDA(cudaMemsetAsync(d_ctl_, 0, sizeof(uint32_t) * 8, stream_));
     TY_CUDA(upload(d_level_off_, sched_.level_offset.data(), sched_.level_offset.size(), stream_));
     TY_CUDA(cudaMalloc(&d_barrier_, sizeof(unsigned long long)));
-    // Default launch shape: warp tiles (4 warps per block) on the persistent
-    // dataflow schedule; explicit threads-per-item selects the item-parallel
-    // variant.  The autotuner can replace either.
-    const int sched = o.schedule == 1 ? 1 : 2;
-    TY_CHECK(configure(0, sched, o.tpi64 ? 0 : 1, o.tpi64 ? o.tpi64 : 4, err));
-    TY_CHECK(configure(1, sched, o.tpi32 ? 0 : 1, o.tpi32 ? o.tpi32 : 4, err));
+    // Default launch shape: compact records in registers, one launch per
+    // level (64-thread blocks); schedule 2 asks for the persistent dataflow
+    // kernel (warp tiles); explicit threads-per-item selects the
+    // item-parallel variant.  The autotuner can replace any of them.
+    for (int prec = 0; prec < (fp32_ ? 2 : 1); ++prec) {
+        const int tpi = prec ? o.tpi32 : o.tpi64;
+        if (tpi) TY_CHECK(configure(prec, o.schedule == 1 ? 1 : 2, 0, tpi, err));
+        else if (o.schedule == 2) TY_CHECK(configure(prec, 2, 1, 4, err));
+        else TY_CHECK(configure(prec, 1, 4, 64, err));
+    }
     TY_CUDA(cudaStreamSynchronize(stream_));
     return kOk;
 }
 
 int Sweeper::configure(int prec, int schedule, int variant, int knob, std::string &err, int vg)
 {
+    if (prec == 1 && !fp32_) { err = "sweeper was created without the FP32 sweep"; return kErrArg; }
     if (vg == 0) vg = (int)record_vg(prec != 0, (uint32_t)G_);
     if (vg != 1 && vg != 2 && !(vg == 4 && prec == 1)) {
         err = "group vector width must be 1 or 2 (FP64), 1, 2 or 4 (FP32)";

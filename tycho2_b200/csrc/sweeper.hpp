@@ -23,7 +23,7 @@ struct SweeperOptions {
     bool fp32 = false;
     int tpi64 = 0;  // 0 = auto
     int tpi32 = 0;
-    int schedule = 0;  // 0 auto (dataflow), 1 level-synchronous, 2 dataflow
+    int schedule = 0;  // 0 auto (levels, compact records), 1 level-synchronous, 2 dataflow
 };
 
 // Launch shape of one precision's sweep.

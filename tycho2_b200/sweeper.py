@@ -277,7 +277,7 @@ class BatchSolver:
         self._h = h
         self._members = {}
 
-    def add(self, sweeper, method="mixed", iter_max=1000, err_max=1e-10, inner_tol=1e-4,
+    def add(self, sweeper, method="mixed", iter_max=1000, err_max=1e-10, inner_tol=1e-5,
             inner_max=200, refine_max=30):
         o = _capi.BatchOpts(self.BATCH_METHODS[method], iter_max, err_max, inner_tol, inner_max,
                             refine_max)
@@ -337,7 +337,7 @@ class SolveServer:
     STATES = {0: "queued", 1: "building", 2: "built", 3: "in batch", 4: "done", 5: "failed"}
 
     def __init__(self, method="mixed", budget_bytes=150e9, device=0, setup_threads=2, ipw32=0,
-                 ipw64=0, iter_max=3000, err_max=1e-10, inner_tol=1e-4, inner_max=200, refine_max=30):
+                 ipw64=0, iter_max=3000, err_max=1e-10, inner_tol=1e-5, inner_max=200, refine_max=30):
         solve = _capi.BatchOpts(BatchSolver.BATCH_METHODS[method], iter_max, err_max, inner_tol,
                                 inner_max, refine_max)
         o = _capi.ServerOpts(device, float(budget_bytes), setup_threads, ipw32, ipw64, solve)
