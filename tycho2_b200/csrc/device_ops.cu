@@ -27,6 +27,9 @@ template cudaError_t record_persist_blocks_per_sm<double>(int, int, int *);
 template cudaError_t launch_direct_level<double>(int, const LevelArgs &, const void *, uint64_t, uint64_t, cudaStream_t,
                                                   bool);
 template cudaError_t launch_compact_records<double>(const LevelArgs &, uint64_t, void *, cudaStream_t);
+template cudaError_t launch_direct_dataflow<double>(const LevelArgs &, const void *, bool, const DataflowArgs &,
+                                                     unsigned, cudaStream_t);
+template cudaError_t direct_dataflow_blocks_per_sm<double>(int, bool, int *);
 
 namespace {
 

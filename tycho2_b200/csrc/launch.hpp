@@ -81,6 +81,14 @@ cudaError_t record_dataflow_blocks_per_sm(int ipw, int vg, int *blocks);
 template <typename Real>
 cudaError_t launch_direct_level(int bs, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
                                 cudaStream_t s, bool compact);
+// Direct variants on the dataflow schedule: one cooperative launch, a
+// completion flag per (item, group vector) in df.done (n_cells * A * G/vg
+// words, G/vg a power of two <= 32).
+template <typename Real>
+cudaError_t launch_direct_dataflow(const LevelArgs &p, const void *rec, bool compact, const DataflowArgs &df,
+                                   unsigned grid, cudaStream_t s);
+template <typename Real>
+cudaError_t direct_dataflow_blocks_per_sm(int vg, bool compact, int *blocks);
 // Compact records (64 B per item for float, 96 B for double): the inputs of
 // each item's matrix, from which the direct kernels rebuild its factors.
 constexpr size_t compact_record_bytes(bool fp32) { return fp32 ? 64 : 96; }

@@ -24,5 +24,8 @@ template cudaError_t record_persist_blocks_per_sm<float>(int, int, int *);
 template cudaError_t launch_direct_level<float>(int, const LevelArgs &, const void *, uint64_t, uint64_t, cudaStream_t,
                                                   bool);
 template cudaError_t launch_compact_records<float>(const LevelArgs &, uint64_t, void *, cudaStream_t);
+template cudaError_t launch_direct_dataflow<float>(const LevelArgs &, const void *, bool, const DataflowArgs &,
+                                                     unsigned, cudaStream_t);
+template cudaError_t direct_dataflow_blocks_per_sm<float>(int, bool, int *);
 
 }  // namespace tycho

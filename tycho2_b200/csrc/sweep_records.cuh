@@ -515,8 +515,8 @@ sweep_record_level_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict_
 // are read after it.  No shared memory.  Tasks of a level: item t / (G/VG),
 // groups VG * (t % (G/VG)) and on (the host keeps a level's task count
 // below 2^26 so that the multiply-high division is exact).
-template <typename Real, int VG, int BS, typename Rec>
-__global__ void __launch_bounds__(BS)
+template <typename Real, int VG, int BS, typename Rec, int MINB = 1>
+__global__ void __launch_bounds__(BS, MINB)
 sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const uint64_t begin, const uint64_t end)
 {
     pdl_launch_dependents();
@@ -537,6 +537,80 @@ sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const 
     if (!live) return;
     pair_load_upwind<Real, VG, false>(p, R, g, in);
     pair_solve_store_any<Real, VG>(p, R, g, in);
+}
+
+// Wait on one completion flag: back-to-back polls first (one poll is an L2
+// round trip), then polls 64 ns apart; gives up after df.spin_limit polls
+// (records the item and face, raises abort) so that no wait can hang.
+__device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Polls with relaxed loads (no L1 invalidation per poll); the caller follows
+// its last successful wait with one fence.acq_rel.gpu, which with the
+// observed release forms the acquire pattern of the PTX memory model.
+__device__ __forceinline__ bool wait_flag_tight(const DataflowArgs &df, uint32_t epoch, const uint32_t *flag,
+                                                uint32_t ca, int f)
+{
+    for (uint32_t spin = 0; spin < df.spin_limit; ++spin) {
+        if (ld_relaxed_gpu(flag) == epoch) return true;
+        if ((spin & 31u) == 31u && *(volatile const uint32_t *)df.abort) return false;
+        if (spin >= 128) __nanosleep(64);
+    }
+    if (atomicCAS(df.err, 0u, (uint32_t)kErrTimeoutCode) == 0u) {
+        df.err[1] = ca;
+        df.err[2] = (uint32_t)f;
+    }
+    atomicExch(df.abort, 1u);
+    return false;
+}
+
+// Direct dataflow: one cooperative launch per sweep; warps take chunks of 32
+// (item, group vector) tasks in level order, round-robin; a lane loads its
+// record and source, waits for the completion flags of its upwind tasks (the
+// same group vector of the neighbour's item, flag index = row * (G/VG) + gv),
+// sweeps its groups and releases its own flag.  G/VG must be a power of two
+// up to 32, so a chunk is 32/(G/VG) whole items and never spans two levels
+// (levels hold multiples of 32 items).  Deadlock freedom as for the other
+// dataflow kernels: tasks wait only on lower levels, warps visit chunks in
+// increasing order, every warp is resident.
+template <typename Real, int VG, typename Rec>
+__global__ void __launch_bounds__(128)
+sweep_direct_dataflow_kernel(const LevelArgs p, const Rec *__restrict__ rec, const DataflowArgs df)
+{
+    const uint32_t gpv = p.G / VG;
+    const uint32_t lg = 31u - __clz(gpv);  // log2(gpv)
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t ipc = 32u >> lg;  // items per chunk
+    const uint64_t nchunks = df.n_items / ipc;
+    const uint32_t epoch = *df.epoch;
+    const uint32_t gv = lane & (gpv - 1u), g = gv * VG;
+    for (uint64_t ch = warp; ch < nchunks; ch += nwarps) {
+        if (*(volatile const uint32_t *)df.abort) break;
+        const uint64_t it = ch * ipc + (lane >> lg);
+        RegRecord<Real> R;
+        load_record(rec + it, R);
+        if (R.u(0) == kSentinel) continue;
+        PairIn<Real, VG> in;
+        pair_load_source<Real, VG>(p, R, g, in);
+        bool ok = true;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            const uint32_t row = R.u(3 + f);
+            if (ok && R.f(f) < Real(0) && row != kNoRow)
+                ok = wait_flag_tight(df, epoch, df.done + (size_t)row * gpv + gv, R.u(1), f);
+        }
+        if (!ok) continue;
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        pair_load_upwind<Real, VG, true>(p, R, g, in);
+        pair_solve_store_any<Real, VG>(p, R, g, in);
+        st_release_gpu(df.done + (size_t)R.u(1) * gpv + gv, epoch);  // orders this thread's psi stores first
+    }
 }
 
 // Dataflow schedule: persistent warps take IPW-item chunks round-robin; lane
@@ -732,39 +806,45 @@ cudaError_t launch_item_records(const LevelArgs &p, uint64_t n, void *out, cudaS
     return cudaGetLastError();
 }
 
-template <typename Real, int BS, typename Rec>
+template <typename Real, int BS, typename Rec, int MINB>
 static const void *direct_fn_vg(int vg)
 {
     switch (vg) {
-    case 1: return (const void *)sweep_direct_level_kernel<Real, 1, BS, Rec>;
-    case 2: return (const void *)sweep_direct_level_kernel<Real, 2, BS, Rec>;
+    case 1: return (const void *)sweep_direct_level_kernel<Real, 1, BS, Rec, MINB>;
+    case 2: return (const void *)sweep_direct_level_kernel<Real, 2, BS, Rec, MINB>;
     case 4:
-        if constexpr (sizeof(Real) == 4) return (const void *)sweep_direct_level_kernel<Real, 4, BS, Rec>;
+        if constexpr (sizeof(Real) == 4) return (const void *)sweep_direct_level_kernel<Real, 4, BS, Rec, MINB>;
         else return nullptr;
     default: return nullptr;
     }
 }
 
 template <typename Real, typename Rec>
-static const void *direct_fn(int bs, int vg)
+static const void *direct_fn(int knob, int vg)
 {
-    return bs == 64 ? direct_fn_vg<Real, 64, Rec>(vg)
-           : bs == 128 ? direct_fn_vg<Real, 128, Rec>(vg)
-           : bs == 256 ? direct_fn_vg<Real, 256, Rec>(vg)
-                       : nullptr;
+    switch (knob) {
+    case 64: return direct_fn_vg<Real, 64, Rec, 1>(vg);
+    case 128: return direct_fn_vg<Real, 128, Rec, 1>(vg);
+    case 256: return direct_fn_vg<Real, 256, Rec, 1>(vg);
+    case -64: return direct_fn_vg<Real, 64, Rec, 16>(vg);   // <= 64 registers
+    case -128: return direct_fn_vg<Real, 128, Rec, 8>(vg);  // <= 64 registers
+    default: return nullptr;
+    }
 }
 
-// Direct variant: knob = threads per block (64, 128 or 256); compact picks
-// the compact record format.
+// Direct variant: knob = threads per block (64, 128 or 256; -64 / -128: the
+// same with registers capped at 64 so that more blocks are resident); compact
+// picks the compact record format.
 template <typename Real>
-cudaError_t launch_direct_level(int bs, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
+cudaError_t launch_direct_level(int knob, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
                                 cudaStream_t s, bool compact)
 {
+    const int bs = knob < 0 ? -knob : knob;
     if (end <= begin) return cudaSuccess;
     const uint64_t tasks = (end - begin) * (p.G / p.vg);
     if (tasks >= (1ull << 26)) return cudaErrorInvalidValue;
-    const void *fn = compact ? direct_fn<Real, CompactRecord<Real>>(bs, (int)p.vg)
-                             : direct_fn<Real, ItemRecord<Real>>(bs, (int)p.vg);
+    const void *fn = compact ? direct_fn<Real, CompactRecord<Real>>(knob, (int)p.vg)
+                             : direct_fn<Real, ItemRecord<Real>>(knob, (int)p.vg);
     if (!fn) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)((tasks + bs - 1) / bs));
@@ -777,6 +857,52 @@ cudaError_t launch_direct_level(int bs, const LevelArgs &p, const void *rec, uin
     cfg.numAttrs = 1;
     const void *r = rec;
     void *args[] = {(void *)&p, (void *)&r, (void *)&begin, (void *)&end};
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+template <typename Real, typename Rec>
+static const void *direct_dataflow_fn(int vg)
+{
+    switch (vg) {
+    case 1: return (const void *)sweep_direct_dataflow_kernel<Real, 1, Rec>;
+    case 2: return (const void *)sweep_direct_dataflow_kernel<Real, 2, Rec>;
+    case 4:
+        if constexpr (sizeof(Real) == 4) return (const void *)sweep_direct_dataflow_kernel<Real, 4, Rec>;
+        else return nullptr;
+    default: return nullptr;
+    }
+}
+
+template <typename Real>
+cudaError_t direct_dataflow_blocks_per_sm(int vg, bool compact, int *blocks)
+{
+    const void *fn = compact ? direct_dataflow_fn<Real, CompactRecord<Real>>(vg)
+                             : direct_dataflow_fn<Real, ItemRecord<Real>>(vg);
+    if (!fn) return cudaErrorInvalidValue;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, fn, 128, 0);
+}
+
+// df.done must hold n_cells * A * (G / vg) flags; G / vg a power of two <= 32.
+template <typename Real>
+cudaError_t launch_direct_dataflow(const LevelArgs &p, const void *rec, bool compact, const DataflowArgs &df,
+                                   unsigned grid, cudaStream_t s)
+{
+    const uint32_t gpv = p.G / p.vg;
+    if (grid == 0 || gpv == 0 || gpv > 32 || (gpv & (gpv - 1)) != 0) return cudaErrorInvalidValue;
+    const void *fn = compact ? direct_dataflow_fn<Real, CompactRecord<Real>>((int)p.vg)
+                             : direct_dataflow_fn<Real, ItemRecord<Real>>((int)p.vg);
+    if (!fn) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(128);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const void *r = rec;
+    void *args[] = {(void *)&p, (void *)&r, (void *)&df};
     return cudaLaunchKernelExC(&cfg, fn, args);
 }
 

@@ -57,7 +57,7 @@ Sweeper::~Sweeper()
     void *bufs[] = {d_items_, d_abar64_, d_abar32_, d_adj_, d_nbrmap_, d_cellk64_, d_cellk32_,
                     d_w_, d_sigs_, d_scat_, d_qiso_, d_qang_, d_src_, d_iso_, d_iso32_, d_psi_,
                     d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_, d_done_, d_ctl_, d_rec_[0], d_rec_[1],
-                    d_level_off_, d_barrier_, d_crec_[0], d_crec_[1]};
+                    d_level_off_, d_barrier_, d_crec_[0], d_crec_[1], d_flags_};
     for (void *b : bufs)
         if (b) cudaFree(b);
     reducer_free(red_);
@@ -194,8 +194,21 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
         err = "persistent levels in FP64: items per warp must be 8 or 16";
         return kErrArg;
     }
-    if (variant >= 3 && (schedule != 1 || (knob != 64 && knob != 128 && knob != 256))) {
-        err = "direct record variants: level schedule only, 64, 128 or 256 threads per block";
+    if (variant >= 3 && schedule == 1 && knob != 64 && knob != 128 && knob != 256 && knob != -64 &&
+        knob != -128) {
+        err = "direct record variants on levels: 64, 128 or 256 threads per block (-64, -128: 64 registers)";
+        return kErrArg;
+    }
+    if (variant >= 3 && schedule == 2) {
+        const int gv = vg ? vg : (int)record_vg(prec != 0, (uint32_t)G_);
+        const int gpv = G_ % gv == 0 ? G_ / gv : 0;
+        if (knob != 128 || gpv == 0 || gpv > 32 || (gpv & (gpv - 1)) != 0) {
+            err = "direct record variants on dataflow: 128 threads per block, nGroups / vector a power of two <= 32";
+            return kErrArg;
+        }
+    }
+    if (variant >= 3 && schedule == 3) {
+        err = "the persistent-levels schedule runs the record variant only";
         return kErrArg;
     }
     if (variant < 0 || variant > 4) {
@@ -228,6 +241,23 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
     sh.vg = variant >= 2 ? vg : 1;
     sh.grid = (unsigned)(sms * per_sm);
     sh.persist_grid = (unsigned)(sms * persist_per_sm);
+    sh.direct_grid = 0;
+    if (variant >= 3 && schedule == 2) {
+        int direct_per_sm = 0;
+        TY_CUDA(prec ? direct_dataflow_blocks_per_sm<float>(vg, variant == 4, &direct_per_sm)
+                     : direct_dataflow_blocks_per_sm<double>(vg, variant == 4, &direct_per_sm));
+        if (direct_per_sm < 1) { err = "direct dataflow kernel does not fit on an SM"; return kErrCuda; }
+        sh.direct_grid = (unsigned)(sms * direct_per_sm);
+        const size_t flags = (size_t)nc_ * A_ * (G_ / vg);
+        if (flags > flags_cap_) {
+            if (d_flags_) cudaFree(d_flags_);
+            d_flags_ = nullptr;
+            flags_cap_ = 0;
+            TY_CUDA(cudaMalloc(&d_flags_, sizeof(uint32_t) * flags));
+            TY_CUDA(cudaMemsetAsync(d_flags_, 0, sizeof(uint32_t) * flags, stream_));
+            flags_cap_ = flags;
+        }
+    }
     // cached level graphs were captured for the previous launch shape
     for (auto it = graphs_.begin(); it != graphs_.end();) {
         if (std::get<0>(it->first) == prec) {
@@ -250,14 +280,20 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
     LaunchShape keep = shape_[prec ? 1 : 0];
     for (int sched = 1; sched <= 3; ++sched)
         for (int variant = 0; variant <= 4; ++variant)
-            for (int knob : {1, 2, 4, 8, 16, 32, 64, 128, 256}) {
+            for (int knob : {1, 2, 4, 8, 16, 32, 64, 128, 256, -64, -128}) {
+                if (knob < 0 && (variant < 3 || sched != 1)) continue;
                 if (variant == 0 && ((knob > 2 * G_ && knob > 1) || knob > 16)) continue;  // idle lanes
                 if (variant == 1 && knob > 4) continue;
                 if (variant == 2 && (knob < 8 || knob > 32)) continue;
-                if (variant >= 3 && (knob < 64 || sched != 1)) continue;
+                if (variant >= 3 && ((knob > 0 && knob < 64) || sched == 3 || (sched == 2 && knob != 128)))
+                    continue;
                 if (sched == 3 && (variant != 2 || (prec == 0 && knob == 32))) continue;
                 for (int vg : {1, 2, 4}) {
                     if (vg > 1 && (variant < 2 || G_ % vg != 0 || (vg == 4 && prec == 0))) continue;
+                    if (variant >= 3 && sched == 2) {
+                        const int gpv = G_ / vg;
+                        if (gpv > 32 || (gpv & (gpv - 1)) != 0) continue;
+                    }
                     const int cs = configure(prec, sched, variant, knob, err, vg);
                     if (cs == kErrOom) continue;  // records do not fit next to psi
                     TY_CHECK(cs);
@@ -458,6 +494,24 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
                                                     d_barrier_, df, sh.persist_grid, stream_)
                      : launch_persist_record<double>(sh.knob, p, d_rec_[0], d_level_off_, sched_.n_levels,
                                                      d_barrier_, df, sh.persist_grid, stream_));
+        if (end) TY_CUDA(cudaEventRecord(end, stream_));
+        return kOk;
+    }
+    if (sh.schedule == 2 && sh.variant >= 3) {
+        TY_CHECK(ensure_records(prec, true, err, sh.variant == 4));
+        const LevelArgs p = level_args(prec, iso, qang, d_psi_);
+        DataflowArgs df;
+        df.done = d_flags_;
+        df.err = d_ctl_;
+        df.abort = d_ctl_ + 3;
+        df.epoch = d_ctl_ + 4;
+        df.n_items = sched_.items.size();
+        df.spin_limit = 1u << 22;  // ~2 s of polling
+        TY_CUDA(launch_bump_epoch(d_ctl_ + 4, stream_));
+        if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
+        const void *rec = sh.variant == 4 ? d_crec_[prec ? 1 : 0] : d_rec_[prec ? 1 : 0];
+        TY_CUDA(prec ? launch_direct_dataflow<float>(p, rec, sh.variant == 4, df, sh.direct_grid, stream_)
+                     : launch_direct_dataflow<double>(p, rec, sh.variant == 4, df, sh.direct_grid, stream_));
         if (end) TY_CUDA(cudaEventRecord(end, stream_));
         return kOk;
     }

@@ -39,6 +39,7 @@ struct LaunchShape {
     int vg = 1;                 // records: groups per vector access of a psi row
     unsigned grid = 0;          // dataflow kernel of this variant: co-resident blocks
     unsigned persist_grid = 0;  // persistent-levels kernel: co-resident blocks
+    unsigned direct_grid = 0;   // direct variants on the dataflow schedule: co-resident blocks
 };
 
 struct SolveOptions {
@@ -172,6 +173,9 @@ private:
     // compact records (direct compact variant and the batch driver)
     void *d_crec_[2] = {nullptr, nullptr};
     bool crec_valid_[2] = {false, false};
+    // direct dataflow: a completion epoch per (item, group vector)
+    uint32_t *d_flags_ = nullptr;
+    size_t flags_cap_ = 0;
     // persistent-levels schedule: level offsets and the grid barrier counter
     uint64_t *d_level_off_ = nullptr;
     unsigned long long *d_barrier_ = nullptr;
