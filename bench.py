@@ -15,7 +15,9 @@ iteration vs FP32-sweep iteration inside FP64 refinement, one batched pass
 per step), and `serve`, Poisson-arriving solve requests (the batch size
 distribution plus 5% large 48^3-hex S8 G=8 ones) admitted by device-memory
 footprint against 150 GB with continuous batching: p50/p99 latency and
-solves/s of the mixed and the FP64 service.
+solves/s of the mixed and the FP64 service; and `large`, the 64^3 x 6-tet
+S8 G=16 problem (psi 103 GB): sweep rates and the mixed-precision GMRES solve
+against FP64 GMRES (skip with --no-large).
 
 Multi-GPU: the sweep does not shard across GPUs here (one mesh partition per
 GPU by design); --gpus N runs N independent replicas, one per rank, and
@@ -53,6 +55,7 @@ def parse():
     p.add_argument("--no-solve", action="store_true", help="skip the solve-error check")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-large", action="store_true", help="skip the 64^3 S8 G=16 leg")
     p.add_argument("--no-batch", action="store_true", help="skip the batched-instances leg")
     p.add_argument("--batch-instances", type=int, default=256)
     p.add_argument("--no-serve", action="store_true", help="skip the served-solves leg")
@@ -329,6 +332,53 @@ def run_serve_leg(grp, dev, count, rate, seed=99):
     return out
 
 
+def run_large_leg(grp, dev, workload="kuhn64_s8_g16"):
+    """The 64^3 x 6 = 1,572,864-tet S8 G=16 problem (lognormal(0, 1) sigma_t,
+    scattering ratio 0.99): FP32 and FP64 sweep rates, then the
+    mixed-precision solve (FP32-sweep GMRES(30) in FP64 refinement) against
+    FP64 GMRES(30), both to 1e-10.  psi alone is 103 GB (FP64-sized), so the
+    FP64 sweep runs the record-free warp-tile kernel and the FP32 sweep the
+    compact records."""
+    import tycho2_b200 as ty
+    w, mesh, st, ss, mat, q = build_problem(workload)
+    nc, A, G = mesh.n_cells, 2 * w["sn"] ** 2, w["groups"]
+    t0 = time.perf_counter()
+    sw = ty.SweeperCuda(mesh, w["sn"], G, fp32=True, device=dev)
+    sw.set_cross_sections(st, ss, mat)
+    sw.set_source(q, "isotropic")
+    setup = time.perf_counter() - t0
+    info = sw.schedule_info()
+    sw.configure(1, "levels", "compact", 64)
+    sw.configure(0, "levels", "tiles", 4)
+    sw.time_sweeps(1, 2)
+    sw.time_sweeps(0, 2)
+    grp.barrier()
+    ms32, k32 = sw.time_sweeps(1, 3, True)
+    ms64, k64 = sw.time_sweeps(0, 3, True)
+    ms32, k32, ms64, k64 = (grp.max(x) for x in (ms32, k32, ms64, k64))
+    upd = nc * A * G
+    peak, peak_kind = hbm_peak()
+    b32 = algorithmic_bytes(nc, A, G, info["n_incoming_interior"], 4)
+    tol, m = w.get("tol", 1e-10), w.get("restart", 30)
+    phim, _, sm = sw.solve("mixed", iter_max=600, err_max=tol, restart=m, want_psi=False)
+    phi64, _, s64 = sw.solve("gmres", iter_max=600, err_max=tol, restart=m, want_psi=False)
+    err = float(np.abs(phim - phi64).sum() / np.abs(phi64).sum())
+    sw.close()
+    return {"workload": workload, "cells": nc, "angles": A, "groups": G, "levels": info["n_levels"],
+            "setup_s": setup,
+            "fp32": {"updates_per_s": grp.sum(upd) / (ms32 * 1e-3), "ms_per_sweep": ms32,
+                     "kernel": "sweep_direct_level_kernel<float,4,64,compact>", "kernel_ms": k32,
+                     "roofline_frac": b32 / (k32 * 1e-3) / 1e9 / peak, "peak_kind": peak_kind},
+            "fp64": {"updates_per_s": grp.sum(upd) / (ms64 * 1e-3), "ms_per_sweep": ms64,
+                     "kernel": "sweep_tile_level_kernel<double,4>", "kernel_ms": k64},
+            "mixed_solve": {"seconds": sm["seconds"], "sweeps_fp32": sm["sweeps_fp32"],
+                            "sweeps_fp64": sm["sweeps_fp64"], "residual": sm["final_error"]},
+            "fp64_gmres_solve": {"seconds": s64["seconds"], "sweeps_fp64": s64["sweeps_fp64"],
+                                 "residual": s64["final_error"]},
+            "phi_rel_err_l1_mixed_vs_fp64": grp.max(err),
+            "mixed_vs_fp64_solve_speedup": s64["seconds"] / sm["seconds"]}
+
+
 def run_b200(args):
     import torch
     import tycho2_b200 as ty
@@ -347,7 +397,7 @@ def run_b200(args):
 
     # Launch shapes: the autotuner's pick per precision (or a fixed shape).
     if args.shape == "auto":
-        tuned = {1: sw.autotune(1, 3), 0: sw.autotune(0, 3)}
+        tuned = {1: sw.autotune(1, 5), 0: sw.autotune(0, 5)}
     else:
         s, v, k = args.shape.split(",")
         for prec in (1, 0):
@@ -435,6 +485,12 @@ def run_b200(args):
             serve = run_serve_leg(grp, dev, args.serve_requests, args.serve_rate)
         except Exception as e:
             serve = {"error": str(e)[:300]}
+    large = None
+    if not args.no_large:
+        try:
+            large = run_large_leg(grp, dev)
+        except Exception as e:
+            large = {"error": str(e)[:300]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -471,6 +527,7 @@ def run_b200(args):
             "e2e": e2e,
             "batch": batch,
             "serve": serve,
+            "large": large,
             "gpu_launches": args.steps * (launches_per_sweep(shape32, info["n_levels"])
                                           + launches_per_sweep(shape64, info["n_levels"])),
             "clocks": clocks,

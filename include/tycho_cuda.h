@@ -225,6 +225,10 @@ typedef struct tycho_launch_shape {
     int variant;
     int knob;
     int vector;
+    int streams;  /* level schedule: the octant groups of every level sweep
+                     on this many concurrent streams (1, 2, 4, 8) inside one
+                     captured graph; directions of different octants never
+                     depend on each other */
 } tycho_launch_shape;
 
 /* Autotuner: times every launch shape of the given precision's sweep with
@@ -337,6 +341,10 @@ typedef struct tycho_server_opts {
     int setup_threads;      /* host threads building sweepers */
     int ipw32, ipw64;       /* batched level kernels: items per warp (8, 16, 32; 0 = direct) */
     tycho_batch_opts solve; /* method TYCHO_SOURCE_ITERATION or TYCHO_MIXED_GMRES */
+    double large_items;     /* cells x angles from which a request runs in the
+                               second lane (its own batch and stream, stepped
+                               concurrently, so a deep mesh does not set the
+                               step time of small ones); 0 = 32e6 */
 } tycho_server_opts;
 
 typedef struct tycho_request_info {

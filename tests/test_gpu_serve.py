@@ -18,9 +18,10 @@ def _requests(count, seed):
     return out
 
 
-def _serve(reqs, method, arrivals, budget=150e9, threads=2):
+def _serve(reqs, method, arrivals, budget=150e9, threads=2, large_items=0.0):
     import tycho2_b200 as ty
-    srv = ty.SolveServer(method=method, budget_bytes=budget, setup_threads=threads, err_max=1e-10)
+    srv = ty.SolveServer(method=method, budget_bytes=budget, setup_threads=threads, err_max=1e-10,
+                         large_items=large_items)
     ids = [srv.submit(mesh, p["sn"], p["groups"], st, ss, mat, q, arrival=t)
            for (p, mesh, st, ss, mat, q), t in zip(reqs, arrivals)]
     srv.run()
@@ -30,13 +31,18 @@ def _serve(reqs, method, arrivals, budget=150e9, threads=2):
     return res, stats
 
 
-@pytest.mark.parametrize("method", ["mixed", "si"])
-def test_served_result_same_alone_and_in_mix(built, method):
+@pytest.mark.parametrize("method,large_items", [("mixed", 0.0), ("si", 0.0), ("mixed", 20000.0)])
+def test_served_result_same_alone_and_in_mix(built, method, large_items):
+    """large_items 20000: the bigger requests run in the second lane (own
+    batch and stream) concurrently with the small ones."""
     reqs = _requests(6, seed=11)
     alone = [_serve([r], method, [0.0])[0][0] for r in reqs]
     rng = np.random.default_rng(3)
     arrivals = np.cumsum(rng.exponential(0.01, len(reqs)))  # overlapping arrivals
-    mixed, stats = _serve(reqs, method, arrivals)
+    mixed, stats = _serve(reqs, method, arrivals, large_items=large_items)
+    if large_items:
+        sizes = [r[1].n_cells * 2 * r[0]["sn"] ** 2 for r in reqs]
+        assert min(sizes) < large_items <= max(sizes)  # both lanes in use
     assert stats["peak_active"] >= 2  # the requests did share the GPU
     for (pa, ia), (pm, im) in zip(alone, mixed):
         assert ia["state"] == "done" and im["state"] == "done"

@@ -39,7 +39,8 @@ def test_fp64_sweep_bit_exact_vs_reference_fixture(built, kuhn3_ref):
     ("levels", "items", 0), ("levels", "tiles", 0), ("levels", "records", 0), ("levels", "records", 1),
     ("dataflow", "items", 0), ("dataflow", "tiles", 0), ("dataflow", "records", 0),
     ("persist", "records", 0), ("persist", "records", 1), ("levels", "direct", 0), ("levels", "direct", 1),
-    ("levels", "compact", 0), ("levels", "compact", 1), ("dataflow", "compact", 0), ("dataflow", "direct", 1)])
+    ("levels", "compact", 0), ("levels", "compact", 1), ("dataflow", "compact", 0), ("dataflow", "direct", 1),
+    ("levels", "compact", 4)])
 @pytest.mark.parametrize("n,jitter,sn,G,tpi", [
     (4, 0.05, 4, 1, 1), (5, 0.05, 8, 2, 2), (3, 0.0, 2, 3, 1), (6, 0.05, 6, 4, 4),
     (4, 0.07, 8, 8, 8), (2, 0.05, 4, 16, 16), (7, 0.05, 4, 5, 2), (1, 0.0, 4, 1, 1),
@@ -55,6 +56,8 @@ def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi, v
     knob = {"items": tpi, "tiles": min(tpi, 4), "records": 8 if tpi <= 2 else (16 if tpi <= 4 else 32),
             "direct": 64 * min(tpi, 4) if tpi != 4 else 128}
     knob["compact"] = knob["direct"]
+    if vector == 4 and G % 4:
+        pytest.skip("two 2-group vectors per task need nGroups divisible by 4")
     if schedule == "dataflow" and variant in ("direct", "compact"):
         vg = vector or (2 if G % 2 == 0 else 1)
         if (G // vg) & (G // vg - 1) or G // vg > 32:
@@ -69,6 +72,27 @@ def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi, v
     assert bits_equal(psi, o.sweep(st, src_ang=src))
     sw.sweep(psi, src)  # a second sweep (next completion epoch) is identical
     assert bits_equal(psi, o.sweep(st, src_ang=src))
+
+
+@pytest.mark.parametrize("streams", [2, 4, 8])
+@pytest.mark.parametrize("variant,knob", [("compact", 64), ("direct", 128), ("records", 16), ("tiles", 4)])
+def test_fp64_sweep_on_several_streams_bit_exact(built, workdir, streams, variant, knob):
+    """Octant groups of every level on concurrent streams: the same psi."""
+    from oracle.oracle import Oracle
+    for n, sn, G in [(5, 8, 4), (3, 6, 2), (2, 4, 1)]:
+        mesh, om = kuhn(workdir, n, 0.05, seed=31)
+        o = Oracle(om, sn, G)
+        rng = np.random.default_rng(n + G)
+        st = rng.lognormal(0.0, 0.5, mesh.n_cells)
+        src = rng.uniform(-0.2, 1.0, o.psi_shape)
+        sw = make(mesh, sn, G)
+        sw.configure(0, "levels", variant, knob, 0, streams)
+        assert sw.shape(0)["streams"] == streams
+        sw.set_cross_sections(st, np.zeros(mesh.n_cells))
+        psi = np.empty(sw.psi_shape)
+        sw.sweep(psi, src)
+        assert bits_equal(psi, o.sweep(st, src_ang=src)), (n, sn, G)
+        sw.close()
 
 
 def test_fp64_operator_bit_exact_vs_oracle_downscatter(built, workdir):
@@ -184,7 +208,8 @@ def test_fp32_sweep_within_tolerance(built, workdir):
                   ("dataflow", "records", 32), ("persist", "records", 8), ("persist", "records", 32),
                   ("levels", "records", 16, 1), ("levels", "records", 16, 2), ("levels", "direct", 128),
                   ("levels", "direct", 64, 1), ("levels", "compact", 64), ("levels", "compact", 128, 2),
-                  ("dataflow", "compact", 128), ("dataflow", "direct", 128, 2)):
+                  ("dataflow", "compact", 128), ("dataflow", "direct", 128, 2), ("levels", "compact", 64, 8),
+                  ("levels", "direct", 128, 8), ("levels", "compact", 64, 4, 8), ("levels", "compact", 64, 2, 2)):
         sw = make(mesh, 8, G, fp32=True)
         sw.configure(1, *shape)
         sw.set_cross_sections(st, st, mat)
@@ -273,7 +298,7 @@ def test_autotune_keeps_results_bit_exact(built, workdir):
     best64 = sw.autotune(0, reps=2)
     best32 = sw.autotune(1, reps=2)
     assert best64["variant"] in ("items", "tiles", "records", "direct", "compact") and best32["schedule"] in ("levels", "dataflow", "persist")
-    assert sw.shape(0) == {k: best64[k] for k in ("schedule", "variant", "knob", "vector")}
+    assert sw.shape(0) == {k: best64[k] for k in ("schedule", "variant", "knob", "vector", "streams")}
     psi = np.empty(sw.psi_shape)
     sw.sweep(psi, src)
     assert bits_equal(psi, o.sweep(st, src_ang=src))

@@ -39,7 +39,8 @@ class SolveOpts(C.Structure):
 
 
 class LaunchShape(C.Structure):
-    _fields_ = [("schedule", C.c_int), ("variant", C.c_int), ("knob", C.c_int), ("vector", C.c_int)]
+    _fields_ = [("schedule", C.c_int), ("variant", C.c_int), ("knob", C.c_int), ("vector", C.c_int),
+                ("streams", C.c_int)]
 
 
 class BatchOpts(C.Structure):
@@ -49,7 +50,7 @@ class BatchOpts(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("budget_bytes", C.c_double), ("setup_threads", C.c_int),
-                ("ipw32", C.c_int), ("ipw64", C.c_int), ("solve", BatchOpts)]
+                ("ipw32", C.c_int), ("ipw64", C.c_int), ("solve", BatchOpts), ("large_items", C.c_double)]
 
 
 class SolveStats(C.Structure):

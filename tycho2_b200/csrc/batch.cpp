@@ -352,17 +352,37 @@ int Batch::pass(int prec, std::string &err)
 
 int Batch::step(int &n_running, std::string &err)
 {
-    n_running = 0;
-    for (const auto &m : members_) n_running += m.state != kDone;
-    if (n_running == 0) return kOk;
+    TB_CHECK(step_launch(err));
+    return step_finish(n_running, err);
+}
+
+int Batch::step_launch(std::string &err)
+{
+    launched_ = false;
+    int running = 0;
+    for (const auto &m : members_) running += m.state != kDone;
+    if (running == 0) return kOk;
     TB_CUDA(cudaSetDevice(device_));
     TB_CHECK(ensure_capacity(err));
-    const int before[2] = {passes_[0], passes_[1]};
+    before_[0] = passes_[0];
+    before_[1] = passes_[1];
     TB_CHECK(pass(0, err));
     TB_CHECK(pass(1, err));
-    const size_t n = members_.size();
-    TB_CUDA(cudaMemcpyAsync(h_norms_, plan_.norms, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaMemcpyAsync(h_norms_, plan_.norms, sizeof(double) * 2 * members_.size(), cudaMemcpyDeviceToHost,
+                            stream_));
+    launched_ = true;
+    return kOk;
+}
+
+int Batch::step_finish(int &n_running, std::string &err)
+{
+    n_running = 0;
+    if (!launched_) return kOk;
+    launched_ = false;
+    TB_CUDA(cudaSetDevice(device_));
     TB_CUDA(cudaStreamSynchronize(stream_));
+    const size_t n = members_.size();
+    const int *before = before_;
     for (int p = 0; p < 2; ++p)
         if (passes_[p] > before[p]) {
             float ms = 0;
@@ -410,6 +430,13 @@ int Batch::step(int &n_running, std::string &err)
         }
     }
     return kOk;
+}
+
+int Batch::running() const
+{
+    int n = 0;
+    for (const auto &m : members_) n += m.state != kDone;
+    return n;
 }
 
 int Batch::run(std::string &err)

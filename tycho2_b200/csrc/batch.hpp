@@ -49,6 +49,15 @@ public:
     int remove(int id, std::string &err);
     // One step of every running member; n_running receives how many still run.
     int step(int &n_running, std::string &err);
+    // The same in two halves: enqueue the step's passes on the batch's own
+    // stream, then wait for them and advance the members (so that several
+    // batches can run on the GPU at once).
+    int step_launch(std::string &err);
+    int step_finish(int &n_running, std::string &err);
+    int running() const;
+    // The launched step has finished on the GPU, failed (step_finish reports
+    // it), or nothing is in flight.
+    bool step_done() const { return !launched_ || cudaStreamQuery(stream_) != cudaErrorNotReady; }
     int run(std::string &err);
     int result(int id, double *phi_host, BatchMemberStats &st, std::string &err);
     // Device time of the passes so far: [0] FP64, [1] FP32 (ms), and counts.
@@ -99,6 +108,8 @@ private:
     double ms_[2] = {0, 0};
     int passes_[2] = {0, 0};
     double updates_[2] = {0, 0};
+    bool launched_ = false;
+    int before_[2] = {0, 0};
 };
 
 }  // namespace tycho

@@ -384,6 +384,7 @@ int tycho_sweeper_autotune(tycho_sweeper *h, int precision, int reps, tycho_laun
             best->variant = sh.variant;
             best->knob = sh.knob;
             best->vector = sh.vg;
+            best->streams = sh.streams;
         }
         return finish(s, err);
     });
@@ -394,7 +395,8 @@ int tycho_sweeper_configure(tycho_sweeper *h, int precision, const tycho_launch_
     if (!h || !shape || (precision != 0 && precision != 1))
         return finish(TYCHO_ERR_ARG, "bad sweeper, precision or shape");
     std::string err;
-    return finish(h->sw.configure(precision, shape->schedule, shape->variant, shape->knob, err, shape->vector),
+    return finish(h->sw.configure(precision, shape->schedule, shape->variant, shape->knob, err, shape->vector,
+                                  shape->streams ? shape->streams : 1),
                   err);
 }
 
@@ -407,6 +409,7 @@ int tycho_sweeper_get_shape(const tycho_sweeper *h, int precision, tycho_launch_
     shape->variant = sh.variant;
     shape->knob = sh.knob;
     shape->vector = sh.vg;
+    shape->streams = sh.streams;
     return TYCHO_OK;
 }
 
@@ -538,6 +541,7 @@ int tycho_server_create(const tycho_server_opts *o, tycho_server **out)
         so.solve.inner_tol = o->solve.inner_tol;
         so.solve.inner_max = o->solve.inner_max;
         so.solve.refine_max = o->solve.refine_max;
+        if (o->large_items > 0) so.large_items = o->large_items;
         auto *h = new tycho_server();
         int s = h->s.init(so, err);
         if (s != tycho::kOk) {

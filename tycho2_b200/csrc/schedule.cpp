@@ -131,24 +131,28 @@ int build_schedule(const MeshTables &t, const Quadrature &q, Schedule &s, std::s
     }
     s.n_incoming_interior = incoming_total;
     s.n_levels = *std::max_element(level_count_per_angle.begin(), level_count_per_angle.end());
-    std::vector<uint64_t> count(s.n_levels + 1, 0);
+    // Items per (level, octant); each such segment is padded to a multiple
+    // of kLevelPad with sentinel items, so that a warp's chunk never spans
+    // two levels (or two octants).
+    std::vector<int> oct(A);
+    for (int a = 0; a < A; ++a) oct[a] = octant(q, a);
+    const size_t nseg = (size_t)s.n_levels * kOctants;
+    std::vector<uint64_t> count(nseg, 0);
     for (uint64_t c = 0; c < nc; ++c)
-        for (int a = 0; a < A; ++a) count[s.tlevel[(size_t)a * nc + c] + 1]++;
-    // Each level is padded to a multiple of kLevelPad with sentinel items, so
-    // that a warp's chunk of the persistent schedule never spans two levels.
+        for (int a = 0; a < A; ++a) count[(size_t)s.tlevel[(size_t)a * nc + c] * kOctants + oct[a]]++;
+    s.octant_offset.resize(nseg + 1);
+    s.octant_offset[0] = 0;
+    for (size_t k = 0; k < nseg; ++k)
+        s.octant_offset[k + 1] = s.octant_offset[k] + (count[k] + kLevelPad - 1) / kLevelPad * kLevelPad;
     s.level_offset.resize(s.n_levels + 1);
-    s.level_offset[0] = 0;
-    for (uint32_t l = 0; l < s.n_levels; ++l) {
-        const uint64_t padded = (count[l + 1] + kLevelPad - 1) / kLevelPad * kLevelPad;
-        s.level_offset[l + 1] = s.level_offset[l] + padded;
-    }
+    for (uint32_t l = 0; l <= s.n_levels; ++l) s.level_offset[l] = s.octant_offset[(size_t)l * kOctants];
     s.n_items = (uint64_t)A * nc;
-    std::vector<uint64_t> pos(s.level_offset.begin(), s.level_offset.end() - 1);
+    std::vector<uint64_t> pos(s.octant_offset.begin(), s.octant_offset.end() - 1);
     s.items.assign(s.level_offset[s.n_levels], kSentinelItem);
     for (uint64_t c = 0; c < nc; ++c)
         for (int a = 0; a < A; ++a) {
-            uint32_t l = s.tlevel[(size_t)a * nc + c];
-            s.items[pos[l]++] = (uint32_t)(c * A + a);
+            const size_t k = (size_t)s.tlevel[(size_t)a * nc + c] * kOctants + oct[a];
+            s.items[pos[k]++] = (uint32_t)(c * A + a);
         }
     return kOk;
 }

@@ -5,8 +5,10 @@
 // (cell, angle) pair is levelled once: its t-level is the length of the
 // longest upwind chain that ends at it, so all pairs of one level depend only
 // on pairs of lower levels and can be updated together.  Items of a level are
-// stored contiguously, in increasing (cell*A + angle) order, which is the psi
-// row order, so neighbouring items write neighbouring psi rows.
+// stored contiguously, grouped by the octant of their direction (directions
+// of different octants never depend on each other, so the octant groups of a
+// level can sweep on different streams) and within an octant in increasing
+// (cell*A + angle) order, the psi row order.
 #pragma once
 
 #include <cstdint>
@@ -28,13 +30,23 @@ int make_quadrature(int sn_order, Quadrature &q, std::string &err);
 
 constexpr uint32_t kSentinelItem = 0xFFFFFFFFu;  // level padding
 constexpr uint64_t kLevelPad = 32;
+constexpr int kOctants = 8;
+
+// Octant of a direction: bit 2 xi < 0, bit 1 eta < 0, bit 0 mu < 0.
+inline int octant(const Quadrature &q, int a)
+{
+    return (q.xi[a] < 0 ? 4 : 0) | (q.eta[a] < 0 ? 2 : 0) | (q.mu[a] < 0 ? 1 : 0);
+}
 
 struct Schedule {
     uint32_t n_levels = 0;
     uint64_t n_items = 0;                // cells x angles (without padding)
     std::vector<uint64_t> level_offset;  // n_levels + 1 offsets into items
+    std::vector<uint64_t> octant_offset; // n_levels * kOctants + 1: level l, octant o
+                                         // starts at [l * kOctants + o]
     std::vector<uint32_t> items;         // cell*A + angle, grouped by level,
-                                         // each level padded to kLevelPad
+                                         // then octant, each (level, octant)
+                                         // padded to kLevelPad
     std::vector<uint32_t> tlevel;        // (angle, cell)
     uint64_t n_incoming_interior = 0;    // sum over items of incoming interior faces
 };

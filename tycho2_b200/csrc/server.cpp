@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <thread>
 
 #include "status.hpp"
 
@@ -42,7 +43,11 @@ int Server::init(const ServerOptions &o, std::string &err)
     }
     if (o.solve.method != 0 && o.solve.method != 2) { err = "server method must be 0 or 2"; return kErrArg; }
     o_ = o;
-    return batch_.init(o.device, o.ipw32, o.ipw64, err);
+    for (auto &b : lanes_) {
+        const int s = b.init(o.device, o.ipw32, o.ipw64, err);
+        if (s != kOk) return s;
+    }
+    return kOk;
 }
 
 double Server::now() const
@@ -72,6 +77,7 @@ int Server::submit(const MeshTables &t, int sn, int G, const double *sigma_t, co
     r->arrival = arrival;
     r->phi_out = phi_out;
     r->footprint = footprint_bytes(nc, sn, G, o_.solve.method == 2, o_.ipw32 == 0 && o_.ipw64 == 0);
+    r->lane = (double)nc * 2.0 * sn * sn >= o_.large_items ? 1 : 0;
     id = r->id;
     reqs_.push_back(std::move(r));
     return kOk;
@@ -144,7 +150,10 @@ int Server::run(std::string &err)
     std::stable_sort(order.begin(), order.end(), [](Request *a, Request *b) { return a->arrival < b->arrival; });
     size_t next = 0;  // next request to admit, in arrival order
     double reserved = 0;
-    int pending = (int)order.size(), in_batch = 0, building = 0;
+    int pending = (int)order.size(), building = 0;
+    int in_lane[kLanes] = {0, 0};
+    bool inflight[kLanes] = {false, false};
+    std::vector<Request *> waiting[kLanes];  // built, joining at the lane's next step boundary
     while (pending > 0) {
         // admission in arrival order: first come, first served, no overtaking
         const double t = now();
@@ -172,16 +181,17 @@ int Server::run(std::string &err)
             cv_work_.notify_one();
             ++next;
         }
-        // built requests join the batch
+        // built requests wait for their lane's next step boundary
         std::vector<Request *> ready;
         {
             std::unique_lock<std::mutex> lk(mu_);
-            if (in_batch == 0 && built_.empty()) {
+            const bool idle = !inflight[0] && !inflight[1] && in_lane[0] + in_lane[1] == 0 &&
+                              waiting[0].empty() && waiting[1].empty();
+            if (idle && built_.empty()) {
                 // idle GPU: wait for a build or the next arrival
                 const double wait = next < order.size() && order[next]->arrival > t ? order[next]->arrival - t : 0.05;
-                if (building > 0 || wait > 0)
-                    cv_built_.wait_for(lk, duration<double>(std::min(wait > 0 ? wait : 0.05, 0.05)),
-                                       [&] { return !built_.empty(); });
+                cv_built_.wait_for(lk, duration<double>(std::min(std::max(wait, 1e-4), 0.05)),
+                                   [&] { return !built_.empty(); });
             }
             ready.swap(built_);
         }
@@ -194,37 +204,58 @@ int Server::run(std::string &err)
                 --pending;
                 continue;
             }
-            int s = batch_.add(r->sw.get(), o_.solve, r->member, err);
-            if (s != kOk) return s;
-            r->state = 3;
-            ++in_batch;
+            r->state = 2;
+            waiting[r->lane].push_back(r);
         }
-        peak_active_ = std::max(peak_active_, in_batch);
-        if (in_batch == 0) continue;
-        int running = 0;
-        int s = batch_.step(running, err);
-        if (s != kOk) return s;
-        ++steps_;
-        // finished members leave the batch and free their memory
-        for (auto &rp : reqs_) {
-            Request *r = rp.get();
-            if (r->state != 3) continue;
-            BatchMemberStats st;
-            s = batch_.result(r->member, nullptr, st, err);
-            if (s != kOk) return s;
-            if (!st.done) continue;
-            s = batch_.result(r->member, r->phi_out, st, err);
-            if (s != kOk) return s;
-            r->stats = st;
-            s = batch_.remove(r->member, err);
-            if (s != kOk) return s;
-            r->sw.reset();
-            r->state = 4;
-            r->t_done = now();
-            reserved -= (double)r->footprint;
-            --in_batch;
-            --pending;
+        // each lane steps on its own stream: finish a step when its stream is
+        // done, retire finished members, admit waiting ones, launch the next
+        bool progressed = false;
+        for (int L = 0; L < kLanes; ++L) {
+            Batch &b = lanes_[L];
+            if (inflight[L]) {
+                if (!b.step_done()) continue;
+                int running = 0;
+                int s = b.step_finish(running, err);
+                if (s != kOk) return s;
+                inflight[L] = false;
+                progressed = true;
+                for (auto &rp : reqs_) {
+                    Request *r = rp.get();
+                    if (r->state != 3 || r->lane != L) continue;
+                    BatchMemberStats st;
+                    s = b.result(r->member, nullptr, st, err);
+                    if (s != kOk) return s;
+                    if (!st.done) continue;
+                    s = b.result(r->member, r->phi_out, st, err);
+                    if (s != kOk) return s;
+                    r->stats = st;
+                    s = b.remove(r->member, err);
+                    if (s != kOk) return s;
+                    r->sw.reset();
+                    r->state = 4;
+                    r->t_done = now();
+                    reserved -= (double)r->footprint;
+                    --in_lane[L];
+                    --pending;
+                }
+            }
+            for (Request *r : waiting[L]) {
+                int s = b.add(r->sw.get(), o_.solve, r->member, err);
+                if (s != kOk) return s;
+                r->state = 3;
+                ++in_lane[L];
+            }
+            waiting[L].clear();
+            peak_active_ = std::max(peak_active_, in_lane[0] + in_lane[1]);
+            if (in_lane[L] > 0 && b.running() > 0) {
+                int s = b.step_launch(err);
+                if (s != kOk) return s;
+                inflight[L] = true;
+                ++steps_;
+                progressed = true;
+            }
         }
+        if (!progressed && (inflight[0] || inflight[1])) std::this_thread::sleep_for(microseconds(20));
     }
     makespan_ = now();
     return kOk;

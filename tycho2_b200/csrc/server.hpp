@@ -27,6 +27,7 @@ struct ServerOptions {
     int setup_threads = 2;        // host threads building sweepers
     int ipw32 = 0, ipw64 = 0;     // batch level kernels: items per warp (0 = direct, compact records)
     BatchOptions solve;           // method 0 FP64 source iteration, 2 mixed
+    double large_items = 32e6;    // cells x angles from which a request runs in the large lane
 };
 
 // Device bytes one resident request holds (sweeper + batch vectors), an
@@ -48,6 +49,7 @@ public:
         int state = 0;          // 0 queued, 1 building, 2 built, 3 in batch, 4 done, 5 failed
         double t_admit = -1, t_built = -1, t_done = -1;
         int member = -1, status = 0;
+        int lane = 0;           // 0 small, 1 large (its own batch and stream)
         std::string error;
         BatchMemberStats stats;
         std::unique_ptr<Sweeper> sw;
@@ -70,7 +72,11 @@ private:
 
     ServerOptions o_;
     std::vector<std::unique_ptr<Request>> reqs_;
-    Batch batch_;
+    // Two lanes, each a batch on its own stream: requests of at least
+    // large_items cells x angles sweep in lane 1, so a deep mesh does not set
+    // the step time of the small ones; both lanes run on the GPU at once.
+    static constexpr int kLanes = 2;
+    Batch lanes_[kLanes];
     // build queue shared with the workers
     std::mutex mu_;
     std::condition_variable cv_work_, cv_built_;

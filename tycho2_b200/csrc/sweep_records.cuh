@@ -539,6 +539,40 @@ sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const 
     pair_solve_store_any<Real, VG>(p, R, g, in);
 }
 
+// Direct variant, two group vectors per task: the task covers 2*VG groups
+// of one item (vector width 8 in FP32, 4 in FP64), swept as two halves that
+// share the record (one load, one LU rebuild for compact records) and whose
+// sources are both read before the wait; half the threads of the one-vector
+// kernel for the same level.
+template <typename Real, int VG, int BS, typename Rec>
+__global__ void __launch_bounds__(BS)
+sweep_direct2_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const uint64_t begin, const uint64_t end)
+{
+    pdl_launch_dependents();
+    const uint32_t gpv = p.G / (2 * VG);
+    const uint32_t t = blockIdx.x * (uint32_t)BS + threadIdx.x;
+    const uint32_t itl = gpv == 1u ? t : __umulhi(t, p.vmagic);
+    const uint32_t g = (t - itl * gpv) * (2 * VG);
+    const uint64_t it = begin + itl;
+    bool live = it < end;
+    RegRecord<Real> R;
+    PairIn<Real, VG> in0, in1;
+    if (live) {
+        load_record(rec + it, R);
+        live = R.u(0) != kSentinel;
+    }
+    if (live) {
+        pair_load_source<Real, VG>(p, R, g, in0);
+        pair_load_source<Real, VG>(p, R, g + VG, in1);
+    }
+    pdl_wait_prerequisites();
+    if (!live) return;
+    pair_load_upwind<Real, VG, false>(p, R, g, in0);
+    pair_solve_store_any<Real, VG>(p, R, g, in0);
+    pair_load_upwind<Real, VG, false>(p, R, g + VG, in1);
+    pair_solve_store_any<Real, VG>(p, R, g + VG, in1);
+}
+
 // Wait on one completion flag: back-to-back polls first (one poll is an L2
 // round trip), then polls 64 ns apart; gives up after df.spin_limit polls
 // (records the item and face, raises abort) so that no wait can hang.
@@ -810,10 +844,14 @@ template <typename Real, int BS, typename Rec, int MINB>
 static const void *direct_fn_vg(int vg)
 {
     switch (vg) {
+    case 8:  // two 4-group halves per task (FP32)
+        if constexpr (sizeof(Real) == 4 && MINB == 1) return (const void *)sweep_direct2_level_kernel<Real, 4, BS, Rec>;
+        else return nullptr;
     case 1: return (const void *)sweep_direct_level_kernel<Real, 1, BS, Rec, MINB>;
     case 2: return (const void *)sweep_direct_level_kernel<Real, 2, BS, Rec, MINB>;
     case 4:
         if constexpr (sizeof(Real) == 4) return (const void *)sweep_direct_level_kernel<Real, 4, BS, Rec, MINB>;
+        else if constexpr (MINB == 1) return (const void *)sweep_direct2_level_kernel<Real, 2, BS, Rec>;  // FP64 halves
         else return nullptr;
     default: return nullptr;
     }

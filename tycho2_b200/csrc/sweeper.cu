@@ -61,6 +61,11 @@ Sweeper::~Sweeper()
     for (void *b : bufs)
         if (b) cudaFree(b);
     reducer_free(red_);
+    for (auto &st : aux_)
+        if (st) cudaStreamDestroy(st);
+    for (auto &ev : join_)
+        if (ev) cudaEventDestroy(ev);
+    if (fork_) cudaEventDestroy(fork_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -83,6 +88,9 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     fp32_ = o.fp32;
     TY_CHECK(build_schedule(tables_, quad_, sched_, err));
     TY_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    for (auto &st : aux_) TY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    TY_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    for (auto &ev : join_) TY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
 
     // Per-cell topology: neighbours and, per (face, local vertex), the
     // neighbour's vertex index (neighborVrtx o cellToFaceVrtx).
@@ -161,12 +169,24 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     return kOk;
 }
 
-int Sweeper::configure(int prec, int schedule, int variant, int knob, std::string &err, int vg)
+int Sweeper::configure(int prec, int schedule, int variant, int knob, std::string &err, int vg, int streams)
 {
     if (prec == 1 && !fp32_) { err = "sweeper was created without the FP32 sweep"; return kErrArg; }
+    if (streams != 1 && streams != 2 && streams != 4 && streams != 8) {
+        err = "streams must be 1, 2, 4 or 8";
+        return kErrArg;
+    }
+    if (streams > 1 && schedule != 1) { err = "several streams: level schedule only"; return kErrArg; }
     if (vg == 0) vg = (int)record_vg(prec != 0, (uint32_t)G_);
-    if (vg != 1 && vg != 2 && !(vg == 4 && prec == 1)) {
-        err = "group vector width must be 1 or 2 (FP64), 1, 2 or 4 (FP32)";
+    // one access moves up to 16 bytes (4 FP32 / 2 FP64 groups); the direct
+    // variants on levels also take two such vectors per task (8 / 4)
+    const bool halves = (prec == 1 && vg == 8) || (prec == 0 && vg == 4);
+    if (vg != 1 && vg != 2 && !(vg == 4 && prec == 1) && !halves) {
+        err = "group vector width must be 1, 2 (FP64: or 4) or 1, 2, 4 (FP32: or 8)";
+        return kErrArg;
+    }
+    if (halves && (variant < 3 || schedule != 1 || knob < 0)) {
+        err = "two group vectors per task: direct variants on the level schedule only";
         return kErrArg;
     }
     if (G_ % vg != 0) { err = "group vector width must divide the number of groups"; return kErrArg; }
@@ -225,8 +245,8 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
         TY_CUDA(prec ? tile_dataflow_blocks_per_sm<float>(variant == 4 ? 4 : knob, &per_sm)
                      : tile_dataflow_blocks_per_sm<double>(variant == 4 ? 4 : knob, &per_sm));
     else  // records; the direct variant's no-alloc sweep runs the 16-item record dataflow kernel
-        TY_CUDA(prec ? record_dataflow_blocks_per_sm<float>(variant == 3 ? 16 : knob, vg, &per_sm)
-                     : record_dataflow_blocks_per_sm<double>(variant == 3 ? 16 : knob, vg, &per_sm));
+        TY_CUDA(prec ? record_dataflow_blocks_per_sm<float>(variant == 3 ? 16 : knob, halves ? vg / 2 : vg, &per_sm)
+                     : record_dataflow_blocks_per_sm<double>(variant == 3 ? 16 : knob, halves ? vg / 2 : vg, &per_sm));
     if (per_sm < 1) { err = "dataflow kernel does not fit on an SM"; return kErrCuda; }
     int persist_per_sm = 0;
     if (schedule == 3) {
@@ -239,6 +259,7 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
     sh.variant = variant;
     sh.knob = knob;
     sh.vg = variant >= 2 ? vg : 1;
+    sh.streams = streams;
     sh.grid = (unsigned)(sms * per_sm);
     sh.persist_grid = (unsigned)(sms * persist_per_sm);
     sh.direct_grid = 0;
@@ -288,22 +309,28 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
                 if (variant >= 3 && ((knob > 0 && knob < 64) || sched == 3 || (sched == 2 && knob != 128)))
                     continue;
                 if (sched == 3 && (variant != 2 || (prec == 0 && knob == 32))) continue;
-                for (int vg : {1, 2, 4}) {
-                    if (vg > 1 && (variant < 2 || G_ % vg != 0 || (vg == 4 && prec == 0))) continue;
+                for (int vg : {1, 2, 4, 8}) {
+                    if (vg > 1 && (variant < 2 || G_ % vg != 0)) continue;
+                    const bool halves = (prec == 1 && vg == 8) || (prec == 0 && vg == 4);
+                    if (prec == 0 && vg == 8) continue;
+                    if (halves && (variant < 3 || sched != 1 || knob < 0)) continue;
                     if (variant >= 3 && sched == 2) {
                         const int gpv = G_ / vg;
                         if (gpv > 32 || (gpv & (gpv - 1)) != 0) continue;
                     }
-                    const int cs = configure(prec, sched, variant, knob, err, vg);
-                    if (cs == kErrOom) continue;  // records do not fit next to psi
-                    TY_CHECK(cs);
-                    double ms[2];
-                    TY_CHECK(time_sweeps(prec, 1, false, ms, err));  // warm-up (and graph capture)
-                    TY_CHECK(time_sweeps(prec, reps, false, ms, err));
-                    if (ms[0] < best) { best = ms[0]; keep = shape_[prec ? 1 : 0]; }
+                    for (int streams : {1, 2, 4, 8}) {
+                        if (streams > 1 && (sched != 1 || variant < 3)) continue;
+                        const int cs = configure(prec, sched, variant, knob, err, vg, streams);
+                        if (cs == kErrOom) continue;  // records do not fit next to psi
+                        TY_CHECK(cs);
+                        double ms[2];
+                        TY_CHECK(time_sweeps(prec, 1, false, ms, err));  // warm-up (and graph capture)
+                        TY_CHECK(time_sweeps(prec, reps, true, ms, err));   // L2 flushed, as in use
+                        if (ms[0] < best) { best = ms[0]; keep = shape_[prec ? 1 : 0]; }
+                    }
                 }
             }
-    TY_CHECK(configure(prec, keep.schedule, keep.variant, keep.knob, err, keep.vg));
+    TY_CHECK(configure(prec, keep.schedule, keep.variant, keep.knob, err, keep.vg, keep.streams));
     if (best_shape) *best_shape = shape_[prec ? 1 : 0];
     if (best_ms) *best_ms = best;
     return kOk;
@@ -323,8 +350,13 @@ int Sweeper::launch_dataflow_shape(int prec, const LevelArgs &p, const DataflowA
     else {
         TY_CHECK(ensure_records(prec, true, err));
         const int ipw = sh.variant == 3 ? 16 : sh.knob;
-        e = prec ? launch_dataflow_record<float>(ipw, p, d_rec_[1], df, sh.grid, s)
-                 : launch_dataflow_record<double>(ipw, p, d_rec_[0], df, sh.grid, s);
+        LevelArgs q = p;
+        if (q.vg > (prec ? 4u : 2u)) {  // two vectors per task: the record kernels take one
+            q.vg /= 2;
+            q.vmagic = group_magic(q.G / q.vg);
+        }
+        e = prec ? launch_dataflow_record<float>(ipw, q, d_rec_[1], df, sh.grid, s)
+                 : launch_dataflow_record<double>(ipw, q, d_rec_[0], df, sh.grid, s);
     }
     TY_CUDA(e);
     return kOk;
@@ -538,23 +570,35 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         cudaGraph_t graph;
         TY_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         cudaError_t le = cudaSuccess;
+        // one chain of level launches per octant group, each on its own
+        // stream (forked from and joined into stream_ inside the graph)
+        const int S = sh.streams;
+        if (S > 1) le = cudaEventRecord(fork_, stream_);
+        for (int g = 0; g < S && le == cudaSuccess; ++g) {
+        cudaStream_t st = S > 1 ? aux_[g] : stream_;
+        if (S > 1) le = cudaStreamWaitEvent(st, fork_, 0);
         for (uint32_t l = 0; l < sched_.n_levels && le == cudaSuccess; ++l) {
-            const uint64_t b = sched_.level_offset[l], e = sched_.level_offset[l + 1];
+            const uint64_t b = sched_.octant_offset[(size_t)l * kOctants + g * kOctants / S];
+            const uint64_t e = sched_.octant_offset[(size_t)l * kOctants + (g + 1) * kOctants / S];
+            if (e <= b) continue;
             if (sh.variant == 0)
-                le = prec ? launch_level<float>(sh.knob, p, b, e, stream_)
-                          : launch_level<double>(sh.knob, p, b, e, stream_);
+                le = prec ? launch_level<float>(sh.knob, p, b, e, st)
+                          : launch_level<double>(sh.knob, p, b, e, st);
             else if (sh.variant == 1)
-                le = prec ? launch_level_tile<float>(sh.knob, p, b, e, stream_)
-                          : launch_level_tile<double>(sh.knob, p, b, e, stream_);
+                le = prec ? launch_level_tile<float>(sh.knob, p, b, e, st)
+                          : launch_level_tile<double>(sh.knob, p, b, e, st);
             else if (sh.variant == 2)
-                le = prec ? launch_level_record<float>(sh.knob, p, d_rec_[1], b, e, stream_)
-                          : launch_level_record<double>(sh.knob, p, d_rec_[0], b, e, stream_);
+                le = prec ? launch_level_record<float>(sh.knob, p, d_rec_[1], b, e, st)
+                          : launch_level_record<double>(sh.knob, p, d_rec_[0], b, e, st);
             else if (sh.variant == 3)
-                le = prec ? launch_direct_level<float>(sh.knob, p, d_rec_[1], b, e, stream_, false)
-                          : launch_direct_level<double>(sh.knob, p, d_rec_[0], b, e, stream_, false);
+                le = prec ? launch_direct_level<float>(sh.knob, p, d_rec_[1], b, e, st, false)
+                          : launch_direct_level<double>(sh.knob, p, d_rec_[0], b, e, st, false);
             else
-                le = prec ? launch_direct_level<float>(sh.knob, p, d_crec_[1], b, e, stream_, true)
-                          : launch_direct_level<double>(sh.knob, p, d_crec_[0], b, e, stream_, true);
+                le = prec ? launch_direct_level<float>(sh.knob, p, d_crec_[1], b, e, st, true)
+                          : launch_direct_level<double>(sh.knob, p, d_crec_[0], b, e, st, true);
+        }
+        if (S > 1 && le == cudaSuccess) le = cudaEventRecord(join_[g], st);
+        if (S > 1 && le == cudaSuccess) le = cudaStreamWaitEvent(stream_, join_[g], 0);
         }
         cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
         TY_CUDA(le);

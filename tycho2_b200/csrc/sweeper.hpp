@@ -37,6 +37,7 @@ struct LaunchShape {
                         //   (knob = threads per block; level schedule)
     int knob = 4;
     int vg = 1;                 // records: groups per vector access of a psi row
+    int streams = 1;            // level schedule: octant groups swept on this many streams
     unsigned grid = 0;          // dataflow kernel of this variant: co-resident blocks
     unsigned persist_grid = 0;  // persistent-levels kernel: co-resident blocks
     unsigned direct_grid = 0;   // direct variants on the dataflow schedule: co-resident blocks
@@ -70,7 +71,7 @@ public:
     int write_psi(const std::string &path, std::string &err);
     int time_sweeps(int precision, int n, bool flush_l2, double *ms, std::string &err);
     // vg: record variant's groups per vector access (0 = widest dividing G).
-    int configure(int prec, int schedule, int variant, int knob, std::string &err, int vg = 0);
+    int configure(int prec, int schedule, int variant, int knob, std::string &err, int vg = 0, int streams = 1);
     int autotune(int prec, int reps, LaunchShape *best, double *best_ms, std::string &err);
     const LaunchShape &shape(int prec) const { return shape_[prec ? 1 : 0]; }
 
@@ -141,6 +142,10 @@ private:
     int last_psi_prec_ = -1;
 
     cudaStream_t stream_ = nullptr;
+    // level schedule on several streams: one per octant group, forked from
+    // and joined into stream_ inside the captured graph
+    cudaStream_t aux_[8] = {};
+    cudaEvent_t fork_ = nullptr, join_[8] = {};
     uint32_t *d_items_ = nullptr;
     double4 *d_abar64_ = nullptr;
     float4 *d_abar32_ = nullptr;

@@ -229,7 +229,7 @@ class SweeperCuda:
         return {"schedule": {1: "levels", 2: "dataflow", 3: "persist"}[sh.schedule],
                 "variant": {0: "items", 1: "tiles", 2: "records", 3: "direct", 4: "compact"}[sh.variant],
                 "knob": sh.knob,
-                "vector": sh.vector}
+                "vector": sh.vector, "streams": sh.streams}
 
     def autotune(self, precision, reps=3):
         """Picks the fastest launch shape (schedule, variant, knob) for one precision."""
@@ -239,12 +239,13 @@ class SweeperCuda:
         d["ms"] = ms.value
         return d
 
-    def configure(self, precision, schedule, variant, knob, vector=0):
+    def configure(self, precision, schedule, variant, knob, vector=0, streams=1):
         """schedule 'levels'|'dataflow'|'persist' (records only); variant 'items' (knob = lanes per item),
         'tiles' (knob = warps per block), 'records' (knob = items per warp) or 'direct' (records
         in registers, level schedule, knob = threads per block); vector = records' groups per
-        psi-row access, 0 = widest dividing nGroups."""
-        sh = _capi.LaunchShape(self.SCHEDULES[schedule], self.VARIANTS[variant], knob, vector)
+        psi-row access, 0 = widest dividing nGroups; streams: level schedule on 1, 2, 4 or 8 concurrent
+        streams (octant groups)."""
+        sh = _capi.LaunchShape(self.SCHEDULES[schedule], self.VARIANTS[variant], knob, vector, streams)
         check(lib().tycho_sweeper_configure(self._h, precision, C.byref(sh)))
 
     def shape(self, precision):
@@ -337,10 +338,12 @@ class SolveServer:
     STATES = {0: "queued", 1: "building", 2: "built", 3: "in batch", 4: "done", 5: "failed"}
 
     def __init__(self, method="mixed", budget_bytes=150e9, device=0, setup_threads=2, ipw32=0,
-                 ipw64=0, iter_max=3000, err_max=1e-10, inner_tol=1e-5, inner_max=200, refine_max=30):
+                 ipw64=0, iter_max=3000, err_max=1e-10, inner_tol=1e-5, inner_max=200, refine_max=30,
+                 large_items=0.0):
         solve = _capi.BatchOpts(BatchSolver.BATCH_METHODS[method], iter_max, err_max, inner_tol,
                                 inner_max, refine_max)
-        o = _capi.ServerOpts(device, float(budget_bytes), setup_threads, ipw32, ipw64, solve)
+        o = _capi.ServerOpts(device, float(budget_bytes), setup_threads, ipw32, ipw64, solve,
+                             float(large_items))
         h = C.c_void_p()
         check(lib().tycho_server_create(C.byref(o), C.byref(h)))
         self._h = h
