@@ -62,7 +62,8 @@ def parse():
     p.add_argument("--serve-requests", type=int, default=40)
     p.add_argument("--serve-rate", type=float, default=10.0, help="Poisson arrivals per second")
     p.add_argument("--shape", default="auto",
-                   help="launch shape 'schedule,variant,knob' for both precisions, or auto (autotuner)")
+                   help="launch shape 'schedule,variant,knob[,vector[,streams]]' for both precisions "
+                        "(an FP32-only vector width falls back to the widest for FP64), or auto (autotuner)")
     return p.parse_args()
 
 
@@ -399,9 +400,12 @@ def run_b200(args):
     if args.shape == "auto":
         tuned = {1: sw.autotune(1, 5), 0: sw.autotune(0, 5)}
     else:
-        s, v, k = args.shape.split(",")
+        parts = args.shape.split(",")
+        s, v, k = parts[:3]
+        vec = int(parts[3]) if len(parts) > 3 else 0
+        streams = int(parts[4]) if len(parts) > 4 else 1
         for prec in (1, 0):
-            sw.configure(prec, s, v, int(k))
+            sw.configure(prec, s, v, int(k), vec if (prec == 1 or vec <= 2) else 0, streams)
         tuned = {1: sw.shape(1), 0: sw.shape(0)}
     shape32, shape64 = sw.shape(1), sw.shape(0)
 

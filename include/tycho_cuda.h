@@ -57,8 +57,17 @@ typedef enum tycho_method {
     TYCHO_MIXED_GMRES = 2       /* FP32-sweep GMRES inside FP64 iterative refinement */
 } tycho_method;
 
-/* Local 4x4 solve (deck key GaussElim, src/Global.hh:99-105). */
-typedef enum tycho_gauss_elim { TYCHO_GAUSS_ORIGINAL = 0, TYCHO_GAUSS_NOPIVOT = 1 } tycho_gauss_elim;
+/* Local 4x4 solve (deck key GaussElim, src/Global.hh:99-105; the four cases
+   of gaussElim4, src/Transport.cc:277-677).  NoPivot runs in every kernel;
+   Original and the Cramer solvers in the direct record kernels on the level
+   schedule (128 threads per block), which a sweeper with one of them
+   configures by default. */
+typedef enum tycho_gauss_elim {
+    TYCHO_GAUSS_ORIGINAL = 0,
+    TYCHO_GAUSS_NOPIVOT = 1,
+    TYCHO_GAUSS_CRAMER_GLU = 2,
+    TYCHO_GAUSS_CRAMER_INTEL = 3
+} tycho_gauss_elim;
 
 typedef struct tycho_mesh tycho_mesh;       /* host-side mesh (ingest + tables) */
 typedef struct tycho_sweeper tycho_sweeper; /* device-resident sweep instance */

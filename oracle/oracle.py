@@ -92,7 +92,8 @@ class Oracle:
         self.A = lib().oc_num_angles(self.h)
         self.G = groups
         self.nc = mesh.n_cells
-        lib().oc_set_gauss_elim(self.h, {"Original": 0, "NoPivot": 1}[gauss_elim])
+        lib().oc_set_gauss_elim(self.h, {"Original": 0, "NoPivot": 1, "CramerGlu": 2,
+                                         "CramerIntel": 3}[gauss_elim])
         if lib().oc_cyclic(self.h):
             raise ValueError("cyclic sweep graph")
 

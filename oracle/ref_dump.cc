@@ -77,6 +77,13 @@ static void setup(const char *pmesh, int sn, int groups)
     g_intraAngleP = 1;   /* b-level priorities: priorities == b-levels */
     g_interAngleP = 0;   /* interleaved: no per-angle offset */
     g_gaussElim = GaussElim_NoPivot;
+    if (const char *ge = getenv("TYCHO_GAUSS_ELIM")) {  // deck key GaussElim
+        std::string k = ge;
+        g_gaussElim = k == "Original" ? GaussElim_Original
+                      : k == "CramerGlu" ? GaussElim_CramerGlu
+                      : k == "CramerIntel" ? GaussElim_CramerIntel
+                                           : GaussElim_NoPivot;
+    }
     g_mpiType = MPIType_TychoTwoSided;
     g_sweepType = SweepType_TraverseGraph;
     g_quadrature = new Quadrature(g_snOrder);

@@ -328,7 +328,8 @@ typedef struct {
     uint32_t *tlevel;   /* (a, c): longest upwind chain */
     uint32_t *ndep;     /* (a, c): dependency count, src/GraphTraverser.cc:442-458 */
     int cyclic;         /* 1 if some angle's graph has a cycle */
-    int gauss_elim;     /* 0 Original (pivoting), 1 NoPivot (src/Global.hh:99-105) */
+    int gauss_elim;     /* 0 Original (pivoting), 1 NoPivot, 2 CramerGlu, 3 CramerIntel
+                           (src/Global.hh:99-105) */
 } OCtx;
 
 void oc_free(OCtx *x)
@@ -530,6 +531,87 @@ static void gauss_nopivot(double A[4][4], double b[4])
     b[0] = b[0] - A[0][3] * b[3] - A[0][2] * b[2] - A[0][1] * b[1];
 }
 
+/* gaussElim4 CramerGlu (src/Transport.cc:414-557): the inverse by cofactors,
+   then x = inv b.  inv[4a + b] is the (b, a) cofactor, (-1)^(a+b) times the
+   minor without row b and column a, expanded along its first column c0 over
+   the rows r in increasing order, each row's 2x2 minor written as
+   m[r][c0] m[r'][c1] m[r''][c2] - m[r][c0] m[r'][c2] m[r''][c1] (r' < r'',
+   c0 < c1 < c2), every product left to right and the six terms summed left
+   to right: the operation order the reference's expressions have. */
+static void gauss_cramer_glu(double A[4][4], double b[4])
+{
+    double inv[16], det;
+    for (int a = 0; a < 4; a++)
+        for (int bb = 0; bb < 4; bb++) {
+            int rows[3], cols[3], nr = 0, ncl = 0;
+            for (int r = 0; r < 4; r++) if (r != bb) rows[nr++] = r;
+            for (int c = 0; c < 4; c++) if (c != a) cols[ncl++] = c;
+            double sign = ((a + bb) & 1) ? -1.0 : 1.0, acc = 0.0;
+            for (int k = 0; k < 3; k++) {
+                int r = rows[k], r1 = rows[k == 0 ? 1 : 0], r2 = rows[k == 2 ? 1 : 2];
+                double sg = (k & 1) ? -sign : sign;
+                double t1 = A[r][cols[0]] * A[r1][cols[1]] * A[r2][cols[2]];
+                double t2 = A[r][cols[0]] * A[r1][cols[2]] * A[r2][cols[1]];
+                if (k == 0) acc = sg > 0 ? t1 : -t1;
+                else acc = sg > 0 ? acc + t1 : acc - t1;
+                acc = sg > 0 ? acc - t2 : acc + t2;
+            }
+            inv[4 * a + bb] = acc;
+        }
+    det = A[0][0] * inv[0] + A[0][1] * inv[4] + A[0][2] * inv[8] + A[0][3] * inv[12];
+    det = 1.0 / det;
+    for (int i = 0; i < 16; i++) inv[i] = inv[i] * det;
+    double x[4];
+    for (int r = 0; r < 4; r++) x[r] = inv[4 * r] * b[0] + inv[4 * r + 1] * b[1] + inv[4 * r + 2] * b[2] + inv[4 * r + 3] * b[3];
+    for (int r = 0; r < 4; r++) b[r] = x[r];
+}
+
+/* gaussElim4 CramerIntel (src/Transport.cc:559-677): the scalar form of
+   Intel's SSE 4x4 inverse (application note "Streaming SIMD Extensions -
+   Inverse of 4x4 Matrix").  src is A column-major; pairs of products of two
+   rows of src (tmp), cofactors as (three tmp x src products) minus (three
+   more), determinant, scaling, x = inv b.  The tables give each cofactor's
+   (tmp, src) pairs in the order the reference sums them. */
+static const unsigned char kIntelCof[16][6][2] = {
+    {{0, 5}, {3, 6}, {4, 7}, {1, 5}, {2, 6}, {5, 7}},       {{1, 4}, {6, 6}, {9, 7}, {0, 4}, {7, 6}, {8, 7}},
+    {{2, 4}, {7, 5}, {10, 7}, {3, 4}, {6, 5}, {11, 7}},     {{5, 4}, {8, 5}, {11, 6}, {4, 4}, {9, 5}, {10, 6}},
+    {{1, 1}, {2, 2}, {5, 3}, {0, 1}, {3, 2}, {4, 3}},       {{0, 0}, {7, 2}, {8, 3}, {1, 0}, {6, 2}, {9, 3}},
+    {{3, 0}, {6, 1}, {11, 3}, {2, 0}, {7, 1}, {10, 3}},     {{4, 0}, {9, 1}, {10, 2}, {5, 0}, {8, 1}, {11, 2}},
+    {{0, 13}, {3, 14}, {4, 15}, {1, 13}, {2, 14}, {5, 15}}, {{1, 12}, {6, 14}, {9, 15}, {0, 12}, {7, 14}, {8, 15}},
+    {{2, 12}, {7, 13}, {10, 15}, {3, 12}, {6, 13}, {11, 15}}, {{5, 12}, {8, 13}, {11, 14}, {4, 12}, {9, 13}, {10, 14}},
+    {{2, 10}, {5, 11}, {1, 9}, {4, 11}, {0, 9}, {3, 10}},   {{8, 11}, {0, 8}, {7, 10}, {6, 10}, {9, 11}, {1, 8}},
+    {{6, 9}, {11, 11}, {3, 8}, {10, 11}, {2, 8}, {7, 9}},   {{10, 10}, {4, 8}, {9, 9}, {8, 9}, {11, 10}, {5, 8}}};
+/* column pairs (p, q) of the tmp products, in order: tmp[2k] = s[p] s[q'] ... */
+static const unsigned char kIntelPairs[6][2] = {{2, 3}, {1, 3}, {1, 2}, {0, 3}, {0, 2}, {0, 1}};
+
+static void gauss_cramer_intel(double A[4][4], double b[4])
+{
+    double src[16], dst[16], tmp[12], det;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) src[i + 4 * j] = A[i][j];
+    for (int half = 0; half < 2; half++) {
+        /* first half: rows 2, 3 of src (8..15); second: rows 0, 1 (0..7) */
+        const int lo = half ? 0 : 8, hi = half ? 4 : 12;
+        for (int k = 0; k < 6; k++) {
+            const int p = kIntelPairs[k][0], q = kIntelPairs[k][1];
+            tmp[2 * k] = src[lo + p] * src[hi + q];
+            tmp[2 * k + 1] = src[lo + q] * src[hi + p];
+        }
+        for (int j = 8 * half; j < 8 * half + 8; j++) {
+            const unsigned char(*t)[2] = kIntelCof[j];
+            double plus = tmp[t[0][0]] * src[t[0][1]] + tmp[t[1][0]] * src[t[1][1]] + tmp[t[2][0]] * src[t[2][1]];
+            double minus = tmp[t[3][0]] * src[t[3][1]] + tmp[t[4][0]] * src[t[4][1]] + tmp[t[5][0]] * src[t[5][1]];
+            dst[j] = plus - minus;
+        }
+    }
+    det = src[0] * dst[0] + src[1] * dst[1] + src[2] * dst[2] + src[3] * dst[3];
+    det = 1 / det;
+    for (int j = 0; j < 16; j++) dst[j] *= det;
+    double x[4];
+    for (int r = 0; r < 4; r++) x[r] = dst[4 * r] * b[0] + dst[4 * r + 1] * b[1] + dst[4 * r + 2] * b[2] + dst[4 * r + 3] * b[3];
+    for (int r = 0; r < 4; r++) b[r] = x[r];
+}
+
 /* One (cell, angle) update: SweepData::update + Transport::populateLocalPsiBound
    + Transport::solve (src/SweepData.hh:139-174, src/Transport.cc:57-271,
    :687-776).  Source per (v,g): angular part (psi layout, may be NULL) plus
@@ -602,7 +684,12 @@ static void cell_update(const OCtx *x, uint64_t c, int a, const double *src_ang,
                 }
             }
         }
-        if (x->gauss_elim == 0) gauss_original(M, b); else gauss_nopivot(M, b);
+        switch (x->gauss_elim) {
+        case 0: gauss_original(M, b); break;
+        case 2: gauss_cramer_glu(M, b); break;
+        case 3: gauss_cramer_intel(M, b); break;
+        default: gauss_nopivot(M, b); break;
+        }
         for (int v = 0; v < 4; v++) psi[(((size_t)c * A + a) * 4 + v) * G + g] = b[v];
     }
 }

@@ -14,7 +14,10 @@ reference built from it by `make -C oracle ref` (oracle/_ref).  Writes:
                                s{4,8}_{adj,nbr,f2c,c2f,deps,blev}  integer tables
                                s4_vol, s4_area, s4_odn             geometry (f64)
                                sweep_* : one SweeperTraverse::sweep of a seeded
-                                         angular source, S4, G=3
+                                         angular source, S4, G=3 (GaussElim
+                                         NoPivot); sweep_psi_<kind>: its first
+                                         group with GaussElim Original,
+                                         CramerGlu, CramerIntel
                                si_*    : SourceIteration::fixedPoint with the
                                          hat source, per-cell sigma, S4, G=2
 
@@ -37,8 +40,9 @@ REF = os.environ.get("TYCHO2_REF", "/root/reference")
 REF_BIN = os.path.join(ROOT, "oracle", "_ref")
 
 
-def run(*args, cwd=None):
-    subprocess.run(list(args), check=True, cwd=cwd, stdout=subprocess.DEVNULL)
+def run(*args, cwd=None, env=None):
+    subprocess.run(list(args), check=True, cwd=cwd, stdout=subprocess.DEVNULL,
+                   env=None if env is None else dict(os.environ, **env))
 
 
 def kuhn3_fixture(tmp):
@@ -72,6 +76,13 @@ def kuhn3_fixture(tmp):
     out["sweep_sigma_t"] = sig_t
     out["sweep_source"] = src
     out["sweep_psi"] = np.fromfile(f_psi, np.float64).reshape(nc, A, 4, G)
+    # The same sweep, first group only, with each other GaussElim solver.
+    src1 = np.ascontiguousarray(src[..., :1])
+    src1.tofile(f_src)
+    for kind in ("Original", "CramerGlu", "CramerIntel"):
+        run(os.path.join(REF_BIN, "ref_dump.x"), "sweep", pmesh, "4", "1", f_st, f_src, f_psi,
+            env={"TYCHO_GAUSS_ELIM": kind})
+        out["sweep_psi_" + kind] = np.fromfile(f_psi, np.float64).reshape(nc, A, 4, 1)
     # Source iteration with the hat source and per-cell cross sections.
     G = 2
     sig_t = rng.uniform(1.0, 4.0, nc)

@@ -122,3 +122,40 @@ def test_batch_errors(built, workdir):
     with pytest.raises(ty.TychoError):
         b.add(plain, "mixed")
     b.close()
+
+
+def test_batch_members_with_other_solvers(built, workdir):
+    """Members with GaussElim Original / CramerGlu / CramerIntel next to
+    NoPivot ones: each bit-identical alone and in the mix, and each member's
+    FP64 source iteration equal to the oracle's with its own solver."""
+    import tycho2_b200 as ty
+    from oracle.oracle import Oracle
+    kinds = ["Original", "NoPivot", "CramerGlu", "CramerIntel"]
+    sws, refs = [], []
+    for k, (kind, case) in enumerate(zip(kinds, CASES)):
+        n, jitter, sn, G, ratio, down = case
+        mesh, om = kuhn(workdir, n, jitter, seed=200 + k)
+        rng = np.random.default_rng(200 + k)
+        st = rng.lognormal(0.0, 0.5, mesh.n_cells)
+        ss = ratio * st
+        q = np.ones((mesh.n_cells, 4, G))
+        sw = ty.SweeperCuda(mesh, sn, G, fp32=True, gauss_elim=kind)
+        sw.set_cross_sections(st, ss)
+        sw.set_source(q, "isotropic")
+        sws.append(sw)
+        _, phi_ref, it_ref, _ = Oracle(om, sn, G, gauss_elim=kind).source_iteration(
+            st, ss, q_iso=q, iter_max=400, err_max=1e-10)
+        refs.append((phi_ref, it_ref))
+    alone = [_solve([sw], "si", ipw=0, err_max=1e-10, iter_max=400)[0] for sw in sws]
+    mixed = _solve(sws, "si", ipw=0, err_max=1e-10, iter_max=400)
+    for kind, (pa, sa, _), (pm, _, _), (phi_ref, it_ref) in zip(kinds, alone, mixed, refs):
+        assert bits_equal(pa, pm), kind
+        if sa["iterations"] == it_ref:
+            assert bits_equal(pa, phi_ref), kind
+        else:
+            assert rel_l1(pa, phi_ref) <= 1e-9, kind
+    mixed32 = _solve(sws, "mixed", ipw=0, err_max=1e-11)
+    for kind, (pm, _, done), (phi_ref, _) in zip(kinds, mixed32, refs):
+        assert done and rel_l1(pm, phi_ref) <= 1e-8, kind
+    with pytest.raises(ty.TychoError):  # the shared-memory batch kernels take NoPivot only
+        ty.BatchSolver(ipw32=16, ipw64=16).add(sws[0], "si")

@@ -302,3 +302,70 @@ def test_autotune_keeps_results_bit_exact(built, workdir):
     psi = np.empty(sw.psi_shape)
     sw.sweep(psi, src)
     assert bits_equal(psi, o.sweep(st, src_ang=src))
+
+
+@pytest.mark.parametrize("kind", ["Original", "CramerGlu", "CramerIntel"])
+def test_fp64_sweep_other_solvers_bit_exact(built, workdir, kuhn3_ref, kind):
+    """GaussElim Original / CramerGlu / CramerIntel: the reference's own sweep
+    (fixture) and the oracle, bit for bit, in both direct record forms."""
+    import tycho2_b200 as ty
+    from oracle.oracle import Oracle
+    r = kuhn3_ref
+    mesh = ty.TychoMesh.kuhn_cube(3, 0.05, 2024, 100.0)
+    src1 = np.ascontiguousarray(r["sweep_source"][..., :1])
+    for variant, streams in (("compact", 1), ("direct", 2)):
+        sw = ty.SweeperCuda(mesh, 4, 1, gauss_elim=kind)
+        assert sw.shape(0)["variant"] == "compact"  # the default for these solvers
+        sw.configure(0, "levels", variant, 128, 0, streams)
+        sw.set_cross_sections(r["sweep_sigma_t"], np.zeros(mesh.n_cells))
+        psi = np.empty(sw.psi_shape)
+        sw.sweep(psi, src1)
+        assert bits_equal(psi, r["sweep_psi_" + kind]), (kind, variant)
+        sw.close()
+    for n, sn, G in [(4, 8, 4), (3, 6, 3)]:
+        mesh, om = kuhn(workdir, n, 0.05, seed=77)
+        o = Oracle(om, sn, G, gauss_elim=kind)
+        rng = np.random.default_rng(n * G)
+        st = rng.lognormal(0.0, 0.5, mesh.n_cells)
+        src = rng.uniform(-0.2, 1.0, o.psi_shape)
+        for variant in ("compact", "direct"):
+            sw = ty.SweeperCuda(mesh, sn, G, gauss_elim=kind)
+            sw.configure(0, "levels", variant, 128)
+            sw.set_cross_sections(st, np.zeros(mesh.n_cells))
+            psi = np.empty(sw.psi_shape)
+            sw.sweep(psi, src)
+            assert bits_equal(psi, o.sweep(st, src_ang=src)), (kind, variant, n, sn, G)
+            sw.close()
+
+
+def test_other_solvers_reject_unsupported_shapes(built, workdir):
+    import tycho2_b200 as ty
+    mesh, _ = kuhn(workdir, 2, 0.05, seed=1)
+    sw = ty.SweeperCuda(mesh, 4, 2, gauss_elim="Original")
+    for shape in (("levels", "tiles", 4), ("dataflow", "compact", 128), ("levels", "compact", 64),
+                  ("levels", "records", 16)):
+        with pytest.raises(ty.TychoError):
+            sw.configure(0, *shape)
+    with pytest.raises(ty.TychoError):
+        ty.SweeperCuda(mesh, 4, 2, gauss_elim="CramerGlu", schedule="dataflow")
+    sw.close()
+
+
+@pytest.mark.parametrize("kind", ["Original", "CramerIntel"])
+def test_fp32_other_solvers_within_tolerance(built, workdir, kind):
+    from oracle.oracle import Oracle
+    import tycho2_b200 as ty
+    mesh, om = kuhn(workdir, 5, 0.05, seed=9)
+    G = 4
+    o = Oracle(om, 8, G, gauss_elim=kind)
+    rng = np.random.default_rng(5)
+    st = rng.lognormal(0.0, 0.5, mesh.n_cells)
+    src = rng.uniform(0.0, 1.0, (mesh.n_cells, 4, G))
+    sw = ty.SweeperCuda(mesh, 8, G, fp32=True, gauss_elim=kind)
+    sw.set_cross_sections(st, 0.5 * st)
+    sw.set_source(src, "isotropic")
+    phi, _, stats = sw.solve("mixed", iter_max=200, err_max=1e-12)
+    assert stats["sweeps_fp32"] > 0
+    _, phi_ref, _, _ = o.source_iteration(st, 0.5 * st, q_iso=src, iter_max=400, err_max=1e-13)
+    assert rel_l1(phi, phi_ref) <= 1e-8
+    sw.close()

@@ -81,6 +81,11 @@ def test_oracle_sweep_and_si_match_reference(built, workdir, kuhn3_ref):
     o = Oracle(om, 4, 3)
     psi = o.sweep(r["sweep_sigma_t"], src_ang=np.ascontiguousarray(r["sweep_source"]))
     assert bits_equal(psi, r["sweep_psi"])
+    # the other 4x4 solvers of gaussElim4 (deck key GaussElim), bit for bit
+    src1 = np.ascontiguousarray(r["sweep_source"][..., :1])
+    for kind in ("Original", "CramerGlu", "CramerIntel"):
+        psi = Oracle(om, 4, 1, gauss_elim=kind).sweep(r["sweep_sigma_t"], src_ang=src1)
+        assert bits_equal(psi, r["sweep_psi_" + kind]), kind
     o = Oracle(om, 4, 2)
     src = o.hat_source(r["si_sigma_t"], r["si_sigma_s"])
     psi, phi, iters, err = o.source_iteration(r["si_sigma_t"], r["si_sigma_s"], q_ang=src,

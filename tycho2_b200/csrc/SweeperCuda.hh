@@ -60,8 +60,10 @@ public:
         tycho_sweeper_opts opts;
         opts.sn_order = (int)g_snOrder;
         opts.n_groups = (int)g_nGroups;
-        opts.gauss_elim = g_gaussElim == GaussElim_Original ? TYCHO_GAUSS_ORIGINAL
-                                                             : TYCHO_GAUSS_NOPIVOT;
+        opts.gauss_elim = g_gaussElim == GaussElim_Original     ? TYCHO_GAUSS_ORIGINAL
+                          : g_gaussElim == GaussElim_CramerGlu   ? TYCHO_GAUSS_CRAMER_GLU
+                          : g_gaussElim == GaussElim_CramerIntel ? TYCHO_GAUSS_CRAMER_INTEL
+                                                                 : TYCHO_GAUSS_NOPIVOT;
         opts.device = 0;
         opts.fp32 = 0;
         opts.tpi64 = 0;

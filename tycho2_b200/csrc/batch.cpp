@@ -109,6 +109,10 @@ int Batch::add(Sweeper *sw, const BatchOptions &o, int &id, std::string &err)
     }
     for (const auto &m : members_)
         if (m.sw == sw) { err = "sweeper is already in the batch"; return kErrArg; }
+    if (sw->solver() != kSolveNoPivot && (ipw_[0] != 0 || (o.method == 2 && ipw_[1] != 0))) {
+        err = "GaussElim Original / Cramer members need the direct batch kernels (items per warp 0)";
+        return kErrArg;
+    }
     TB_CUDA(cudaSetDevice(device_));
     Member m;
     m.sw = sw;
@@ -258,6 +262,7 @@ void Batch::fill_slot(int prec, const Member &m, BatchSlot &s) const
     s.vmagic = magic(s.G / s.vg);
     s.n_levels = v.n_levels;
     s.level_shift = m.shift;
+    s.solver = (uint32_t)m.sw->solver();
     s.active = 0;
     if (prec == 0 && m.state == kRunSI) {
         s.active = 1;
@@ -308,6 +313,8 @@ int Batch::build_graph(int prec, std::string &err)
         for (uint32_t c = 0; c < kBatchClasses; ++c)
             cuts[L].c[c + 1] = cuts[L].c[c] + (unsigned)std::min<uint64_t>((chunks[c] + 3) / 4, kLevelGridCap);
     }
+    bool any_solver = false;
+    for (const auto &m : members_) any_solver = any_solver || m.sw->solver() != kSolveNoPivot;
     cudaGraph_t g;
     TB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     const uint32_t rec_bytes =
@@ -316,8 +323,8 @@ int Batch::build_graph(int prec, std::string &err)
     if (e == cudaSuccess && prec == 0) e = launch_batch_accept(d_slots_[prec], plan_, kStreamGrid, stream_);
     if (e == cudaSuccess) e = launch_batch_scatter(d_slots_[prec], plan_, kStreamGrid, stream_);
     for (uint32_t L = 0; L < max_levels_ && e == cudaSuccess; ++L)
-        e = prec ? launch_batch_level<float>(ipw, d_slots_[prec], plan_, L, cuts[L], stream_)
-                 : launch_batch_level<double>(ipw, d_slots_[prec], plan_, L, cuts[L], stream_);
+        e = prec ? launch_batch_level<float>(ipw, d_slots_[prec], plan_, L, cuts[L], any_solver, stream_)
+                 : launch_batch_level<double>(ipw, d_slots_[prec], plan_, L, cuts[L], any_solver, stream_);
     if (e == cudaSuccess) e = launch_batch_psi_to_phi(prec == 1, d_slots_[prec], plan_, kStreamGrid, stream_);
     if (e == cudaSuccess) e = launch_batch_post(d_slots_[prec], plan_, kStreamGrid, stream_);
     if (e == cudaSuccess) e = launch_batch_finish(d_slots_[prec], plan_, 64, stream_);

@@ -9,9 +9,10 @@ cudaError_t batch_level_launch(const void *fn, const BatchSlot *slots, const Bat
 
 template <>
 cudaError_t launch_batch_level<float>(int ipw, const BatchSlot *slots, const BatchPlan &pl, uint32_t level,
-                                      const BatchCuts &cut, cudaStream_t s)
+                                      const BatchCuts &cut, bool any_solver, cudaStream_t s)
 {
-    const void *fn = ipw == 0    ? (const void *)batch_direct_level_kernel<float>
+    const void *fn = ipw == 0    ? (any_solver ? (const void *)batch_direct_level_kernel<float, true>
+                                               : (const void *)batch_direct_level_kernel<float, false>)
                      : ipw == 8  ? (const void *)batch_level_kernel<float, 8>
                      : ipw == 16 ? (const void *)batch_level_kernel<float, 16>
                      : ipw == 32 ? (const void *)batch_level_kernel<float, 32>

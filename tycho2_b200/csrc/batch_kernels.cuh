@@ -93,6 +93,7 @@ batch_plan_kernel(const BatchSlot *__restrict__ slots, uint32_t n_slots, uint32_
                     sg.chunk_begin = chunk_run + ex_c;
                     sg.G = sl.G;
                     sg.vmagic = sl.vmagic;
+                    sg.solver = sl.solver;
                     segs[seg_run + ex_s] = sg;
                 }
                 chunk_run += tot_c;
@@ -153,6 +154,7 @@ __device__ __forceinline__ LevelArgs slot_args(const BatchSlot &s)
     p.G = s.G;
     p.vg = s.vg;
     p.vmagic = s.vmagic;
+    p.solver = s.solver;
     return p;
 }
 
@@ -192,7 +194,7 @@ __device__ __forceinline__ void batch_class_body(const BatchSlot *__restrict__ s
 // in global memory), so a warp's member lookup is a shared-memory search.
 constexpr uint32_t kBatchSegSmem = 256;
 
-template <typename Real, int VG>
+template <typename Real, int VG, bool ANY>
 __device__ __forceinline__ void batch_direct_body(const BatchPlan &pl, uint32_t L, uint32_t cls, uint32_t blk,
                                                   uint32_t nblk, BatchSeg *sseg, bool &waited)
 {
@@ -214,12 +216,13 @@ __device__ __forceinline__ void batch_direct_body(const BatchPlan &pl, uint32_t 
         p.G = sg.G;
         p.vg = VG;
         p.vmagic = sg.vmagic;
+        p.solver = sg.solver;
         const uint32_t gpv = p.G / VG;
         const uint32_t task = (ch - sg.chunk_begin) * 32u + lane;
         const uint32_t itl = gpv == 1u ? task : __umulhi(task, p.vmagic);
         const uint32_t g = (task - itl * gpv) * VG;
         RegRecord<Real> R;
-        load_record((const CompactRecord<Real> *)sg.rec + itl, R);
+        load_record((const CompactRecord<Real> *)sg.rec + itl, R, ANY ? p.solver : (uint32_t)kSolveNoPivot);
         const bool live = R.u(0) != kSentinel;
         PairIn<Real, VG> in;
         if (live) pair_load_source<Real, VG>(p, R, g, in);
@@ -229,12 +232,14 @@ __device__ __forceinline__ void batch_direct_body(const BatchPlan &pl, uint32_t 
         }
         if (live) {
             pair_load_upwind<Real, VG, false>(p, R, g, in);
-            pair_solve_store_any<Real, VG>(p, R, g, in);
+            pair_solve_store_any<Real, VG, RegRecord<Real>, ANY>(p, R, g, in);
         }
     }
 }
 
-template <typename Real>
+// ANY: some member solves with Original or a Cramer solver (each member's
+// own p.solver); otherwise every member uses NoPivot.
+template <typename Real, bool ANY>
 __global__ void __launch_bounds__(128)
 batch_direct_level_kernel(const BatchSlot *__restrict__ slots, BatchPlan pl, uint32_t L, BatchCuts cut)
 {
@@ -243,11 +248,11 @@ batch_direct_level_kernel(const BatchSlot *__restrict__ slots, BatchPlan pl, uin
     bool waited = false;
     const uint32_t b = blockIdx.x;
     if (b < cut.c[1]) {
-        batch_direct_body<Real, 1>(pl, L, 0, b, cut.c[1], sseg, waited);
+        batch_direct_body<Real, 1, ANY>(pl, L, 0, b, cut.c[1], sseg, waited);
     } else if (b < cut.c[2]) {
-        batch_direct_body<Real, 2>(pl, L, 1, b - cut.c[1], cut.c[2] - cut.c[1], sseg, waited);
+        batch_direct_body<Real, 2, ANY>(pl, L, 1, b - cut.c[1], cut.c[2] - cut.c[1], sseg, waited);
     } else if constexpr (sizeof(Real) == 4) {
-        batch_direct_body<Real, 4>(pl, L, 2, b - cut.c[2], cut.c[3] - cut.c[2], sseg, waited);
+        batch_direct_body<Real, 4, ANY>(pl, L, 2, b - cut.c[2], cut.c[3] - cut.c[2], sseg, waited);
     }
     if (!waited) pdl_wait_prerequisites();
     (void)slots;

@@ -31,6 +31,7 @@ struct alignas(16) BatchSlot {
     uint64_t nc;
     uint32_t A, G, vg, vmagic, n_levels, op, active, accept;
     uint32_t level_shift;  // the member's level l runs at global level level_shift + l
+    uint32_t solver;       // 4x4 solver (GaussElim), numbered as tycho_gauss_elim
 };
 
 // One member's items at one level, with what a warp needs to sweep them
@@ -44,6 +45,7 @@ struct alignas(16) BatchSeg {
     uint32_t chunk_begin;  // first chunk of this segment within the level
     uint32_t G;
     uint32_t vmagic;
+    uint32_t solver;       // the member's 4x4 solver (GaussElim)
 };
 
 // Members are split by vector width (groups per psi-row access): class 0
@@ -79,15 +81,17 @@ cudaError_t launch_batch_psi_to_phi(bool fp32, const BatchSlot *slots, const Bat
                                     cudaStream_t s);
 cudaError_t launch_batch_post(const BatchSlot *slots, const BatchPlan &pl, unsigned grid, cudaStream_t s);
 cudaError_t launch_batch_finish(const BatchSlot *slots, const BatchPlan &pl, unsigned grid, cudaStream_t s);
-// One global level: cut.c[3] blocks of 4 warps (programmatic dependent launch).
+// One global level: cut.c[3] blocks of 4 warps (programmatic dependent launch);
+// any_solver: some member solves with Original or a Cramer solver (direct
+// kernel only; the shared-memory record kernels take NoPivot).
 template <typename Real>
 cudaError_t launch_batch_level(int ipw, const BatchSlot *slots, const BatchPlan &pl, uint32_t level,
-                               const BatchCuts &cut, cudaStream_t s);
+                               const BatchCuts &cut, bool any_solver, cudaStream_t s);
 template <>
 cudaError_t launch_batch_level<double>(int ipw, const BatchSlot *slots, const BatchPlan &pl, uint32_t level,
-                                       const BatchCuts &cut, cudaStream_t s);
+                                       const BatchCuts &cut, bool any_solver, cudaStream_t s);
 template <>
 cudaError_t launch_batch_level<float>(int ipw, const BatchSlot *slots, const BatchPlan &pl, uint32_t level,
-                                      const BatchCuts &cut, cudaStream_t s);
+                                      const BatchCuts &cut, bool any_solver, cudaStream_t s);
 
 }  // namespace tycho

@@ -270,10 +270,11 @@ int tycho_sweeper_create(const tycho_mesh *mesh, const tycho_sweeper_opts *opts,
             return finish(TYCHO_ERR_ARG, "schedule must be 0, 1 or 2");
         }
         std::string err;
-        if (opts->gauss_elim != TYCHO_GAUSS_NOPIVOT && opts->gauss_elim != TYCHO_GAUSS_ORIGINAL) {
+        if (opts->gauss_elim < TYCHO_GAUSS_ORIGINAL || opts->gauss_elim > TYCHO_GAUSS_CRAMER_INTEL) {
             delete h;
-            return finish(TYCHO_ERR_ARG, "GaussElim must be Original or NoPivot");
+            return finish(TYCHO_ERR_ARG, "GaussElim must be Original, NoPivot, CramerGlu or CramerIntel");
         }
+        o.gauss_elim = opts->gauss_elim;
         int st = h->sw.init(mesh->tab, o, err);
         if (st != tycho::kOk) { delete h; return finish(st, err); }
         *out = h;

@@ -8,6 +8,12 @@
 
 namespace tycho {
 
+// The 4x4 solvers of gaussElim4 (deck key GaussElim, src/Global.hh:99-105),
+// numbered as tycho_gauss_elim.  Each one factors the group-independent
+// matrix once per item into 16 numbers (and, for Original, a row order) and
+// applies them to every group's right-hand side in the reference's order.
+enum SolveKind : uint32_t { kSolveOriginal = 0, kSolveNoPivot = 1, kSolveCramerGlu = 2, kSolveCramerIntel = 3 };
+
 struct LevelArgs {
     const uint32_t *items;   // cell*A + angle, level-sorted
     const void *abar;        // Real4 per item: face area * omega.n, faces 0..3
@@ -21,6 +27,7 @@ struct LevelArgs {
     uint32_t gmagic;         // ceil(2^32 / G): pair -> item in the warp-tile variant (0 when G == 1)
     uint32_t vg;             // record variant: groups per vector access (divides G)
     uint32_t vmagic;         // ceil(2^32 / (G / vg)): task -> item (0 when G == vg)
+    uint32_t solver;         // 4x4 solver (deck key GaussElim), numbered as tycho_gauss_elim
 };
 
 // Record variant's group vector width: 16-byte accesses where G allows.

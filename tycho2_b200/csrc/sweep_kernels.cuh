@@ -38,7 +38,8 @@ template <> struct Vec4Of<float> { using type = float4; };
 
 constexpr uint32_t kSentinel = 0xFFFFFFFFu;  // padding item of a level
 
-// The group-independent part of one item's update.
+// The group-independent part of one item's update.  NoPivot keeps its
+// factors in the named fields; the other solvers in f16 (+ perm).
 template <typename Real>
 struct ItemFactor {
     uint32_t c, a;
@@ -46,6 +47,8 @@ struct ItemFactor {
     uint32_t nmap;
     Real ab[4], t1[4], t2[4], vs20;
     Real r0, u01, u02, u03, l1, l2, l3, r1, u12, u13, a21, a31, r2, u23, b32, c33;
+    Real f16[16];
+    uint32_t perm;  // Original: b row i comes from row (perm >> 2i) & 3
 };
 
 // FP64 keeps the reference's IEEE divisions (bit-identical results); FP32,
@@ -65,7 +68,8 @@ __device__ __forceinline__ Real over12(Real x)
 }
 
 template <typename Real>
-__device__ __forceinline__ void item_lu(ItemFactor<Real> &F, Real d1, Real d2, const bool (&out)[4]);
+__device__ __forceinline__ void item_lu(ItemFactor<Real> &F, Real d1, Real d2, const bool (&out)[4],
+                                        uint32_t kind = kSolveNoPivot);
 
 template <typename Real>
 __device__ __forceinline__ void item_setup(const LevelArgs &p, uint64_t it, uint32_t ca, ItemFactor<Real> &F)
@@ -90,14 +94,163 @@ __device__ __forceinline__ void item_setup(const LevelArgs &p, uint64_t it, uint
         F.t2[f] = over12(Real(2) * F.ab[f]);
         out[f] = F.ab[f] > Real(0);
     }
-    item_lu(F, d1, d2, out);
+    item_lu(F, d1, d2, out, p.solver);
+}
+
+template <typename Real>
+__device__ __forceinline__ Real abs_real(Real x)
+{
+    return x < Real(0) ? -x : x;
+}
+
+// gaussElim4 Original (src/Transport.cc:284-337): column by column, the row
+// of largest |entry| becomes the pivot row, the pivot is replaced by its
+// reciprocal, the column below is scaled by it, and the next column is
+// updated Crout-style.  Leaves the factored matrix in A (row major) and the
+// row order of b in perm.
+template <typename Real>
+__device__ __forceinline__ void factor_original(Real (&A)[4][4], uint32_t &perm)
+{
+    uint32_t idx = 0u | (1u << 2) | (2u << 4) | (3u << 6);
+    for (int column = 0; column < 3; ++column) {
+        int rowmax = column;
+        Real colmax = abs_real(A[column][column]);
+        for (int row = column + 1; row < 4; ++row) {
+            const Real t = abs_real(A[row][column]);
+            if (t > colmax) {
+                rowmax = row;
+                colmax = t;
+            }
+        }
+        if (rowmax != column) {
+            for (int c2 = 0; c2 < 4; ++c2) {
+                const Real t = A[rowmax][c2];
+                A[rowmax][c2] = A[column][c2];
+                A[column][c2] = t;
+            }
+            const uint32_t ir = (idx >> (2 * rowmax)) & 3u, ic = (idx >> (2 * column)) & 3u;
+            idx &= ~((3u << (2 * rowmax)) | (3u << (2 * column)));
+            idx |= (ic << (2 * rowmax)) | (ir << (2 * column));
+        }
+        A[column][column] = div_ref(Real(1), A[column][column]);
+        for (int row = column + 1; row < 4; ++row) A[row][column] *= A[column][column];
+        for (int c2 = 0; c2 <= column; ++c2)
+            for (int row = c2 + 1; row < 4; ++row) A[row][column + 1] -= A[row][c2] * A[c2][column + 1];
+    }
+    A[3][3] = div_ref(Real(1), A[3][3]);
+    perm = idx;
+}
+
+// gaussElim4 CramerGlu (src/Transport.cc:414-557): inv[4a + b] is the
+// (b, a) cofactor, (-1)^(a+b) times the minor without row b and column a,
+// expanded along its first column over its rows in increasing order, each
+// row's 2x2 minor as m[r][c0] m[r'][c1] m[r''][c2] - m[r][c0] m[r'][c2]
+// m[r''][c1]; products and the six terms left to right (the reference's
+// expressions); then det = row 0 . column 0 of inv, inv *= 1/det.
+template <typename Real>
+__device__ __forceinline__ void factor_cramer_glu(const Real (&A)[4][4], Real (&inv)[16])
+{
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) {
+            int rows[3], cols[3];
+            int nr = 0, ncl = 0;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (r != bb) rows[nr++] = r;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (c != a) cols[ncl++] = c;
+            const bool neg = ((a + bb) & 1) != 0;
+            Real acc = Real(0);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int r = rows[k], r1 = rows[k == 0 ? 1 : 0], r2 = rows[k == 2 ? 1 : 2];
+                const bool plus = neg == ((k & 1) != 0);
+                const Real t1 = A[r][cols[0]] * A[r1][cols[1]] * A[r2][cols[2]];
+                const Real t2 = A[r][cols[0]] * A[r1][cols[2]] * A[r2][cols[1]];
+                if (k == 0) acc = plus ? t1 : -t1;
+                else acc = plus ? acc + t1 : acc - t1;
+                acc = plus ? acc - t2 : acc + t2;
+            }
+            inv[4 * a + bb] = acc;
+        }
+    Real det = A[0][0] * inv[0] + A[0][1] * inv[4] + A[0][2] * inv[8] + A[0][3] * inv[12];
+    det = div_ref(Real(1), det);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) inv[i] = inv[i] * det;
+}
+
+// gaussElim4 CramerIntel (src/Transport.cc:559-677): the scalar form of
+// Intel's SSE 4x4 inverse (application note "Streaming SIMD Extensions -
+// Inverse of 4x4 Matrix").  src = A column major; for each half, products of
+// pairs of two src rows (tmp), then every cofactor as the sum of three
+// (tmp x src) products minus the sum of three more, in the (tmp, src) order
+// of the tables; det = src row 0 . dst, dst *= 1/det.
+__constant__ const unsigned char kIntelCof[16][6][2] = {
+    {{0, 5}, {3, 6}, {4, 7}, {1, 5}, {2, 6}, {5, 7}},       {{1, 4}, {6, 6}, {9, 7}, {0, 4}, {7, 6}, {8, 7}},
+    {{2, 4}, {7, 5}, {10, 7}, {3, 4}, {6, 5}, {11, 7}},     {{5, 4}, {8, 5}, {11, 6}, {4, 4}, {9, 5}, {10, 6}},
+    {{1, 1}, {2, 2}, {5, 3}, {0, 1}, {3, 2}, {4, 3}},       {{0, 0}, {7, 2}, {8, 3}, {1, 0}, {6, 2}, {9, 3}},
+    {{3, 0}, {6, 1}, {11, 3}, {2, 0}, {7, 1}, {10, 3}},     {{4, 0}, {9, 1}, {10, 2}, {5, 0}, {8, 1}, {11, 2}},
+    {{0, 13}, {3, 14}, {4, 15}, {1, 13}, {2, 14}, {5, 15}}, {{1, 12}, {6, 14}, {9, 15}, {0, 12}, {7, 14}, {8, 15}},
+    {{2, 12}, {7, 13}, {10, 15}, {3, 12}, {6, 13}, {11, 15}}, {{5, 12}, {8, 13}, {11, 14}, {4, 12}, {9, 13}, {10, 14}},
+    {{2, 10}, {5, 11}, {1, 9}, {4, 11}, {0, 9}, {3, 10}},   {{8, 11}, {0, 8}, {7, 10}, {6, 10}, {9, 11}, {1, 8}},
+    {{6, 9}, {11, 11}, {3, 8}, {10, 11}, {2, 8}, {7, 9}},   {{10, 10}, {4, 8}, {9, 9}, {8, 9}, {11, 10}, {5, 8}}};
+
+template <typename Real>
+__device__ __forceinline__ void factor_cramer_intel(const Real (&A)[4][4], Real (&dst)[16])
+{
+    constexpr int pairs[6][2] = {{2, 3}, {1, 3}, {1, 2}, {0, 3}, {0, 2}, {0, 1}};
+    Real src[16], tmp[12];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) src[i + 4 * j] = A[i][j];
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        const int lo = half ? 0 : 8, hi = half ? 4 : 12;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            tmp[2 * k] = src[lo + pairs[k][0]] * src[hi + pairs[k][1]];
+            tmp[2 * k + 1] = src[lo + pairs[k][1]] * src[hi + pairs[k][0]];
+        }
+#pragma unroll
+        for (int j = 8 * half; j < 8 * half + 8; ++j) {
+            const Real plus = tmp[kIntelCof[j][0][0]] * src[kIntelCof[j][0][1]] +
+                              tmp[kIntelCof[j][1][0]] * src[kIntelCof[j][1][1]] +
+                              tmp[kIntelCof[j][2][0]] * src[kIntelCof[j][2][1]];
+            const Real minus = tmp[kIntelCof[j][3][0]] * src[kIntelCof[j][3][1]] +
+                               tmp[kIntelCof[j][4][0]] * src[kIntelCof[j][4][1]] +
+                               tmp[kIntelCof[j][5][0]] * src[kIntelCof[j][5][1]];
+            dst[j] = plus - minus;
+        }
+    }
+    Real det = src[0] * dst[0] + src[1] * dst[1] + src[2] * dst[2] + src[3] * dst[3];
+    det = div_ref(Real(1), det);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) dst[j] *= det;
+}
+
+// The 16 per-item numbers of a solver as stored in a record (f[5..20]).
+template <typename Real>
+__device__ __forceinline__ void factor16(const ItemFactor<Real> &F, uint32_t kind, Real (&out)[16])
+{
+    if (kind == kSolveNoPivot) {
+        out[0] = F.r0; out[1] = F.u01; out[2] = F.u02; out[3] = F.u03; out[4] = F.l1; out[5] = F.l2;
+        out[6] = F.l3; out[7] = F.r1; out[8] = F.u12; out[9] = F.u13; out[10] = F.a21; out[11] = F.a31;
+        out[12] = F.r2; out[13] = F.u23; out[14] = F.b32; out[15] = F.c33;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) out[i] = F.f16[i];
+    }
 }
 
 // The matrix of one (cell, angle) item from its face terms t1, t2 and the
 // volume terms d1 = sigma_t V/20, d2 = 2 sigma_t V/20 (out[f]: face f is
 // outgoing), and its LU factors.
 template <typename Real>
-__device__ __forceinline__ void item_lu(ItemFactor<Real> &F, Real d1, Real d2, const bool (&out)[4])
+__device__ __forceinline__ void item_lu(ItemFactor<Real> &F, Real d1, Real d2, const bool (&out)[4], uint32_t kind)
 {
     // Streaming + collision (volume integrals), then outgoing-face terms in
     // increasing face order.
@@ -115,6 +268,23 @@ __device__ __forceinline__ void item_lu(ItemFactor<Real> &F, Real d1, Real d2, c
                 for (int j = 0; j < 4; ++j)
                     if (i != f && j != f) M[i][j] += (i == j ? F.t2[f] : F.t1[f]);
         }
+    }
+    F.perm = 0u | (1u << 2) | (2u << 4) | (3u << 6);
+    if (kind == kSolveOriginal) {
+        factor_original(M, F.perm);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) F.f16[4 * i + j] = M[i][j];
+        return;
+    }
+    if (kind == kSolveCramerGlu) {
+        factor_cramer_glu(M, F.f16);
+        return;
+    }
+    if (kind == kSolveCramerIntel) {
+        factor_cramer_intel(M, F.f16);
+        return;
     }
     // LU without pivoting: the elimination steps of gaussElim4 NoPivot that
     // touch only the matrix.

@@ -11,7 +11,10 @@
 //                                with rounding; t1 < 0 marks an upwind face)
 //   f[4..20]  vs20 r0 u01 u02 u03 l1 l2 l3 r1 u12 u13 a21 a31 r2 u23 b32 c33
 //   u[0..6]   c, c*A + a, nmap, row[f] = nb*A + a of the neighbour across face
-//             f (kNoRow on the boundary)
+//             f (kNoRow on the boundary); the word after u[6] holds the
+//             row order of the Original solver
+// f[5..20] are the 16 numbers of the 4x4 solver (GaussElim): the NoPivot
+// factors below, Original's factored matrix, or the Cramer inverses.
 // A padding item has c == kSentinel.
 //
 // A warp takes IPW consecutive items; lane i < IPW copies record i into a
@@ -50,6 +53,7 @@ __global__ void item_record_kernel(const LevelArgs p, uint64_t n, ItemRecord<Rea
     if (it >= n) return;
     const uint32_t ca = p.items[it];
     ItemRecord<Real> r;
+    for (unsigned i = 0; i < sizeof(r.pad) / 4; ++i) r.pad[i] = 0;
     if (ca == kSentinel) {
         for (int i = 0; i < 21; ++i) r.f[i] = Real(0);
         r.u[0] = kSentinel; r.u[1] = 0; r.u[2] = 0;
@@ -58,14 +62,14 @@ __global__ void item_record_kernel(const LevelArgs p, uint64_t n, ItemRecord<Rea
         ItemFactor<Real> F;
         item_setup(p, it, ca, F);
         for (int f = 0; f < 4; ++f) r.f[f] = F.t1[f];
-        r.f[4] = F.vs20; r.f[5] = F.r0; r.f[6] = F.u01; r.f[7] = F.u02; r.f[8] = F.u03;
-        r.f[9] = F.l1; r.f[10] = F.l2; r.f[11] = F.l3; r.f[12] = F.r1; r.f[13] = F.u12;
-        r.f[14] = F.u13; r.f[15] = F.a21; r.f[16] = F.a31; r.f[17] = F.r2; r.f[18] = F.u23;
-        r.f[19] = F.b32; r.f[20] = F.c33;
+        r.f[4] = F.vs20;
+        Real f16[16];
+        factor16(F, p.solver, f16);
+        for (int i = 0; i < 16; ++i) r.f[5 + i] = f16[i];
         r.u[0] = F.c; r.u[1] = ca; r.u[2] = F.nmap;
         for (int f = 0; f < 4; ++f) r.u[3 + f] = F.adj[f] < 0 ? kNoRow : (uint32_t)F.adj[f] * p.A + F.a;
+        r.pad[0] = F.perm;  // the Original solver's row order, right after u[]
     }
-    for (unsigned i = 0; i < sizeof(r.pad) / 4; ++i) r.pad[i] = 0;
     out[it] = r;
 }
 
@@ -114,7 +118,7 @@ __global__ void compact_record_kernel(const LevelArgs p, uint64_t n, CompactReco
 template <typename Real, int IPW>
 struct RecordTile {
     Real f[21][IPW];
-    uint32_t u[7][IPW];
+    uint32_t u[8][IPW];  // u[7]: the Original solver's row order
 };
 
 template <typename Real, int IPW>
@@ -123,7 +127,7 @@ __device__ __forceinline__ void tile_fill(RecordTile<Real, IPW> &T, const ItemRe
 {
     if (lane >= (uint32_t)IPW) return;
     if (!valid) { T.u[0][lane] = kSentinel; return; }
-    constexpr int N = (21 * sizeof(Real) + 28 + 15) / 16;  // 16-byte chunks holding f[] and u[]
+    constexpr int N = (21 * sizeof(Real) + 32 + 15) / 16;  // 16-byte chunks holding f[], u[] and the row order
     uint4 v[N];
     const uint4 *s = reinterpret_cast<const uint4 *>(src);
 #pragma unroll
@@ -133,7 +137,7 @@ __device__ __forceinline__ void tile_fill(RecordTile<Real, IPW> &T, const ItemRe
 #pragma unroll
     for (int k = 0; k < 21; ++k) T.f[k][lane] = fr[k];
 #pragma unroll
-    for (int k = 0; k < 7; ++k) T.u[k][lane] = ur[k];
+    for (int k = 0; k < 8; ++k) T.u[k][lane] = ur[k];
 }
 
 // VG consecutive groups of one psi/phi row move as one vector access (the
@@ -183,31 +187,39 @@ struct TileView {
 template <typename Real>
 struct RegRecord {
     Real fv[21];
-    uint32_t uv[7];
+    uint32_t uv[8];  // uv[7]: the Original solver's row order
     __device__ __forceinline__ Real f(int k) const { return fv[k]; }
     __device__ __forceinline__ uint32_t u(int k) const { return uv[k]; }
 };
 
 // One record from global memory straight into registers (read-only path).
+// kind: the solver the caller applies; only Original needs the row-order
+// word after u[] (NoPivot callers pass the constant and skip its load).
 template <typename Real>
-__device__ __forceinline__ void load_record(const ItemRecord<Real> *__restrict__ src, RegRecord<Real> &r)
+__device__ __forceinline__ void load_record(const ItemRecord<Real> *__restrict__ src, RegRecord<Real> &r,
+                                            uint32_t kind = kSolveNoPivot)
 {
-    constexpr int N = (21 * sizeof(Real) + 28 + 15) / 16;
-    uint4 v[N];
+    constexpr int N = (21 * sizeof(Real) + 28 + 15) / 16;  // f[] and u[]
+    uint4 v[N + 1];
     const uint4 *s = reinterpret_cast<const uint4 *>(src);
 #pragma unroll
     for (int i = 0; i < N; ++i) v[i] = __ldg(s + i);
+    const bool order = kind == kSolveOriginal;
+    constexpr int tail = (21 * sizeof(Real) + 28) / 16;  // the chunk holding the row order
+    if (order && tail == N) v[N] = __ldg(s + N);
     const Real *fr = reinterpret_cast<const Real *>(v);
     const uint32_t *ur = reinterpret_cast<const uint32_t *>(reinterpret_cast<const char *>(v) + 21 * sizeof(Real));
 #pragma unroll
     for (int k = 0; k < 21; ++k) r.fv[k] = fr[k];
 #pragma unroll
     for (int k = 0; k < 7; ++k) r.uv[k] = ur[k];
+    r.uv[7] = order ? ur[7] : 0u;
 }
 
 // A compact record into registers, with the factors rebuilt.
 template <typename Real>
-__device__ __forceinline__ void load_record(const CompactRecord<Real> *__restrict__ src, RegRecord<Real> &r)
+__device__ __forceinline__ void load_record(const CompactRecord<Real> *__restrict__ src, RegRecord<Real> &r,
+                                            uint32_t kind = kSolveNoPivot)
 {
     constexpr int N = sizeof(CompactRecord<Real>) / 16;
     uint4 v[N];
@@ -218,6 +230,7 @@ __device__ __forceinline__ void load_record(const CompactRecord<Real> *__restric
     const uint32_t *ur = reinterpret_cast<const uint32_t *>(reinterpret_cast<const char *>(v) + 7 * sizeof(Real));
 #pragma unroll
     for (int k = 0; k < 7; ++k) r.uv[k] = ur[k];
+    r.uv[7] = 0;
     if (r.uv[0] == kSentinel) return;
     ItemFactor<Real> F;
     bool out[4];
@@ -227,13 +240,15 @@ __device__ __forceinline__ void load_record(const CompactRecord<Real> *__restric
         F.t2[f] = Real(2) * fr[f];
         out[f] = fr[f] > Real(0);
     }
-    item_lu(F, fr[5], fr[6], out);
+    item_lu(F, fr[5], fr[6], out, kind);
 #pragma unroll
     for (int f = 0; f < 4; ++f) r.fv[f] = F.t1[f];
-    r.fv[4] = fr[4]; r.fv[5] = F.r0; r.fv[6] = F.u01; r.fv[7] = F.u02; r.fv[8] = F.u03;
-    r.fv[9] = F.l1; r.fv[10] = F.l2; r.fv[11] = F.l3; r.fv[12] = F.r1; r.fv[13] = F.u12;
-    r.fv[14] = F.u13; r.fv[15] = F.a21; r.fv[16] = F.a31; r.fv[17] = F.r2; r.fv[18] = F.u23;
-    r.fv[19] = F.b32; r.fv[20] = F.c33;
+    r.fv[4] = fr[4];
+    Real f16[16];
+    factor16(F, kind, f16);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) r.fv[5 + i] = f16[i];
+    r.uv[7] = F.perm;
 }
 
 // All the inputs of one (item, VG groups) task, loaded before any arithmetic.
@@ -311,9 +326,60 @@ __device__ __forceinline__ void pair_load(const LevelArgs &p, const RecordTile<R
     pair_load_upwind<Real, VG, L2_ONLY>(p, R, g, in);
 }
 
+// The right-hand-side steps of the record's 4x4 solver on one group, in the
+// reference's order: NoPivot's elimination and back substitution, Original's
+// row order then forward and backward substitution with the factored matrix
+// (its diagonal holds reciprocals), Cramer's x = inv b summed left to right.
+template <typename Real, bool ANY, typename View>
+__device__ __forceinline__ void solve_apply(uint32_t kind, const View &R, Real (&b)[4])
+{
+    if (!ANY || kind == kSolveNoPivot) {
+        b[0] = b[0] * R.f(5);
+        b[1] = b[1] - b[0] * R.f(9);
+        b[2] = b[2] - b[0] * R.f(10);
+        b[3] = b[3] - b[0] * R.f(11);
+        b[1] = b[1] * R.f(12);
+        b[2] = b[2] - b[1] * R.f(15);
+        b[3] = b[3] - b[1] * R.f(16);
+        b[2] = b[2] * R.f(17);
+        b[3] = b[3] - b[2] * R.f(19);
+        b[3] = div_ref(b[3], R.f(20));
+        b[2] = b[2] - R.f(18) * b[3];
+        b[1] = b[1] - R.f(14) * b[3] - R.f(13) * b[2];
+        b[0] = b[0] - R.f(8) * b[3] - R.f(7) * b[2] - R.f(6) * b[1];
+    } else if (kind == kSolveOriginal) {
+        const uint32_t perm = R.u(7);
+        Real x[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t src = (perm >> (2 * i)) & 3u;
+            x[i] = src == 0 ? b[0] : src == 1 ? b[1] : src == 2 ? b[2] : b[3];
+        }
+#pragma unroll
+        for (int column = 0; column < 3; ++column)
+#pragma unroll
+            for (int row = column + 1; row < 4; ++row) x[row] -= R.f(5 + 4 * row + column) * x[column];
+#pragma unroll
+        for (int column = 3; column >= 0; --column) {
+            x[column] *= R.f(5 + 5 * column);
+#pragma unroll
+            for (int row = column - 1; row >= 0; --row) x[row] -= R.f(5 + 4 * row + column) * x[column];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) b[i] = x[i];
+    } else {
+        Real x[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            x[r] = R.f(5 + 4 * r) * b[0] + R.f(6 + 4 * r) * b[1] + R.f(7 + 4 * r) * b[2] + R.f(8 + 4 * r) * b[3];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) b[i] = x[i];
+    }
+}
+
 // The per-group arithmetic of one task, group by group in the reference's
 // operation order (the factors are read once per task).
-template <typename Real, int VG, typename View>
+template <typename Real, int VG, typename View, bool ANY = false>
 __device__ __forceinline__ void pair_solve_store_v(const LevelArgs &p, const View &R, uint32_t g,
                                                    const PairIn<Real, VG> &in)
 {
@@ -346,19 +412,7 @@ __device__ __forceinline__ void pair_solve_store_v(const LevelArgs &p, const Vie
                 }
             }
         }
-        b[0] = b[0] * R.f(5);
-        b[1] = b[1] - b[0] * R.f(9);
-        b[2] = b[2] - b[0] * R.f(10);
-        b[3] = b[3] - b[0] * R.f(11);
-        b[1] = b[1] * R.f(12);
-        b[2] = b[2] - b[1] * R.f(15);
-        b[3] = b[3] - b[1] * R.f(16);
-        b[2] = b[2] * R.f(17);
-        b[3] = b[3] - b[2] * R.f(19);
-        b[3] = div_ref(b[3], R.f(20));
-        b[2] = b[2] - R.f(18) * b[3];
-        b[1] = b[1] - R.f(14) * b[3] - R.f(13) * b[2];
-        b[0] = b[0] - R.f(8) * b[3] - R.f(7) * b[2] - R.f(6) * b[1];
+        solve_apply<Real, ANY>(p.solver, R, b);
 #pragma unroll
         for (int v = 0; v < 4; ++v) res[v][e] = b[v];
     }
@@ -431,13 +485,14 @@ __device__ __forceinline__ void pair_solve_store_f32x2(const LevelArgs &p, const
     for (int v = 0; v < 4; ++v) gv_store(out + v * p.G, res[v]);
 }
 
-// The arithmetic of one task: packed FP32x2 where it applies.
-template <typename Real, int VG, typename View>
+// The arithmetic of one task: packed FP32x2 where it applies.  ANY: the
+// record may hold any of the four solvers (p.solver); otherwise NoPivot.
+template <typename Real, int VG, typename View, bool ANY = false>
 __device__ __forceinline__ void pair_solve_store_any(const LevelArgs &p, const View &R, uint32_t g,
                                                      const PairIn<Real, VG> &in)
 {
-    if constexpr (std::is_same<Real, float>::value && VG % 2 == 0) pair_solve_store_f32x2<VG>(p, R, g, in);
-    else pair_solve_store_v<Real, VG>(p, R, g, in);
+    if constexpr (std::is_same<Real, float>::value && VG % 2 == 0 && !ANY) pair_solve_store_f32x2<VG>(p, R, g, in);
+    else pair_solve_store_v<Real, VG, View, ANY>(p, R, g, in);
 }
 
 template <typename Real, int IPW, int VG>
@@ -515,7 +570,7 @@ sweep_record_level_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict_
 // are read after it.  No shared memory.  Tasks of a level: item t / (G/VG),
 // groups VG * (t % (G/VG)) and on (the host keeps a level's task count
 // below 2^26 so that the multiply-high division is exact).
-template <typename Real, int VG, int BS, typename Rec, int MINB = 1>
+template <typename Real, int VG, int BS, typename Rec, int MINB = 1, bool ANY = false>
 __global__ void __launch_bounds__(BS, MINB)
 sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const uint64_t begin, const uint64_t end)
 {
@@ -529,14 +584,14 @@ sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const 
     RegRecord<Real> R;
     PairIn<Real, VG> in;
     if (live) {
-        load_record(rec + it, R);
+        load_record(rec + it, R, ANY ? p.solver : (uint32_t)kSolveNoPivot);
         live = R.u(0) != kSentinel;
     }
     if (live) pair_load_source<Real, VG>(p, R, g, in);
     pdl_wait_prerequisites();
     if (!live) return;
     pair_load_upwind<Real, VG, false>(p, R, g, in);
-    pair_solve_store_any<Real, VG>(p, R, g, in);
+    pair_solve_store_any<Real, VG, RegRecord<Real>, ANY>(p, R, g, in);
 }
 
 // Direct variant, two group vectors per task: the task covers 2*VG groups
@@ -858,8 +913,23 @@ static const void *direct_fn_vg(int vg)
 }
 
 template <typename Real, typename Rec>
-static const void *direct_fn(int knob, int vg)
+static const void *direct_any_fn(int vg)
 {
+    switch (vg) {
+    case 1: return (const void *)sweep_direct_level_kernel<Real, 1, 128, Rec, 1, true>;
+    case 2: return (const void *)sweep_direct_level_kernel<Real, 2, 128, Rec, 1, true>;
+    case 4:
+        if constexpr (sizeof(Real) == 4) return (const void *)sweep_direct_level_kernel<Real, 4, 128, Rec, 1, true>;
+        else return nullptr;
+    default: return nullptr;
+    }
+}
+
+template <typename Real, typename Rec>
+static const void *direct_fn(int knob, int vg, uint32_t solver)
+{
+    // Original and the Cramer solvers: one 128-thread kernel per vector width
+    if (solver != kSolveNoPivot) return knob == 128 ? direct_any_fn<Real, Rec>(vg) : nullptr;
     switch (knob) {
     case 64: return direct_fn_vg<Real, 64, Rec, 1>(vg);
     case 128: return direct_fn_vg<Real, 128, Rec, 1>(vg);
@@ -881,8 +951,8 @@ cudaError_t launch_direct_level(int knob, const LevelArgs &p, const void *rec, u
     if (end <= begin) return cudaSuccess;
     const uint64_t tasks = (end - begin) * (p.G / p.vg);
     if (tasks >= (1ull << 26)) return cudaErrorInvalidValue;
-    const void *fn = compact ? direct_fn<Real, CompactRecord<Real>>(knob, (int)p.vg)
-                             : direct_fn<Real, ItemRecord<Real>>(knob, (int)p.vg);
+    const void *fn = compact ? direct_fn<Real, CompactRecord<Real>>(knob, (int)p.vg, p.solver)
+                             : direct_fn<Real, ItemRecord<Real>>(knob, (int)p.vg, p.solver);
     if (!fn) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)((tasks + bs - 1) / bs));

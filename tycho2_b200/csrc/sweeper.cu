@@ -72,6 +72,8 @@ Sweeper::~Sweeper()
 int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err)
 {
     if (o.n_groups < 1 || o.n_groups > 64) { err = "nGroups must be in 1..64"; return kErrArg; }
+    if (o.gauss_elim < 0 || o.gauss_elim > 3) { err = "GaussElim must be 0..3"; return kErrArg; }
+    solver_ = o.gauss_elim;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         err = "no CUDA device: the B200 sweep has no CPU fallback";
@@ -159,11 +161,17 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     // level (64-thread blocks); schedule 2 asks for the persistent dataflow
     // kernel (warp tiles); explicit threads-per-item selects the
     // item-parallel variant.  The autotuner can replace any of them.
+    // Original and the Cramer solvers run in the direct kernels (128 threads)
+    const bool nopivot = solver_ == kSolveNoPivot;
     for (int prec = 0; prec < (fp32_ ? 2 : 1); ++prec) {
         const int tpi = prec ? o.tpi32 : o.tpi64;
+        if (!nopivot && (tpi || o.schedule == 2)) {
+            err = "GaussElim Original / CramerGlu / CramerIntel run on the level schedule with compact records";
+            return kErrArg;
+        }
         if (tpi) TY_CHECK(configure(prec, o.schedule == 1 ? 1 : 2, 0, tpi, err));
         else if (o.schedule == 2) TY_CHECK(configure(prec, 2, 1, 4, err));
-        else TY_CHECK(configure(prec, 1, 4, 64, err));
+        else TY_CHECK(configure(prec, 1, 4, nopivot ? 64 : 128, err));
     }
     TY_CUDA(cudaStreamSynchronize(stream_));
     return kOk;
@@ -181,6 +189,11 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
     // one access moves up to 16 bytes (4 FP32 / 2 FP64 groups); the direct
     // variants on levels also take two such vectors per task (8 / 4)
     const bool halves = (prec == 1 && vg == 8) || (prec == 0 && vg == 4);
+    if (solver_ != kSolveNoPivot && (variant < 3 || schedule != 1 || knob != 128 || halves)) {
+        err = "GaussElim Original / CramerGlu / CramerIntel: direct record variants on the level schedule, "
+              "128 threads per block, one group vector per task";
+        return kErrArg;
+    }
     if (vg != 1 && vg != 2 && !(vg == 4 && prec == 1) && !halves) {
         err = "group vector width must be 1, 2 (FP64: or 4) or 1, 2, 4 (FP32: or 8)";
         return kErrArg;
@@ -303,6 +316,7 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
         for (int variant = 0; variant <= 4; ++variant)
             for (int knob : {1, 2, 4, 8, 16, 32, 64, 128, 256, -64, -128}) {
                 if (knob < 0 && (variant < 3 || sched != 1)) continue;
+                if (solver_ != kSolveNoPivot && (variant < 3 || sched != 1 || knob != 128)) continue;
                 if (variant == 0 && ((knob > 2 * G_ && knob > 1) || knob > 16)) continue;  // idle lanes
                 if (variant == 1 && knob > 4) continue;
                 if (variant == 2 && (knob < 8 || knob > 32)) continue;
@@ -313,7 +327,7 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
                     if (vg > 1 && (variant < 2 || G_ % vg != 0)) continue;
                     const bool halves = (prec == 1 && vg == 8) || (prec == 0 && vg == 4);
                     if (prec == 0 && vg == 8) continue;
-                    if (halves && (variant < 3 || sched != 1 || knob < 0)) continue;
+                    if (halves && (variant < 3 || sched != 1 || knob < 0 || solver_ != kSolveNoPivot)) continue;
                     if (variant >= 3 && sched == 2) {
                         const int gpv = G_ / vg;
                         if (gpv > 32 || (gpv & (gpv - 1)) != 0) continue;
@@ -378,6 +392,7 @@ LevelArgs Sweeper::level_args(int prec, const void *iso, const double *qang, voi
     p.gmagic = group_magic((uint32_t)G_);
     p.vg = (uint32_t)shape_[prec ? 1 : 0].vg;
     p.vmagic = group_magic((uint32_t)G_ / p.vg);
+    p.solver = (uint32_t)solver_;
     return p;
 }
 

@@ -24,6 +24,7 @@ struct SweeperOptions {
     int tpi64 = 0;  // 0 = auto
     int tpi32 = 0;
     int schedule = 0;  // 0 auto (levels, compact records), 1 level-synchronous, 2 dataflow
+    int gauss_elim = 1;  // 4x4 solver, numbered as tycho_gauss_elim (deck key GaussElim)
 };
 
 // Launch shape of one precision's sweep.
@@ -106,6 +107,7 @@ public:
     // The resident psi was written by a sweep of this precision elsewhere.
     void note_psi_precision(int prec) { last_psi_prec_ = prec; }
     uint64_t n_items() const { return sched_.items.size(); }
+    int solver() const { return solver_; }
 
     const MeshTables &tables() const { return tables_; }
     const Quadrature &quadrature() const { return quad_; }
@@ -139,6 +141,7 @@ private:
     uint64_t nc_ = 0;
     int A_ = 0, G_ = 0, device_ = 0;
     bool fp32_ = false, have_xs_ = false;
+    int solver_ = 1;  // SolveKind
     int last_psi_prec_ = -1;
 
     cudaStream_t stream_ = nullptr;

@@ -16,7 +16,7 @@ from ._capi import check, lib, ptr
 
 NONE = np.uint64(0xFFFFFFFFFFFFFFFF)  # TychoMesh::BOUNDARY_FACE
 
-GAUSS_ELIM = {"Original": 0, "NoPivot": 1}
+GAUSS_ELIM = {"Original": 0, "NoPivot": 1, "CramerGlu": 2, "CramerIntel": 3}
 METHODS = {"si": 0, "gmres": 1, "mixed": 2}
 
 
