@@ -223,16 +223,21 @@ def launches_per_sweep(shape, n_levels):
     return sweep + 2
 
 
-def profiled_traffic(workload, kernel):
+def traffic_family(shape, fp32):
+    """What a sweep's DRAM traffic depends on: variant, precision, group vector."""
+    return "%s %s vg%d" % (shape["variant"], "float" if fp32 else "double", shape["vector"])
+
+
+def profiled_traffic(workload, family):
     """DRAM bytes of one sweep (dram__bytes_read.sum + dram__bytes_write.sum over
     the sweep's launches) from the ncu summary table in profiles/, if that
-    kernel was captured on this workload; else None."""
+    kernel family was captured on this workload; else None."""
     path = os.path.join(ROOT, "profiles", "sweep_traffic.md")
     try:
         with open(path) as f:
             for ln in f:
                 cells = [c.strip() for c in ln.strip().strip("|").split("|")]
-                if len(cells) >= 3 and cells[0] == workload and cells[1] == "`%s`" % kernel:
+                if len(cells) >= 3 and cells[0] == workload and cells[1] == "`%s`" % family:
                     return float(cells[2])
     except (OSError, ValueError):
         pass
@@ -504,8 +509,8 @@ def run_b200(args):
             cpu = {"value": None, "error": str(e)[:200]}
 
     if rank == 0:
-        t32 = profiled_traffic(args.workload, k32)
-        t64 = profiled_traffic(args.workload, k64)
+        t32 = profiled_traffic(args.workload, traffic_family(shape32, True))
+        t64 = profiled_traffic(args.workload, traffic_family(shape64, False))
         line = {
             "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": warm, "ms_per_step": ms32,
