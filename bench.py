@@ -48,7 +48,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=30)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="kuhn32_s8_g8")
@@ -83,9 +83,10 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
+            time.sleep(0.5)  # sampling is running before the timed region starts
         except OSError:
             self.proc = None
         return self
@@ -215,12 +216,6 @@ SCHED = {"levels": 1, "dataflow": 2, "persist": 3}
 def kernel_name(shape, fp32):
     return KERNELS[(SCHED[shape["schedule"]], shape["variant"])].format(
         r="float" if fp32 else "double", k=shape["knob"], vg=shape["vector"])
-
-
-def launches_per_sweep(shape, n_levels):
-    """Kernels of one operator application: scatter-source, the sweep, psi->phi."""
-    sweep = {"levels": n_levels, "dataflow": 2, "persist": 1}[shape["schedule"]]
-    return sweep + 2
 
 
 def traffic_family(shape, fp32):
@@ -413,6 +408,7 @@ def run_b200(args):
             sw.configure(prec, s, v, int(k), vec if (prec == 1 or vec <= 2) else 0, streams)
         tuned = {1: sw.shape(1), 0: sw.shape(0)}
     shape32, shape64 = sw.shape(1), sw.shape(0)
+    launches = {1: sw.launches(1), 0: sw.launches(0)}
 
     # Untimed warm-up (graph capture of both precisions), then K timed steps
     # of each precision.  psi (6.4 GB FP64 / 3.2 GB FP32) is far larger than
@@ -537,8 +533,7 @@ def run_b200(args):
             "batch": batch,
             "serve": serve,
             "large": large,
-            "gpu_launches": args.steps * (launches_per_sweep(shape32, info["n_levels"])
-                                          + launches_per_sweep(shape64, info["n_levels"])),
+            "gpu_launches": args.steps * (launches[1] + launches[0]),
             "clocks": clocks,
             "wall_check_s": wall32,
         }

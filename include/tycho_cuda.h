@@ -200,6 +200,9 @@ int tycho_sweeper_write_psi(tycho_sweeper *sw, const char *path);
    number of incoming interior faces summed over items. */
 int tycho_sweeper_schedule_info(const tycho_sweeper *sw, uint32_t *n_levels, uint64_t *n_items,
                                 uint64_t *n_incoming_interior);
+/* Kernel launches of one operator application of the given precision with
+   its current launch shape (source, the sweep's launches, psi -> phi). */
+int tycho_sweeper_launches(const tycho_sweeper *sw, int precision, uint64_t *launches);
 /* Integer tables for parity, (angle, cell) order, any pointer may be NULL:
    t-levels of the wavefront schedule, the GraphTraverser constructor's
    dependency counts and Priorities' b-levels. */

@@ -82,6 +82,7 @@ SIGNATURES = {
     "tycho_sweeper_write_psi": (C.c_int, [_P, C.c_char_p]),
     "tycho_sweeper_schedule_info": (C.c_int, [_P, _U32P, _U64P, _U64P]),
     "tycho_sweeper_levels": (C.c_int, [_P, _P, _P, _P]),
+    "tycho_sweeper_launches": (C.c_int, [_P, C.c_int, _U64P]),
     "tycho_sweeper_time_sweeps": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P]),
     "tycho_sweeper_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(LaunchShape),
                                          C.POINTER(C.c_double)]),

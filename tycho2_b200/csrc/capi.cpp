@@ -351,6 +351,13 @@ int tycho_sweeper_schedule_info(const tycho_sweeper *h, uint32_t *n_levels, uint
     return TYCHO_OK;
 }
 
+int tycho_sweeper_launches(const tycho_sweeper *h, int precision, uint64_t *launches)
+{
+    if (!h || !launches || (precision != 0 && precision != 1)) return finish(TYCHO_ERR_ARG, "bad argument");
+    *launches = h->sw.launches_per_apply(precision);
+    return TYCHO_OK;
+}
+
 int tycho_sweeper_levels(const tycho_sweeper *h, uint32_t *tlevel, uint32_t *deps, uint32_t *blevel)
 {
     if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");

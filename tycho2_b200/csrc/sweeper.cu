@@ -872,6 +872,24 @@ int Sweeper::write_psi(const std::string &path, std::string &err)
     return kOk;
 }
 
+uint64_t Sweeper::launches_per_apply(int prec) const
+{
+    const LaunchShape &sh = shape_[prec ? 1 : 0];
+    uint64_t sweep = 0;
+    if (sh.schedule == 1) {
+        const int S = sh.streams;
+        for (uint32_t l = 0; l < sched_.n_levels; ++l)
+            for (int g = 0; g < S; ++g) {
+                const uint64_t b = sched_.octant_offset[(size_t)l * kOctants + g * kOctants / S];
+                const uint64_t e = sched_.octant_offset[(size_t)l * kOctants + (g + 1) * kOctants / S];
+                sweep += e > b;
+            }
+    } else {
+        sweep = sh.schedule == 2 ? 2 : 1;  // dataflow: epoch bump + the sweep
+    }
+    return sweep + 2;  // the scattering source before, psi -> phi after
+}
+
 int Sweeper::time_sweeps(int prec, int n, bool flush_l2, double *ms, std::string &err)
 {
     TY_CUDA(cudaSetDevice(device_));

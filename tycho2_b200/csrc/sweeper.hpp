@@ -75,6 +75,9 @@ public:
     int configure(int prec, int schedule, int variant, int knob, std::string &err, int vg = 0, int streams = 1);
     int autotune(int prec, int reps, LaunchShape *best, double *best_ms, std::string &err);
     const LaunchShape &shape(int prec) const { return shape_[prec ? 1 : 0]; }
+    // Kernel launches of one operator application with the current shape
+    // (source, the sweep's launches, psi -> phi).
+    uint64_t launches_per_apply(int prec) const;
 
     // One operator application, on the device:
     //   phi_out = D L^{-1} ( [Q] + M S phi_in )     (phi_in / phi_out nullable)

@@ -217,6 +217,12 @@ class SweeperCuda:
         check(lib().tycho_sweeper_schedule_info(self._h, C.byref(nl), C.byref(ni), C.byref(nin)))
         return {"n_levels": nl.value, "n_items": ni.value, "n_incoming_interior": nin.value}
 
+    def launches(self, precision):
+        """Kernel launches of one operator application with the current shape."""
+        n = C.c_uint64()
+        check(lib().tycho_sweeper_launches(self._h, precision, C.byref(n)))
+        return n.value
+
     def time_sweeps(self, precision, n, flush_l2=True):
         ms = np.zeros(2)
         check(lib().tycho_sweeper_time_sweeps(self._h, precision, n, int(flush_l2), ptr(ms)))
