@@ -77,7 +77,15 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.lines = []
+        self.lines = []  # (arrival time, line)
+        self.window = [None, None]
+
+    def start(self):
+        """The timed region begins: only samples from here on count."""
+        self.window[0] = time.monotonic()
+
+    def stop(self):
+        self.window[1] = time.monotonic()
 
     def __enter__(self):
         try:
@@ -93,7 +101,7 @@ class Clocks:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def __exit__(self, *a):
         if self.proc:
@@ -107,7 +115,11 @@ class Clocks:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0 = self.window[0] if self.window[0] is not None else -1e300
+        t1 = self.window[1] if self.window[1] is not None else 1e300
+        for t, ln in self.lines:
+            if not (t0 <= t <= t1 + 0.06):  # a sample arrives up to one period late
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -420,12 +432,14 @@ def run_b200(args):
     with Clocks(dev) as clk:
         grp.barrier()
         torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
+        clk.start()
         t0 = time.perf_counter()
         ms32, lvl32 = sw.time_sweeps(1, args.steps, True)
         grp.barrier()
         wall32 = time.perf_counter() - t0
         ms64, lvl64 = sw.time_sweeps(0, args.steps, True)
         grp.barrier()
+        clk.stop()
         torch.cuda.profiler.stop()
     clocks = clk.summary()
 
