@@ -349,9 +349,9 @@ def run_large_leg(grp, dev, workload="kuhn64_s8_g16"):
     """The 64^3 x 6 = 1,572,864-tet S8 G=16 problem (lognormal(0, 1) sigma_t,
     scattering ratio 0.99): FP32 and FP64 sweep rates, then the
     mixed-precision solve (FP32-sweep GMRES(30) in FP64 refinement) against
-    FP64 GMRES(30), both to 1e-10.  psi alone is 103 GB (FP64-sized), so the
-    FP64 sweep runs the record-free warp-tile kernel and the FP32 sweep the
-    compact records."""
+    FP64 GMRES(30), both to 1e-10.  psi alone is 103 GB (FP64-sized), so both
+    precisions sweep with compact records (the record-free warp-tile kernel
+    for FP64 if those do not fit)."""
     import tycho2_b200 as ty
     w, mesh, st, ss, mat, q = build_problem(workload)
     nc, A, G = mesh.n_cells, 2 * w["sn"] ** 2, w["groups"]
@@ -361,8 +361,11 @@ def run_large_leg(grp, dev, workload="kuhn64_s8_g16"):
     sw.set_source(q, "isotropic")
     setup = time.perf_counter() - t0
     info = sw.schedule_info()
-    sw.configure(1, "levels", "compact", 64)
-    sw.configure(0, "levels", "tiles", 4)
+    sw.configure(1, "levels", "compact", 64, 4, 2)
+    try:  # compact FP64 records (19 GB) fit beside psi (103 GB) and the GMRES(30) basis
+        sw.configure(0, "levels", "compact", 64, 2, 2)
+    except ty.TychoError:
+        sw.configure(0, "levels", "tiles", 4)
     sw.time_sweeps(1, 2)
     sw.time_sweeps(0, 2)
     grp.barrier()
@@ -372,6 +375,8 @@ def run_large_leg(grp, dev, workload="kuhn64_s8_g16"):
     upd = nc * A * G
     peak, peak_kind = hbm_peak()
     b32 = algorithmic_bytes(nc, A, G, info["n_incoming_interior"], 4)
+    b64 = algorithmic_bytes(nc, A, G, info["n_incoming_interior"], 8)
+    sw_shape32, sw_shape64 = sw.shape(1), sw.shape(0)
     tol, m = w.get("tol", 1e-10), w.get("restart", 30)
     phim, _, sm = sw.solve("mixed", iter_max=600, err_max=tol, restart=m, want_psi=False)
     phi64, _, s64 = sw.solve("gmres", iter_max=600, err_max=tol, restart=m, want_psi=False)
@@ -380,10 +385,11 @@ def run_large_leg(grp, dev, workload="kuhn64_s8_g16"):
     return {"workload": workload, "cells": nc, "angles": A, "groups": G, "levels": info["n_levels"],
             "setup_s": setup,
             "fp32": {"updates_per_s": grp.sum(upd) / (ms32 * 1e-3), "ms_per_sweep": ms32,
-                     "kernel": "sweep_direct_level_kernel<float,4,64,compact>", "kernel_ms": k32,
+                     "kernel": kernel_name(sw_shape32, True), "shape": sw_shape32, "kernel_ms": k32,
                      "roofline_frac": b32 / (k32 * 1e-3) / 1e9 / peak, "peak_kind": peak_kind},
             "fp64": {"updates_per_s": grp.sum(upd) / (ms64 * 1e-3), "ms_per_sweep": ms64,
-                     "kernel": "sweep_tile_level_kernel<double,4>", "kernel_ms": k64},
+                     "kernel": kernel_name(sw_shape64, False), "shape": sw_shape64, "kernel_ms": k64,
+                     "roofline_frac": b64 / (k64 * 1e-3) / 1e9 / peak},
             "mixed_solve": {"seconds": sm["seconds"], "sweeps_fp32": sm["sweeps_fp32"],
                             "sweeps_fp64": sm["sweeps_fp64"], "residual": sm["final_error"]},
             "fp64_gmres_solve": {"seconds": s64["seconds"], "sweeps_fp64": s64["sweeps_fp64"],

@@ -54,16 +54,20 @@ Batch::~Batch()
         if (h_slots_[p]) cudaFreeHost(h_slots_[p]);
     }
     if (h_norms_) cudaFreeHost(h_norms_);
-    free_dev(plan_.segs);
-    free_dev(plan_.level_nseg);
-    free_dev(plan_.level_nchunk);
-    free_dev(plan_.act);
-    free_dev(plan_.chunk_prefix);
-    free_dev(plan_.n_act);
-    free_dev(plan_.partials);
-    free_dev(plan_.norms);
+    for (auto &pl : plan_) {
+        free_dev(pl.segs);
+        free_dev(pl.level_nseg);
+        free_dev(pl.level_nchunk);
+        free_dev(pl.act);
+        free_dev(pl.chunk_prefix);
+        free_dev(pl.n_act);
+        free_dev(pl.partials);
+    }
+    free_dev(norms_);
     for (auto &e : ev_)
         if (e) cudaEventDestroy(e);
+    if (join_) cudaEventDestroy(join_);
+    if (stream32_) cudaStreamDestroy(stream32_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -85,7 +89,9 @@ int Batch::init(int device, int ipw32, int ipw64, std::string &err)
     ipw_[1] = ipw32;
     TB_CUDA(cudaSetDevice(device_));
     TB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    TB_CUDA(cudaStreamCreateWithFlags(&stream32_, cudaStreamNonBlocking));
     for (auto &e : ev_) TB_CUDA(cudaEventCreate(&e));
+    TB_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
     return kOk;
 }
 
@@ -180,31 +186,36 @@ int Batch::ensure_capacity(std::string &err)
         if (h_norms_) cudaFreeHost(h_norms_);
         h_norms_ = nullptr;
         TB_CUDA(cudaMallocHost(&h_norms_, sizeof(double) * 2 * cs));
-        free_dev(plan_.segs);
-        free_dev(plan_.level_nseg);
-        free_dev(plan_.level_nchunk);
-        free_dev(plan_.act);
-        free_dev(plan_.chunk_prefix);
-        free_dev(plan_.n_act);
-        free_dev(plan_.norms);
+        free_dev(norms_);
+        TB_CUDA(cudaMalloc(&norms_, sizeof(double) * 2 * cs));
+        TB_CUDA(cudaMemsetAsync(norms_, 0, sizeof(double) * 2 * cs, stream_));
         const size_t lc = std::max<size_t>(cl, 1) * kBatchClasses;
-        TB_CUDA(cudaMalloc(&plan_.segs, sizeof(BatchSeg) * cs * lc));
-        TB_CUDA(cudaMalloc(&plan_.level_nseg, sizeof(uint32_t) * lc));
-        TB_CUDA(cudaMalloc(&plan_.level_nchunk, sizeof(uint32_t) * lc));
-        TB_CUDA(cudaMalloc(&plan_.act, sizeof(uint32_t) * cs));
-        TB_CUDA(cudaMalloc(&plan_.chunk_prefix, sizeof(uint32_t) * (cs + 1)));
-        TB_CUDA(cudaMalloc(&plan_.n_act, sizeof(uint32_t)));
-        TB_CUDA(cudaMalloc(&plan_.norms, sizeof(double) * 2 * cs));
-        TB_CUDA(cudaMemsetAsync(plan_.norms, 0, sizeof(double) * 2 * cs, stream_));
-        plan_.seg_stride = (uint32_t)cs;
+        for (auto &pl : plan_) {  // one work list per pass: the two passes run at once
+            free_dev(pl.segs);
+            free_dev(pl.level_nseg);
+            free_dev(pl.level_nchunk);
+            free_dev(pl.act);
+            free_dev(pl.chunk_prefix);
+            free_dev(pl.n_act);
+            TB_CUDA(cudaMalloc(&pl.segs, sizeof(BatchSeg) * cs * lc));
+            TB_CUDA(cudaMalloc(&pl.level_nseg, sizeof(uint32_t) * lc));
+            TB_CUDA(cudaMalloc(&pl.level_nchunk, sizeof(uint32_t) * lc));
+            TB_CUDA(cudaMalloc(&pl.act, sizeof(uint32_t) * cs));
+            TB_CUDA(cudaMalloc(&pl.chunk_prefix, sizeof(uint32_t) * (cs + 1)));
+            TB_CUDA(cudaMalloc(&pl.n_act, sizeof(uint32_t)));
+            pl.norms = norms_;  // members of the two passes are disjoint
+            pl.seg_stride = (uint32_t)cs;
+        }
         cap_slots_ = cs;
         cap_levels_ = cl;
         invalidate();  // the graphs hold the old buffers
     }
     if (chunks > cap_chunks_) {
-        free_dev(plan_.partials);
         const size_t cc = std::max(chunks, cap_chunks_ * 2);
-        TB_CUDA(cudaMalloc(&plan_.partials, sizeof(double) * 2 * cc));
+        for (auto &pl : plan_) {
+            free_dev(pl.partials);
+            TB_CUDA(cudaMalloc(&pl.partials, sizeof(double) * 2 * cc));
+        }
         cap_chunks_ = cc;
         invalidate();
     }
@@ -316,19 +327,21 @@ int Batch::build_graph(int prec, std::string &err)
     bool any_solver = false;
     for (const auto &m : members_) any_solver = any_solver || m.sw->solver() != kSolveNoPivot;
     cudaGraph_t g;
-    TB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    cudaStream_t st = prec ? stream32_ : stream_;
+    const BatchPlan &plan = plan_[prec];
+    TB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     const uint32_t rec_bytes =
         (uint32_t)(ipw ? record_bytes(prec == 1) : compact_record_bytes(prec == 1));
-    cudaError_t e = launch_batch_plan(ipw, d_slots_[prec], n, max_levels_, rec_bytes, plan_, stream_);
-    if (e == cudaSuccess && prec == 0) e = launch_batch_accept(d_slots_[prec], plan_, kStreamGrid, stream_);
-    if (e == cudaSuccess) e = launch_batch_scatter(d_slots_[prec], plan_, kStreamGrid, stream_);
+    cudaError_t e = launch_batch_plan(ipw, d_slots_[prec], n, max_levels_, rec_bytes, plan, st);
+    if (e == cudaSuccess && prec == 0) e = launch_batch_accept(d_slots_[prec], plan, kStreamGrid, st);
+    if (e == cudaSuccess) e = launch_batch_scatter(d_slots_[prec], plan, kStreamGrid, st);
     for (uint32_t L = 0; L < max_levels_ && e == cudaSuccess; ++L)
-        e = prec ? launch_batch_level<float>(ipw, d_slots_[prec], plan_, L, cuts[L], any_solver, stream_)
-                 : launch_batch_level<double>(ipw, d_slots_[prec], plan_, L, cuts[L], any_solver, stream_);
-    if (e == cudaSuccess) e = launch_batch_psi_to_phi(prec == 1, d_slots_[prec], plan_, kStreamGrid, stream_);
-    if (e == cudaSuccess) e = launch_batch_post(d_slots_[prec], plan_, kStreamGrid, stream_);
-    if (e == cudaSuccess) e = launch_batch_finish(d_slots_[prec], plan_, 64, stream_);
-    cudaError_t ce = cudaStreamEndCapture(stream_, &g);
+        e = prec ? launch_batch_level<float>(ipw, d_slots_[prec], plan, L, cuts[L], any_solver, st)
+                 : launch_batch_level<double>(ipw, d_slots_[prec], plan, L, cuts[L], any_solver, st);
+    if (e == cudaSuccess) e = launch_batch_psi_to_phi(prec == 1, d_slots_[prec], plan, kStreamGrid, st);
+    if (e == cudaSuccess) e = launch_batch_post(d_slots_[prec], plan, kStreamGrid, st);
+    if (e == cudaSuccess) e = launch_batch_finish(d_slots_[prec], plan, 64, st);
+    cudaError_t ce = cudaStreamEndCapture(st, &g);
     TB_CUDA(e);
     TB_CUDA(ce);
     cudaError_t ie = cudaGraphInstantiate(&graph_[prec], g, 0);
@@ -347,10 +360,11 @@ int Batch::pass(int prec, std::string &err)
     // the graph (and with it the members' level shifts) before the slot table
     if (!graph_[prec]) TB_CHECK(build_graph(prec, err));
     for (size_t j = 0; j < n; ++j) fill_slot(prec, members_[j], h_slots_[prec][j]);
-    TB_CUDA(cudaMemcpyAsync(d_slots_[prec], h_slots_[prec], sizeof(BatchSlot) * n, cudaMemcpyHostToDevice, stream_));
-    TB_CUDA(cudaEventRecord(ev_[2 * prec], stream_));
-    TB_CUDA(cudaGraphLaunch(graph_[prec], stream_));
-    TB_CUDA(cudaEventRecord(ev_[2 * prec + 1], stream_));
+    cudaStream_t st = prec ? stream32_ : stream_;
+    TB_CUDA(cudaMemcpyAsync(d_slots_[prec], h_slots_[prec], sizeof(BatchSlot) * n, cudaMemcpyHostToDevice, st));
+    TB_CUDA(cudaEventRecord(ev_[2 * prec], st));
+    TB_CUDA(cudaGraphLaunch(graph_[prec], st));
+    TB_CUDA(cudaEventRecord(ev_[2 * prec + 1], st));
     passes_[prec]++;
     for (size_t j = 0; j < n; ++j)
         if (h_slots_[prec][j].active) updates_[prec] += (double)members_[j].updates;
@@ -373,9 +387,16 @@ int Batch::step_launch(std::string &err)
     TB_CHECK(ensure_capacity(err));
     before_[0] = passes_[0];
     before_[1] = passes_[1];
+    // the FP32 pass waits for the previous step's end on the main stream;
+    // both passes then run concurrently (their members are disjoint) and
+    // the main stream joins the FP32 one before reading the norms
+    TB_CUDA(cudaEventRecord(join_, stream_));
+    TB_CUDA(cudaStreamWaitEvent(stream32_, join_, 0));
     TB_CHECK(pass(0, err));
     TB_CHECK(pass(1, err));
-    TB_CUDA(cudaMemcpyAsync(h_norms_, plan_.norms, sizeof(double) * 2 * members_.size(), cudaMemcpyDeviceToHost,
+    TB_CUDA(cudaEventRecord(join_, stream32_));
+    TB_CUDA(cudaStreamWaitEvent(stream_, join_, 0));
+    TB_CUDA(cudaMemcpyAsync(h_norms_, norms_, sizeof(double) * 2 * members_.size(), cudaMemcpyDeviceToHost,
                             stream_));
     launched_ = true;
     return kOk;

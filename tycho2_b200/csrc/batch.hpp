@@ -101,7 +101,10 @@ private:
     BatchSlot *d_slots_[2] = {nullptr, nullptr};
     BatchSlot *h_slots_[2] = {nullptr, nullptr};  // pinned staging
     double *h_norms_ = nullptr;                    // pinned
-    BatchPlan plan_ = {};
+    BatchPlan plan_[2] = {};        // [0] FP64 pass, [1] FP32 pass
+    double *norms_ = nullptr;        // per member: the two norms of its last pass
+    cudaStream_t stream32_ = nullptr;  // the FP32 pass runs here, beside the FP64 one
+    cudaEvent_t join_ = nullptr;
     size_t cap_slots_ = 0, cap_levels_ = 0, cap_chunks_ = 0;
     cudaGraphExec_t graph_[2] = {nullptr, nullptr};
     uint32_t max_levels_ = 0;
