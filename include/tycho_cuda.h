@@ -141,6 +141,9 @@ typedef struct tycho_sweeper_opts {
     int schedule;   /* 0 = auto (one launch per level, compact records in
                        registers), 1 = one launch per wavefront level,
                        2 = one persistent dataflow launch per sweep */
+    int levelling;  /* where the wavefront levels are computed: 0 = auto (on
+                       the device from 1M cells x angles), 1 = host threads,
+                       2 = device; the result is the same either way */
 } tycho_sweeper_opts;
 
 /* Builds the device-resident instance: uploads the mesh tables, levels every
@@ -200,6 +203,11 @@ int tycho_sweeper_write_psi(tycho_sweeper *sw, const char *path);
    number of incoming interior faces summed over items. */
 int tycho_sweeper_schedule_info(const tycho_sweeper *sw, uint32_t *n_levels, uint64_t *n_items,
                                 uint64_t *n_incoming_interior);
+/* The wavefront schedule itself (any pointer may be NULL): the item list
+   (cell*A + angle, UINT32_MAX for padding) in level, then octant order, its
+   length, and the n_levels * 8 + 1 offsets of its (level, octant) segments. */
+int tycho_sweeper_schedule_arrays(const tycho_sweeper *sw, uint64_t *n_padded, uint32_t *items,
+                                  uint64_t *octant_offset);
 /* Kernel launches of one operator application of the given precision with
    its current launch shape (source, the sweep's launches, psi -> phi). */
 int tycho_sweeper_launches(const tycho_sweeper *sw, int precision, uint64_t *launches);

@@ -369,3 +369,20 @@ def test_fp32_other_solvers_within_tolerance(built, workdir, kind):
     _, phi_ref, _, _ = o.source_iteration(st, 0.5 * st, q_iso=src, iter_max=400, err_max=1e-13)
     assert rel_l1(phi, phi_ref) <= 1e-8
     sw.close()
+
+
+@pytest.mark.parametrize("n,jitter,sn", [(3, 0.05, 4), (6, 0.05, 8), (4, 0.0, 6), (9, 0.05, 8), (1, 0.0, 2)])
+def test_device_levelling_equals_host(built, workdir, n, jitter, sn):
+    """The wavefront schedule levelled on the device: the same t-levels, item
+    order, segment offsets and incoming-face count as the host levelling."""
+    import tycho2_b200 as ty
+    mesh, _ = kuhn(workdir, n, jitter, seed=41)
+    host = ty.SweeperCuda(mesh, sn, 1, levelling="host")
+    dev = ty.SweeperCuda(mesh, sn, 1, levelling="device")
+    assert host.schedule_info() == dev.schedule_info()
+    ih, oh = host.schedule_arrays()
+    idv, odv = dev.schedule_arrays()
+    assert np.array_equal(ih, idv) and np.array_equal(oh, odv)
+    assert host.launches(0) == dev.launches(0)
+    host.close()
+    dev.close()

@@ -30,7 +30,7 @@ _U32P = C.POINTER(C.c_uint32)
 class SweeperOpts(C.Structure):
     _fields_ = [("sn_order", C.c_int), ("n_groups", C.c_int), ("gauss_elim", C.c_int),
                 ("device", C.c_int), ("fp32", C.c_int), ("tpi64", C.c_int), ("tpi32", C.c_int),
-                ("schedule", C.c_int)]
+                ("schedule", C.c_int), ("levelling", C.c_int)]
 
 
 class SolveOpts(C.Structure):
@@ -83,6 +83,7 @@ SIGNATURES = {
     "tycho_sweeper_schedule_info": (C.c_int, [_P, _U32P, _U64P, _U64P]),
     "tycho_sweeper_levels": (C.c_int, [_P, _P, _P, _P]),
     "tycho_sweeper_launches": (C.c_int, [_P, C.c_int, _U64P]),
+    "tycho_sweeper_schedule_arrays": (C.c_int, [_P, _U64P, _P, _P]),
     "tycho_sweeper_time_sweeps": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P]),
     "tycho_sweeper_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(LaunchShape),
                                          C.POINTER(C.c_double)]),

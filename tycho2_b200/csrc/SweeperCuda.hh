@@ -57,7 +57,7 @@ public:
         }
         check(tycho_mesh_from_arrays(nc, nn, cellNodes.data(), coords.data(), adj.data(),
                                      f2c.data(), gid.data(), &c_mesh));
-        tycho_sweeper_opts opts;
+        tycho_sweeper_opts opts = {};
         opts.sn_order = (int)g_snOrder;
         opts.n_groups = (int)g_nGroups;
         opts.gauss_elim = g_gaussElim == GaussElim_Original     ? TYCHO_GAUSS_ORIGINAL

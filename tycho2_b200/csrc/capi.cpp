@@ -265,6 +265,7 @@ int tycho_sweeper_create(const tycho_mesh *mesh, const tycho_sweeper_opts *opts,
         o.tpi64 = opts->tpi64;
         o.tpi32 = opts->tpi32;
         o.schedule = opts->schedule;
+        o.levelling = opts->levelling;
         if (o.schedule < 0 || o.schedule > 2) {
             delete h;
             return finish(TYCHO_ERR_ARG, "schedule must be 0, 1 or 2");
@@ -351,6 +352,20 @@ int tycho_sweeper_schedule_info(const tycho_sweeper *h, uint32_t *n_levels, uint
     return TYCHO_OK;
 }
 
+int tycho_sweeper_schedule_arrays(const tycho_sweeper *h, uint64_t *n_padded, uint32_t *items,
+                                  uint64_t *octant_offset)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    return guarded([&] {
+        const auto &s = items ? h->sw.schedule_host() : h->sw.schedule();
+        if (n_padded) *n_padded = s.n_padded;
+        if (items) std::memcpy(items, s.items.data(), sizeof(uint32_t) * s.items.size());
+        if (octant_offset)
+            std::memcpy(octant_offset, s.octant_offset.data(), sizeof(uint64_t) * s.octant_offset.size());
+        return (int)TYCHO_OK;
+    });
+}
+
 int tycho_sweeper_launches(const tycho_sweeper *h, int precision, uint64_t *launches)
 {
     if (!h || !launches || (precision != 0 && precision != 1)) return finish(TYCHO_ERR_ARG, "bad argument");
@@ -363,7 +378,7 @@ int tycho_sweeper_levels(const tycho_sweeper *h, uint32_t *tlevel, uint32_t *dep
     if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
     return guarded([&] {
         const auto &sw = h->sw;
-        if (tlevel) std::memcpy(tlevel, sw.schedule().tlevel.data(), sw.schedule().tlevel.size() * 4);
+        if (tlevel) std::memcpy(tlevel, sw.schedule_host().tlevel.data(), sw.schedule_host().tlevel.size() * 4);
         if (deps) {
             std::vector<uint32_t> d;
             tycho::dependency_counts(sw.tables(), sw.quadrature(), d);
@@ -371,7 +386,7 @@ int tycho_sweeper_levels(const tycho_sweeper *h, uint32_t *tlevel, uint32_t *dep
         }
         if (blevel) {
             std::vector<uint32_t> b;
-            tycho::b_levels(sw.tables(), sw.quadrature(), sw.schedule(), b);
+            tycho::b_levels(sw.tables(), sw.quadrature(), sw.schedule_host(), b);
             std::memcpy(blevel, b.data(), b.size() * 4);
         }
         return (int)TYCHO_OK;

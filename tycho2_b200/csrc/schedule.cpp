@@ -147,6 +147,7 @@ int build_schedule(const MeshTables &t, const Quadrature &q, Schedule &s, std::s
     s.level_offset.resize(s.n_levels + 1);
     for (uint32_t l = 0; l <= s.n_levels; ++l) s.level_offset[l] = s.octant_offset[(size_t)l * kOctants];
     s.n_items = (uint64_t)A * nc;
+    s.n_padded = s.level_offset[s.n_levels];
     std::vector<uint64_t> pos(s.octant_offset.begin(), s.octant_offset.end() - 1);
     s.items.assign(s.level_offset[s.n_levels], kSentinelItem);
     for (uint64_t c = 0; c < nc; ++c)
@@ -155,6 +156,19 @@ int build_schedule(const MeshTables &t, const Quadrature &q, Schedule &s, std::s
             s.items[pos[k]++] = (uint32_t)(c * A + a);
         }
     return kOk;
+}
+
+void tlevel_from_items(Schedule &s, uint64_t n_cells, int n_angles)
+{
+    s.tlevel.assign((size_t)n_angles * n_cells, 0);
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t l = 0; l < (int64_t)s.n_levels; ++l)
+        for (uint64_t i = s.level_offset[l]; i < s.level_offset[l + 1]; ++i) {
+            const uint32_t ca = s.items[i];
+            if (ca == kSentinelItem) continue;
+            const uint64_t c = ca / (uint32_t)n_angles, a = ca % (uint32_t)n_angles;
+            s.tlevel[a * n_cells + c] = (uint32_t)l;
+        }
 }
 
 void b_levels(const MeshTables &t, const Quadrature &q, const Schedule &s, std::vector<uint32_t> &blev)

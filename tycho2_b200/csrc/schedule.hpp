@@ -15,6 +15,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "mesh.hpp"
 
 namespace tycho {
@@ -41,6 +43,7 @@ inline int octant(const Quadrature &q, int a)
 struct Schedule {
     uint32_t n_levels = 0;
     uint64_t n_items = 0;                // cells x angles (without padding)
+    uint64_t n_padded = 0;               // length of items (with padding)
     std::vector<uint64_t> level_offset;  // n_levels + 1 offsets into items
     std::vector<uint64_t> octant_offset; // n_levels * kOctants + 1: level l, octant o
                                          // starts at [l * kOctants + o]
@@ -60,6 +63,16 @@ inline double omega_dot_n(const Quadrature &q, int a, const double *n)
 // Levels every (cell, angle) pair.  Fails with kErrCycle if some direction's
 // graph has a cycle (the reference would spin forever on such a mesh).
 int build_schedule(const MeshTables &t, const Quadrature &q, Schedule &s, std::string &err);
+// The same on the current CUDA device (schedule_gpu.cu), on stream `st`:
+// level-by-level frontiers for all directions at once and a stable radix
+// sort into (level, octant, cell*A + angle) order.  Identical result.  With
+// d_items non-null the item list stays on the device: *d_items receives it
+// (cudaMalloc'd, owned by the caller) and s.items and s.tlevel stay empty;
+// tlevel_from_items derives s.tlevel once s.items has been copied back.
+int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s, uint32_t **d_items,
+                          cudaStream_t st, std::string &err);
+// s.tlevel from s.items and s.level_offset (every item of segment l has level l).
+void tlevel_from_items(Schedule &s, uint64_t n_cells, int n_angles);
 
 // Dependency counts as the GraphTraverser constructor sets them
 // (src/GraphTraverser.cc:442-458) and b-levels as Priorities' BLevelData

@@ -1,0 +1,293 @@
+// Device-side levelling of every (cell, angle) item: the GPU form of
+// build_schedule (schedule.cpp), with the same result -- t-levels, the
+// (level, octant, cell*A + angle) item order with each (level, octant)
+// segment padded to a multiple of 32, and the incoming-face count.
+//
+// Per direction the reference walks the cell graph with priority queues
+// (src/GraphTraverser.cc:467-759); here all directions advance together one
+// frontier per level (Kahn's algorithm): an item enters level L + 1 when the
+// last of its upwind neighbours leaves level L, which makes its level the
+// longest upwind chain ending at it.  Compiled with -fmad=false: omega.n is
+// formed exactly as on the host (src/TychoMesh.cc:212-223).
+#include <cub/device/device_radix_sort.cuh>
+
+#include "schedule.hpp"
+#include "status.hpp"
+
+namespace tycho {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// Per item (angle-major index a*nc + c): upwind mask (bits 0-3), downwind
+// mask (bits 4-7), count of upwind interior faces; level-0 items seed the
+// frontier.  Faces with omega.n == 0 carry no flux and order nothing (see
+// flux_mask in schedule.cpp).
+__global__ void level_init_kernel(const double *__restrict__ normal, const int4 *__restrict__ adj,
+                                  const double *__restrict__ omega, uint32_t A, uint64_t nc,
+                                  uint8_t *__restrict__ mask, uint32_t *__restrict__ cnt,
+                                  uint32_t *__restrict__ tlevel, uint32_t *__restrict__ frontier,
+                                  uint32_t *__restrict__ n_frontier, unsigned long long *__restrict__ incoming)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint64_t)A * nc) return;
+    const uint32_t a = (uint32_t)(i / nc);
+    const uint64_t c = i - (uint64_t)a * nc;
+    const double xi = omega[a], eta = omega[A + a], mu = omega[2 * A + a];
+    const int4 nb = adj[c];
+    const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+    unsigned m = 0;
+    uint32_t d = 0;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        const double *n = normal + (c * 4 + f) * 3;
+        const double odn = xi * n[0] + eta * n[1] + mu * n[2];
+        if (odn < 0) {
+            m |= 1u << f;
+            if (nbs[f] >= 0) ++d;
+        }
+        if (odn > 0) m |= 16u << f;
+    }
+    mask[i] = (uint8_t)m;
+    cnt[i] = d;
+    if (d) {
+        atomicAdd(incoming, (unsigned long long)d);
+    } else {
+        tlevel[i] = 0;
+        frontier[atomicAdd(n_frontier, 1u)] = (uint32_t)i;
+    }
+}
+
+// One level: every frontier item releases its downwind neighbours; the last
+// release of a neighbour puts it on the next frontier one level higher.
+__global__ void level_step_kernel(const uint32_t *__restrict__ frontier, uint32_t n, uint32_t level,
+                                  const int4 *__restrict__ adj, const uint8_t *__restrict__ mask, uint64_t nc,
+                                  uint32_t *__restrict__ cnt, uint32_t *__restrict__ tlevel,
+                                  uint32_t *__restrict__ next, uint32_t *__restrict__ n_next)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t i = frontier[k];
+    const uint64_t a = i / nc, c = i - a * nc;
+    const int4 nb = adj[c];
+    const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+    const unsigned m = mask[i];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        if (!(m >> (f + 4) & 1u) || nbs[f] < 0) continue;
+        const uint64_t j = a * nc + (uint64_t)nbs[f];
+        if (atomicSub(&cnt[j], 1u) == 1u) {
+            tlevel[j] = level + 1;
+            next[atomicAdd(n_next, 1u)] = (uint32_t)j;
+        }
+    }
+}
+
+// Sort keys in (cell*A + angle) order: level * 8 + octant.
+__global__ void level_keys_kernel(const uint32_t *__restrict__ tlevel, const uint8_t *__restrict__ oct, uint32_t A,
+                                  uint64_t nc, uint32_t *__restrict__ keys, uint32_t *__restrict__ vals)
+{
+    const uint64_t ca = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ca >= (uint64_t)A * nc) return;
+    const uint64_t c = ca / A, a = ca - c * A;
+    keys[ca] = tlevel[a * nc + c] * (uint32_t)kOctants + oct[a];
+    vals[ca] = (uint32_t)ca;
+}
+
+// Sorted item j (key k) goes to padded[k] + (j - unpadded[k]).
+__global__ void level_scatter_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
+                                     uint64_t n, const uint64_t *__restrict__ unpadded,
+                                     const uint64_t *__restrict__ padded, uint32_t *__restrict__ items)
+{
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t k = keys[j];
+    items[padded[k] + (j - unpadded[k])] = vals[j];
+}
+
+__global__ void level_hist_kernel(const uint32_t *__restrict__ keys, uint64_t n, unsigned long long *__restrict__ hist)
+{
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) atomicAdd(&hist[keys[j]], 1ull);
+}
+
+unsigned blocks_for(uint64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+#define TS_CUDA(expr)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (expr);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            err = std::string(#expr) + ": " + cudaGetErrorString(e_);                  \
+            return e_ == cudaErrorMemoryAllocation ? kErrOom : kErrCuda;               \
+        }                                                                              \
+    } while (0)
+
+#define TS_CHECK_HOST(expr)                                                            \
+    do {                                                                               \
+        const int st_ = (expr);                                                        \
+        if (st_ != kOk) return st_;                                                    \
+    } while (0)
+
+int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s, uint32_t **d_items_out,
+                          cudaStream_t st, std::string &err)
+{
+    const uint64_t nc = t.n_cells;
+    const uint32_t A = (uint32_t)q.n_angles;
+    const uint64_t n = (uint64_t)A * nc;
+    if (n >= (1ull << 32) || nc >= (1ull << 31)) {
+        err = "cells x angles exceeds 2^32 items";
+        return kErrArg;
+    }
+    if (n == 0) {
+        TS_CHECK_HOST(build_schedule(t, q, s, err));
+        if (d_items_out) {
+            *d_items_out = nullptr;
+            s.items.clear();
+            s.tlevel.clear();
+        }
+        return kOk;
+    }
+    s = Schedule();
+    std::vector<int4> adj(nc);
+    for (uint64_t c = 0; c < nc; ++c) {
+        int v[4];
+        for (int f = 0; f < 4; ++f) {
+            const uint64_t nb = t.adj_cell[c * 4 + f];
+            v[f] = nb == kNone ? -1 : (int)nb;
+        }
+        adj[c] = make_int4(v[0], v[1], v[2], v[3]);
+    }
+    std::vector<double> omega(3 * (size_t)A);
+    std::vector<uint8_t> oct(A);
+    for (uint32_t a = 0; a < A; ++a) {
+        omega[a] = q.xi[a];
+        omega[A + a] = q.eta[a];
+        omega[2 * A + a] = q.mu[a];
+        oct[a] = (uint8_t)octant(q, (int)a);
+    }
+    DevBuf d_normal, d_adj, d_omega, d_oct, d_mask, d_cnt, d_tlevel, d_front[2], d_ctr, d_inc;
+    TS_CUDA(cudaMalloc(&d_normal.p, sizeof(double) * t.normal.size()));
+    TS_CUDA(cudaMalloc(&d_adj.p, sizeof(int4) * nc));
+    TS_CUDA(cudaMalloc(&d_omega.p, sizeof(double) * omega.size()));
+    TS_CUDA(cudaMalloc(&d_oct.p, A));
+    TS_CUDA(cudaMalloc(&d_mask.p, n));
+    TS_CUDA(cudaMalloc(&d_cnt.p, sizeof(uint32_t) * n));
+    TS_CUDA(cudaMalloc(&d_tlevel.p, sizeof(uint32_t) * n));
+    TS_CUDA(cudaMalloc(&d_front[0].p, sizeof(uint32_t) * n));
+    TS_CUDA(cudaMalloc(&d_front[1].p, sizeof(uint32_t) * n));
+    TS_CUDA(cudaMalloc(&d_ctr.p, sizeof(uint32_t) * 2));
+    TS_CUDA(cudaMalloc(&d_inc.p, sizeof(unsigned long long)));
+    TS_CUDA(cudaMemcpyAsync(d_normal.p, t.normal.data(), sizeof(double) * t.normal.size(), cudaMemcpyHostToDevice, st));
+    TS_CUDA(cudaMemcpyAsync(d_adj.p, adj.data(), sizeof(int4) * nc, cudaMemcpyHostToDevice, st));
+    TS_CUDA(cudaMemcpyAsync(d_omega.p, omega.data(), sizeof(double) * omega.size(), cudaMemcpyHostToDevice, st));
+    TS_CUDA(cudaMemcpyAsync(d_oct.p, oct.data(), A, cudaMemcpyHostToDevice, st));
+    TS_CUDA(cudaMemsetAsync(d_ctr.p, 0, sizeof(uint32_t) * 2, st));
+    TS_CUDA(cudaMemsetAsync(d_inc.p, 0, sizeof(unsigned long long), st));
+    uint32_t *ctr = (uint32_t *)d_ctr.p;
+    level_init_kernel<<<blocks_for(n), kThreads, 0, st>>>(
+        (const double *)d_normal.p, (const int4 *)d_adj.p, (const double *)d_omega.p, A, nc, (uint8_t *)d_mask.p,
+        (uint32_t *)d_cnt.p, (uint32_t *)d_tlevel.p, (uint32_t *)d_front[0].p, ctr,
+        (unsigned long long *)d_inc.p);
+    TS_CUDA(cudaGetLastError());
+    uint32_t h_n = 0;
+    TS_CUDA(cudaMemcpyAsync(&h_n, ctr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    TS_CUDA(cudaStreamSynchronize(st));
+    uint64_t done = 0;
+    uint32_t level = 0;
+    int cur = 0;
+    while (h_n > 0) {
+        done += h_n;
+        TS_CUDA(cudaMemsetAsync(ctr + 1 - cur, 0, sizeof(uint32_t), st));
+        level_step_kernel<<<blocks_for(h_n), kThreads, 0, st>>>(
+            (const uint32_t *)d_front[cur].p, h_n, level, (const int4 *)d_adj.p, (const uint8_t *)d_mask.p, nc,
+            (uint32_t *)d_cnt.p, (uint32_t *)d_tlevel.p, (uint32_t *)d_front[1 - cur].p, ctr + 1 - cur);
+        TS_CUDA(cudaGetLastError());
+        TS_CUDA(cudaMemcpyAsync(&h_n, ctr + 1 - cur, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        TS_CUDA(cudaStreamSynchronize(st));
+        cur = 1 - cur;
+        ++level;
+    }
+    if (done != n) {
+        err = "a direction's cell dependency graph has a cycle";
+        return kErrCycle;
+    }
+    s.n_levels = level;
+    s.n_items = n;
+    unsigned long long inc = 0;
+    TS_CUDA(cudaMemcpyAsync(&inc, d_inc.p, sizeof inc, cudaMemcpyDeviceToHost, st));
+    // (level, octant, cell*A + angle) order: a stable radix sort of the keys
+    // of the items taken in cell*A + angle order
+    DevBuf d_keys[2], d_vals[2], d_temp, d_hist, d_unpad, d_pad, d_items;
+    for (int k = 0; k < 2; ++k) {
+        TS_CUDA(cudaMalloc(&d_keys[k].p, sizeof(uint32_t) * n));
+        TS_CUDA(cudaMalloc(&d_vals[k].p, sizeof(uint32_t) * n));
+    }
+    level_keys_kernel<<<blocks_for(n), kThreads, 0, st>>>((const uint32_t *)d_tlevel.p, (const uint8_t *)d_oct.p, A,
+                                                          nc, (uint32_t *)d_keys[0].p, (uint32_t *)d_vals[0].p);
+    TS_CUDA(cudaGetLastError());
+    const uint64_t nseg = (uint64_t)s.n_levels * kOctants;
+    int end_bit = 1;
+    while (end_bit < 32 && (1ull << end_bit) < nseg) ++end_bit;
+    cub::DoubleBuffer<uint32_t> kb((uint32_t *)d_keys[0].p, (uint32_t *)d_keys[1].p);
+    cub::DoubleBuffer<uint32_t> vb((uint32_t *)d_vals[0].p, (uint32_t *)d_vals[1].p);
+    size_t temp = 0;
+    TS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, kb, vb, (int64_t)n, 0, end_bit, st));
+    TS_CUDA(cudaMalloc(&d_temp.p, temp));
+    TS_CUDA(cub::DeviceRadixSort::SortPairs(d_temp.p, temp, kb, vb, (int64_t)n, 0, end_bit, st));
+    // segment sizes, then padded and unpadded offsets
+    TS_CUDA(cudaMalloc(&d_hist.p, sizeof(unsigned long long) * nseg));
+    TS_CUDA(cudaMemsetAsync(d_hist.p, 0, sizeof(unsigned long long) * nseg, st));
+    level_hist_kernel<<<blocks_for(n), kThreads, 0, st>>>(kb.Current(), n, (unsigned long long *)d_hist.p);
+    TS_CUDA(cudaGetLastError());
+    std::vector<unsigned long long> hist(nseg);
+    TS_CUDA(cudaMemcpyAsync(hist.data(), d_hist.p, sizeof(unsigned long long) * nseg, cudaMemcpyDeviceToHost, st));
+    TS_CUDA(cudaStreamSynchronize(st));
+    std::vector<uint64_t> unpadded(nseg + 1);
+    s.octant_offset.resize(nseg + 1);
+    unpadded[0] = s.octant_offset[0] = 0;
+    for (uint64_t k = 0; k < nseg; ++k) {
+        unpadded[k + 1] = unpadded[k] + hist[k];
+        s.octant_offset[k + 1] = s.octant_offset[k] + (hist[k] + kLevelPad - 1) / kLevelPad * kLevelPad;
+    }
+    s.level_offset.resize(s.n_levels + 1);
+    for (uint32_t l = 0; l <= s.n_levels; ++l) s.level_offset[l] = s.octant_offset[(size_t)l * kOctants];
+    const uint64_t total = s.level_offset[s.n_levels];
+    TS_CUDA(cudaMalloc(&d_unpad.p, sizeof(uint64_t) * (nseg + 1)));
+    TS_CUDA(cudaMalloc(&d_pad.p, sizeof(uint64_t) * (nseg + 1)));
+    TS_CUDA(cudaMalloc(&d_items.p, sizeof(uint32_t) * total));
+    TS_CUDA(cudaMemcpyAsync(d_unpad.p, unpadded.data(), sizeof(uint64_t) * (nseg + 1), cudaMemcpyHostToDevice, st));
+    TS_CUDA(cudaMemcpyAsync(d_pad.p, s.octant_offset.data(), sizeof(uint64_t) * (nseg + 1), cudaMemcpyHostToDevice,
+                            st));
+    TS_CUDA(cudaMemsetAsync(d_items.p, 0xFF, sizeof(uint32_t) * total, st));  // kSentinelItem
+    level_scatter_kernel<<<blocks_for(n), kThreads, 0, st>>>(kb.Current(), vb.Current(), n,
+                                                             (const uint64_t *)d_unpad.p, (const uint64_t *)d_pad.p,
+                                                             (uint32_t *)d_items.p);
+    TS_CUDA(cudaGetLastError());
+    s.n_padded = total;
+    s.n_incoming_interior = inc;
+    if (d_items_out) {
+        TS_CUDA(cudaStreamSynchronize(st));
+        *d_items_out = (uint32_t *)d_items.p;
+        d_items.p = nullptr;
+        return kOk;
+    }
+    s.items.resize(total);
+    s.tlevel.resize(n);
+    TS_CUDA(cudaMemcpyAsync(s.items.data(), d_items.p, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, st));
+    TS_CUDA(cudaMemcpyAsync(s.tlevel.data(), d_tlevel.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
+    TS_CUDA(cudaStreamSynchronize(st));
+    return kOk;
+}
+
+}  // namespace tycho

@@ -96,7 +96,7 @@ int Sweeper::sweep_external(int prec, const void *iso, void *psi, uint32_t *done
     df.err = ctl;
     df.abort = ctl + 3;
     df.epoch = ctl + 4;
-    df.n_items = sched_.items.size();
+    df.n_items = sched_.n_padded;
     df.spin_limit = 1u << 22;
     cudaError_t e = cudaSetDevice(device_);
     if (e == cudaSuccess) {

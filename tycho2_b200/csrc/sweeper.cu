@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <stdexcept>
 
 #include "status.hpp"
 
@@ -69,6 +70,21 @@ Sweeper::~Sweeper()
     if (stream_) cudaStreamDestroy(stream_);
 }
 
+const Schedule &Sweeper::schedule_host() const
+{
+    if (sched_.items.size() != sched_.n_padded) {
+        sched_.items.resize(sched_.n_padded);
+        if (cudaSetDevice(device_) != cudaSuccess ||
+            cudaMemcpy(sched_.items.data(), d_items_, sizeof(uint32_t) * sched_.n_padded,
+                       cudaMemcpyDeviceToHost) != cudaSuccess) {
+            sched_.items.clear();
+            throw std::runtime_error("copying the schedule back from the device failed");
+        }
+        tlevel_from_items(sched_, nc_, A_);
+    }
+    return sched_;
+}
+
 int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err)
 {
     if (o.n_groups < 1 || o.n_groups > 64) { err = "nGroups must be in 1..64"; return kErrArg; }
@@ -88,8 +104,13 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     A_ = quad_.n_angles;
     G_ = o.n_groups;
     fp32_ = o.fp32;
-    TY_CHECK(build_schedule(tables_, quad_, sched_, err));
     TY_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    if (o.levelling < 0 || o.levelling > 2) { err = "levelling must be 0, 1 or 2"; return kErrArg; }
+    const bool on_device = o.levelling == 2 || (o.levelling == 0 && nc_ * (uint64_t)A_ >= (1ull << 20));
+    // Levelled on the device, the item list stays there; the host copy is
+    // made only for the diagnostics that ask for it (schedule_host).
+    if (on_device) TY_CHECK(build_schedule_device(tables_, quad_, sched_, &d_items_, stream_, err));
+    else TY_CHECK(build_schedule(tables_, quad_, sched_, err));
     for (auto &st : aux_) TY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     TY_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
     for (auto &ev : join_) TY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -114,8 +135,8 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
         adj[c] = make_int4(a4[0], a4[1], a4[2], a4[3]);
     }
     if (nc_ >= (1ull << 31)) { err = "too many cells"; return kErrArg; }
-    const uint64_t nitems = sched_.items.size();
-    TY_CUDA(upload(d_items_, sched_.items.data(), nitems, stream_));
+    const uint64_t nitems = sched_.n_padded;
+    if (!on_device || !d_items_) TY_CUDA(upload(d_items_, sched_.items.data(), nitems, stream_));
     TY_CUDA(upload(d_adj_, adj.data(), nc_, stream_));
     TY_CUDA(upload(d_nbrmap_, nmap.data(), nc_, stream_));
     TY_CUDA(upload(d_w_, quad_.wt.data(), (size_t)A_, stream_));
@@ -428,7 +449,7 @@ int Sweeper::ensure_records(int prec, bool need_filled, std::string &err, bool c
     bool &valid = compact ? crec_valid_[k] : rec_valid_[k];
     if (!buf) {
         const size_t bytes =
-            (compact ? compact_record_bytes(prec == 1) : record_bytes(prec == 1)) * sched_.items.size();
+            (compact ? compact_record_bytes(prec == 1) : record_bytes(prec == 1)) * sched_.n_padded;
         cudaError_t e = cudaMalloc(&buf, bytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -441,7 +462,7 @@ int Sweeper::ensure_records(int prec, bool need_filled, std::string &err, bool c
     }
     if (!valid && have_xs_) {
         const LevelArgs p = level_args(prec, nullptr, nullptr, d_psi_);
-        const uint64_t n = sched_.items.size();
+        const uint64_t n = sched_.n_padded;
         if (compact)
             TY_CUDA(prec ? launch_compact_records<float>(p, n, buf, stream_)
                          : launch_compact_records<double>(p, n, buf, stream_));
@@ -534,7 +555,7 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         df.err = d_ctl_;
         df.abort = d_ctl_ + 3;
         df.epoch = d_ctl_ + 4;
-        df.n_items = sched_.items.size();
+        df.n_items = sched_.n_padded;
         df.spin_limit = 1u << 22;
         if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
         TY_CUDA(prec ? launch_persist_record<float>(sh.knob, p, d_rec_[1], d_level_off_, sched_.n_levels,
@@ -552,7 +573,7 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         df.err = d_ctl_;
         df.abort = d_ctl_ + 3;
         df.epoch = d_ctl_ + 4;
-        df.n_items = sched_.items.size();
+        df.n_items = sched_.n_padded;
         df.spin_limit = 1u << 22;  // ~2 s of polling
         TY_CUDA(launch_bump_epoch(d_ctl_ + 4, stream_));
         if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
@@ -569,7 +590,7 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         df.err = d_ctl_;
         df.abort = d_ctl_ + 3;
         df.epoch = d_ctl_ + 4;
-        df.n_items = sched_.items.size();
+        df.n_items = sched_.n_padded;
         df.spin_limit = 1u << 22;  // ~4 s of polling with backoff
         TY_CUDA(launch_bump_epoch(d_ctl_ + 4, stream_));
         if (beg) TY_CUDA(cudaEventRecord(beg, stream_));

@@ -25,6 +25,7 @@ struct SweeperOptions {
     int tpi32 = 0;
     int schedule = 0;  // 0 auto (levels, compact records), 1 level-synchronous, 2 dataflow
     int gauss_elim = 1;  // 4x4 solver, numbered as tycho_gauss_elim (deck key GaussElim)
+    int levelling = 0;   // 0 auto, 1 host, 2 device
 };
 
 // Launch shape of one precision's sweep.
@@ -109,12 +110,18 @@ public:
     int device_view(int prec, DeviceView &v, std::string &err, bool compact);
     // The resident psi was written by a sweep of this precision elsewhere.
     void note_psi_precision(int prec) { last_psi_prec_ = prec; }
-    uint64_t n_items() const { return sched_.items.size(); }
+    uint64_t n_items() const { return sched_.n_padded; }
     int solver() const { return solver_; }
 
     const MeshTables &tables() const { return tables_; }
     const Quadrature &quadrature() const { return quad_; }
+    // Levels, offsets and counts; items and tlevel are empty when the
+    // schedule was levelled on the device (schedule_host fills them).
     const Schedule &schedule() const { return sched_; }
+    // The schedule with its item list and t-levels on the host, copied back
+    // from the device on first use.  Not safe to call concurrently with
+    // other calls on the same sweeper.
+    const Schedule &schedule_host() const;
     uint64_t n_cells() const { return nc_; }
     int n_angles() const { return A_; }
     int n_groups() const { return G_; }
@@ -140,7 +147,7 @@ private:
 
     MeshTables tables_;
     Quadrature quad_;
-    Schedule sched_;
+    mutable Schedule sched_;
     uint64_t nc_ = 0;
     int A_ = 0, G_ = 0, device_ = 0;
     bool fp32_ = false, have_xs_ = false;

@@ -145,8 +145,10 @@ class SweeperCuda:
 
     SCHEDULES = {"auto": 0, "levels": 1, "dataflow": 2, "persist": 3}
 
+    LEVELLING = {"auto": 0, "host": 1, "device": 2}
+
     def __init__(self, mesh, sn_order, n_groups, gauss_elim="NoPivot", fp32=False, device=0,
-                 tpi64=0, tpi32=0, schedule="auto"):
+                 tpi64=0, tpi32=0, schedule="auto", levelling="auto"):
         if gauss_elim not in GAUSS_ELIM:
             raise ValueError("GaussElim must be one of %s" % sorted(GAUSS_ELIM))
         self.mesh = mesh
@@ -154,7 +156,7 @@ class SweeperCuda:
         self.quadrature = Quadrature(sn_order)
         self.n_angles = self.quadrature.n_angles
         opts = _capi.SweeperOpts(sn_order, n_groups, GAUSS_ELIM[gauss_elim], device, int(fp32),
-                                 tpi64, tpi32, self.SCHEDULES[schedule])
+                                 tpi64, tpi32, self.SCHEDULES[schedule], self.LEVELLING[levelling])
         h = C.c_void_p()
         check(lib().tycho_sweeper_create(mesh._h, C.byref(opts), C.byref(h)))
         self._h = h
@@ -216,6 +218,15 @@ class SweeperCuda:
         nl, ni, nin = C.c_uint32(), C.c_uint64(), C.c_uint64()
         check(lib().tycho_sweeper_schedule_info(self._h, C.byref(nl), C.byref(ni), C.byref(nin)))
         return {"n_levels": nl.value, "n_items": ni.value, "n_incoming_interior": nin.value}
+
+    def schedule_arrays(self):
+        """(items in level/octant order with padding, (level, octant) segment offsets)."""
+        n = C.c_uint64()
+        check(lib().tycho_sweeper_schedule_arrays(self._h, C.byref(n), None, None))
+        items = np.empty(n.value, np.uint32)
+        offs = np.empty(self.schedule_info()["n_levels"] * 8 + 1, np.uint64)
+        check(lib().tycho_sweeper_schedule_arrays(self._h, None, ptr(items), ptr(offs)))
+        return items, offs
 
     def launches(self, precision):
         """Kernel launches of one operator application with the current shape."""
