@@ -47,9 +47,21 @@ template <typename Real>
 __global__ void __launch_bounds__(256) batch_psi_to_phi_kernel(const BatchSlot *__restrict__ slots, BatchPlan pl)
 {
     for_each_chunk(slots, pl, [&](const BatchSlot &s, uint64_t i0, uint64_t i1, uint32_t) {
+        // from 8 groups on one element per thread (a warp's elements share
+        // a 128-byte line per angle), else four (chunks and rows are
+        // multiples of 4)
         const Real *psi = (const Real *)s.psi;
-        for (uint64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x)
-            s.phi_out[i] = psi_to_phi_elem(psi, s.w, i, s.A, s.G);
+        if (s.G >= 8) {
+            for (uint64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+                s.phi_out[i] = psi_to_phi_elem(psi, s.w, i, s.A, s.G);
+            return;
+        }
+        for (uint64_t i = i0 + 4 * threadIdx.x; i < i1; i += 4 * blockDim.x) {
+            double v[4];
+            psi_to_phi_quad(psi, s.w, i, s.A, s.G, v);
+            reinterpret_cast<double2 *>(s.phi_out + i)[0] = make_double2(v[0], v[1]);
+            reinterpret_cast<double2 *>(s.phi_out + i)[1] = make_double2(v[2], v[3]);
+        }
     });
 }
 

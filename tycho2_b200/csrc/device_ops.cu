@@ -63,9 +63,18 @@ template <typename Real>
 __global__ void psi_to_phi_kernel(const Real *__restrict__ psi, const double *__restrict__ w,
                                   double *__restrict__ phi, uint64_t nc, uint32_t A, uint32_t G)
 {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (G >= 8) {  // a warp's 32 elements share one 128-byte line per angle
+        const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= nc * 4 * G) return;
+        phi[i] = psi_to_phi_elem(psi, w, i, A, G);
+        return;
+    }
+    const uint64_t i = 4 * ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x);
     if (i >= nc * 4 * G) return;
-    phi[i] = psi_to_phi_elem(psi, w, i, A, G);
+    double s[4];
+    psi_to_phi_quad(psi, w, i, A, G, s);
+    reinterpret_cast<double2 *>(phi + i)[0] = make_double2(s[0], s[1]);
+    reinterpret_cast<double2 *>(phi + i)[1] = make_double2(s[2], s[3]);
 }
 
 __global__ void scatter_source_kernel(const double *__restrict__ phi, const double *__restrict__ q,
@@ -190,10 +199,12 @@ cudaError_t launch_psi_to_phi(const void *psi, bool psi_fp32, const double *w, d
 {
     const uint64_t n = nc * 4 * G;
     if (n == 0) return cudaSuccess;
+    // one thread per element from 8 groups on, else per four elements
+    const unsigned grid = G >= 8 ? blocks_for(n) : blocks_for(n / 4);
     if (psi_fp32)
-        psi_to_phi_kernel<float><<<blocks_for(n), 256, 0, s>>>((const float *)psi, w, phi, nc, A, G);
+        psi_to_phi_kernel<float><<<grid, 256, 0, s>>>((const float *)psi, w, phi, nc, A, G);
     else
-        psi_to_phi_kernel<double><<<blocks_for(n), 256, 0, s>>>((const double *)psi, w, phi, nc, A, G);
+        psi_to_phi_kernel<double><<<grid, 256, 0, s>>>((const double *)psi, w, phi, nc, A, G);
     return cudaGetLastError();
 }
 

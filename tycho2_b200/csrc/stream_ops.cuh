@@ -55,6 +55,48 @@ __device__ __forceinline__ double psi_to_phi_elem(const Real *__restrict__ psi, 
     return s;
 }
 
+// The same for the four elements i .. i+3 (i a multiple of 4: they lie in one
+// cell's row and are contiguous in psi for every angle): one 16-byte (FP32)
+// or two 16-byte (FP64) loads per angle, eight angles in flight, and for
+// each element the same products and sums in the same order as
+// psi_to_phi_elem.
+template <typename Real>
+__device__ __forceinline__ void psi_to_phi_quad(const Real *__restrict__ psi, const double *__restrict__ w,
+                                                uint64_t i, uint32_t A, uint32_t G, double (&s)[4])
+{
+    const uint64_t row = (uint64_t)4 * G;
+    const uint64_t c = i / row;
+    const Real *p = psi + c * A * row + (i - c * row);
+    s[0] = s[1] = s[2] = s[3] = 0.0;
+    uint32_t a = 0;
+    for (; a + 8 <= A; a += 8) {
+        Real v[8][4];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const Real *q = p + (size_t)(a + k) * row;
+            if constexpr (sizeof(Real) == 4) {
+                const float4 t = *reinterpret_cast<const float4 *>(q);
+                v[k][0] = t.x; v[k][1] = t.y; v[k][2] = t.z; v[k][3] = t.w;
+            } else {
+                const double2 t0 = reinterpret_cast<const double2 *>(q)[0];
+                const double2 t1 = reinterpret_cast<const double2 *>(q)[1];
+                v[k][0] = t0.x; v[k][1] = t0.y; v[k][2] = t1.x; v[k][3] = t1.y;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const double wa = w[a + k];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) s[e] += (double)v[k][e] * wa;
+        }
+    }
+    for (; a < A; ++a) {
+        const Real *q = p + (size_t)a * row;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) s[e] += (double)q[e] * w[a];
+    }
+}
+
 __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll
