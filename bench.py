@@ -64,6 +64,9 @@ def parse():
     p.add_argument("--shape", default="auto",
                    help="launch shape 'schedule,variant,knob[,vector[,streams]]' for both precisions "
                         "(an FP32-only vector width falls back to the widest for FP64), or auto (autotuner)")
+    p.add_argument("--profile-leg", default="main", choices=["main", "batch"],
+                   help="what cudaProfilerStart/Stop bracket (for ncu --profile-from-start off): the main "
+                        "leg's timed steps, or steps 4-6 of each batched solve")
     return p.parse_args()
 
 
@@ -251,11 +254,12 @@ def profiled_traffic(workload, family):
     return None
 
 
-def run_batch_leg(grp, dev, count, seed=4321):
+def run_batch_leg(grp, dev, count, seed=4321, profile=False):
     """Batched uneven instances: `count` problems (n ~ U{4..24}, G ~ U{1,2,4,8},
     S ~ U{4,6,8}, sigma_t ~ lognormal(0, 0.5), c ~ U[0.3, 0.95], q = 1, all
     seeded) solved together, FP64 source iteration vs FP32-sweep source
     iteration inside FP64 refinement, both to 1e-10 relative change."""
+    import torch
     import tycho2_b200 as ty
     from tycho2_b200 import problems
     t0 = time.perf_counter()
@@ -275,7 +279,16 @@ def run_batch_leg(grp, dev, count, seed=4321):
         grp.barrier()
         t = time.perf_counter()
         steps = 0
-        while b.step() > 0:
+        while True:
+            if profile and steps == 3:
+                torch.cuda.synchronize()
+                torch.cuda.profiler.start()
+            active = b.step()
+            if profile and steps == 5:
+                torch.cuda.synchronize()
+                torch.cuda.profiler.stop()
+            if active <= 0:
+                break
             steps += 1
         wall = grp.max(time.perf_counter() - t)
         tm = b.timing()
@@ -339,6 +352,11 @@ def run_serve_leg(grp, dev, count, rate, seed=99):
                     "build_p50_s": float(np.percentile([i["built"] - i["admitted"] for i in done], 50)),
                     "peak_resident_gb": st_["peak_bytes"] / 1e9, "peak_in_batch": st_["peak_active"],
                     "batch_steps": st_["steps"]}
+        big = [i for p, i in zip(params, info) if p["n"] == 48 and i["state"] == "done"]
+        if big:  # where the large requests' latency goes
+            out[key]["large_requests"] = [
+                {"latency_s": i["latency"], "queue_s": i["admitted"] - i["arrival"],
+                 "build_s": i["built"] - i["admitted"], "solve_s": i["finished"] - i["built"]} for i in big]
         srv.close()
     out["phi_rel_err_l1_max_mixed_vs_fp64"] = grp.max(max(
         float(np.abs(a - b).sum() / np.abs(b).sum()) for a, b in zip(phis["mixed"], phis["fp64"])))
@@ -361,9 +379,9 @@ def run_large_leg(grp, dev, workload="kuhn64_s8_g16"):
     sw.set_source(q, "isotropic")
     setup = time.perf_counter() - t0
     info = sw.schedule_info()
-    sw.configure(1, "levels", "compact", 64, 4, 2)
+    sw.configure(1, "levels", "compact", -96, 4, 2)
     try:  # compact FP64 records (19 GB) fit beside psi (103 GB) and the GMRES(30) basis
-        sw.configure(0, "levels", "compact", 64, 2, 2)
+        sw.configure(0, "levels", "compact", -96, 2, 2)
     except ty.TychoError:
         sw.configure(0, "levels", "tiles", 4)
     sw.time_sweeps(1, 2)
@@ -437,7 +455,8 @@ def run_b200(args):
 
     with Clocks(dev) as clk:
         grp.barrier()
-        torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
+        if args.profile_leg == "main":
+            torch.cuda.profiler.start()  # ncu --profile-from-start off captures the timed steps only
         clk.start()
         t0 = time.perf_counter()
         ms32, lvl32 = sw.time_sweeps(1, args.steps, True)
@@ -446,7 +465,8 @@ def run_b200(args):
         ms64, lvl64 = sw.time_sweeps(0, args.steps, True)
         grp.barrier()
         clk.stop()
-        torch.cuda.profiler.stop()
+        if args.profile_leg == "main":
+            torch.cuda.profiler.stop()
     clocks = clk.summary()
 
     ms32, lvl32, ms64, lvl64 = (grp.max(x) for x in (ms32, lvl32, ms64, lvl64))
@@ -502,7 +522,7 @@ def run_b200(args):
     batch = serve = None
     if not args.no_batch:
         try:
-            batch = run_batch_leg(grp, dev, args.batch_instances)
+            batch = run_batch_leg(grp, dev, args.batch_instances, profile=args.profile_leg == "batch")
         except Exception as e:  # reported, never fatal to the headline line
             batch = {"error": str(e)[:300]}
     if not args.no_serve:

@@ -232,7 +232,9 @@ int tycho_sweeper_levels(const tycho_sweeper *sw, uint32_t *tlevel, uint32_t *de
               3 = direct records: the same records loaded straight into
                   registers, one thread per (item, group vector), the source
                   read before the wait on the previous level; level schedule
-                  only, knob threads per block (64, 128, 256),
+                  only, knob threads per block (64, 128, 256; -64 / -128:
+                  the same capped at 64 registers; -96 / -80: 64 threads
+                  capped at 102 / 85 registers),
               4 = direct compact records: 64 B (FP32) / 96 B (FP64) per item
                   holding the matrix inputs (face terms, sigma_t V/20, V/20)
                   and topology; the factors are rebuilt in registers with the

@@ -55,9 +55,12 @@ def test_fp64_sweep_bit_exact_vs_oracle(built, workdir, n, jitter, sn, G, tpi, v
     sw = make(mesh, sn, G)
     knob = {"items": tpi, "tiles": min(tpi, 4), "records": 8 if tpi <= 2 else (16 if tpi <= 4 else 32),
             "direct": 64 * min(tpi, 4) if tpi != 4 else 128}
-    knob["compact"] = knob["direct"]
+    # compact: also the register-capped blocks (64 threads; at most 102, 85, 64 registers)
+    knob["compact"] = {1: 64, 2: -96, 4: -80, 8: 256, 16: -64}[tpi]
     if vector == 4 and G % 4:
         pytest.skip("two 2-group vectors per task need nGroups divisible by 4")
+    if vector == 4:
+        knob["compact"] = 128  # two vectors per task: no register cap
     if schedule == "dataflow" and variant in ("direct", "compact"):
         vg = vector or (2 if G % 2 == 0 else 1)
         if (G // vg) & (G // vg - 1) or G // vg > 32:
@@ -209,7 +212,9 @@ def test_fp32_sweep_within_tolerance(built, workdir):
                   ("levels", "records", 16, 1), ("levels", "records", 16, 2), ("levels", "direct", 128),
                   ("levels", "direct", 64, 1), ("levels", "compact", 64), ("levels", "compact", 128, 2),
                   ("dataflow", "compact", 128), ("dataflow", "direct", 128, 2), ("levels", "compact", 64, 8),
-                  ("levels", "direct", 128, 8), ("levels", "compact", 64, 4, 8), ("levels", "compact", 64, 2, 2)):
+                  ("levels", "direct", 128, 8), ("levels", "compact", 64, 4, 8), ("levels", "compact", 64, 2, 2),
+                  ("levels", "compact", -96, 4, 2), ("levels", "direct", -96, 4), ("levels", "compact", -80, 4),
+                  ("levels", "direct", -64, 2, 2)):
         sw = make(mesh, 8, G, fp32=True)
         sw.configure(1, *shape)
         sw.set_cross_sections(st, st, mat)

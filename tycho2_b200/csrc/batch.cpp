@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "devmem.hpp"
 #include "status.hpp"
 
 namespace tycho {
@@ -30,12 +31,6 @@ constexpr unsigned kLevelGridCap = 148 * 16;  // level kernels loop beyond this
 
 uint32_t magic(uint32_t d) { return d == 1 ? 0u : (uint32_t)(((1ull << 32) + d - 1) / d); }
 
-template <typename T>
-void free_dev(T *&p)
-{
-    if (p) cudaFree(p);
-    p = nullptr;
-}
 
 }  // namespace
 
@@ -45,25 +40,25 @@ Batch::~Batch()
     for (auto &g : graph_)
         if (g) cudaGraphExecDestroy(g);
     for (auto &m : members_) {
-        free_dev(m.r);
-        free_dev(m.d);
-        free_dev(m.k);
+        dev_release(m.r, stream_);
+        dev_release(m.d, stream_);
+        dev_release(m.k, stream_);
     }
     for (int p = 0; p < 2; ++p) {
-        free_dev(d_slots_[p]);
+        dev_release(d_slots_[p], stream_);
         if (h_slots_[p]) cudaFreeHost(h_slots_[p]);
     }
     if (h_norms_) cudaFreeHost(h_norms_);
     for (auto &pl : plan_) {
-        free_dev(pl.segs);
-        free_dev(pl.level_nseg);
-        free_dev(pl.level_nchunk);
-        free_dev(pl.act);
-        free_dev(pl.chunk_prefix);
-        free_dev(pl.n_act);
-        free_dev(pl.partials);
+        dev_release(pl.segs, stream_);
+        dev_release(pl.level_nseg, stream_);
+        dev_release(pl.level_nchunk, stream_);
+        dev_release(pl.act, stream_);
+        dev_release(pl.chunk_prefix, stream_);
+        dev_release(pl.n_act, stream_);
+        dev_release(pl.partials, stream_);
     }
-    free_dev(norms_);
+    dev_release(norms_, stream_);
     for (auto &e : ev_)
         if (e) cudaEventDestroy(e);
     if (join_) cudaEventDestroy(join_);
@@ -127,9 +122,9 @@ int Batch::add(Sweeper *sw, const BatchOptions &o, int &id, std::string &err)
     if (o.method == 2) {
         TB_CHECK(sw->device_view(1, m.v[1], err, ipw_[1] == 0));
         const size_t n = sw->phi_size();
-        TB_CUDA(cudaMalloc(&m.r, sizeof(double) * n));
-        TB_CUDA(cudaMalloc(&m.d, sizeof(double) * n));
-        TB_CUDA(cudaMalloc(&m.k, sizeof(double) * n));
+        TB_CUDA(dev_malloc(&m.r, sizeof(double) * n, stream_));
+        TB_CUDA(dev_malloc(&m.d, sizeof(double) * n, stream_));
+        TB_CUDA(dev_malloc(&m.k, sizeof(double) * n, stream_));
         m.state = kRunOuter;
     } else {
         m.v[1] = m.v[0];
@@ -152,9 +147,9 @@ int Batch::remove(int id, std::string &err)
         if (members_[i].id == id) {
             TB_CUDA(cudaSetDevice(device_));
             TB_CUDA(cudaStreamSynchronize(stream_));
-            free_dev(members_[i].r);
-            free_dev(members_[i].d);
-            free_dev(members_[i].k);
+            dev_release(members_[i].r, stream_);
+            dev_release(members_[i].d, stream_);
+            dev_release(members_[i].k, stream_);
             members_.erase(members_.begin() + (long)i);
             invalidate();
             return kOk;
@@ -177,32 +172,32 @@ int Batch::ensure_capacity(std::string &err)
         const size_t cs = std::max(n, cap_slots_ * 2 > 16 ? cap_slots_ * 2 : (size_t)16);
         const size_t cl = std::max((size_t)lv, cap_levels_);
         for (int p = 0; p < 2; ++p) {
-            free_dev(d_slots_[p]);
+            dev_release(d_slots_[p], stream_);
             if (h_slots_[p]) cudaFreeHost(h_slots_[p]);
             h_slots_[p] = nullptr;
-            TB_CUDA(cudaMalloc(&d_slots_[p], sizeof(BatchSlot) * cs));
+            TB_CUDA(dev_malloc(&d_slots_[p], sizeof(BatchSlot) * cs, stream_));
             TB_CUDA(cudaMallocHost(&h_slots_[p], sizeof(BatchSlot) * cs));
         }
         if (h_norms_) cudaFreeHost(h_norms_);
         h_norms_ = nullptr;
         TB_CUDA(cudaMallocHost(&h_norms_, sizeof(double) * 2 * cs));
-        free_dev(norms_);
-        TB_CUDA(cudaMalloc(&norms_, sizeof(double) * 2 * cs));
+        dev_release(norms_, stream_);
+        TB_CUDA(dev_malloc(&norms_, sizeof(double) * 2 * cs, stream_));
         TB_CUDA(cudaMemsetAsync(norms_, 0, sizeof(double) * 2 * cs, stream_));
         const size_t lc = std::max<size_t>(cl, 1) * kBatchClasses;
         for (auto &pl : plan_) {  // one work list per pass: the two passes run at once
-            free_dev(pl.segs);
-            free_dev(pl.level_nseg);
-            free_dev(pl.level_nchunk);
-            free_dev(pl.act);
-            free_dev(pl.chunk_prefix);
-            free_dev(pl.n_act);
-            TB_CUDA(cudaMalloc(&pl.segs, sizeof(BatchSeg) * cs * lc));
-            TB_CUDA(cudaMalloc(&pl.level_nseg, sizeof(uint32_t) * lc));
-            TB_CUDA(cudaMalloc(&pl.level_nchunk, sizeof(uint32_t) * lc));
-            TB_CUDA(cudaMalloc(&pl.act, sizeof(uint32_t) * cs));
-            TB_CUDA(cudaMalloc(&pl.chunk_prefix, sizeof(uint32_t) * (cs + 1)));
-            TB_CUDA(cudaMalloc(&pl.n_act, sizeof(uint32_t)));
+            dev_release(pl.segs, stream_);
+            dev_release(pl.level_nseg, stream_);
+            dev_release(pl.level_nchunk, stream_);
+            dev_release(pl.act, stream_);
+            dev_release(pl.chunk_prefix, stream_);
+            dev_release(pl.n_act, stream_);
+            TB_CUDA(dev_malloc(&pl.segs, sizeof(BatchSeg) * cs * lc, stream_));
+            TB_CUDA(dev_malloc(&pl.level_nseg, sizeof(uint32_t) * lc, stream_));
+            TB_CUDA(dev_malloc(&pl.level_nchunk, sizeof(uint32_t) * lc, stream_));
+            TB_CUDA(dev_malloc(&pl.act, sizeof(uint32_t) * cs, stream_));
+            TB_CUDA(dev_malloc(&pl.chunk_prefix, sizeof(uint32_t) * (cs + 1), stream_));
+            TB_CUDA(dev_malloc(&pl.n_act, sizeof(uint32_t), stream_));
             pl.norms = norms_;  // members of the two passes are disjoint
             pl.seg_stride = (uint32_t)cs;
         }
@@ -213,8 +208,8 @@ int Batch::ensure_capacity(std::string &err)
     if (chunks > cap_chunks_) {
         const size_t cc = std::max(chunks, cap_chunks_ * 2);
         for (auto &pl : plan_) {
-            free_dev(pl.partials);
-            TB_CUDA(cudaMalloc(&pl.partials, sizeof(double) * 2 * cc));
+            dev_release(pl.partials, stream_);
+            TB_CUDA(dev_malloc(&pl.partials, sizeof(double) * 2 * cc, stream_));
         }
         cap_chunks_ = cc;
         invalidate();

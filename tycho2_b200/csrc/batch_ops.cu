@@ -162,7 +162,7 @@ cudaError_t launch_batch_level<double>(int ipw, const BatchSlot *slots, const Ba
                                        const BatchCuts &cut, bool any_solver, cudaStream_t s)
 {
     const void *fn = ipw == 0    ? (any_solver ? (const void *)batch_direct_level_kernel<double, true>
-                                               : (const void *)batch_direct_level_kernel<double, false>)
+                                               : (const void *)batch_direct_level_kernel<double, false, 4>)
                      : ipw == 8  ? (const void *)batch_level_kernel<double, 8>
                      : ipw == 16 ? (const void *)batch_level_kernel<double, 16>
                      : ipw == 32 ? (const void *)batch_level_kernel<double, 32>

@@ -3,6 +3,7 @@
 // -fmad=false: the FP64 wavefront kernel, the per-item face terms, the
 // scalar flux and the scattering source keep the reference's rounding.
 #include "device_ops.hpp"
+#include "devmem.hpp"
 #include "sweep_kernels.cuh"
 #include "sweep_tiles.cuh"
 #include "sweep_records.cuh"
@@ -224,19 +225,19 @@ cudaError_t launch_bump_epoch(uint32_t *epoch, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t reducer_init(Reducer &r)
+cudaError_t reducer_init(Reducer &r, cudaStream_t s)
 {
-    cudaError_t e = cudaMalloc(&r.partials, sizeof(double) * kReduceBlocks * 64);
-    if (e == cudaSuccess) e = cudaMalloc(&r.result, sizeof(double) * 64);
-    if (e == cudaSuccess) e = cudaMallocHost(&r.host, sizeof(double) * 64);
+    cudaError_t e = dev_malloc(&r.partials, sizeof(double) * kReduceBlocks * 64, s);
+    if (e == cudaSuccess) e = dev_malloc(&r.result, sizeof(double) * 64, s);
+    if (e == cudaSuccess) r.host = new double[64]();
     return e;
 }
 
-void reducer_free(Reducer &r)
+void reducer_free(Reducer &r, cudaStream_t s)
 {
-    if (r.partials) cudaFree(r.partials);
-    if (r.result) cudaFree(r.result);
-    if (r.host) cudaFreeHost(r.host);
+    dev_free(r.partials, s);
+    dev_free(r.result, s);
+    delete[] r.host;
     r = Reducer();
 }
 

@@ -34,10 +34,13 @@ constexpr int kReduceBlocks = 592;  // 4 per SM on 148 SMs
 struct Reducer {
     double *partials = nullptr;  // kReduceBlocks * 64
     double *result = nullptr;    // 64 device doubles
-    double *host = nullptr;      // 64 pinned doubles
+    double *host = nullptr;      // 64 host doubles
 };
-cudaError_t reducer_init(Reducer &r);
-void reducer_free(Reducer &r);
+// Device buffers from the stream-ordered pool on stream s; the host copy of
+// the results is ordinary host memory (each reduction synchronizes s before
+// reading it).
+cudaError_t reducer_init(Reducer &r, cudaStream_t s);
+void reducer_free(Reducer &r, cudaStream_t s);
 
 // result[j] = <w, V_j> for j < k (V_j = V + j*ld), k <= 64; host copy in r.host.
 cudaError_t multi_dot(const double *w, const double *V, size_t ld, int k, uint64_t n, Reducer &r,

@@ -1,0 +1,55 @@
+#include "devmem.hpp"
+
+#include <mutex>
+
+namespace tycho {
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxDevices] = {};
+
+// The pool of the current device, made on first use.  Memory beyond what is
+// in use goes back to the system at synchronization points (release
+// threshold 0), as with cudaMalloc / cudaFree.
+cudaError_t pool_of_current(cudaMemPool_t *out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        e = cudaMemPoolCreate(&g_pool[dev], &props);
+        if (e != cudaSuccess) {
+            g_pool[dev] = nullptr;
+            return e;
+        }
+    }
+    *out = g_pool[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t dev_malloc(void **p, size_t bytes, cudaStream_t s)
+{
+    *p = nullptr;
+    cudaMemPool_t pool;
+    cudaError_t e = pool_of_current(&pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s);
+}
+
+void dev_free(void *p, cudaStream_t s)
+{
+    if (p) cudaFreeAsync(p, s);
+}
+
+}  // namespace tycho

@@ -11,6 +11,7 @@
 // formed exactly as on the host (src/TychoMesh.cc:212-223).
 #include <cub/device/device_radix_sort.cuh>
 
+#include "devmem.hpp"
 #include "schedule.hpp"
 #include "status.hpp"
 
@@ -114,13 +115,18 @@ __global__ void level_hist_kernel(const uint32_t *__restrict__ keys, uint64_t n,
 
 unsigned blocks_for(uint64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
+// A temporary from the stream-ordered pool, returned on scope exit.
 struct DevBuf {
     void *p = nullptr;
-    ~DevBuf()
-    {
-        if (p) cudaFree(p);
-    }
+    cudaStream_t s = nullptr;
+    ~DevBuf() { dev_free(p, s); }
 };
+
+cudaError_t take(DevBuf &b, size_t bytes, cudaStream_t st)
+{
+    b.s = st;
+    return dev_malloc(&b.p, bytes, st);
+}
 
 }  // namespace
 
@@ -177,17 +183,17 @@ int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s,
         oct[a] = (uint8_t)octant(q, (int)a);
     }
     DevBuf d_normal, d_adj, d_omega, d_oct, d_mask, d_cnt, d_tlevel, d_front[2], d_ctr, d_inc;
-    TS_CUDA(cudaMalloc(&d_normal.p, sizeof(double) * t.normal.size()));
-    TS_CUDA(cudaMalloc(&d_adj.p, sizeof(int4) * nc));
-    TS_CUDA(cudaMalloc(&d_omega.p, sizeof(double) * omega.size()));
-    TS_CUDA(cudaMalloc(&d_oct.p, A));
-    TS_CUDA(cudaMalloc(&d_mask.p, n));
-    TS_CUDA(cudaMalloc(&d_cnt.p, sizeof(uint32_t) * n));
-    TS_CUDA(cudaMalloc(&d_tlevel.p, sizeof(uint32_t) * n));
-    TS_CUDA(cudaMalloc(&d_front[0].p, sizeof(uint32_t) * n));
-    TS_CUDA(cudaMalloc(&d_front[1].p, sizeof(uint32_t) * n));
-    TS_CUDA(cudaMalloc(&d_ctr.p, sizeof(uint32_t) * 2));
-    TS_CUDA(cudaMalloc(&d_inc.p, sizeof(unsigned long long)));
+    TS_CUDA(take(d_normal, sizeof(double) * t.normal.size(), st));
+    TS_CUDA(take(d_adj, sizeof(int4) * nc, st));
+    TS_CUDA(take(d_omega, sizeof(double) * omega.size(), st));
+    TS_CUDA(take(d_oct, A, st));
+    TS_CUDA(take(d_mask, n, st));
+    TS_CUDA(take(d_cnt, sizeof(uint32_t) * n, st));
+    TS_CUDA(take(d_tlevel, sizeof(uint32_t) * n, st));
+    TS_CUDA(take(d_front[0], sizeof(uint32_t) * n, st));
+    TS_CUDA(take(d_front[1], sizeof(uint32_t) * n, st));
+    TS_CUDA(take(d_ctr, sizeof(uint32_t) * 2, st));
+    TS_CUDA(take(d_inc, sizeof(unsigned long long), st));
     TS_CUDA(cudaMemcpyAsync(d_normal.p, t.normal.data(), sizeof(double) * t.normal.size(), cudaMemcpyHostToDevice, st));
     TS_CUDA(cudaMemcpyAsync(d_adj.p, adj.data(), sizeof(int4) * nc, cudaMemcpyHostToDevice, st));
     TS_CUDA(cudaMemcpyAsync(d_omega.p, omega.data(), sizeof(double) * omega.size(), cudaMemcpyHostToDevice, st));
@@ -230,8 +236,8 @@ int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s,
     // of the items taken in cell*A + angle order
     DevBuf d_keys[2], d_vals[2], d_temp, d_hist, d_unpad, d_pad, d_items;
     for (int k = 0; k < 2; ++k) {
-        TS_CUDA(cudaMalloc(&d_keys[k].p, sizeof(uint32_t) * n));
-        TS_CUDA(cudaMalloc(&d_vals[k].p, sizeof(uint32_t) * n));
+        TS_CUDA(take(d_keys[k], sizeof(uint32_t) * n, st));
+        TS_CUDA(take(d_vals[k], sizeof(uint32_t) * n, st));
     }
     level_keys_kernel<<<blocks_for(n), kThreads, 0, st>>>((const uint32_t *)d_tlevel.p, (const uint8_t *)d_oct.p, A,
                                                           nc, (uint32_t *)d_keys[0].p, (uint32_t *)d_vals[0].p);
@@ -243,10 +249,10 @@ int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s,
     cub::DoubleBuffer<uint32_t> vb((uint32_t *)d_vals[0].p, (uint32_t *)d_vals[1].p);
     size_t temp = 0;
     TS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, kb, vb, (int64_t)n, 0, end_bit, st));
-    TS_CUDA(cudaMalloc(&d_temp.p, temp));
+    TS_CUDA(take(d_temp, temp, st));
     TS_CUDA(cub::DeviceRadixSort::SortPairs(d_temp.p, temp, kb, vb, (int64_t)n, 0, end_bit, st));
     // segment sizes, then padded and unpadded offsets
-    TS_CUDA(cudaMalloc(&d_hist.p, sizeof(unsigned long long) * nseg));
+    TS_CUDA(take(d_hist, sizeof(unsigned long long) * nseg, st));
     TS_CUDA(cudaMemsetAsync(d_hist.p, 0, sizeof(unsigned long long) * nseg, st));
     level_hist_kernel<<<blocks_for(n), kThreads, 0, st>>>(kb.Current(), n, (unsigned long long *)d_hist.p);
     TS_CUDA(cudaGetLastError());
@@ -263,9 +269,9 @@ int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s,
     s.level_offset.resize(s.n_levels + 1);
     for (uint32_t l = 0; l <= s.n_levels; ++l) s.level_offset[l] = s.octant_offset[(size_t)l * kOctants];
     const uint64_t total = s.level_offset[s.n_levels];
-    TS_CUDA(cudaMalloc(&d_unpad.p, sizeof(uint64_t) * (nseg + 1)));
-    TS_CUDA(cudaMalloc(&d_pad.p, sizeof(uint64_t) * (nseg + 1)));
-    TS_CUDA(cudaMalloc(&d_items.p, sizeof(uint32_t) * total));
+    TS_CUDA(take(d_unpad, sizeof(uint64_t) * (nseg + 1), st));
+    TS_CUDA(take(d_pad, sizeof(uint64_t) * (nseg + 1), st));
+    TS_CUDA(take(d_items, sizeof(uint32_t) * total, st));
     TS_CUDA(cudaMemcpyAsync(d_unpad.p, unpadded.data(), sizeof(uint64_t) * (nseg + 1), cudaMemcpyHostToDevice, st));
     TS_CUDA(cudaMemcpyAsync(d_pad.p, s.octant_offset.data(), sizeof(uint64_t) * (nseg + 1), cudaMemcpyHostToDevice,
                             st));

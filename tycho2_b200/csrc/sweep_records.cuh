@@ -935,19 +935,23 @@ static const void *direct_fn(int knob, int vg, uint32_t solver)
     case 128: return direct_fn_vg<Real, 128, Rec, 1>(vg);
     case 256: return direct_fn_vg<Real, 256, Rec, 1>(vg);
     case -64: return direct_fn_vg<Real, 64, Rec, 16>(vg);   // <= 64 registers
+    case -96: return direct_fn_vg<Real, 64, Rec, 10>(vg);   // <= 102 registers
+    case -80: return direct_fn_vg<Real, 64, Rec, 12>(vg);   // <= 85 registers
     case -128: return direct_fn_vg<Real, 128, Rec, 8>(vg);  // <= 64 registers
     default: return nullptr;
     }
 }
 
 // Direct variant: knob = threads per block (64, 128 or 256; -64 / -128: the
-// same with registers capped at 64 so that more blocks are resident); compact
+// same with registers capped at 64 so that more blocks are resident; -96 /
+// -80: 64 threads with at most 102 / 85 registers, 10 / 12 blocks per SM);
+// compact
 // picks the compact record format.
 template <typename Real>
 cudaError_t launch_direct_level(int knob, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
                                 cudaStream_t s, bool compact)
 {
-    const int bs = knob < 0 ? -knob : knob;
+    const int bs = knob == -96 || knob == -80 ? 64 : knob < 0 ? -knob : knob;
     if (end <= begin) return cudaSuccess;
     const uint64_t tasks = (end - begin) * (p.G / p.vg);
     if (tasks >= (1ull << 26)) return cudaErrorInvalidValue;

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <stdexcept>
 
+#include "devmem.hpp"
 #include "status.hpp"
 
 namespace tycho {
@@ -38,7 +39,7 @@ namespace {
 template <typename T>
 cudaError_t upload(T *&dst, const T *src, size_t n, cudaStream_t s)
 {
-    cudaError_t e = cudaMalloc(&dst, sizeof(T) * std::max<size_t>(n, 1));
+    cudaError_t e = dev_malloc(&dst, sizeof(T) * std::max<size_t>(n, 1), s);
     if (e != cudaSuccess) return e;
     if (n) e = cudaMemcpyAsync(dst, src, sizeof(T) * n, cudaMemcpyHostToDevice, s);
     return e;
@@ -59,9 +60,8 @@ Sweeper::~Sweeper()
                     d_w_, d_sigs_, d_scat_, d_qiso_, d_qang_, d_src_, d_iso_, d_iso32_, d_psi_,
                     d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_, d_done_, d_ctl_, d_rec_[0], d_rec_[1],
                     d_level_off_, d_barrier_, d_crec_[0], d_crec_[1], d_flags_};
-    for (void *b : bufs)
-        if (b) cudaFree(b);
-    reducer_free(red_);
+    for (void *b : bufs) dev_free(b, stream_);
+    reducer_free(red_, stream_);
     for (auto &st : aux_)
         if (st) cudaStreamDestroy(st);
     for (auto &ev : join_)
@@ -149,35 +149,35 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
         TY_CUDA(upload(d_omega, omega.data(), omega.size(), stream_));
         TY_CUDA(upload(d_normal, t.normal.data(), t.normal.size(), stream_));
         TY_CUDA(upload(d_area, t.area.data(), t.area.size(), stream_));
-        TY_CUDA(cudaMalloc(&d_abar64_, sizeof(double4) * std::max<uint64_t>(nitems, 1)));
-        if (fp32_) TY_CUDA(cudaMalloc(&d_abar32_, sizeof(float4) * std::max<uint64_t>(nitems, 1)));
+        TY_CUDA(dev_malloc(&d_abar64_, sizeof(double4) * std::max<uint64_t>(nitems, 1), stream_));
+        if (fp32_) TY_CUDA(dev_malloc(&d_abar32_, sizeof(float4) * std::max<uint64_t>(nitems, 1), stream_));
         TY_CUDA(launch_item_abar(d_items_, nitems, A_, d_normal, d_area, d_omega, d_abar64_,
                                  d_abar32_, stream_));
         TY_CUDA(cudaStreamSynchronize(stream_));
-        cudaFree(d_omega); cudaFree(d_normal); cudaFree(d_area);
+        dev_free(d_omega, stream_); dev_free(d_normal, stream_); dev_free(d_area, stream_);
     }
     const size_t nphi = phi_size(), npsi = psi_size();
-    TY_CUDA(cudaMalloc(&d_psi_, sizeof(double) * std::max<size_t>(npsi, 1)));
+    TY_CUDA(dev_malloc(&d_psi_, sizeof(double) * std::max<size_t>(npsi, 1), stream_));
     TY_CUDA(cudaMemsetAsync(d_psi_, 0, sizeof(double) * npsi, stream_));
-    TY_CUDA(cudaMalloc(&d_iso_, sizeof(double) * nphi));
-    if (fp32_) TY_CUDA(cudaMalloc(&d_iso32_, sizeof(float) * nphi));
-    TY_CUDA(cudaMalloc(&d_phi_, sizeof(double) * nphi));
-    TY_CUDA(cudaMalloc(&d_r_, sizeof(double) * nphi));
-    TY_CUDA(cudaMalloc(&d_tmp_, sizeof(double) * nphi));
+    TY_CUDA(dev_malloc(&d_iso_, sizeof(double) * nphi, stream_));
+    if (fp32_) TY_CUDA(dev_malloc(&d_iso32_, sizeof(float) * nphi, stream_));
+    TY_CUDA(dev_malloc(&d_phi_, sizeof(double) * nphi, stream_));
+    TY_CUDA(dev_malloc(&d_r_, sizeof(double) * nphi, stream_));
+    TY_CUDA(dev_malloc(&d_tmp_, sizeof(double) * nphi, stream_));
     TY_CUDA(cudaMemsetAsync(d_phi_, 0, sizeof(double) * nphi, stream_));
-    TY_CUDA(cudaMalloc(&d_cellk64_, sizeof(double) * 3 * nc_));
-    if (fp32_) TY_CUDA(cudaMalloc(&d_cellk32_, sizeof(float) * 3 * nc_));
-    TY_CUDA(cudaMalloc(&d_sigs_, sizeof(double) * nc_));
-    TY_CUDA(reducer_init(red_));
+    TY_CUDA(dev_malloc(&d_cellk64_, sizeof(double) * 3 * nc_, stream_));
+    if (fp32_) TY_CUDA(dev_malloc(&d_cellk32_, sizeof(float) * 3 * nc_, stream_));
+    TY_CUDA(dev_malloc(&d_sigs_, sizeof(double) * nc_, stream_));
+    TY_CUDA(reducer_init(red_, stream_));
 
     // Dataflow schedule: completion epochs per item and a control block;
     // grid = every block that can be co-resident (cooperative launch).
-    TY_CUDA(cudaMalloc(&d_done_, sizeof(uint32_t) * (size_t)nc_ * A_));
+    TY_CUDA(dev_malloc(&d_done_, sizeof(uint32_t) * (size_t)nc_ * A_, stream_));
     TY_CUDA(cudaMemsetAsync(d_done_, 0, sizeof(uint32_t) * (size_t)nc_ * A_, stream_));
-    TY_CUDA(cudaMalloc(&d_ctl_, sizeof(uint32_t) * 8));
+    TY_CUDA(dev_malloc(&d_ctl_, sizeof(uint32_t) * 8, stream_));
     TY_CUDA(cudaMemsetAsync(d_ctl_, 0, sizeof(uint32_t) * 8, stream_));
     TY_CUDA(upload(d_level_off_, sched_.level_offset.data(), sched_.level_offset.size(), stream_));
-    TY_CUDA(cudaMalloc(&d_barrier_, sizeof(unsigned long long)));
+    TY_CUDA(dev_malloc(&d_barrier_, sizeof(unsigned long long), stream_));
     // Default launch shape: compact records in registers, one launch per
     // level (64-thread blocks); schedule 2 asks for the persistent dataflow
     // kernel (warp tiles); explicit threads-per-item selects the
@@ -192,7 +192,9 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
         }
         if (tpi) TY_CHECK(configure(prec, o.schedule == 1 ? 1 : 2, 0, tpi, err));
         else if (o.schedule == 2) TY_CHECK(configure(prec, 2, 1, 4, err));
-        else TY_CHECK(configure(prec, 1, 4, nopivot ? 64 : 128, err));
+        // compact records, 64 threads at most 102 registers, 2 octant streams:
+        // the fastest measured shape on the 32^3 and 64^3 S8 workloads
+        else TY_CHECK(configure(prec, 1, 4, nopivot ? -96 : 128, err, 0, nopivot ? 2 : 1));
     }
     TY_CUDA(cudaStreamSynchronize(stream_));
     return kOk;
@@ -249,8 +251,9 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
         return kErrArg;
     }
     if (variant >= 3 && schedule == 1 && knob != 64 && knob != 128 && knob != 256 && knob != -64 &&
-        knob != -128) {
-        err = "direct record variants on levels: 64, 128 or 256 threads per block (-64, -128: 64 registers)";
+        knob != -128 && knob != -96 && knob != -80) {
+        err = "direct record variants on levels: 64, 128 or 256 threads per block (-64, -128: 64 registers; "
+              "-96 / -80: 64 threads, at most 102 / 85 registers)";
         return kErrArg;
     }
     if (variant >= 3 && schedule == 2) {
@@ -305,10 +308,10 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
         sh.direct_grid = (unsigned)(sms * direct_per_sm);
         const size_t flags = (size_t)nc_ * A_ * (G_ / vg);
         if (flags > flags_cap_) {
-            if (d_flags_) cudaFree(d_flags_);
+            if (d_flags_) dev_free(d_flags_, stream_);
             d_flags_ = nullptr;
             flags_cap_ = 0;
-            TY_CUDA(cudaMalloc(&d_flags_, sizeof(uint32_t) * flags));
+            TY_CUDA(dev_malloc(&d_flags_, sizeof(uint32_t) * flags, stream_));
             TY_CUDA(cudaMemsetAsync(d_flags_, 0, sizeof(uint32_t) * flags, stream_));
             flags_cap_ = flags;
         }
@@ -335,7 +338,7 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
     LaunchShape keep = shape_[prec ? 1 : 0];
     for (int sched = 1; sched <= 3; ++sched)
         for (int variant = 0; variant <= 4; ++variant)
-            for (int knob : {1, 2, 4, 8, 16, 32, 64, 128, 256, -64, -128}) {
+            for (int knob : {1, 2, 4, 8, 16, 32, 64, 128, 256, -64, -80, -96, -128}) {
                 if (knob < 0 && (variant < 3 || sched != 1)) continue;
                 if (solver_ != kSolveNoPivot && (variant < 3 || sched != 1 || knob != 128)) continue;
                 if (variant == 0 && ((knob > 2 * G_ && knob > 1) || knob > 16)) continue;  // idle lanes
@@ -450,7 +453,7 @@ int Sweeper::ensure_records(int prec, bool need_filled, std::string &err, bool c
     if (!buf) {
         const size_t bytes =
             (compact ? compact_record_bytes(prec == 1) : record_bytes(prec == 1)) * sched_.n_padded;
-        cudaError_t e = cudaMalloc(&buf, bytes);
+        cudaError_t e = dev_malloc(&buf, bytes, stream_);
         if (e != cudaSuccess) {
             cudaGetLastError();
             buf = nullptr;
@@ -470,6 +473,8 @@ int Sweeper::ensure_records(int prec, bool need_filled, std::string &err, bool c
             TY_CUDA(prec ? launch_item_records<float>(p, n, buf, stream_)
                          : launch_item_records<double>(p, n, buf, stream_));
         valid = true;
+        // the records are read on other streams too (octant chains, batches)
+        TY_CUDA(cudaStreamSynchronize(stream_));
     }
     if (need_filled && !valid) { err = "cross sections not set"; return kErrMissing; }
     return kOk;
@@ -510,10 +515,10 @@ int Sweeper::set_cross_sections(const double *sigma_t, const double *sigma_s, co
         TY_CUDA(cudaMemcpyAsync(d_cellk32_, k32.data(), sizeof(float) * k32.size(), cudaMemcpyHostToDevice, stream_));
     TY_CUDA(cudaMemcpyAsync(d_sigs_, sigma_s, sizeof(double) * nc_, cudaMemcpyHostToDevice, stream_));
     if (scatter) {
-        if (!d_scat_) TY_CUDA(cudaMalloc(&d_scat_, sizeof(double) * G_ * G_));
+        if (!d_scat_) TY_CUDA(dev_malloc(&d_scat_, sizeof(double) * G_ * G_, stream_));
         TY_CUDA(cudaMemcpyAsync(d_scat_, scatter, sizeof(double) * G_ * G_, cudaMemcpyHostToDevice, stream_));
     } else if (d_scat_) {
-        cudaFree(d_scat_);
+        dev_free(d_scat_, stream_);
         d_scat_ = nullptr;
     }
     TY_CUDA(cudaStreamSynchronize(stream_));
@@ -532,11 +537,11 @@ int Sweeper::set_source(int kind, const double *q, std::string &err)
     double *&dst = kind == 0 ? d_qang_ : d_qiso_;
     const size_t n = kind == 0 ? psi_size() : phi_size();
     if (!q) {
-        if (dst) cudaFree(dst);
+        if (dst) dev_free(dst, stream_);
         dst = nullptr;
         return kOk;
     }
-    if (!dst) TY_CUDA(cudaMalloc(&dst, sizeof(double) * n));
+    if (!dst) TY_CUDA(dev_malloc(&dst, sizeof(double) * n, stream_));
     TY_CUDA(cudaMemcpyAsync(dst, q, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
     TY_CUDA(cudaStreamSynchronize(stream_));
     return kOk;
@@ -676,7 +681,7 @@ int Sweeper::sweep_host(const double *source, double *psi, std::string &err)
     if (!source || !psi) { err = "source and psi are required"; return kErrArg; }
     TY_CUDA(cudaSetDevice(device_));
     const size_t n = psi_size();
-    if (!d_src_) TY_CUDA(cudaMalloc(&d_src_, sizeof(double) * n));
+    if (!d_src_) TY_CUDA(dev_malloc(&d_src_, sizeof(double) * n, stream_));
     TY_CUDA(cudaMemcpyAsync(d_src_, source, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
     TY_CHECK(apply(0, nullptr, false, nullptr, d_src_, err));
     TY_CUDA(cudaMemcpyAsync(psi, d_psi_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
@@ -688,10 +693,10 @@ int Sweeper::ensure_krylov(int m, std::string &err)
 {
     if (m < 1 || m > 60) { err = "GMRES restart must be in 1..60"; return kErrArg; }
     if (krylov_m_ >= m) return kOk;
-    if (d_V_) cudaFree(d_V_);
+    if (d_V_) dev_free(d_V_, stream_);
     d_V_ = nullptr;
-    TY_CUDA(cudaMalloc(&d_V_, sizeof(double) * phi_size() * (m + 1)));
-    if (!d_h_) TY_CUDA(cudaMalloc(&d_h_, sizeof(double) * 64));
+    TY_CUDA(dev_malloc(&d_V_, sizeof(double) * phi_size() * (m + 1), stream_));
+    if (!d_h_) TY_CUDA(dev_malloc(&d_h_, sizeof(double) * 64, stream_));
     krylov_m_ = m;
     return kOk;
 }
@@ -916,7 +921,7 @@ int Sweeper::time_sweeps(int prec, int n, bool flush_l2, double *ms, std::string
     TY_CUDA(cudaSetDevice(device_));
     if (n < 1) { err = "n must be >= 1"; return kErrArg; }
     const size_t flush_bytes = 256ull << 20;  // > 126 MB L2
-    if (flush_l2 && !d_flush_) TY_CUDA(cudaMalloc(&d_flush_, flush_bytes));
+    if (flush_l2 && !d_flush_) TY_CUDA(dev_malloc(&d_flush_, flush_bytes, stream_));
     cudaEvent_t e0, e1, l0, l1;
     TY_CUDA(cudaEventCreate(&e0));
     TY_CUDA(cudaEventCreate(&e1));
