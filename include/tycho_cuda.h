@@ -355,6 +355,13 @@ int tycho_batch_timing(const tycho_batch *b, double *ms, int *passes, double *up
    compact records. */
 uint64_t tycho_footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, int mixed, int compact);
 
+/* Sweepers, batches and servers take device memory from one stream-ordered
+   pool per device, which keeps freed memory for the next allocation (freeing
+   never waits for the device, and the next problem of the same size maps no
+   new memory).  This hands the pool's unused memory back to the system;
+   it waits for the device first. */
+int tycho_release_cached_memory(int device);
+
 typedef struct tycho_server tycho_server;
 
 typedef struct tycho_server_opts {

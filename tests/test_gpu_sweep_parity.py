@@ -391,3 +391,25 @@ def test_device_levelling_equals_host(built, workdir, n, jitter, sn):
     assert host.launches(0) == dev.launches(0)
     host.close()
     dev.close()
+
+
+def test_pool_memory_reused_and_released(built, workdir):
+    """Sweepers take device memory from the library's pool: a second sweeper
+    reuses what the first freed, the pool can be trimmed, and results do not
+    depend on either."""
+    import tycho2_b200 as ty
+    mesh, _ = kuhn(workdir, 5, 0.05, seed=3)
+    rng = np.random.default_rng(8)
+    st = rng.lognormal(0.0, 0.5, mesh.n_cells)
+    psis = []
+    for trim in (False, True, False):
+        sw = make(mesh, 8, 4)
+        sw.set_cross_sections(st, np.zeros(mesh.n_cells))
+        src = np.random.default_rng(1).uniform(0.0, 1.0, sw.psi_shape)
+        psi = np.empty(sw.psi_shape)
+        sw.sweep(psi, src)
+        psis.append(psi)
+        sw.close()
+        if trim:
+            ty.release_cached_memory(0)
+    assert bits_equal(psis[0], psis[1]) and bits_equal(psis[0], psis[2])

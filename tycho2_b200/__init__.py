@@ -5,8 +5,9 @@ CUDA kernels in libtycho_b200.so (C ABI: include/tycho_cuda.h); this package
 is the host-side mirror of the reference's interface over that ABI.
 """
 from ._capi import TychoError, lib  # noqa: F401
-from .sweeper import BatchSolver, Quadrature, SolveServer, SweeperCuda, TychoMesh, footprint_bytes  # noqa: F401
+from .sweeper import (BatchSolver, Quadrature, SolveServer, SweeperCuda, TychoMesh, footprint_bytes,  # noqa: F401
+                      release_cached_memory)
 from . import problems  # noqa: F401
 
 __all__ = ["TychoError", "TychoMesh", "Quadrature", "SweeperCuda", "BatchSolver", "SolveServer",
-           "footprint_bytes", "problems", "lib"]
+           "footprint_bytes", "release_cached_memory", "problems", "lib"]

@@ -83,6 +83,7 @@ SIGNATURES = {
     "tycho_sweeper_schedule_info": (C.c_int, [_P, _U32P, _U64P, _U64P]),
     "tycho_sweeper_levels": (C.c_int, [_P, _P, _P, _P]),
     "tycho_sweeper_launches": (C.c_int, [_P, C.c_int, _U64P]),
+    "tycho_release_cached_memory": (C.c_int, [C.c_int]),
     "tycho_sweeper_schedule_arrays": (C.c_int, [_P, _U64P, _P, _P]),
     "tycho_sweeper_time_sweeps": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P]),
     "tycho_sweeper_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(LaunchShape),

@@ -2,6 +2,7 @@
 #include "../../include/tycho_cuda.h"
 
 #include <cstring>
+#include <memory>
 #include <exception>
 #include <new>
 #include <string>
@@ -10,12 +11,16 @@
 #include "schedule.hpp"
 #include "status.hpp"
 #include "batch.hpp"
+#include "devmem.hpp"
 #include "server.hpp"
 #include "sweeper.hpp"
 
 struct tycho_mesh {
     tycho::MeshRecords rec;
-    tycho::MeshTables tab;
+    // shared with the sweepers and served requests made from this mesh, so
+    // that they hold the tables without copying them
+    std::shared_ptr<tycho::MeshTables> tabp = std::make_shared<tycho::MeshTables>();
+    tycho::MeshTables &tab = *tabp;
 };
 
 struct tycho_sweeper {
@@ -276,7 +281,7 @@ int tycho_sweeper_create(const tycho_mesh *mesh, const tycho_sweeper_opts *opts,
             return finish(TYCHO_ERR_ARG, "GaussElim must be Original, NoPivot, CramerGlu or CramerIntel");
         }
         o.gauss_elim = opts->gauss_elim;
-        int st = h->sw.init(mesh->tab, o, err);
+        int st = h->sw.init(mesh->tabp, o, err);
         if (st != tycho::kOk) { delete h; return finish(st, err); }
         *out = h;
         return (int)TYCHO_OK;
@@ -546,6 +551,13 @@ uint64_t tycho_footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, int
     return tycho::footprint_bytes(n_cells, sn_order, n_groups, mixed != 0, compact != 0);
 }
 
+int tycho_release_cached_memory(int device)
+{
+    const cudaError_t e = tycho::dev_trim(device);
+    if (e != cudaSuccess) return finish(TYCHO_ERR_CUDA, std::string("releasing cached memory: ") + cudaGetErrorString(e));
+    return TYCHO_OK;
+}
+
 int tycho_server_create(const tycho_server_opts *o, tycho_server **out)
 {
     if (!o || !out) return finish(TYCHO_ERR_ARG, "null argument");
@@ -586,7 +598,7 @@ int tycho_server_submit(tycho_server *s, const tycho_mesh *mesh, int sn_order, i
     if (sn_order < 2 || sn_order > 32 || sn_order % 2) return finish(TYCHO_ERR_ARG, "bad SN order");
     std::string err;
     return guarded([&] {
-        return finish(s->s.submit(mesh->tab, sn_order, n_groups, sigma_t, sigma_s, scatter, q_iso, arrival,
+        return finish(s->s.submit(mesh->tabp, sn_order, n_groups, sigma_t, sigma_s, scatter, q_iso, arrival,
                                   phi_out, *id, err),
                       err);
     });

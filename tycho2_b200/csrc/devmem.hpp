@@ -27,4 +27,8 @@ void dev_release(T *&p, cudaStream_t s)
     p = nullptr;
 }
 
+// Returns the pool's unused memory on `device` to the system (waits for the
+// device first).
+cudaError_t dev_trim(int device);
+
 }  // namespace tycho

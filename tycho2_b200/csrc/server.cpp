@@ -5,6 +5,7 @@
 #include <chrono>
 #include <thread>
 
+#include "devmem.hpp"
 #include "status.hpp"
 
 namespace tycho {
@@ -47,7 +48,32 @@ int Server::init(const ServerOptions &o, std::string &err)
         const int s = b.init(o.device, o.ipw32, o.ipw64, err);
         if (s != kOk) return s;
     }
+    reserve_pool();
     return kOk;
+}
+
+// Maps the budget (at most 90% of the free device memory) into the device
+// pool once, so that no request's build waits for fresh device memory to be
+// mapped (a 48^3 S8 G=8 request holds ~40 GB: mapping it took ~0.4 s).  A
+// failed reservation only costs that time later.
+void Server::reserve_pool()
+{
+    size_t free_b = 0, total_b = 0;
+    if (cudaSetDevice(o_.device) != cudaSuccess || cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    const size_t want = (size_t)std::min(o_.budget_bytes, 0.9 * (double)free_b);
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    void *p = nullptr;
+    if (dev_malloc(&p, want, s) == cudaSuccess) dev_free(p, s);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    cudaGetLastError();
 }
 
 double Server::now() const
@@ -56,17 +82,18 @@ double Server::now() const
     return duration<double>(steady_clock::now().time_since_epoch()).count() - t0_;
 }
 
-int Server::submit(const MeshTables &t, int sn, int G, const double *sigma_t, const double *sigma_s,
+int Server::submit(std::shared_ptr<const MeshTables> tp, int sn, int G, const double *sigma_t, const double *sigma_s,
                    const double *scatter, const double *q_iso, double arrival, double *phi_out, int &id,
                    std::string &err)
 {
-    if (!sigma_t || !sigma_s || !phi_out || G < 1 || G > 64 || arrival < 0) {
+    if (!tp || !sigma_t || !sigma_s || !phi_out || G < 1 || G > 64 || arrival < 0) {
         err = "bad request (cross sections, phi buffer, 1..64 groups, arrival >= 0)";
         return kErrArg;
     }
     auto r = std::make_unique<Request>();
     r->id = (int)reqs_.size() + 1;
-    r->tables = t;
+    const MeshTables &t = *tp;
+    r->tables = tp;
     r->sn = sn;
     r->G = G;
     const size_t nc = t.n_cells;
@@ -105,7 +132,16 @@ void Server::worker()
         Request *r = nullptr;
         {
             std::unique_lock<std::mutex> lk(mu_);
-            cv_work_.wait(lk, [&] { return stop_ || !build_q_.empty(); });
+            cv_work_.wait(lk, [&] { return stop_ || !build_q_.empty() || !retire_q_.empty(); });
+            if (!retire_q_.empty()) {
+                auto job = std::move(retire_q_.front());
+                retire_q_.pop_front();
+                lk.unlock();
+                job.first.reset();
+                lk.lock();
+                freed_bytes_ += job.second;
+                continue;
+            }
             if (stop_ && build_q_.empty()) return;
             r = build_q_.front();
             build_q_.pop_front();
@@ -185,6 +221,8 @@ int Server::run(std::string &err)
         std::vector<Request *> ready;
         {
             std::unique_lock<std::mutex> lk(mu_);
+            reserved -= freed_bytes_;  // retired sweepers the workers have destroyed
+            freed_bytes_ = 0;
             const bool idle = !inflight[0] && !inflight[1] && in_lane[0] + in_lane[1] == 0 &&
                               waiting[0].empty() && waiting[1].empty();
             if (idle && built_.empty()) {
@@ -231,10 +269,13 @@ int Server::run(std::string &err)
                     r->stats = st;
                     s = b.remove(r->member, err);
                     if (s != kOk) return s;
-                    r->sw.reset();
+                    {
+                        std::lock_guard<std::mutex> lk(mu_);
+                        retire_q_.emplace_back(std::move(r->sw), (double)r->footprint);
+                    }
+                    cv_work_.notify_one();
                     r->state = 4;
                     r->t_done = now();
-                    reserved -= (double)r->footprint;
                     --in_lane[L];
                     --pending;
                 }

@@ -39,7 +39,7 @@ class Server {
 public:
     struct Request {
         int id = 0;
-        MeshTables tables;
+        std::shared_ptr<const MeshTables> tables;
         int sn = 4, G = 1;
         std::vector<double> sigma_t, sigma_s, scatter, q;
         double arrival = 0;     // seconds after run() starts
@@ -57,7 +57,7 @@ public:
 
     ~Server();
     int init(const ServerOptions &o, std::string &err);
-    int submit(const MeshTables &t, int sn, int G, const double *sigma_t, const double *sigma_s,
+    int submit(std::shared_ptr<const MeshTables> t, int sn, int G, const double *sigma_t, const double *sigma_s,
                const double *scatter, const double *q_iso, double arrival, double *phi_out, int &id,
                std::string &err);
     // Serves every submitted request (arrivals relative to the call).
@@ -75,6 +75,7 @@ private:
     // Two lanes, each a batch on its own stream: requests of at least
     // large_items cells x angles sweep in lane 1, so a deep mesh does not set
     // the step time of the small ones; both lanes run on the GPU at once.
+    void reserve_pool();
     static constexpr int kLanes = 2;
     Batch lanes_[kLanes];
     // build queue shared with the workers
@@ -82,6 +83,10 @@ private:
     std::condition_variable cv_work_, cv_built_;
     std::deque<Request *> build_q_;
     std::vector<Request *> built_;
+    // finished requests' sweepers, destroyed by the workers (not on the loop
+    // thread); their footprints go back to the budget once destroyed
+    std::deque<std::pair<std::unique_ptr<Sweeper>, double>> retire_q_;
+    double freed_bytes_ = 0;
     bool stop_ = false;
     std::vector<std::thread> workers_;
     double t0_ = 0;

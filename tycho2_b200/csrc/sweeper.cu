@@ -16,6 +16,7 @@
 
 #include "devmem.hpp"
 #include "status.hpp"
+#include "trace.hpp"
 
 namespace tycho {
 
@@ -54,6 +55,7 @@ uint32_t group_magic(uint32_t G)
 
 Sweeper::~Sweeper()
 {
+    TraceScope trace("sweeper.destroy");
     if (device_ >= 0) cudaSetDevice(device_);
     for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
     void *bufs[] = {d_items_, d_abar64_, d_abar32_, d_adj_, d_nbrmap_, d_cellk64_, d_cellk32_,
@@ -85,11 +87,14 @@ const Schedule &Sweeper::schedule_host() const
     return sched_;
 }
 
-int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err)
+int Sweeper::init(std::shared_ptr<const MeshTables> tp, const SweeperOptions &o, std::string &err)
 {
+    if (!tp) { err = "no mesh tables"; return kErrArg; }
+    const MeshTables &t = *tp;
     if (o.n_groups < 1 || o.n_groups > 64) { err = "nGroups must be in 1..64"; return kErrArg; }
     if (o.gauss_elim < 0 || o.gauss_elim > 3) { err = "GaussElim must be 0..3"; return kErrArg; }
     solver_ = o.gauss_elim;
+    TraceScope trace_init("sweeper.init");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         err = "no CUDA device: the B200 sweep has no CPU fallback";
@@ -99,7 +104,7 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     device_ = o.device;
     TY_CUDA(cudaSetDevice(device_));
     TY_CHECK(make_quadrature(o.sn_order, quad_, err));
-    tables_ = t;
+    tables_ = std::move(tp);
     nc_ = t.n_cells;
     A_ = quad_.n_angles;
     G_ = o.n_groups;
@@ -109,8 +114,12 @@ int Sweeper::init(const MeshTables &t, const SweeperOptions &o, std::string &err
     const bool on_device = o.levelling == 2 || (o.levelling == 0 && nc_ * (uint64_t)A_ >= (1ull << 20));
     // Levelled on the device, the item list stays there; the host copy is
     // made only for the diagnostics that ask for it (schedule_host).
-    if (on_device) TY_CHECK(build_schedule_device(tables_, quad_, sched_, &d_items_, stream_, err));
-    else TY_CHECK(build_schedule(tables_, quad_, sched_, err));
+    {
+        TraceScope ts(on_device ? "sweeper.init.levelling_device" : "sweeper.init.levelling_host");
+        if (on_device) TY_CHECK(build_schedule_device(t, quad_, sched_, &d_items_, stream_, err));
+        else TY_CHECK(build_schedule(t, quad_, sched_, err));
+    }
+    TraceScope trace_rest("sweeper.init.topology_uploads_buffers");
     for (auto &st : aux_) TY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     TY_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
     for (auto &ev : join_) TY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -502,7 +511,7 @@ int Sweeper::set_cross_sections(const double *sigma_t, const double *sigma_s, co
     std::vector<double> k64(3 * nc_);
     std::vector<float> k32(3 * nc_);
     for (uint64_t c = 0; c < nc_; ++c) {
-        const double volume = tables_.volume[c], sigma = sigma_t[c];
+        const double volume = tables_->volume[c], sigma = sigma_t[c];
         if (!(sigma >= 0.0) || !std::isfinite(sigma)) { err = "sigma_t must be finite and >= 0"; return kErrArg; }
         // Transport.cc:66-69 and :84-102 with the reference's grouping.
         k64[3 * c + 0] = volume / 20.0;
@@ -890,7 +899,7 @@ int Sweeper::write_psi(const std::string &path, std::string &err)
     bool ok = std::fwrite(name, 1, 32, fp) == 32 && std::fwrite(hdr, 8, 4, fp) == 4;
     const size_t per = (size_t)A_ * 4 * G_;
     for (uint64_t c = 0; c < nc_ && ok; ++c) {
-        ok = std::fseek(fp, (long)(64 + tables_.cell_gid[c] * per * 8), SEEK_SET) == 0 &&
+        ok = std::fseek(fp, (long)(64 + tables_->cell_gid[c] * per * 8), SEEK_SET) == 0 &&
              std::fwrite(&psi[c * per], 8, per, fp) == per;
     }
     std::fclose(fp);

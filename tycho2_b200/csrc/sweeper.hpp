@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -62,7 +63,8 @@ struct SolveStats {
 class Sweeper {
 public:
     ~Sweeper();
-    int init(const MeshTables &t, const SweeperOptions &o, std::string &err);
+    // The sweeper keeps a reference to the tables (no copy).
+    int init(std::shared_ptr<const MeshTables> t, const SweeperOptions &o, std::string &err);
 
     int set_cross_sections(const double *sigma_t, const double *sigma_s, const double *scatter,
                            std::string &err);
@@ -113,7 +115,7 @@ public:
     uint64_t n_items() const { return sched_.n_padded; }
     int solver() const { return solver_; }
 
-    const MeshTables &tables() const { return tables_; }
+    const MeshTables &tables() const { return *tables_; }
     const Quadrature &quadrature() const { return quad_; }
     // Levels, offsets and counts; items and tlevel are empty when the
     // schedule was levelled on the device (schedule_host fills them).
@@ -145,7 +147,7 @@ private:
     // (and computes, when stale) its contents for the current cross sections.
     int ensure_records(int prec, bool need_filled, std::string &err, bool compact = false);
 
-    MeshTables tables_;
+    std::shared_ptr<const MeshTables> tables_;
     Quadrature quad_;
     mutable Schedule sched_;
     uint64_t nc_ = 0;

@@ -342,6 +342,12 @@ class BatchSolver:
         self.close()
 
 
+def release_cached_memory(device=0):
+    """Hands the device memory pool's unused memory back to the system (the
+    pool keeps what sweepers free for reuse, like a caching allocator)."""
+    check(lib().tycho_release_cached_memory(device))
+
+
 def footprint_bytes(n_cells, sn_order, n_groups, mixed=True, compact=True):
     """Device bytes one resident solve request holds (tycho_footprint_bytes)."""
     return int(lib().tycho_footprint_bytes(n_cells, sn_order, n_groups, int(mixed), int(compact)))
