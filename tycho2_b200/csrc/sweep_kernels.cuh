@@ -52,11 +52,13 @@ struct ItemFactor {
 };
 
 // FP64 keeps the reference's IEEE divisions (bit-identical results); FP32,
-// checked by tolerance, uses reciprocals.
+// checked by tolerance, uses the hardware's approximate reciprocal (about 1
+// ulp; the pivots are far inside its range), which keeps the chain of the
+// per-item factorization short.
 template <typename Real>
 __device__ __forceinline__ Real div_ref(Real x, Real y)
 {
-    if constexpr (std::is_same<Real, float>::value) return x * __frcp_rn(y);
+    if constexpr (std::is_same<Real, float>::value) return __fdividef(x, y);
     else return x / y;
 }
 
