@@ -264,12 +264,12 @@ template <typename Real, int VG, typename View>
 __device__ __forceinline__ void pair_load_source(const LevelArgs &p, const View &R, uint32_t g, PairIn<Real, VG> &in)
 {
     const uint32_t G = p.G;
-    const size_t rowG = (size_t)4 * G;
+    const uint32_t rowG = 4u * G;  // G <= 64: 32-bit operands, one widening multiply per address
     const uint32_t c = R.u(0);
     const Real *__restrict__ iso = reinterpret_cast<const Real *>(p.iso);
     if (p.qang) {
-        const double *qa = p.qang + (size_t)R.u(1) * rowG + g;
-        const Real *ic = iso ? iso + (size_t)c * rowG + g : nullptr;
+        const double *qa = p.qang + (uint64_t)R.u(1) * rowG + g;
+        const Real *ic = iso ? iso + (uint64_t)c * rowG + g : nullptr;
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             Real icv[VG];
@@ -278,7 +278,7 @@ __device__ __forceinline__ void pair_load_source(const LevelArgs &p, const View 
             for (int k = 0; k < VG; ++k) in.q[v][k] = ic ? (Real)qa[v * G + k] + icv[k] : (Real)qa[v * G + k];
         }
     } else if (iso) {
-        const Real *ic = iso + (size_t)c * rowG + g;
+        const Real *ic = iso + (uint64_t)c * rowG + g;
 #pragma unroll
         for (int v = 0; v < 4; ++v) gv_load<Real, VG, false>(ic + v * G, in.q[v]);
     } else {
@@ -295,14 +295,14 @@ template <typename Real, int VG, bool L2_ONLY, typename View>
 __device__ __forceinline__ void pair_load_upwind(const LevelArgs &p, const View &R, uint32_t g, PairIn<Real, VG> &in)
 {
     const uint32_t G = p.G;
-    const size_t rowG = (size_t)4 * G;
+    const uint32_t rowG = 4u * G;  // G <= 64: 32-bit operands, one widening multiply per address
     const Real *__restrict__ psi = reinterpret_cast<const Real *>(p.psi);
     const uint32_t nmap = R.u(2);
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
         const uint32_t row = R.u(3 + f);
         const bool live = R.f(f) < Real(0) && row != kNoRow;
-        const Real *nrow = psi + (size_t)(live ? row : 0u) * rowG + g;
+        const Real *nrow = psi + (uint64_t)(live ? row : 0u) * rowG + g;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const int j = k < f ? k : k + 1;
@@ -416,7 +416,7 @@ __device__ __forceinline__ void pair_solve_store_v(const LevelArgs &p, const Vie
 #pragma unroll
         for (int v = 0; v < 4; ++v) res[v][e] = b[v];
     }
-    Real *__restrict__ out = reinterpret_cast<Real *>(p.psi) + (size_t)R.u(1) * 4 * p.G + g;
+    Real *__restrict__ out = reinterpret_cast<Real *>(p.psi) + (uint64_t)R.u(1) * (4u * p.G) + g;
 #pragma unroll
     for (int v = 0; v < 4; ++v) gv_store(out + v * p.G, res[v]);
 }
@@ -480,7 +480,7 @@ __device__ __forceinline__ void pair_solve_store_f32x2(const LevelArgs &p, const
             res[v][e + 1] = b[v].y;
         }
     }
-    float *__restrict__ out = reinterpret_cast<float *>(p.psi) + (size_t)R.u(1) * 4 * p.G + g;
+    float *__restrict__ out = reinterpret_cast<float *>(p.psi) + (uint64_t)R.u(1) * (4u * p.G) + g;
 #pragma unroll
     for (int v = 0; v < 4; ++v) gv_store(out + v * p.G, res[v]);
 }
