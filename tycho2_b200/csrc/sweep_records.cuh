@@ -426,7 +426,31 @@ __device__ __forceinline__ void pair_solve_store_v(const LevelArgs &p, const Vie
 // the arithmetic instructions).  The source sum is reassociated as
 // vs20 * ((q0 + q1) + (q2 + q3) + q_v); FP32 results are checked by
 // tolerance, the FP64 path above keeps the reference's order.
+// The volume source term of the right-hand side, V/20 (sum_j q_j + q_v), in
+// place of the sources (packed FP32x2): it does not depend on the previous
+// level, so the direct kernel forms it before waiting for that level.
 template <int VG, typename View>
+__device__ __forceinline__ void pair_source_rhs_f32x2(const View &R, PairIn<float, VG> &in)
+{
+    const float vs = R.f(4);
+    const float2 vs2 = make_float2(vs, vs);
+#pragma unroll
+    for (int e = 0; e < VG; e += 2) {
+        float2 q[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) q[v] = make_float2(in.q[v][e], in.q[v][e + 1]);
+        const float2 s = __fadd2_rn(__fadd2_rn(q[0], q[1]), __fadd2_rn(q[2], q[3]));
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const float2 b = __fmul2_rn(vs2, __fadd2_rn(s, q[v]));
+            in.q[v][e] = b.x;
+            in.q[v][e + 1] = b.y;
+        }
+    }
+}
+
+// PRE: in.q already holds the volume source term (pair_source_rhs_f32x2).
+template <int VG, typename View, bool PRE = false>
 __device__ __forceinline__ void pair_solve_store_f32x2(const LevelArgs &p, const View &R, uint32_t g,
                                                        const PairIn<float, VG> &in)
 {
@@ -439,10 +463,15 @@ __device__ __forceinline__ void pair_solve_store_f32x2(const LevelArgs &p, const
         float2 q[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) q[v] = make_float2(in.q[v][e], in.q[v][e + 1]);
-        const float2 s = __fadd2_rn(__fadd2_rn(q[0], q[1]), __fadd2_rn(q[2], q[3]));
         float2 b[4];
+        if constexpr (PRE) {
 #pragma unroll
-        for (int v = 0; v < 4; ++v) b[v] = __fmul2_rn(vs2, __fadd2_rn(s, q[v]));
+            for (int v = 0; v < 4; ++v) b[v] = q[v];
+        } else {
+            const float2 s = __fadd2_rn(__fadd2_rn(q[0], q[1]), __fadd2_rn(q[2], q[3]));
+#pragma unroll
+            for (int v = 0; v < 4; ++v) b[v] = __fmul2_rn(vs2, __fadd2_rn(s, q[v]));
+        }
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
             const float t1 = R.f(f);
@@ -470,7 +499,7 @@ __device__ __forceinline__ void pair_solve_store_f32x2(const LevelArgs &p, const
         b[3] = __ffma2_rn(sp(-R.f(16)), b[1], b[3]);
         b[2] = __fmul2_rn(b[2], sp(R.f(17)));
         b[3] = __ffma2_rn(sp(-R.f(19)), b[2], b[3]);
-        b[3] = __fmul2_rn(b[3], sp(__frcp_rn(R.f(20))));
+        b[3] = __fmul2_rn(b[3], sp(__fdividef(1.0f, R.f(20))));
         b[2] = __ffma2_rn(sp(-R.f(18)), b[3], b[2]);
         b[1] = __ffma2_rn(sp(-R.f(13)), b[2], __ffma2_rn(sp(-R.f(14)), b[3], b[1]));
         b[0] = __ffma2_rn(sp(-R.f(6)), b[1], __ffma2_rn(sp(-R.f(7)), b[2], __ffma2_rn(sp(-R.f(8)), b[3], b[0])));
@@ -494,6 +523,11 @@ __device__ __forceinline__ void pair_solve_store_any(const LevelArgs &p, const V
     if constexpr (std::is_same<Real, float>::value && VG % 2 == 0 && !ANY) pair_solve_store_f32x2<VG>(p, R, g, in);
     else pair_solve_store_v<Real, VG, View, ANY>(p, R, g, in);
 }
+
+// Whether a task's arithmetic runs packed FP32x2 (and can form its volume
+// source term before the wait).
+template <typename Real, int VG, bool ANY>
+constexpr bool kPairedF32 = std::is_same<Real, float>::value && VG % 2 == 0 && !ANY;
 
 template <typename Real, int IPW, int VG>
 __device__ __forceinline__ void pair_solve_store(const LevelArgs &p, const RecordTile<Real, IPW> &T, uint32_t i,
@@ -587,11 +621,15 @@ sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const 
         load_record(rec + it, R, ANY ? p.solver : (uint32_t)kSolveNoPivot);
         live = R.u(0) != kSentinel;
     }
-    if (live) pair_load_source<Real, VG>(p, R, g, in);
+    if (live) {
+        pair_load_source<Real, VG>(p, R, g, in);
+        if constexpr (kPairedF32<Real, VG, ANY>) pair_source_rhs_f32x2<VG>(R, in);
+    }
     pdl_wait_prerequisites();
     if (!live) return;
     pair_load_upwind<Real, VG, false>(p, R, g, in);
-    pair_solve_store_any<Real, VG, RegRecord<Real>, ANY>(p, R, g, in);
+    if constexpr (kPairedF32<Real, VG, ANY>) pair_solve_store_f32x2<VG, RegRecord<Real>, true>(p, R, g, in);
+    else pair_solve_store_any<Real, VG, RegRecord<Real>, ANY>(p, R, g, in);
 }
 
 // Direct variant, two group vectors per task: the task covers 2*VG groups
