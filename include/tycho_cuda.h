@@ -264,11 +264,11 @@ int tycho_sweeper_configure(tycho_sweeper *sw, int precision, const tycho_launch
 int tycho_sweeper_get_shape(const tycho_sweeper *sw, int precision, tycho_launch_shape *shape);
 
 /* A sweep that allocates nothing.  No counterpart in the reference.
-   For callers that cannot allocate device memory when they sweep: code under
-   CUDA stream capture (cudaMalloc is refused during a global-mode capture), a
-   host framework that owns all device memory through its own pool and
-   budget, or a time-critical loop that cannot afford cudaMalloc's implicit
-   synchronization.  psi = L^{-1} iso for an isotropic source on the caller's
+   For callers that cannot allocate device memory when they sweep: a host
+   framework that owns all device memory through its own pool and budget (an
+   allocation behind its back breaks its accounting), a plugin that may only
+   use the buffers its host hands it, or a time-critical loop that cannot
+   afford cudaMalloc's implicit synchronization.  psi = L^{-1} iso for an isotropic source on the caller's
    own device buffers, in the sweep precision (0: double, 1: float):
      iso  phi layout (cell*4 + vertex)*G + group, may be NULL (zero source);
      psi  psi layout, written.

@@ -1,8 +1,8 @@
 """tycho_sweeper_sweep_noalloc: the sweep for callers that cannot allocate
-device memory when they sweep (code under stream capture, hosts that own all
-device memory through their own pool, time-critical loops).  The caller owns
-the source and psi buffers; the sweep's scratch is a fixed file-scope device
-array.  Checked through the C ABI against the existing entry point
+device memory when they sweep (hosts that own all device memory through their
+own pool and budget, plugins limited to the buffers they are given,
+time-critical loops).  The caller owns the source and psi buffers; the
+sweep's scratch is a fixed file-scope device array.  Checked through the C ABI against the existing entry point
 (tycho_sweeper_sweep) on two calls in a row: FP64 bit for bit, FP32 within
 the FP32 tolerance used elsewhere (relative L1 <= 1e-5 of the FP64 psi)."""
 import ctypes as C

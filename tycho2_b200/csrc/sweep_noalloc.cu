@@ -1,15 +1,14 @@
 // The sweep entry point that allocates nothing (tycho_sweeper_sweep_noalloc).
 //
 // Some callers cannot allocate device memory at the moment they need a sweep:
-// code running under CUDA stream capture (cudaMalloc is not allowed while a
-// stream is being captured in global mode), a host framework that owns all
-// device memory through its own pool and budget (a serving loop admitting
-// work by its HBM footprint cannot tolerate hidden allocations), or a
-// time-critical loop where cudaMalloc's implicit synchronization would stall
-// every stream.  For them the persistent dataflow sweep runs on the caller's
-// own source and psi buffers, and its scratch -- the per-item completion
-// flags and the control words -- lives in one file-scope device array of
-// fixed size instead of memory the sweeper allocates.
+// a host framework that owns all device memory through its own pool and
+// budget (a serving loop admitting work by its HBM footprint cannot tolerate
+// hidden allocations), a plugin that may only use the buffers its host hands
+// it, or a time-critical loop where cudaMalloc's implicit synchronization
+// would stall every stream.  For them the persistent dataflow sweep runs on
+// the caller's own source and psi buffers, and its scratch -- the per-item
+// completion flags and the control words -- lives in one file-scope device
+// array of fixed size instead of memory the sweeper allocates.
 //
 // Limits and sharing, as documented in include/tycho_cuda.h:
 //   * at most kNoAllocMaxItems (cells x angles) items; larger problems are
