@@ -168,7 +168,9 @@ int tycho_sweeper_set_source(tycho_sweeper *sw, int kind, const double *q);
 
 /* The drop-in SweeperAbstract::sweep(psi, source): psi = L^{-1} source for
    an angular source in psi layout, vacuum boundaries.  Host buffers; the
-   copies in and out are part of the call. */
+   copies in and out are part of the call.  From 64 MiB of psi (NoPivot), the
+   copies and the sweep run in angle chunks on three streams so that uploads,
+   downloads and the sweep overlap; page-locked (pinned) buffers let them. */
 int tycho_sweeper_sweep(tycho_sweeper *sw, const double *source, double *psi);
 
 typedef struct tycho_solve_opts {

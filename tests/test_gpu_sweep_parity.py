@@ -413,3 +413,32 @@ def test_pool_memory_reused_and_released(built, workdir):
         if trim:
             ty.release_cached_memory(0)
     assert bits_equal(psis[0], psis[1]) and bits_equal(psis[0], psis[2])
+
+
+@pytest.mark.parametrize("n,G,chunks", [(8, 8, 4), (12, 3, 4), (16, 16, 16)])
+def test_dropin_sweep_in_angle_chunks_bit_exact(built, workdir, n, G, chunks):
+    """The drop-in sweep of a large psi (64 MiB and up) moves and sweeps K
+    contiguous angle ranges so that its host copies overlap the sweep: psi
+    bit-identical to the oracle's, on two calls in a row and after a solve
+    on the same sweeper."""
+    from oracle.oracle import Oracle
+    mesh, om = kuhn(workdir, n, 0.05, seed=23)
+    o = Oracle(om, 8, G)
+    rng = np.random.default_rng(n * G)
+    st = rng.lognormal(0.0, 0.5, mesh.n_cells)
+    sw = make(mesh, 8, G)
+    assert mesh.n_cells * 128 * 4 * G * 8 >= (64 << 20) * (16 if chunks == 16 else 1)
+    sw.set_cross_sections(st, np.zeros(mesh.n_cells))
+    src = rng.uniform(-0.2, 1.0, o.psi_shape)
+    ref = o.sweep(st, src_ang=src)
+    psi = np.empty(sw.psi_shape)
+    for _ in range(2):
+        psi[...] = np.nan
+        sw.sweep(psi, src)
+        assert bits_equal(psi, ref)
+    sw.set_source(np.ones(sw.phi_shape), "isotropic")
+    sw.solve("si", iter_max=2, err_max=-1.0, want_psi=False)
+    psi[...] = np.nan
+    sw.sweep(psi, src)
+    assert bits_equal(psi, ref)
+    sw.close()

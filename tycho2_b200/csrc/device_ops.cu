@@ -25,6 +25,8 @@ template cudaError_t record_dataflow_blocks_per_sm<double>(int, int, int *);
 template cudaError_t launch_persist_record<double>(int, const LevelArgs &, const void *, const uint64_t *, uint32_t,
                                                    unsigned long long *, const DataflowArgs &, unsigned, cudaStream_t);
 template cudaError_t record_persist_blocks_per_sm<double>(int, int, int *);
+template cudaError_t launch_direct_subset<double>(const LevelArgs &, const void *, const uint32_t *, uint64_t, uint64_t,
+                                                   cudaStream_t);
 template cudaError_t launch_direct_level<double>(int, const LevelArgs &, const void *, uint64_t, uint64_t, cudaStream_t,
                                                   bool);
 template cudaError_t launch_compact_records<double>(const LevelArgs &, uint64_t, void *, cudaStream_t);

@@ -96,6 +96,11 @@ cudaError_t launch_direct_dataflow(const LevelArgs &p, const void *rec, bool com
                                    unsigned grid, cudaStream_t s);
 template <typename Real>
 cudaError_t direct_dataflow_blocks_per_sm(int vg, bool compact, int *blocks);
+// Direct kernel (compact records, NoPivot, p.vg 1 or 2) over the schedule
+// positions pos[begin, end).
+template <typename Real>
+cudaError_t launch_direct_subset(const LevelArgs &p, const void *rec, const uint32_t *pos, uint64_t begin,
+                                 uint64_t end, cudaStream_t s);
 // Compact records (64 B per item for float, 96 B for double): the inputs of
 // each item's matrix, from which the direct kernels rebuild its factors.
 constexpr size_t compact_record_bytes(bool fp32) { return fp32 ? 64 : 96; }

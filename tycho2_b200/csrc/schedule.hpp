@@ -71,6 +71,14 @@ int build_schedule(const MeshTables &t, const Quadrature &q, Schedule &s, std::s
 // tlevel_from_items derives s.tlevel once s.items has been copied back.
 int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s, uint32_t **d_items,
                           cudaStream_t st, std::string &err);
+// The schedule's positions grouped by angle chunk, then level (stable in
+// schedule order), on the device: chunk j holds the angles [j*A/K,
+// (j+1)*A/K).  *d_pos receives the positions (from the device pool, owned by
+// the caller); positions off[j*n_levels + l] .. off[j*n_levels + l + 1] are
+// chunk j's items of level l.  Padding items are left out.
+int angle_chunks_device(const uint32_t *d_items, uint64_t n_padded, const uint64_t *d_level_off, uint32_t n_levels,
+                        uint32_t A, uint32_t K, uint32_t **d_pos, std::vector<uint64_t> &off, cudaStream_t st,
+                        std::string &err);
 // s.tlevel from s.items and s.level_offset (every item of segment l has level l).
 void tlevel_from_items(Schedule &s, uint64_t n_cells, int n_angles);
 

@@ -113,6 +113,31 @@ __global__ void level_hist_kernel(const uint32_t *__restrict__ keys, uint64_t n,
     if (j < n) atomicAdd(&hist[keys[j]], 1ull);
 }
 
+// Key of schedule position i for the angle-chunked sweep: chunk(angle) *
+// n_levels + level(i), or the trailing bucket K * n_levels for padding.  The
+// level of position i is found by bisection of the level offsets.
+__global__ void chunk_keys_kernel(const uint32_t *__restrict__ items, uint64_t n_padded,
+                                  const uint64_t *__restrict__ level_off, uint32_t n_levels, uint32_t A,
+                                  uint32_t K, uint32_t *__restrict__ keys, uint32_t *__restrict__ vals)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_padded) return;
+    const uint32_t ca = items[i];
+    uint32_t key = K * n_levels;
+    if (ca != 0xFFFFFFFFu) {
+        uint32_t lo = 0, hi = n_levels;  // level_off[lo] <= i < level_off[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (level_off[mid] <= i) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t a = ca % A;
+        key = (uint32_t)(((uint64_t)a * K) / A) * n_levels + lo;
+    }
+    keys[i] = key;
+    vals[i] = (uint32_t)i;
+}
+
 unsigned blocks_for(uint64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
 // A temporary from the stream-ordered pool, returned on scope exit.
@@ -293,6 +318,50 @@ int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s,
     TS_CUDA(cudaMemcpyAsync(s.items.data(), d_items.p, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, st));
     TS_CUDA(cudaMemcpyAsync(s.tlevel.data(), d_tlevel.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st));
     TS_CUDA(cudaStreamSynchronize(st));
+    return kOk;
+}
+
+int angle_chunks_device(const uint32_t *d_items, uint64_t n_padded, const uint64_t *d_level_off, uint32_t n_levels,
+                        uint32_t A, uint32_t K, uint32_t **d_pos_out, std::vector<uint64_t> &off, cudaStream_t st,
+                        std::string &err)
+{
+    *d_pos_out = nullptr;
+    const uint64_t nseg = (uint64_t)K * n_levels;
+    off.assign(nseg + 1, 0);
+    if (n_padded == 0 || K == 0 || K > A) {
+        err = "angle chunks: empty schedule or more chunks than angles";
+        return kErrArg;
+    }
+    DevBuf d_keys[2], d_vals[2], d_temp, d_hist;
+    for (int k = 0; k < 2; ++k) {
+        TS_CUDA(take(d_keys[k], sizeof(uint32_t) * n_padded, st));
+        TS_CUDA(take(d_vals[k], sizeof(uint32_t) * n_padded, st));
+    }
+    chunk_keys_kernel<<<blocks_for(n_padded), kThreads, 0, st>>>(d_items, n_padded, d_level_off, n_levels, A, K,
+                                                                (uint32_t *)d_keys[0].p, (uint32_t *)d_vals[0].p);
+    TS_CUDA(cudaGetLastError());
+    int end_bit = 1;
+    while (end_bit < 32 && (1ull << end_bit) <= nseg) ++end_bit;
+    cub::DoubleBuffer<uint32_t> kb((uint32_t *)d_keys[0].p, (uint32_t *)d_keys[1].p);
+    cub::DoubleBuffer<uint32_t> vb((uint32_t *)d_vals[0].p, (uint32_t *)d_vals[1].p);
+    size_t temp = 0;
+    TS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, kb, vb, (int64_t)n_padded, 0, end_bit, st));
+    TS_CUDA(take(d_temp, temp, st));
+    TS_CUDA(cub::DeviceRadixSort::SortPairs(d_temp.p, temp, kb, vb, (int64_t)n_padded, 0, end_bit, st));
+    TS_CUDA(take(d_hist, sizeof(unsigned long long) * (nseg + 1), st));
+    TS_CUDA(cudaMemsetAsync(d_hist.p, 0, sizeof(unsigned long long) * (nseg + 1), st));
+    level_hist_kernel<<<blocks_for(n_padded), kThreads, 0, st>>>(kb.Current(), n_padded,
+                                                                 (unsigned long long *)d_hist.p);
+    TS_CUDA(cudaGetLastError());
+    std::vector<unsigned long long> hist(nseg + 1);
+    TS_CUDA(cudaMemcpyAsync(hist.data(), d_hist.p, sizeof(unsigned long long) * (nseg + 1), cudaMemcpyDeviceToHost,
+                            st));
+    TS_CUDA(cudaStreamSynchronize(st));
+    for (uint64_t k = 0; k < nseg; ++k) off[k + 1] = off[k] + hist[k];
+    // the sorted positions (the padding bucket sorts last and is not used)
+    DevBuf &cur = vb.Current() == (uint32_t *)d_vals[0].p ? d_vals[0] : d_vals[1];
+    *d_pos_out = (uint32_t *)cur.p;
+    cur.p = nullptr;
     return kOk;
 }
 

@@ -1010,6 +1010,62 @@ cudaError_t launch_direct_level(int knob, const LevelArgs &p, const void *rec, u
     return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
+// The direct kernel over a list of schedule positions instead of a
+// contiguous range: the items of one level that belong to a chunk of angles,
+// for the drop-in sweep that overlaps its host copies with the sweep chunk by
+// chunk.  Compact records, NoPivot, 64 threads with at most 102 registers;
+// the same per-item arithmetic as the level kernels.
+template <typename Real, int VG>
+__global__ void __launch_bounds__(64, 10)
+sweep_direct_subset_kernel(const LevelArgs p, const CompactRecord<Real> *__restrict__ rec,
+                           const uint32_t *__restrict__ pos, const uint64_t begin, const uint64_t end)
+{
+    pdl_launch_dependents();
+    const uint32_t gpv = p.G / VG;
+    const uint32_t t = blockIdx.x * 64u + threadIdx.x;
+    const uint32_t itl = gpv == 1u ? t : __umulhi(t, p.vmagic);
+    const uint32_t g = (t - itl * gpv) * VG;
+    const uint64_t k = begin + itl;
+    bool live = k < end;
+    RegRecord<Real> R;
+    PairIn<Real, VG> in;
+    if (live) {
+        load_record(rec + pos[k], R, (uint32_t)kSolveNoPivot);
+        live = R.u(0) != kSentinel;
+    }
+    if (live) pair_load_source<Real, VG>(p, R, g, in);
+    pdl_wait_prerequisites();
+    if (!live) return;
+    pair_load_upwind<Real, VG, false>(p, R, g, in);
+    pair_solve_store_any<Real, VG>(p, R, g, in);
+}
+
+// Positions pos[begin, end) of compact records `rec` (p.vg 1 or 2).
+template <typename Real>
+cudaError_t launch_direct_subset(const LevelArgs &p, const void *rec, const uint32_t *pos, uint64_t begin,
+                                 uint64_t end, cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    if (p.solver != kSolveNoPivot) return cudaErrorInvalidValue;
+    const uint64_t tasks = (end - begin) * (p.G / p.vg);
+    if (tasks >= (1ull << 26)) return cudaErrorInvalidValue;
+    const void *fn = p.vg == 1   ? (const void *)sweep_direct_subset_kernel<Real, 1>
+                     : p.vg == 2 ? (const void *)sweep_direct_subset_kernel<Real, 2>
+                                 : nullptr;
+    if (!fn) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((tasks + 63) / 64));
+    cfg.blockDim = dim3(64);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void *args[] = {(void *)&p, (void *)&rec, (void *)&pos, (void *)&begin, (void *)&end};
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
 template <typename Real, typename Rec>
 static const void *direct_dataflow_fn(int vg)
 {

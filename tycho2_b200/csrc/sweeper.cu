@@ -58,6 +58,17 @@ Sweeper::~Sweeper()
     TraceScope trace("sweeper.destroy");
     if (device_ >= 0) cudaSetDevice(device_);
     for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+    for (auto &g : chunk_graphs_)
+        if (g) cudaGraphExecDestroy(g);
+    dev_free(d_chunk_pos_, stream_);
+    for (cudaEvent_t ev : {ev_start_})
+        if (ev) cudaEventDestroy(ev);
+    for (int j = 0; j < kMaxHostChunks; ++j) {
+        if (ev_h2d_[j]) cudaEventDestroy(ev_h2d_[j]);
+        if (ev_swept_[j]) cudaEventDestroy(ev_swept_[j]);
+    }
+    if (h2d_stream_) cudaStreamDestroy(h2d_stream_);
+    if (d2h_stream_) cudaStreamDestroy(d2h_stream_);
     void *bufs[] = {d_items_, d_abar64_, d_abar32_, d_adj_, d_nbrmap_, d_cellk64_, d_cellk32_,
                     d_w_, d_sigs_, d_scat_, d_qiso_, d_qang_, d_src_, d_iso_, d_iso32_, d_psi_,
                     d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_, d_done_, d_ctl_, d_rec_[0], d_rec_[1],
@@ -685,12 +696,100 @@ int Sweeper::apply(int prec, const double *phi_in, bool with_fixed, double *phi_
     return kOk;
 }
 
+// Chunks of the drop-in sweep: large psi (copies of ~0.1 s and more over
+// PCIe) is moved and swept in K contiguous angle ranges, so that uploading
+// chunk j+1 and downloading chunk j-1 overlap the sweep of chunk j and each
+// other; small problems keep one copy each way (a chunk's level launches
+// would cost more than the overlap saves).
+int Sweeper::host_chunks() const
+{
+    if (solver_ != kSolveNoPivot || !have_xs_) return 1;
+    const uint64_t bytes = psi_size() * sizeof(double);
+    const int K = bytes >= (1ull << 30) ? kMaxHostChunks : bytes >= (64ull << 20) ? 4 : 1;
+    return std::min(K, A_);
+}
+
+// Each angle is swept independently (the upwind values of an item come from
+// the same angle), so chunk j's sweep needs only chunk j's source and
+// writes only chunk j's psi.  Chunk j's angles are contiguous in every
+// cell's row of the reference layout: one strided (2D) copy per chunk and
+// direction.  Chunk j sweeps its items level by level in schedule order
+// (the same per-item arithmetic and results as the whole sweep).
+int Sweeper::sweep_host_chunked(const double *source, double *psi, int K, std::string &err)
+{
+    TY_CHECK(ensure_records(0, true, err, true));
+    if (chunk_k_ != K) {
+        for (auto &g : chunk_graphs_)
+            if (g) cudaGraphExecDestroy(g);
+        chunk_graphs_.clear();
+        dev_free(d_chunk_pos_, stream_);
+        d_chunk_pos_ = nullptr;
+        chunk_k_ = 0;
+        TY_CHECK(angle_chunks_device(d_items_, sched_.n_padded, d_level_off_, sched_.n_levels, (uint32_t)A_,
+                                     (uint32_t)K, &d_chunk_pos_, chunk_off_, stream_, err));
+        chunk_graphs_.assign(K, nullptr);
+        chunk_k_ = K;
+    }
+    if (!h2d_stream_) TY_CUDA(cudaStreamCreateWithFlags(&h2d_stream_, cudaStreamNonBlocking));
+    if (!d2h_stream_) TY_CUDA(cudaStreamCreateWithFlags(&d2h_stream_, cudaStreamNonBlocking));
+    if (!ev_start_) TY_CUDA(cudaEventCreateWithFlags(&ev_start_, cudaEventDisableTiming));
+    for (int j = 0; j < K; ++j) {
+        if (!ev_h2d_[j]) TY_CUDA(cudaEventCreateWithFlags(&ev_h2d_[j], cudaEventDisableTiming));
+        if (!ev_swept_[j]) TY_CUDA(cudaEventCreateWithFlags(&ev_swept_[j], cudaEventDisableTiming));
+    }
+    const uint32_t n_levels = sched_.n_levels;
+    for (int j = 0; j < K; ++j) {
+        if (chunk_graphs_[j]) continue;
+        LevelArgs p = level_args(0, nullptr, d_src_, d_psi_);
+        p.vg = G_ % 2 == 0 ? 2u : 1u;
+        p.vmagic = group_magic((uint32_t)G_ / p.vg);
+        cudaGraph_t graph;
+        TY_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        cudaError_t le = cudaSuccess;
+        for (uint32_t l = 0; l < n_levels && le == cudaSuccess; ++l)
+            le = launch_direct_subset<double>(p, d_crec_[0], d_chunk_pos_, chunk_off_[(size_t)j * n_levels + l],
+                                              chunk_off_[(size_t)j * n_levels + l + 1], stream_);
+        cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
+        TY_CUDA(le);
+        TY_CUDA(ce);
+        cudaError_t ie = cudaGraphInstantiate(&chunk_graphs_[j], graph, 0);
+        cudaGraphDestroy(graph);
+        TY_CUDA(ie);
+    }
+    // after whatever ran on the sweeper's stream before
+    TY_CUDA(cudaEventRecord(ev_start_, stream_));
+    TY_CUDA(cudaStreamWaitEvent(h2d_stream_, ev_start_, 0));
+    TY_CUDA(cudaStreamWaitEvent(d2h_stream_, ev_start_, 0));
+    const size_t per_angle = (size_t)4 * G_ * sizeof(double), row = per_angle * A_;
+    for (int j = 0; j < K; ++j) {
+        const size_t a0 = (size_t)j * A_ / K, a1 = (size_t)(j + 1) * A_ / K;
+        const size_t off = a0 * per_angle, width = (a1 - a0) * per_angle;
+        TY_CUDA(cudaMemcpy2DAsync(reinterpret_cast<char *>(d_src_) + off, row,
+                                  reinterpret_cast<const char *>(source) + off, row, width, nc_,
+                                  cudaMemcpyHostToDevice, h2d_stream_));
+        TY_CUDA(cudaEventRecord(ev_h2d_[j], h2d_stream_));
+        TY_CUDA(cudaStreamWaitEvent(stream_, ev_h2d_[j], 0));
+        TY_CUDA(cudaGraphLaunch(chunk_graphs_[j], stream_));
+        TY_CUDA(cudaEventRecord(ev_swept_[j], stream_));
+        TY_CUDA(cudaStreamWaitEvent(d2h_stream_, ev_swept_[j], 0));
+        TY_CUDA(cudaMemcpy2DAsync(reinterpret_cast<char *>(psi) + off, row,
+                                  reinterpret_cast<const char *>(d_psi_) + off, row, width, nc_,
+                                  cudaMemcpyDeviceToHost, d2h_stream_));
+    }
+    TY_CUDA(cudaStreamSynchronize(d2h_stream_));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    last_psi_prec_ = 0;
+    return check_device_error(err);
+}
+
 int Sweeper::sweep_host(const double *source, double *psi, std::string &err)
 {
     if (!source || !psi) { err = "source and psi are required"; return kErrArg; }
     TY_CUDA(cudaSetDevice(device_));
     const size_t n = psi_size();
     if (!d_src_) TY_CUDA(dev_malloc(&d_src_, sizeof(double) * n, stream_));
+    const int K = host_chunks();
+    if (K > 1) return sweep_host_chunked(source, psi, K, err);
     TY_CUDA(cudaMemcpyAsync(d_src_, source, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
     TY_CHECK(apply(0, nullptr, false, nullptr, d_src_, err));
     TY_CUDA(cudaMemcpyAsync(psi, d_psi_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));

@@ -143,6 +143,10 @@ private:
     int gmres(int prec, const double *b, double *x, int restart, double rtol, int iter_max,
               int &its, double &rnorm, SolveStats &st, std::string &err);
     int ensure_krylov(int restart, std::string &err);
+    // The drop-in sweep with its host copies overlapped: angle chunks (0 or 1:
+    // one copy in, one sweep, one copy out) and the pipelined form.
+    int host_chunks() const;
+    int sweep_host_chunked(const double *source, double *psi, int K, std::string &err);
     // Allocates the record array of one precision; need_filled also requires
     // (and computes, when stale) its contents for the current cross sections.
     int ensure_records(int prec, bool need_filled, std::string &err, bool compact = false);
@@ -198,6 +202,15 @@ private:
     size_t flags_cap_ = 0;
     // persistent-levels schedule: level offsets and the grid barrier counter
     uint64_t *d_level_off_ = nullptr;
+    // drop-in sweep in angle chunks: schedule positions grouped by chunk then
+    // level, one level graph per chunk, copy streams and their events
+    int chunk_k_ = 0;
+    uint32_t *d_chunk_pos_ = nullptr;
+    std::vector<uint64_t> chunk_off_;
+    std::vector<cudaGraphExec_t> chunk_graphs_;
+    cudaStream_t h2d_stream_ = nullptr, d2h_stream_ = nullptr;
+    static constexpr int kMaxHostChunks = 16;
+    cudaEvent_t ev_start_ = nullptr, ev_h2d_[kMaxHostChunks] = {}, ev_swept_[kMaxHostChunks] = {};
     unsigned long long *d_barrier_ = nullptr;
 };
 
