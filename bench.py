@@ -513,7 +513,7 @@ def run_b200(args):
         grp.barrier()
         dt = grp.max((time.perf_counter() - t0) / n_e2e)
         e2e = {"value": grp.sum(updates) / dt, "unit": "updates/s", "h2d_bytes_per_step": npsi * 8,
-               "d2h_bytes_per_step": npsi * 8, "path": "tycho_sweeper_sweep (FP64, host buffers)",
+               "d2h_bytes_per_step": npsi * 8, "path": "tycho_sweeper_sweep (FP64, page-locked host buffers)",
                "seconds_per_step": dt}
         del src_t, psi_t
 

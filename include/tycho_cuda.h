@@ -168,9 +168,10 @@ int tycho_sweeper_set_source(tycho_sweeper *sw, int kind, const double *q);
 
 /* The drop-in SweeperAbstract::sweep(psi, source): psi = L^{-1} source for
    an angular source in psi layout, vacuum boundaries.  Host buffers; the
-   copies in and out are part of the call.  From 64 MiB of psi (NoPivot), the
-   copies and the sweep run in angle chunks on three streams so that uploads,
-   downloads and the sweep overlap; page-locked (pinned) buffers let them. */
+   copies in and out are part of the call.  With page-locked (pinned or
+   registered) buffers and from 64 MiB of psi (NoPivot), the copies and the
+   sweep run in angle chunks on three streams so that uploads, downloads and
+   the sweep overlap. */
 int tycho_sweeper_sweep(tycho_sweeper *sw, const double *source, double *psi);
 
 typedef struct tycho_solve_opts {

@@ -782,13 +782,31 @@ int Sweeper::sweep_host_chunked(const double *source, double *psi, int K, std::s
     return check_device_error(err);
 }
 
+namespace {
+
+// Page-locked (or registered) host memory: copies from and to it run
+// asynchronously, so chunks in the two directions can overlap.  From
+// pageable memory each copy is staged by the calling thread, and chunking
+// would only add launches.
+bool page_locked(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
 int Sweeper::sweep_host(const double *source, double *psi, std::string &err)
 {
     if (!source || !psi) { err = "source and psi are required"; return kErrArg; }
     TY_CUDA(cudaSetDevice(device_));
     const size_t n = psi_size();
     if (!d_src_) TY_CUDA(dev_malloc(&d_src_, sizeof(double) * n, stream_));
-    const int K = host_chunks();
+    const int K = page_locked(source) && page_locked(psi) ? host_chunks() : 1;
     if (K > 1) return sweep_host_chunked(source, psi, K, err);
     TY_CUDA(cudaMemcpyAsync(d_src_, source, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
     TY_CHECK(apply(0, nullptr, false, nullptr, d_src_, err));
