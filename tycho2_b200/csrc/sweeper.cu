@@ -717,7 +717,7 @@ int Sweeper::host_chunks() const
 // (the same per-item arithmetic and results as the whole sweep).
 int Sweeper::sweep_host_chunked(const double *source, double *psi, int K, std::string &err)
 {
-    TY_CHECK(ensure_records(0, true, err, true));
+    TY_CHECK(ensure_records(0, true, err, true));  // kErrOom before any copy
     if (chunk_k_ != K) {
         for (auto &g : chunk_graphs_)
             if (g) cudaGraphExecDestroy(g);
@@ -807,7 +807,13 @@ int Sweeper::sweep_host(const double *source, double *psi, std::string &err)
     const size_t n = psi_size();
     if (!d_src_) TY_CUDA(dev_malloc(&d_src_, sizeof(double) * n, stream_));
     const int K = page_locked(source) && page_locked(psi) ? host_chunks() : 1;
-    if (K > 1) return sweep_host_chunked(source, psi, K, err);
+    if (K > 1) {
+        // no room for the chunk plan or the compact FP64 records: one copy
+        // each way instead (nothing was copied yet)
+        const int st = sweep_host_chunked(source, psi, K, err);
+        if (st != kErrOom) return st;
+        err.clear();
+    }
     TY_CUDA(cudaMemcpyAsync(d_src_, source, sizeof(double) * n, cudaMemcpyHostToDevice, stream_));
     TY_CHECK(apply(0, nullptr, false, nullptr, d_src_, err));
     TY_CUDA(cudaMemcpyAsync(psi, d_psi_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
