@@ -14,12 +14,31 @@
 #include "devmem.hpp"
 #include "schedule.hpp"
 #include "status.hpp"
+#include "trace.hpp"
 
 namespace tycho {
 
 namespace {
 
 constexpr int kThreads = 256;
+constexpr uint32_t kMaxLevels = 1u << 16;    // frontier counters kept on the device
+constexpr uint32_t kLevelBatch = 32;         // level steps launched between host checks
+constexpr unsigned kStepGrid = 148 * 8;      // blocks of the grid-stride level step
+
+// Appends v where pred holds to buf, with one atomic per warp for the slots
+// (lanes active at the call take part; pred false appends nothing).
+__device__ __forceinline__ void warp_append(bool pred, uint32_t v, uint32_t *buf, uint32_t *count)
+{
+    const unsigned active = __activemask();
+    const unsigned ballot = __ballot_sync(active, pred);
+    if (!ballot) return;
+    const int leader = __ffs(ballot) - 1;
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(count, (uint32_t)__popc(ballot));
+    base = __shfl_sync(active, base, leader);
+    if (pred) buf[base + __popc(ballot & ((1u << lane) - 1u))] = v;
+}
 
 // Per item (angle-major index a*nc + c): upwind mask (bits 0-3), downwind
 // mask (bits 4-7), count of upwind interior faces; level-0 items seed the
@@ -32,7 +51,7 @@ __global__ void level_init_kernel(const double *__restrict__ normal, const int4 
                                   uint32_t *__restrict__ n_frontier, unsigned long long *__restrict__ incoming)
 {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (uint64_t)A * nc) return;
+    if (i >= (uint64_t)A * nc) return;  // whole warps past the end, or a tail the intrinsics below mask out
     const uint32_t a = (uint32_t)(i / nc);
     const uint64_t c = i - (uint64_t)a * nc;
     const double xi = omega[a], eta = omega[A + a], mu = omega[2 * A + a];
@@ -52,35 +71,38 @@ __global__ void level_init_kernel(const double *__restrict__ normal, const int4 
     }
     mask[i] = (uint8_t)m;
     cnt[i] = d;
-    if (d) {
-        atomicAdd(incoming, (unsigned long long)d);
-    } else {
-        tlevel[i] = 0;
-        frontier[atomicAdd(n_frontier, 1u)] = (uint32_t)i;
-    }
+    if (!d) tlevel[i] = 0;
+    // one atomic per warp for the incoming-face total and the frontier slots
+    const unsigned active = __activemask();
+    const unsigned wsum = __reduce_add_sync(active, d);
+    if ((threadIdx.x & 31u) == (unsigned)(__ffs(active) - 1)) atomicAdd(incoming, (unsigned long long)wsum);
+    warp_append(d == 0, (uint32_t)i, frontier, n_frontier);
 }
 
 // One level: every frontier item releases its downwind neighbours; the last
-// release of a neighbour puts it on the next frontier one level higher.
-__global__ void level_step_kernel(const uint32_t *__restrict__ frontier, uint32_t n, uint32_t level,
+// release of a neighbour puts it on the next frontier one level higher.  The
+// frontier's size is read on the device (level_count[level]), so the host
+// launches many levels without waiting for each; a level past the last
+// non-empty one has nothing to do.
+__global__ void level_step_kernel(const uint32_t *__restrict__ frontier, uint32_t level,
                                   const int4 *__restrict__ adj, const uint8_t *__restrict__ mask, uint64_t nc,
                                   uint32_t *__restrict__ cnt, uint32_t *__restrict__ tlevel,
-                                  uint32_t *__restrict__ next, uint32_t *__restrict__ n_next)
+                                  uint32_t *__restrict__ next, uint32_t *__restrict__ level_count)
 {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const uint32_t i = frontier[k];
-    const uint64_t a = i / nc, c = i - a * nc;
-    const int4 nb = adj[c];
-    const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
-    const unsigned m = mask[i];
+    const uint32_t n = level_count[level];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = frontier[k];
+        const uint64_t a = i / nc, c = i - a * nc;
+        const int4 nb = adj[c];
+        const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+        const unsigned m = mask[i];
 #pragma unroll
-    for (int f = 0; f < 4; ++f) {
-        if (!(m >> (f + 4) & 1u) || nbs[f] < 0) continue;
-        const uint64_t j = a * nc + (uint64_t)nbs[f];
-        if (atomicSub(&cnt[j], 1u) == 1u) {
-            tlevel[j] = level + 1;
-            next[atomicAdd(n_next, 1u)] = (uint32_t)j;
+        for (int f = 0; f < 4; ++f) {
+            const bool down = (m >> (f + 4) & 1u) && nbs[f] >= 0;
+            const uint64_t j = a * nc + (uint64_t)(down ? nbs[f] : 0);
+            const bool ready = down && atomicSub(&cnt[j], 1u) == 1u;
+            if (ready) tlevel[j] = level + 1;
+            warp_append(ready, (uint32_t)j, next, level_count + level + 1);
         }
     }
 }
@@ -107,10 +129,19 @@ __global__ void level_scatter_kernel(const uint32_t *__restrict__ keys, const ui
     items[padded[k] + (j - unpadded[k])] = vals[j];
 }
 
-__global__ void level_hist_kernel(const uint32_t *__restrict__ keys, uint64_t n, unsigned long long *__restrict__ hist)
+// Segment starts of sorted keys: start[s] = the first j with keys[j] >= s,
+// for s in [0, nseg]; each s is written by exactly one j (no atomics: sorted
+// keys would put every lane of a warp on the same counter).
+__global__ void seg_starts_kernel(const uint32_t *__restrict__ keys, uint64_t n, uint32_t nseg,
+                                  uint64_t *__restrict__ start)
 {
     const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < n) atomicAdd(&hist[keys[j]], 1ull);
+    if (j >= n) return;
+    const uint32_t k = keys[j];
+    const uint32_t prev_end = j == 0 ? 0u : keys[j - 1] + 1u;  // s in [prev_end, k] starts at j
+    for (uint32_t s = prev_end; s <= k && s <= nseg; ++s) start[s] = j;
+    if (j == n - 1)
+        for (uint32_t s = k + 1; s <= nseg; ++s) start[s] = n;
 }
 
 // Key of schedule position i for the angle-chunked sweep: chunk(angle) *
@@ -201,6 +232,7 @@ int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s,
     }
     std::vector<double> omega(3 * (size_t)A);
     std::vector<uint8_t> oct(A);
+    TraceScope trace_prep("levelling.upload_init");
     for (uint32_t a = 0; a < A; ++a) {
         omega[a] = q.xi[a];
         omega[A + a] = q.eta[a];
@@ -217,13 +249,13 @@ int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s,
     TS_CUDA(take(d_tlevel, sizeof(uint32_t) * n, st));
     TS_CUDA(take(d_front[0], sizeof(uint32_t) * n, st));
     TS_CUDA(take(d_front[1], sizeof(uint32_t) * n, st));
-    TS_CUDA(take(d_ctr, sizeof(uint32_t) * 2, st));
+    TS_CUDA(take(d_ctr, sizeof(uint32_t) * (kMaxLevels + 1), st));  // frontier size per level
     TS_CUDA(take(d_inc, sizeof(unsigned long long), st));
     TS_CUDA(cudaMemcpyAsync(d_normal.p, t.normal.data(), sizeof(double) * t.normal.size(), cudaMemcpyHostToDevice, st));
     TS_CUDA(cudaMemcpyAsync(d_adj.p, adj.data(), sizeof(int4) * nc, cudaMemcpyHostToDevice, st));
     TS_CUDA(cudaMemcpyAsync(d_omega.p, omega.data(), sizeof(double) * omega.size(), cudaMemcpyHostToDevice, st));
     TS_CUDA(cudaMemcpyAsync(d_oct.p, oct.data(), A, cudaMemcpyHostToDevice, st));
-    TS_CUDA(cudaMemsetAsync(d_ctr.p, 0, sizeof(uint32_t) * 2, st));
+    TS_CUDA(cudaMemsetAsync(d_ctr.p, 0, sizeof(uint32_t) * (kMaxLevels + 1), st));
     TS_CUDA(cudaMemsetAsync(d_inc.p, 0, sizeof(unsigned long long), st));
     uint32_t *ctr = (uint32_t *)d_ctr.p;
     level_init_kernel<<<blocks_for(n), kThreads, 0, st>>>(
@@ -231,28 +263,42 @@ int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s,
         (uint32_t *)d_cnt.p, (uint32_t *)d_tlevel.p, (uint32_t *)d_front[0].p, ctr,
         (unsigned long long *)d_inc.p);
     TS_CUDA(cudaGetLastError());
-    uint32_t h_n = 0;
-    TS_CUDA(cudaMemcpyAsync(&h_n, ctr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    TS_CUDA(cudaStreamSynchronize(st));
+    trace_prep.next("levelling.frontiers");
+    // Levels in batches of kLevelBatch launches, each reading its frontier's
+    // size on the device; between batches the host reads the batch's sizes
+    // and stops at the first empty level.
     uint64_t done = 0;
-    uint32_t level = 0;
-    int cur = 0;
-    while (h_n > 0) {
-        done += h_n;
-        TS_CUDA(cudaMemsetAsync(ctr + 1 - cur, 0, sizeof(uint32_t), st));
-        level_step_kernel<<<blocks_for(h_n), kThreads, 0, st>>>(
-            (const uint32_t *)d_front[cur].p, h_n, level, (const int4 *)d_adj.p, (const uint8_t *)d_mask.p, nc,
-            (uint32_t *)d_cnt.p, (uint32_t *)d_tlevel.p, (uint32_t *)d_front[1 - cur].p, ctr + 1 - cur);
+    uint32_t level = 0;  // number of non-empty levels found so far
+    std::vector<uint32_t> h_cnt(kLevelBatch);
+    for (bool more = true; more;) {
+        if (level + kLevelBatch > kMaxLevels) {
+            err = "more than 65536 wavefront levels";
+            return kErrArg;
+        }
+        for (uint32_t b = 0; b < kLevelBatch; ++b) {
+            const uint32_t l = level + b;
+            level_step_kernel<<<kStepGrid, kThreads, 0, st>>>(
+                (const uint32_t *)d_front[l & 1u].p, l, (const int4 *)d_adj.p, (const uint8_t *)d_mask.p, nc,
+                (uint32_t *)d_cnt.p, (uint32_t *)d_tlevel.p, (uint32_t *)d_front[(l + 1) & 1u].p, ctr);
+        }
         TS_CUDA(cudaGetLastError());
-        TS_CUDA(cudaMemcpyAsync(&h_n, ctr + 1 - cur, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        TS_CUDA(cudaMemcpyAsync(h_cnt.data(), ctr + level, sizeof(uint32_t) * kLevelBatch, cudaMemcpyDeviceToHost,
+                                st));
         TS_CUDA(cudaStreamSynchronize(st));
-        cur = 1 - cur;
-        ++level;
+        for (uint32_t b = 0; b < kLevelBatch; ++b) {
+            if (h_cnt[b] == 0) {
+                more = false;
+                break;
+            }
+            done += h_cnt[b];
+            ++level;
+        }
     }
     if (done != n) {
         err = "a direction's cell dependency graph has a cycle";
         return kErrCycle;
     }
+    trace_prep.next("levelling.sort_scatter");
     s.n_levels = level;
     s.n_items = n;
     unsigned long long inc = 0;
@@ -276,20 +322,18 @@ int build_schedule_device(const MeshTables &t, const Quadrature &q, Schedule &s,
     TS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, kb, vb, (int64_t)n, 0, end_bit, st));
     TS_CUDA(take(d_temp, temp, st));
     TS_CUDA(cub::DeviceRadixSort::SortPairs(d_temp.p, temp, kb, vb, (int64_t)n, 0, end_bit, st));
-    // segment sizes, then padded and unpadded offsets
-    TS_CUDA(take(d_hist, sizeof(unsigned long long) * nseg, st));
-    TS_CUDA(cudaMemsetAsync(d_hist.p, 0, sizeof(unsigned long long) * nseg, st));
-    level_hist_kernel<<<blocks_for(n), kThreads, 0, st>>>(kb.Current(), n, (unsigned long long *)d_hist.p);
+    // segment starts (unpadded offsets), then padded offsets
+    TS_CUDA(take(d_hist, sizeof(uint64_t) * (nseg + 1), st));
+    seg_starts_kernel<<<blocks_for(n), kThreads, 0, st>>>(kb.Current(), n, (uint32_t)nseg, (uint64_t *)d_hist.p);
     TS_CUDA(cudaGetLastError());
-    std::vector<unsigned long long> hist(nseg);
-    TS_CUDA(cudaMemcpyAsync(hist.data(), d_hist.p, sizeof(unsigned long long) * nseg, cudaMemcpyDeviceToHost, st));
-    TS_CUDA(cudaStreamSynchronize(st));
     std::vector<uint64_t> unpadded(nseg + 1);
+    TS_CUDA(cudaMemcpyAsync(unpadded.data(), d_hist.p, sizeof(uint64_t) * (nseg + 1), cudaMemcpyDeviceToHost, st));
+    TS_CUDA(cudaStreamSynchronize(st));
     s.octant_offset.resize(nseg + 1);
-    unpadded[0] = s.octant_offset[0] = 0;
+    s.octant_offset[0] = 0;
     for (uint64_t k = 0; k < nseg; ++k) {
-        unpadded[k + 1] = unpadded[k] + hist[k];
-        s.octant_offset[k + 1] = s.octant_offset[k] + (hist[k] + kLevelPad - 1) / kLevelPad * kLevelPad;
+        const uint64_t cnt = unpadded[k + 1] - unpadded[k];
+        s.octant_offset[k + 1] = s.octant_offset[k] + (cnt + kLevelPad - 1) / kLevelPad * kLevelPad;
     }
     s.level_offset.resize(s.n_levels + 1);
     for (uint32_t l = 0; l <= s.n_levels; ++l) s.level_offset[l] = s.octant_offset[(size_t)l * kOctants];
@@ -348,16 +392,13 @@ int angle_chunks_device(const uint32_t *d_items, uint64_t n_padded, const uint64
     TS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, kb, vb, (int64_t)n_padded, 0, end_bit, st));
     TS_CUDA(take(d_temp, temp, st));
     TS_CUDA(cub::DeviceRadixSort::SortPairs(d_temp.p, temp, kb, vb, (int64_t)n_padded, 0, end_bit, st));
-    TS_CUDA(take(d_hist, sizeof(unsigned long long) * (nseg + 1), st));
-    TS_CUDA(cudaMemsetAsync(d_hist.p, 0, sizeof(unsigned long long) * (nseg + 1), st));
-    level_hist_kernel<<<blocks_for(n_padded), kThreads, 0, st>>>(kb.Current(), n_padded,
-                                                                 (unsigned long long *)d_hist.p);
+    // starts of the nseg chunk-level segments (keys nseg: the padding, last)
+    TS_CUDA(take(d_hist, sizeof(uint64_t) * (nseg + 1), st));
+    seg_starts_kernel<<<blocks_for(n_padded), kThreads, 0, st>>>(kb.Current(), n_padded, (uint32_t)nseg,
+                                                                 (uint64_t *)d_hist.p);
     TS_CUDA(cudaGetLastError());
-    std::vector<unsigned long long> hist(nseg + 1);
-    TS_CUDA(cudaMemcpyAsync(hist.data(), d_hist.p, sizeof(unsigned long long) * (nseg + 1), cudaMemcpyDeviceToHost,
-                            st));
+    TS_CUDA(cudaMemcpyAsync(off.data(), d_hist.p, sizeof(uint64_t) * (nseg + 1), cudaMemcpyDeviceToHost, st));
     TS_CUDA(cudaStreamSynchronize(st));
-    for (uint64_t k = 0; k < nseg; ++k) off[k + 1] = off[k] + hist[k];
     // the sorted positions (the padding bucket sorts last and is not used)
     DevBuf &cur = vb.Current() == (uint32_t *)d_vals[0].p ? d_vals[0] : d_vals[1];
     *d_pos_out = (uint32_t *)cur.p;

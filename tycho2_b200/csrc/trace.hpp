@@ -20,17 +20,25 @@ inline bool trace_on()
 class TraceScope {
 public:
     explicit TraceScope(const char *name) : name_(name), t0_(std::chrono::steady_clock::now()) {}
-    ~TraceScope()
+    ~TraceScope() { report(); }
+    // Ends the current phase (reported now) and starts the next one.
+    void next(const char *name)
+    {
+        report();
+        name_ = name;
+        t0_ = std::chrono::steady_clock::now();
+    }
+    TraceScope(const TraceScope &) = delete;
+    TraceScope &operator=(const TraceScope &) = delete;
+
+private:
+    void report() const
     {
         if (!trace_on()) return;
         const double ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count();
         std::fprintf(stderr, "[tycho] %s %.3f\n", name_, ms);
     }
-    TraceScope(const TraceScope &) = delete;
-    TraceScope &operator=(const TraceScope &) = delete;
-
-private:
     const char *name_;
     std::chrono::steady_clock::time_point t0_;
 };
