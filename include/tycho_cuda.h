@@ -373,10 +373,16 @@ typedef struct tycho_server_opts {
     int setup_threads;      /* host threads building sweepers */
     int ipw32, ipw64;       /* batched level kernels: items per warp (8, 16, 32; 0 = direct) */
     tycho_batch_opts solve; /* method TYCHO_SOURCE_ITERATION or TYCHO_MIXED_GMRES */
-    double large_items;     /* cells x angles from which a request runs in the
-                               second lane (its own batch and stream, stepped
-                               concurrently, so a deep mesh does not set the
-                               step time of small ones); 0 = 32e6 */
+    double large_items;     /* cells x angles from which a request is large; 0 =
+                               32e6.  Large requests do not join the batch of
+                               small ones (a deep mesh would set its step
+                               time): they run beside it on their own
+                               streams */
+    int large_batched;      /* 0: large requests are solved one at a time by
+                               the single-instance solver (source iteration;
+                               for the mixed service FP32-sweep GMRES(20) in
+                               FP64 refinement to err_max in the residual
+                               2-norm); 1: as members of a second batch */
 } tycho_server_opts;
 
 typedef struct tycho_request_info {

@@ -18,10 +18,10 @@ def _requests(count, seed):
     return out
 
 
-def _serve(reqs, method, arrivals, budget=150e9, threads=2, large_items=0.0):
+def _serve(reqs, method, arrivals, budget=150e9, threads=2, large_items=0.0, large_batched=False):
     import tycho2_b200 as ty
     srv = ty.SolveServer(method=method, budget_bytes=budget, setup_threads=threads, err_max=1e-10,
-                         large_items=large_items)
+                         large_items=large_items, large_batched=large_batched)
     ids = [srv.submit(mesh, p["sn"], p["groups"], st, ss, mat, q, arrival=t)
            for (p, mesh, st, ss, mat, q), t in zip(reqs, arrivals)]
     srv.run()
@@ -31,15 +31,18 @@ def _serve(reqs, method, arrivals, budget=150e9, threads=2, large_items=0.0):
     return res, stats
 
 
-@pytest.mark.parametrize("method,large_items", [("mixed", 0.0), ("si", 0.0), ("mixed", 20000.0)])
-def test_served_result_same_alone_and_in_mix(built, method, large_items):
-    """large_items 20000: the bigger requests run in the second lane (own
-    batch and stream) concurrently with the small ones."""
+@pytest.mark.parametrize("method,large_items,batched", [("mixed", 0.0, False), ("si", 0.0, False),
+                                                       ("mixed", 20000.0, False), ("si", 20000.0, False),
+                                                       ("mixed", 20000.0, True)])
+def test_served_result_same_alone_and_in_mix(built, method, large_items, batched):
+    """large_items 20000: the bigger requests run beside the batch of small
+    ones, solved one at a time by the single-instance solver (or in a second
+    batch with its own stream)."""
     reqs = _requests(6, seed=11)
-    alone = [_serve([r], method, [0.0])[0][0] for r in reqs]
+    alone = [_serve([r], method, [0.0], large_items=large_items, large_batched=batched)[0][0] for r in reqs]
     rng = np.random.default_rng(3)
     arrivals = np.cumsum(rng.exponential(0.01, len(reqs)))  # overlapping arrivals
-    mixed, stats = _serve(reqs, method, arrivals, large_items=large_items)
+    mixed, stats = _serve(reqs, method, arrivals, large_items=large_items, large_batched=batched)
     if large_items:
         sizes = [r[1].n_cells * 2 * r[0]["sn"] ** 2 for r in reqs]
         assert min(sizes) < large_items <= max(sizes)  # both lanes in use
@@ -77,3 +80,23 @@ def test_admission_respects_the_budget(built):
         assert res2[big][1]["state"] == "failed" and res2[1 - big][1]["state"] == "done"
     else:
         assert states == ["done", "done"]
+
+
+@pytest.mark.parametrize("method", ["si", "mixed"])
+def test_large_requests_solo_match_batched(built, method):
+    """Large requests solved by the single-instance solver: the FP64 source
+    iteration bit-identical to the batched one; the mixed service's GMRES-
+    based refinement within 1e-8 of its batched source-iteration form."""
+    reqs = _requests(6, seed=17)
+    arrivals = [0.0, 0.0, 0.004, 0.008, 0.012, 0.02]
+    sizes = [r[1].n_cells * 2 * r[0]["sn"] ** 2 for r in reqs]
+    large = float(sorted(sizes)[-2])  # the two largest run beside the batch
+    solo, _ = _serve(reqs, method, arrivals, large_items=large, large_batched=False)
+    batched, _ = _serve(reqs, method, arrivals, large_items=large, large_batched=True)
+    for (ps, i_s), (pb, ib), size in zip(solo, batched, sizes):
+        assert i_s["state"] == "done" and ib["state"] == "done"
+        if method == "si" or size < large:
+            assert bits_equal(ps, pb)
+        else:
+            assert rel_l1(ps, pb) <= 1e-8
+            assert i_s["stats"]["sweeps_fp32"] > 0

@@ -50,7 +50,8 @@ class BatchOpts(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("budget_bytes", C.c_double), ("setup_threads", C.c_int),
-                ("ipw32", C.c_int), ("ipw64", C.c_int), ("solve", BatchOpts), ("large_items", C.c_double)]
+                ("ipw32", C.c_int), ("ipw64", C.c_int), ("solve", BatchOpts), ("large_items", C.c_double),
+                ("large_batched", C.c_int)]
 
 
 class SolveStats(C.Structure):

@@ -577,6 +577,7 @@ int tycho_server_create(const tycho_server_opts *o, tycho_server **out)
         so.solve.inner_max = o->solve.inner_max;
         so.solve.refine_max = o->solve.refine_max;
         if (o->large_items > 0) so.large_items = o->large_items;
+        so.large_solo = o->large_batched == 0;
         auto *h = new tycho_server();
         int s = h->s.init(so, err);
         if (s != tycho::kOk) {

@@ -10,6 +10,8 @@
 
 namespace tycho {
 
+constexpr int kSoloRestart = 20;  // GMRES restart of the large requests' mixed solve
+
 uint64_t footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, bool fp32, bool compact)
 {
     const uint64_t A = 2ull * sn_order * sn_order;
@@ -33,7 +35,50 @@ Server::~Server()
         stop_ = true;
     }
     cv_work_.notify_all();
+    cv_solo_.notify_all();
+    if (solo_thread_.joinable()) solo_thread_.join();
     for (auto &t : workers_) t.join();
+}
+
+// Large requests, one at a time, each with the single-instance solver on its
+// sweeper's own streams (concurrently with the batch of small requests).
+// A request's result does not depend on what else is being served.
+void Server::solo()
+{
+    for (;;) {
+        Request *r = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_solo_.wait(lk, [&] { return stop_ || !solo_q_.empty(); });
+            if (solo_q_.empty()) return;
+            r = solo_q_.front();
+            solo_q_.pop_front();
+        }
+        SolveOptions so;
+        so.method = o_.solve.method == 2 ? 2 : 0;
+        so.iter_max = o_.solve.iter_max;
+        so.err_max = o_.solve.err_max;
+        so.restart = kSoloRestart;
+        so.inner_tol = o_.solve.inner_tol;
+        so.refine_max = o_.solve.refine_max;
+        SolveStats st;
+        std::string err;
+        const int s = r->sw->solve(so, r->phi_out, nullptr, st, err);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            r->status = s;
+            r->error = err;
+            r->stats.iterations = st.iterations;
+            r->stats.sweeps_fp64 = st.sweeps_fp64;
+            r->stats.sweeps_fp32 = st.sweeps_fp32;
+            r->stats.refinements = st.refinements;
+            r->stats.final_error = st.final_error;
+            r->stats.done = s == kOk;
+            r->stats.steps = 0;
+            solo_done_.push_back(r);
+        }
+        cv_built_.notify_all();
+    }
 }
 
 int Server::init(const ServerOptions &o, std::string &err)
@@ -105,6 +150,8 @@ int Server::submit(std::shared_ptr<const MeshTables> tp, int sn, int G, const do
     r->phi_out = phi_out;
     r->footprint = footprint_bytes(nc, sn, G, o_.solve.method == 2, o_.ipw32 == 0 && o_.ipw64 == 0);
     r->lane = (double)nc * 2.0 * sn * sn >= o_.large_items ? 1 : 0;
+    if (r->lane == 1 && o_.large_solo && o_.solve.method == 2)  // the GMRES basis and Hessenberg
+        r->footprint += (uint64_t)(kSoloRestart + 1) * nc * 4 * G * 8 + 4096;
     id = r->id;
     reqs_.push_back(std::move(r));
     return kOk;
@@ -180,6 +227,7 @@ int Server::run(std::string &err)
     t0_ = now();
     if (workers_.empty())
         for (int i = 0; i < o_.setup_threads; ++i) workers_.emplace_back([this] { worker(); });
+    if (o_.large_solo && !solo_thread_.joinable()) solo_thread_ = std::thread([this] { solo(); });
     std::vector<Request *> order;
     for (auto &r : reqs_)
         if (r->state == 0) order.push_back(r.get());
@@ -188,6 +236,7 @@ int Server::run(std::string &err)
     double reserved = 0;
     int pending = (int)order.size(), building = 0;
     int in_lane[kLanes] = {0, 0};
+    int in_solo = 0;  // large requests with the solo thread
     bool inflight[kLanes] = {false, false};
     std::vector<Request *> waiting[kLanes];  // built, joining at the lane's next step boundary
     while (pending > 0) {
@@ -225,13 +274,23 @@ int Server::run(std::string &err)
             freed_bytes_ = 0;
             const bool idle = !inflight[0] && !inflight[1] && in_lane[0] + in_lane[1] == 0 &&
                               waiting[0].empty() && waiting[1].empty();
-            if (idle && built_.empty()) {
-                // idle GPU: wait for a build or the next arrival
+            if (idle && built_.empty() && solo_done_.empty()) {
+                // no batch step to drive: wait for a build, a solo solve or
+                // the next arrival
                 const double wait = next < order.size() && order[next]->arrival > t ? order[next]->arrival - t : 0.05;
                 cv_built_.wait_for(lk, duration<double>(std::min(std::max(wait, 1e-4), 0.05)),
-                                   [&] { return !built_.empty(); });
+                                   [&] { return !built_.empty() || !solo_done_.empty(); });
             }
             ready.swap(built_);
+            for (Request *r : solo_done_) {
+                r->state = r->status == kOk ? 4 : 5;
+                r->t_done = now();
+                retire_q_.emplace_back(std::move(r->sw), (double)r->footprint);
+                --in_solo;
+                --pending;
+            }
+            if (!solo_done_.empty()) cv_work_.notify_one();
+            solo_done_.clear();
         }
         for (Request *r : ready) {
             --building;
@@ -243,6 +302,17 @@ int Server::run(std::string &err)
                 continue;
             }
             r->state = 2;
+            if (r->lane == 1 && o_.large_solo) {
+                r->state = 3;
+                ++in_solo;
+                {
+                    std::lock_guard<std::mutex> lk(mu_);
+                    solo_q_.push_back(r);
+                }
+                cv_solo_.notify_one();
+                peak_active_ = std::max(peak_active_, in_lane[0] + in_lane[1] + in_solo);
+                continue;
+            }
             waiting[r->lane].push_back(r);
         }
         // each lane steps on its own stream: finish a step when its stream is
@@ -287,7 +357,7 @@ int Server::run(std::string &err)
                 ++in_lane[L];
             }
             waiting[L].clear();
-            peak_active_ = std::max(peak_active_, in_lane[0] + in_lane[1]);
+            peak_active_ = std::max(peak_active_, in_lane[0] + in_lane[1] + in_solo);
             if (in_lane[L] > 0 && b.running() > 0) {
                 int s = b.step_launch(err);
                 if (s != kOk) return s;

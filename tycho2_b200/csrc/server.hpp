@@ -28,6 +28,11 @@ struct ServerOptions {
     int ipw32 = 0, ipw64 = 0;     // batch level kernels: items per warp (0 = direct, compact records)
     BatchOptions solve;           // method 0 FP64 source iteration, 2 mixed
     double large_items = 32e6;    // cells x angles from which a request runs in the large lane
+    // Large requests: solved one at a time by the single-instance solver on
+    // their sweeper's own streams (true: FP64 source iteration, or for the
+    // mixed service FP32-sweep GMRES(20) in FP64 refinement), or as members
+    // of a second batch (false).
+    bool large_solo = true;
 };
 
 // Device bytes one resident request holds (sweeper + batch vectors), an
@@ -68,6 +73,7 @@ public:
 
 private:
     void worker();
+    void solo();  // the large requests' single-instance solves, in order
     double now() const;
 
     ServerOptions o_;
@@ -87,6 +93,11 @@ private:
     // thread); their footprints go back to the budget once destroyed
     std::deque<std::pair<std::unique_ptr<Sweeper>, double>> retire_q_;
     double freed_bytes_ = 0;
+    // large requests for the solo thread, and those it has finished
+    std::condition_variable cv_solo_;
+    std::deque<Request *> solo_q_;
+    std::vector<Request *> solo_done_;
+    std::thread solo_thread_;
     bool stop_ = false;
     std::vector<std::thread> workers_;
     double t0_ = 0;

@@ -356,17 +356,19 @@ def footprint_bytes(n_cells, sn_order, n_groups, mixed=True, compact=True):
 class SolveServer:
     """Solve service on one GPU (tycho_server_*): requests with arrival times
     are admitted by device-memory footprint against `budget_bytes`, built by
-    host threads and solved by continuous batching."""
+    host threads and solved by continuous batching; requests of at least
+    `large_items` cells x angles are solved one at a time beside the batch by
+    the single-instance solver (or, large_batched, in a second batch)."""
 
     STATES = {0: "queued", 1: "building", 2: "built", 3: "in batch", 4: "done", 5: "failed"}
 
     def __init__(self, method="mixed", budget_bytes=150e9, device=0, setup_threads=2, ipw32=0,
                  ipw64=0, iter_max=3000, err_max=1e-10, inner_tol=1e-5, inner_max=200, refine_max=30,
-                 large_items=0.0):
+                 large_items=0.0, large_batched=False):
         solve = _capi.BatchOpts(BatchSolver.BATCH_METHODS[method], iter_max, err_max, inner_tol,
                                 inner_max, refine_max)
         o = _capi.ServerOpts(device, float(budget_bytes), setup_threads, ipw32, ipw64, solve,
-                             float(large_items))
+                             float(large_items), int(bool(large_batched)))
         h = C.c_void_p()
         check(lib().tycho_server_create(C.byref(o), C.byref(h)))
         self._h = h
