@@ -450,3 +450,28 @@ def test_dropin_sweep_in_angle_chunks_bit_exact(built, workdir, n, G, chunks, pi
     sw.sweep(psi, src)
     assert bits_equal(psi, ref)
     sw.close()
+
+
+def test_invalid_arguments_are_errors(built, workdir):
+    """Bad sizes and launch shapes come back as TYCHO_ERR_ARG (status 1),
+    never as a fault: 0 or 65 groups, an SN order without a quadrature table,
+    a knob, vector width or stream count the kernels do not have."""
+    import tycho2_b200 as ty
+    mesh, _ = kuhn(workdir, 2, 0.05, seed=3)
+    for sn, G in ((4, 0), (4, 65), (3, 1), (0, 1)):
+        with pytest.raises(ty.TychoError) as e:
+            make(mesh, sn, G)
+        assert e.value.status == 1, (sn, G)
+    sw = make(mesh, 4, 4, fp32=True)
+    for args in (("levels", "compact", 96), ("levels", "direct", -72), ("levels", "compact", 64, 3),
+                 ("levels", "compact", 64, 2, 3), ("dataflow", "tiles", 4, 0, 2), ("persist", "direct", 64)):
+        for prec in (0, 1):
+            with pytest.raises(ty.TychoError) as e:
+                sw.configure(prec, *args)
+            assert e.value.status == 1, (prec, args)
+    sw.configure(1, "levels", "compact", -96, 4, 2)  # still usable after the refusals
+    sw.set_cross_sections(np.ones(mesh.n_cells), np.full(mesh.n_cells, 0.5))
+    sw.set_source(np.ones(sw.phi_shape), "isotropic")
+    phi, _, _ = sw.solve("mixed", iter_max=50, err_max=1e-10, want_psi=False)
+    assert np.all(np.isfinite(phi))
+    sw.close()
