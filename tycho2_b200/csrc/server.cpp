@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <exception>
+#include <new>
 #include <thread>
 
 #include "devmem.hpp"
@@ -63,7 +65,16 @@ void Server::solo()
         so.refine_max = o_.solve.refine_max;
         SolveStats st;
         std::string err;
-        const int s = r->sw->solve(so, r->phi_out, nullptr, st, err);
+        int s = kOk;
+        try {
+            s = r->sw->solve(so, r->phi_out, nullptr, st, err);
+        } catch (const std::bad_alloc &) {
+            s = kErrOom;
+            err = "host memory exhausted while solving the request";
+        } catch (const std::exception &e) {
+            s = kErrArg;
+            err = std::string("solving the request: ") + e.what();
+        }
         {
             std::lock_guard<std::mutex> lk(mu_);
             r->status = s;
@@ -200,14 +211,23 @@ void Server::worker()
         so.n_groups = r->G;
         so.device = o_.device;
         so.fp32 = o_.solve.method == 2;
-        int s = sw->init(r->tables, so, err);
-        if (s == kOk)
-            s = sw->set_cross_sections(r->sigma_t.data(), r->sigma_s.data(),
-                                       r->scatter.empty() ? nullptr : r->scatter.data(), err);
-        if (s == kOk && !r->q.empty()) s = sw->set_source(1, r->q.data(), err);
-        Sweeper::DeviceView v;
-        if (s == kOk) s = sw->device_view(0, v, err, o_.ipw64 == 0);
-        if (s == kOk && so.fp32) s = sw->device_view(1, v, err, o_.ipw32 == 0);
+        int s = kOk;
+        try {  // a failed build fails its request, never the service
+            s = sw->init(r->tables, so, err);
+            if (s == kOk)
+                s = sw->set_cross_sections(r->sigma_t.data(), r->sigma_s.data(),
+                                           r->scatter.empty() ? nullptr : r->scatter.data(), err);
+            if (s == kOk && !r->q.empty()) s = sw->set_source(1, r->q.data(), err);
+            Sweeper::DeviceView v;
+            if (s == kOk) s = sw->device_view(0, v, err, o_.ipw64 == 0);
+            if (s == kOk && so.fp32) s = sw->device_view(1, v, err, o_.ipw32 == 0);
+        } catch (const std::bad_alloc &) {
+            s = kErrOom;
+            err = "host memory exhausted while building the request";
+        } catch (const std::exception &e) {
+            s = kErrArg;
+            err = std::string("building the request: ") + e.what();
+        }
         {
             std::lock_guard<std::mutex> lk(mu_);
             r->status = s;
