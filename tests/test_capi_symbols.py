@@ -52,3 +52,24 @@ def test_footprint_estimate_covers_psi_and_records():
         assert ty.footprint_bytes(nc, sn, G, False, False) < b
         assert ty.footprint_bytes(2 * nc, sn, G, True, False) > b
         assert ty.footprint_bytes(nc, sn, 2 * G, True, False) > b
+
+
+def test_header_is_plain_c(tmp_path):
+    """The boundary is a C ABI: the header compiles as strict C99 (a cgo,
+    JNI or ctypes binding sees no C++), and every struct zero-initialises."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "abi.c"
+    src.write_text('#include "tycho_cuda.h"\n'
+                   "int main(void) {\n"
+                   "    tycho_sweeper_opts o = {0}; tycho_launch_shape s = {0};\n"
+                   "    tycho_solve_opts so = {0}; tycho_batch_opts b = {0}; tycho_server_opts sv = {0};\n"
+                   "    (void)o; (void)s; (void)so; (void)b; (void)sv; return 0;\n"
+                   "}\n")
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                        "-I" + os.path.join(ROOT, "include"), "-c", str(src), "-o", str(tmp_path / "abi.o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
