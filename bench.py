@@ -228,7 +228,14 @@ KERNELS = {
 SCHED = {"levels": 1, "dataflow": 2, "persist": 3}
 
 
+SLOT_KNOBS = {-196: 10, -180: 12, -172: 14}  # FP32 slotted upwind rows: blocks of 64 per SM
+
+
 def kernel_name(shape, fp32):
+    if shape["knob"] in SLOT_KNOBS and shape["variant"] in ("direct", "compact"):
+        return "sweep_direct_slot_kernel<{vg},64,{rec},{m}>".format(
+            vg=shape["vector"], rec="compact" if shape["variant"] == "compact" else "full",
+            m=SLOT_KNOBS[shape["knob"]])
     return KERNELS[(SCHED[shape["schedule"]], shape["variant"])].format(
         r="float" if fp32 else "double", k=shape["knob"], vg=shape["vector"])
 
@@ -379,7 +386,7 @@ def run_large_leg(grp, dev, workload="kuhn64_s8_g16"):
     sw.set_source(q, "isotropic")
     setup = time.perf_counter() - t0
     info = sw.schedule_info()
-    sw.configure(1, "levels", "compact", -96, 4, 2)
+    sw.configure(1, "levels", "compact", -172, 4, 2)
     try:  # compact FP64 records (19 GB) fit beside psi (103 GB) and the GMRES(30) basis
         sw.configure(0, "levels", "compact", -96, 2, 2)
     except ty.TychoError:
@@ -533,6 +540,9 @@ def run_b200(args):
     large = None
     if not args.no_large:
         try:
+            # a clean device for the largest problem: the earlier legs' cached
+            # pool memory (and the service's reservation) goes back first
+            ty.release_cached_memory(dev)
             large = run_large_leg(grp, dev)
         except Exception as e:
             large = {"error": str(e)[:300]}

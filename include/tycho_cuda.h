@@ -237,7 +237,11 @@ int tycho_sweeper_levels(const tycho_sweeper *sw, uint32_t *tlevel, uint32_t *de
                   read before the wait on the previous level; level schedule
                   only, knob threads per block (64, 128, 256; -64 / -128:
                   the same capped at 64 registers; -96 / -80: 64 threads
-                  capped at 102 / 85 registers),
+                  capped at 102 / 85 registers; FP32 with 2 or 4 groups per
+                  vector also -196 / -180 / -172: the upwind faces (at most
+                  three per cell and direction) in three slots instead of
+                  four face positions, 64 threads capped at 102 / 85 / 73
+                  registers),
               4 = direct compact records: 64 B (FP32) / 96 B (FP64) per item
                   holding the matrix inputs (face terms, sigma_t V/20, V/20)
                   and topology; the factors are rebuilt in registers with the

@@ -214,7 +214,8 @@ def test_fp32_sweep_within_tolerance(built, workdir):
                   ("dataflow", "compact", 128), ("dataflow", "direct", 128, 2), ("levels", "compact", 64, 8),
                   ("levels", "direct", 128, 8), ("levels", "compact", 64, 4, 8), ("levels", "compact", 64, 2, 2),
                   ("levels", "compact", -96, 4, 2), ("levels", "direct", -96, 4), ("levels", "compact", -80, 4),
-                  ("levels", "direct", -64, 2, 2)):
+                  ("levels", "direct", -64, 2, 2), ("levels", "compact", -180, 4, 2), ("levels", "direct", -196, 2),
+                  ("levels", "compact", -196, 4), ("levels", "compact", -172, 4, 2), ("levels", "direct", -180, 4)):
         sw = make(mesh, 8, G, fp32=True)
         sw.configure(1, *shape)
         sw.set_cross_sections(st, st, mat)
@@ -464,7 +465,8 @@ def test_invalid_arguments_are_errors(built, workdir):
         assert e.value.status == 1, (sn, G)
     sw = make(mesh, 4, 4, fp32=True)
     for args in (("levels", "compact", 96), ("levels", "direct", -72), ("levels", "compact", 64, 3),
-                 ("levels", "compact", 64, 2, 3), ("dataflow", "tiles", 4, 0, 2), ("persist", "direct", 64)):
+                 ("levels", "compact", 64, 2, 3), ("dataflow", "tiles", 4, 0, 2), ("persist", "direct", 64),
+                 ("levels", "compact", -180, 1)):
         for prec in (0, 1):
             with pytest.raises(ty.TychoError) as e:
                 sw.configure(prec, *args)
@@ -474,4 +476,19 @@ def test_invalid_arguments_are_errors(built, workdir):
     sw.set_source(np.ones(sw.phi_shape), "isotropic")
     phi, _, _ = sw.solve("mixed", iter_max=50, err_max=1e-10, want_psi=False)
     assert np.all(np.isfinite(phi))
+    sw.close()
+
+
+def test_fp64_refuses_slotted_rows(built, workdir):
+    """The slotted upwind rows change the summation order, so they exist for
+    the FP32 sweep only; the FP64 sweep keeps the reference's order."""
+    import tycho2_b200 as ty
+    mesh, _ = kuhn(workdir, 2, 0.05, seed=3)
+    sw = make(mesh, 4, 4, fp32=True)
+    for knob in (-196, -180, -172):
+        with pytest.raises(ty.TychoError) as e:
+            sw.configure(0, "levels", "compact", knob, 2)
+        assert e.value.status == 1
+        sw.configure(1, "levels", "compact", knob, 4)
+    assert sw.shape(1)["knob"] == -172
     sw.close()

@@ -524,6 +524,119 @@ __device__ __forceinline__ void pair_solve_store_any(const LevelArgs &p, const V
     else pair_solve_store_v<Real, VG, View, ANY>(p, R, g, in);
 }
 
+// FP32: a tet has at most three faces with omega.n < 0, so the upwind rows
+// of a task fit three slots (the item's interior upwind faces in increasing
+// face order) instead of four face-indexed ones: 3*3*VG loaded values live
+// at once instead of 4*3*VG.  Slot s keeps the neighbour's psi at the face's
+// three vertices j != f in increasing j.  Summation order differs from the
+// face-indexed form (FP32 is checked by tolerance).
+template <int VG>
+struct SlotIn {
+    float p[3][3][VG];
+    uint32_t faces;  // slot s's face in bits 2s, 2s+1
+    uint32_t count;  // occupied slots
+};
+
+template <int VG, typename View>
+__device__ __forceinline__ void slot_load_upwind(const LevelArgs &p, const View &R, uint32_t g, SlotIn<VG> &in)
+{
+    const float *__restrict__ psi = reinterpret_cast<const float *>(p.psi);
+    const uint32_t G = p.G, rowG = 4u * G, nmap = R.u(2);
+    uint32_t live = 0;
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+        if (R.f(f) < 0.0f && R.u(3 + f) != kNoRow) live |= 1u << f;
+    uint32_t faces = 0, count = 0;
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        const bool has = live != 0u;
+        const uint32_t f = has ? (uint32_t)(__ffs(live) - 1) : 0u;
+        live &= live - 1u;
+        faces |= f << (2 * s);
+        count += has ? 1u : 0u;
+        const uint32_t row = f == 0u ? R.u(3) : f == 1u ? R.u(4) : f == 2u ? R.u(5) : R.u(6);
+        const float *nrow = psi + (uint64_t)(has ? row : 0u) * rowG + g;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const uint32_t j = (uint32_t)k < f ? (uint32_t)k : (uint32_t)k + 1u;
+            const uint32_t nv = (nmap >> ((f * 4u + j) * 2u)) & 3u;
+            if (has) {
+                gv_load<float, VG, false>(nrow + nv * G, in.p[s][k]);
+            } else {
+#pragma unroll
+                for (int e = 0; e < VG; ++e) in.p[s][k][e] = 0.0f;
+            }
+        }
+    }
+    in.faces = faces;
+    in.count = count;
+}
+
+// The solve of a slotted task (packed FP32x2; in.q holds the volume source
+// term): for an upwind face f with A_f/12 = t, row r != f loses t (S + p_r),
+// S the sum of the face's three vertex values and p_r the value at vertex r.
+template <int VG, typename View>
+__device__ __forceinline__ void slot_solve_store_f32x2(const LevelArgs &p, const View &R, uint32_t g,
+                                                       const float (&q)[4][VG], const SlotIn<VG> &in)
+{
+    static_assert(VG % 2 == 0, "pairs of groups");
+    float c[3][4];  // per slot and row: -t, or 0 on the face's own row and for an empty slot
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        const uint32_t f = (in.faces >> (2 * s)) & 3u;
+        const float t = (uint32_t)s < in.count ? (f == 0u ? R.f(0) : f == 1u ? R.f(1) : f == 2u ? R.f(2) : R.f(3))
+                                               : 0.0f;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) c[s][r] = f == (uint32_t)r ? 0.0f : -t;
+    }
+    float res[4][VG];
+#pragma unroll
+    for (int e = 0; e < VG; e += 2) {
+        float2 b[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) b[v] = make_float2(q[v][e], q[v][e + 1]);
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            const uint32_t f = (in.faces >> (2 * s)) & 3u;
+            float2 pk[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) pk[k] = make_float2(in.p[s][k][e], in.p[s][k][e + 1]);
+            const float2 S = __fadd2_rn(__fadd2_rn(pk[0], pk[1]), pk[2]);
+            // vertex r is k = r (r < f) or k = r - 1 (r > f)
+            const float2 p0 = pk[0];
+            const float2 p1 = f > 1u ? pk[1] : pk[0];
+            const float2 p2 = f > 2u ? pk[2] : pk[1];
+            const float2 p3 = pk[2];
+            b[0] = __ffma2_rn(make_float2(c[s][0], c[s][0]), __fadd2_rn(S, p0), b[0]);
+            b[1] = __ffma2_rn(make_float2(c[s][1], c[s][1]), __fadd2_rn(S, p1), b[1]);
+            b[2] = __ffma2_rn(make_float2(c[s][2], c[s][2]), __fadd2_rn(S, p2), b[2]);
+            b[3] = __ffma2_rn(make_float2(c[s][3], c[s][3]), __fadd2_rn(S, p3), b[3]);
+        }
+        auto sp = [](float x) { return make_float2(x, x); };
+        b[0] = __fmul2_rn(b[0], sp(R.f(5)));
+        b[1] = __ffma2_rn(sp(-R.f(9)), b[0], b[1]);
+        b[2] = __ffma2_rn(sp(-R.f(10)), b[0], b[2]);
+        b[3] = __ffma2_rn(sp(-R.f(11)), b[0], b[3]);
+        b[1] = __fmul2_rn(b[1], sp(R.f(12)));
+        b[2] = __ffma2_rn(sp(-R.f(15)), b[1], b[2]);
+        b[3] = __ffma2_rn(sp(-R.f(16)), b[1], b[3]);
+        b[2] = __fmul2_rn(b[2], sp(R.f(17)));
+        b[3] = __ffma2_rn(sp(-R.f(19)), b[2], b[3]);
+        b[3] = __fmul2_rn(b[3], sp(__fdividef(1.0f, R.f(20))));
+        b[2] = __ffma2_rn(sp(-R.f(18)), b[3], b[2]);
+        b[1] = __ffma2_rn(sp(-R.f(13)), b[2], __ffma2_rn(sp(-R.f(14)), b[3], b[1]));
+        b[0] = __ffma2_rn(sp(-R.f(6)), b[1], __ffma2_rn(sp(-R.f(7)), b[2], __ffma2_rn(sp(-R.f(8)), b[3], b[0])));
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            res[v][e] = b[v].x;
+            res[v][e + 1] = b[v].y;
+        }
+    }
+    float *__restrict__ out = reinterpret_cast<float *>(p.psi) + (uint64_t)R.u(1) * (4u * p.G) + g;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) gv_store(out + v * p.G, res[v]);
+}
+
 // Whether a task's arithmetic runs packed FP32x2 (and can form its volume
 // source term before the wait).
 template <typename Real, int VG, bool ANY>
@@ -630,6 +743,35 @@ sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const 
     pair_load_upwind<Real, VG, false>(p, R, g, in);
     if constexpr (kPairedF32<Real, VG, ANY>) pair_solve_store_f32x2<VG, RegRecord<Real>, true>(p, R, g, in);
     else pair_solve_store_any<Real, VG, RegRecord<Real>, ANY>(p, R, g, in);
+}
+
+// The FP32 direct kernel with slotted upwind rows (even vector widths).
+template <int VG, int BS, typename Rec, int MINB>
+__global__ void __launch_bounds__(BS, MINB)
+sweep_direct_slot_kernel(const LevelArgs p, const Rec *__restrict__ rec, const uint64_t begin, const uint64_t end)
+{
+    pdl_launch_dependents();
+    const uint32_t gpv = p.G / VG;
+    const uint32_t t = blockIdx.x * (uint32_t)BS + threadIdx.x;
+    const uint32_t itl = gpv == 1u ? t : __umulhi(t, p.vmagic);
+    const uint32_t g = (t - itl * gpv) * VG;
+    const uint64_t it = begin + itl;
+    bool live = it < end;
+    RegRecord<float> R;
+    PairIn<float, VG> in;  // sources only
+    if (live) {
+        load_record(rec + it, R, (uint32_t)kSolveNoPivot);
+        live = R.u(0) != kSentinel;
+    }
+    if (live) {
+        pair_load_source<float, VG>(p, R, g, in);
+        pair_source_rhs_f32x2<VG>(R, in);
+    }
+    pdl_wait_prerequisites();
+    if (!live) return;
+    SlotIn<VG> sl;
+    slot_load_upwind<VG>(p, R, g, sl);
+    slot_solve_store_f32x2<VG>(p, R, g, in.q, sl);
 }
 
 // Direct variant, two group vectors per task: the task covers 2*VG groups
@@ -963,12 +1105,25 @@ static const void *direct_any_fn(int vg)
     }
 }
 
+template <typename Real, typename Rec, int MINB>
+static const void *direct_slot_fn(int vg)
+{
+    if constexpr (sizeof(Real) == 4) {
+        if (vg == 2) return (const void *)sweep_direct_slot_kernel<2, 64, Rec, MINB>;
+        if (vg == 4) return (const void *)sweep_direct_slot_kernel<4, 64, Rec, MINB>;
+    }
+    return nullptr;
+}
+
 template <typename Real, typename Rec>
 static const void *direct_fn(int knob, int vg, uint32_t solver)
 {
     // Original and the Cramer solvers: one 128-thread kernel per vector width
     if (solver != kSolveNoPivot) return knob == 128 ? direct_any_fn<Real, Rec>(vg) : nullptr;
     switch (knob) {
+    case -196: return direct_slot_fn<Real, Rec, 10>(vg);  // slotted upwind rows, <= 102 registers
+    case -180: return direct_slot_fn<Real, Rec, 12>(vg);  // slotted upwind rows, <= 85 registers
+    case -172: return direct_slot_fn<Real, Rec, 14>(vg);  // slotted upwind rows, <= 73 registers
     case 64: return direct_fn_vg<Real, 64, Rec, 1>(vg);
     case 128: return direct_fn_vg<Real, 128, Rec, 1>(vg);
     case 256: return direct_fn_vg<Real, 256, Rec, 1>(vg);
@@ -982,14 +1137,17 @@ static const void *direct_fn(int knob, int vg, uint32_t solver)
 
 // Direct variant: knob = threads per block (64, 128 or 256; -64 / -128: the
 // same with registers capped at 64 so that more blocks are resident; -96 /
-// -80: 64 threads with at most 102 / 85 registers, 10 / 12 blocks per SM);
-// compact
-// picks the compact record format.
+// -80: 64 threads with at most 102 / 85 registers, 10 / 12 blocks per SM;
+// -196 / -180 / -172: the FP32 kernel with slotted upwind rows, 64 threads
+// with at most 102 / 85 / 73 registers); compact picks the compact record
+// format.
 template <typename Real>
 cudaError_t launch_direct_level(int knob, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
                                 cudaStream_t s, bool compact)
 {
-    const int bs = knob == -96 || knob == -80 ? 64 : knob < 0 ? -knob : knob;
+    const int bs = knob == -96 || knob == -80 || knob == -196 || knob == -180 || knob == -172 ? 64
+                   : knob < 0                                                             ? -knob
+                                                                                          : knob;
     if (end <= begin) return cudaSuccess;
     const uint64_t tasks = (end - begin) * (p.G / p.vg);
     if (tasks >= (1ull << 26)) return cudaErrorInvalidValue;

