@@ -63,7 +63,8 @@ def parse():
     p.add_argument("--serve-rate", type=float, default=10.0, help="Poisson arrivals per second")
     p.add_argument("--shape", default="auto",
                    help="launch shape 'schedule,variant,knob[,vector[,streams]]' for both precisions "
-                        "(an FP32-only vector width falls back to the widest for FP64), or auto (autotuner)")
+                        "(an FP32-only vector width falls back to the widest for FP64, an FP32-only knob "
+                        "to -96), or auto (autotuner)")
     p.add_argument("--profile-leg", default="main", choices=["main", "batch"],
                    help="what cudaProfilerStart/Stop bracket (for ncu --profile-from-start off): the main "
                         "leg's timed steps, or steps 4-6 of each batched solve")
@@ -448,7 +449,9 @@ def run_b200(args):
         vec = int(parts[3]) if len(parts) > 3 else 0
         streams = int(parts[4]) if len(parts) > 4 else 1
         for prec in (1, 0):
-            sw.configure(prec, s, v, int(k), vec if (prec == 1 or vec <= 2) else 0, streams)
+            # FP32-only knobs (slotted upwind rows) fall back to -96 for FP64
+            pk = -96 if prec == 0 and int(k) in SLOT_KNOBS else int(k)
+            sw.configure(prec, s, v, pk, vec if (prec == 1 or vec <= 2) else 0, streams)
         tuned = {1: sw.shape(1), 0: sw.shape(0)}
     shape32, shape64 = sw.shape(1), sw.shape(0)
     launches = {1: sw.launches(1), 0: sw.launches(0)}
