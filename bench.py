@@ -229,14 +229,15 @@ KERNELS = {
 SCHED = {"levels": 1, "dataflow": 2, "persist": 3}
 
 
-SLOT_KNOBS = {-196: 10, -180: 12, -172: 14}  # FP32 slotted upwind rows: blocks of 64 per SM
+# FP32 slotted upwind rows: knob -> (threads per block, blocks per SM)
+SLOT_KNOBS = {-196: (64, 10), -180: (64, 12), -172: (64, 14)}
 
 
 def kernel_name(shape, fp32):
     if shape["knob"] in SLOT_KNOBS and shape["variant"] in ("direct", "compact"):
-        return "sweep_direct_slot_kernel<{vg},64,{rec},{m}>".format(
-            vg=shape["vector"], rec="compact" if shape["variant"] == "compact" else "full",
-            m=SLOT_KNOBS[shape["knob"]])
+        bs, minb = SLOT_KNOBS[shape["knob"]]
+        return "sweep_direct_slot_kernel<{vg},{bs},{rec},{m}>".format(
+            vg=shape["vector"], bs=bs, rec="compact" if shape["variant"] == "compact" else "full", m=minb)
     return KERNELS[(SCHED[shape["schedule"]], shape["variant"])].format(
         r="float" if fp32 else "double", k=shape["knob"], vg=shape["vector"])
 

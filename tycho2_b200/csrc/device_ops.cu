@@ -80,16 +80,26 @@ __global__ void psi_to_phi_kernel(const Real *__restrict__ psi, const double *__
     reinterpret_cast<double2 *>(phi + i)[1] = make_double2(s[2], s[3]);
 }
 
+// One thread per (cell, group): the group's four vertex elements (groups
+// fastest, so a warp writes runs of G consecutive elements per vertex).
 __global__ void scatter_source_kernel(const double *__restrict__ phi, const double *__restrict__ q,
                                       const double *__restrict__ sigma_s,
                                       const double *__restrict__ scat, double *__restrict__ iso,
                                       float *__restrict__ iso32, uint64_t nc, uint32_t G)
 {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nc * 4 * G) return;
-    const double s = scatter_elem(phi, q, sigma_s, scat, i, G);
-    iso[i] = s;
-    if (iso32) iso32[i] = (float)s;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nc * G) return;
+    const uint64_t c = t < (1ull << 32) ? (uint64_t)((uint32_t)t / G) : t / G;
+    const uint32_t g = (uint32_t)(t - c * G);
+    double s[4];
+    scatter_cell_group(phi, q, sigma_s, scat, c, g, G, s);
+    const uint64_t base = c * 4 * G + g;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) iso[base + v * G] = s[v];
+    if (iso32) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) iso32[base + v * G] = (float)s[v];
+    }
 }
 
 template <int K>
@@ -215,7 +225,7 @@ cudaError_t launch_scatter_source(const double *phi_in, const double *q_fixed, c
                                   const double *scatter, double *iso, float *iso32, uint64_t nc,
                                   uint32_t G, cudaStream_t s)
 {
-    const uint64_t n = nc * 4 * G;
+    const uint64_t n = nc * G;
     if (n == 0) return cudaSuccess;
     scatter_source_kernel<<<blocks_for(n), 256, 0, s>>>(phi_in, q_fixed, sigma_s, scatter, iso, iso32, nc, G);
     return cudaGetLastError();

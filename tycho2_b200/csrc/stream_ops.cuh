@@ -40,6 +40,43 @@ __device__ __forceinline__ double scatter_elem(const double *__restrict__ phi, c
     return s;
 }
 
+// The four vertex elements (c, v, g), v = 0..3, of the total isotropic
+// source, with the arithmetic of scatter_elem term by term (the same
+// coefficient sigma_s[c] * k / 4pi, the same summation order over g'), so
+// the results are bit-identical; the coefficient is formed once for the four
+// vertices instead of once per element.
+__device__ __forceinline__ void scatter_cell_group(const double *__restrict__ phi, const double *__restrict__ q,
+                                                   const double *__restrict__ sigma_s,
+                                                   const double *__restrict__ scat, uint64_t c, uint32_t g,
+                                                   uint32_t G, double (&s)[4])
+{
+    const uint64_t base = c * 4 * G;
+    if (phi) {
+        if (!scat) {
+            const double k = sigma_s[c] / kFourPi;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) s[v] = k * phi[base + v * G + g];
+        } else {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) s[v] = 0.0;
+            for (uint32_t gp = 0; gp < G; ++gp) {
+                const double k = scat[g * G + gp];
+                if (k == 0.0) continue;
+                const double kc = sigma_s[c] * k / kFourPi;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) s[v] += kc * phi[base + v * G + gp];
+            }
+        }
+        if (q) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) s[v] = q[base + v * G + g] + s[v];
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) s[v] = q ? q[base + v * G + g] : 0.0;
+    }
+}
+
 // Scalar flux of phi element i: sum_a w_a psi(c,a,v,g), angles in increasing
 // order, FP64 accumulation (Util::psiToPhi, Util.cc:85-97).
 template <typename Real>

@@ -1105,12 +1105,12 @@ static const void *direct_any_fn(int vg)
     }
 }
 
-template <typename Real, typename Rec, int MINB>
+template <typename Real, typename Rec, int BS, int MINB>
 static const void *direct_slot_fn(int vg)
 {
     if constexpr (sizeof(Real) == 4) {
-        if (vg == 2) return (const void *)sweep_direct_slot_kernel<2, 64, Rec, MINB>;
-        if (vg == 4) return (const void *)sweep_direct_slot_kernel<4, 64, Rec, MINB>;
+        if (vg == 2) return (const void *)sweep_direct_slot_kernel<2, BS, Rec, MINB>;
+        if (vg == 4) return (const void *)sweep_direct_slot_kernel<4, BS, Rec, MINB>;
     }
     return nullptr;
 }
@@ -1121,9 +1121,10 @@ static const void *direct_fn(int knob, int vg, uint32_t solver)
     // Original and the Cramer solvers: one 128-thread kernel per vector width
     if (solver != kSolveNoPivot) return knob == 128 ? direct_any_fn<Real, Rec>(vg) : nullptr;
     switch (knob) {
-    case -196: return direct_slot_fn<Real, Rec, 10>(vg);  // slotted upwind rows, <= 102 registers
-    case -180: return direct_slot_fn<Real, Rec, 12>(vg);  // slotted upwind rows, <= 85 registers
-    case -172: return direct_slot_fn<Real, Rec, 14>(vg);  // slotted upwind rows, <= 73 registers
+    // slotted upwind rows: 64 threads with <= 102 / 85 / 73 registers
+    case -196: return direct_slot_fn<Real, Rec, 64, 10>(vg);
+    case -180: return direct_slot_fn<Real, Rec, 64, 12>(vg);
+    case -172: return direct_slot_fn<Real, Rec, 64, 14>(vg);
     case 64: return direct_fn_vg<Real, 64, Rec, 1>(vg);
     case 128: return direct_fn_vg<Real, 128, Rec, 1>(vg);
     case 256: return direct_fn_vg<Real, 256, Rec, 1>(vg);
@@ -1141,13 +1142,19 @@ static const void *direct_fn(int knob, int vg, uint32_t solver)
 // -196 / -180 / -172: the FP32 kernel with slotted upwind rows, 64 threads
 // with at most 102 / 85 / 73 registers); compact picks the compact record
 // format.
+inline int direct_block_threads(int knob)
+{
+    switch (knob) {
+    case -96: case -80: case -196: case -180: case -172: return 64;
+    default: return knob < 0 ? -knob : knob;
+    }
+}
+
 template <typename Real>
 cudaError_t launch_direct_level(int knob, const LevelArgs &p, const void *rec, uint64_t begin, uint64_t end,
                                 cudaStream_t s, bool compact)
 {
-    const int bs = knob == -96 || knob == -80 || knob == -196 || knob == -180 || knob == -172 ? 64
-                   : knob < 0                                                             ? -knob
-                                                                                          : knob;
+    const int bs = direct_block_threads(knob);
     if (end <= begin) return cudaSuccess;
     const uint64_t tasks = (end - begin) * (p.G / p.vg);
     if (tasks >= (1ull << 26)) return cudaErrorInvalidValue;
