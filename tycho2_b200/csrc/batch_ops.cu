@@ -32,9 +32,30 @@ __global__ void __launch_bounds__(256) batch_accept_kernel(const BatchSlot *__re
     });
 }
 
+// One thread per (cell, group) of the chunk when chunks hold whole cells
+// (4 G divides the chunk size), as in the single-instance scatter; else one
+// per element.  Bit-identical either way.
 __global__ void __launch_bounds__(256) batch_scatter_kernel(const BatchSlot *__restrict__ slots, BatchPlan pl)
 {
     for_each_chunk(slots, pl, [&](const BatchSlot &s, uint64_t i0, uint64_t i1, uint32_t) {
+        const uint32_t row = 4u * s.G;
+        if (kBatchChunk % row == 0) {
+            const uint64_t c0 = i0 / row;
+            const uint32_t pairs = (uint32_t)((i1 - i0) / 4);
+            for (uint32_t q = threadIdx.x; q < pairs; q += blockDim.x) {
+                const uint32_t dc = q / s.G, g = q - dc * s.G;
+                double v[4];
+                scatter_cell_group(s.phi_in, s.q_fixed, s.sigma_s, s.scat, c0 + dc, g, s.G, v);
+                const uint64_t base = (c0 + dc) * row + g;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) s.iso[base + k * s.G] = v[k];
+                if (s.iso32) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) s.iso32[base + k * s.G] = (float)v[k];
+                }
+            }
+            return;
+        }
         for (uint64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
             const double v = scatter_elem(s.phi_in, s.q_fixed, s.sigma_s, s.scat, i, s.G);
             s.iso[i] = v;
