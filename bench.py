@@ -61,10 +61,12 @@ def parse():
     p.add_argument("--no-serve", action="store_true", help="skip the served-solves leg")
     p.add_argument("--serve-requests", type=int, default=40)
     p.add_argument("--serve-rate", type=float, default=10.0, help="Poisson arrivals per second")
-    p.add_argument("--shape", default="auto",
+    p.add_argument("--shape", default="default",
                    help="launch shape 'schedule,variant,knob[,vector[,streams]]' for both precisions "
                         "(an FP32-only vector width falls back to the widest for FP64, an FP32-only knob "
-                        "to -96), or auto (autotuner)")
+                        "to -96), default (the sweeper's own: FP32 slotted compact records, FP64 compact "
+                        "records, 2 octant streams; the autotuner's pick on this workload), or auto "
+                        "(run the autotuner first)")
     p.add_argument("--profile-leg", default="main", choices=["main", "batch"],
                    help="what cudaProfilerStart/Stop bracket (for ncu --profile-from-start off): the main "
                         "leg's timed steps, or steps 4-6 of each batched solve")
@@ -441,9 +443,12 @@ def run_b200(args):
     sw.set_source(q, "isotropic")
     info = sw.schedule_info()
 
-    # Launch shapes: the autotuner's pick per precision (or a fixed shape).
+    # Launch shapes: the sweeper's defaults, the autotuner's pick per
+    # precision, or a fixed shape.
     if args.shape == "auto":
         tuned = {1: sw.autotune(1, 5), 0: sw.autotune(0, 5)}
+    elif args.shape == "default":
+        tuned = {1: sw.shape(1), 0: sw.shape(0)}
     else:
         parts = args.shape.split(",")
         s, v, k = parts[:3]

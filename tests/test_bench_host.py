@@ -54,4 +54,4 @@ def test_defaults_keep_the_timing_rules(monkeypatch):
     monkeypatch.setattr(sys, "argv", ["bench.py"])
     a = bench.parse()
     assert a.gpus == 1 and a.warmup >= 3 and a.steps >= 1
-    assert a.impl == "b200" and a.workload == "kuhn32_s8_g8" and a.shape == "auto"
+    assert a.impl == "b200" and a.workload == "kuhn32_s8_g8" and a.shape == "default"
