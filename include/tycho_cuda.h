@@ -123,6 +123,17 @@ void tycho_mesh_free(tycho_mesh *mesh);
 int tycho_mesh_levels(const tycho_mesh *mesh, int sn_order, uint32_t *tlevel, uint32_t *deps,
                       uint32_t *blevel, uint32_t *n_levels);
 
+/* b-levels of SweepSchedule's constructor (calcDependencies and calcLevels,
+   src/SweepSchedule.cc:107-125, :472-508), no device needed: a face is a
+   child face of (cell, angle) when omega.n > 1e-10, a parent face when
+   omega.n < -1e-10 (interior faces only), and a pair's level is the longest
+   chain of child faces below it.  Unlike the GraphTraverser rule, faces with
+   |omega.n| <= 1e-10 order nothing, so S6's exact ties form no cycle.
+   levels [A * n_cells] in (angle, cell) order (may be NULL); n_levels
+   receives the largest level, as calcLevels returns it. */
+int tycho_mesh_sweep_schedule_levels(const tycho_mesh *mesh, int sn_order, uint32_t *levels,
+                                     uint32_t *n_levels);
+
 /* ---- quadrature: Quadrature::Quadrature (src/Quadrature.cc:150-244) ----- */
 
 /* Fills the 2*sn^2 directions and weights; returns the count or -1. */
@@ -283,15 +294,29 @@ int tycho_sweeper_get_shape(const tycho_sweeper *sw, int precision, tycho_launch
    control words) lives in one file-scope device array of 64 MiB + 256 B,
    which every GPU that loads this library holds until the process exits, so
    at most 16,777,216 cells x angles are accepted (larger: TYCHO_ERR_ARG).
-   The first call on a device looks up that array's device address; make it
-   before any stream capture.  All calls share the array and each leaves its
-   flags behind (a per-call epoch makes them stale; the error and abort words
-   are cleared at the start of every call), so calls that overlap on the GPU
-   race.  The call runs on `stream` (a cudaStream_t, NULL = legacy default
-   stream), synchronizes it and returns TYCHO_ERR_TIMEOUT if a bounded wait
-   gave up.  The sweeper's own buffers and results are not touched. */
+   tycho_sweeper_create looks up that array's device address (once per
+   device and process; the first lookup loads the module holding it), so the
+   call itself maps and loads nothing.  All calls share the array and each
+   leaves its flags behind (a per-call epoch makes them stale; the error and
+   abort words are cleared at the start of every call), so calls that
+   overlap on the GPU race.  The call runs on `stream` (a cudaStream_t, NULL
+   = legacy default stream), reads the error words back and synchronizes
+   `stream` before it returns.  It returns TYCHO_ERR_TIMEOUT if a bounded wait gave up
+   (tycho_sweeper_set_wait_limit).  The sweeper's psi and results are not
+   touched; with a records or direct-records launch shape whose records are
+   stale (new cross sections), it recomputes them in place on `stream`. */
 int tycho_sweeper_sweep_noalloc(tycho_sweeper *sw, int precision, const void *iso, void *psi,
                                 void *stream);
+
+/* Bounded waits of the persistent kernels (dataflow schedule, persistent
+   levels, tycho_sweeper_sweep_noalloc): polls of one completion flag or
+   level barrier before a wait gives up, records the item and face it waited
+   for, makes every warp drain, and the call returns TYCHO_ERR_TIMEOUT with
+   the sweeper still usable.  Default 4,194,304 (seconds of polling).  The
+   reference spins without a bound on the same waits
+   (src/GraphTraverser.cc:518).  0 gives up at the first wait that is not
+   already satisfied: the failure path can be exercised without a hang. */
+int tycho_sweeper_set_wait_limit(tycho_sweeper *sw, uint32_t polls);
 
 /* Device timing of n back-to-back operator applications
    phi_out = D L^{-1} (M S phi_in + Q) in the given precision, on the
@@ -368,6 +393,9 @@ uint64_t tycho_footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, int
    new memory).  This hands the pool's unused memory back to the system;
    it waits for the device first. */
 int tycho_release_cached_memory(int device);
+/* Bytes that pool holds from the system on `device` and bytes of it in use
+   (0 and 0 before the library's first allocation there). */
+int tycho_device_memory(int device, uint64_t *pool_reserved, uint64_t *pool_used);
 
 typedef struct tycho_server tycho_server;
 

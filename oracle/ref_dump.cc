@@ -14,6 +14,19 @@
  *   si <pmesh> <snOrder> <nGroups> <sigmaT.f64> <sigmaS.f64> <source.f64>
  *      <iterMax> <errMax> <out.f64>
  *       SourceIteration::fixedPoint with per-cell sigma_t/sigma_s.
+ *   levels <pmesh> <snOrder> <out.u64>
+ *       SweepSchedule's b-levels: calcDependencies and calcLevels
+ *       (src/SweepSchedule.cc:107-125, :472-508; the +-1e-10 omega.n rule)
+ *       over every angle, (angle, cell) order, followed by their count.
+ *   bench <pmesh> <snOrder> <nGroups> <sigmaT.f64> <qiso.f64> <steps> <warmup> [<phi.f64>]
+ *       times SweeperTraverse::sweep of an isotropic source on all OpenMP
+ *       threads; prints REFBENCH with a hash of the last psi's bytes and,
+ *       given <phi.f64>, writes Util::psiToPhi of that psi.
+ *
+ * The psi hash: the psi array read as 64-bit words x_i, sum of x_i * (2i+1)
+ * modulo 2^64.  Equal hashes of two arrays of the same length mean equal
+ * bits (up to a 2^-64 chance); the sum is order-free, so a caller can form
+ * it in chunks or in parallel.
  */
 #include <cstdio>
 #include <cstdlib>
@@ -36,6 +49,12 @@
 #include "SourceIteration.hh"
 #include "Priorities.hh"
 #include "SweeperTraverse.hh"
+#include "Util.hh"
+/* calcDependencies and calcLevels are file-static in the reference: its
+   SweepSchedule translation unit is compiled into this driver (and left out
+   of the driver's link line) so that the dump calls the reference's own
+   functions. */
+#include "SweepSchedule.cc"
 
 static void dump_u64(const std::string &path, const std::vector<UINT> &v)
 {
@@ -162,7 +181,33 @@ int main(int argc, char **argv)
         dump_f64(argv[10], &psi[0], psi.size());
         return 0;
     }
-    if (mode == "bench" && argc == 9) {
+    if (mode == "levels" && argc == 5) {
+        setup(argv[2], atoi(argv[3]), 1);
+        const UINT na = g_nAngles, nc = g_nCells;
+        std::vector<UINT> angles(na);
+        for (UINT a = 0; a < na; a++) angles[a] = a;
+        std::set<UINT> neighborProcs;
+        calcNeighborProcs(neighborProcs);
+        Mat3<bool> hasChild(na, nc, g_nFacePerCell), hasParent(na, nc, g_nFacePerCell);
+        /* the reference's constructor leaves hasParent unset where
+           calcDependencies writes nothing: start both from false */
+        for (UINT a = 0; a < na; a++)
+            for (UINT c = 0; c < nc; c++)
+                for (UINT f = 0; f < g_nFacePerCell; f++) hasChild(a, c, f) = hasParent(a, c, f) = false;
+        calcDependencies(angles, hasChild, hasParent);
+        Mat2<UINT> cellLevels(na, nc), sideLevels(na, g_tychoMesh->getNSides());
+        cellLevels.setAll(0);
+        sideLevels.setAll(0);
+        const UINT nlevels = calcLevels(cellLevels, sideLevels, hasChild, hasParent, neighborProcs, angles,
+                                        na, g_maxCellsPerStep);
+        std::vector<UINT> out(na * nc + 1);
+        for (UINT a = 0; a < na; a++)
+            for (UINT c = 0; c < nc; c++) out[a * nc + c] = cellLevels(a, c);
+        out[na * nc] = nlevels;
+        dump_u64(argv[4], out);
+        return 0;
+    }
+    if (mode == "bench" && (argc == 9 || argc == 10)) {
         /* bench <pmesh> <snOrder> <nGroups> <sigmaT.f64> <qiso.f64> <steps> <warmup>:
            times the reference's own SweeperTraverse::sweep of an isotropic
            source (phi layout, copied to every angle as the reference's PsiData
@@ -188,9 +233,20 @@ int main(int argc, char **argv)
             if (dt < best) best = dt;
         }
         double checksum = 0.0;
-        for (size_t i = 0; i < psi.size(); i++) checksum += psi[i];
+        uint64_t hash = 0;
+        const uint64_t *words = reinterpret_cast<const uint64_t *>(&psi[0]);
+        for (size_t i = 0; i < psi.size(); i++) {
+            checksum += psi[i];
+            hash += words[i] * (2 * (uint64_t)i + 1);
+        }
+        if (argc == 10) {
+            PhiData phi;
+            Util::psiToPhi(phi, psi);
+            dump_f64(argv[9], &phi[0], phi.size());
+        }
         printf("REFBENCH {\"seconds_per_sweep\": %.9g, \"best_seconds\": %.9g, \"threads\": %d, "
-               "\"steps\": %d, \"checksum\": %.17g}\n", tot / steps, best, (int)g_nThreads, steps, checksum);
+               "\"steps\": %d, \"checksum\": %.17g, \"psi_hash\": \"%016llx\", \"psi_words\": %zu}\n",
+               tot / steps, best, (int)g_nThreads, steps, checksum, (unsigned long long)hash, psi.size());
         return 0;
     }
     fprintf(stderr, "ref_dump: bad arguments\n");

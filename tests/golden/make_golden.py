@@ -1,6 +1,7 @@
 """Regenerates the golden fixtures in this directory from the reference.
 
-Needs the tycho2 source tree (default /root/reference, or $TYCHO2_REF) and the
+Needs the tycho2 source tree ($TYCHO2_REF, default: a tree named reference
+beside this repository) and the
 reference built from it by `make -C oracle ref` (oracle/_ref).  Writes:
 
   gold.psi, cube-208.smesh   the reference's own regression vector and mesh
@@ -20,8 +21,15 @@ reference built from it by `make -C oracle ref` (oracle/_ref).  Writes:
                                          CramerGlu, CramerIntel
                                si_*    : SourceIteration::fixedPoint with the
                                          hat source, per-cell sigma, S4, G=2
+  sweep_schedule_levels.npz  SweepSchedule's b-levels (calcDependencies and
+                             calcLevels with their +-1e-10 omega.n rule) on the
+                             jittered cube above and on an unjittered one
+                             (3^3 hexes on [0,1]^3, where S6 has exact
+                             omega.n ties), S4, S6 and S8:
+                               {jit,flat}_s{4,6,8}  (angle, cell) levels, then
+                                                    their maximum
 
-Run:  python tests/golden/make_golden.py
+Run:  python tests/golden/make_golden.py [--levels-only]
 """
 import hashlib
 import os
@@ -36,7 +44,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-REF = os.environ.get("TYCHO2_REF", "/root/reference")
+REF = os.environ.get("TYCHO2_REF", os.path.join(os.path.dirname(ROOT), "reference"))
 REF_BIN = os.path.join(ROOT, "oracle", "_ref")
 
 
@@ -101,6 +109,22 @@ def kuhn3_fixture(tmp):
     np.savez_compressed(os.path.join(HERE, "kuhn3_ref.npz"), **out)
 
 
+def levels_fixture(tmp):
+    import tycho2_b200 as ty
+
+    out = {}
+    meshes = {"jit": ty.TychoMesh.kuhn_cube(3, 0.05, 2024, 100.0), "flat": ty.TychoMesh.kuhn_cube(3, 0.0, 0, 1.0)}
+    for name, mesh in meshes.items():
+        smesh, pmesh = os.path.join(tmp, name + ".smesh"), os.path.join(tmp, name + ".pmesh")
+        mesh.write_smesh(smesh)
+        run(os.path.join(REF_BIN, "PartitionColumns.x"), "1", "1", smesh, pmesh)
+        for sn in (4, 6, 8):
+            f = os.path.join(tmp, "%s_s%d.u64" % (name, sn))
+            run(os.path.join(REF_BIN, "ref_dump.x"), "levels", pmesh, str(sn), f)
+            out["%s_s%d" % (name, sn)] = np.fromfile(f, np.uint64)
+    np.savez_compressed(os.path.join(HERE, "sweep_schedule_levels.npz"), **out)
+
+
 def main():
     if not os.path.isdir(REF):
         sys.exit("reference tree not found: %s" % REF)
@@ -108,7 +132,9 @@ def main():
     shutil.copyfile(os.path.join(REF, "test", "regression", "gold.psi"), os.path.join(HERE, "gold.psi"))
     shutil.copyfile(os.path.join(REF, "util", "cube-208.smesh"), os.path.join(HERE, "cube-208.smesh"))
     with tempfile.TemporaryDirectory() as tmp:
-        kuhn3_fixture(tmp)
+        if "--levels-only" not in sys.argv:
+            kuhn3_fixture(tmp)
+        levels_fixture(tmp)
 
 
 if __name__ == "__main__":

@@ -5,9 +5,9 @@ CUDA kernels in libtycho_b200.so (C ABI: include/tycho_cuda.h); this package
 is the host-side mirror of the reference's interface over that ABI.
 """
 from ._capi import TychoError, lib  # noqa: F401
-from .sweeper import (BatchSolver, Quadrature, SolveServer, SweeperCuda, TychoMesh, footprint_bytes,  # noqa: F401
-                      release_cached_memory)
+from .sweeper import (BatchSolver, Quadrature, SolveServer, SweeperCuda, TychoMesh, device_memory,  # noqa: F401
+                      footprint_bytes, release_cached_memory)
 from . import problems  # noqa: F401
 
 __all__ = ["TychoError", "TychoMesh", "Quadrature", "SweeperCuda", "BatchSolver", "SolveServer",
-           "footprint_bytes", "release_cached_memory", "problems", "lib"]
+           "device_memory", "footprint_bytes", "release_cached_memory", "problems", "lib"]

@@ -73,6 +73,7 @@ SIGNATURES = {
     "tycho_mesh_tables": (C.c_int, [_P] + [_P] * 10),
     "tycho_mesh_free": (None, [_P]),
     "tycho_mesh_levels": (C.c_int, [_P, C.c_int, _P, _P, _P, _U32P]),
+    "tycho_mesh_sweep_schedule_levels": (C.c_int, [_P, C.c_int, _P, _U32P]),
     "tycho_quadrature": (C.c_int, [C.c_int, _P, _P, _P, _P]),
     "tycho_sweeper_create": (C.c_int, [_P, C.POINTER(SweeperOpts), _PP]),
     "tycho_sweeper_destroy": (None, [_P]),
@@ -85,6 +86,7 @@ SIGNATURES = {
     "tycho_sweeper_levels": (C.c_int, [_P, _P, _P, _P]),
     "tycho_sweeper_launches": (C.c_int, [_P, C.c_int, _U64P]),
     "tycho_release_cached_memory": (C.c_int, [C.c_int]),
+    "tycho_device_memory": (C.c_int, [C.c_int, _U64P, _U64P]),
     "tycho_sweeper_schedule_arrays": (C.c_int, [_P, _U64P, _P, _P]),
     "tycho_sweeper_time_sweeps": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P]),
     "tycho_sweeper_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(LaunchShape),
@@ -92,6 +94,7 @@ SIGNATURES = {
     "tycho_sweeper_configure": (C.c_int, [_P, C.c_int, C.POINTER(LaunchShape)]),
     "tycho_sweeper_get_shape": (C.c_int, [_P, C.c_int, C.POINTER(LaunchShape)]),
     "tycho_sweeper_sweep_noalloc": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+    "tycho_sweeper_set_wait_limit": (C.c_int, [_P, C.c_uint32]),
     "tycho_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, _PP]),
     "tycho_batch_destroy": (None, [_P]),
     "tycho_batch_add": (C.c_int, [_P, _P, C.POINTER(BatchOpts), C.POINTER(C.c_int)]),

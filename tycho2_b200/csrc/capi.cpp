@@ -241,6 +241,23 @@ int tycho_mesh_levels(const tycho_mesh *m, int sn, uint32_t *tlevel, uint32_t *d
     });
 }
 
+int tycho_mesh_sweep_schedule_levels(const tycho_mesh *m, int sn, uint32_t *levels, uint32_t *n_levels)
+{
+    if (!m) return finish(TYCHO_ERR_ARG, "null mesh");
+    return guarded([&] {
+        tycho::Quadrature q;
+        std::string err;
+        const int st = tycho::make_quadrature(sn, q, err);
+        if (st != tycho::kOk) return finish(st, err);
+        std::vector<uint32_t> lev;
+        uint32_t top = 0;
+        tycho::sweep_schedule_levels(m->tab, q, lev, top);
+        if (levels) std::memcpy(levels, lev.data(), lev.size() * 4);
+        if (n_levels) *n_levels = top;
+        return (int)TYCHO_OK;
+    });
+}
+
 int tycho_quadrature(int sn, double *xi, double *eta, double *mu, double *wt)
 {
     tycho::Quadrature q;
@@ -448,6 +465,13 @@ int tycho_sweeper_sweep_noalloc(tycho_sweeper *h, int precision, const void *iso
     return finish(tycho::sweep_noalloc(h->sw, precision, iso, psi, stream, err), err);
 }
 
+int tycho_sweeper_set_wait_limit(tycho_sweeper *h, uint32_t polls)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    h->sw.set_wait_limit(polls);
+    return TYCHO_OK;
+}
+
 int tycho_sweeper_time_sweeps(tycho_sweeper *h, int precision, int n, int flush_l2, double *ms)
 {
     if (!h || !ms) return finish(TYCHO_ERR_ARG, "null argument");
@@ -555,6 +579,13 @@ int tycho_release_cached_memory(int device)
 {
     const cudaError_t e = tycho::dev_trim(device);
     if (e != cudaSuccess) return finish(TYCHO_ERR_CUDA, std::string("releasing cached memory: ") + cudaGetErrorString(e));
+    return TYCHO_OK;
+}
+
+int tycho_device_memory(int device, uint64_t *pool_reserved, uint64_t *pool_used)
+{
+    const cudaError_t e = tycho::dev_pool_usage(device, pool_reserved, pool_used);
+    if (e != cudaSuccess) return finish(TYCHO_ERR_CUDA, std::string("reading the memory pool: ") + cudaGetErrorString(e));
     return TYCHO_OK;
 }
 

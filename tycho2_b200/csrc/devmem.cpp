@@ -73,4 +73,23 @@ cudaError_t dev_trim(int device)
     return e;
 }
 
+cudaError_t dev_pool_usage(int device, uint64_t *reserved, uint64_t *used)
+{
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        pool = g_pool[device];
+    }
+    uint64_t r = 0, u = 0;
+    cudaError_t e = cudaSuccess;
+    if (pool) {
+        e = cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r);
+        if (e == cudaSuccess) e = cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u);
+    }
+    if (reserved) *reserved = r;
+    if (used) *used = u;
+    return e;
+}
+
 }  // namespace tycho

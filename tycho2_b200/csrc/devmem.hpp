@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cstddef>
+#include <cstdint>
 #include <cuda_runtime.h>
 
 namespace tycho {
@@ -30,5 +31,9 @@ void dev_release(T *&p, cudaStream_t s)
 // Returns the pool's unused memory on `device` to the system (waits for the
 // device first).
 cudaError_t dev_trim(int device);
+
+// Bytes the pool of `device` holds from the system and bytes of it in use
+// (both 0 before its first allocation).
+cudaError_t dev_pool_usage(int device, uint64_t *reserved, uint64_t *used);
 
 }  // namespace tycho

@@ -198,4 +198,47 @@ void b_levels(const MeshTables &t, const Quadrature &q, const Schedule &s, std::
     }
 }
 
+void sweep_schedule_levels(const MeshTables &t, const Quadrature &q, std::vector<uint32_t> &lev,
+                           uint32_t &n_levels)
+{
+    constexpr double kTol = 1.e-10;  // src/SweepSchedule.cc:56
+    const uint64_t nc = t.n_cells;
+    const int A = q.n_angles;
+    lev.assign((size_t)A * nc, 0);
+    uint32_t top = 0;
+    #pragma omp parallel for schedule(dynamic) reduction(max : top)
+    for (int a = 0; a < A; ++a) {
+        // bits 0-3 child faces, 4-7 parent faces (interior only)
+        std::vector<unsigned char> rel(nc);
+        std::vector<uint32_t> need(nc), queue;
+        queue.reserve(nc);
+        uint32_t *L = &lev[(size_t)a * nc];
+        for (uint64_t c = 0; c < nc; ++c) {
+            unsigned m = 0, kids = 0;
+            for (int f = 0; f < 4; ++f) {
+                if (t.adj_cell[c * 4 + f] == kNone) continue;
+                const double odn = omega_dot_n(q, a, &t.normal[(c * 4 + f) * 3]);
+                if (odn > kTol) { m |= 1u << f; ++kids; }
+                else if (odn < -kTol) m |= 16u << f;
+            }
+            rel[c] = (unsigned char)m;
+            need[c] = kids;
+            if (kids == 0) queue.push_back((uint32_t)c);
+        }
+        // Leaves first; a cell is visited once its last child is, so its
+        // level is final when it passes it on to its parents.
+        for (size_t h = 0; h < queue.size(); ++h) {
+            const uint32_t c = queue[h];
+            for (int f = 0; f < 4; ++f) {
+                if (!(rel[c] >> (f + 4) & 1u)) continue;
+                const uint64_t p = t.adj_cell[(uint64_t)c * 4 + f];
+                if (L[p] < L[c] + 1) L[p] = L[c] + 1;
+                if (--need[p] == 0) queue.push_back((uint32_t)p);
+            }
+            top = std::max(top, L[c]);
+        }
+    }
+    n_levels = top;
+}
+
 }  // namespace tycho

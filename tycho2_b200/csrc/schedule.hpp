@@ -88,4 +88,15 @@ void tlevel_from_items(Schedule &s, uint64_t n_cells, int n_angles);
 void dependency_counts(const MeshTables &t, const Quadrature &q, std::vector<uint32_t> &deps);
 void b_levels(const MeshTables &t, const Quadrature &q, const Schedule &s, std::vector<uint32_t> &blev);
 
+// b-levels as SweepSchedule's constructor computes them (calcDependencies and
+// calcLevels, src/SweepSchedule.cc:107-125, :472-508): face f is a child face
+// of (cell, angle) when omega.n > 1e-10 and a parent face when omega.n <
+// -1e-10, interior faces only; a cell's level is the longest chain of child
+// faces below it (0 when it has none).  (angle, cell) order; n_levels gets
+// the largest level, as calcLevels returns it.  A cycle cannot stall it: as
+// in the reference, a pair that a cycle keeps waiting is never passed on to
+// its parents.
+void sweep_schedule_levels(const MeshTables &t, const Quadrature &q, std::vector<uint32_t> &lev,
+                           uint32_t &n_levels);
+
 }  // namespace tycho

@@ -14,8 +14,11 @@
 //   * at most kNoAllocMaxItems (cells x angles) items; larger problems are
 //     rejected with TYCHO_ERR_ARG;
 //   * every GPU that loads the library holds the array until the process
-//     exits;
-//   * all calls share the array; calls that overlap on the GPU race.
+//     exits; its device address is looked up when a sweeper is created on
+//     that device (Sweeper::init), which also loads the module that holds
+//     it, so the sweep calls themselves map and load nothing;
+//   * all calls share the array; calls that overlap on the GPU race;
+//   * a call reads its error words back and synchronizes its stream.
 #include <cstring>
 #include <mutex>
 
@@ -75,6 +78,12 @@ __global__ void noalloc_begin_kernel(uint32_t *ctl)
 
 }  // namespace
 
+int noalloc_scratch_prepare(int device, std::string &err)
+{
+    uint32_t *base = nullptr;
+    return scratch_address(device, &base, err);
+}
+
 int Sweeper::sweep_external(int prec, const void *iso, void *psi, uint32_t *done, uint32_t *ctl,
                             cudaStream_t s, std::string &err)
 {
@@ -96,7 +105,7 @@ int Sweeper::sweep_external(int prec, const void *iso, void *psi, uint32_t *done
     df.abort = ctl + 3;
     df.epoch = ctl + 4;
     df.n_items = sched_.n_padded;
-    df.spin_limit = 1u << 22;
+    df.spin_limit = spin_limit_;
     cudaError_t e = cudaSetDevice(device_);
     if (e == cudaSuccess) {
         noalloc_begin_kernel<<<1, 1, 0, s>>>(ctl);
@@ -105,6 +114,27 @@ int Sweeper::sweep_external(int prec, const void *iso, void *psi, uint32_t *done
     if (e != cudaSuccess) {
         err = std::string("no-alloc sweep: ") + cudaGetErrorString(e);
         return kErrCuda;
+    }
+    // The record and direct-record shapes sweep with the per-item records,
+    // which tycho_sweeper_configure allocated; this call never allocates them.
+    // Stale ones (new cross sections) are recomputed in place on `s`.
+    const LaunchShape &sh = shape_[prec ? 1 : 0];
+    if (sh.variant == 2 || sh.variant == 3) {
+        const int k = prec ? 1 : 0;
+        if (!d_rec_[k]) {
+            err = "no-alloc sweep: the launch shape's per-item records were never allocated";
+            return kErrMissing;
+        }
+        if (!rec_valid_[k]) {
+            const LevelArgs rp = level_args(prec, nullptr, nullptr, d_psi_);
+            e = prec ? launch_item_records<float>(rp, sched_.n_padded, d_rec_[1], s)
+                     : launch_item_records<double>(rp, sched_.n_padded, d_rec_[0], s);
+            if (e != cudaSuccess) {
+                err = std::string("no-alloc sweep (records): ") + cudaGetErrorString(e);
+                return kErrCuda;
+            }
+            rec_valid_[k] = true;
+        }
     }
     const int st = launch_dataflow_shape(prec, p, df, s, err);
     if (st != kOk) return st;

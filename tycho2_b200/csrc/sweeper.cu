@@ -114,6 +114,9 @@ int Sweeper::init(std::shared_ptr<const MeshTables> tp, const SweeperOptions &o,
     if (o.device < 0 || o.device >= ndev) { err = "bad device ordinal"; return kErrArg; }
     device_ = o.device;
     TY_CUDA(cudaSetDevice(device_));
+    // the no-alloc sweep's fixed scratch array: resolved here, once per
+    // device, so that tycho_sweeper_sweep_noalloc itself loads nothing
+    TY_CHECK(noalloc_scratch_prepare(device_, err));
     TY_CHECK(make_quadrature(o.sn_order, quad_, err));
     tables_ = std::move(tp);
     nc_ = t.n_cells;
@@ -591,7 +594,7 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         df.abort = d_ctl_ + 3;
         df.epoch = d_ctl_ + 4;
         df.n_items = sched_.n_padded;
-        df.spin_limit = 1u << 22;
+        df.spin_limit = spin_limit_;
         if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
         TY_CUDA(prec ? launch_persist_record<float>(sh.knob, p, d_rec_[1], d_level_off_, sched_.n_levels,
                                                     d_barrier_, df, sh.persist_grid, stream_)
@@ -609,7 +612,7 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         df.abort = d_ctl_ + 3;
         df.epoch = d_ctl_ + 4;
         df.n_items = sched_.n_padded;
-        df.spin_limit = 1u << 22;  // ~2 s of polling
+        df.spin_limit = spin_limit_;
         TY_CUDA(launch_bump_epoch(d_ctl_ + 4, stream_));
         if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
         const void *rec = sh.variant == 4 ? d_crec_[prec ? 1 : 0] : d_rec_[prec ? 1 : 0];
@@ -626,7 +629,7 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         df.abort = d_ctl_ + 3;
         df.epoch = d_ctl_ + 4;
         df.n_items = sched_.n_padded;
-        df.spin_limit = 1u << 22;  // ~4 s of polling with backoff
+        df.spin_limit = spin_limit_;
         TY_CUDA(launch_bump_epoch(d_ctl_ + 4, stream_));
         if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
         TY_CHECK(launch_dataflow_shape(prec, p, df, stream_, err));

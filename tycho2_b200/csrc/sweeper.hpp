@@ -113,6 +113,10 @@ public:
     // The resident psi was written by a sweep of this precision elsewhere.
     void note_psi_precision(int prec) { last_psi_prec_ = prec; }
     uint64_t n_items() const { return sched_.n_padded; }
+    // Polls of one flag or barrier before a persistent kernel's bounded wait
+    // gives up (dataflow, persistent levels and the no-alloc sweep).
+    void set_wait_limit(uint32_t polls) { spin_limit_ = polls; }
+    uint32_t wait_limit() const { return spin_limit_; }
     int solver() const { return solver_; }
 
     const MeshTables &tables() const { return *tables_; }
@@ -159,6 +163,7 @@ private:
     bool fp32_ = false, have_xs_ = false;
     int solver_ = 1;  // SolveKind
     int last_psi_prec_ = -1;
+    uint32_t spin_limit_ = 1u << 22;  // about 2-4 s of polling
 
     cudaStream_t stream_ = nullptr;
     // level schedule on several streams: one per octant group, forked from
@@ -218,5 +223,8 @@ private:
 // in a fixed file-scope device array instead of allocated memory.
 int sweep_noalloc(Sweeper &sw, int precision, const void *iso, void *psi, void *stream,
                   std::string &err);
+// Looks up the no-alloc scratch array's address on `device` (the current
+// device) once per process; the first lookup loads the module holding it.
+int noalloc_scratch_prepare(int device, std::string &err);
 
 }  // namespace tycho

@@ -100,6 +100,15 @@ class TychoMesh:
         check(lib().tycho_mesh_levels(self._h, sn_order, ptr(t), ptr(d), ptr(b), C.byref(nl)))
         return t, d, b, nl.value
 
+    def sweep_schedule_levels(self, sn_order):
+        """SweepSchedule's b-levels (calcLevels, +-1e-10 omega.n rule) in
+        (angle, cell) order and their maximum."""
+        A = 2 * sn_order * sn_order
+        lev = np.empty((A, self.n_cells), np.uint32)
+        nl = C.c_uint32()
+        check(lib().tycho_mesh_sweep_schedule_levels(self._h, sn_order, ptr(lev), C.byref(nl)))
+        return lev, nl.value
+
     def centroids(self):
         t = self.tables()
         return t["coords"][t["cell_nodes"].astype(np.int64)].mean(axis=1)
@@ -265,6 +274,12 @@ class SweeperCuda:
         sh = _capi.LaunchShape(self.SCHEDULES[schedule], self.VARIANTS[variant], knob, vector, streams)
         check(lib().tycho_sweeper_configure(self._h, precision, C.byref(sh)))
 
+    def set_wait_limit(self, polls):
+        """Polls of one flag or level barrier before a persistent kernel's
+        bounded wait gives up (TYCHO_ERR_TIMEOUT); 0 gives up at the first
+        wait that is not already satisfied."""
+        check(lib().tycho_sweeper_set_wait_limit(self._h, int(polls)))
+
     def shape(self, precision):
         sh = _capi.LaunchShape()
         check(lib().tycho_sweeper_get_shape(self._h, precision, C.byref(sh)))
@@ -346,6 +361,13 @@ def release_cached_memory(device=0):
     """Hands the device memory pool's unused memory back to the system (the
     pool keeps what sweepers free for reuse, like a caching allocator)."""
     check(lib().tycho_release_cached_memory(device))
+
+
+def device_memory(device=0):
+    """(bytes the library's memory pool holds on `device`, bytes in use)."""
+    r, u = C.c_uint64(), C.c_uint64()
+    check(lib().tycho_device_memory(device, C.byref(r), C.byref(u)))
+    return r.value, u.value
 
 
 def footprint_bytes(n_cells, sn_order, n_groups, mixed=True, compact=True):
