@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--no-batch", action="store_true", help="skip the batched-instances leg")
     p.add_argument("--batch-instances", type=int, default=256)
     p.add_argument("--no-serve", action="store_true", help="skip the served-solves leg")
+    p.add_argument("--no-parity", action="store_true",
+                   help="skip the oracle checks of the benchmarked solves (run after the timed legs)")
     p.add_argument("--serve-requests", type=int, default=40)
     p.add_argument("--serve-rate", type=float, default=10.0, help="Poisson arrivals per second")
     p.add_argument("--shape", default="default",
@@ -165,50 +167,148 @@ def build_problem(name):
     return w, mesh, st, ss, mat, q
 
 
-def cpu_baseline(w, mesh, st, q, steps=1, warmup=0):
-    """Times the reference's own CPU sweep (oracle/_ref) if present, else the
-    oracle restatement, on all host cores; one full sweep of the workload."""
+REF_BIN = os.path.join(ROOT, "oracle", "_ref")
+
+
+def reference_inputs(workload, d):
+    """The workload's files for the reference, made without the product
+    library: a .smesh from oracle/kuhn_problem.py, turned into the .pmesh the
+    reference's TychoMesh reads by the reference's own PartitionColumns (one
+    partition), and sigma_t / q as raw f64."""
+    from oracle import kuhn_problem as kp
+    mesh, st, q, w = kp.make_workload(workload)
+    pmesh = kp.partition(mesh, d, "m", os.path.join(REF_BIN, "PartitionColumns.x"))
+    st_f, q_f = os.path.join(d, "st.f64"), os.path.join(d, "q.f64")
+    np.ascontiguousarray(st).tofile(st_f)
+    np.ascontiguousarray(q).tofile(q_f)
+    return {"pmesh": pmesh, "st": st_f, "q": q_f, "sn": w["sn"], "groups": w["groups"],
+            "cells": int(mesh[0].shape[0])}
+
+
+def reference_sweep(inp, steps=1, warmup=0, phi_path=None):
+    """Times the reference's own SweeperTraverse::sweep (oracle/_ref/ref_dump.x
+    bench) on every host core it can use: seconds per sweep, thread count and
+    the hash of the last psi's bytes."""
     ncpu = os.cpu_count() or 1
-    ref = os.path.join(ROOT, "oracle", "_ref", "ref_dump.x")
-    nc, A, G = mesh.n_cells, 2 * w["sn"] ** 2, w["groups"]
+    A = 2 * inp["sn"] ** 2
+    env = dict(os.environ, OMP_NUM_THREADS=str(min(ncpu, A)))
+    cmd = [os.path.join(REF_BIN, "ref_dump.x"), "bench", inp["pmesh"], str(inp["sn"]), str(inp["groups"]),
+           inp["st"], inp["q"], str(steps), str(warmup)] + ([phi_path] if phi_path else [])
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("REFBENCH ")]
+    if r.returncode != 0 or not line:
+        raise RuntimeError("reference bench failed: %s" % r.stderr[-500:])
+    return json.loads(line[0][len("REFBENCH "):])
+
+
+def psi_hash(psi, chunk=1 << 25):
+    """The hash ref_dump.x prints for a psi array: its 64-bit words x_i summed
+    as x_i * (2i + 1) modulo 2^64 (equal hashes: equal bits, up to 2^-64)."""
+    words = np.ascontiguousarray(psi).reshape(-1).view(np.uint64)
+    h = np.uint64(0)
+    with np.errstate(over="ignore"):
+        for k in range(0, words.size, chunk):
+            idx = np.arange(k, min(k + chunk, words.size), dtype=np.uint64)
+            h = h + np.sum(words[k:k + idx.size] * (idx * np.uint64(2) + np.uint64(1)), dtype=np.uint64)
+    return "%016x" % int(h)
+
+
+def cpu_baseline(workload, steps=1, warmup=0):
+    """Times the reference's own CPU sweep (oracle/_ref) on all host cores, one
+    full sweep of the workload; falls back to the oracle restatement (on a
+    mesh the product writes) where the reference was not built."""
     with tempfile.TemporaryDirectory() as d:
+        if os.path.exists(os.path.join(REF_BIN, "ref_dump.x")):
+            inp = reference_inputs(workload, d)
+            res = reference_sweep(inp, steps, warmup)
+            upd = inp["cells"] * 2 * inp["sn"] ** 2 * inp["groups"]
+            return {"value": upd / res["seconds_per_sweep"], "unit": "updates/s", "cores": res["threads"],
+                    "kind": "reference",
+                    "sample": "%d full sweep(s) of the workload, SweeperTraverse::sweep" % steps,
+                    "build": "g++ -O3 -fopenmp -ffp-contract=off (oracle/Makefile)",
+                    "seconds_per_sweep": res["seconds_per_sweep"], "psi_hash": res["psi_hash"]}
+        from oracle.oracle import Oracle, OracleMesh
+        w, mesh, st, ss, mat, q = build_problem(workload)
         pm = os.path.join(d, "m.pmesh")
         mesh.write_pmesh(pm)
-        if os.path.exists(ref):
-            np.ascontiguousarray(st).tofile(os.path.join(d, "st.f64"))
-            np.ascontiguousarray(q).tofile(os.path.join(d, "q.f64"))
-            env = dict(os.environ, OMP_NUM_THREADS=str(min(ncpu, A)))
-            r = subprocess.run([ref, "bench", pm, str(w["sn"]), str(G), os.path.join(d, "st.f64"),
-                                os.path.join(d, "q.f64"), str(steps), str(warmup)],
-                               capture_output=True, text=True, env=env, timeout=1800)
-            line = [ln for ln in r.stdout.splitlines() if ln.startswith("REFBENCH ")]
-            if r.returncode != 0 or not line:
-                raise RuntimeError("reference bench failed: %s" % r.stderr[-500:])
-            res = json.loads(line[0][len("REFBENCH "):])
-            return {"value": nc * A * G / res["seconds_per_sweep"], "unit": "updates/s",
-                    "cores": res["threads"], "kind": "reference",
-                    "sample": "%d full sweep(s) of the workload, SweeperTraverse::sweep" % steps,
-                    "seconds_per_sweep": res["seconds_per_sweep"]}
-        from oracle.oracle import Oracle, OracleMesh
+        G = w["groups"]
         o = Oracle(OracleMesh(pm), w["sn"], G)
         t0 = time.perf_counter()
         for _ in range(steps):
-            o.sweep(st, src_iso=np.ascontiguousarray(q))
+            psi = o.sweep(st, src_iso=np.ascontiguousarray(q))
         dt = (time.perf_counter() - t0) / steps
-        return {"value": nc * A * G / dt, "unit": "updates/s", "cores": ncpu, "kind": "port",
+        return {"value": mesh.n_cells * 2 * w["sn"] ** 2 * G / dt, "unit": "updates/s",
+                "cores": os.cpu_count() or 1, "kind": "port",
                 "sample": "%d full sweep(s) of the workload, oracle restatement" % steps,
-                "seconds_per_sweep": dt}
+                "seconds_per_sweep": dt, "psi_hash": psi_hash(psi)}
+
+
+def oracle_phi(params, d, name, restart=20, rtol=1e-12, iter_max=600):
+    """The oracle's converged phi of one problem (its GMRES(restart), to a
+    2-norm residual of rtol relative to the right-hand side), on a mesh and
+    inputs written without the product library where the reference's
+    PartitionColumns was built.  Returns (phi, iterations, seconds)."""
+    from oracle import kuhn_problem as kp
+    from oracle.oracle import Oracle, OracleMesh
+    mesh, st, ss, mat, q = kp.make_problem(**params)
+    pc = os.path.join(REF_BIN, "PartitionColumns.x")
+    if os.path.exists(pc):
+        pm = kp.partition(mesh, d, name, pc)
+    else:
+        from tycho2_b200 import problems
+        pm = os.path.join(d, name + ".pmesh")
+        problems.make_problem(**params)[0].write_pmesh(pm)
+    t0 = time.perf_counter()
+    o = Oracle(OracleMesh(pm), params["sn"], params["groups"])
+    _, phi, it, _ = o.krylov(st, ss, scatter=mat, q_iso=np.ascontiguousarray(q), restart=restart,
+                             iter_max=iter_max, rtol=rtol)
+    return phi, it, time.perf_counter() - t0
+
+
+def rel_l1(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).sum() / np.abs(np.asarray(b)).sum())
+
+
+def parity_c1(dev):
+    """The 3,072-tet S4 G=1 problem: FP64 source iteration on the GPU against
+    the oracle's (same criterion, 1e-10 relative change: bit-identical
+    expected) and the mixed solve against the oracle's converged phi."""
+    import tycho2_b200 as ty
+    from oracle import kuhn_problem as kp
+    from oracle.oracle import Oracle, OracleMesh
+    w = dict(kp.WORKLOADS["kuhn8_s4_g1"])
+    mesh, st, ss, mat, q = ty.problems.make_problem(**w)
+    sw = ty.SweeperCuda(mesh, w["sn"], w["groups"], fp32=True, device=dev)
+    sw.set_cross_sections(st, ss, mat)
+    sw.set_source(q, "isotropic")
+    phi64, _, s64 = sw.solve("si", iter_max=2000, err_max=1e-10, want_psi=False)
+    phim, _, sm = sw.solve("mixed", iter_max=500, err_max=1e-10, want_psi=False)
+    sw.close()
+    with tempfile.TemporaryDirectory() as d:
+        pm = os.path.join(d, "c1.pmesh")
+        mesh.write_pmesh(pm)
+        o = Oracle(OracleMesh(pm), w["sn"], w["groups"])
+        _, phi_o, it_o, _ = o.source_iteration(st, ss, scatter=mat, q_iso=np.ascontiguousarray(q),
+                                               iter_max=2000, err_max=1e-10)
+        phi_k, _, _ = oracle_phi(w, d, "c1k", rtol=1e-13)
+    return {"workload": "kuhn8_s4_g1",
+            "fp64_si_bitexact_vs_oracle_si": bool(np.array_equal(phi64.view(np.uint64), phi_o.view(np.uint64))),
+            "fp64_si_phi_rel_l1_vs_oracle_si": rel_l1(phi64, phi_o),
+            "fp64_si_iterations": s64["iterations"], "oracle_si_iterations": it_o,
+            "fp64_si_phi_rel_l1_vs_oracle_converged": rel_l1(phi64, phi_k),
+            "mixed_phi_rel_l1_vs_oracle_converged": rel_l1(phim, phi_k)}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    w, mesh, st, ss, mat, q = build_problem(args.workload)
-    nc, A, G = mesh.n_cells, 2 * w["sn"] ** 2, w["groups"]
     steps = max(1, min(args.steps, 3))
-    res = cpu_baseline(w, mesh, st, q, steps=steps, warmup=min(args.warmup, 1))
+    res = cpu_baseline(args.workload, steps=steps, warmup=min(args.warmup, 1))
     v = res["value"]
+    from oracle import kuhn_problem as kp
+    w = kp.WORKLOADS[args.workload]
+    nc, A, G = 6 * w["n"] ** 3, 2 * w["sn"] ** 2, w["groups"]
     line = {"metric": METRIC, "value": v, "unit": "updates/s", "n_gpus": args.gpus,
             "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": res["seconds_per_sweep"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -265,7 +365,17 @@ def profiled_traffic(workload, family):
     return None
 
 
-def run_batch_leg(grp, dev, count, seed=4321, profile=False):
+def batch_sample(params, k=8, seed=17):
+    """Indices of the batch members checked against the oracle: the member
+    with the most updates per sweep and k - 1 others drawn with a seed."""
+    cost = [6 * p["n"] ** 3 * 2 * p["sn"] ** 2 * p["groups"] for p in params]
+    big = int(np.argmax(cost))
+    rest = [i for i in range(len(params)) if i != big]
+    pick = np.random.default_rng(seed).choice(rest, size=min(k - 1, len(rest)), replace=False)
+    return [big] + sorted(int(i) for i in pick)
+
+
+def run_batch_leg(grp, dev, count, seed=4321, profile=False, sample=None):
     """Batched uneven instances: `count` problems (n ~ U{4..24}, G ~ U{1,2,4,8},
     S ~ U{4,6,8}, sigma_t ~ lognormal(0, 0.5), c ~ U[0.3, 0.95], q = 1, all
     seeded) solved together, FP64 source iteration vs FP32-sweep source
@@ -275,7 +385,8 @@ def run_batch_leg(grp, dev, count, seed=4321, profile=False):
     from tycho2_b200 import problems
     t0 = time.perf_counter()
     sws, upd = [], 0
-    for p in problems.batch_instances(count, seed=seed + 7919 * grp.rank):
+    params = problems.batch_instances(count, seed=seed + 7919 * grp.rank)
+    for p in params:
         mesh, st, ss, mat, q = problems.make_problem(**p)
         sw = ty.SweeperCuda(mesh, p["sn"], p["groups"], fp32=True, device=dev)
         sw.set_cross_sections(st, ss, mat)
@@ -318,6 +429,9 @@ def run_batch_leg(grp, dev, count, seed=4321, profile=False):
     err = [float(np.abs(m - f).sum() / np.abs(f).sum()) for m, f in zip(phis["mixed"], phis["si"])]
     for sw in sws:
         sw.close()
+    if sample is not None:  # the members the oracle checks after the timed legs
+        for i in batch_sample(params):
+            sample.append((i, params[i], phis["si"][i], phis["mixed"][i]))
     return {"instances": count * grp.world, "updates_per_sweep": upd, "setup_s": setup,
             "kernel": "batch_direct_level_kernel (compact records)",
             "fp64_si": out["si"], "mixed": out["mixed"],
@@ -427,6 +541,60 @@ def run_large_leg(grp, dev, workload="kuhn64_s8_g16"):
             "mixed_vs_fp64_solve_speedup": s64["seconds"] / sm["seconds"]}
 
 
+def run_parity(args, dev, cpu, gpu_psi_hash, phi_c2, sample, large, serve):
+    """Checks of the benchmarked solves against the reference and the oracle,
+    after the timed legs (relative L1 norms, the reference's diff.py norm):
+    c1 the 3,072-tet problem; c2 the benchmark workload: the FP64 sweep's psi
+    bits against the reference's own SweeperTraverse::sweep (hash of psi from
+    ref_dump.x) and the FP64-GMRES and mixed phi against the oracle's GMRES
+    to 1e-12; c3 the 64^3 problem's mixed phi against the FP64 GPU GMRES (its
+    FP64 oracle does not fit host memory); c4 a seeded sample of the batch
+    members (the largest included), FP64 source iteration and mixed phi
+    against the oracle's GMRES to 1e-12; c5 the mixed service against the
+    FP64 service."""
+    out = {"norm": "relative L1", "tolerances": {"fp64_sweep": "bit-identical", "mixed_phi": 1e-8}}
+    try:
+        out["c1"] = parity_c1(dev)
+    except Exception as e:
+        out["c1"] = {"error": str(e)[:200]}
+    c2 = {"workload": args.workload}
+    if gpu_psi_hash and cpu and cpu.get("psi_hash"):
+        c2["fp64_sweep_bitexact_vs_reference"] = gpu_psi_hash == cpu["psi_hash"]
+        c2["psi_hash"] = {"gpu": gpu_psi_hash, "reference": cpu["psi_hash"]}
+    if phi_c2:
+        try:
+            from oracle import kuhn_problem as kp
+            with tempfile.TemporaryDirectory() as d:
+                w = dict(kp.WORKLOADS[args.workload])
+                phi_o, it, sec = oracle_phi(w, d, "c2", restart=20, rtol=1e-12)
+            c2.update({"oracle_gmres_iterations": it, "oracle_seconds": sec,
+                       "fp64_gmres_phi_rel_l1_vs_oracle": rel_l1(phi_c2["fp64_gmres"], phi_o),
+                       "mixed_phi_rel_l1_vs_oracle": rel_l1(phi_c2["mixed"], phi_o)})
+        except Exception as e:
+            c2["error"] = str(e)[:200]
+    out["c2"] = c2
+    if large and "phi_rel_err_l1_mixed_vs_fp64" in large:
+        out["c3"] = {"workload": large["workload"], "mixed_phi_rel_l1_vs_fp64_gpu": large["phi_rel_err_l1_mixed_vs_fp64"]}
+    if sample:
+        members, e64, emx = [], [], []
+        try:
+            with tempfile.TemporaryDirectory() as d:
+                for i, p, phi64, phim in sample:
+                    phi_o, it, sec = oracle_phi(p, d, "m%d" % i, restart=30, rtol=1e-12)
+                    members.append({"index": i, "n": p["n"], "sn": p["sn"], "groups": p["groups"],
+                                    "ratio": p["ratio"], "oracle_seconds": sec,
+                                    "fp64_si": rel_l1(phi64, phi_o), "mixed": rel_l1(phim, phi_o)})
+                    e64.append(members[-1]["fp64_si"])
+                    emx.append(members[-1]["mixed"])
+            out["c4"] = {"members": members, "fp64_si_max_rel_l1_vs_oracle": max(e64),
+                         "mixed_max_rel_l1_vs_oracle": max(emx)}
+        except Exception as e:
+            out["c4"] = {"members": members, "error": str(e)[:200]}
+    if serve and "phi_rel_err_l1_max_mixed_vs_fp64" in serve:
+        out["c5"] = {"mixed_phi_rel_l1_max_vs_fp64_service": serve["phi_rel_err_l1_max_mixed_vs_fp64"]}
+    return out
+
+
 def run_b200(args):
     import torch
     import tycho2_b200 as ty
@@ -498,6 +666,7 @@ def run_b200(args):
 
     # Solve-level check: mixed precision vs FP64 GMRES on the same problem.
     solve = None
+    phi_c2 = {}
     if not args.no_solve:
         tol = w.get("tol", 1e-10)
         phi64, _, s64 = sw.solve("gmres", iter_max=500, err_max=tol, restart=w.get("restart", 20),
@@ -505,6 +674,7 @@ def run_b200(args):
         phim, _, sm = sw.solve("mixed", iter_max=500, err_max=tol, restart=w.get("restart", 20),
                                want_psi=False)
         err = float(np.abs(phim - phi64).sum() / np.abs(phi64).sum())
+        phi_c2 = {"fp64_gmres": phi64, "mixed": phim}
         solve = {"phi_rel_err_l1_mixed_vs_fp64": err, "fp64_gmres_seconds": s64["seconds"],
                  "mixed_seconds": sm["seconds"], "fp64_sweeps": s64["sweeps_fp64"],
                  "mixed_sweeps_fp32": sm["sweeps_fp32"], "mixed_sweeps_fp64": sm["sweeps_fp64"],
@@ -513,6 +683,7 @@ def run_b200(args):
 
     # End to end through the drop-in sweep with host buffers.
     e2e = None
+    gpu_psi_hash = None
     if not args.no_e2e:
         npsi = nc * A * 4 * G
         src_t = torch.empty(npsi, dtype=torch.float64, pin_memory=True)
@@ -531,14 +702,17 @@ def run_b200(args):
         e2e = {"value": grp.sum(updates) / dt, "unit": "updates/s", "h2d_bytes_per_step": npsi * 8,
                "d2h_bytes_per_step": npsi * 8, "path": "tycho_sweeper_sweep (FP64, page-locked host buffers)",
                "seconds_per_step": dt}
+        gpu_psi_hash = psi_hash(psi) if rank == 0 and world == 1 and not args.no_parity else None
         del src_t, psi_t
 
     # the batch and serve legs need the device memory of this instance
     sw.close()
     batch = serve = None
+    sample = []
     if not args.no_batch:
         try:
-            batch = run_batch_leg(grp, dev, args.batch_instances, profile=args.profile_leg == "batch")
+            batch = run_batch_leg(grp, dev, args.batch_instances, profile=args.profile_leg == "batch",
+                                  sample=sample)
         except Exception as e:  # reported, never fatal to the headline line
             batch = {"error": str(e)[:300]}
     if not args.no_serve:
@@ -559,9 +733,13 @@ def run_b200(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu = cpu_baseline(w, mesh, st, q, steps=1)
+            cpu = cpu_baseline(args.workload, steps=1)
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "error": str(e)[:200]}
+
+    parity = None
+    if rank == 0 and world == 1 and not args.no_parity:
+        parity = run_parity(args, dev, cpu, gpu_psi_hash, phi_c2, sample, large, serve)
 
     if rank == 0:
         t32 = profiled_traffic(args.workload, traffic_family(shape32, True))
@@ -588,6 +766,7 @@ def run_b200(args):
                                   "bytes_per_sweep": b64, "kernel_ms_per_sweep": lvl64,
                                   "traffic": t64}},
             "cpu_baseline": cpu,
+            "parity": parity,
             "e2e": e2e,
             "batch": batch,
             "serve": serve,

@@ -55,3 +55,30 @@ def test_defaults_keep_the_timing_rules(monkeypatch):
     a = bench.parse()
     assert a.gpus == 1 and a.warmup >= 3 and a.steps >= 1
     assert a.impl == "b200" and a.workload == "kuhn32_s8_g8" and a.shape == "default"
+
+
+def test_reference_inputs_are_written_without_the_product(tmp_path):
+    """The reference arm's mesh and inputs (oracle/kuhn_problem.py) equal the
+    product's byte for byte: the same .smesh, sigma_t, sigma_s and q."""
+    import numpy as np
+    import tycho2_b200 as ty
+    from oracle import kuhn_problem as kp
+    for n, jitter, seed in ((3, 0.05, 7), (4, 0.0, 0), (5, 0.05, 1234)):
+        a, b = str(tmp_path / "a.smesh"), str(tmp_path / "b.smesh")
+        kp.write_smesh(a, kp.kuhn_cube(n, jitter, seed))
+        ty.TychoMesh.kuhn_cube(n, jitter, seed, 1.0).write_smesh(b)
+        assert open(a, "rb").read() == open(b, "rb").read()
+    for p in ty.problems.batch_instances(4, seed=4321) + [ty.problems.WORKLOADS["kuhn8_s4_g1"]]:
+        ours, theirs = kp.make_problem(**p)[1:], ty.problems.make_problem(**p)[1:]
+        for x, y in zip(ours, theirs):
+            assert (x is None and y is None) or np.array_equal(x, y)
+
+
+def test_psi_hash_is_the_weighted_word_sum():
+    import numpy as np
+    rng = np.random.default_rng(3)
+    psi = rng.normal(size=1000)
+    words = [int(x) for x in psi.view(np.uint64)]
+    want = sum(x * (2 * i + 1) for i, x in enumerate(words)) % (1 << 64)
+    assert bench.psi_hash(psi) == "%016x" % want
+    assert bench.psi_hash(psi, chunk=7) == "%016x" % want

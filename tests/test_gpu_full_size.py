@@ -1,0 +1,92 @@
+"""The benchmark's own workload checked at full size: 32^3 hexes x 6 =
+196,608 tets, +-0.05h jitter, S8 (128 directions), G=8, lognormal(0, 0.5)
+sigma_t, downscatter rows summing to 0.6 sigma_t, q = 1 in the central 1/8.
+
+* One FP64 sweep psi = L^-1 q through the drop-in entry point is
+  bit-identical to the reference's own SweeperTraverse::sweep (ref_dump.x,
+  built from the reference's sources, on a mesh written by
+  oracle/kuhn_problem.py and partitioned by the reference's PartitionColumns),
+  compared through a hash of psi's 64-bit words; without the reference build,
+  to the oracle's sweep bit for bit.
+* FP64 GMRES(20) phi to 1e-12 within 1e-10 relative L1 of the oracle's
+  GMRES(20) to 1e-12 (the iterates differ in rounding: the inner products
+  sum in a different order), and the mixed-precision solve to 1e-10 within
+  1e-8 of it.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, bits_equal, rel_l1
+
+pytestmark = pytest.mark.gpu
+
+WORKLOAD = "kuhn32_s8_g8"
+
+
+@pytest.fixture(scope="module")
+def c2(built, tmp_path_factory):
+    sys.path.insert(0, ROOT)
+    from oracle import kuhn_problem as kp
+    d = str(tmp_path_factory.mktemp("c2"))
+    w = dict(kp.WORKLOADS[WORKLOAD])
+    mesh, st, ss, mat, q = kp.make_problem(**w)
+    pc = os.path.join(ROOT, "oracle", "_ref", "PartitionColumns.x")
+    if os.path.exists(pc):
+        pmesh = kp.partition(mesh, d, "c2", pc)
+    else:
+        import tycho2_b200 as ty
+        pmesh = os.path.join(d, "c2.pmesh")
+        ty.problems.make_problem(**w)[0].write_pmesh(pmesh)
+    return dict(w=w, st=st, ss=ss, mat=mat, q=q, pmesh=pmesh, dir=d)
+
+
+def _sweeper(c2):
+    import tycho2_b200 as ty
+    w = c2["w"]
+    mesh = ty.TychoMesh.read_pmesh(c2["pmesh"])
+    sw = ty.SweeperCuda(mesh, w["sn"], w["groups"], fp32=True)
+    sw.set_cross_sections(c2["st"], c2["ss"], c2["mat"])
+    sw.set_source(c2["q"], "isotropic")
+    return sw
+
+
+def test_c2_fp64_sweep_bit_identical_to_reference(c2):
+    import bench
+    sw = _sweeper(c2)
+    src = np.empty(sw.psi_shape)
+    src[:] = c2["q"][:, None, :, :]
+    psi = np.empty(sw.psi_shape)
+    sw.sweep(psi, src)
+    sw.close()
+    del src
+    ref_dump = os.path.join(ROOT, "oracle", "_ref", "ref_dump.x")
+    if os.path.exists(ref_dump):
+        st_f, q_f = os.path.join(c2["dir"], "st.f64"), os.path.join(c2["dir"], "q.f64")
+        c2["st"].tofile(st_f)
+        np.ascontiguousarray(c2["q"]).tofile(q_f)
+        res = bench.reference_sweep({"pmesh": c2["pmesh"], "st": st_f, "q": q_f, "sn": c2["w"]["sn"],
+                                     "groups": c2["w"]["groups"]}, steps=1, warmup=0)
+        assert res["psi_words"] == psi.size
+        assert bench.psi_hash(psi) == res["psi_hash"]
+    else:
+        from oracle.oracle import Oracle, OracleMesh
+        o = Oracle(OracleMesh(c2["pmesh"]), c2["w"]["sn"], c2["w"]["groups"])
+        assert bits_equal(psi, o.sweep(c2["st"], src_iso=np.ascontiguousarray(c2["q"])))
+
+
+def test_c2_gmres_phi_matches_oracle(c2):
+    from oracle.oracle import Oracle, OracleMesh
+    sw = _sweeper(c2)
+    phi64, _, s64 = sw.solve("gmres", iter_max=500, err_max=1e-12, restart=20, want_psi=False)
+    phim, _, sm = sw.solve("mixed", iter_max=500, err_max=1e-10, restart=20, want_psi=False)
+    sw.close()
+    assert s64["final_error"] <= 1e-12 and sm["final_error"] <= 1e-10
+    o = Oracle(OracleMesh(c2["pmesh"]), c2["w"]["sn"], c2["w"]["groups"])
+    _, phi_o, _, _ = o.krylov(c2["st"], c2["ss"], c2["mat"], q_iso=np.ascontiguousarray(c2["q"]), restart=20,
+                              iter_max=200, rtol=1e-12)
+    assert rel_l1(phi64, phi_o) <= 1e-10
+    assert rel_l1(phim, phi_o) <= 1e-8
