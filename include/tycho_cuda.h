@@ -190,22 +190,34 @@ typedef struct tycho_solve_opts {
     int iter_max;      /* SI steps / Krylov iterations (deck key iterMax) */
     double err_max;    /* SI: L1 relative change; Krylov: relative residual (errMax) */
     int restart;       /* GMRES restart length */
-    double inner_tol;  /* mixed: relative tolerance of each FP32 correction solve */
-    int refine_max;    /* mixed: maximum FP64 refinement steps */
+    double inner_tol;  /* mixed: relative tolerance of the first FP32 solve (at most 1e-6) */
+    int refine_max;    /* mixed: maximum correction solves */
 } tycho_solve_opts;
 
 typedef struct tycho_solve_stats {
     int iterations;        /* SI steps or total Krylov iterations */
     int sweeps_fp64;       /* FP64 sweeps performed */
     int sweeps_fp32;       /* FP32 sweeps performed */
-    int refinements;       /* mixed: FP64 refinement steps */
+    int refinements;       /* mixed: correction solves */
     double final_error;    /* SI: last L1 relative change; Krylov: relative residual */
     double seconds;        /* device time of the solve */
 } tycho_solve_stats;
 
 /* SweeperAbstract::solve (src/SweeperTraverse.cc:65-74): psi starts at 0 and
    the chosen outer iteration runs on the device.  phi_out / psi_out (host,
-   may be NULL) receive the result; psi stays resident on the device. */
+   may be NULL) receive the result; psi stays resident on the device.
+   GMRES ends with the FP64 sweep psi = L^{-1}(M S phi + Q) of the reference's
+   krylov (src/SourceIteration.cc:254-260) when psi_out is given; without it
+   phi is the GMRES iterate and that sweep is skipped.
+   TYCHO_MIXED_GMRES: x solves (I - K32) x = D L32^{-1} Q by FP32-sweep
+   GMRES (FP64 vectors) to min(inner_tol, 1e-6); then r = T64(x) - x with one
+   FP64 sweep (T = D L^{-1}(Q + M S .)), (I - K32) d = r by FP32-sweep GMRES,
+   x += d.  The residual after a correction comes from the GMRES Arnoldi
+   relation, without a sweep, when d is small enough that the FP32
+   operator's error on it stays below a tenth of err_max; otherwise from
+   another FP64 sweep.  Stops at ||r|| <= err_max ||D L32^{-1} Q||; with
+   psi_out one FP64 sweep at the final phi supplies psi (unless the last
+   residual sweep was at it). */
 int tycho_sweeper_solve(tycho_sweeper *sw, const tycho_solve_opts *opts, double *phi_out,
                         double *psi_out, tycho_solve_stats *stats);
 

@@ -851,7 +851,7 @@ int Sweeper::ensure_krylov(int m, std::string &err)
 // on the host, stop when the residual estimate <= rtol ||b||; the true
 // residual is recomputed at each restart.
 int Sweeper::gmres(int prec, const double *b, double *x, int m, double rtol, int iter_max, int &its,
-                   double &rnorm, SolveStats &st, std::string &err)
+                   double &rnorm, SolveStats &st, std::string &err, double *r_out)
 {
     TY_CHECK(ensure_krylov(m, err));
     const uint64_t n = phi_size();
@@ -861,12 +861,19 @@ int Sweeper::gmres(int prec, const double *b, double *x, int m, double rtol, int
     TY_CUDA(multi_dot(b, b, n, 1, n, red_, stream_));
     const double bnorm = std::sqrt(red_.host[0]);
     rnorm = bnorm;
-    if (bnorm == 0.0) return kOk;
+    if (bnorm == 0.0) {
+        if (r_out) TY_CUDA(cudaMemsetAsync(r_out, 0, sizeof(double) * n, stream_));
+        return kOk;
+    }
     TY_CUDA(cudaMemcpyAsync(V, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
     double beta = bnorm;
     std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
     for (;;) {
-        if (beta <= rtol * bnorm || its >= iter_max) { rnorm = beta; break; }
+        if (beta <= rtol * bnorm || its >= iter_max) {
+            rnorm = beta;
+            if (r_out) TY_CUDA(cudaMemcpyAsync(r_out, V, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+            break;
+        }
         TY_CUDA(axpby(1.0 / beta, V, 0.0, V, n, stream_));
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
@@ -916,6 +923,21 @@ int Sweeper::gmres(int prec, const double *b, double *x, int m, double rtol, int
         TY_CUDA(multi_axpy(x, V, n, d_h_, k, n, stream_));
         if (converged || its >= iter_max) {
             rnorm = est;
+            if (r_out) {
+                // beta e1 - H y = Omega^T (0, ..., 0, g_k): the rotations
+                // undone in reverse order; r = V_{0..k} z
+                std::vector<double> negz(k + 1, 0.0);
+                double zj1 = g[k];
+                for (int j = k - 1; j >= 0; --j) {
+                    negz[j + 1] = -(cs[j] * zj1);
+                    zj1 = -sn[j] * zj1;
+                }
+                negz[0] = -zj1;
+                if (k == 0) negz[0] = -g[0];
+                TY_CUDA(cudaMemsetAsync(r_out, 0, sizeof(double) * n, stream_));
+                TY_CUDA(cudaMemcpyAsync(d_h_, negz.data(), sizeof(double) * (k + 1), cudaMemcpyHostToDevice, stream_));
+                TY_CUDA(multi_axpy(r_out, V, n, d_h_, k + 1, n, stream_));
+            }
             TY_CUDA(cudaStreamSynchronize(stream_));
             break;
         }
@@ -961,7 +983,8 @@ int Sweeper::solve(const SolveOptions &o, double *phi_out, double *psi_out, Solv
         st.final_error = error;
         result = d_phi_;
     } else if (o.method == 1) {
-        // SourceIteration::krylov: b = D L^{-1} Q, GMRES, psi = L^{-1}(MS phi + Q).
+        // SourceIteration::krylov: b = D L^{-1} Q, GMRES, psi = L^{-1}(MS phi + Q)
+        // (the last sweep only when psi is asked for; phi is then that psi's).
         TY_CHECK(apply(0, nullptr, true, d_r_, nullptr, err));
         st.sweeps_fp64++;
         int its = 0;
@@ -969,39 +992,79 @@ int Sweeper::solve(const SolveOptions &o, double *phi_out, double *psi_out, Solv
         TY_CHECK(gmres(0, d_r_, d_phi_, o.restart, o.err_max, o.iter_max, its, rn, st, err));
         TY_CUDA(multi_dot(d_r_, d_r_, n, 1, n, red_, stream_));
         const double bnorm = std::sqrt(red_.host[0]);
-        TY_CHECK(apply(0, d_phi_, true, d_tmp_, nullptr, err));
-        st.sweeps_fp64++;
         st.iterations = its;
         st.final_error = bnorm > 0 ? rn / bnorm : 0.0;
-        result = d_tmp_;
-    } else if (o.method == 2) {
-        // FP64 iterative refinement: r = T(phi) - phi with one FP64 sweep,
-        // correction (I - K32) delta = r by FP32-sweep GMRES, phi += delta.
-        if (!fp32_) { err = "mixed precision needs a sweeper created with fp32"; return kErrArg; }
-        if (d_qang_) { err = "mixed precision takes an isotropic fixed source"; return kErrArg; }
-        TY_CUDA(cudaMemsetAsync(d_phi_, 0, sizeof(double) * n, stream_));
-        double bnorm = 0.0, rnorm = 0.0;
-        int ref = 0;
-        for (;;) {
+        result = d_phi_;
+        if (psi_out) {  // psi = L^{-1}(M S phi + Q), src/SourceIteration.cc:254-260
             TY_CHECK(apply(0, d_phi_, true, d_tmp_, nullptr, err));
             st.sweeps_fp64++;
-            TY_CUDA(cudaMemcpyAsync(d_r_, d_tmp_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
-            TY_CUDA(axpby(-1.0, d_phi_, 1.0, d_r_, n, stream_));
-            TY_CUDA(multi_dot(d_r_, d_r_, n, 1, n, red_, stream_));
-            rnorm = std::sqrt(red_.host[0]);
-            if (ref == 0) bnorm = rnorm;
-            if (rnorm <= o.err_max * bnorm || ref >= o.refine_max || st.iterations >= o.iter_max) break;
+            result = d_tmp_;
+        }
+    } else if (o.method == 2) {
+        // FP64 iterative refinement around FP32-sweep GMRES, with as few FP64
+        // sweeps as the FP32 sweep's accuracy allows:
+        //  1. x = 0 refined against the FP32 sweep of the fixed source
+        //     b32 = D L32^{-1} Q: (I - K32) x = b32 to min(inner_tol, 1e-6);
+        //  2. r = T64(x) - x, one FP64 sweep (T = D L^{-1} (Q + M S .));
+        //  3. (I - K32) d = r by GMRES, x += d; the new residual r - (I - K32) d
+        //     comes from the GMRES Arnoldi relation, without a sweep, when the
+        //     FP32 operator's error on d (at most kFp32OpErr ||d||) is below a
+        //     tenth of the tolerance; otherwise back to 2.
+        // Stop when ||r|| <= errMax ||b32||.  psi_out: one more FP64 sweep at
+        // the final x unless the last step was one.
+        if (!fp32_) { err = "mixed precision needs a sweeper created with fp32"; return kErrArg; }
+        if (d_qang_) { err = "mixed precision takes an isotropic fixed source"; return kErrArg; }
+        constexpr double kFp32OpErr = 2e-6;  // relative error of one FP32 operator application
+        TY_CUDA(cudaMemsetAsync(d_phi_, 0, sizeof(double) * n, stream_));
+        TY_CHECK(apply(1, nullptr, true, d_r_, nullptr, err));
+        st.sweeps_fp32++;
+        TY_CUDA(multi_dot(d_r_, d_r_, n, 1, n, red_, stream_));
+        const double bnorm = std::sqrt(red_.host[0]);
+        double rnorm = bnorm;
+        int ref = 0;
+        bool at_t64 = false;  // d_tmp_ holds T64(x) and psi is its FP64 sweep
+        if (bnorm > 0.0) {
             int its = 0;
             double rn = 0;
-            TY_CHECK(gmres(1, d_r_, d_tmp_, o.restart, o.inner_tol, o.iter_max - st.iterations, its, rn, st, err));
+            TY_CHECK(gmres(1, d_r_, d_phi_, o.restart, std::min(o.inner_tol, 1e-6), o.iter_max, its, rn, st, err));
             st.iterations += its;
-            TY_CUDA(axpby(1.0, d_tmp_, 1.0, d_phi_, n, stream_));
-            ++ref;
+            bool need_true = true;
+            for (;;) {
+                if (need_true) {
+                    TY_CHECK(apply(0, d_phi_, true, d_tmp_, nullptr, err));
+                    st.sweeps_fp64++;
+                    at_t64 = true;
+                    TY_CUDA(cudaMemcpyAsync(d_r_, d_tmp_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+                    TY_CUDA(axpby(-1.0, d_phi_, 1.0, d_r_, n, stream_));
+                    TY_CUDA(multi_dot(d_r_, d_r_, n, 1, n, red_, stream_));
+                    rnorm = std::sqrt(red_.host[0]);
+                }
+                if (rnorm <= o.err_max * bnorm || ref >= o.refine_max || st.iterations >= o.iter_max) break;
+                const double rtol = std::max(0.5 * o.err_max * bnorm / rnorm, 1e-8);
+                its = 0;
+                TY_CHECK(gmres(1, d_r_, d_tmp_, o.restart, rtol, o.iter_max - st.iterations, its, rn, st, err,
+                               d_r_));
+                at_t64 = false;
+                st.iterations += its;
+                TY_CUDA(axpby(1.0, d_tmp_, 1.0, d_phi_, n, stream_));
+                ++ref;
+                TY_CUDA(multi_dot(d_tmp_, d_tmp_, n, 1, n, red_, stream_));
+                const double dnorm = std::sqrt(red_.host[0]);
+                need_true = kFp32OpErr * dnorm > 0.1 * o.err_max * bnorm;
+                if (!need_true) {
+                    TY_CUDA(multi_dot(d_r_, d_r_, n, 1, n, red_, stream_));
+                    rnorm = std::sqrt(red_.host[0]);
+                }
+            }
         }
-        // psi is the FP64 sweep of the last residual; its phi is T(phi) (d_tmp_).
+        if (!at_t64 && psi_out) {
+            TY_CHECK(apply(0, d_phi_, true, d_tmp_, nullptr, err));
+            st.sweeps_fp64++;
+            at_t64 = true;
+        }
         st.refinements = ref;
         st.final_error = bnorm > 0 ? rnorm / bnorm : 0.0;
-        result = d_tmp_;
+        result = at_t64 ? d_tmp_ : d_phi_;
     } else {
         err = "unknown method";
         return kErrArg;

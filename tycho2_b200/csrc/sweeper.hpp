@@ -144,8 +144,10 @@ private:
     LevelArgs level_args(int prec, const void *iso, const double *qang, void *psi) const;
     int launch_dataflow_shape(int prec, const LevelArgs &p, const DataflowArgs &df, cudaStream_t s,
                               std::string &err);
+    // r_out (nullable): on return b - (I - K) x from the last cycle's Arnoldi
+    // relation, without another sweep.
     int gmres(int prec, const double *b, double *x, int restart, double rtol, int iter_max,
-              int &its, double &rnorm, SolveStats &st, std::string &err);
+              int &its, double &rnorm, SolveStats &st, std::string &err, double *r_out = nullptr);
     int ensure_krylov(int restart, std::string &err);
     // The drop-in sweep with its host copies overlapped: angle chunks (0 or 1:
     // one copy in, one sweep, one copy out) and the pipelined form.
