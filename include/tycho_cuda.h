@@ -353,13 +353,20 @@ typedef struct tycho_batch tycho_batch;
 typedef struct tycho_batch_opts {
     int method;       /* TYCHO_SOURCE_ITERATION (FP64 throughout) or
                          TYCHO_MIXED_GMRES's batched form: FP32-sweep source
-                         iteration on the correction inside FP64 refinement */
+                         iteration on phi from 0 to min(inner_tol, 1e-6),
+                         then FP64 residuals r = T64(phi) - phi with FP32
+                         source iteration on the correction; a correction
+                         small enough that the FP32 operator's error on it
+                         is below a tenth of err_max ends the solve without
+                         another FP64 sweep (phi += d when the result is
+                         read; psi is then not an FP64 sweep of phi) */
     int iter_max;     /* sweeps of the solve (FP32 inner sweeps included) */
     double err_max;   /* stop: L1 relative change of phi over one FP64 sweep
-                         (SourceIteration.cc:167-175) */
+                         (SourceIteration.cc:167-175), or the same bound on
+                         the residual after the last correction */
     double inner_tol; /* mixed: inner stop, L1 relative change of the correction */
-    int inner_max;    /* mixed: inner sweeps per refinement */
-    int refine_max;   /* mixed: refinements */
+    int inner_max;    /* mixed: inner sweeps per correction */
+    int refine_max;   /* mixed: corrections */
 } tycho_batch_opts;
 
 /* ipw32 / ipw64: items per warp of the FP32 / FP64 wavefront kernels (8, 16,

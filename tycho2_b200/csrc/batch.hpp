@@ -67,7 +67,7 @@ public:
     int size() const { return (int)members_.size(); }
 
 private:
-    enum State { kRunSI = 0, kRunOuter = 1, kRunInner = 2, kDone = 3 };
+    enum State { kRunSI = 0, kRunOuter = 1, kRunInner = 2, kDone = 3, kRunFirst = 4 };
     struct Member {
         int id = 0;
         Sweeper *sw = nullptr;
@@ -78,6 +78,9 @@ private:
         double *r = nullptr, *d = nullptr, *k = nullptr;  // residual, correction, K delta
         double *cur = nullptr, *nxt = nullptr;            // SI: phi and the next iterate
         bool accept = false;
+        bool accept_at_result = false;  // mixed, finished after an inner solve: phi += d on read
+        double phi_l1 = 0.0;            // mixed: ||T64(phi)||_1 of the last FP64 pass
+        const double *res = nullptr;    // mixed: where the result lives once done
         int inner_its = 0;
         uint64_t updates = 0;                             // per sweep
         uint32_t shift = 0;                               // global level of the member's level 0
