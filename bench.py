@@ -681,29 +681,49 @@ def run_b200(args):
                  "fp64_residual": s64["final_error"], "mixed_residual": sm["final_error"],
                  "tol": tol, "speedup": s64["seconds"] / sm["seconds"]}
 
-    # End to end through the drop-in sweep with host buffers.
+    # End to end through the drop-in sweep with host buffers, in the buffer
+    # kinds the reference hands it: SweeperTraverse::solve passes the
+    # sweeper's own psi (c_psi, which the SweeperCuda adapter page-locks) and
+    # fixedPoint's local totalSource (pageable); also both page-locked and
+    # both pageable, for context.
     e2e = None
     gpu_psi_hash = None
     if not args.no_e2e:
         npsi = nc * A * 4 * G
+        n_e2e = max(1, min(args.steps, 3))
+
+        def timed(src, psi):
+            src[:] = q[:, None, :, :]
+            sw.sweep(psi, src)
+            grp.barrier()
+            t0 = time.perf_counter()
+            for _ in range(n_e2e):
+                sw.sweep(psi, src)
+            grp.barrier()
+            return grp.max((time.perf_counter() - t0) / n_e2e)
+
+        legs = {}
+        src = np.empty(sw.psi_shape)
+        psi = np.empty(sw.psi_shape)
+        ty.lib().tycho_host_register(psi.ctypes.data, psi.nbytes)  # the adapter's c_psi
+        legs["adapter"] = timed(src, psi)
+        if rank == 0 and world == 1 and not args.no_parity:
+            gpu_psi_hash = psi_hash(psi)
+        ty.lib().tycho_host_unregister(psi.ctypes.data)
+        legs["pageable"] = timed(src, psi)
+        del src, psi
         src_t = torch.empty(npsi, dtype=torch.float64, pin_memory=True)
         psi_t = torch.empty(npsi, dtype=torch.float64, pin_memory=True)
-        src = src_t.numpy().reshape(sw.psi_shape)
-        src[:] = q[:, None, :, :]
-        psi = psi_t.numpy().reshape(sw.psi_shape)
-        sw.sweep(psi, src)
-        n_e2e = max(1, min(args.steps, 3))
-        grp.barrier()
-        t0 = time.perf_counter()
-        for _ in range(n_e2e):
-            sw.sweep(psi, src)
-        grp.barrier()
-        dt = grp.max((time.perf_counter() - t0) / n_e2e)
-        e2e = {"value": grp.sum(updates) / dt, "unit": "updates/s", "h2d_bytes_per_step": npsi * 8,
-               "d2h_bytes_per_step": npsi * 8, "path": "tycho_sweeper_sweep (FP64, page-locked host buffers)",
-               "seconds_per_step": dt}
-        gpu_psi_hash = psi_hash(psi) if rank == 0 and world == 1 and not args.no_parity else None
+        legs["pinned"] = timed(src_t.numpy().reshape(sw.psi_shape), psi_t.numpy().reshape(sw.psi_shape))
         del src_t, psi_t
+        dt = legs["adapter"]
+        e2e = {"value": grp.sum(updates) / dt, "unit": "updates/s", "h2d_bytes_per_step": npsi * 8,
+               "d2h_bytes_per_step": npsi * 8,
+               "path": "tycho_sweeper_sweep (FP64): psi page-locked as the SweeperCuda adapter locks its c_psi, "
+                       "source pageable as fixedPoint's totalSource",
+               "seconds_per_step": dt,
+               "by_buffers": {k: {"updates_per_s": grp.sum(updates) / v, "seconds_per_step": v}
+                              for k, v in legs.items()}}
 
     # the batch and serve legs need the device memory of this instance
     sw.close()

@@ -179,11 +179,22 @@ int tycho_sweeper_set_source(tycho_sweeper *sw, int kind, const double *q);
 
 /* The drop-in SweeperAbstract::sweep(psi, source): psi = L^{-1} source for
    an angular source in psi layout, vacuum boundaries.  Host buffers; the
-   copies in and out are part of the call.  With page-locked (pinned or
-   registered) buffers and from 64 MiB of psi (NoPivot), the copies and the
-   sweep run in angle chunks on three streams so that uploads, downloads and
-   the sweep overlap. */
+   copies in and out are part of the call.  From 64 MiB of psi (NoPivot),
+   when at least one of the two buffers is page-locked (pinned, or
+   registered with tycho_host_register), the copies and the sweep run in
+   angle chunks on three streams so that uploads, downloads and the sweep
+   overlap; a pageable buffer's copies are staged by the calling thread
+   while the rest runs beside them. */
 int tycho_sweeper_sweep(tycho_sweeper *sw, const double *source, double *psi);
+
+/* Page-locks (cudaHostRegister, portable) / releases a host buffer that the
+   caller keeps for many sweeps, such as the PsiData arrays a sweeper owns
+   (SweeperAbstract's c_psi and c_source, src/SweeperAbstract.hh:68-69, host
+   `new double[]`, src/PsiData.hh:94-103).  The buffer must be unregistered
+   before it is freed.  No counterpart in the reference, which never copies
+   to a device. */
+int tycho_host_register(void *p, size_t bytes);
+int tycho_host_unregister(void *p);
 
 typedef struct tycho_solve_opts {
     int method;        /* tycho_method */

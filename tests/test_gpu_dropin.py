@@ -37,20 +37,41 @@ GaussElim NoPivot
 """
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(BIN, "sweep_cuda.x")),
-                    reason="reference-side binding not built (needs the tycho2 tree at build time)")
-@pytest.mark.parametrize("si", ["true", "false"])
-def test_reference_driver_with_gpu_sweeper_reproduces_gold(workdir, si):
-    d = os.path.join(str(workdir), "dropin_" + si)
+def _run_driver(workdir, name, si, gauss="NoPivot", extra=()):
+    d = os.path.join(str(workdir), name)
     os.makedirs(d, exist_ok=True)
     subprocess.run([os.path.join(BIN, "PartitionColumns.x"), "1", "1",
                     os.path.join(GOLDEN, "cube-208.smesh"), os.path.join(d, "c.pmesh")],
                    check=True, stdout=subprocess.DEVNULL)
     with open(os.path.join(d, "gold.deck"), "w") as f:
-        f.write(DECK.format(si=si))
-    r = subprocess.run([os.path.join(BIN, "sweep_cuda.x"), "c.pmesh", "gold.deck"], cwd=d,
+        f.write(DECK.format(si=si).replace("GaussElim NoPivot", "GaussElim " + gauss))
+    r = subprocess.run([os.path.join(BIN, "sweep_cuda.x"), "c.pmesh", "gold.deck", *extra], cwd=d,
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
-    psi = np.fromfile(os.path.join(d, "out.psi"))[8:]
+    return np.fromfile(os.path.join(d, "out.psi"))[8:], r.stdout
+
+
+NOT_BUILT = "reference-side binding not built (needs the tycho2 tree at build time)"
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(BIN, "sweep_cuda.x")), reason=NOT_BUILT)
+@pytest.mark.parametrize("si", ["true", "false"])
+def test_reference_driver_with_gpu_sweeper_reproduces_gold(workdir, si):
+    psi, _ = _run_driver(workdir, "dropin_" + si, si)
     gold = gold_psi().ravel()
     assert rel_l1(psi, gold) < 1e-10 and rel_linf(psi, gold) < 1e-10
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(BIN, "sweep_cuda.x")), reason=NOT_BUILT)
+@pytest.mark.parametrize("gauss", ["NoPivot", "Original", "CramerGlu", "CramerIntel"])
+def test_reference_fixed_point_over_gpu_sweep_reproduces_gold(workdir, gauss):
+    """The reference's own SourceIteration::fixedPoint (its psiToPhi,
+    calcTotalSource and L1 stopping rule on the host) calls
+    SweeperCuda::sweep with the reference's PsiData buffers, as
+    SweeperTraverse::solve calls SweeperTraverse::sweep; every deck value of
+    GaussElim is parsed and reaches the GPU solver.  gold.psi within
+    test/diff.py's 1e-10, in the gold run's 34 iterations."""
+    psi, out = _run_driver(workdir, "fixedpoint_" + gauss, "true", gauss, ("reference-loop",))
+    gold = gold_psi().ravel()
+    assert rel_l1(psi, gold) < 1e-10 and rel_linf(psi, gold) < 1e-10
+    assert "fixedPoint over SweeperCuda::sweep: 34 iterations" in out

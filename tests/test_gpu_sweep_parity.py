@@ -416,14 +416,16 @@ def test_pool_memory_reused_and_released(built, workdir):
     assert bits_equal(psis[0], psis[1]) and bits_equal(psis[0], psis[2])
 
 
-@pytest.mark.parametrize("n,G,chunks,pinned", [(8, 8, 4, True), (12, 3, 4, True), (16, 16, 16, True),
-                                               (8, 8, 1, False)])
-def test_dropin_sweep_in_angle_chunks_bit_exact(built, workdir, n, G, chunks, pinned):
-    """The drop-in sweep of a large psi (64 MiB and up) between page-locked
-    host buffers moves and sweeps K contiguous angle ranges so that its host
-    copies overlap the sweep (pageable buffers: one copy each way): psi
-    bit-identical to the oracle's, on two calls in a row and after a solve
-    on the same sweeper."""
+@pytest.mark.parametrize("n,G,chunks,locked", [(8, 8, 4, "both"), (12, 3, 4, "both"), (16, 16, 16, "both"),
+                                               (8, 8, 4, "none"), (12, 3, 4, "psi"), (16, 16, 16, "source"),
+                                               (16, 16, 16, "none")])
+def test_dropin_sweep_in_angle_chunks_bit_exact(built, workdir, n, G, chunks, locked):
+    """The drop-in sweep of a large psi (64 MiB and up) moves and sweeps K
+    contiguous angle ranges so that its host copies overlap the sweep;
+    page-locked host buffers are copied directly, pageable ones through
+    page-locked staging pieces of 64 MiB (two pieces per chunk at 16^3 G=16):
+    psi bit-identical to the oracle's, on two calls in a row and after a
+    solve on the same sweeper."""
     import torch
     from oracle.oracle import Oracle
     mesh, om = kuhn(workdir, n, 0.05, seed=23)
@@ -435,12 +437,13 @@ def test_dropin_sweep_in_angle_chunks_bit_exact(built, workdir, n, G, chunks, pi
     sw.set_cross_sections(st, np.zeros(mesh.n_cells))
     src0 = rng.uniform(-0.2, 1.0, o.psi_shape)
     ref = o.sweep(st, src_ang=src0)
-    if pinned:
-        src = torch.empty(o.psi_shape, dtype=torch.float64, pin_memory=True).numpy()
-        psi = torch.empty(sw.psi_shape, dtype=torch.float64, pin_memory=True).numpy()
-        src[...] = src0
-    else:
-        src, psi = src0, np.empty(sw.psi_shape)
+    def buffer(lock):
+        if lock:
+            return torch.empty(o.psi_shape, dtype=torch.float64, pin_memory=True).numpy()
+        return np.empty(o.psi_shape)
+    src = buffer(locked in ("both", "source"))
+    psi = buffer(locked in ("both", "psi"))
+    src[...] = src0
     for _ in range(2):
         psi[...] = np.nan
         sw.sweep(psi, src)

@@ -87,6 +87,8 @@ SIGNATURES = {
     "tycho_sweeper_launches": (C.c_int, [_P, C.c_int, _U64P]),
     "tycho_release_cached_memory": (C.c_int, [C.c_int]),
     "tycho_device_memory": (C.c_int, [C.c_int, _U64P, _U64P]),
+    "tycho_host_register": (C.c_int, [_P, C.c_size_t]),
+    "tycho_host_unregister": (C.c_int, [_P]),
     "tycho_sweeper_schedule_arrays": (C.c_int, [_P, _U64P, _P, _P]),
     "tycho_sweeper_time_sweeps": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P]),
     "tycho_sweeper_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(LaunchShape),

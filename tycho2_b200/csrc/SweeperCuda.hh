@@ -20,6 +20,14 @@
  * quadrature from g_snOrder, cross sections from g_sigmaT / g_sigmaS.  A
  * nonzero status is reported through Insist, as the reference reports its
  * own failures (src/Assert.hh:62).
+ *
+ * The sweeper's own psi and source (c_psi, c_source: host `new double[]`,
+ * src/PsiData.hh:94-103) are page-locked for its lifetime, so a sweep that
+ * receives c_psi -- SweeperTraverse::solve hands it to fixedPoint and
+ * krylov (src/SweeperTraverse.cc:65-74) -- copies it back asynchronously,
+ * in angle chunks that overlap the other direction's copies and the sweep.
+ * Buffers the adapter does not own (fixedPoint's local totalSource) stay
+ * pageable: the adapter cannot know when they are freed.
  */
 #ifndef __SWEEPER_CUDA_HH__
 #define __SWEEPER_CUDA_HH__
@@ -41,6 +49,7 @@ public:
     SweeperCuda()
     : c_mesh(NULL), c_sweeper(NULL)
     {
+        c_locked[0] = c_locked[1] = false;
         const UINT nc = g_nCells, nn = g_tychoMesh->getNNodes();
         std::vector<uint64_t> cellNodes(nc * 4), adj(nc * 4), f2c(nc * 12), gid(nc);
         std::vector<double> coords(nn * 3);
@@ -71,10 +80,15 @@ public:
         opts.schedule = 0;
         check(tycho_sweeper_create(c_mesh, &opts, &c_sweeper));
         check(tycho_sweeper_set_cross_sections(c_sweeper, g_sigmaT.data(), g_sigmaS.data(), NULL));
+        // page-locked if the system allows it; pageable otherwise
+        c_locked[0] = tycho_host_register(&c_psi[0], c_psi.size() * sizeof(double)) == TYCHO_OK;
+        c_locked[1] = tycho_host_register(&c_source[0], c_source.size() * sizeof(double)) == TYCHO_OK;
     }
 
     ~SweeperCuda()
     {
+        if (c_locked[0]) tycho_host_unregister(&c_psi[0]);
+        if (c_locked[1]) tycho_host_unregister(&c_source[0]);
         tycho_sweeper_destroy(c_sweeper);
         tycho_mesh_free(c_mesh);
     }
@@ -115,6 +129,7 @@ private:
 
     tycho_mesh *c_mesh;
     tycho_sweeper *c_sweeper;
+    bool c_locked[2];
 };
 
 #endif

@@ -575,6 +575,28 @@ uint64_t tycho_footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, int
     return tycho::footprint_bytes(n_cells, sn_order, n_groups, mixed != 0, compact != 0);
 }
 
+int tycho_host_register(void *p, size_t bytes)
+{
+    if (!p || !bytes) return finish(TYCHO_ERR_ARG, "null pointer or zero size");
+    const cudaError_t e = cudaHostRegister(p, bytes, cudaHostRegisterPortable);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return finish(TYCHO_ERR_CUDA, std::string("page-locking host memory: ") + cudaGetErrorString(e));
+    }
+    return TYCHO_OK;
+}
+
+int tycho_host_unregister(void *p)
+{
+    if (!p) return finish(TYCHO_ERR_ARG, "null pointer");
+    const cudaError_t e = cudaHostUnregister(p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return finish(TYCHO_ERR_CUDA, std::string("unlocking host memory: ") + cudaGetErrorString(e));
+    }
+    return TYCHO_OK;
+}
+
 int tycho_release_cached_memory(int device)
 {
     const cudaError_t e = tycho::dev_trim(device);

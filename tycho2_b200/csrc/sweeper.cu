@@ -10,6 +10,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
+
+#include <omp.h>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -67,6 +72,10 @@ Sweeper::~Sweeper()
         if (ev_h2d_[j]) cudaEventDestroy(ev_h2d_[j]);
         if (ev_swept_[j]) cudaEventDestroy(ev_swept_[j]);
     }
+    for (void *b : h_stage_)
+        if (b) cudaFreeHost(b);
+    for (auto &e : ev_stage_)
+        if (e) cudaEventDestroy(e);
     if (h2d_stream_) cudaStreamDestroy(h2d_stream_);
     if (d2h_stream_) cudaStreamDestroy(d2h_stream_);
     void *bufs[] = {d_items_, d_abar64_, d_abar32_, d_adj_, d_nbrmap_, d_cellk64_, d_cellk32_,
@@ -728,6 +737,23 @@ int Sweeper::host_chunks() const
 // cell's row of the reference layout: one strided (2D) copy per chunk and
 // direction.  Chunk j sweeps its items level by level in schedule order
 // (the same per-item arithmetic and results as the whole sweep).
+namespace {
+
+// Page-locked (or registered) host memory: copies from and to it run
+// asynchronously, so chunks in the two directions can overlap.  Pageable
+// memory is staged through page-locked buffers (sweep_host_chunked).
+bool page_locked(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
 int Sweeper::sweep_host_chunked(const double *source, double *psi, int K, std::string &err)
 {
     TY_CHECK(ensure_records(0, true, err, true));  // kErrOom before any copy
@@ -769,49 +795,150 @@ int Sweeper::sweep_host_chunked(const double *source, double *psi, int K, std::s
         cudaGraphDestroy(graph);
         TY_CUDA(ie);
     }
+    // Pageable host buffers go through two page-locked staging buffers per
+    // direction, in pieces of at most kStageBytes: the calling thread gathers
+    // a piece of the source (OpenMP threads over the rows) while the previous
+    // piece uploads; a second host thread scatters downloaded pieces of psi
+    // while the next one downloads.  Page-locked buffers are copied directly.
+    const bool stage_in = !page_locked(source), stage_out = !page_locked(psi);
+    if ((stage_in || stage_out) && !h_stage_[0]) {
+        cudaError_t ae = cudaSuccess;
+        for (auto &b : h_stage_)
+            if (ae == cudaSuccess) ae = cudaHostAlloc(&b, kStageBytes, cudaHostAllocPortable);
+        if (ae != cudaSuccess) {  // no page-locked memory to spare: the one-copy form
+            cudaGetLastError();
+            for (auto &b : h_stage_) {
+                if (b) cudaFreeHost(b);
+                b = nullptr;
+            }
+            err = "no page-locked staging memory";
+            return kErrOom;
+        }
+        for (auto &e : ev_stage_) TY_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
     // after whatever ran on the sweeper's stream before
     TY_CUDA(cudaEventRecord(ev_start_, stream_));
     TY_CUDA(cudaStreamWaitEvent(h2d_stream_, ev_start_, 0));
     TY_CUDA(cudaStreamWaitEvent(d2h_stream_, ev_start_, 0));
     const size_t per_angle = (size_t)4 * G_ * sizeof(double), row = per_angle * A_;
-    for (int j = 0; j < K; ++j) {
+    auto span = [&](int j, size_t &off, size_t &width) {
         const size_t a0 = (size_t)j * A_ / K, a1 = (size_t)(j + 1) * A_ / K;
-        const size_t off = a0 * per_angle, width = (a1 - a0) * per_angle;
-        TY_CUDA(cudaMemcpy2DAsync(reinterpret_cast<char *>(d_src_) + off, row,
+        off = a0 * per_angle;
+        width = (a1 - a0) * per_angle;
+    };
+    const int nt = std::max(1, omp_get_max_threads() / (stage_in && stage_out ? 2 : 1));
+    // rows [r0, r1) of the chunk's columns [off, off + width) to or from a
+    // packed staging buffer
+    auto pack = [&](char *dst, const char *src, size_t off, size_t width, uint64_t r0, uint64_t r1) {
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t r = (int64_t)r0; r < (int64_t)r1; ++r)
+            std::memcpy(dst + (size_t)(r - r0) * width, src + (size_t)r * row + off, width);
+    };
+    auto unpack = [&](char *dst, const char *src, size_t off, size_t width, uint64_t r0, uint64_t r1) {
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t r = (int64_t)r0; r < (int64_t)r1; ++r)
+            std::memcpy(dst + (size_t)r * row + off, src + (size_t)(r - r0) * width, width);
+    };
+    // the downloading side: in this thread when psi is page-locked (plain
+    // asynchronous copies), else on a helper thread that scatters the pieces
+    std::mutex mu;
+    std::condition_variable cv;
+    int swept = 0;  // chunks whose sweep has been enqueued
+    cudaError_t out_err = cudaSuccess;
+    auto download = [&]() {
+        char *dst = reinterpret_cast<char *>(psi);
+        const char *dev = reinterpret_cast<const char *>(d_psi_);
+        uint64_t q = 0;  // pieces enqueued so far
+        struct Pending { size_t off, width; uint64_t r0, r1; } last[2];
+        cudaError_t e = cudaSuccess;
+        for (int j = 0; j < K && e == cudaSuccess; ++j) {
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait(lk, [&] { return swept > j || out_err != cudaSuccess; });
+                if (out_err != cudaSuccess) return;
+            }
+            size_t off, width;
+            span(j, off, width);
+            e = cudaStreamWaitEvent(d2h_stream_, ev_swept_[j], 0);
+            const uint64_t rows = std::max<uint64_t>(1, kStageBytes / width);
+            for (uint64_t r0 = 0; r0 < nc_ && e == cudaSuccess; r0 += rows, ++q) {
+                const uint64_t r1 = std::min<uint64_t>(nc_, r0 + rows);
+                char *buf = reinterpret_cast<char *>(h_stage_[2 + q % 2]);
+                e = cudaMemcpy2DAsync(buf, width, dev + r0 * row + off, row, width, r1 - r0, cudaMemcpyDeviceToHost,
+                                      d2h_stream_);
+                if (e == cudaSuccess) e = cudaEventRecord(ev_stage_[2 + q % 2], d2h_stream_);
+                last[q % 2] = {off, width, r0, r1};
+                if (q >= 1 && e == cudaSuccess) {  // the previous piece has landed: scatter it
+                    const Pending &pp = last[(q - 1) % 2];
+                    e = cudaEventSynchronize(ev_stage_[2 + (q - 1) % 2]);
+                    if (e == cudaSuccess)
+                        unpack(dst, reinterpret_cast<const char *>(h_stage_[2 + (q - 1) % 2]), pp.off, pp.width, pp.r0,
+                               pp.r1);
+                }
+            }
+        }
+        if (q >= 1 && e == cudaSuccess) {
+            const Pending &pp = last[(q - 1) % 2];
+            e = cudaEventSynchronize(ev_stage_[2 + (q - 1) % 2]);
+            if (e == cudaSuccess)
+                unpack(dst, reinterpret_cast<const char *>(h_stage_[2 + (q - 1) % 2]), pp.off, pp.width, pp.r0, pp.r1);
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        if (out_err == cudaSuccess) out_err = e;
+    };
+    std::thread helper;
+    if (stage_out) helper = std::thread(download);
+    cudaError_t e = cudaSuccess;
+    uint64_t p = 0;  // source pieces enqueued so far
+    for (int j = 0; j < K && e == cudaSuccess; ++j) {
+        size_t off, width;
+        span(j, off, width);
+        if (!stage_in) {
+            e = cudaMemcpy2DAsync(reinterpret_cast<char *>(d_src_) + off, row,
                                   reinterpret_cast<const char *>(source) + off, row, width, nc_,
-                                  cudaMemcpyHostToDevice, h2d_stream_));
-        TY_CUDA(cudaEventRecord(ev_h2d_[j], h2d_stream_));
-        TY_CUDA(cudaStreamWaitEvent(stream_, ev_h2d_[j], 0));
-        TY_CUDA(cudaGraphLaunch(chunk_graphs_[j], stream_));
-        TY_CUDA(cudaEventRecord(ev_swept_[j], stream_));
-        TY_CUDA(cudaStreamWaitEvent(d2h_stream_, ev_swept_[j], 0));
-        TY_CUDA(cudaMemcpy2DAsync(reinterpret_cast<char *>(psi) + off, row,
-                                  reinterpret_cast<const char *>(d_psi_) + off, row, width, nc_,
-                                  cudaMemcpyDeviceToHost, d2h_stream_));
+                                  cudaMemcpyHostToDevice, h2d_stream_);
+        } else {
+            const uint64_t rows = std::max<uint64_t>(1, kStageBytes / width);
+            for (uint64_t r0 = 0; r0 < nc_ && e == cudaSuccess; r0 += rows, ++p) {
+                const uint64_t r1 = std::min<uint64_t>(nc_, r0 + rows);
+                if (p >= 2) e = cudaEventSynchronize(ev_stage_[p % 2]);  // its last upload is done
+                if (e != cudaSuccess) break;
+                char *buf = reinterpret_cast<char *>(h_stage_[p % 2]);
+                pack(buf, reinterpret_cast<const char *>(source), off, width, r0, r1);
+                e = cudaMemcpy2DAsync(reinterpret_cast<char *>(d_src_) + r0 * row + off, row, buf, width, width,
+                                      r1 - r0, cudaMemcpyHostToDevice, h2d_stream_);
+                if (e == cudaSuccess) e = cudaEventRecord(ev_stage_[p % 2], h2d_stream_);
+            }
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(ev_h2d_[j], h2d_stream_);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(stream_, ev_h2d_[j], 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(chunk_graphs_[j], stream_);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_swept_[j], stream_);
+        if (e == cudaSuccess && !stage_out) {
+            e = cudaStreamWaitEvent(d2h_stream_, ev_swept_[j], 0);
+            if (e == cudaSuccess)
+                e = cudaMemcpy2DAsync(reinterpret_cast<char *>(psi) + off, row,
+                                      reinterpret_cast<const char *>(d_psi_) + off, row, width, nc_,
+                                      cudaMemcpyDeviceToHost, d2h_stream_);
+        }
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            if (e == cudaSuccess) swept = j + 1;
+            else if (out_err == cudaSuccess) out_err = e;
+        }
+        cv.notify_all();
     }
+    if (helper.joinable()) helper.join();
+    TY_CUDA(e);
+    TY_CUDA(out_err);
     TY_CUDA(cudaStreamSynchronize(d2h_stream_));
+    TY_CUDA(cudaStreamSynchronize(h2d_stream_));
     TY_CUDA(cudaStreamSynchronize(stream_));
     last_psi_prec_ = 0;
     return check_device_error(err);
 }
 
-namespace {
 
-// Page-locked (or registered) host memory: copies from and to it run
-// asynchronously, so chunks in the two directions can overlap.  From
-// pageable memory each copy is staged by the calling thread, and chunking
-// would only add launches.
-bool page_locked(const void *p)
-{
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type == cudaMemoryTypeHost;
-}
-
-}  // namespace
 
 int Sweeper::sweep_host(const double *source, double *psi, std::string &err)
 {
@@ -819,7 +946,9 @@ int Sweeper::sweep_host(const double *source, double *psi, std::string &err)
     TY_CUDA(cudaSetDevice(device_));
     const size_t n = psi_size();
     if (!d_src_) TY_CUDA(dev_malloc(&d_src_, sizeof(double) * n, stream_));
-    const int K = page_locked(source) && page_locked(psi) ? host_chunks() : 1;
+    // page-locked buffers are copied directly, pageable ones through the
+    // staging buffers of the chunked form
+    const int K = host_chunks();
     if (K > 1) {
         // no room for the chunk plan or the compact FP64 records: one copy
         // each way instead (nothing was copied yet)

@@ -218,6 +218,11 @@ private:
     cudaStream_t h2d_stream_ = nullptr, d2h_stream_ = nullptr;
     static constexpr int kMaxHostChunks = 16;
     cudaEvent_t ev_start_ = nullptr, ev_h2d_[kMaxHostChunks] = {}, ev_swept_[kMaxHostChunks] = {};
+    // page-locked staging for pageable host buffers: [0, 1] source pieces,
+    // [2, 3] psi pieces, each with the event of its last copy
+    static constexpr size_t kStageBytes = 64ull << 20;
+    void *h_stage_[4] = {};
+    cudaEvent_t ev_stage_[4] = {};
     unsigned long long *d_barrier_ = nullptr;
 };
 
