@@ -14,8 +14,9 @@ Two more legs ride on the same line (skip with --no-batch / --no-serve):
 iteration vs FP32-sweep iteration inside FP64 refinement, one batched pass
 per step), and `serve`, Poisson-arriving solve requests (the batch size
 distribution plus 5% large 48^3-hex S8 G=8 ones) admitted by device-memory
-footprint against 150 GB with continuous batching: p50/p99 latency and
-solves/s of the mixed and the FP64 service; and `large`, the 64^3 x 6-tet
+footprint against 150 GB with continuous batching, at a swept arrival rate:
+p50/p99 latency, solves/s and requests in the batch of the mixed and the
+FP64 service; and `large`, the 64^3 x 6-tet
 S8 G=16 problem (psi 103 GB): sweep rates and the mixed-precision GMRES solve
 against FP64 GMRES (skip with --no-large).
 
@@ -61,8 +62,9 @@ def parse():
     p.add_argument("--no-serve", action="store_true", help="skip the served-solves leg")
     p.add_argument("--no-parity", action="store_true",
                    help="skip the oracle checks of the benchmarked solves (run after the timed legs)")
-    p.add_argument("--serve-requests", type=int, default=40)
-    p.add_argument("--serve-rate", type=float, default=10.0, help="Poisson arrivals per second")
+    p.add_argument("--serve-requests", type=int, default=200, help="requests per arrival rate")
+    p.add_argument("--serve-rates", default="20,50,100,200",
+                   help="Poisson arrival rates (requests per second), comma-separated")
     p.add_argument("--shape", default="default",
                    help="launch shape 'schedule,variant,knob[,vector[,streams]]' for both precisions "
                         "(an FP32-only vector width falls back to the widest for FP64, an FP32-only knob "
@@ -441,10 +443,13 @@ def run_batch_leg(grp, dev, count, seed=4321, profile=False, sample=None):
                                            / out["si"]["fp64_pass_updates_per_s"])}
 
 
-def run_serve_leg(grp, dev, count, rate, seed=99):
-    """Served solves: `count` requests drawn like the batch instances plus 5%
-    large ones (48^3 hexes x 6 tets, G=8, S8), Poisson arrivals at `rate` per
-    second, admitted by footprint against 150 GB, mixed vs FP64 service."""
+def run_serve_leg(grp, dev, count, rates, seed=99):
+    """Served solves at a swept arrival rate: `count` requests drawn like the
+    batch instances plus 5% large ones (48^3 hexes x 6 tets, G=8, S8), the
+    same requests at each Poisson rate (the arrival gaps of one seeded
+    exponential draw, scaled by 1/rate), admitted by footprint against 150
+    GB, mixed vs FP64 service: p50/p99 latency, solves/s, mean and peak
+    requests in the batch."""
     import tycho2_b200 as ty
     from tycho2_b200 import problems
     rng = np.random.default_rng(seed + grp.rank)
@@ -454,37 +459,43 @@ def run_serve_leg(grp, dev, count, rate, seed=99):
             params[k] = dict(n=48, jitter=0.05, sn=8, groups=8, sigma="lognormal", lognormal_s=0.5,
                              ratio=0.6, scatter="down", source="all", seed=5000 + k)
     probs = [problems.make_problem(**p) for p in params]
-    gaps = rng.exponential(1.0 / rate, count)
-    arrivals = np.cumsum(gaps) - gaps[0]
+    unit_gaps = rng.exponential(1.0, count)
     out = {"requests": count * grp.world, "large": int(sum(p["n"] == 48 for p in params)),
-           "rate_per_s": rate * grp.world, "budget_gb": 150.0}
-    phis = {}
-    for method, key in (("mixed", "mixed"), ("si", "fp64")):
-        srv = ty.SolveServer(method=method, budget_bytes=150e9, device=dev, setup_threads=4, err_max=1e-10,
-                             inner_tol=1e-5)
-        ids = [srv.submit(m, p["sn"], p["groups"], st, ss, mat, q, arrival=float(a))
-               for p, (m, st, ss, mat, q), a in zip(params, probs, arrivals)]
-        grp.barrier()
-        srv.run()
-        info = [srv.info(i) for i in ids]
-        done = [i for i in info if i["state"] == "done"]
-        lat = np.array([i["latency"] for i in done])
-        st_ = srv.stats()
-        phis[key] = [srv.phi(i).copy() for i in ids]
-        out[key] = {"done": len(done), "p50_latency_s": grp.max(float(np.percentile(lat, 50))),
-                    "p99_latency_s": grp.max(float(np.percentile(lat, 99))),
-                    "solves_per_s": grp.sum(len(done)) / grp.max(st_["makespan"]),
-                    "build_p50_s": float(np.percentile([i["built"] - i["admitted"] for i in done], 50)),
-                    "peak_resident_gb": st_["peak_bytes"] / 1e9, "peak_in_batch": st_["peak_active"],
-                    "batch_steps": st_["steps"]}
-        big = [i for p, i in zip(params, info) if p["n"] == 48 and i["state"] == "done"]
-        if big:  # where the large requests' latency goes
-            out[key]["large_requests"] = [
-                {"latency_s": i["latency"], "queue_s": i["admitted"] - i["arrival"],
-                 "build_s": i["built"] - i["admitted"], "solve_s": i["finished"] - i["built"]} for i in big]
-        srv.close()
-    out["phi_rel_err_l1_max_mixed_vs_fp64"] = grp.max(max(
-        float(np.abs(a - b).sum() / np.abs(b).sum()) for a, b in zip(phis["mixed"], phis["fp64"])))
+           "budget_gb": 150.0, "rates": []}
+    worst = 0.0
+    for rate in rates:
+        arrivals = (np.cumsum(unit_gaps) - unit_gaps[0]) / rate
+        entry = {"rate_per_s": rate * grp.world}
+        phis = {}
+        for method, key in (("mixed", "mixed"), ("si", "fp64")):
+            srv = ty.SolveServer(method=method, budget_bytes=150e9, device=dev, setup_threads=4, err_max=1e-10,
+                                 inner_tol=1e-5)
+            ids = [srv.submit(m, p["sn"], p["groups"], st, ss, mat, q, arrival=float(a))
+                   for p, (m, st, ss, mat, q), a in zip(params, probs, arrivals)]
+            grp.barrier()
+            srv.run()
+            info = [srv.info(i) for i in ids]
+            done = [i for i in info if i["state"] == "done"]
+            lat = np.array([i["latency"] for i in done])
+            st_ = srv.stats()
+            phis[key] = [srv.phi(i).copy() for i in ids]
+            span = max(st_["makespan"], 1e-9)
+            entry[key] = {"done": len(done), "p50_latency_s": grp.max(float(np.percentile(lat, 50))),
+                          "p99_latency_s": grp.max(float(np.percentile(lat, 99))),
+                          "solves_per_s": grp.sum(len(done)) / grp.max(st_["makespan"]),
+                          "build_p50_s": float(np.percentile([i["built"] - i["admitted"] for i in done], 50)),
+                          "mean_in_batch": float(sum(i["finished"] - i["built"] for i in done) / span),
+                          "peak_in_batch": st_["peak_active"],
+                          "peak_resident_gb": st_["peak_bytes"] / 1e9, "batch_steps": st_["steps"]}
+            big = [i for p, i in zip(params, info) if p["n"] == 48 and i["state"] == "done"]
+            if big:  # where the large requests' latency goes
+                entry[key]["large_p50_latency_s"] = float(np.percentile([i["latency"] for i in big], 50))
+            srv.close()
+        entry["phi_rel_err_l1_max_mixed_vs_fp64"] = grp.max(max(
+            float(np.abs(a - b).sum() / np.abs(b).sum()) for a, b in zip(phis["mixed"], phis["fp64"])))
+        worst = max(worst, entry["phi_rel_err_l1_max_mixed_vs_fp64"])
+        out["rates"].append(entry)
+    out["phi_rel_err_l1_max_mixed_vs_fp64"] = worst
     return out
 
 
@@ -737,7 +748,8 @@ def run_b200(args):
             batch = {"error": str(e)[:300]}
     if not args.no_serve:
         try:
-            serve = run_serve_leg(grp, dev, args.serve_requests, args.serve_rate)
+            serve = run_serve_leg(grp, dev, args.serve_requests,
+                                  [float(r) for r in args.serve_rates.split(",") if r.strip()])
         except Exception as e:
             serve = {"error": str(e)[:300]}
     large = None
