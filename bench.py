@@ -351,10 +351,15 @@ def traffic_family(shape, fp32):
     return "%s %s vg%d" % (shape["variant"], "float" if fp32 else "double", shape["vector"])
 
 
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of 3 mid-sweep launches of the kernel on "
+                  "kuhn24_s8_g8 (warm caches), per item, times this sweep's items: profiles/sweep_traffic.md; "
+                  "not measured in this run")
+
+
 def profiled_traffic(workload, family):
-    """DRAM bytes of one sweep (dram__bytes_read.sum + dram__bytes_write.sum over
-    the sweep's launches) from the ncu summary table in profiles/, if that
-    kernel family was captured on this workload; else None."""
+    """DRAM bytes of one sweep from the ncu summary table in profiles/ (three
+    sampled launches of the kernel, bytes per item scaled to the sweep's
+    items), if that kernel family was captured for this workload; else None."""
     path = os.path.join(ROOT, "profiles", "sweep_traffic.md")
     try:
         with open(path) as f:
@@ -791,7 +796,8 @@ def run_b200(args):
             "mixed_vs_fp64_sweep_speedup": value / fp64_value,
             "solve": solve,
             "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
-                         "frac": ach32 / peak, "traffic": t32, "peak_kind": peak_kind,
+                         "frac": ach32 / peak, "traffic": t32,
+                         "traffic_source": TRAFFIC_SOURCE if t32 is not None else None, "peak_kind": peak_kind,
                          "kernel": k32, "bytes_per_sweep": b32, "kernel_ms_per_sweep": lvl32,
                          "per": "one sweep (all of its launches)",
                          "fp64": {"kernel": k64, "achieved": ach64, "frac": ach64 / peak,
