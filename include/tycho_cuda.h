@@ -163,6 +163,16 @@ typedef struct tycho_sweeper_opts {
    and allocates psi.  Fails with TYCHO_ERR_CYCLE on a cyclic direction. */
 int tycho_sweeper_create(const tycho_mesh *mesh, const tycho_sweeper_opts *opts,
                          tycho_sweeper **out);
+
+/* The same for the directions [angle_begin, angle_end) of the quadrature
+   only: an angle shard.  Each direction sweeps independently of the others,
+   so the shards of one problem on several GPUs (one process each) sweep in
+   parallel and the sum of their phi (tycho_sweeper_apply) over the shards
+   is the whole problem's psiToPhi (src/Util.cc:85-97; the reference
+   parallelises over spatial partitions instead, src/GraphTraverser.cc:659-731).
+   Both 0: every direction, as tycho_sweeper_create. */
+int tycho_sweeper_create_angles(const tycho_mesh *mesh, const tycho_sweeper_opts *opts, int angle_begin,
+                                int angle_end, tycho_sweeper **sw);
 void tycho_sweeper_destroy(tycho_sweeper *sw);
 
 /* Cross sections (Problem::createCrossSections, src/Problem.cc:149-172):
@@ -340,6 +350,17 @@ int tycho_sweeper_sweep_noalloc(tycho_sweeper *sw, int precision, const void *is
    (src/GraphTraverser.cc:518).  0 gives up at the first wait that is not
    already satisfied: the failure path can be exercised without a hang. */
 int tycho_sweeper_set_wait_limit(tycho_sweeper *sw, uint32_t polls);
+
+/* One operator application on caller-owned device vectors (phi layout,
+   FP64): phi_out = D L^{-1} ([Q] + M S phi_in) in the given precision
+   (lhsOperator's sweep with calcTotalSource and psiToPhi around it,
+   src/SourceIteration.cc:76-114; phi_in NULL: no scattering source;
+   with_fixed: add the fixed source).  For an angle shard phi_out is its
+   directions' part of the sum.  Ordered after the work queued on `stream`
+   (a cudaStream_t, NULL = legacy default stream); returns once phi_out is
+   written. */
+int tycho_sweeper_apply(tycho_sweeper *sw, int precision, const double *phi_in, int with_fixed, double *phi_out,
+                        void *stream);
 
 /* Device timing of n back-to-back operator applications
    phi_out = D L^{-1} (M S phi_in + Q) in the given precision, on the

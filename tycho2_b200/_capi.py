@@ -76,6 +76,8 @@ SIGNATURES = {
     "tycho_mesh_sweep_schedule_levels": (C.c_int, [_P, C.c_int, _P, _U32P]),
     "tycho_quadrature": (C.c_int, [C.c_int, _P, _P, _P, _P]),
     "tycho_sweeper_create": (C.c_int, [_P, C.POINTER(SweeperOpts), _PP]),
+    "tycho_sweeper_create_angles": (C.c_int, [_P, C.POINTER(SweeperOpts), C.c_int, C.c_int, _PP]),
+    "tycho_sweeper_apply": (C.c_int, [_P, C.c_int, _P, C.c_int, _P, _P]),
     "tycho_sweeper_destroy": (None, [_P]),
     "tycho_sweeper_set_cross_sections": (C.c_int, [_P, _P, _P, _P]),
     "tycho_sweeper_set_source": (C.c_int, [_P, C.c_int, _P]),

@@ -276,6 +276,12 @@ int tycho_quadrature(int sn, double *xi, double *eta, double *mu, double *wt)
 
 int tycho_sweeper_create(const tycho_mesh *mesh, const tycho_sweeper_opts *opts, tycho_sweeper **out)
 {
+    return tycho_sweeper_create_angles(mesh, opts, 0, 0, out);
+}
+
+int tycho_sweeper_create_angles(const tycho_mesh *mesh, const tycho_sweeper_opts *opts, int angle_begin,
+                                int angle_end, tycho_sweeper **out)
+{
     if (!mesh || !opts || !out) return finish(TYCHO_ERR_ARG, "null argument");
     return guarded([&] {
         auto *h = new tycho_sweeper;
@@ -298,6 +304,8 @@ int tycho_sweeper_create(const tycho_mesh *mesh, const tycho_sweeper_opts *opts,
             return finish(TYCHO_ERR_ARG, "GaussElim must be Original, NoPivot, CramerGlu or CramerIntel");
         }
         o.gauss_elim = opts->gauss_elim;
+        o.angle_begin = angle_begin;
+        o.angle_end = angle_end;
         int st = h->sw.init(mesh->tabp, o, err);
         if (st != tycho::kOk) { delete h; return finish(st, err); }
         *out = h;
@@ -463,6 +471,18 @@ int tycho_sweeper_sweep_noalloc(tycho_sweeper *h, int precision, const void *iso
     if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
     std::string err;
     return finish(tycho::sweep_noalloc(h->sw, precision, iso, psi, stream, err), err);
+}
+
+int tycho_sweeper_apply(tycho_sweeper *h, int precision, const double *phi_in, int with_fixed, double *phi_out,
+                        void *stream)
+{
+    if (!h || !phi_out) return finish(TYCHO_ERR_ARG, "null argument");
+    if (precision != 0 && precision != 1) return finish(TYCHO_ERR_ARG, "precision must be 0 (FP64) or 1 (FP32)");
+    std::string err;
+    return guarded([&] {
+        return finish(h->sw.apply_external(precision, phi_in, with_fixed != 0, phi_out, (cudaStream_t)stream, err),
+                      err);
+    });
 }
 
 int tycho_sweeper_set_wait_limit(tycho_sweeper *h, uint32_t polls)

@@ -127,6 +127,23 @@ int Sweeper::init(std::shared_ptr<const MeshTables> tp, const SweeperOptions &o,
     // device, so that tycho_sweeper_sweep_noalloc itself loads nothing
     TY_CHECK(noalloc_scratch_prepare(device_, err));
     TY_CHECK(make_quadrature(o.sn_order, quad_, err));
+    if (o.angle_begin != 0 || o.angle_end != 0) {
+        // an angle shard: the directions [begin, end) with their weights, so
+        // that phi is the partial sum over them (src/Util.cc:85-97 split by
+        // angle range); every direction sweeps independently
+        if (o.angle_begin < 0 || o.angle_end > quad_.n_angles || o.angle_begin >= o.angle_end) {
+            err = "angle range must satisfy 0 <= begin < end <= " + std::to_string(quad_.n_angles);
+            return kErrArg;
+        }
+        auto cut = [&](std::vector<double> &v) {
+            v = std::vector<double>(v.begin() + o.angle_begin, v.begin() + o.angle_end);
+        };
+        cut(quad_.xi);
+        cut(quad_.eta);
+        cut(quad_.mu);
+        cut(quad_.wt);
+        quad_.n_angles = o.angle_end - o.angle_begin;
+    }
     tables_ = std::move(tp);
     nc_ = t.n_cells;
     A_ = quad_.n_angles;
@@ -716,6 +733,22 @@ int Sweeper::apply(int prec, const double *phi_in, bool with_fixed, double *phi_
     if (phi_out) TY_CUDA(launch_psi_to_phi(d_psi_, prec == 1, d_w_, phi_out, nc_, (uint32_t)A_, (uint32_t)G_, stream_));
     last_psi_prec_ = prec;
     return kOk;
+}
+
+int Sweeper::apply_external(int prec, const double *phi_in, bool with_fixed, double *phi_out, cudaStream_t s,
+                            std::string &err)
+{
+    TY_CUDA(cudaSetDevice(device_));
+    if (prec == 1 && !fp32_) { err = "sweeper was created without the FP32 sweep"; return kErrArg; }
+    cudaEvent_t ev;
+    TY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ev, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream_, ev, 0);
+    cudaEventDestroy(ev);
+    TY_CUDA(e);
+    TY_CHECK(apply(prec, phi_in, with_fixed, phi_out, nullptr, err));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    return check_device_error(err);
 }
 
 // Chunks of the drop-in sweep: large psi (copies of ~0.1 s and more over

@@ -27,6 +27,9 @@ struct SweeperOptions {
     int schedule = 0;  // 0 auto (levels, compact records), 1 level-synchronous, 2 dataflow
     int gauss_elim = 1;  // 4x4 solver, numbered as tycho_gauss_elim (deck key GaussElim)
     int levelling = 0;   // 0 auto, 1 host, 2 device
+    // directions [angle_begin, angle_end) of the quadrature only (both 0:
+    // all): an angle shard whose phi is the partial sum over its directions
+    int angle_begin = 0, angle_end = 0;
 };
 
 // Launch shape of one precision's sweep.
@@ -87,6 +90,11 @@ public:
     // prec 0 = FP64, 1 = FP32.  qang overrides the angular fixed source.
     int apply(int prec, const double *phi_in, bool with_fixed, double *phi_out,
               const double *qang_override, std::string &err);
+    // apply() on caller-owned device vectors, ordered after the work already
+    // queued on `s` (nullable: the legacy default stream); returns once
+    // phi_out is written.
+    int apply_external(int prec, const double *phi_in, bool with_fixed, double *phi_out, cudaStream_t s,
+                       std::string &err);
 
     // One persistent-dataflow sweep psi = L^{-1} iso on caller-owned device
     // buffers (iso: phi layout, may be null; psi: psi layout; both in the

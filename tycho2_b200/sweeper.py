@@ -157,17 +157,24 @@ class SweeperCuda:
     LEVELLING = {"auto": 0, "host": 1, "device": 2}
 
     def __init__(self, mesh, sn_order, n_groups, gauss_elim="NoPivot", fp32=False, device=0,
-                 tpi64=0, tpi32=0, schedule="auto", levelling="auto"):
+                 tpi64=0, tpi32=0, schedule="auto", levelling="auto", angles=None):
+        """angles=(begin, end): the directions [begin, end) of the quadrature
+        only (an angle shard, tycho_sweeper_create_angles)."""
         if gauss_elim not in GAUSS_ELIM:
             raise ValueError("GaussElim must be one of %s" % sorted(GAUSS_ELIM))
         self.mesh = mesh
         self.n_groups = n_groups
         self.quadrature = Quadrature(sn_order)
-        self.n_angles = self.quadrature.n_angles
+        a0, a1 = angles if angles is not None else (0, self.quadrature.n_angles)
+        self.angles = (a0, a1)
+        self.n_angles = a1 - a0
         opts = _capi.SweeperOpts(sn_order, n_groups, GAUSS_ELIM[gauss_elim], device, int(fp32),
                                  tpi64, tpi32, self.SCHEDULES[schedule], self.LEVELLING[levelling])
         h = C.c_void_p()
-        check(lib().tycho_sweeper_create(mesh._h, C.byref(opts), C.byref(h)))
+        if angles is None:
+            check(lib().tycho_sweeper_create(mesh._h, C.byref(opts), C.byref(h)))
+        else:
+            check(lib().tycho_sweeper_create_angles(mesh._h, C.byref(opts), int(a0), int(a1), C.byref(h)))
         self._h = h
         self.stats = None
 
@@ -273,6 +280,22 @@ class SweeperCuda:
         streams (octant groups)."""
         sh = _capi.LaunchShape(self.SCHEDULES[schedule], self.VARIANTS[variant], knob, vector, streams)
         check(lib().tycho_sweeper_configure(self._h, precision, C.byref(sh)))
+
+    def apply(self, phi_in, phi_out, precision=0, with_fixed=True):
+        """phi_out = D L^-1 ([Q] + M S phi_in) on device tensors (torch, FP64,
+        phi layout; phi_in may be None), ordered after the current torch
+        stream's work (tycho_sweeper_apply).  For an angle shard phi_out is
+        its directions' part of phi."""
+        import torch
+        for t in (phi_in, phi_out):
+            if t is not None:
+                assert t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+                assert tuple(t.shape) == self.phi_shape or t.numel() == int(np.prod(self.phi_shape))
+        stream = torch.cuda.current_stream(phi_out.device)
+        check(lib().tycho_sweeper_apply(self._h, int(precision),
+                                        C.c_void_p(phi_in.data_ptr()) if phi_in is not None else None,
+                                        int(bool(with_fixed)), C.c_void_p(phi_out.data_ptr()),
+                                        C.c_void_p(stream.cuda_stream)))
 
     def set_wait_limit(self, polls):
         """Polls of one flag or level barrier before a persistent kernel's
