@@ -3,6 +3,8 @@
 // -fmad=false: the FP64 wavefront kernel, the per-item face terms, the
 // scalar flux and the scattering source keep the reference's rounding.
 #include "device_ops.hpp"
+
+#include <cstring>
 #include "devmem.hpp"
 #include "sweep_kernels.cuh"
 #include "sweep_tiles.cuh"
@@ -165,6 +167,17 @@ __global__ void reduce_partials_kernel(const double *__restrict__ partials, int 
     out[j] = s;
 }
 
+// w /= sqrt(*sq) (left as is when the norm is 0); *norm_out = sqrt(*sq).
+__global__ void scale_by_norm_kernel(double *__restrict__ w, uint64_t n, const double *__restrict__ sq,
+                                     double *__restrict__ norm_out)
+{
+    const double hn = sqrt(*sq);
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && norm_out) *norm_out = hn;
+    if (i >= n || !(hn > 0.0)) return;
+    w[i] = w[i] * (1.0 / hn);
+}
+
 __global__ void multi_axpy_kernel(double *__restrict__ w, const double *__restrict__ V, size_t ld,
                                   const double *__restrict__ h, int k, uint64_t n)
 {
@@ -240,8 +253,9 @@ cudaError_t launch_bump_epoch(uint32_t *epoch, cudaStream_t s)
 cudaError_t reducer_init(Reducer &r, cudaStream_t s)
 {
     cudaError_t e = dev_malloc(&r.partials, sizeof(double) * kReduceBlocks * 64, s);
-    if (e == cudaSuccess) e = dev_malloc(&r.result, sizeof(double) * 64, s);
-    if (e == cudaSuccess) r.host = new double[64]();
+    if (e == cudaSuccess) e = dev_malloc(&r.result, sizeof(double) * kReduceSlots, s);
+    if (e == cudaSuccess) e = cudaMallocHost(&r.host, sizeof(double) * kReduceSlots);
+    if (e == cudaSuccess) std::memset(r.host, 0, sizeof(double) * kReduceSlots);
     return e;
 }
 
@@ -249,8 +263,31 @@ void reducer_free(Reducer &r, cudaStream_t s)
 {
     dev_free(r.partials, s);
     dev_free(r.result, s);
-    delete[] r.host;
+    if (r.host) cudaFreeHost(r.host);
     r = Reducer();
+}
+
+cudaError_t multi_dot_dev(const double *w, const double *V, size_t ld, int k, uint64_t n, Reducer &r, double *dst,
+                          cudaStream_t s)
+{
+    if (k < 1 || k > 64) return cudaErrorInvalidValue;
+    for (int j0 = 0; j0 < k; j0 += 16)
+        multi_dot_kernel<16><<<kReduceBlocks, 256, 0, s>>>(w, V, ld, k, j0, n, r.partials);
+    reduce_partials_kernel<<<1, 64, 0, s>>>(r.partials, kReduceBlocks, k, dst);
+    return cudaGetLastError();
+}
+
+cudaError_t l1_pair_dev(const double *x, const double *y, uint64_t n, Reducer &r, double *dst, cudaStream_t s)
+{
+    l1_kernel<<<kReduceBlocks, 256, 0, s>>>(x, y, n, r.partials);
+    reduce_partials_kernel<<<1, 64, 0, s>>>(r.partials, kReduceBlocks, 2, dst);
+    return cudaGetLastError();
+}
+
+cudaError_t scale_by_norm(double *w, uint64_t n, const double *sq, double *norm_out, cudaStream_t s)
+{
+    scale_by_norm_kernel<<<blocks_for(std::max<uint64_t>(n, 1)), 256, 0, s>>>(w, n, sq, norm_out);
+    return cudaGetLastError();
 }
 
 cudaError_t multi_dot(const double *w, const double *V, size_t ld, int k, uint64_t n, Reducer &r,

@@ -31,10 +31,11 @@ cudaError_t launch_bump_epoch(uint32_t *epoch, cudaStream_t s);
 // Deterministic reductions: a fixed grid writes per-block partials that one
 // block sums in a fixed order, so results do not depend on scheduling.
 constexpr int kReduceBlocks = 592;  // 4 per SM on 148 SMs
+constexpr int kReduceSlots = 256;   // result / host doubles
 struct Reducer {
     double *partials = nullptr;  // kReduceBlocks * 64
-    double *result = nullptr;    // 64 device doubles
-    double *host = nullptr;      // 64 host doubles
+    double *result = nullptr;    // kReduceSlots device doubles
+    double *host = nullptr;      // kReduceSlots page-locked host doubles
 };
 // Device buffers from the stream-ordered pool on stream s; the host copy of
 // the results is ordinary host memory (each reduction synchronizes s before
@@ -47,6 +48,14 @@ cudaError_t multi_dot(const double *w, const double *V, size_t ld, int k, uint64
                       cudaStream_t s);
 // result[0] = sum |x - y| (y may be null), result[1] = sum |x|.
 cudaError_t l1_pair(const double *x, const double *y, uint64_t n, Reducer &r, cudaStream_t s);
+// The same reductions into device memory dst (dst[j], j < k; dst[0..1]),
+// without a copy to the host or a synchronization: usable in a captured
+// graph (the same partial sums in the same order, so the same results).
+cudaError_t multi_dot_dev(const double *w, const double *V, size_t ld, int k, uint64_t n, Reducer &r, double *dst,
+                          cudaStream_t s);
+cudaError_t l1_pair_dev(const double *x, const double *y, uint64_t n, Reducer &r, double *dst, cudaStream_t s);
+// w /= sqrt(*sq) unless it is 0; *norm_out (nullable) = sqrt(*sq).
+cudaError_t scale_by_norm(double *w, uint64_t n, const double *sq, double *norm_out, cudaStream_t s);
 // w -= sum_j h[j] V_j (h on device), j < k.
 cudaError_t multi_axpy(double *w, const double *V, size_t ld, const double *h, int k, uint64_t n,
                        cudaStream_t s);

@@ -62,7 +62,8 @@ Sweeper::~Sweeper()
 {
     TraceScope trace("sweeper.destroy");
     if (device_ >= 0) cudaSetDevice(device_);
-    for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+    for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
+    for (auto &kv : step_graphs_) cudaGraphExecDestroy(kv.second);
     for (auto &g : chunk_graphs_)
         if (g) cudaGraphExecDestroy(g);
     dev_free(d_chunk_pos_, stream_);
@@ -377,13 +378,20 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
     // cached level graphs were captured for the previous launch shape
     for (auto it = graphs_.begin(); it != graphs_.end();) {
         if (std::get<0>(it->first) == prec) {
-            cudaGraphExecDestroy(it->second);
+            cudaGraphExecDestroy(it->second.exec);
             it = graphs_.erase(it);
         } else {
             ++it;
         }
     }
+    drop_step_graphs();
     return kOk;
+}
+
+void Sweeper::drop_step_graphs()
+{
+    for (auto &kv : step_graphs_) cudaGraphExecDestroy(kv.second);
+    step_graphs_.clear();
 }
 
 // Times every launch shape -- schedule x variant x (threads per item or warps
@@ -581,6 +589,7 @@ int Sweeper::set_cross_sections(const double *sigma_t, const double *sigma_s, co
         d_scat_ = nullptr;
     }
     TY_CUDA(cudaStreamSynchronize(stream_));
+    drop_step_graphs();  // they hold the source and scattering buffers' addresses
     have_xs_ = true;
     rec_valid_[0] = rec_valid_[1] = false;
     crec_valid_[0] = crec_valid_[1] = false;
@@ -593,6 +602,7 @@ int Sweeper::set_source(int kind, const double *q, std::string &err)
 {
     TY_CUDA(cudaSetDevice(device_));
     if (kind != 0 && kind != 1) { err = "source kind must be 0 (angular) or 1 (isotropic)"; return kErrArg; }
+    drop_step_graphs();
     double *&dst = kind == 0 ? d_qang_ : d_qiso_;
     const size_t n = kind == 0 ? psi_size() : phi_size();
     if (!q) {
@@ -662,19 +672,27 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         if (end) TY_CUDA(cudaEventRecord(end, stream_));
         return kOk;
     }
-    if (sh.variant >= 2) TY_CHECK(ensure_records(prec, true, err, sh.variant == 4));
-    auto key = std::make_tuple(prec, has_iso, qang);
-    auto it = graphs_.find(key);
-    if (it == graphs_.end()) {
-        const LevelArgs p = level_args(prec, iso, qang, d_psi_);
-        cudaGraph_t graph;
-        TY_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-        cudaError_t le = cudaSuccess;
-        // one chain of level launches per octant group, each on its own
-        // stream (forked from and joined into stream_ inside the graph)
-        const int S = sh.streams;
-        if (S > 1) le = cudaEventRecord(fork_, stream_);
-        for (int g = 0; g < S && le == cudaSuccess; ++g) {
+    LevelGraph *lg = nullptr;
+    TY_CHECK(level_graph(prec, has_iso, qang, lg, err));
+    if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
+    TY_CUDA(cudaGraphLaunch(lg->exec, stream_));
+    if (end) TY_CUDA(cudaEventRecord(end, stream_));
+    return kOk;
+}
+
+// The level schedule's launches on stream_ (into a capture): one chain of
+// level launches per octant group, each on its own stream, forked from and
+// joined into stream_; consecutive levels of a chain use programmatic
+// dependent launch.
+cudaError_t Sweeper::enqueue_levels(int prec, bool has_iso, const double *qang)
+{
+    const void *iso = has_iso ? (prec ? (const void *)d_iso32_ : (const void *)d_iso_) : nullptr;
+    const LaunchShape &sh = shape_[prec ? 1 : 0];
+    const LevelArgs p = level_args(prec, iso, qang, d_psi_);
+    cudaError_t le = cudaSuccess;
+    const int S = sh.streams;
+    if (S > 1) le = cudaEventRecord(fork_, stream_);
+    for (int g = 0; g < S && le == cudaSuccess; ++g) {
         cudaStream_t st = S > 1 ? aux_[g] : stream_;
         if (S > 1) le = cudaStreamWaitEvent(st, fork_, 0);
         for (uint32_t l = 0; l < sched_.n_levels && le == cudaSuccess; ++l) {
@@ -699,7 +717,21 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         }
         if (S > 1 && le == cudaSuccess) le = cudaEventRecord(join_[g], st);
         if (S > 1 && le == cudaSuccess) le = cudaStreamWaitEvent(stream_, join_[g], 0);
-        }
+    }
+    return le;
+}
+
+int Sweeper::level_graph(int prec, bool has_iso, const double *qang, LevelGraph *&lg, std::string &err)
+{
+    const LaunchShape &sh = shape_[prec ? 1 : 0];
+    if (sh.schedule != 1) { err = "no level graph for this schedule"; return kErrArg; }
+    if (sh.variant >= 2) TY_CHECK(ensure_records(prec, true, err, sh.variant == 4));
+    auto key = std::make_tuple(prec, has_iso, qang);
+    auto it = graphs_.find(key);
+    if (it == graphs_.end()) {
+        cudaGraph_t graph;
+        TY_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t le = enqueue_levels(prec, has_iso, qang);
         cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
         TY_CUDA(le);
         TY_CUDA(ce);
@@ -707,11 +739,100 @@ int Sweeper::levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg,
         cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
         TY_CUDA(ie);
-        it = graphs_.emplace(key, exec).first;
+        LevelGraph g;
+        g.exec = exec;
+        it = graphs_.emplace(key, g).first;
     }
-    if (beg) TY_CUDA(cudaEventRecord(beg, stream_));
-    TY_CUDA(cudaGraphLaunch(it->second, stream_));
-    if (end) TY_CUDA(cudaEventRecord(end, stream_));
+    lg = &it->second;
+    return kOk;
+}
+
+int Sweeper::capture_apply(int prec, const double *phi_in, bool with_fixed, double *phi_out, std::string &err)
+{
+    const double *qang = with_fixed ? d_qang_ : nullptr;
+    const double *qfix = with_fixed ? d_qiso_ : nullptr;
+    const bool has_iso = phi_in != nullptr || qfix != nullptr;
+    LevelGraph *lg = nullptr;
+    TY_CHECK(level_graph(prec, has_iso, qang, lg, err));  // cached: nothing is captured here
+    if (has_iso)
+        TY_CUDA(launch_scatter_source(phi_in, qfix, d_sigs_, d_scat_, d_iso_, prec ? d_iso32_ : nullptr, nc_,
+                                      (uint32_t)G_, stream_));
+    // the level launches themselves (not the level graph as a child node:
+    // a child graph loses the programmatic edges between its levels)
+    TY_CUDA(enqueue_levels(prec, has_iso, qang));
+    if (phi_out)
+        TY_CUDA(launch_psi_to_phi(d_psi_, prec == 1, d_w_, phi_out, nc_, (uint32_t)A_, (uint32_t)G_, stream_));
+    return kOk;
+}
+
+int Sweeper::si_step_graph(cudaGraphExec_t &exec, std::string &err)
+{
+    exec = nullptr;
+    if (shape_[0].schedule != 1) return kOk;
+    auto key = std::make_tuple(0, 0, 0);
+    auto it = step_graphs_.find(key);
+    if (it != step_graphs_.end()) { exec = it->second; return kOk; }
+    LevelGraph *lg = nullptr;
+    TY_CHECK(level_graph(0, true, d_qang_, lg, err));
+    const uint64_t n = phi_size();
+    // phi_old = phi; phi = T(phi_old); the L1 change and norm to the host
+    cudaGraph_t graph;
+    TY_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    int st = kOk;
+    cudaError_t e = cudaMemcpyAsync(d_tmp_, d_phi_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
+    if (e == cudaSuccess) st = capture_apply(0, d_tmp_, true, d_phi_, err);
+    if (e == cudaSuccess && st == kOk) e = l1_pair_dev(d_phi_, d_tmp_, n, red_, red_.result, stream_);
+    if (e == cudaSuccess && st == kOk)
+        e = cudaMemcpyAsync(red_.host, red_.result, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream_);
+    cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
+    TY_CHECK(st);
+    TY_CUDA(e);
+    TY_CUDA(ce);
+    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    TY_CUDA(ie);
+    step_graphs_.emplace(key, exec);
+    TY_CUDA(cudaGraphUpload(exec, stream_));  // its first launch then pays no upload
+    return kOk;
+}
+
+// Arnoldi step k of GMRES(m) with the precision-prec operator: w = V_{k+1} =
+// (I - K) V_k, classical Gram-Schmidt twice against V_0..V_k (coefficients
+// to result[0..k] and result[64..64+k]), ||w||^2 to result[128], w
+// normalized, its norm to result[129]; result[0..130) to the host.
+int Sweeper::arnoldi_step_graph(int prec, int k, cudaGraphExec_t &exec, std::string &err)
+{
+    exec = nullptr;
+    if (shape_[prec ? 1 : 0].schedule != 1 || k + 1 > 64) return kOk;
+    auto key = std::make_tuple(1, prec, k);
+    auto it = step_graphs_.find(key);
+    if (it != step_graphs_.end()) { exec = it->second; return kOk; }
+    LevelGraph *lg = nullptr;
+    TY_CHECK(level_graph(prec, true, nullptr, lg, err));
+    const uint64_t n = phi_size();
+    double *V = d_V_, *vk = V + (size_t)k * n, *w = V + (size_t)(k + 1) * n, *res = red_.result;
+    cudaGraph_t graph;
+    TY_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    int st = capture_apply(prec, vk, false, w, err);
+    cudaError_t e = cudaSuccess;
+    if (st == kOk) e = sub_from(vk, w, n, stream_);
+    for (int pass = 0; pass < 2 && st == kOk && e == cudaSuccess; ++pass) {
+        e = multi_dot_dev(w, V, n, k + 1, n, red_, res + 64 * pass, stream_);
+        if (e == cudaSuccess) e = multi_axpy(w, V, n, res + 64 * pass, k + 1, n, stream_);
+    }
+    if (st == kOk && e == cudaSuccess) e = multi_dot_dev(w, w, n, 1, n, red_, res + 128, stream_);
+    if (st == kOk && e == cudaSuccess) e = scale_by_norm(w, n, res + 128, res + 129, stream_);
+    if (st == kOk && e == cudaSuccess)
+        e = cudaMemcpyAsync(red_.host, res, sizeof(double) * 130, cudaMemcpyDeviceToHost, stream_);
+    cudaError_t ce = cudaStreamEndCapture(stream_, &graph);
+    TY_CHECK(st);
+    TY_CUDA(e);
+    TY_CUDA(ce);
+    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    TY_CUDA(ie);
+    step_graphs_.emplace(key, exec);
+    TY_CUDA(cudaGraphUpload(exec, stream_));  // its first launch then pays no upload
     return kOk;
 }
 
@@ -1000,6 +1121,7 @@ int Sweeper::ensure_krylov(int m, std::string &err)
 {
     if (m < 1 || m > 60) { err = "GMRES restart must be in 1..60"; return kErrArg; }
     if (krylov_m_ >= m) return kOk;
+    drop_step_graphs();  // they hold the basis's addresses
     if (d_V_) dev_free(d_V_, stream_);
     d_V_ = nullptr;
     TY_CUDA(dev_malloc(&d_V_, sizeof(double) * phi_size() * (m + 1), stream_));
@@ -1044,19 +1166,33 @@ int Sweeper::gmres(int prec, const double *b, double *x, int m, double rtol, int
         double est = beta;
         for (; k < m && its < iter_max;) {
             double *vk = V + (size_t)k * n, *w = V + (size_t)(k + 1) * n;
-            TY_CHECK(apply(prec, vk, false, w, nullptr, err));
-            (prec ? st.sweeps_fp32 : st.sweeps_fp64)++;
-            TY_CUDA(sub_from(vk, w, n, stream_));
+            // the whole Arnoldi step as one captured graph with the level
+            // schedule (one host synchronization for its coefficients)
+            cudaGraphExec_t step = nullptr;
+            TY_CHECK(arnoldi_step_graph(prec, k, step, err));
+            double hn = 0.0;
             for (int j = 0; j <= k; ++j) H[(size_t)j * m + k] = 0.0;
-            for (int pass = 0; pass < 2; ++pass) {
-                TY_CUDA(multi_dot(w, V, n, k + 1, n, red_, stream_));
-                for (int j = 0; j <= k; ++j) H[(size_t)j * m + k] += red_.host[j];
-                TY_CUDA(multi_axpy(w, V, n, red_.result, k + 1, n, stream_));
+            if (step) {
+                TY_CUDA(cudaGraphLaunch(step, stream_));
+                TY_CUDA(cudaStreamSynchronize(stream_));
+                last_psi_prec_ = prec;
+                for (int pass = 0; pass < 2; ++pass)
+                    for (int j = 0; j <= k; ++j) H[(size_t)j * m + k] += red_.host[64 * pass + j];
+                hn = red_.host[129];
+            } else {
+                TY_CHECK(apply(prec, vk, false, w, nullptr, err));
+                TY_CUDA(sub_from(vk, w, n, stream_));
+                for (int pass = 0; pass < 2; ++pass) {
+                    TY_CUDA(multi_dot(w, V, n, k + 1, n, red_, stream_));
+                    for (int j = 0; j <= k; ++j) H[(size_t)j * m + k] += red_.host[j];
+                    TY_CUDA(multi_axpy(w, V, n, red_.result, k + 1, n, stream_));
+                }
+                TY_CUDA(multi_dot(w, w, n, 1, n, red_, stream_));
+                hn = std::sqrt(red_.host[0]);
+                if (hn > 0.0) TY_CUDA(axpby(1.0 / hn, w, 0.0, w, n, stream_));
             }
-            TY_CUDA(multi_dot(w, w, n, 1, n, red_, stream_));
-            const double hn = std::sqrt(red_.host[0]);
+            (prec ? st.sweeps_fp32 : st.sweeps_fp64)++;
             H[(size_t)(k + 1) * m + k] = hn;
-            if (hn > 0.0) TY_CUDA(axpby(1.0 / hn, w, 0.0, w, n, stream_));
             for (int j = 0; j < k; ++j) {
                 const double h0 = H[(size_t)j * m + k], h1 = H[(size_t)(j + 1) * m + k];
                 H[(size_t)j * m + k] = cs[j] * h0 + sn[j] * h1;
@@ -1120,8 +1256,17 @@ int Sweeper::solve(const SolveOptions &o, double *phi_out, double *psi_out, Solv
     TY_CUDA(cudaSetDevice(device_));
     st = SolveStats();
     const uint64_t n = phi_size();
-    // the Krylov basis is set-up, not solve time: allocated before the timed region
-    if (o.method == 1 || o.method == 2) TY_CHECK(ensure_krylov(o.restart, err));
+    // the Krylov basis and the captured step graphs are set-up, not solve
+    // time: made before the timed region
+    if (o.method == 1 || o.method == 2) {
+        TY_CHECK(ensure_krylov(o.restart, err));
+        const int prec = o.method == 2 ? 1 : 0;
+        cudaGraphExec_t g = nullptr;
+        for (int k = 0; k < o.restart; ++k) TY_CHECK(arnoldi_step_graph(prec, k, g, err));
+    } else if (o.method == 0) {
+        cudaGraphExec_t g = nullptr;
+        TY_CHECK(si_step_graph(g, err));
+    }
     cudaEvent_t e0, e1;
     TY_CUDA(cudaEventCreate(&e0));
     TY_CUDA(cudaEventCreate(&e1));
@@ -1130,14 +1275,24 @@ int Sweeper::solve(const SolveOptions &o, double *phi_out, double *psi_out, Solv
     int status = kOk;
     if (o.method == 0) {
         // SourceIteration::fixedPoint: L1 relative change of phi.
+        // each step one captured graph (copy, scattering source, the level
+        // graph, psi -> phi, the L1 pair to the host) with the level schedule
         TY_CUDA(cudaMemsetAsync(d_phi_, 0, sizeof(double) * n, stream_));
+        cudaGraphExec_t step = nullptr;
+        TY_CHECK(si_step_graph(step, err));
         int iter = 0;
         double error = 1.0;
         while (iter < o.iter_max && error > o.err_max) {
-            TY_CUDA(cudaMemcpyAsync(d_tmp_, d_phi_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
-            TY_CHECK(apply(0, d_tmp_, true, d_phi_, nullptr, err));
+            if (step) {
+                TY_CUDA(cudaGraphLaunch(step, stream_));
+                TY_CUDA(cudaStreamSynchronize(stream_));
+                last_psi_prec_ = 0;
+            } else {
+                TY_CUDA(cudaMemcpyAsync(d_tmp_, d_phi_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+                TY_CHECK(apply(0, d_tmp_, true, d_phi_, nullptr, err));
+                TY_CUDA(l1_pair(d_phi_, d_tmp_, n, red_, stream_));
+            }
             st.sweeps_fp64++;
-            TY_CUDA(l1_pair(d_phi_, d_tmp_, n, red_, stream_));
             error = red_.host[0] / red_.host[1];
             ++iter;
         }

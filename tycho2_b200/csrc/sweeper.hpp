@@ -145,8 +145,21 @@ public:
     int device() const { return device_; }
 
 private:
+    struct LevelGraph {
+        cudaGraphExec_t exec = nullptr;
+    };
     int levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg, cudaEvent_t end,
                std::string &err);
+    cudaError_t enqueue_levels(int prec, bool has_iso, const double *qang);
+    // The level graph of the level schedule (built and cached on first use).
+    int level_graph(int prec, bool has_iso, const double *qang, LevelGraph *&lg, std::string &err);
+    // One operator application appended to the graph being captured on
+    // stream_ (level schedule only; its level graph must exist already).
+    int capture_apply(int prec, const double *phi_in, bool with_fixed, double *phi_out, std::string &err);
+    // Captures (once) and returns the step graph of a source-iteration step
+    // or of Arnoldi step k; nullptr when the shape has no level graph.
+    int si_step_graph(cudaGraphExec_t &exec, std::string &err);
+    int arnoldi_step_graph(int prec, int k, cudaGraphExec_t &exec, std::string &err);
     // Reads (and clears) the dataflow schedule's device error word.
     int check_device_error(std::string &err);
     LevelArgs level_args(int prec, const void *iso, const double *qang, void *psi) const;
@@ -201,7 +214,12 @@ private:
     int krylov_m_ = 0;
     void *d_flush_ = nullptr;
     Reducer red_;
-    std::map<std::tuple<int, bool, const double *>, cudaGraphExec_t> graphs_;
+    // level graphs by (precision, with an isotropic source, angular source)
+    std::map<std::tuple<int, bool, const double *>, LevelGraph> graphs_;
+    // whole solver steps as graphs: (kind 0 = source iteration step, 1 =
+    // Arnoldi step k; precision; k); rebuilt when buffers or shapes change
+    std::map<std::tuple<int, int, int>, cudaGraphExec_t> step_graphs_;
+    void drop_step_graphs();
     // dataflow schedule
     LaunchShape shape_[2];  // [0] FP64, [1] FP32
     uint32_t *d_done_ = nullptr;   // per item: epoch of completion
