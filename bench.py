@@ -402,9 +402,10 @@ def run_batch_leg(grp, dev, count, seed=4321, profile=False, sample=None):
         upd += mesh.n_cells * 2 * p["sn"] ** 2 * p["groups"]
     setup = time.perf_counter() - t0
     out, phis = {}, {}
-    for method in ("si", "mixed"):
-        b = ty.BatchSolver(device=dev)
-        ids = [b.add(sw, method, err_max=1e-10, iter_max=5000, inner_tol=1e-5) for sw in sws]
+    for method in ("si", "mixed", "si_persistent", "mixed_persistent"):
+        b = ty.BatchSolver(device=dev, persistent=method.endswith("_persistent"))
+        method_name = method.split("_")[0]
+        ids = [b.add(sw, method_name, err_max=1e-10, iter_max=5000, inner_tol=1e-5) for sw in sws]
         grp.barrier()
         t = time.perf_counter()
         steps = 0
@@ -434,6 +435,8 @@ def run_batch_leg(grp, dev, count, seed=4321, profile=False, sample=None):
             "all_converged": all(r[1]["final_error"] <= 1e-10 for r in res)}
         b.close()
     err = [float(np.abs(m - f).sum() / np.abs(f).sum()) for m, f in zip(phis["mixed"], phis["si"])]
+    same = all(np.array_equal(a.view(np.uint64), b.view(np.uint64))
+               for k in ("si", "mixed") for a, b in zip(phis[k], phis[k + "_persistent"]))
     for sw in sws:
         sw.close()
     if sample is not None:  # the members the oracle checks after the timed legs
@@ -442,6 +445,13 @@ def run_batch_leg(grp, dev, count, seed=4321, profile=False, sample=None):
     return {"instances": count * grp.world, "updates_per_sweep": upd, "setup_s": setup,
             "kernel": "batch_direct_level_kernel (compact records)",
             "fp64_si": out["si"], "mixed": out["mixed"],
+            "persistent": {"form": "one persistent kernel per pass, device work queue over (member, level), "
+                                   "bounded grid barrier between levels",
+                           "fp64_si_solve_wall_s": out["si_persistent"]["solve_wall_s"],
+                           "mixed_solve_wall_s": out["mixed_persistent"]["solve_wall_s"],
+                           "fp64_pass_updates_per_s": out["si_persistent"]["fp64_pass_updates_per_s"],
+                           "fp32_pass_updates_per_s": out["mixed_persistent"]["fp32_pass_updates_per_s"],
+                           "bit_identical_to_level_launches": same},
             "phi_rel_err_l1_max_mixed_vs_fp64": grp.max(max(err)),
             "mixed_vs_fp64_solve_speedup": out["si"]["solve_wall_s"] / out["mixed"]["solve_wall_s"],
             "mixed_vs_fp64_pass_speedup": (out["mixed"]["fp32_pass_updates_per_s"]

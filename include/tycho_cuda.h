@@ -406,6 +406,20 @@ typedef struct tycho_batch_opts {
    registers, one thread per (item, group vector). */
 int tycho_batch_create(int device, int ipw32, int ipw64, tycho_batch **out);
 void tycho_batch_destroy(tycho_batch *b);
+/* The form of each pass's wavefront.  0 (default): one launch per global
+   level (captured in the pass's graph, consecutive levels overlapped by
+   programmatic dependent launch).  1: one persistent cooperative kernel per
+   pass that walks every global level, its warps taking (member, level)
+   chunks from a device work queue (one counter per level and vector-width
+   class), with a bounded grid barrier between levels; the per-chunk
+   arithmetic is the same, so results are bit-identical.  Direct kernels
+   only (ipw32 = ipw64 = 0).  The reference has no batched form
+   (src/GraphTraverser.cc:467-759 is its per-problem task queue). */
+int tycho_batch_set_persistent(tycho_batch *b, int on);
+/* Polls of the persistent form's grid barrier before it gives up: the step
+   then returns TYCHO_ERR_TIMEOUT and the batch stays usable.  Default
+   4,194,304; 0 gives up at the first barrier that is not already met. */
+int tycho_batch_set_wait_limit(tycho_batch *b, uint32_t polls);
 /* Adds a member (the sweeper must outlive its membership); its solve starts
    from phi = 0 at the next step.  *id identifies it. */
 int tycho_batch_add(tycho_batch *b, tycho_sweeper *sw, const tycho_batch_opts *opts, int *id);
@@ -416,7 +430,8 @@ int tycho_batch_step(tycho_batch *b, int *n_running);
 int tycho_batch_run(tycho_batch *b);
 /* A member's statistics and (phi != NULL) its phi, phi layout.  *done is 1
    once it has converged or hit a limit.  The member's sweeper keeps the FP64
-   psi of its last sweep (tycho_sweeper_write_psi). */
+   psi of its last sweep (tycho_sweeper_write_psi), except for a mixed
+   member that finished on a correction without a final FP64 sweep. */
 int tycho_batch_result(tycho_batch *b, int id, double *phi, tycho_solve_stats *stats, int *done);
 /* Device time of all passes so far (ms) and pass counts, [0] FP64, [1] FP32,
    and the cell x angle x group updates swept in each. */

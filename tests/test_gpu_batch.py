@@ -37,9 +37,9 @@ def _problem(workdir, case, seed):
     return sw, om, (st, ss, mat, q)
 
 
-def _solve(sws, method, ipw=16, **kw):
+def _solve(sws, method, ipw=16, persistent=False, **kw):
     import tycho2_b200 as ty
-    b = ty.BatchSolver(ipw32=ipw, ipw64=ipw)
+    b = ty.BatchSolver(ipw32=ipw, ipw64=ipw, persistent=persistent)
     ids = [b.add(sw, method, **kw) for sw in sws]
     b.run()
     out = [b.result(i) for i in ids]
@@ -159,3 +159,50 @@ def test_batch_members_with_other_solvers(built, workdir):
         assert done and rel_l1(pm, phi_ref) <= 1e-8, kind
     with pytest.raises(ty.TychoError):  # the shared-memory batch kernels take NoPivot only
         ty.BatchSolver(ipw32=16, ipw64=16).add(sws[0], "si")
+
+
+@pytest.mark.parametrize("method", ["si", "mixed"])
+def test_persistent_batch_is_bit_identical_to_level_launches(built, workdir, method):
+    """One persistent kernel per pass (device work queue over (member, level),
+    bounded grid barrier between levels) gives the same bits as one launch
+    per level, alone and in the mix; its FP64 source iteration is the
+    oracle's."""
+    probs = [_problem(workdir, c, 120 + k) for k, c in enumerate(CASES)]
+    sws = [p[0] for p in probs]
+    levels = _solve(sws, method, ipw=0, err_max=1e-10)
+    persist = _solve(sws, method, ipw=0, persistent=True, err_max=1e-10)
+    alone = [_solve([sw], method, ipw=0, persistent=True, err_max=1e-10)[0] for sw in sws[:2]]
+    for case, (pl, sl, _), (pp, sp, done) in zip(CASES, levels, persist):
+        assert done and bits_equal(pl, pp), case
+        assert sl == sp, case
+    for (pa, _, _), (pp, _, _) in zip(alone, persist[:2]):
+        assert bits_equal(pa, pp)
+    if method == "si":
+        from oracle.oracle import Oracle
+        (sw, om, (st, ss, mat, q)), case = probs[0], CASES[0]
+        o = Oracle(om, case[2], case[3])
+        _, phi_ref, it_ref, _ = o.source_iteration(st, ss, mat, q_iso=q, iter_max=400, err_max=1e-10)
+        if persist[0][1]["iterations"] == it_ref:
+            assert bits_equal(persist[0][0], phi_ref)
+
+
+def test_persistent_batch_barrier_timeout_is_an_error(built, workdir):
+    """A wait limit of 0 makes the grid barrier give up at its first level
+    that is not already met: the step fails with TYCHO_ERR_TIMEOUT (status
+    8), no fault, and a new batch on the same device then solves normally."""
+    import tycho2_b200 as ty
+    from tycho2_b200._capi import TychoError
+    probs = [_problem(workdir, c, 140 + k) for k, c in enumerate(CASES[:2])]
+    sws = [p[0] for p in probs]
+    b = ty.BatchSolver(ipw32=0, ipw64=0, persistent=True)
+    b.set_wait_limit(0)
+    for sw in sws:
+        b.add(sw, "si", err_max=1e-10)
+    with pytest.raises(TychoError) as e:
+        b.run()
+    assert e.value.status == 8 and "timed out" in str(e.value)
+    b.close()
+    ref = _solve(sws, "si", ipw=0, err_max=1e-10)
+    again = _solve(sws, "si", ipw=0, persistent=True, err_max=1e-10)
+    for (pr, _, _), (pa, _, done) in zip(ref, again):
+        assert done and bits_equal(pr, pa)

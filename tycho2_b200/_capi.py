@@ -101,6 +101,8 @@ SIGNATURES = {
     "tycho_sweeper_set_wait_limit": (C.c_int, [_P, C.c_uint32]),
     "tycho_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, _PP]),
     "tycho_batch_destroy": (None, [_P]),
+    "tycho_batch_set_persistent": (C.c_int, [_P, C.c_int]),
+    "tycho_batch_set_wait_limit": (C.c_int, [_P, C.c_uint32]),
     "tycho_batch_add": (C.c_int, [_P, _P, C.POINTER(BatchOpts), C.POINTER(C.c_int)]),
     "tycho_batch_remove": (C.c_int, [_P, C.c_int]),
     "tycho_batch_step": (C.c_int, [_P, C.POINTER(C.c_int)]),

@@ -65,6 +65,11 @@ Batch::~Batch()
         dev_release(pl.partials, stream_);
     }
     dev_release(norms_, stream_);
+    for (int p = 0; p < 2; ++p) {
+        dev_release(d_barrier_[p], stream_);
+        dev_release(d_queue_[p], stream_);
+    }
+    dev_release(d_ctl_, stream_);
     for (auto &e : ev_)
         if (e) cudaEventDestroy(e);
     if (join_) cudaEventDestroy(join_);
@@ -191,6 +196,16 @@ int Batch::ensure_capacity(std::string &err)
         TB_CUDA(dev_malloc(&norms_, sizeof(double) * 2 * cs, stream_));
         TB_CUDA(cudaMemsetAsync(norms_, 0, sizeof(double) * 2 * cs, stream_));
         const size_t lc = std::max<size_t>(cl, 1) * kBatchClasses;
+        for (int p = 0; p < 2; ++p) {  // the persistent form's counters, per pass
+            dev_release(d_barrier_[p], stream_);
+            dev_release(d_queue_[p], stream_);
+            TB_CUDA(dev_malloc(&d_barrier_[p], sizeof(unsigned long long), stream_));
+            TB_CUDA(dev_malloc(&d_queue_[p], sizeof(uint32_t) * lc, stream_));
+        }
+        if (!d_ctl_) {
+            TB_CUDA(dev_malloc(&d_ctl_, sizeof(uint32_t) * 4, stream_));
+            TB_CUDA(cudaMemsetAsync(d_ctl_, 0, sizeof(uint32_t) * 4, stream_));
+        }
         for (auto &pl : plan_) {  // one work list per pass: the two passes run at once
             dev_release(pl.segs, stream_);
             dev_release(pl.level_nseg, stream_);
@@ -343,9 +358,25 @@ int Batch::build_graph(int prec, std::string &err)
     cudaError_t e = launch_batch_plan(ipw, d_slots_[prec], n, max_levels_, rec_bytes, plan, st);
     if (e == cudaSuccess && prec == 0) e = launch_batch_accept(d_slots_[prec], plan, kStreamGrid, st);
     if (e == cudaSuccess) e = launch_batch_scatter(d_slots_[prec], plan, kStreamGrid, st);
-    for (uint32_t L = 0; L < max_levels_ && e == cudaSuccess; ++L)
-        e = prec ? launch_batch_level<float>(ipw, d_slots_[prec], plan, L, cuts[L], any_solver, st)
-                 : launch_batch_level<double>(ipw, d_slots_[prec], plan, L, cuts[L], any_solver, st);
+    if (persist_) {
+        const size_t lc = (size_t)std::max<uint32_t>(max_levels_, 1) * kBatchClasses;
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_barrier_[prec], 0, sizeof(unsigned long long), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_queue_[prec], 0, sizeof(uint32_t) * lc, st);
+        BatchPersistArgs a = {};
+        a.barrier = d_barrier_[prec];
+        a.queue = d_queue_[prec];
+        a.max_levels = max_levels_;
+        a.df.err = d_ctl_;
+        a.df.abort = d_ctl_ + 3;
+        a.df.spin_limit = spin_limit_;
+        if (e == cudaSuccess)
+            e = prec ? launch_batch_persist<float>(d_slots_[prec], plan, a, any_solver, st)
+                     : launch_batch_persist<double>(d_slots_[prec], plan, a, any_solver, st);
+    } else {
+        for (uint32_t L = 0; L < max_levels_ && e == cudaSuccess; ++L)
+            e = prec ? launch_batch_level<float>(ipw, d_slots_[prec], plan, L, cuts[L], any_solver, st)
+                     : launch_batch_level<double>(ipw, d_slots_[prec], plan, L, cuts[L], any_solver, st);
+    }
     if (e == cudaSuccess) e = launch_batch_psi_to_phi(prec == 1, d_slots_[prec], plan, kStreamGrid, st);
     if (e == cudaSuccess) e = launch_batch_post(d_slots_[prec], plan, kStreamGrid, st);
     if (e == cudaSuccess) e = launch_batch_finish(d_slots_[prec], plan, 64, st);
@@ -356,6 +387,33 @@ int Batch::build_graph(int prec, std::string &err)
     cudaGraphDestroy(g);
     TB_CUDA(ie);
     return kOk;
+}
+
+int Batch::set_persistent(bool on, std::string &err)
+{
+    if (on && (ipw_[0] != 0 || ipw_[1] != 0)) {
+        err = "the persistent batched form runs the direct kernels (items per warp 0)";
+        return kErrArg;
+    }
+    if (persist_ != on) {
+        persist_ = on;
+        invalidate();
+    }
+    return kOk;
+}
+
+// The persistent form's error words: a grid barrier that gave up.
+int Batch::check_ctl(std::string &err)
+{
+    if (!persist_ || !d_ctl_) return kOk;
+    uint32_t ctl[4] = {0, 0, 0, 0};
+    TB_CUDA(cudaMemcpyAsync(ctl, d_ctl_, sizeof ctl, cudaMemcpyDeviceToHost, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    if (ctl[0] == 0) return kOk;
+    TB_CUDA(cudaMemsetAsync(d_ctl_, 0, sizeof ctl, stream_));
+    TB_CUDA(cudaStreamSynchronize(stream_));
+    err = "batched persistent pass: grid barrier timed out at level " + std::to_string(ctl[1]);
+    return kErrTimeout;
 }
 
 int Batch::pass(int prec, std::string &err)
@@ -418,6 +476,7 @@ int Batch::step_finish(int &n_running, std::string &err)
     launched_ = false;
     TB_CUDA(cudaSetDevice(device_));
     TB_CUDA(cudaStreamSynchronize(stream_));
+    TB_CHECK(check_ctl(err));  // before any member advances on this step's norms
     const size_t n = members_.size();
     const int *before = before_;
     for (int p = 0; p < 2; ++p)

@@ -65,6 +65,13 @@ public:
     // Updates (cell x angle x group) swept so far, per precision.
     void updates(double out[2]) const { out[0] = updates_[0]; out[1] = updates_[1]; }
     int size() const { return (int)members_.size(); }
+    // Wavefront of each pass: false (default) one launch per global level;
+    // true one persistent cooperative launch with a device work queue and a
+    // bounded grid barrier between levels (direct kernels only).
+    int set_persistent(bool on, std::string &err);
+    // Polls of the persistent form's grid barrier before it gives up
+    // (the step then fails with a timeout and the batch stays usable).
+    void set_wait_limit(uint32_t polls) { spin_limit_ = polls; }
 
 private:
     enum State { kRunSI = 0, kRunOuter = 1, kRunInner = 2, kDone = 3, kRunFirst = 4 };
@@ -116,6 +123,14 @@ private:
     double updates_[2] = {0, 0};
     bool launched_ = false;
     int before_[2] = {0, 0};
+    // persistent form: per pass a barrier counter and a work-queue counter
+    // per (level, class); control words [0..2] error, [3] abort
+    bool persist_ = false;
+    uint32_t spin_limit_ = 1u << 22;
+    unsigned long long *d_barrier_[2] = {nullptr, nullptr};
+    uint32_t *d_queue_[2] = {nullptr, nullptr};
+    uint32_t *d_ctl_ = nullptr;
+    int check_ctl(std::string &err);
 };
 
 }  // namespace tycho

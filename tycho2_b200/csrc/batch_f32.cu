@@ -21,4 +21,12 @@ cudaError_t launch_batch_level<float>(int ipw, const BatchSlot *slots, const Bat
     return batch_level_launch(fn, slots, pl, level, cut, s);
 }
 
+template <>
+cudaError_t launch_batch_persist<float>(const BatchSlot *slots, const BatchPlan &pl, const BatchPersistArgs &a,
+                                        bool any_solver, cudaStream_t s)
+{
+    return any_solver ? batch_persist_launch<float, true, 1>(slots, pl, a, s)
+                      : batch_persist_launch<float, false, 4>(slots, pl, a, s);
+}
+
 }  // namespace tycho

@@ -194,47 +194,70 @@ __device__ __forceinline__ void batch_class_body(const BatchSlot *__restrict__ s
 // in global memory), so a warp's member lookup is a shared-memory search.
 constexpr uint32_t kBatchSegSmem = 256;
 
+// One chunk (32 tasks of one member at one level) of the direct form: the
+// member's segment found by binary search, its compact record rebuilt in
+// registers, the source loaded, then (after `wait`, which the caller uses to
+// wait for the previous level) the upwind rows and the solve.  L2_ONLY: the
+// upwind rows are read around L1 (they were written by other SMs during the
+// same launch).
+template <typename Real, int VG, bool ANY, bool L2_ONLY, typename Wait>
+__device__ __forceinline__ void batch_direct_chunk(const BatchSeg *segs, uint32_t nseg, uint32_t ch, uint32_t lane,
+                                                   Wait wait)
+{
+    const uint32_t k = upper_index(nseg, ch, [&](uint32_t m) { return segs[m].chunk_begin; });
+    const BatchSeg &sg = segs[k];
+    LevelArgs p = {};
+    p.psi = sg.psi;
+    p.iso = sg.iso;
+    p.G = sg.G;
+    p.vg = VG;
+    p.vmagic = sg.vmagic;
+    p.solver = sg.solver;
+    const uint32_t gpv = p.G / VG;
+    const uint32_t task = (ch - sg.chunk_begin) * 32u + lane;
+    const uint32_t itl = gpv == 1u ? task : __umulhi(task, p.vmagic);
+    const uint32_t g = (task - itl * gpv) * VG;
+    RegRecord<Real> R;
+    load_record((const CompactRecord<Real> *)sg.rec + itl, R, ANY ? p.solver : (uint32_t)kSolveNoPivot);
+    const bool live = R.u(0) != kSentinel;
+    PairIn<Real, VG> in;
+    if (live) pair_load_source<Real, VG>(p, R, g, in);
+    wait();
+    if (live) {
+        pair_load_upwind<Real, VG, L2_ONLY>(p, R, g, in);
+        pair_solve_store_any<Real, VG, RegRecord<Real>, ANY>(p, R, g, in);
+    }
+}
+
+// Stages a (level, class) list of segments in shared memory when it fits
+// (block-wide); returns the list to search.
+__device__ __forceinline__ const BatchSeg *batch_stage_segs(const BatchPlan &pl, uint32_t L, uint32_t cls,
+                                                            BatchSeg *sseg, uint32_t &nseg)
+{
+    nseg = pl.level_nseg[L * kBatchClasses + cls];
+    const BatchSeg *gsegs = pl.segs + ((size_t)L * kBatchClasses + cls) * pl.seg_stride;
+    const bool staged = nseg <= kBatchSegSmem;
+    if (staged)
+        for (uint32_t i = threadIdx.x; i < nseg; i += blockDim.x) sseg[i] = gsegs[i];
+    __syncthreads();
+    return staged ? sseg : gsegs;
+}
+
 template <typename Real, int VG, bool ANY>
 __device__ __forceinline__ void batch_direct_body(const BatchPlan &pl, uint32_t L, uint32_t cls, uint32_t blk,
                                                   uint32_t nblk, BatchSeg *sseg, bool &waited)
 {
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     const uint32_t nchunk = pl.level_nchunk[L * kBatchClasses + cls];
-    const uint32_t nseg = pl.level_nseg[L * kBatchClasses + cls];
-    const BatchSeg *gsegs = pl.segs + ((size_t)L * kBatchClasses + cls) * pl.seg_stride;
-    const bool staged = nseg <= kBatchSegSmem;
-    if (staged)
-        for (uint32_t i = threadIdx.x; i < nseg; i += blockDim.x) sseg[i] = gsegs[i];
-    __syncthreads();
-    const BatchSeg *segs = staged ? sseg : gsegs;
-    for (uint32_t ch = blk * 4u + w; ch < nchunk; ch += nblk * 4u) {
-        const uint32_t k = upper_index(nseg, ch, [&](uint32_t m) { return segs[m].chunk_begin; });
-        const BatchSeg &sg = segs[k];
-        LevelArgs p = {};
-        p.psi = sg.psi;
-        p.iso = sg.iso;
-        p.G = sg.G;
-        p.vg = VG;
-        p.vmagic = sg.vmagic;
-        p.solver = sg.solver;
-        const uint32_t gpv = p.G / VG;
-        const uint32_t task = (ch - sg.chunk_begin) * 32u + lane;
-        const uint32_t itl = gpv == 1u ? task : __umulhi(task, p.vmagic);
-        const uint32_t g = (task - itl * gpv) * VG;
-        RegRecord<Real> R;
-        load_record((const CompactRecord<Real> *)sg.rec + itl, R, ANY ? p.solver : (uint32_t)kSolveNoPivot);
-        const bool live = R.u(0) != kSentinel;
-        PairIn<Real, VG> in;
-        if (live) pair_load_source<Real, VG>(p, R, g, in);
-        if (!waited) {
-            pdl_wait_prerequisites();
-            waited = true;
-        }
-        if (live) {
-            pair_load_upwind<Real, VG, false>(p, R, g, in);
-            pair_solve_store_any<Real, VG, RegRecord<Real>, ANY>(p, R, g, in);
-        }
-    }
+    uint32_t nseg;
+    const BatchSeg *segs = batch_stage_segs(pl, L, cls, sseg, nseg);
+    for (uint32_t ch = blk * 4u + w; ch < nchunk; ch += nblk * 4u)
+        batch_direct_chunk<Real, VG, ANY, false>(segs, nseg, ch, lane, [&] {
+            if (!waited) {
+                pdl_wait_prerequisites();
+                waited = true;
+            }
+        });
 }
 
 // ANY: some member solves with Original or a Cramer solver (each member's
@@ -260,6 +283,49 @@ batch_direct_level_kernel(const BatchSlot *__restrict__ slots, BatchPlan pl, uin
     (void)slots;
 }
 
+// Persistent form of a pass's wavefront: one cooperative launch walks every
+// global level.  Within a level, for each vector-width class, the warps take
+// chunks from a device work queue (one counter per level and class, zeroed
+// before the launch) until the level's chunks run out; then every block
+// meets at a bounded grid barrier before the next level.  The per-chunk
+// arithmetic is the level kernels' (bit-identical results); upwind rows are
+// read around L1, since other SMs wrote them during this launch.
+template <typename Real, int VG, bool ANY>
+__device__ __noinline__ void batch_persist_class(const BatchPlan &pl, const BatchPersistArgs &a, uint32_t L,
+                                                    uint32_t cls, BatchSeg *sseg)
+{
+    const uint32_t nchunk = pl.level_nchunk[L * kBatchClasses + cls];
+    if (nchunk == 0) return;  // the same for every thread of the block
+    uint32_t nseg;
+    const BatchSeg *segs = batch_stage_segs(pl, L, cls, sseg, nseg);
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t *q = a.queue + L * kBatchClasses + cls;
+    for (;;) {
+        uint32_t ch = 0;
+        if (lane == 0) ch = atomicAdd(q, 1u);
+        ch = __shfl_sync(0xffffffffu, ch, 0);
+        if (ch >= nchunk) break;
+        batch_direct_chunk<Real, VG, ANY, true>(segs, nseg, ch, lane, [] {});
+    }
+    __syncthreads();  // the segment list is restaged for the next class
+}
+
+template <typename Real, bool ANY, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB)
+batch_persist_kernel(const BatchSlot *__restrict__ slots, BatchPlan pl, BatchPersistArgs a)
+{
+    __shared__ BatchSeg sseg[kBatchSegSmem];
+    for (uint32_t L = 0; L < a.max_levels; ++L) {
+        batch_persist_class<Real, 1, ANY>(pl, a, L, 0, sseg);
+        batch_persist_class<Real, 2, ANY>(pl, a, L, 1, sseg);
+        if constexpr (sizeof(Real) == 4) batch_persist_class<Real, 4, ANY>(pl, a, L, 2, sseg);
+        if (L + 1 < a.max_levels &&
+            !grid_barrier(a.barrier, (unsigned long long)(L + 1) * gridDim.x, a.df, L))
+            return;
+    }
+    (void)slots;
+}
+
 // One global level of the batched sweep, 4 warps per block, IPW items per
 // chunk.  Blocks [cut[c], cut[c+1]) serve vector-width class c (1, 2, 4
 // groups per access), so each block runs one kernel body.  The work list was
@@ -281,6 +347,38 @@ batch_level_kernel(const BatchSlot *__restrict__ slots, BatchPlan pl, uint32_t L
         batch_class_body<Real, IPW, 4>(slots, pl, L, 2, b - cut.c[2], cut.c[3] - cut.c[2], T, waited);
     }
     if (!waited) pdl_wait_prerequisites();
+}
+
+}  // namespace tycho
+
+namespace tycho {
+
+// Cooperative launch of the persistent form with as many blocks as can be
+// resident at once.
+template <typename Real, bool ANY, int MINB>
+cudaError_t batch_persist_launch(const BatchSlot *slots, const BatchPlan &pl, const BatchPersistArgs &a,
+                                 cudaStream_t s)
+{
+    const void *fn = (const void *)batch_persist_kernel<Real, ANY, MINB>;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(per_sm * sms));
+    cfg.blockDim = dim3(128);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    BatchPlan plc = pl;
+    BatchPersistArgs ac = a;
+    void *args[] = {(void *)&slots, (void *)&plc, (void *)&ac};
+    return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 }  // namespace tycho

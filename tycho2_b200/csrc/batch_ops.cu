@@ -192,6 +192,14 @@ cudaError_t launch_batch_level<double>(int ipw, const BatchSlot *slots, const Ba
     return level_launch(fn, slots, pl, level, cut, s);
 }
 
+template <>
+cudaError_t launch_batch_persist<double>(const BatchSlot *slots, const BatchPlan &pl, const BatchPersistArgs &a,
+                                         bool any_solver, cudaStream_t s)
+{
+    return any_solver ? batch_persist_launch<double, true, 1>(slots, pl, a, s)
+                      : batch_persist_launch<double, false, 4>(slots, pl, a, s);
+}
+
 cudaError_t launch_batch_plan(int ipw, const BatchSlot *slots, uint32_t n_slots, uint32_t max_levels,
                               uint32_t rec_bytes, const BatchPlan &pl, cudaStream_t s)
 {

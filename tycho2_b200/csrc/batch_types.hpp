@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "launch.hpp"
+
 namespace tycho {
 
 constexpr uint32_t kBatchChunk = 4096;  // phi elements per reduction chunk
@@ -87,6 +89,18 @@ cudaError_t launch_batch_finish(const BatchSlot *slots, const BatchPlan &pl, uns
 template <typename Real>
 cudaError_t launch_batch_level(int ipw, const BatchSlot *slots, const BatchPlan &pl, uint32_t level,
                                const BatchCuts &cut, bool any_solver, cudaStream_t s);
+// The whole wavefront of a pass in one cooperative launch (as many blocks as
+// can be resident; direct kernels only): barrier and queue counters zeroed
+// before the launch, the bounded barrier's control words in df.
+struct BatchPersistArgs {
+    unsigned long long *barrier;  // arrivals
+    uint32_t *queue;              // [level][class] chunks taken
+    uint32_t max_levels;
+    DataflowArgs df;              // err / abort / spin_limit of the barrier
+};
+template <typename Real>
+cudaError_t launch_batch_persist(const BatchSlot *slots, const BatchPlan &pl, const BatchPersistArgs &a,
+                                 bool any_solver, cudaStream_t s);
 template <>
 cudaError_t launch_batch_level<double>(int ipw, const BatchSlot *slots, const BatchPlan &pl, uint32_t level,
                                        const BatchCuts &cut, bool any_solver, cudaStream_t s);

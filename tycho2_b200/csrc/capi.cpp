@@ -518,6 +518,20 @@ int tycho_batch_create(int device, int ipw32, int ipw64, tycho_batch **out)
 
 void tycho_batch_destroy(tycho_batch *b) { delete b; }
 
+int tycho_batch_set_persistent(tycho_batch *b, int on)
+{
+    if (!b) return finish(TYCHO_ERR_ARG, "null batch");
+    std::string err;
+    return guarded([&] { return finish(b->b.set_persistent(on != 0, err), err); });
+}
+
+int tycho_batch_set_wait_limit(tycho_batch *b, uint32_t polls)
+{
+    if (!b) return finish(TYCHO_ERR_ARG, "null batch");
+    b->b.set_wait_limit(polls);
+    return TYCHO_OK;
+}
+
 int tycho_batch_add(tycho_batch *b, tycho_sweeper *sw, const tycho_batch_opts *o, int *id)
 {
     if (!b || !sw || !o || !id) return finish(TYCHO_ERR_ARG, "null argument");

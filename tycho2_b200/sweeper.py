@@ -327,11 +327,21 @@ class BatchSolver:
 
     BATCH_METHODS = {"si": 0, "mixed": 2}
 
-    def __init__(self, device=0, ipw32=0, ipw64=0):
+    def __init__(self, device=0, ipw32=0, ipw64=0, persistent=False):
+        """persistent: each pass's wavefront in one persistent kernel with a
+        device work queue over (member, level) instead of one launch per
+        level (tycho_batch_set_persistent)."""
         h = C.c_void_p()
         check(lib().tycho_batch_create(device, ipw32, ipw64, C.byref(h)))
         self._h = h
         self._members = {}
+        if persistent:
+            check(lib().tycho_batch_set_persistent(h, 1))
+
+    def set_wait_limit(self, polls):
+        """Polls of the persistent form's grid barrier before a step fails
+        with TYCHO_ERR_TIMEOUT."""
+        check(lib().tycho_batch_set_wait_limit(self._h, int(polls)))
 
     def add(self, sweeper, method="mixed", iter_max=1000, err_max=1e-10, inner_tol=1e-5,
             inner_max=200, refine_max=30):
