@@ -401,9 +401,17 @@ def run_batch_leg(grp, dev, count, seed=4321, profile=False, sample=None):
         sws.append(sw)
         upd += mesh.n_cells * 2 * p["sn"] ** 2 * p["groups"]
     setup = time.perf_counter() - t0
+    # the project's autotuner picks the batch's kernel shapes for these members
+    t0 = time.perf_counter()
+    tuned, tune_table = ty.BatchSolver.autotune(sws, device=dev)
+    tune_s = time.perf_counter() - t0
     out, phis = {}, {}
-    for method in ("si", "mixed", "si_persistent", "mixed_persistent"):
-        b = ty.BatchSolver(device=dev, persistent=method.endswith("_persistent"))
+    for method in ("si", "mixed", "si_other", "mixed_other"):
+        if method.endswith("_other"):  # the form the autotuner did not pick, for comparison
+            shape = {"ipw32": 0, "ipw64": 0, "persistent": not tuned["persistent"]}
+        else:
+            shape = tuned
+        b = ty.BatchSolver(device=dev, **shape)
         method_name = method.split("_")[0]
         ids = [b.add(sw, method_name, err_max=1e-10, iter_max=5000, inner_tol=1e-5) for sw in sws]
         grp.barrier()
@@ -436,22 +444,25 @@ def run_batch_leg(grp, dev, count, seed=4321, profile=False, sample=None):
         b.close()
     err = [float(np.abs(m - f).sum() / np.abs(f).sum()) for m, f in zip(phis["mixed"], phis["si"])]
     same = all(np.array_equal(a.view(np.uint64), b.view(np.uint64))
-               for k in ("si", "mixed") for a, b in zip(phis[k], phis[k + "_persistent"]))
+               for k in ("si", "mixed") for a, b in zip(phis[k], phis[k + "_other"]))
     for sw in sws:
         sw.close()
     if sample is not None:  # the members the oracle checks after the timed legs
         for i in batch_sample(params):
             sample.append((i, params[i], phis["si"][i], phis["mixed"][i]))
     return {"instances": count * grp.world, "updates_per_sweep": upd, "setup_s": setup,
-            "kernel": "batch_direct_level_kernel (compact records)",
+            "kernel": ("batch_persist_kernel" if tuned["persistent"] else "batch_direct_level_kernel")
+                      + (" (compact records)" if tuned["ipw32"] == 0 else " (ipw %d)" % tuned["ipw32"]),
             "fp64_si": out["si"], "mixed": out["mixed"],
-            "persistent": {"form": "one persistent kernel per pass, device work queue over (member, level), "
-                                   "bounded grid barrier between levels",
-                           "fp64_si_solve_wall_s": out["si_persistent"]["solve_wall_s"],
-                           "mixed_solve_wall_s": out["mixed_persistent"]["solve_wall_s"],
-                           "fp64_pass_updates_per_s": out["si_persistent"]["fp64_pass_updates_per_s"],
-                           "fp32_pass_updates_per_s": out["mixed_persistent"]["fp32_pass_updates_per_s"],
-                           "bit_identical_to_level_launches": same},
+            "autotune": {"pick": tuned, "seconds": tune_s, "table": tune_table},
+            "other_form": {"form": ("one launch per level" if tuned["persistent"] else
+                                    "one persistent kernel per pass, device work queue over (member, level), "
+                                    "bounded grid barrier between levels") + " (the form the autotuner did not pick)",
+                           "fp64_si_solve_wall_s": out["si_other"]["solve_wall_s"],
+                           "mixed_solve_wall_s": out["mixed_other"]["solve_wall_s"],
+                           "fp64_pass_updates_per_s": out["si_other"]["fp64_pass_updates_per_s"],
+                           "fp32_pass_updates_per_s": out["mixed_other"]["fp32_pass_updates_per_s"],
+                           "bit_identical_to_the_pick": same},
             "phi_rel_err_l1_max_mixed_vs_fp64": grp.max(max(err)),
             "mixed_vs_fp64_solve_speedup": out["si"]["solve_wall_s"] / out["mixed"]["solve_wall_s"],
             "mixed_vs_fp64_pass_speedup": (out["mixed"]["fp32_pass_updates_per_s"]

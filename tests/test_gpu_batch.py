@@ -206,3 +206,27 @@ def test_persistent_batch_barrier_timeout_is_an_error(built, workdir):
     again = _solve(sws, "si", ipw=0, persistent=True, err_max=1e-10)
     for (pr, _, _), (pa, _, done) in zip(ref, again):
         assert done and bits_equal(pr, pa)
+
+
+def test_batch_autotuner_picks_a_measured_shape(built, workdir):
+    """BatchSolver.autotune times each candidate shape on the members and
+    returns the fastest; the batch built with its pick solves as the default
+    one does (bit-identical: the shapes share the per-chunk arithmetic)."""
+    import tycho2_b200 as ty
+    probs = [_problem(workdir, c, 160 + k) for k, c in enumerate(CASES)]
+    sws = [p[0] for p in probs]
+    pick, table = ty.BatchSolver.autotune(sws, steps=2)
+    assert {"ipw32", "ipw64", "persistent"} <= set(pick)
+    assert len(table) == len(ty.BatchSolver.TUNE_SHAPES)
+    timed = [r for r in table if r.get("fp64_ms_per_pass") is not None]
+    assert timed and all(r["fp64_ms_per_pass"] > 0 and r["fp32_ms_per_pass"] > 0 for r in timed)
+    fastest64 = min(r["fp64_ms_per_pass"] for r in timed if r["persistent"] == pick["persistent"])
+    assert any(r["ipw"] == pick["ipw64"] and r["fp64_ms_per_pass"] == fastest64 for r in timed)
+    ref = _solve(sws, "si", ipw=0, err_max=1e-10)
+    b = ty.BatchSolver(**pick)
+    ids = [b.add(sw, "si", err_max=1e-10) for sw in sws]
+    b.run()
+    got = [b.result(i) for i in ids]
+    b.close()
+    for (pr, _, _), (pg, _, done) in zip(ref, got):
+        assert done and bits_equal(pr, pg)

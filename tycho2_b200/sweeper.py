@@ -373,6 +373,68 @@ class BatchSolver:
         stats = {k: getattr(st, k) for k, _ in _capi.SolveStats._fields_ if k != "seconds"}
         return phi, stats, bool(done.value)
 
+    # the shapes `autotune` tries: (items per warp, persistent)
+    TUNE_SHAPES = ((0, False), (0, True), (16, False), (8, False))
+
+    @classmethod
+    def autotune(cls, sweepers, device=0, steps=3, shapes=None):
+        """Picks the batch's kernel shapes for these members by timing them:
+        for each shape (items per warp 0 = compact records in registers, 8 /
+        16 = records staged in shared memory; one launch per level or the
+        persistent kernel), `steps` steps of FP64 source iteration (FP64
+        passes) and of the mixed solve's first FP32 passes, all members
+        active, pass time from CUDA events.  Shapes that do not fit in device
+        memory (full records for every member) are skipped.  Returns
+        (dict(ipw32, ipw64, persistent) of the fastest, the table)."""
+        table = []
+        items = sum(sw.mesh.n_cells * sw.n_angles for sw in sweepers)
+        try:
+            import torch
+            free = torch.cuda.mem_get_info(device)[0]
+        except Exception:
+            free = 0
+        for ipw, persistent in (shapes or cls.TUNE_SHAPES):
+            row = {"ipw": ipw, "persistent": persistent}
+            if ipw and items * (256 + 128) > 0.5 * free:
+                # full FP64 + FP32 records for every member would not fit
+                row.update(fp64_ms_per_pass=None, fp32_ms_per_pass=None, skipped="records do not fit")
+                table.append(row)
+                continue
+            for method, key in (("si", "fp64_ms_per_pass"), ("mixed", "fp32_ms_per_pass")):
+                b = None
+                try:
+                    b = cls(device=device, ipw32=ipw, ipw64=ipw, persistent=persistent)
+                    for sw in sweepers:
+                        b.add(sw, method, iter_max=10 * steps)
+                    for _ in range(steps):
+                        b.step()
+                    t = b.timing()
+                    p = "fp64" if method == "si" else "fp32"
+                    row[key] = t[p + "_ms"] / max(1, t[p + "_passes"])
+                except _capi.TychoError as e:
+                    row[key] = None
+                    row["skipped"] = str(e)[:120]
+                finally:
+                    if b is not None:
+                        b.close()
+            table.append(row)
+
+        def best(key, ok):
+            rows = [r for r in table if r.get(key) is not None and ok(r)]
+            return min(rows, key=lambda r: r[key]) if rows else None
+
+        # the form is shared by both passes: pick it on their sum, then each
+        # precision's items per warp within that form
+        forms = {}
+        for persistent in (False, True):
+            r64 = best("fp64_ms_per_pass", lambda r: r["persistent"] == persistent)
+            r32 = best("fp32_ms_per_pass", lambda r: r["persistent"] == persistent)
+            if r64 and r32:
+                forms[persistent] = (r64["fp64_ms_per_pass"] + r32["fp32_ms_per_pass"], r64["ipw"], r32["ipw"])
+        persistent = min(forms, key=lambda k: forms[k][0])
+        _, ipw64, ipw32 = forms[persistent]
+        return {"ipw32": ipw32, "ipw64": ipw64, "persistent": persistent}, table
+
     def timing(self):
         ms, passes, upd = np.zeros(2), np.zeros(2, np.int32), np.zeros(2)
         check(lib().tycho_batch_timing(self._h, ptr(ms), ptr(passes), ptr(upd)))
