@@ -193,7 +193,11 @@ def reference_sweep(inp, steps=1, warmup=0, phi_path=None):
     the hash of the last psi's bytes."""
     ncpu = os.cpu_count() or 1
     A = 2 * inp["sn"] ** 2
+    # one thread per core, each bound to its core (the reference parallelises
+    # over angle groups with OpenMP)
     env = dict(os.environ, OMP_NUM_THREADS=str(min(ncpu, A)))
+    env.setdefault("OMP_PROC_BIND", "close")
+    env.setdefault("OMP_PLACES", "cores")
     cmd = [os.path.join(REF_BIN, "ref_dump.x"), "bench", inp["pmesh"], str(inp["sn"]), str(inp["groups"]),
            inp["st"], inp["q"], str(steps), str(warmup)] + ([phi_path] if phi_path else [])
     r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
