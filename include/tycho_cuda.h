@@ -341,6 +341,17 @@ int tycho_sweeper_get_shape(const tycho_sweeper *sw, int precision, tycho_launch
 int tycho_sweeper_sweep_noalloc(tycho_sweeper *sw, int precision, const void *iso, void *psi,
                                 void *stream);
 
+/* The order in which each wavefront's (cell, direction) items are taken
+   within a (level, octant) segment: the reference's traversal priorities
+   (Priorities::calcPriorities, src/Priorities.cc:396-435, and the
+   schedules of src/Sweeper.cc:373-515) as work orders of the level
+   schedule.  0: increasing cell * A + angle (default); 1: b-levels, the
+   longest downwind chain first (intraAngleP 1); 2: a seeded random order
+   (intraAngleP 0).  psi is the same in every order (each item's arithmetic
+   does not depend on it); only the dataflow and persistent schedules, which
+   take items in this order, can run faster or slower. */
+int tycho_sweeper_set_work_order(tycho_sweeper *sw, int order);
+
 /* Bounded waits of the persistent kernels (dataflow schedule, persistent
    levels, tycho_sweeper_sweep_noalloc): polls of one completion flag or
    level barrier before a wait gives up, records the item and face it waited

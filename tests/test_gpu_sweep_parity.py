@@ -495,3 +495,49 @@ def test_fp64_refuses_slotted_rows(built, workdir):
         sw.configure(1, "levels", "compact", knob, 4)
     assert sw.shape(1)["knob"] == -172
     sw.close()
+
+
+@pytest.mark.parametrize("order", ["blevel", "random", "cell"])
+def test_work_orders_permute_each_segment_and_keep_psi(built, workdir, order):
+    """The reference's traversal priorities as work orders of the level
+    schedule (tycho_sweeper_set_work_order): each (level, octant) segment
+    holds the same items in another order -- for 'blevel' in non-increasing
+    b-level, the reference's Priorities -- and the FP64 psi stays
+    bit-identical to the oracle's under every schedule that takes items in
+    that order."""
+    from oracle.oracle import Oracle
+    mesh, om = kuhn(workdir, 5, 0.05, seed=37)
+    sn, G = 8, 4
+    o = Oracle(om, sn, G)
+    rng = np.random.default_rng(77)
+    st = rng.lognormal(0.0, 0.5, mesh.n_cells)
+    src = rng.uniform(-0.2, 1.0, o.psi_shape)
+    ref = o.sweep(st, src_ang=src)
+    sw = make(mesh, sn, G, levelling="host")
+    sw.set_cross_sections(st, np.zeros(mesh.n_cells))
+    items0, off0 = sw.schedule_arrays()
+    sw.set_work_order(order)
+    items1, off1 = sw.schedule_arrays()
+    assert np.array_equal(off0, off1)
+    for b, e in zip(off0[:-1], off0[1:]):
+        assert np.array_equal(np.sort(items0[b:e]), np.sort(items1[b:e]))
+    if order == "blevel":
+        _, _, blev, _ = mesh.levels(sn)
+        A = 2 * sn * sn
+        for b, e in zip(off1[:-1], off1[1:]):
+            seg = items1[b:e]
+            seg = seg[seg != 0xFFFFFFFF]
+            key = blev[seg % A, seg // A]
+            # within each octant group of the level: non-increasing b-level
+            octs = np.array([int(o.quadrature()[0][a] < 0) * 4 + int(o.quadrature()[1][a] < 0) * 2
+                             + int(o.quadrature()[2][a] < 0) for a in seg % A])
+            for oc in np.unique(octs):
+                k = key[octs == oc]
+                assert np.all(np.diff(k.astype(np.int64)) <= 0)
+    for shape in (("levels", "compact", 128), ("levels", "direct", 256), ("dataflow", "records", 16),
+                  ("persist", "records", 16), ("dataflow", "tiles", 2)):
+        sw.configure(0, *shape)
+        psi = np.full(sw.psi_shape, np.nan)
+        sw.sweep(psi, src)
+        assert bits_equal(psi, ref), (order, shape)
+    sw.close()

@@ -99,6 +99,7 @@ SIGNATURES = {
     "tycho_sweeper_get_shape": (C.c_int, [_P, C.c_int, C.POINTER(LaunchShape)]),
     "tycho_sweeper_sweep_noalloc": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "tycho_sweeper_set_wait_limit": (C.c_int, [_P, C.c_uint32]),
+    "tycho_sweeper_set_work_order": (C.c_int, [_P, C.c_int]),
     "tycho_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, _PP]),
     "tycho_batch_destroy": (None, [_P]),
     "tycho_batch_set_persistent": (C.c_int, [_P, C.c_int]),

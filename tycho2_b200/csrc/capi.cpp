@@ -485,6 +485,13 @@ int tycho_sweeper_apply(tycho_sweeper *h, int precision, const double *phi_in, i
     });
 }
 
+int tycho_sweeper_set_work_order(tycho_sweeper *h, int order)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    std::string err;
+    return guarded([&] { return finish(h->sw.set_work_order(order, err), err); });
+}
+
 int tycho_sweeper_set_wait_limit(tycho_sweeper *h, uint32_t polls)
 {
     if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");

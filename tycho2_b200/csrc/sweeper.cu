@@ -20,6 +20,7 @@
 #include <stdexcept>
 
 #include "devmem.hpp"
+#include "rng.hpp"
 #include "status.hpp"
 #include "trace.hpp"
 
@@ -91,6 +92,78 @@ Sweeper::~Sweeper()
         if (ev) cudaEventDestroy(ev);
     if (fork_) cudaEventDestroy(fork_);
     if (stream_) cudaStreamDestroy(stream_);
+}
+
+// A_f = area * omega.n of every item position (the schedule's order).
+int Sweeper::compute_item_abar(std::string &err)
+{
+    const MeshTables &t = *tables_;
+    std::vector<double> omega(3 * (size_t)A_);
+    std::copy(quad_.xi.begin(), quad_.xi.end(), omega.begin());
+    std::copy(quad_.eta.begin(), quad_.eta.end(), omega.begin() + A_);
+    std::copy(quad_.mu.begin(), quad_.mu.end(), omega.begin() + 2 * A_);
+    double *d_omega = nullptr, *d_normal = nullptr, *d_area = nullptr;
+    cudaError_t e = upload(d_omega, omega.data(), omega.size(), stream_);
+    if (e == cudaSuccess) e = upload(d_normal, t.normal.data(), t.normal.size(), stream_);
+    if (e == cudaSuccess) e = upload(d_area, t.area.data(), t.area.size(), stream_);
+    if (e == cudaSuccess)
+        e = launch_item_abar(d_items_, sched_.n_padded, A_, d_normal, d_area, d_omega, d_abar64_, d_abar32_, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    dev_free(d_omega, stream_);
+    dev_free(d_normal, stream_);
+    dev_free(d_area, stream_);
+    TY_CUDA(e);
+    return kOk;
+}
+
+int Sweeper::set_work_order(int order, std::string &err)
+{
+    if (order < 0 || order > 2) { err = "work order must be 0 (cell), 1 (b-level) or 2 (random)"; return kErrArg; }
+    if (order == work_order_) return kOk;
+    TY_CUDA(cudaSetDevice(device_));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    schedule_host();  // the item list on the host
+    std::vector<uint32_t> blev;
+    if (order == 1) b_levels(*tables_, quad_, sched_, blev);
+    const uint64_t nc = nc_;
+    const uint32_t A = (uint32_t)A_;
+    const size_t nseg = sched_.octant_offset.size() - 1;
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (size_t k = 0; k < nseg; ++k) {
+        const uint64_t b = sched_.octant_offset[k], e = sched_.octant_offset[k + 1];
+        uint64_t n = b;
+        while (n < e && sched_.items[n] != kSentinelItem) ++n;  // padding sits at the segment's end
+        uint32_t *it = sched_.items.data();
+        std::sort(it + b, it + n);  // the cell order: increasing cell * A + angle
+        if (order == 1) {
+            // Priorities' b-levels (src/Priorities.cc:59-164, intraAngleP 1):
+            // the longest downwind chain first
+            std::stable_sort(it + b, it + n, [&](uint32_t x, uint32_t y) {
+                return blev[(size_t)(x % A) * nc + x / A] > blev[(size_t)(y % A) * nc + y / A];
+            });
+        } else if (order == 2) {
+            // a seeded random order (intraAngleP 0), the same on every run
+            Rng rng(0x5eedull + k);
+            for (uint64_t i = n - b; i > 1; --i) std::swap(it[b + i - 1], it[b + rng.range(0, (int64_t)i - 1)]);
+        }
+    }
+    TY_CUDA(cudaMemcpyAsync(d_items_, sched_.items.data(), sizeof(uint32_t) * sched_.n_padded,
+                            cudaMemcpyHostToDevice, stream_));
+    TY_CHECK(compute_item_abar(err));
+    // everything kept per item position is stale
+    rec_valid_[0] = rec_valid_[1] = false;
+    crec_valid_[0] = crec_valid_[1] = false;
+    for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
+    graphs_.clear();
+    drop_step_graphs();
+    for (auto &g : chunk_graphs_)
+        if (g) cudaGraphExecDestroy(g);
+    chunk_graphs_.clear();
+    dev_free(d_chunk_pos_, stream_);
+    d_chunk_pos_ = nullptr;
+    chunk_k_ = 0;
+    work_order_ = order;
+    return kOk;
 }
 
 const Schedule &Sweeper::schedule_host() const
@@ -190,22 +263,9 @@ int Sweeper::init(std::shared_ptr<const MeshTables> tp, const SweeperOptions &o,
     TY_CUDA(upload(d_adj_, adj.data(), nc_, stream_));
     TY_CUDA(upload(d_nbrmap_, nmap.data(), nc_, stream_));
     TY_CUDA(upload(d_w_, quad_.wt.data(), (size_t)A_, stream_));
-    {
-        std::vector<double> omega(3 * (size_t)A_);
-        std::copy(quad_.xi.begin(), quad_.xi.end(), omega.begin());
-        std::copy(quad_.eta.begin(), quad_.eta.end(), omega.begin() + A_);
-        std::copy(quad_.mu.begin(), quad_.mu.end(), omega.begin() + 2 * A_);
-        double *d_omega = nullptr, *d_normal = nullptr, *d_area = nullptr;
-        TY_CUDA(upload(d_omega, omega.data(), omega.size(), stream_));
-        TY_CUDA(upload(d_normal, t.normal.data(), t.normal.size(), stream_));
-        TY_CUDA(upload(d_area, t.area.data(), t.area.size(), stream_));
-        TY_CUDA(dev_malloc(&d_abar64_, sizeof(double4) * std::max<uint64_t>(nitems, 1), stream_));
-        if (fp32_) TY_CUDA(dev_malloc(&d_abar32_, sizeof(float4) * std::max<uint64_t>(nitems, 1), stream_));
-        TY_CUDA(launch_item_abar(d_items_, nitems, A_, d_normal, d_area, d_omega, d_abar64_,
-                                 d_abar32_, stream_));
-        TY_CUDA(cudaStreamSynchronize(stream_));
-        dev_free(d_omega, stream_); dev_free(d_normal, stream_); dev_free(d_area, stream_);
-    }
+    TY_CUDA(dev_malloc(&d_abar64_, sizeof(double4) * std::max<uint64_t>(nitems, 1), stream_));
+    if (fp32_) TY_CUDA(dev_malloc(&d_abar32_, sizeof(float4) * std::max<uint64_t>(nitems, 1), stream_));
+    TY_CHECK(compute_item_abar(err));
     const size_t nphi = phi_size(), npsi = psi_size();
     TY_CUDA(dev_malloc(&d_psi_, sizeof(double) * std::max<size_t>(npsi, 1), stream_));
     TY_CUDA(cudaMemsetAsync(d_psi_, 0, sizeof(double) * npsi, stream_));

@@ -124,6 +124,11 @@ public:
     // Polls of one flag or barrier before a persistent kernel's bounded wait
     // gives up (dataflow, persistent levels and the no-alloc sweep).
     void set_wait_limit(uint32_t polls) { spin_limit_ = polls; }
+    // Order of the items within each (level, octant) segment of the schedule
+    // (results are the same in any order): 0 increasing cell * A + angle, 1
+    // Priorities' b-levels, longest downwind chain first, 2 seeded random.
+    int set_work_order(int order, std::string &err);
+    int work_order() const { return work_order_; }
     uint32_t wait_limit() const { return spin_limit_; }
     int solver() const { return solver_; }
 
@@ -150,6 +155,7 @@ private:
     };
     int levels(int prec, bool has_iso, const double *qang, cudaEvent_t beg, cudaEvent_t end,
                std::string &err);
+    int compute_item_abar(std::string &err);
     cudaError_t enqueue_levels(int prec, bool has_iso, const double *qang);
     // The level graph of the level schedule (built and cached on first use).
     int level_graph(int prec, bool has_iso, const double *qang, LevelGraph *&lg, std::string &err);
@@ -187,6 +193,7 @@ private:
     int solver_ = 1;  // SolveKind
     int last_psi_prec_ = -1;
     uint32_t spin_limit_ = 1u << 22;  // about 2-4 s of polling
+    int work_order_ = 0;
 
     cudaStream_t stream_ = nullptr;
     // level schedule on several streams: one per octant group, forked from

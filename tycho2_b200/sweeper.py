@@ -297,6 +297,14 @@ class SweeperCuda:
                                         int(bool(with_fixed)), C.c_void_p(phi_out.data_ptr()),
                                         C.c_void_p(stream.cuda_stream)))
 
+    WORK_ORDERS = {"cell": 0, "blevel": 1, "random": 2}
+
+    def set_work_order(self, order):
+        """Order of the items within each wavefront segment: 'cell'
+        (default), 'blevel' (the reference's b-level priorities, longest
+        downwind chain first) or 'random' (seeded); psi is the same."""
+        check(lib().tycho_sweeper_set_work_order(self._h, self.WORK_ORDERS[order]))
+
     def set_wait_limit(self, polls):
         """Polls of one flag or level barrier before a persistent kernel's
         bounded wait gives up (TYCHO_ERR_TIMEOUT); 0 gives up at the first
