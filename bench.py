@@ -44,6 +44,7 @@ sys.path.insert(0, ROOT)
 METRIC = "sweep cell*dir*grp updates/s (mixed-precision FP32 sweep, FP64 refinement)"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+NOMINAL_HBM_GBS = 7700.0  # B200 HBM3e, HGX figure
 
 
 def parse():
@@ -825,6 +826,7 @@ def run_b200(args):
                          "traffic_source": TRAFFIC_SOURCE if t32 is not None else None, "peak_kind": peak_kind,
                          "kernel": k32, "bytes_per_sweep": b32, "kernel_ms_per_sweep": lvl32,
                          "per": "one sweep (all of its launches)",
+                         "frac_of_nominal": ach32 / NOMINAL_HBM_GBS, "nominal_peak": NOMINAL_HBM_GBS,
                          "fp64": {"kernel": k64, "achieved": ach64, "frac": ach64 / peak,
                                   "bytes_per_sweep": b64, "kernel_ms_per_sweep": lvl64,
                                   "traffic": t64}},

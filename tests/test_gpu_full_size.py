@@ -90,3 +90,30 @@ def test_c2_gmres_phi_matches_oracle(c2):
                               iter_max=200, rtol=1e-12)
     assert rel_l1(phi64, phi_o) <= 1e-10
     assert rel_l1(phim, phi_o) <= 1e-8
+
+
+def test_c3_like_reduced_matches_oracle(built, tmp_path):
+    """The 64^3 S8 G=16 workload's definition (lognormal(0, 1) sigma_t,
+    downscatter rows summing to 0.99 sigma_t, box source) on an 8^3 mesh,
+    where the FP64 oracle fits: FP64 GMRES(30) and the mixed solve on the
+    GPU against the oracle's GMRES(30) to 1e-12 (the 64^3 check itself
+    compares the mixed solve with this FP64 GPU path)."""
+    import tycho2_b200 as ty
+    from oracle import kuhn_problem as kp
+    from oracle.oracle import Oracle, OracleMesh
+    w = dict(ty.problems.WORKLOADS["kuhn64_s8_g16"])
+    w["n"] = 8
+    mesh, st, ss, mat, q = ty.problems.make_problem(**w)
+    path = str(tmp_path / "c3small.pmesh")
+    mesh.write_pmesh(path)
+    sw = ty.SweeperCuda(mesh, 8, 16, fp32=True)
+    sw.set_cross_sections(st, ss, mat)
+    sw.set_source(q, "isotropic")
+    phi64, _, s64 = sw.solve("gmres", iter_max=600, err_max=1e-12, restart=30, want_psi=False)
+    phim, _, sm = sw.solve("mixed", iter_max=600, err_max=1e-10, restart=30, want_psi=False)
+    sw.close()
+    o = Oracle(OracleMesh(path), 8, 16)
+    _, phi_o, _, _ = o.krylov(st, ss, mat, q_iso=np.ascontiguousarray(q), restart=30, iter_max=600, rtol=1e-12)
+    assert rel_l1(phi64, phi_o) <= 1e-10
+    assert rel_l1(phim, phi_o) <= 1e-8
+    del kp
