@@ -99,7 +99,6 @@ def test_c3_like_reduced_matches_oracle(built, tmp_path):
     GPU against the oracle's GMRES(30) to 1e-12 (the 64^3 check itself
     compares the mixed solve with this FP64 GPU path)."""
     import tycho2_b200 as ty
-    from oracle import kuhn_problem as kp
     from oracle.oracle import Oracle, OracleMesh
     w = dict(ty.problems.WORKLOADS["kuhn64_s8_g16"])
     w["n"] = 8
@@ -116,4 +115,3 @@ def test_c3_like_reduced_matches_oracle(built, tmp_path):
     _, phi_o, _, _ = o.krylov(st, ss, mat, q_iso=np.ascontiguousarray(q), restart=30, iter_max=600, rtol=1e-12)
     assert rel_l1(phi64, phi_o) <= 1e-10
     assert rel_l1(phim, phi_o) <= 1e-8
-    del kp
