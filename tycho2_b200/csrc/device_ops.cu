@@ -68,7 +68,12 @@ template <typename Real>
 __global__ void psi_to_phi_kernel(const Real *__restrict__ psi, const double *__restrict__ w,
                                   double *__restrict__ phi, uint64_t nc, uint32_t A, uint32_t G)
 {
-    if (G >= 8) {  // a warp's 32 elements share one 128-byte line per angle
+    // 8..15 groups: one element per thread (a warp's 32 elements share one
+    // 128-byte line per angle); fewer or more: four elements per thread, 16
+    // bytes per angle, eight angles in flight (measured on the 64^3 G=16
+    // pass: 11.6 -> 10.9 ms FP32, 18.9 -> 17.2 ms FP64; at G=8 the element
+    // form is as fast)
+    if (G >= 8 && G < 16) {
         const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= nc * 4 * G) return;
         phi[i] = psi_to_phi_elem(psi, w, i, A, G);
@@ -225,8 +230,8 @@ cudaError_t launch_psi_to_phi(const void *psi, bool psi_fp32, const double *w, d
 {
     const uint64_t n = nc * 4 * G;
     if (n == 0) return cudaSuccess;
-    // one thread per element from 8 groups on, else per four elements
-    const unsigned grid = G >= 8 ? blocks_for(n) : blocks_for(n / 4);
+    // one thread per element for 8..15 groups, else per four elements
+    const unsigned grid = G >= 8 && G < 16 ? blocks_for(n) : blocks_for(n / 4);
     if (psi_fp32)
         psi_to_phi_kernel<float><<<grid, 256, 0, s>>>((const float *)psi, w, phi, nc, A, G);
     else
