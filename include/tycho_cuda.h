@@ -82,6 +82,22 @@ int tycho_version(void);
 
 /* Reads a one-partition .pmesh (src/ParallelMesh.hh:43-81). */
 int tycho_mesh_read_pmesh(const char *path, tycho_mesh **out);
+/* Reads one partition of a multi-partition .pmesh: what MPI rank
+   `partition` reads (ParallelMesh::readInParallel, src/ParallelMesh.cc:
+   581-690) with the tables TychoMesh builds from it, including the sides
+   (faces on the mesh or partition boundary, numbered in (cell, face)
+   order), their global face ids and the partition across each face
+   (src/TychoMeshIO.cc:196-262).  Such a mesh cannot be written back. */
+int tycho_mesh_read_pmesh_partition(const char *path, uint64_t partition, tycho_mesh **out);
+/* partition, number of partitions, and the number of faces toward another
+   partition (any pointer may be NULL). */
+int tycho_mesh_partition_info(const tycho_mesh *mesh, uint64_t *partition, uint64_t *n_partitions,
+                              uint64_t *n_bound_sides);
+/* side [n*4] (TychoMesh::getSide, UINT64_MAX on interior faces), adj_rank
+   [n*4] (getAdjRank: the partition across the face, this one for interior
+   faces, UINT64_MAX on the mesh boundary), side_gid [n_sides] (getLGSide);
+   any pointer may be NULL. */
+int tycho_mesh_side_tables(const tycho_mesh *mesh, uint64_t *side, uint64_t *adj_rank, uint64_t *side_gid);
 /* Reads a .smesh (src/SerialMesh.hh:43-68) as one partition, as the
    reference's util/PartitionColumns 1 1 would convert it. */
 int tycho_mesh_read_smesh(const char *path, tycho_mesh **out);
@@ -372,6 +388,53 @@ int tycho_sweeper_set_wait_limit(tycho_sweeper *sw, uint32_t polls);
    written. */
 int tycho_sweeper_apply(tycho_sweeper *sw, int precision, const double *phi_in, int with_fixed, double *phi_out,
                         void *stream);
+
+/* ---- one partition of a multi-partition mesh: Util::sweepLocal(psi,
+        source, psiBound) and CommSides (src/Util.cc:138-145,
+        src/CommSides.cc:48-240), the local sweep of the reference's PBJ and
+        Schur sweepers (src/SweeperPBJ.cc, src/SweeperSchur.cc) -------------
+   A sweeper made from a partition (tycho_mesh_read_pmesh_partition) reads
+   the incoming psi on faces toward other partitions from psiBound
+   (src/Transport.cc:766-773) instead of vacuum; every sweep, apply and
+   solve uses the values last set.  Level schedule only; not in a batch,
+   the service or the no-alloc sweep. */
+
+/* Number of faces toward other partitions (0: an ordinary sweeper). */
+int tycho_sweeper_bound_sides(const tycho_sweeper *sw, uint64_t *n_bound_sides);
+/* psiBound in the reference's PsiBoundData layout, host memory:
+   ((side * nAngles + angle) * 3 + fv) * nGroups + group over every side and
+   direction of the quadrature (src/PsiData.hh:253-262); only faces toward
+   another partition are read. */
+int tycho_sweeper_set_psi_bound(tycho_sweeper *sw, const double *psi_bound);
+/* The values held, in the same layout (zeros elsewhere). */
+int tycho_sweeper_get_psi_bound(tycho_sweeper *sw, double *psi_bound);
+
+/* CommSides on the device.  Toward partition q this partition sends, for
+   every (cell, face toward q, direction) with the face outgoing, in that
+   order (src/CommSides.cc:68-95), psi at the face's vertices fv = 0, 1, 2
+   for every group: a packet of 3 * nGroups doubles.  n_send / n_recv: the
+   reference's packet counts (any pointer may be NULL). */
+int tycho_sweeper_side_counts(tycho_sweeper *sw, uint64_t q, uint64_t *n_send, uint64_t *n_recv);
+/* (global side id, direction) of each packet sent to q, [n_send] each. */
+int tycho_sweeper_side_send_list(tycho_sweeper *sw, uint64_t q, uint64_t *gside, uint32_t *angle);
+/* The packets to q from the resident psi (the last sweep's) into dst, a
+   device buffer of n_send * 3 * nGroups doubles.  Ordered after the work on
+   `stream` and the sweeper's own; stream NULL: returns when done. */
+int tycho_sweeper_side_pack(tycho_sweeper *sw, uint64_t q, double *dst, void *stream);
+/* Once per neighbour: q's send list (from q's tycho_sweeper_side_send_list),
+   so that each packet from q lands at psiBound(g, fv, angle, this
+   partition's side with that global id) -- CommSides' receive
+   (src/CommSides.cc:209-234).  A packet for a direction outside an angle
+   shard is dropped. */
+int tycho_sweeper_side_link(tycho_sweeper *sw, uint64_t q, uint64_t n, const uint64_t *gside,
+                            const uint32_t *angle);
+/* Packets from q (device, n * 3 * nGroups doubles, in q's send order) into
+   psiBound.  Stream as for tycho_sweeper_side_pack. */
+int tycho_sweeper_side_unpack(tycho_sweeper *sw, uint64_t q, const double *src, void *stream);
+/* SweeperPBJ's convergence measure (src/SweeperPBJ.cc:181-195): L1 norms of
+   psi - psi_prev and of psi over the resident FP64 psi, then psi_prev = psi
+   (psi_prev starts at zero). */
+int tycho_sweeper_psi_change(tycho_sweeper *sw, double *diff, double *norm);
 
 /* Device timing of n back-to-back operator applications
    phi_out = D L^{-1} (M S phi_in + Q) in the given precision, on the

@@ -26,7 +26,8 @@ def lib():
         L = C.CDLL(LIB)
         P = C.c_void_p
         sig = {
-            "om_load_pmesh": (P, [C.c_char_p]), "om_free": (None, [P]),
+            "om_load_pmesh": (P, [C.c_char_p]), "om_load_pmesh_part": (P, [C.c_char_p, C.c_int64]),
+            "om_free": (None, [P]), "om_partition": (None, [P] * 5),
             "om_ncells": (C.c_uint64, [P]), "om_nnodes": (C.c_uint64, [P]),
             "om_nsides": (C.c_uint64, [P]), "om_tables": (None, [P] * 11),
             "oq_quadrature": (C.c_int, [C.c_int, P, P, P, P]),
@@ -35,7 +36,8 @@ def lib():
             "oc_set_gauss_elim": (None, [P, C.c_int]),
             "oc_quadrature": (None, [P] * 5), "oc_omega_dot_n": (None, [P, P]),
             "oc_levels": (None, [P, P, P]), "oc_blevels": (None, [P, P]),
-            "oc_sweep": (C.c_int, [P] * 5), "oc_psi_to_phi": (None, [P] * 3),
+            "oc_sweep": (C.c_int, [P] * 5), "oc_sweep_local": (C.c_int, [P] * 6),
+            "oc_psi_to_phi": (None, [P] * 3),
             "oc_scatter": (None, [P] * 5),
             "oc_source_iteration": (C.c_int, [P] * 6 + [C.c_int, C.c_double, P, P, P]),
             "oc_krylov": (C.c_int, [P] * 6 + [C.c_int, C.c_int, C.c_double, P, P, P]),
@@ -56,12 +58,25 @@ def _p(a):
 
 
 class OracleMesh:
-    def __init__(self, path):
-        self.h = lib().om_load_pmesh(str(path).encode())
+    """One partition of a .pmesh (partition None: the file must hold one)."""
+
+    def __init__(self, path, partition=None):
+        self.h = lib().om_load_pmesh_part(str(path).encode(), -1 if partition is None else int(partition))
         if not self.h:
             raise ValueError("oracle could not read %s" % path)
         self.n_cells = lib().om_ncells(self.h)
         self.n_sides = lib().om_nsides(self.h)
+        part, nparts = C.c_uint64(), C.c_uint64()
+        lib().om_partition(self.h, C.byref(part), C.byref(nparts), None, None)
+        self.partition, self.n_partitions = part.value, nparts.value
+
+    def partition_tables(self):
+        """adj_rank (c,4): the partition across each face (UINT64_MAX on the
+        mesh boundary); side_gid (n_sides): each side's global face id."""
+        ar = np.empty((self.n_cells, 4), np.uint64)
+        sg = np.empty(max(self.n_sides, 1), np.uint64)
+        lib().om_partition(self.h, None, None, _p(ar), _p(sg))
+        return ar, sg[:self.n_sides]
 
     def tables(self):
         n = self.n_cells
@@ -127,6 +142,18 @@ class Oracle:
         psi = np.zeros(self.psi_shape)
         st = np.ascontiguousarray(sigma_t, np.float64)
         r = lib().oc_sweep(self.h, _p(src_ang), _p(src_iso), _p(st), _p(psi))
+        assert r == 0
+        return psi
+
+    def sweep_local(self, sigma_t, psi_bound, src_ang=None, src_iso=None):
+        """Util::sweepLocal of this partition: psi_bound in PsiBoundData
+        layout (n_sides, A, 3, G), read on faces whose neighbour is another
+        partition."""
+        psi = np.zeros(self.psi_shape)
+        st = np.ascontiguousarray(sigma_t, np.float64)
+        pb = np.ascontiguousarray(psi_bound, np.float64)
+        assert pb.size == self.mesh.n_sides * self.A * 3 * self.G
+        r = lib().oc_sweep_local(self.h, _p(src_ang), _p(src_iso), _p(st), _p(pb), _p(psi))
         assert r == 0
         return psi
 

@@ -18,6 +18,14 @@
  *       SweepSchedule's b-levels: calcDependencies and calcLevels
  *       (src/SweepSchedule.cc:107-125, :472-508; the +-1e-10 omega.n rule)
  *       over every angle, (angle, cell) order, followed by their count.
+ *   sweep_local <pmesh> <snOrder> <nGroups> <sigmaT.f64> <source.f64> <psiBound.f64>
+ *               <out.f64> <outprefix>
+ *       one rank's partition (TYCHO_SHIM_RANK of TYCHO_SHIM_SIZE, see
+ *       ref_shim/mpi.h): Util::sweepLocal(psi, source, psiBound) under a
+ *       GraphTraverser without communication, as the PBJ and Schur sweepers
+ *       build it (src/Main.cc:283-315, src/Util.cc:138-145); psiBound in
+ *       PsiBoundData layout (nSides, A, 3, G).  Also dumps the partition's
+ *       adjCell, adjRank, side (u64, (c,4)) and lGSides (u64, nSides).
  *   bench <pmesh> <snOrder> <nGroups> <sigmaT.f64> <qiso.f64> <steps> <warmup> [<phi.f64>]
  *       times SweeperTraverse::sweep of an isotropic source on all OpenMP
  *       threads; prints REFBENCH with a hash of the last psi's bytes and,
@@ -82,7 +90,7 @@ static std::vector<double> load_f64(const std::string &path, size_t n)
     return v;
 }
 
-static void setup(const char *pmesh, int sn, int groups)
+static void setup(const char *pmesh, int sn, int groups, bool comm = true)
 {
     g_nAngleGroups = 1;
     #pragma omp parallel
@@ -108,7 +116,7 @@ static void setup(const char *pmesh, int sn, int groups)
     g_quadrature = new Quadrature(g_snOrder);
     g_tychoMesh = new TychoMesh(pmesh);
     g_graphTraverserForward =
-        new GraphTraverser(Direction_Forward, true, SweepData::getDataSizeInBytes());
+        new GraphTraverser(Direction_Forward, comm, SweepData::getDataSizeInBytes());
 }
 
 int main(int argc, char **argv)
@@ -165,6 +173,35 @@ int main(int argc, char **argv)
         SweeperTraverse sweeper;
         sweeper.sweep(psi, source, false);
         dump_f64(argv[7], &psi[0], psi.size());
+        return 0;
+    }
+    if (mode == "sweep_local" && argc == 10) {
+        setup(argv[2], atoi(argv[3]), atoi(argv[4]), false);
+        g_sigmaT = load_f64(argv[5], g_nCells);
+        g_sigmaS.assign(g_nCells, 0.0);
+        PsiData source, psi;
+        PsiBoundData psiBound;
+        std::vector<double> s = load_f64(argv[6], source.size());
+        for (size_t i = 0; i < source.size(); i++) source[i] = s[i];
+        std::vector<double> b = load_f64(argv[7], psiBound.size());
+        for (size_t i = 0; i < psiBound.size(); i++) psiBound[i] = b[i];
+        psi.setToValue(0.0);
+        Util::sweepLocal(psi, source, psiBound);
+        dump_f64(argv[8], &psi[0], psi.size());
+        const UINT nc = g_nCells, ns = g_tychoMesh->getNSides();
+        std::vector<UINT> adj(nc * 4), rank(nc * 4), side(nc * 4), lg(ns);
+        for (UINT c = 0; c < nc; c++)
+            for (UINT f = 0; f < 4; f++) {
+                adj[c * 4 + f] = g_tychoMesh->getAdjCell(c, f);
+                rank[c * 4 + f] = g_tychoMesh->getAdjRank(c, f);
+                side[c * 4 + f] = g_tychoMesh->getSide(c, f);
+            }
+        for (UINT i = 0; i < ns; i++) lg[i] = g_tychoMesh->getLGSide(i);
+        std::string pre = argv[9];
+        dump_u64(pre + "adj.u64", adj);
+        dump_u64(pre + "rank.u64", rank);
+        dump_u64(pre + "side.u64", side);
+        dump_u64(pre + "lgside.u64", lg);
         return 0;
     }
     if (mode == "si" && argc == 11) {

@@ -9,6 +9,17 @@
  * reached with one partition (the reference only talks to adjacent ranks,
  * of which a one-partition mesh has none), so they fail loudly if called.
  * MPI-IO maps onto stdio, which is all that a single writer/reader needs.
+ *
+ * One rank's view of a multi-partition run: TYCHO_SHIM_RANK and
+ * TYCHO_SHIM_SIZE (default 0 and 1) set what MPI_Comm_rank / MPI_Comm_size
+ * report, so that the reference reads that rank's partition of a .pmesh.
+ * With a size above 1, the only point-to-point exchange that a dump without
+ * inter-rank sweeps reaches -- TychoMesh's constructor asking each
+ * neighbouring rank for its cell and face across a partition side
+ * (src/TychoMeshIO.cc:298-333) -- completes without a peer: sends are
+ * dropped and receives read zeros, so getAdjCellFromSide /
+ * getAdjFaceFromSide hold zeros.  A dump run that way must not read them;
+ * probes and message counts still fail loudly.
  */
 #ifndef TYCHO_ORACLE_MPI_SHIM_H
 #define TYCHO_ORACLE_MPI_SHIM_H
@@ -62,6 +73,12 @@ static inline size_t tycho_shim_type_size(MPI_Datatype t)
     }
 }
 
+static inline int tycho_shim_env(const char *name, int dflt)
+{
+    const char *v = getenv(name);
+    return v ? atoi(v) : dflt;
+}
+
 static inline int tycho_shim_unreachable(const char *what)
 {
     fprintf(stderr, "mpi shim: %s called with one rank\n", what);
@@ -74,8 +91,11 @@ static inline int MPI_Init(int *argc, char ***argv)
 static inline int MPI_Init_thread(int *argc, char ***argv, int req, int *prov)
 { (void)argc; (void)argv; *prov = req; return MPI_SUCCESS; }
 static inline int MPI_Finalize(void) { return MPI_SUCCESS; }
-static inline int MPI_Comm_rank(MPI_Comm c, int *r) { (void)c; *r = 0; return MPI_SUCCESS; }
-static inline int MPI_Comm_size(MPI_Comm c, int *s) { (void)c; *s = 1; return MPI_SUCCESS; }
+static inline int MPI_Comm_rank(MPI_Comm c, int *r)
+{ (void)c; *r = tycho_shim_env("TYCHO_SHIM_RANK", 0); return MPI_SUCCESS; }
+static inline int MPI_Comm_size(MPI_Comm c, int *s)
+{ (void)c; *s = tycho_shim_env("TYCHO_SHIM_SIZE", 1); return MPI_SUCCESS; }
+static inline int tycho_shim_view(void) { return tycho_shim_env("TYCHO_SHIM_SIZE", 1) > 1; }
 static inline int MPI_Barrier(MPI_Comm c) { (void)c; return MPI_SUCCESS; }
 
 static inline int MPI_Allreduce(const void *s, void *r, int n, MPI_Datatype t,
@@ -89,9 +109,19 @@ static inline int MPI_Allreduce(const void *s, void *r, int n, MPI_Datatype t,
 static inline int MPI_Send(const void *b, int n, MPI_Datatype t, int d, int tag, MPI_Comm c)
 { (void)b; (void)n; (void)t; (void)d; (void)tag; (void)c; return tycho_shim_unreachable("MPI_Send"); }
 static inline int MPI_Isend(const void *b, int n, MPI_Datatype t, int d, int tag, MPI_Comm c, MPI_Request *rq)
-{ (void)b; (void)n; (void)t; (void)d; (void)tag; (void)c; (void)rq; return tycho_shim_unreachable("MPI_Isend"); }
+{
+    (void)b; (void)n; (void)t; (void)d; (void)tag; (void)c;
+    if (!tycho_shim_view()) return tycho_shim_unreachable("MPI_Isend");
+    *rq = MPI_REQUEST_NULL;
+    return MPI_SUCCESS;
+}
 static inline int MPI_Recv(void *b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Status *st)
-{ (void)b; (void)n; (void)t; (void)s; (void)tag; (void)c; (void)st; return tycho_shim_unreachable("MPI_Recv"); }
+{
+    (void)s; (void)tag; (void)c; (void)st;
+    if (!tycho_shim_view()) return tycho_shim_unreachable("MPI_Recv");
+    memset(b, 0, (size_t)n * tycho_shim_type_size(t));
+    return MPI_SUCCESS;
+}
 static inline int MPI_Irecv(void *b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Request *rq)
 { (void)b; (void)n; (void)t; (void)s; (void)tag; (void)c; (void)rq; return tycho_shim_unreachable("MPI_Irecv"); }
 static inline int MPI_Iprobe(int s, int tag, MPI_Comm c, int *flag, MPI_Status *st)
@@ -102,7 +132,7 @@ static inline int MPI_Get_count(const MPI_Status *st, MPI_Datatype t, int *n)
 static inline int MPI_Waitall(int n, MPI_Request *rq, MPI_Status *st)
 {
     (void)rq; (void)st;
-    return n == 0 ? MPI_SUCCESS : tycho_shim_unreachable("MPI_Waitall");
+    return n == 0 || tycho_shim_view() ? MPI_SUCCESS : tycho_shim_unreachable("MPI_Waitall");
 }
 static inline int MPI_Waitany(int n, MPI_Request *rq, int *idx, MPI_Status *st)
 {

@@ -45,7 +45,12 @@ typedef struct {
     uint64_t *face_cells;    /* (face,2) */
     uint64_t *face_nodes;    /* (face,3) */
     uint64_t *face_btype;    /* face boundary type */
+    uint64_t *face_gid;      /* face global id */
+    uint64_t *face_part;     /* (face,2) partitions of its two sides */
     uint64_t *cell_gid, *cell_mat;
+    uint64_t part, nparts;   /* which partition of how many */
+    uint64_t *adj_rank;      /* (c,f) partition across the face, OR_NONE on the mesh boundary */
+    uint64_t *side_gid;      /* (side) global face id of each side */
     /* TychoMesh tables */
     uint64_t *adj_cell;      /* (c,f) */
     uint64_t *adj_face;      /* (c,f) */
@@ -124,25 +129,33 @@ void om_free(OMesh *m)
     if (!m) return;
     free(m->coords); free(m->cell_nodes); free(m->cell_faces); free(m->face_cells);
     free(m->face_nodes); free(m->face_btype); free(m->cell_gid); free(m->cell_mat);
+    free(m->face_gid); free(m->face_part); free(m->adj_rank); free(m->side_gid);
     free(m->adj_cell); free(m->adj_face); free(m->side); free(m->f2c); free(m->c2f);
     free(m->nbr_vrtx); free(m->volume); free(m->area); free(m->normal);
     free(m);
 }
 
-/* Reads a one-partition .pmesh and builds the TychoMesh tables.
-   Returns NULL on any format error. */
-OMesh *om_load_pmesh(const char *path)
+/* Reads partition `part` of a .pmesh (part < 0: the file must hold one
+   partition) and builds the TychoMesh tables of that MPI rank's view
+   (src/ParallelMesh.cc:581-690, src/TychoMeshIO.cc:153-333).  Returns NULL
+   on any format error. */
+OMesh *om_load_pmesh_part(const char *path, int64_t part)
 {
     static const char name[32] = "Tycho 2 Parallel Mesh";
     FILE *fp = fopen(path, "rb");
     if (!fp) return NULL;
     OMesh *m = (OMesh *)calloc(1, sizeof(OMesh));
     char hdr[32];
-    uint64_t vp[2], off[2], cnt[3];
+    uint64_t vp[2], off, cnt[3];
     if (fread(hdr, 1, 32, fp) != 32 || memcmp(hdr, name, 32) != 0) goto fail;
-    if (read_u64(fp, vp, 2) || vp[0] != 2 || vp[1] != 1) goto fail;
-    if (read_u64(fp, off, 2)) goto fail;
-    if (fseek(fp, (long)off[0], SEEK_SET) != 0) goto fail;
+    if (read_u64(fp, vp, 2) || vp[0] != 2 || vp[1] == 0) goto fail;
+    if (part < 0 && vp[1] != 1) goto fail;
+    if (part < 0) part = 0;
+    if ((uint64_t)part >= vp[1]) goto fail;
+    m->part = (uint64_t)part;
+    m->nparts = vp[1];
+    if (fseek(fp, (long)(32 + (2 + part) * 8), SEEK_SET) != 0 || read_u64(fp, &off, 1)) goto fail;
+    if (fseek(fp, (long)off, SEEK_SET) != 0) goto fail;
     if (read_u64(fp, cnt, 3)) goto fail;
     m->nc = cnt[0]; m->nf = cnt[1]; m->nn = cnt[2];
     {
@@ -167,10 +180,15 @@ OMesh *om_load_pmesh(const char *path)
         m->face_cells = (uint64_t *)malloc(sizeof(uint64_t) * m->nf * 2);
         m->face_nodes = (uint64_t *)malloc(sizeof(uint64_t) * m->nf * 3);
         m->face_btype = (uint64_t *)malloc(sizeof(uint64_t) * m->nf);
+        m->face_gid = (uint64_t *)malloc(sizeof(uint64_t) * m->nf);
+        m->face_part = (uint64_t *)malloc(sizeof(uint64_t) * m->nf * 2);
         for (uint64_t f = 0; f < m->nf; f++) {
             m->face_cells[f * 2 + 0] = fbuf[f * 9 + 0];
             m->face_cells[f * 2 + 1] = fbuf[f * 9 + 1];
             for (int k = 0; k < 3; k++) m->face_nodes[f * 3 + k] = fbuf[f * 9 + 2 + k];
+            m->face_gid[f] = fbuf[f * 9 + 5];
+            m->face_part[f * 2 + 0] = fbuf[f * 9 + 6];
+            m->face_part[f * 2 + 1] = fbuf[f * 9 + 7];
             m->face_btype[f] = fbuf[f * 9 + 8];
         }
         m->coords = (double *)malloc(sizeof(double) * m->nn * 3);
@@ -208,12 +226,24 @@ OMesh *om_load_pmesh(const char *path)
             }
         }
     }
-    /* side numbering (src/TychoMeshIO.cc:230-254) */
+    /* side numbering and global ids (src/TychoMeshIO.cc:228-248), the
+       partition across each face (src/TychoMeshIO.cc:250-262) */
+    m->side_gid = (uint64_t *)malloc(sizeof(uint64_t) * (m->nsides ? m->nsides : 1));
+    m->adj_rank = (uint64_t *)malloc(sizeof(uint64_t) * nc * 4);
     {
         uint64_t s = 0;
         for (uint64_t c = 0; c < nc; c++)
-            for (uint64_t f = 0; f < 4; f++)
-                m->side[c * 4 + f] = (m->adj_cell[c * 4 + f] == OR_NONE) ? s++ : OR_NONE;
+            for (uint64_t f = 0; f < 4; f++) {
+                uint64_t face = m->cell_faces[c * 4 + handle[c * 4 + f]];
+                uint64_t p1 = m->face_part[face * 2], p2 = m->face_part[face * 2 + 1];
+                m->adj_rank[c * 4 + f] = (p1 == m->part) ? p2 : p1;
+                if (m->adj_cell[c * 4 + f] == OR_NONE) {
+                    m->side_gid[s] = m->face_gid[face];
+                    m->side[c * 4 + f] = s++;
+                } else {
+                    m->side[c * 4 + f] = OR_NONE;
+                }
+            }
     }
     /* faceToCellVrtx / cellToFaceVrtx (src/TychoMeshIO.cc:273-296): the face
        vertex index is the position of the node in the face record. */
@@ -293,6 +323,18 @@ void om_tables(const OMesh *m, uint64_t *adj_cell, uint64_t *nbr_vrtx, uint64_t 
 }
 
 void om_node_coords(const OMesh *m, double *out) { memcpy(out, m->coords, m->nn * 24); }
+
+OMesh *om_load_pmesh(const char *path) { return om_load_pmesh_part(path, -1); }
+
+/* partition, partition count; adjRank (c,4) and the sides' global ids (any
+   pointer may be NULL). */
+void om_partition(const OMesh *m, uint64_t *part, uint64_t *nparts, uint64_t *adj_rank, uint64_t *side_gid)
+{
+    if (part) *part = m->part;
+    if (nparts) *nparts = m->nparts;
+    if (adj_rank) memcpy(adj_rank, m->adj_rank, m->nc * 4 * 8);
+    if (side_gid) memcpy(side_gid, m->side_gid, m->nsides * 8);
+}
 
 /* ------------------------------------------------------------------------ */
 /* Quadrature (src/Quadrature.cc:150-244)                                    */
@@ -617,7 +659,8 @@ static void gauss_cramer_intel(double A[4][4], double b[4])
    :687-776).  Source per (v,g): angular part (psi layout, may be NULL) plus
    isotropic part (phi layout, may be NULL); exactly one addition when both. */
 static void cell_update(const OCtx *x, uint64_t c, int a, const double *src_ang,
-                        const double *src_iso, const double *sigma_t, double *psi)
+                        const double *src_iso, const double *sigma_t, const double *psi_bound,
+                        double *psi)
 {
     const OMesh *m = x->m;
     const int A = x->A, G = x->G;
@@ -663,7 +706,10 @@ static void cell_update(const OCtx *x, uint64_t c, int a, const double *src_ang,
         }
         /* populateLocalPsiBound + calcIncomingFlux (src/Transport.cc:740-776,
            :174-271).  Upwind psi at the neighbor vertex that shares cell
-           vertex j; vacuum (0) on mesh boundaries. */
+           vertex j; on a face whose neighbour is another partition, the
+           boundary value psiBound(g, fv, a, side) (psi_bound non-NULL:
+           PsiBoundData layout, src/PsiData.hh:253-262); vacuum (0) on mesh
+           boundaries. */
         for (int f = 0; f < 4; f++) {
             if (!(area[f] < 0)) continue;
             double pn[4] = {0.0, 0.0, 0.0, 0.0};
@@ -674,6 +720,13 @@ static void cell_update(const OCtx *x, uint64_t c, int a, const double *src_ang,
                     uint64_t fv = m->c2f[(c * 4 + f) * 4 + j];
                     uint64_t nv = m->nbr_vrtx[(c * 4 + f) * 3 + fv];
                     pn[j] = psi[(((size_t)adj * A + a) * 4 + nv) * G + g];
+                }
+            } else if (is_incoming(x, c, f, a) && psi_bound && m->adj_rank[c * 4 + f] != OR_NONE) {
+                uint64_t side = m->side[c * 4 + f];
+                for (int j = 0; j < 4; j++) {
+                    if (j == f) continue;
+                    uint64_t fv = m->c2f[(c * 4 + f) * 4 + j];
+                    pn[j] = psi_bound[(((size_t)side * A + a) * 3 + fv) * G + g];
                 }
             }
             for (int i = 0; i < 4; i++) {
@@ -703,7 +756,24 @@ int oc_sweep(const OCtx *x, const double *src_ang, const double *src_iso,
     #pragma omp parallel for schedule(dynamic)
     for (int a = 0; a < x->A; a++) {
         const uint32_t *ord = &x->order[(size_t)a * nc];
-        for (uint64_t i = 0; i < nc; i++) cell_update(x, ord[i], a, src_ang, src_iso, sigma_t, psi);
+        for (uint64_t i = 0; i < nc; i++) cell_update(x, ord[i], a, src_ang, src_iso, sigma_t, NULL, psi);
+    }
+    return 0;
+}
+
+/* One partition's local sweep with its incoming partition-boundary values:
+   Util::sweepLocal(psi, source, psiBound) under a GraphTraverser built
+   without communication (src/Util.cc:138-145, src/GraphTraverser.cc:442-458:
+   only faces to cells of this partition order the sweep). */
+int oc_sweep_local(const OCtx *x, const double *src_ang, const double *src_iso,
+                   const double *sigma_t, const double *psi_bound, double *psi)
+{
+    if (x->cyclic) return -1;
+    uint64_t nc = x->m->nc;
+    #pragma omp parallel for schedule(dynamic)
+    for (int a = 0; a < x->A; a++) {
+        const uint32_t *ord = &x->order[(size_t)a * nc];
+        for (uint64_t i = 0; i < nc; i++) cell_update(x, ord[i], a, src_ang, src_iso, sigma_t, psi_bound, psi);
     }
     return 0;
 }

@@ -21,6 +21,17 @@ reference built from it by `make -C oracle ref` (oracle/_ref).  Writes:
                                          CramerGlu, CramerIntel
                                si_*    : SourceIteration::fixedPoint with the
                                          hat source, per-cell sigma, S4, G=2
+  partitions_ref.npz         one partition's local sweep: a jittered Kuhn cube
+                             (4^3 hexes x 6 tets on [0,1]^3, oracle/kuhn_problem)
+                             split by the reference's PartitionColumns 2 1 and
+                             2 2:
+                               p{2,4}_pmesh          the partitioned mesh files
+                               p{P}_{p}_{adj,rank,side,lgside}  each partition's
+                                          adjCell, adjRank, side, lGSides
+                               p{P}_{p}_psi_hash     hash of Util::sweepLocal's
+                                          psi (S4, G=3) for the inputs of
+                                          tests/helpers.partition_inputs with
+                                          salt 10 P + p
   sweep_schedule_levels.npz  SweepSchedule's b-levels (calcDependencies and
                              calcLevels with their +-1e-10 omega.n rule) on the
                              jittered cube above and on an unjittered one
@@ -29,7 +40,7 @@ reference built from it by `make -C oracle ref` (oracle/_ref).  Writes:
                                {jit,flat}_s{4,6,8}  (angle, cell) levels, then
                                                     their maximum
 
-Run:  python tests/golden/make_golden.py [--levels-only]
+Run:  python tests/golden/make_golden.py [--levels-only | --partitions-only]
 """
 import hashlib
 import os
@@ -125,6 +136,41 @@ def levels_fixture(tmp):
     np.savez_compressed(os.path.join(HERE, "sweep_schedule_levels.npz"), **out)
 
 
+def partitions_fixture(tmp):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import partition_inputs, psi_hash
+    from oracle import kuhn_problem
+
+    mesh = kuhn_problem.kuhn_cube(4, 0.05, 7, 1.0)
+    smesh = os.path.join(tmp, "k4.smesh")
+    kuhn_problem.write_smesh(smesh, mesh)
+    out = {}
+    sn, G, A = 4, 3, 32
+    for px, py in ((2, 1), (2, 2)):
+        P = px * py
+        pmesh = os.path.join(tmp, "k4_%d.pmesh" % P)
+        run(os.path.join(REF_BIN, "PartitionColumns.x"), str(px), str(py), smesh, pmesh)
+        out["p%d_pmesh" % P] = np.fromfile(pmesh, np.uint8)
+        for p in range(P):
+            env = {"TYCHO_SHIM_RANK": str(p), "TYCHO_SHIM_SIZE": str(P), "OMP_NUM_THREADS": "2"}
+            pre = os.path.join(tmp, "t%d_%d_" % (P, p))
+            from oracle.oracle import OracleMesh
+            om = OracleMesh(pmesh, p)
+            st, src, pb = partition_inputs(om.n_cells, A, G, om.n_sides, 10 * P + p)
+            f_st, f_src, f_pb, f_psi = (os.path.join(tmp, n) for n in ("st.f64", "src.f64", "pb.f64", "psi.f64"))
+            st.tofile(f_st)
+            src.tofile(f_src)
+            pb.tofile(f_pb)
+            run(os.path.join(REF_BIN, "ref_dump.x"), "sweep_local", pmesh, str(sn), str(G), f_st, f_src, f_pb,
+                f_psi, pre, env=env)
+            for k in ("adj", "rank", "side", "lgside"):
+                out["p%d_%d_%s" % (P, p, k)] = np.fromfile(pre + k + ".u64", np.uint64)
+            psi = np.fromfile(f_psi, np.float64)
+            assert psi.size == om.n_cells * A * 4 * G
+            out["p%d_%d_psi_hash" % (P, p)] = np.array([psi_hash(psi)], np.uint64)
+    np.savez_compressed(os.path.join(HERE, "partitions_ref.npz"), **out)
+
+
 def main():
     if not os.path.isdir(REF):
         sys.exit("reference tree not found: %s" % REF)
@@ -132,9 +178,13 @@ def main():
     shutil.copyfile(os.path.join(REF, "test", "regression", "gold.psi"), os.path.join(HERE, "gold.psi"))
     shutil.copyfile(os.path.join(REF, "util", "cube-208.smesh"), os.path.join(HERE, "cube-208.smesh"))
     with tempfile.TemporaryDirectory() as tmp:
+        if "--partitions-only" in sys.argv:
+            partitions_fixture(tmp)
+            return
         if "--levels-only" not in sys.argv:
             kuhn3_fixture(tmp)
         levels_fixture(tmp)
+        partitions_fixture(tmp)
 
 
 if __name__ == "__main__":

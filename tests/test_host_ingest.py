@@ -160,14 +160,14 @@ def test_ingest_errors(built, workdir):
     with pytest.raises(TychoError) as e:
         ty.TychoMesh.read_pmesh(trunc)
     assert e.value.status == 3
-    # two partitions: the B200 sweep takes one mesh partition
+    # two partitions: the caller names the one to read
     two = bytearray(raw)
     two[40:48] = struct.pack("<Q", 2)
     p2 = os.path.join(d, "two.pmesh")
     open(p2, "wb").write(bytes(two))
     with pytest.raises(TychoError) as e:
         ty.TychoMesh.read_pmesh(p2)
-    assert e.value.status == 3 and "partition" in str(e.value)
+    assert e.value.status == 1 and "name the partition" in str(e.value)
     with pytest.raises(TychoError):
         ty.TychoMesh.kuhn_cube(0)
 

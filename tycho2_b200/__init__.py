@@ -7,7 +7,7 @@ is the host-side mirror of the reference's interface over that ABI.
 from ._capi import TychoError, lib  # noqa: F401
 from .sweeper import (BatchSolver, Quadrature, SolveServer, SweeperCuda, TychoMesh, device_memory,  # noqa: F401
                       footprint_bytes, release_cached_memory)
-from . import angles, problems  # noqa: F401
+from . import angles, partitions, problems  # noqa: F401
 
 __all__ = ["TychoError", "TychoMesh", "Quadrature", "SweeperCuda", "BatchSolver", "SolveServer",
-           "device_memory", "footprint_bytes", "release_cached_memory", "problems", "angles", "lib"]
+           "device_memory", "footprint_bytes", "release_cached_memory", "problems", "angles", "partitions", "lib"]

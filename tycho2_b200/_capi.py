@@ -65,6 +65,9 @@ SIGNATURES = {
     "tycho_version": (C.c_int, []),
     "tycho_mesh_read_pmesh": (C.c_int, [C.c_char_p, _PP]),
     "tycho_mesh_read_smesh": (C.c_int, [C.c_char_p, _PP]),
+    "tycho_mesh_read_pmesh_partition": (C.c_int, [C.c_char_p, C.c_uint64, _PP]),
+    "tycho_mesh_partition_info": (C.c_int, [_P, _U64P, _U64P, _U64P]),
+    "tycho_mesh_side_tables": (C.c_int, [_P, _P, _P, _P]),
     "tycho_mesh_kuhn_cube": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, C.c_double, _PP]),
     "tycho_mesh_from_arrays": (C.c_int, [C.c_uint64, C.c_uint64, _P, _P, _P, _P, _P, _PP]),
     "tycho_mesh_write_smesh": (C.c_int, [_P, C.c_char_p]),
@@ -100,6 +103,15 @@ SIGNATURES = {
     "tycho_sweeper_sweep_noalloc": (C.c_int, [_P, C.c_int, _P, _P, _P]),
     "tycho_sweeper_set_wait_limit": (C.c_int, [_P, C.c_uint32]),
     "tycho_sweeper_set_work_order": (C.c_int, [_P, C.c_int]),
+    "tycho_sweeper_bound_sides": (C.c_int, [_P, _U64P]),
+    "tycho_sweeper_set_psi_bound": (C.c_int, [_P, _P]),
+    "tycho_sweeper_get_psi_bound": (C.c_int, [_P, _P]),
+    "tycho_sweeper_side_counts": (C.c_int, [_P, C.c_uint64, _U64P, _U64P]),
+    "tycho_sweeper_side_send_list": (C.c_int, [_P, C.c_uint64, _P, _P]),
+    "tycho_sweeper_side_pack": (C.c_int, [_P, C.c_uint64, _P, _P]),
+    "tycho_sweeper_side_link": (C.c_int, [_P, C.c_uint64, C.c_uint64, _P, _P]),
+    "tycho_sweeper_side_unpack": (C.c_int, [_P, C.c_uint64, _P, _P]),
+    "tycho_sweeper_psi_change": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "tycho_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, _PP]),
     "tycho_batch_destroy": (None, [_P]),
     "tycho_batch_set_persistent": (C.c_int, [_P, C.c_int]),

@@ -124,6 +124,56 @@ int tycho_mesh_read_pmesh(const char *path, tycho_mesh **out)
     });
 }
 
+int tycho_mesh_read_pmesh_partition(const char *path, uint64_t partition, tycho_mesh **out)
+{
+    if (!path || !out) return finish(TYCHO_ERR_ARG, "null argument");
+    if (partition > (uint64_t)INT64_MAX) return finish(TYCHO_ERR_ARG, "bad partition");
+    return guarded([&] {
+        auto *m = new tycho_mesh;
+        std::string err;
+        int st = tycho::read_pmesh(path, m->rec, err, (int64_t)partition);
+        if (st != tycho::kOk) { delete m; return finish(st, err); }
+        return mesh_from_records(m, out);
+    });
+}
+
+int tycho_mesh_partition_info(const tycho_mesh *m, uint64_t *partition, uint64_t *n_partitions,
+                              uint64_t *n_bound_sides)
+{
+    if (!m) return finish(TYCHO_ERR_ARG, "null mesh");
+    const auto &t = m->tab;
+    if (partition) *partition = t.partition;
+    if (n_partitions) *n_partitions = t.n_partitions;
+    if (n_bound_sides) {
+        uint64_t n = 0;
+        if (!t.adj_rank.empty())
+            for (uint64_t i = 0; i < t.n_cells * 4; ++i)
+                n += t.adj_cell[i] == tycho::kNone && t.adj_rank[i] != tycho::kNone && t.adj_rank[i] != t.partition;
+        *n_bound_sides = n;
+    }
+    return TYCHO_OK;
+}
+
+int tycho_mesh_side_tables(const tycho_mesh *m, uint64_t *side, uint64_t *adj_rank, uint64_t *side_gid)
+{
+    if (!m) return finish(TYCHO_ERR_ARG, "null mesh");
+    const auto &t = m->tab;
+    if (side) std::memcpy(side, t.side.data(), sizeof(uint64_t) * t.side.size());
+    if (adj_rank) {
+        if (t.adj_rank.empty()) {
+            // tables from arrays: one partition, no partition boundary
+            for (uint64_t i = 0; i < t.n_cells * 4; ++i) adj_rank[i] = t.adj_cell[i] == tycho::kNone ? tycho::kNone : 0;
+        } else {
+            std::memcpy(adj_rank, t.adj_rank.data(), sizeof(uint64_t) * t.adj_rank.size());
+        }
+    }
+    if (side_gid) {
+        if (t.side_gid.size() == t.n_sides) std::memcpy(side_gid, t.side_gid.data(), sizeof(uint64_t) * t.n_sides);
+        else for (uint64_t i = 0; i < t.n_sides; ++i) side_gid[i] = i;
+    }
+    return TYCHO_OK;
+}
+
 int tycho_mesh_read_smesh(const char *path, tycho_mesh **out)
 {
     if (!path || !out) return finish(TYCHO_ERR_ARG, "null argument");
@@ -483,6 +533,82 @@ int tycho_sweeper_apply(tycho_sweeper *h, int precision, const double *phi_in, i
         return finish(h->sw.apply_external(precision, phi_in, with_fixed != 0, phi_out, (cudaStream_t)stream, err),
                       err);
     });
+}
+
+int tycho_sweeper_bound_sides(const tycho_sweeper *h, uint64_t *n_bound_sides)
+{
+    if (!h || !n_bound_sides) return finish(TYCHO_ERR_ARG, "null argument");
+    *n_bound_sides = h->sw.n_bound_sides();
+    return TYCHO_OK;
+}
+
+int tycho_sweeper_set_psi_bound(tycho_sweeper *h, const double *psi_bound)
+{
+    if (!h || !psi_bound) return finish(TYCHO_ERR_ARG, "null argument");
+    std::string err;
+    return guarded([&] { return finish(h->sw.set_psi_bound(psi_bound, err), err); });
+}
+
+int tycho_sweeper_get_psi_bound(tycho_sweeper *h, double *psi_bound)
+{
+    if (!h || !psi_bound) return finish(TYCHO_ERR_ARG, "null argument");
+    std::string err;
+    return guarded([&] { return finish(h->sw.get_psi_bound(psi_bound, err), err); });
+}
+
+int tycho_sweeper_side_counts(tycho_sweeper *h, uint64_t partition, uint64_t *n_send, uint64_t *n_recv)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    std::string err;
+    return guarded([&] {
+        uint64_t a = 0, b = 0;
+        int st = h->sw.side_counts(partition, a, b, err);
+        if (st == TYCHO_OK) {
+            if (n_send) *n_send = a;
+            if (n_recv) *n_recv = b;
+        }
+        return finish(st, err);
+    });
+}
+
+int tycho_sweeper_side_send_list(tycho_sweeper *h, uint64_t partition, uint64_t *gside, uint32_t *angle)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    std::string err;
+    return guarded([&] { return finish(h->sw.side_send_list(partition, gside, angle, err), err); });
+}
+
+int tycho_sweeper_side_pack(tycho_sweeper *h, uint64_t partition, double *dst, void *stream)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    std::string err;
+    return guarded([&] {
+        return finish(h->sw.side_pack(partition, dst, (cudaStream_t)stream, stream == nullptr, err), err);
+    });
+}
+
+int tycho_sweeper_side_link(tycho_sweeper *h, uint64_t partition, uint64_t n, const uint64_t *gside,
+                            const uint32_t *angle)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    std::string err;
+    return guarded([&] { return finish(h->sw.side_link(partition, n, gside, angle, err), err); });
+}
+
+int tycho_sweeper_side_unpack(tycho_sweeper *h, uint64_t partition, const double *src, void *stream)
+{
+    if (!h) return finish(TYCHO_ERR_ARG, "null sweeper");
+    std::string err;
+    return guarded([&] {
+        return finish(h->sw.side_unpack(partition, src, (cudaStream_t)stream, stream == nullptr, err), err);
+    });
+}
+
+int tycho_sweeper_psi_change(tycho_sweeper *h, double *diff, double *norm)
+{
+    if (!h || !diff || !norm) return finish(TYCHO_ERR_ARG, "null argument");
+    std::string err;
+    return guarded([&] { return finish(h->sw.psi_change(*diff, *norm, err), err); });
 }
 
 int tycho_sweeper_set_work_order(tycho_sweeper *h, int order)

@@ -108,11 +108,20 @@ void make_single_partition(MeshRecords &m)
     m.cell_gid.resize(m.n_cells);
     for (uint64_t c = 0; c < m.n_cells; ++c) m.cell_gid[c] = c;
     m.face_btype.assign(m.n_faces, 2);
-    for (uint64_t fc = 0; fc < m.n_faces; ++fc)
-        if (m.face_cells[fc * 2] == kNone || m.face_cells[fc * 2 + 1] == kNone) m.face_btype[fc] = 0;
+    m.face_gid.resize(m.n_faces);
+    m.face_part.assign(m.n_faces * 2, 0);
+    for (uint64_t fc = 0; fc < m.n_faces; ++fc) {
+        m.face_gid[fc] = fc;
+        if (m.face_cells[fc * 2] == kNone || m.face_cells[fc * 2 + 1] == kNone) {
+            m.face_btype[fc] = 0;
+            m.face_part[fc * 2 + (m.face_cells[fc * 2] == kNone ? 0 : 1)] = kNone;
+        }
+    }
+    m.partition = 0;
+    m.n_partitions = 1;
 }
 
-int read_pmesh(const std::string &path, MeshRecords &m, std::string &err)
+int read_pmesh(const std::string &path, MeshRecords &m, std::string &err, int64_t partition)
 {
     File f(path, "rb");
     if (!f.fp) { err = "cannot open " + path; return kErrIO; }
@@ -122,16 +131,26 @@ int read_pmesh(const std::string &path, MeshRecords &m, std::string &err)
         err = path + ": not a Tycho 2 parallel mesh"; return kErrFormat;
     }
     if (!rd(f.fp, vp, sizeof vp) || vp[0] != 2) { err = path + ": bad header"; return kErrFormat; }
-    if (vp[1] != 1) {
-        err = path + ": has " + std::to_string(vp[1]) + " partitions; the B200 sweep takes one";
-        return kErrFormat;
+    const uint64_t np = vp[1];
+    if (np == 0 || np > (1u << 24)) { err = path + ": bad partition count"; return kErrFormat; }
+    if (partition < 0 && np != 1) {
+        err = path + ": has " + std::to_string(np) + " partitions; name the partition to read";
+        return kErrArg;
     }
-    uint64_t off[2], cnt[3];
-    if (!rd(f.fp, off, sizeof off) || std::fseek(f.fp, (long)off[0], SEEK_SET) != 0 ||
-        !rd(f.fp, cnt, sizeof cnt)) {
+    const uint64_t part = partition < 0 ? 0 : (uint64_t)partition;
+    if (part >= np) {
+        err = path + ": partition " + std::to_string(part) + " of " + std::to_string(np);
+        return kErrArg;
+    }
+    // offsets[np + 1] follow the header; this partition's is offsets[part]
+    uint64_t off = 0, cnt[3];
+    if (std::fseek(f.fp, (long)(32 + (2 + part) * 8), SEEK_SET) != 0 || !rd(f.fp, &off, sizeof off) ||
+        std::fseek(f.fp, (long)off, SEEK_SET) != 0 || !rd(f.fp, cnt, sizeof cnt)) {
         err = path + ": truncated header"; return kErrFormat;
     }
     m = MeshRecords();
+    m.partition = part;
+    m.n_partitions = np;
     m.n_cells = cnt[0]; m.n_faces = cnt[1]; m.n_nodes = cnt[2];
     std::vector<uint64_t> cb(m.n_cells * 10), fb(m.n_faces * 9), nb(m.n_nodes * 4);
     if (!rd(f.fp, cb.data(), cb.size() * 8) || !rd(f.fp, fb.data(), fb.size() * 8) ||
@@ -149,13 +168,22 @@ int read_pmesh(const std::string &path, MeshRecords &m, std::string &err)
         m.cell_material[c] = cb[c * 10 + 9];
     }
     m.face_cells.resize(m.n_faces * 2); m.face_nodes.resize(m.n_faces * 3);
-    m.face_btype.resize(m.n_faces);
+    m.face_btype.resize(m.n_faces); m.face_gid.resize(m.n_faces); m.face_part.resize(m.n_faces * 2);
     for (uint64_t fc = 0; fc < m.n_faces; ++fc) {
         m.face_cells[fc * 2] = fb[fc * 9];
         m.face_cells[fc * 2 + 1] = fb[fc * 9 + 1];
         for (int k = 0; k < 3; ++k) m.face_nodes[fc * 3 + k] = fb[fc * 9 + 2 + k];
+        m.face_gid[fc] = fb[fc * 9 + 5];
+        m.face_part[fc * 2] = fb[fc * 9 + 6];
+        m.face_part[fc * 2 + 1] = fb[fc * 9 + 7];
         m.face_btype[fc] = fb[fc * 9 + 8];
         if (m.face_btype[fc] > 2) { err = path + ": bad boundary type"; return kErrFormat; }
+        // every face of a partition's records touches that partition
+        // (src/TychoMeshIO.cc:254-256)
+        if (m.face_part[fc * 2] != part && m.face_part[fc * 2 + 1] != part) {
+            err = path + ": a face of partition " + std::to_string(part) + " does not touch it";
+            return kErrFormat;
+        }
     }
     m.coords.resize(m.n_nodes * 3);
     for (uint64_t n = 0; n < m.n_nodes; ++n) std::memcpy(&m.coords[n * 3], &nb[n * 4], 24);
@@ -164,6 +192,10 @@ int read_pmesh(const std::string &path, MeshRecords &m, std::string &err)
 
 int write_pmesh(const std::string &path, const MeshRecords &m, std::string &err)
 {
+    if (m.n_partitions != 1) {
+        err = "one partition of a multi-partition mesh cannot be written as a one-partition .pmesh";
+        return kErrArg;
+    }
     File f(path, "wb");
     if (!f.fp) { err = "cannot open " + path; return kErrIO; }
     // Header, then partition 0 (src/ParallelMesh.hh:43-81, offsets as in
@@ -317,6 +349,25 @@ int build_tables(const MeshRecords &m, MeshTables &t, std::string &err)
     uint64_t s = 0;
     for (uint64_t c = 0; c < nc; ++c)
         for (int f = 0; f < 4; ++f) t.side[c * 4 + f] = (t.adj_cell[c * 4 + f] == kNone) ? s++ : kNone;
+
+    // sides in (cell, face) order with their global face ids, and the
+    // partition across each face (src/TychoMeshIO.cc:228-262)
+    t.partition = m.partition;
+    t.n_partitions = m.n_partitions;
+    t.side_gid.resize(t.n_sides);
+    t.adj_rank.resize(nc * 4);
+    for (uint64_t c = 0; c < nc; ++c)
+        for (int f = 0; f < 4; ++f) {
+            const uint64_t face = m.cell_faces[c * 4 + handle[c * 4 + f]];
+            if (t.side[c * 4 + f] != kNone) t.side_gid[t.side[c * 4 + f]] = m.face_gid[face];
+            const uint64_t p0 = m.face_part[face * 2], p1 = m.face_part[face * 2 + 1];
+            t.adj_rank[c * 4 + f] = p0 == m.partition ? p1 : p0;
+            if (m.face_btype[face] == 1 && (t.adj_rank[c * 4 + f] == kNone ||
+                                            t.adj_rank[c * 4 + f] >= m.n_partitions)) {
+                err = "partition boundary face without a valid neighbouring partition";
+                return kErrFormat;
+            }
+        }
 
     // The face-vertex index of a node is its slot in the face record
     // (src/TychoMeshIO.cc:273-296).

@@ -25,15 +25,24 @@ struct MeshRecords {
     std::vector<uint64_t> face_cells;   // (f,2), second = kNone on the boundary
     std::vector<uint64_t> face_nodes;   // (f,3)
     std::vector<uint64_t> face_btype;   // 0 mesh boundary, 1 partition boundary, 2 interior
+    std::vector<uint64_t> face_gid;     // global face id (identity for one partition)
+    std::vector<uint64_t> face_part;    // (f,2) partitions of the two sides, kNone on the mesh boundary
     std::vector<double> coords;         // (node,3)
+    uint64_t partition = 0, n_partitions = 1;  // which partition of how many the records hold
 };
 
 // The TychoMesh tables the sweep needs, all row-major [cell][face][...].
 struct MeshTables {
     uint64_t n_cells = 0, n_nodes = 0, n_sides = 0;
+    uint64_t partition = 0, n_partitions = 1;
     std::vector<uint64_t> adj_cell;        // (c,4)    kNone on the boundary
     std::vector<uint64_t> adj_face;        // (c,4)
     std::vector<uint64_t> side;            // (c,4)    kNone when interior
+    // (c,4) partition across each face (TychoMesh::getAdjRank): this
+    // partition for interior faces, kNone on the mesh boundary; empty for
+    // tables made from arrays (one partition, no partition boundary)
+    std::vector<uint64_t> adj_rank;
+    std::vector<uint64_t> side_gid;        // (n_sides) global face id of each side (getLGSide)
     std::vector<uint64_t> face_to_cell;    // (c,4,3)  faceToCellVrtx
     std::vector<uint64_t> cell_to_face;    // (c,4,4)  cellToFaceVrtx, kNone at [c][f][f]
     std::vector<uint64_t> neighbor_vrtx;   // (c,4,3)
@@ -49,7 +58,10 @@ struct MeshTables {
 // Status codes shared with the C ABI (see include/tycho_cuda.h).
 int read_smesh(const std::string &path, MeshRecords &out, std::string &err);
 int write_smesh(const std::string &path, const MeshRecords &m, std::string &err);
-int read_pmesh(const std::string &path, MeshRecords &out, std::string &err);
+// partition < 0: the file must hold one partition; otherwise the records of
+// that partition of a multi-partition file (one MPI rank's view,
+// src/ParallelMesh.cc:581-690).
+int read_pmesh(const std::string &path, MeshRecords &out, std::string &err, int64_t partition = -1);
 int write_pmesh(const std::string &path, const MeshRecords &m, std::string &err);
 
 // Adds the partition-0 fields (global ids, boundary types) that a one-partition

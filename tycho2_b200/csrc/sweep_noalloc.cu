@@ -90,6 +90,7 @@ int Sweeper::sweep_external(int prec, const void *iso, void *psi, uint32_t *done
     if (prec == 1 && !fp32_) { err = "sweeper was created without the FP32 sweep"; return kErrArg; }
     if (!have_xs_) { err = "cross sections not set"; return kErrMissing; }
     if (!psi) { err = "psi buffer is required"; return kErrArg; }
+    if (n_bound_sides()) { err = "faces toward other partitions: no no-alloc sweep"; return kErrArg; }
     if (solver_ != kSolveNoPivot) {
         err = "the no-alloc sweep runs the NoPivot solver only (GaussElim NoPivot)";
         return kErrArg;

@@ -83,8 +83,13 @@ Sweeper::~Sweeper()
     void *bufs[] = {d_items_, d_abar64_, d_abar32_, d_adj_, d_nbrmap_, d_cellk64_, d_cellk32_,
                     d_w_, d_sigs_, d_scat_, d_qiso_, d_qang_, d_src_, d_iso_, d_iso32_, d_psi_,
                     d_phi_, d_r_, d_tmp_, d_V_, d_h_, d_flush_, d_done_, d_ctl_, d_rec_[0], d_rec_[1],
-                    d_level_off_, d_barrier_, d_crec_[0], d_crec_[1], d_flags_};
+                    d_level_off_, d_barrier_, d_crec_[0], d_crec_[1], d_flags_, d_adj32_, d_psi_prev_};
     for (void *b : bufs) dev_free(b, stream_);
+    for (auto &kv : links_) {
+        dev_free(kv.second.d_send_row, stream_);
+        dev_free(kv.second.d_send_vtx, stream_);
+        dev_free(kv.second.d_recv_ghost, stream_);
+    }
     reducer_free(red_, stream_);
     for (auto &st : aux_)
         if (st) cudaStreamDestroy(st);
@@ -201,6 +206,8 @@ int Sweeper::init(std::shared_ptr<const MeshTables> tp, const SweeperOptions &o,
     // device, so that tycho_sweeper_sweep_noalloc itself loads nothing
     TY_CHECK(noalloc_scratch_prepare(device_, err));
     TY_CHECK(make_quadrature(o.sn_order, quad_, err));
+    n_angles_full_ = quad_.n_angles;
+    angle_begin_ = o.angle_begin;
     if (o.angle_begin != 0 || o.angle_end != 0) {
         // an angle shard: the directions [begin, end) with their weights, so
         // that phi is the partial sum over them (src/Util.cc:85-97 split by
@@ -238,37 +245,72 @@ int Sweeper::init(std::shared_ptr<const MeshTables> tp, const SweeperOptions &o,
     TY_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
     for (auto &ev : join_) TY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
 
+    // Faces toward another partition (one partition of a multi-partition
+    // mesh; src/TychoMeshIO.cc:250-262): bound sides b = 0.. in side order.
+    bound_side_.clear();
+    side_bound_.assign(t.n_sides, -1);
+    if (!t.adj_rank.empty())
+        for (uint64_t c = 0; c < nc_; ++c)
+            for (int f = 0; f < 4; ++f) {
+                const uint64_t r = t.adj_rank[c * 4 + f];
+                if (t.adj_cell[c * 4 + f] != kNone || r == kNone || r == t.partition) continue;
+                side_bound_[t.side[c * 4 + f]] = (int64_t)bound_side_.size();
+                bound_side_.push_back(t.side[c * 4 + f]);
+            }
+    n_bound_ = bound_side_.size();
+    if (n_bound_ && (2 * (nc_ + n_bound_) + n_bound_) * (uint64_t)A_ >= (1ull << 31)) {
+        err = "too many cells and partition sides";
+        return kErrArg;
+    }
+
     // Per-cell topology: neighbours and, per (face, local vertex), the
-    // neighbour's vertex index (neighborVrtx o cellToFaceVrtx).
-    std::vector<int4> adj(nc_);
+    // neighbour's vertex index (neighborVrtx o cellToFaceVrtx).  A face
+    // toward another partition names its ghost row instead, whose vertex fv
+    // = cellToFaceVrtx(c, f, j) holds psiBound(g, fv, a, side): the kernels
+    // read it as an upwind row, and the schedule orders nothing by it.
+    std::vector<int4> adj(nc_), adj32;
     std::vector<uint32_t> nmap(nc_, 0);
     for (uint64_t c = 0; c < nc_; ++c) {
         int a4[4];
         for (int f = 0; f < 4; ++f) {
             uint64_t n = t.adj_cell[c * 4 + f];
-            a4[f] = n == kNone ? -1 : (int)n;
-            if (n == kNone) continue;
+            const int64_t b = n == kNone && n_bound_ ? side_bound_[t.side[c * 4 + f]] : -1;
+            a4[f] = n != kNone ? (int)n : b >= 0 ? (int)(nc_ + (uint64_t)b) : -1;
+            if (n == kNone && b < 0) continue;
             for (int j = 0; j < 4; ++j) {
                 if (j == f) continue;
                 uint64_t fv = t.cell_to_face[(c * 4 + f) * 4 + j];
-                uint64_t nv = t.neighbor_vrtx[(c * 4 + f) * 3 + fv];
+                uint64_t nv = n == kNone ? fv : t.neighbor_vrtx[(c * 4 + f) * 3 + fv];
                 nmap[c] |= (uint32_t)(nv & 3u) << ((f * 4 + j) * 2);
             }
         }
         adj[c] = make_int4(a4[0], a4[1], a4[2], a4[3]);
     }
+    if (n_bound_ && o.fp32) {
+        adj32 = adj;
+        const int shift = (int)(nc_ + 2 * n_bound_);  // 2 (nc + B) + b = (nc + b) + (nc + 2B)
+        for (auto &a : adj32) {
+            int *v = &a.x;
+            for (int f = 0; f < 4; ++f)
+                if (v[f] >= (int)nc_) v[f] += shift;
+        }
+    }
     if (nc_ >= (1ull << 31)) { err = "too many cells"; return kErrArg; }
     const uint64_t nitems = sched_.n_padded;
     if (!on_device || !d_items_) TY_CUDA(upload(d_items_, sched_.items.data(), nitems, stream_));
     TY_CUDA(upload(d_adj_, adj.data(), nc_, stream_));
+    if (!adj32.empty()) TY_CUDA(upload(d_adj32_, adj32.data(), nc_, stream_));
     TY_CUDA(upload(d_nbrmap_, nmap.data(), nc_, stream_));
     TY_CUDA(upload(d_w_, quad_.wt.data(), (size_t)A_, stream_));
     TY_CUDA(dev_malloc(&d_abar64_, sizeof(double4) * std::max<uint64_t>(nitems, 1), stream_));
     if (fp32_) TY_CUDA(dev_malloc(&d_abar32_, sizeof(float4) * std::max<uint64_t>(nitems, 1), stream_));
     TY_CHECK(compute_item_abar(err));
     const size_t nphi = phi_size(), npsi = psi_size();
-    TY_CUDA(dev_malloc(&d_psi_, sizeof(double) * std::max<size_t>(npsi, 1), stream_));
-    TY_CUDA(cudaMemsetAsync(d_psi_, 0, sizeof(double) * npsi, stream_));
+    // psi rows, then the partition boundary's ghost rows (FP64, then FP32)
+    const size_t ghost = n_bound_ * (size_t)A_ * 4 * G_;
+    const size_t psi_bytes = sizeof(double) * (npsi + ghost) + (fp32_ ? sizeof(float) * ghost : 0);
+    TY_CUDA(dev_malloc(&d_psi_, std::max<size_t>(psi_bytes, 8), stream_));
+    TY_CUDA(cudaMemsetAsync(d_psi_, 0, psi_bytes, stream_));
     TY_CUDA(dev_malloc(&d_iso_, sizeof(double) * nphi, stream_));
     if (fp32_) TY_CUDA(dev_malloc(&d_iso32_, sizeof(float) * nphi, stream_));
     TY_CUDA(dev_malloc(&d_phi_, sizeof(double) * nphi, stream_));
@@ -322,6 +364,11 @@ int Sweeper::configure(int prec, int schedule, int variant, int knob, std::strin
         return kErrArg;
     }
     if (streams > 1 && schedule != 1) { err = "several streams: level schedule only"; return kErrArg; }
+    if (n_bound_ && schedule != 1) {
+        // the dataflow flags cover the cells' rows only
+        err = "faces toward other partitions: the level schedule only";
+        return kErrArg;
+    }
     if (vg == 0) vg = (int)record_vg(prec != 0, (uint32_t)G_);
     // one access moves up to 16 bytes (4 FP32 / 2 FP64 groups); the direct
     // variants on levels also take two such vectors per task (8 / 4)
@@ -462,7 +509,7 @@ int Sweeper::autotune(int prec, int reps, LaunchShape *best_shape, double *best_
     if (!have_xs_) { err = "cross sections not set"; return kErrMissing; }
     double best = 1e300;
     LaunchShape keep = shape_[prec ? 1 : 0];
-    for (int sched = 1; sched <= 3; ++sched)
+    for (int sched = 1; sched <= (n_bound_ ? 1 : 3); ++sched)
         for (int variant = 0; variant <= 4; ++variant)
             for (int knob : {1, 2, 4, 8, 16, 32, 64, 128, 256, -64, -80, -96, -128, -196, -180, -172}) {
                 if (knob < 0 && (variant < 3 || sched != 1)) continue;
@@ -532,7 +579,7 @@ LevelArgs Sweeper::level_args(int prec, const void *iso, const double *qang, voi
     LevelArgs p;
     p.items = d_items_;
     p.abar = prec ? (const void *)d_abar32_ : (const void *)d_abar64_;
-    p.adj = d_adj_;
+    p.adj = prec && d_adj32_ ? d_adj32_ : d_adj_;
     p.nbrmap = d_nbrmap_;
     p.cellk = prec ? (const void *)d_cellk32_ : (const void *)d_cellk64_;
     p.iso = iso;
@@ -550,6 +597,7 @@ LevelArgs Sweeper::level_args(int prec, const void *iso, const double *qang, voi
 int Sweeper::device_view(int prec, DeviceView &v, std::string &err, bool compact)
 {
     if (prec == 1 && !fp32_) { err = "sweeper was created without the FP32 sweep"; return kErrArg; }
+    if (n_bound_) { err = "faces toward other partitions: not in a batch"; return kErrArg; }
     if (!have_xs_) { err = "cross sections not set"; return kErrMissing; }
     TY_CUDA(cudaSetDevice(device_));
     TY_CHECK(ensure_records(prec, true, err, compact));

@@ -132,6 +132,36 @@ public:
     uint32_t wait_limit() const { return spin_limit_; }
     int solver() const { return solver_; }
 
+    // One partition of a multi-partition mesh (the sweep of Util::sweepLocal,
+    // src/Util.cc:138-145): faces whose neighbour is another partition take
+    // their incoming psi from psiBound (src/Transport.cc:766-773), kept on
+    // the device in both precisions.  Level schedule only.
+    uint64_t n_bound_sides() const { return n_bound_; }
+    // psi_bound: host memory in PsiBoundData layout ((side * A + a) * 3 + fv)
+    // * G + g over all sides and the whole quadrature (src/PsiData.hh:253-262);
+    // sides toward no other partition are not read.
+    int set_psi_bound(const double *psi_bound, std::string &err);
+    // The values held, in the same layout (other sides and, for an angle
+    // shard, other directions zero).
+    int get_psi_bound(double *psi_bound, std::string &err);
+    // CommSides (src/CommSides.cc:48-240) on the device: toward partition q,
+    // every (side, direction) whose face is outgoing here, in the reference's
+    // (cell, face, direction) order, carries psi at the face's three vertices
+    // (fv order) for every group.
+    int side_counts(uint64_t q, uint64_t &n_send, uint64_t &n_recv, std::string &err);
+    // (global side id, direction) of each packet sent to q.
+    int side_send_list(uint64_t q, uint64_t *gside, uint32_t *angle, std::string &err);
+    // packets to q from the resident psi into dst (device, FP64, [n][3][G]).
+    int side_pack(uint64_t q, double *dst, cudaStream_t s, bool sync, std::string &err);
+    // q's send list (its side_send_list), once: where each packet from q lands.
+    int side_link(uint64_t q, uint64_t n, const uint64_t *gside, const uint32_t *angle, std::string &err);
+    // packets from q (device, FP64, [n][3][G]) into the boundary values.
+    int side_unpack(uint64_t q, const double *src, cudaStream_t s, bool sync, std::string &err);
+    // L1 norms of psi - psi_prev and of psi over this sweeper's psi (FP64
+    // sweep), then psi_prev = psi: SweeperPBJ's convergence test
+    // (src/SweeperPBJ.cc:181-195).
+    int psi_change(double &diff, double &norm, std::string &err);
+
     const MeshTables &tables() const { return *tables_; }
     const Quadrature &quadrature() const { return quad_; }
     // Levels, offsets and counts; items and tlevel are empty when the
@@ -257,6 +287,29 @@ private:
     void *h_stage_[4] = {};
     cudaEvent_t ev_stage_[4] = {};
     unsigned long long *d_barrier_ = nullptr;
+    // partition boundary: bound side b <-> side; FP64 ghost rows (nc + b) * A
+    // + a follow the cells' psi rows, FP32 ghost rows (2 (nc + B) + b) * A + a
+    // follow the FP64 ghost rows (the FP32 neighbour table names those)
+    uint64_t n_bound_ = 0;
+    std::vector<uint64_t> bound_side_;
+    std::vector<int64_t> side_bound_;
+    int4 *d_adj32_ = nullptr;
+    int angle_begin_ = 0, n_angles_full_ = 0;
+    double *ghost64() const;
+    float *ghost32() const;
+    struct SideLink {
+        bool built = false;
+        std::vector<uint64_t> send_gside;
+        std::vector<uint32_t> send_angle;
+        uint64_t n_recv = 0;
+        uint64_t *d_send_row = nullptr;   // per packet: psi row c * A + a
+        uint32_t *d_send_vtx = nullptr;   // per packet: the face's cell vertices, 2 bits each
+        uint64_t n_link = 0;
+        uint64_t *d_recv_ghost = nullptr;  // per packet from q: ghost row b * A + a, or ~0
+    };
+    std::map<uint64_t, SideLink> links_;
+    int side_link_build(uint64_t q, SideLink *&l, std::string &err);
+    double *d_psi_prev_ = nullptr;
 };
 
 // The no-alloc sweep (tycho_sweeper_sweep_noalloc, sweep_noalloc.cu): scratch

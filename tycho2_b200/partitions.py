@@ -1,0 +1,318 @@
+"""Multi-partition sweeps: the reference's parallel block Jacobi (PBJ)
+sweepers over partition-local B200 sweeps.
+
+The reference splits a mesh into spatial partitions, one per MPI rank
+(util/PartitionColumns, src/ParallelMesh.cc).  Its PBJ sweepers sweep each
+partition on its own -- Util::sweepLocal(psi, source, psiBound), where the
+incoming psi on faces toward other partitions is psiBound, the values those
+partitions sent at the last exchange -- and then exchange boundary psi
+(CommSides::commSides), iterating until the partitions agree
+(src/SweeperPBJ.cc, src/CommSides.cc, src/Util.cc:138-145).
+
+Here a partition is a SweeperCuda made from one partition of the .pmesh
+(TychoMesh.read_pmesh(path, partition)); the exchange runs on the device
+(tycho_sweeper_side_pack / side_unpack).  The partitions of one problem
+live either in one process (PartitionSet: any devices, packets moved by
+device copies) or one per process (DistributedPartitions: packets moved by
+torch.distributed point-to-point sends, NCCL between GPUs).  Both present
+the same operations to the solvers below:
+
+  pbj_si     SweeperPBJSI::solve    src/SweeperPBJ.cc:218-280
+  pbj        SweeperPBJ::solve      src/SweeperPBJ.cc:147-211 (source
+             iteration whose every sweep iterates sweepLocal + commSides
+             until psi changes by at most ddErrMax)
+  pbj_outer  SweeperPBJOuter::solve src/SweeperPBJ.cc:59-141 (source
+             iteration to errMax with the boundary values fixed, then
+             commSides, until psi changes by at most ddErrMax)
+
+Iteration counts and convergence follow the reference's tests; the L1 sums
+run on the device, in another order than the reference's loops, so a
+change that lands within rounding of a tolerance may take one iteration
+more or less.  The converged phi is the single-partition solution's.
+"""
+import numpy as np
+
+from .sweeper import NONE, SweeperCuda, TychoMesh
+
+
+def neighbours_of(mesh):
+    """Partitions across this partition's faces toward other partitions,
+    in increasing order (CommSides::CommSides lists them by first
+    appearance; the order of exchanges does not change any value)."""
+    side, rank, _ = mesh.side_tables()
+    adj = mesh.tables()["adj_cell"]
+    sel = (adj == NONE) & (rank != NONE) & (rank != np.uint64(mesh.partition))
+    return sorted(int(r) for r in np.unique(rank[sel]))
+
+
+class GpuPartition:
+    """One partition's sweeper and its packet buffers."""
+
+    def __init__(self, sweeper):
+        import torch
+        self.sw = sweeper
+        self.mesh = sweeper.mesh
+        self.partition = self.mesh.partition
+        self.device = torch.device("cuda", sweeper.device)
+        self.neighbours = neighbours_of(self.mesh)
+        self._send = {}
+
+    def send_list(self, q):
+        return self.sw.side_send_list(q)
+
+    def link(self, q, gside, angle):
+        self.sw.side_link(q, gside, angle)
+
+    def pack(self, q):
+        import torch
+        n, _ = self.sw.side_counts(q)
+        buf = self._send.get(q)
+        if buf is None:
+            buf = self._send[q] = torch.empty(max(n, 1) * 3 * self.sw.n_groups, dtype=torch.float64,
+                                              device=self.device)
+        with torch.cuda.device(self.device):
+            if n:
+                self.sw.side_pack(q, buf)
+        return buf[:n * 3 * self.sw.n_groups]
+
+    def unpack(self, q, data):
+        import torch
+        with torch.cuda.device(self.device):
+            if data.numel():
+                self.sw.side_unpack(q, data)
+
+    def phi_zeros(self):
+        import torch
+        return torch.zeros(self.sw.phi_shape, dtype=torch.float64, device=self.device)
+
+    def apply(self, phi_in, phi_out, with_fixed):
+        import torch
+        with torch.cuda.device(self.device):
+            self.sw.apply(phi_in, phi_out, with_fixed=with_fixed)
+
+    def psi_change(self):
+        return self.sw.psi_change()
+
+
+class PartitionSet:
+    """Every partition of one problem in this process (emulated ranks).
+
+    `parts`: one GpuPartition (or any object with the same methods) per
+    partition, in partition order.  The exchange packs each partition's
+    packets for every neighbour and unpacks them at the neighbour, on that
+    neighbour's device."""
+
+    def __init__(self, parts):
+        self.parts = list(parts)
+        for p, part in enumerate(self.parts):
+            assert part.partition == p, "partitions must be given in order"
+        for part in self.parts:
+            for q in part.neighbours:
+                gs, an = part.send_list(q)
+                self.parts[q].link(part.partition, gs, an)
+
+    @classmethod
+    def from_pmesh(cls, path, sn_order, n_groups, devices=(0,), **kw):
+        """Sweepers on every partition of a .pmesh, placed round-robin on
+        `devices`; keyword arguments go to SweeperCuda."""
+        m0 = TychoMesh.read_pmesh(path, 0)
+        parts = []
+        for p in range(m0.n_partitions):
+            mesh = m0 if p == 0 else TychoMesh.read_pmesh(path, p)
+            sw = SweeperCuda(mesh, sn_order, n_groups, device=devices[p % len(devices)], **kw)
+            parts.append(GpuPartition(sw))
+        return cls(parts)
+
+    @property
+    def local(self):
+        return self.parts
+
+    def exchange(self):
+        """CommSides::commSides for every partition (src/CommSides.cc:119-240)."""
+        moved = []
+        for part in self.parts:
+            for q in part.neighbours:
+                moved.append((q, part.partition, part.pack(q)))
+        for q, src, data in moved:
+            dst = self.parts[q]
+            dev = getattr(dst, "device", None)
+            dst.unpack(src, data.to(dev) if dev is not None else data)
+
+    def allsum(self, values):
+        return list(values)
+
+    def close(self):
+        for part in self.parts:
+            sw = getattr(part, "sw", None)
+            if sw is not None:
+                sw.close()
+
+
+class DistributedPartitions:
+    """This process's partition of a problem spread over a torch.distributed
+    group, one partition per rank (rank r holds partition r).  Packets go by
+    point-to-point sends (isend / irecv) to each neighbour; sums by
+    all_reduce.  With the gloo backend the packets travel through host
+    memory."""
+
+    def __init__(self, part, group=None):
+        import torch
+        import torch.distributed as dist
+        self.part = part
+        self.group = group
+        self.rank = dist.get_rank(group)
+        assert part.partition == self.rank, "rank r holds partition r"
+        self.host = dist.get_backend(group) != "nccl"
+        self.sizes = {}
+        # send lists to the neighbours, received lists link the packets
+        for q in part.neighbours:
+            gs, an = part.send_list(q)
+            pairs = np.stack([gs.astype(np.int64), an.astype(np.int64)], axis=1).reshape(-1)
+            out = self._wire(torch.from_numpy(pairs.copy()))
+            n_out = self._wire(torch.tensor([pairs.size], dtype=torch.int64))
+            n_in = self._wire(torch.zeros(1, dtype=torch.int64))
+            self._swap(q, n_out, n_in)
+            got = self._wire(torch.zeros(int(n_in.item()), dtype=torch.int64))
+            self._swap(q, out, got)
+            got = got.cpu().numpy().reshape(-1, 2)
+            part.link(q, got[:, 0].astype(np.uint64), got[:, 1].astype(np.uint32))
+            self.sizes[q] = got.shape[0] * 3 * self._groups()
+
+    def _groups(self):
+        sw = getattr(self.part, "sw", None)
+        return sw.n_groups if sw is not None else self.part.n_groups
+
+    def _wire(self, t):
+        import torch
+        return t if self.host else t.to(torch.device("cuda", torch.cuda.current_device()))
+
+    def _swap(self, q, send, recv):
+        import torch.distributed as dist
+        ops = [dist.P2POp(dist.isend, send, q, self.group), dist.P2POp(dist.irecv, recv, q, self.group)]
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+
+    @property
+    def local(self):
+        return [self.part]
+
+    def exchange(self):
+        import torch
+        for q in self.part.neighbours:
+            data = self.part.pack(q)
+            send = data.cpu() if self.host and data.is_cuda else data
+            recv = torch.empty(self.sizes[q], dtype=torch.float64, device=send.device)
+            self._swap(q, send.contiguous(), recv)
+            dev = getattr(self.part, "device", None)
+            self.part.unpack(q, recv.to(dev) if dev is not None else recv)
+
+    def allsum(self, values):
+        import torch
+        import torch.distributed as dist
+        t = self._wire(torch.tensor(values, dtype=torch.float64))
+        dist.all_reduce(t, group=self.group)
+        return t.cpu().tolist()
+
+
+def _l1(parts, a, b):
+    """(sum |a - b|, sum |a|) over this process's partitions (b may be None)."""
+    d = m = 0.0
+    for x, y in zip(a, b if b is not None else [None] * len(a)):
+        m += float(x.abs().sum())
+        if y is not None:
+            d += float((x - y).abs().sum())
+    return d, m
+
+
+def pbj_si(ps, dd_iter_max=100, dd_err_max=1e-10):
+    """SweeperPBJSI::solve: phi1 = T(phi0) on every partition with the last
+    exchanged boundary values, exchange, stop when the L1 relative change of
+    phi is below dd_err_max (the exchange comes before the test, as in the
+    reference).  Returns (phi per local partition, iterations, change)."""
+    phi0 = [p.phi_zeros() for p in ps.local]
+    phi1 = [p.phi_zeros() for p in ps.local]
+    it, err = 1, 1.0
+    while it < dd_iter_max:
+        for p, a, b in zip(ps.local, phi0, phi1):
+            p.apply(a, b, True)
+        ps.exchange()
+        d, m = ps.allsum(_l1(ps.local, phi1, phi0))
+        err = d / m if m > 0 else 0.0
+        phi0, phi1 = phi1, phi0
+        if err < dd_err_max:
+            break
+        it += 1
+    return phi0, it, err
+
+
+def _pbj_sweep(ps, phi_old, phi_out, dd_iter_max, dd_err_max):
+    """SweeperPBJ::sweep: sweepLocal until psi changes by less than
+    dd_err_max (L1, relative), exchanging after every sweep that has not
+    converged.  Returns the number of local sweeps."""
+    it = 1
+    while it < dd_iter_max:
+        for p, a, b in zip(ps.local, phi_old, phi_out):
+            p.apply(a, b, True)
+        d, m = ps.allsum([sum(v) for v in zip(*[p.psi_change() for p in ps.local])])
+        if m > 0 and d / m < dd_err_max:
+            break
+        ps.exchange()
+        it += 1
+    return it
+
+
+def pbj(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10):
+    """SweeperPBJ::solve with source iteration (SourceIteration::fixedPoint,
+    src/SourceIteration.cc:127-207, over SweeperPBJ::sweep).  Returns (phi
+    per local partition, source iterations, last change, local sweeps)."""
+    phi_new = [p.phi_zeros() for p in ps.local]
+    phi_old = [p.phi_zeros() for p in ps.local]
+    it, err, sweeps = 0, 1.0, 0
+    while it < iter_max and err > err_max:
+        for a, b in zip(phi_old, phi_new):
+            a.copy_(b)
+        sweeps += _pbj_sweep(ps, phi_old, phi_new, dd_iter_max, dd_err_max)
+        d, m = ps.allsum(_l1(ps.local, phi_new, phi_old))
+        err = d / m if m > 0 else 0.0
+        it += 1
+    return phi_new, it, err, sweeps
+
+
+def pbj_outer(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10):
+    """SweeperPBJOuter::solve with source iteration: each outer iteration
+    runs SourceIteration::fixedPoint to err_max from the current psi with
+    the boundary values fixed, then tests the L1 change of psi against
+    dd_err_max and exchanges.  Returns (phi per local partition, outer
+    iterations, source iterations per outer iteration)."""
+    phi_new = [p.phi_zeros() for p in ps.local]
+    phi_old = [p.phi_zeros() for p in ps.local]
+    its = []
+    outer = 1
+    while outer < dd_iter_max:
+        it, err = 0, 1.0
+        while it < iter_max and err > err_max:
+            for a, b in zip(phi_old, phi_new):
+                a.copy_(b)
+            for p, a, b in zip(ps.local, phi_old, phi_new):
+                p.apply(a, b, True)
+            d, m = ps.allsum(_l1(ps.local, phi_new, phi_old))
+            err = d / m if m > 0 else 0.0
+            it += 1
+        its.append(it)
+        d, m = ps.allsum([sum(v) for v in zip(*[p.psi_change() for p in ps.local])])
+        if m > 0 and d / m < dd_err_max:
+            break
+        ps.exchange()
+        outer += 1
+    return phi_new, outer, its
+
+
+def gather_phi(ps_meshes, phis, n_cells_global):
+    """phi of every partition into one array in global cell order (cell_gid)."""
+    out = None
+    for mesh, phi in zip(ps_meshes, phis):
+        a = phi.cpu().numpy() if hasattr(phi, "cpu") else np.asarray(phi)
+        if out is None:
+            out = np.zeros((n_cells_global,) + a.shape[1:])
+        out[mesh.tables()["cell_gid"].astype(np.int64)] = a
+    return out

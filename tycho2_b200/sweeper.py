@@ -28,13 +28,31 @@ class TychoMesh:
         nc, nn, ns = C.c_uint64(), C.c_uint64(), C.c_uint64()
         check(lib().tycho_mesh_info(self._h, C.byref(nc), C.byref(nn), C.byref(ns)))
         self.n_cells, self.n_nodes, self.n_sides = nc.value, nn.value, ns.value
+        p, np_, nb = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(lib().tycho_mesh_partition_info(self._h, C.byref(p), C.byref(np_), C.byref(nb)))
+        self.partition, self.n_partitions, self.n_bound_sides = p.value, np_.value, nb.value
         self._tables = None
 
     @classmethod
-    def read_pmesh(cls, path):
+    def read_pmesh(cls, path, partition=None):
+        """A .pmesh; partition: which partition of a multi-partition file
+        (the one MPI rank `partition` reads); None: the file must hold one."""
         h = C.c_void_p()
-        check(lib().tycho_mesh_read_pmesh(str(path).encode(), C.byref(h)))
+        if partition is None:
+            check(lib().tycho_mesh_read_pmesh(str(path).encode(), C.byref(h)))
+        else:
+            check(lib().tycho_mesh_read_pmesh_partition(str(path).encode(), int(partition), C.byref(h)))
         return cls(h.value)
+
+    def side_tables(self):
+        """(side (c,4), adj_rank (c,4), side_gid (n_sides)): TychoMesh::getSide,
+        getAdjRank and getLGSide; UINT64_MAX where the reference has
+        NOT_BOUNDARY_FACE / BAD_RANK."""
+        side = np.empty((self.n_cells, 4), np.uint64)
+        rank = np.empty((self.n_cells, 4), np.uint64)
+        gid = np.empty(max(self.n_sides, 1), np.uint64)
+        check(lib().tycho_mesh_side_tables(self._h, ptr(side), ptr(rank), ptr(gid)))
+        return side, rank, gid[:self.n_sides]
 
     @classmethod
     def read_smesh(cls, path):
@@ -164,6 +182,7 @@ class SweeperCuda:
             raise ValueError("GaussElim must be one of %s" % sorted(GAUSS_ELIM))
         self.mesh = mesh
         self.n_groups = n_groups
+        self.device = device
         self.quadrature = Quadrature(sn_order)
         a0, a1 = angles if angles is not None else (0, self.quadrature.n_angles)
         self.angles = (a0, a1)
@@ -296,6 +315,80 @@ class SweeperCuda:
                                         C.c_void_p(phi_in.data_ptr()) if phi_in is not None else None,
                                         int(bool(with_fixed)), C.c_void_p(phi_out.data_ptr()),
                                         C.c_void_p(stream.cuda_stream)))
+
+    # ---- one partition of a multi-partition mesh (Util::sweepLocal with
+    #      psiBound, CommSides on the device) ------------------------------
+
+    @property
+    def n_bound_sides(self):
+        """Faces toward other partitions (0: an ordinary sweeper)."""
+        n = C.c_uint64()
+        check(lib().tycho_sweeper_bound_sides(self._h, C.byref(n)))
+        return n.value
+
+    @property
+    def psi_bound_shape(self):
+        """PsiBoundData (src/PsiData.hh:168-263): (sides, angles, 3, groups)."""
+        return (self.mesh.n_sides, self.quadrature.n_angles, 3, self.n_groups)
+
+    def set_psi_bound(self, psi_bound):
+        """Incoming psi on faces toward other partitions, PsiBoundData layout
+        (host array of psi_bound_shape); every later sweep reads it."""
+        pb = np.ascontiguousarray(psi_bound, np.float64)
+        assert pb.size == int(np.prod(self.psi_bound_shape))
+        check(lib().tycho_sweeper_set_psi_bound(self._h, ptr(pb)))
+
+    def get_psi_bound(self):
+        pb = np.empty(self.psi_bound_shape)
+        check(lib().tycho_sweeper_get_psi_bound(self._h, ptr(pb)))
+        return pb
+
+    def side_counts(self, q):
+        """(packets sent to partition q, packets q sends here), as CommSides
+        counts them (src/CommSides.cc:68-95)."""
+        a, b = C.c_uint64(), C.c_uint64()
+        check(lib().tycho_sweeper_side_counts(self._h, int(q), C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def side_send_list(self, q):
+        """(global side id, direction) of each packet sent to partition q."""
+        n, _ = self.side_counts(q)
+        gs = np.empty(max(n, 1), np.uint64)
+        an = np.empty(max(n, 1), np.uint32)
+        check(lib().tycho_sweeper_side_send_list(self._h, int(q), ptr(gs), ptr(an)))
+        return gs[:n], an[:n]
+
+    def side_link(self, q, gside, angle):
+        """q's send list, once: where q's packets land here."""
+        gs = np.ascontiguousarray(gside, np.uint64)
+        an = np.ascontiguousarray(angle, np.uint32)
+        assert gs.shape == an.shape
+        check(lib().tycho_sweeper_side_link(self._h, int(q), gs.size, ptr(gs), ptr(an)))
+
+    def side_pack(self, q, dst):
+        """Packets to q from the resident psi into dst (torch FP64 device
+        tensor of side_counts(q)[0] * 3 * G), on the current torch stream."""
+        import torch
+        assert dst.is_cuda and dst.dtype == torch.float64 and dst.is_contiguous()
+        stream = torch.cuda.current_stream(dst.device)
+        check(lib().tycho_sweeper_side_pack(self._h, int(q), C.c_void_p(dst.data_ptr()),
+                                            C.c_void_p(stream.cuda_stream)))
+
+    def side_unpack(self, q, src):
+        """Packets from q (torch FP64 device tensor, q's send order) into
+        psiBound, on the current torch stream."""
+        import torch
+        assert src.is_cuda and src.dtype == torch.float64 and src.is_contiguous()
+        stream = torch.cuda.current_stream(src.device)
+        check(lib().tycho_sweeper_side_unpack(self._h, int(q), C.c_void_p(src.data_ptr()),
+                                              C.c_void_p(stream.cuda_stream)))
+
+    def psi_change(self):
+        """(L1 of psi - psi_prev, L1 of psi) over the resident FP64 psi, then
+        psi_prev = psi (SweeperPBJ's test, src/SweeperPBJ.cc:181-195)."""
+        d, n = C.c_double(), C.c_double()
+        check(lib().tycho_sweeper_psi_change(self._h, C.byref(d), C.byref(n)))
+        return d.value, n.value
 
     WORK_ORDERS = {"cell": 0, "blevel": 1, "random": 2}
 
