@@ -1,0 +1,211 @@
+"""Multi-partition sweeps on the GPU.
+
+A sweeper made from one partition of a 2- or 4-partition .pmesh reads the
+incoming psi on faces toward other partitions from psiBound
+(tycho_sweeper_set_psi_bound):
+  - its FP64 sweep is bit-identical to the reference's Util::sweepLocal on
+    that rank's partition (the psi hash recorded from ref_dump's sweep_local
+    in tests/golden/partitions_ref.npz) and to the oracle, in every launch
+    shape that the level schedule offers;
+  - its FP32 sweep (slotted kernel, FP32 ghost rows) agrees with the oracle
+    to FP32 rounding; an angle shard of a partition sweeps its directions
+    bit for bit;
+  - the device CommSides (side_pack / side_unpack) leaves psiBound
+    bit-identical to the host restatement (tests/helpers.OraclePartition);
+  - the PBJ drivers over the GPU partitions take the oracle partitions'
+    iterations to the same phi, which is the single-partition solution;
+  - the schedules and paths that cannot read ghost rows refuse such a
+    sweeper.
+"""
+import numpy as np
+import pytest
+
+from conftest import bits_equal, rel_l1
+from helpers import OraclePartition, partition_inputs, partitions_fixture, psi_hash
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [
+    None,                                   # default: compact records in registers, 2 octant chains
+    ("levels", "records", 16, 0, 1),
+    ("levels", "direct", 128, 0, 1),
+    ("levels", "items", 2, 0, 1),
+    ("levels", "tiles", 2, 0, 1),
+    ("levels", "compact", -96, 0, 2),
+]
+
+
+@pytest.mark.parametrize("P", [2, 4])
+def test_partition_sweep_bit_identical_to_reference(built, workdir, P):
+    import tycho2_b200 as ty
+    from oracle.oracle import Oracle, OracleMesh
+    path, ref = partitions_fixture(workdir, P)
+    for p in range(P):
+        mesh = ty.TychoMesh.read_pmesh(path, p)
+        o = Oracle(OracleMesh(path, p), 4, 3)
+        st, src, pb = partition_inputs(mesh.n_cells, o.A, 3, mesh.n_sides, 10 * P + p)
+        want = o.sweep_local(st, pb, src_ang=src)
+        assert psi_hash(want) == int(ref["p%d_%d_psi_hash" % (P, p)][0])
+        sw = ty.SweeperCuda(mesh, 4, 3)
+        assert sw.n_bound_sides == mesh.n_bound_sides > 0
+        sw.set_cross_sections(st, np.zeros_like(st))
+        sw.set_psi_bound(pb)
+        for shape in SHAPES:
+            if shape is not None:
+                sw.configure(0, *shape)
+            psi = np.empty(o.psi_shape)
+            sw.sweep(psi, src)
+            assert bits_equal(psi, want), (P, p, shape)
+        # the values held, and vacuum when asked for
+        got = sw.get_psi_bound()
+        side, rank, _ = mesh.side_tables()
+        adj = mesh.tables()["adj_cell"]
+        none = np.uint64(0xFFFFFFFFFFFFFFFF)
+        bsides = side[(adj == none) & (rank != none) & (rank != np.uint64(p))].astype(np.int64)
+        assert bits_equal(got[bsides], pb[bsides])
+        others = np.setdiff1d(np.arange(mesh.n_sides), bsides)
+        assert not got[others].any()
+        psi0 = np.empty(o.psi_shape)
+        sw.sweep(psi0, src, zeroPsiBound=True)
+        assert bits_equal(psi0, o.sweep_local(st, np.zeros_like(pb), src_ang=src))
+        sw.sweep(psi, src)
+        assert bits_equal(psi, want)
+        sw.close()
+
+
+def test_partition_fp32_sweep_and_angle_shard(built, workdir):
+    import torch
+    import tycho2_b200 as ty
+    from oracle.oracle import Oracle, OracleMesh
+    path, _ = partitions_fixture(workdir, 4)
+    for p in range(4):
+        mesh = ty.TychoMesh.read_pmesh(path, p)
+        G = 4
+        o = Oracle(OracleMesh(path, p), 4, G)
+        st, _, pb = partition_inputs(mesh.n_cells, o.A, G, mesh.n_sides, 70 + p)
+        q = 0.5 + np.arange(mesh.n_cells * 4 * G).reshape(mesh.n_cells, 4, G) % 13 / 10.0
+        want = o.sweep_local(st, pb, src_iso=np.ascontiguousarray(q))
+        phi_want = o.psi_to_phi(want)
+        sw = ty.SweeperCuda(mesh, 4, G, fp32=True)
+        sw.set_cross_sections(st, np.zeros_like(st))
+        sw.set_source(q, "isotropic")
+        sw.set_psi_bound(pb)
+        out = torch.empty(sw.phi_shape, dtype=torch.float64, device="cuda")
+        sw.apply(None, out, precision=0)
+        assert bits_equal(out.cpu().numpy(), phi_want)
+        sw.apply(None, out, precision=1)  # FP32 slotted kernel, FP32 ghost rows
+        assert rel_l1(out.cpu().numpy(), phi_want) <= 2e-6
+        sw.configure(1, "levels", "compact", -172, 4, 2)
+        sw.apply(None, out, precision=1)
+        assert rel_l1(out.cpu().numpy(), phi_want) <= 2e-6
+        sw.close()
+        # directions 8..24 of the same partition
+        sh = ty.SweeperCuda(mesh, 4, G, angles=(8, 24))
+        sh.set_cross_sections(st, np.zeros_like(st))
+        sh.set_psi_bound(pb)
+        src = np.ascontiguousarray(np.broadcast_to(q[:, None], (mesh.n_cells, 16, 4, G)))
+        psi = np.empty(src.shape)
+        sh.sweep(psi, src)
+        assert bits_equal(psi, want[:, 8:24])
+        sh.close()
+
+
+def _parts(path, P, kind, sn=4, G=2):
+    import tycho2_b200 as ty
+    from tycho2_b200.partitions import GpuPartition
+    from test_partitions import _problem
+    st, ss, mat, q = _problem(P, G)
+    parts = []
+    for p in range(P):
+        if kind == "oracle":
+            parts.append(OraclePartition(path, p, sn, G, st, ss, mat, q))
+            continue
+        mesh = ty.TychoMesh.read_pmesh(path, p)
+        gid = mesh.tables()["cell_gid"].astype(np.int64)
+        sw = ty.SweeperCuda(mesh, sn, G)
+        sw.set_cross_sections(st[gid], ss[gid], mat)
+        sw.set_source(np.ascontiguousarray(q[gid]), "isotropic")
+        parts.append(GpuPartition(sw))
+    return parts
+
+
+@pytest.mark.parametrize("P", [2, 4])
+def test_device_exchange_matches_commsides(built, workdir, P):
+    import torch
+    from tycho2_b200.partitions import PartitionSet
+    path, _ = partitions_fixture(workdir, P)
+    gpu = PartitionSet(_parts(path, P, "gpu"))
+    ora = PartitionSet(_parts(path, P, "oracle"))
+    for g, o in zip(gpu.parts, ora.parts):
+        assert g.neighbours == o.neighbours
+        for q in g.neighbours:
+            n_send, n_recv = g.sw.side_counts(q)
+            gs, an = g.send_list(q)
+            ogs, oan = o.send_list(q)
+            assert np.array_equal(gs, ogs) and np.array_equal(an, oan) and n_send == gs.size
+            # what q receives from here is what q counts as its receives
+            assert gpu.parts[q].sw.side_counts(g.partition)[1] == n_send
+    phis = [torch.zeros(p.sw.phi_shape, dtype=torch.float64, device="cuda") for p in gpu.parts]
+    ophis = [p.phi_zeros() for p in ora.parts]
+    for step in range(3):
+        for part, a in zip(gpu.parts, phis):
+            part.apply(a.clone(), a, True)
+        for part, a in zip(ora.parts, ophis):
+            part.apply(a.clone(), a, True)
+        gpu.exchange()
+        ora.exchange()
+        for g, o, a, b in zip(gpu.parts, ora.parts, phis, ophis):
+            assert bits_equal(a.cpu().numpy(), b.numpy()), step
+            assert bits_equal(g.sw.get_psi_bound(), o.pb), step
+    gpu.close()
+
+
+@pytest.mark.timeout(600)
+def test_pbj_solvers_on_the_gpu_match_the_oracle(built, workdir):
+    from tycho2_b200.partitions import PartitionSet, pbj, pbj_outer, pbj_si
+    from test_partitions import _gather, _single_partition_si
+    path, _ = partitions_fixture(workdir, 4)
+    ref, it_ref = _single_partition_si(workdir)
+    for solver, kw in ((pbj_si, dict(dd_iter_max=400, dd_err_max=1e-12)),
+                       (pbj, dict(iter_max=400, err_max=1e-12, dd_iter_max=100, dd_err_max=1e-13)),
+                       (pbj_outer, dict(iter_max=400, err_max=1e-13, dd_iter_max=100, dd_err_max=1e-12))):
+        gpu = PartitionSet(_parts(path, 4, "gpu"))
+        ora = PartitionSet(_parts(path, 4, "oracle"))
+        rg = solver(gpu, **kw)
+        ro = solver(ora, **kw)
+        phi_g = _gather(gpu.parts, [x.cpu() for x in rg[0]])
+        phi_o = _gather(ora.parts, ro[0])
+        # iteration counts (pbj_si: iterations; pbj: source iterations and
+        # local sweeps; pbj_outer: outer iterations and source iterations of
+        # each); the L1 sums run in another order on the device, so a change
+        # within rounding of a tolerance may end one iteration apart
+        counts = {pbj_si: lambda r: (r[1],), pbj: lambda r: (r[1], r[3]), pbj_outer: lambda r: (r[1], r[2])}[solver]
+        if counts(rg) == counts(ro):
+            assert bits_equal(phi_g, phi_o), solver.__name__
+        else:
+            assert abs(rg[1] - ro[1]) <= 1, (solver.__name__, counts(rg), counts(ro))
+        assert rel_l1(phi_g, ref) <= 1e-10, solver.__name__
+        gpu.close()
+
+
+def test_partition_sweeper_refusals(built, workdir):
+    import tycho2_b200 as ty
+    path, _ = partitions_fixture(workdir, 2)
+    mesh = ty.TychoMesh.read_pmesh(path, 0)
+    sw = ty.SweeperCuda(mesh, 4, 2)
+    st = np.ones(mesh.n_cells)
+    sw.set_cross_sections(st, 0.5 * st)
+    with pytest.raises(ty.TychoError, match="level schedule"):
+        sw.configure(0, "dataflow", "tiles", 4)
+    with pytest.raises(ty.TychoError, match="level schedule"):
+        sw.configure(0, "persist", "records", 16)
+    b = ty.BatchSolver(0)
+    with pytest.raises(ty.TychoError, match="not in a batch"):
+        b.add(sw, method="si")
+    b.close()
+    with pytest.raises(ty.TychoError):
+        ty.SweeperCuda(mesh, 4, 2, schedule="dataflow")
+    # the autotuner keeps to the level schedule
+    sw.autotune(0, reps=1)
+    assert sw.shape(0)["schedule"] == "levels"
+    sw.close()

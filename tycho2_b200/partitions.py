@@ -55,6 +55,7 @@ class GpuPartition:
         self.partition = self.mesh.partition
         self.device = torch.device("cuda", sweeper.device)
         self.neighbours = neighbours_of(self.mesh)
+        self.gid = self.mesh.tables()["cell_gid"].astype(np.int64)  # global cell of each cell
         self._send = {}
 
     def send_list(self, q):
@@ -307,12 +308,14 @@ def pbj_outer(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10
     return phi_new, outer, its
 
 
-def gather_phi(ps_meshes, phis, n_cells_global):
-    """phi of every partition into one array in global cell order (cell_gid)."""
+def gather_phi(parts, phis):
+    """phi of every partition into one array in global cell order (each
+    part's `gid`: its cells' global ids)."""
+    n = 1 + max(int(p.gid.max()) for p in parts)
     out = None
-    for mesh, phi in zip(ps_meshes, phis):
+    for part, phi in zip(parts, phis):
         a = phi.cpu().numpy() if hasattr(phi, "cpu") else np.asarray(phi)
         if out is None:
-            out = np.zeros((n_cells_global,) + a.shape[1:])
-        out[mesh.tables()["cell_gid"].astype(np.int64)] = a
+            out = np.zeros((n,) + a.shape[1:])
+        out[part.gid] = a
     return out

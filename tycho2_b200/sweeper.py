@@ -227,11 +227,20 @@ class SweeperCuda:
         check(lib().tycho_sweeper_set_source(self._h, k, ptr(arr)))
 
     def sweep(self, psi, source, zeroPsiBound=False):
-        """SweeperAbstract::sweep: psi = L^-1 source (vacuum boundaries)."""
-        del zeroPsiBound  # one partition: no partition-boundary psi exists
+        """SweeperAbstract::sweep: psi = L^-1 source; vacuum on the mesh
+        boundary and, on faces toward other partitions, the psiBound last
+        set (zeroPsiBound: zeros instead, for this sweep only, as
+        SweeperPBJOuter::sweep takes c_zeroPsiBound, src/SweeperPBJ.cc:129-138)."""
         src = np.ascontiguousarray(source, np.float64)
         assert psi.dtype == np.float64 and psi.flags["C_CONTIGUOUS"] and psi.size == src.size
-        check(lib().tycho_sweeper_sweep(self._h, ptr(src), ptr(psi)))
+        keep = self.get_psi_bound() if zeroPsiBound and self.n_bound_sides else None
+        if keep is not None:
+            self.set_psi_bound(np.zeros_like(keep))
+        try:
+            check(lib().tycho_sweeper_sweep(self._h, ptr(src), ptr(psi)))
+        finally:
+            if keep is not None:
+                self.set_psi_bound(keep)
         return psi
 
     def solve(self, method="si", iter_max=100, err_max=1e-10, restart=20, inner_tol=1e-5,
