@@ -93,6 +93,13 @@ int tycho_mesh_read_pmesh_partition(const char *path, uint64_t partition, tycho_
    partition (any pointer may be NULL). */
 int tycho_mesh_partition_info(const tycho_mesh *mesh, uint64_t *partition, uint64_t *n_partitions,
                               uint64_t *n_bound_sides);
+/* For a mesh made from a reference TychoMesh's arrays (tycho_mesh_from_arrays)
+   on one MPI rank of a multi-partition run: the rank, the number of ranks,
+   adj_rank [n*4] (getAdjRank, UINT64_MAX = BAD_RANK on the mesh boundary)
+   and side_gid [n_sides] (getLGSide, sides numbered in (cell, face) order as
+   TychoMesh numbers them).  Call before making sweepers from the mesh. */
+int tycho_mesh_set_partition(tycho_mesh *mesh, uint64_t partition, uint64_t n_partitions,
+                             const uint64_t *adj_rank, const uint64_t *side_gid);
 /* side [n*4] (TychoMesh::getSide, UINT64_MAX on interior faces), adj_rank
    [n*4] (getAdjRank: the partition across the face, this one for interior
    faces, UINT64_MAX on the mesh boundary), side_gid [n_sides] (getLGSide);

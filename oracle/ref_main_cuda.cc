@@ -8,6 +8,7 @@
  * used by the GPU tests to show the drop-in reproduces gold.psi.
  *
  *   sweep_cuda.x <pmesh> <deck> [reference-loop]
+ *   sweep_cuda.x <pmesh> <deck> sweep-local <sigmaT.f64> <source.f64> <psiBound.f64> <out.f64>
  *
  * Default: SweeperCuda::solve (the outer iteration resident on the device).
  * With `reference-loop` (decks with SourceIteration true): the reference's
@@ -16,6 +17,10 @@
  * (src/SweeperTraverse.cc:65-74, src/SourceIteration.cc:127-207), with the
  * reference's PsiData containers (host `new double[]` buffers) handed to
  * the GPU sweep at every iteration.
+ * With `sweep-local`: one rank's partition (TYCHO_SHIM_RANK of
+ * TYCHO_SHIM_SIZE, oracle/ref_shim/mpi.h), per-cell sigma_t, an angular
+ * source and psiBound read from files, one SweeperCuda::sweepLocal -- what
+ * src/Util.cc:138-145 becomes with the GPU -- and psi written to <out.f64>.
  */
 #include <cstdio>
 #include <string>
@@ -38,6 +43,7 @@ int main(int argc, char **argv)
         return 0;
     }
     const bool reference_loop = argc > 3 && std::string(argv[3]) == "reference-loop";
+    const bool sweep_local = argc == 8 && std::string(argv[3]) == "sweep-local";
     int provided = 0;
     MPI_Init_thread(&argc, &argv, MPI_THREAD_SINGLE, &provided);
     CKG_Utils::KeyValueReader kvr;
@@ -69,6 +75,26 @@ int main(int argc, char **argv)
     g_quadrature = new Quadrature(g_snOrder);
     g_tychoMesh = new TychoMesh(argv[1]);
     Problem::createCrossSections(g_sigmaT, g_sigmaS, sigmaT1, sigmaS1, sigmaT2, sigmaS2);
+    if (sweep_local) {
+        auto load = [](const char *path, double *dst, size_t n) {
+            FILE *fp = fopen(path, "rb");
+            Insist(fp && fread(dst, sizeof(double), n, fp) == n, "cannot read an input file");
+            fclose(fp);
+        };
+        load(argv[4], g_sigmaT.data(), g_nCells);
+        for (UINT c = 0; c < g_nCells; c++) g_sigmaS[c] = 0.0;
+        SweeperCuda sweeper;
+        PsiData source, psi;
+        PsiBoundData psiBound;
+        load(argv[5], &source[0], source.size());
+        load(argv[6], &psiBound[0], psiBound.size());
+        sweeper.sweepLocal(psi, source, psiBound);
+        FILE *fp = fopen(argv[7], "wb");
+        Insist(fp && fwrite(&psi[0], sizeof(double), psi.size(), fp) == psi.size(), "cannot write psi");
+        fclose(fp);
+        MPI_Finalize();
+        return 0;
+    }
 
     SweeperCuda sweeper;
     if (reference_loop) {

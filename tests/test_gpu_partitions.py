@@ -17,10 +17,13 @@ incoming psi on faces toward other partitions from psiBound
   - the schedules and paths that cannot read ghost rows refuse such a
     sweeper.
 """
+import os
+import subprocess
+
 import numpy as np
 import pytest
 
-from conftest import bits_equal, rel_l1
+from conftest import ROOT, bits_equal, rel_l1
 from helpers import OraclePartition, partition_inputs, partitions_fixture, psi_hash
 
 pytestmark = pytest.mark.gpu
@@ -209,3 +212,37 @@ def test_partition_sweeper_refusals(built, workdir):
     sw.autotune(0, reps=1)
     assert sw.shape(0)["schedule"] == "levels"
     sw.close()
+
+
+BIN = os.path.join(ROOT, "oracle", "_ref")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(BIN, "sweep_cuda.x")),
+                    reason="reference-side binding not built (needs the tycho2 tree at build time)")
+def test_reference_adapter_sweep_local(built, workdir):
+    """SweeperCuda.hh's sweepLocal inside the reference's own process
+    (sweep_cuda.x sweep-local: its TychoMesh of one rank's partition, its
+    PsiData and PsiBoundData): the psi of Util::sweepLocal, bit for bit."""
+    from oracle.oracle import OracleMesh
+    P = 4
+    path, ref = partitions_fixture(workdir, P)
+    d = os.path.join(str(workdir), "adapter_local")
+    os.makedirs(d, exist_ok=True)
+    deck = os.path.join(d, "local.deck")
+    with open(deck, "w") as f:
+        f.write("snOrder 4\niterMax 10\nerrMax 1e-10\nmaxCellsPerStep 100\nintraAngleP 3\ninterAngleP 1\n"
+                "nGroups 3\nsigmaT1 1\nsigmaS1 0\nsigmaT2 1\nsigmaS2 0\nOutputFile false\n"
+                "OutputFilename out.psi\nSourceIteration true\nMPIType TychoTwoSided\nDD_IterMax 100\n"
+                "DD_ErrMax 1e-10\nSweepType Cuda\nGaussElim NoPivot\n")
+    for p in range(P):
+        om = OracleMesh(path, p)
+        st, src, pb = partition_inputs(om.n_cells, 32, 3, om.n_sides, 10 * P + p)
+        files = [os.path.join(d, n) for n in ("st.f64", "src.f64", "pb.f64", "psi.f64")]
+        for arr, fn in zip((st, src, pb), files):
+            arr.tofile(fn)
+        env = dict(os.environ, TYCHO_SHIM_RANK=str(p), TYCHO_SHIM_SIZE=str(P))
+        r = subprocess.run([os.path.join(BIN, "sweep_cuda.x"), path, deck, "sweep-local", *files], cwd=d,
+                           env=env, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+        psi = np.fromfile(files[3])
+        assert psi_hash(psi) == int(ref["p%d_%d_psi_hash" % (P, p)][0]), p

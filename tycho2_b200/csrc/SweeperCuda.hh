@@ -15,6 +15,11 @@
  *                          same problem and stopping rules (deck keys iterMax,
  *                          errMax, SourceIteration), with the outer iteration
  *                          resident on the device; psi lands in c_psi.
+ *   sweepLocal(psi, source, psiBound)
+ *                       == Util::sweepLocal (src/Util.cc:138-145) on one MPI
+ *                          rank's partition: the PBJ and Schur sweepers'
+ *                          local sweep (src/SweeperPBJ.cc, src/SweeperSchur.cc),
+ *                          with psiBound on the faces toward other ranks.
  *
  * The mesh comes from g_tychoMesh's own tables (no second file read), the
  * quadrature from g_snOrder, cross sections from g_sigmaT / g_sigmaS.  A
@@ -36,6 +41,7 @@
 #include <vector>
 
 #include "Assert.hh"
+#include "Comm.hh"
 #include "Global.hh"
 #include "Problem.hh"
 #include "PsiData.hh"
@@ -66,6 +72,17 @@ public:
         }
         check(tycho_mesh_from_arrays(nc, nn, cellNodes.data(), coords.data(), adj.data(),
                                      f2c.data(), gid.data(), &c_mesh));
+        // this rank's partition: the faces toward other ranks read psiBound
+        // in sweepLocal (src/TychoMeshIO.cc:228-262)
+        if (Comm::numRanks() > 1) {
+            const UINT ns = g_tychoMesh->getNSides();
+            std::vector<uint64_t> rank(nc * 4), lgside(ns);
+            for (UINT c = 0; c < nc; c++)
+                for (UINT f = 0; f < 4; f++) rank[c * 4 + f] = g_tychoMesh->getAdjRank(c, f);
+            for (UINT s = 0; s < ns; s++) lgside[s] = g_tychoMesh->getLGSide(s);
+            check(tycho_mesh_set_partition(c_mesh, (uint64_t)Comm::rank(), (uint64_t)Comm::numRanks(),
+                                           rank.data(), lgside.data()));
+        }
         tycho_sweeper_opts opts = {};
         opts.sn_order = (int)g_snOrder;
         opts.n_groups = (int)g_nGroups;
@@ -95,7 +112,17 @@ public:
 
     void sweep(PsiData &psi, const PsiData &source, bool zeroPsiBound = false)
     {
-        UNUSED_VARIABLE(zeroPsiBound);  // one partition: no partition-boundary psi
+        UNUSED_VARIABLE(zeroPsiBound);  // psiBound as last set (none: vacuum)
+        check(tycho_sweeper_sweep(c_sweeper, &source[0], &psi[0]));
+    }
+
+    // Util::sweepLocal(psi, source, psiBound) (src/Util.cc:138-145) on the
+    // GPU: this rank's partition swept with the incoming psi on faces toward
+    // other ranks taken from psiBound, as the PBJ and Schur sweepers call it
+    // (src/SweeperPBJ.cc:129-138, :179, :287).
+    void sweepLocal(PsiData &psi, const PsiData &source, const PsiBoundData &psiBound)
+    {
+        check(tycho_sweeper_set_psi_bound(c_sweeper, &psiBound[0]));
         check(tycho_sweeper_sweep(c_sweeper, &source[0], &psi[0]));
     }
 

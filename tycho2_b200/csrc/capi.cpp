@@ -154,6 +154,22 @@ int tycho_mesh_partition_info(const tycho_mesh *m, uint64_t *partition, uint64_t
     return TYCHO_OK;
 }
 
+int tycho_mesh_set_partition(tycho_mesh *m, uint64_t partition, uint64_t n_partitions, const uint64_t *adj_rank,
+                             const uint64_t *side_gid)
+{
+    if (!m || !adj_rank || !side_gid) return finish(TYCHO_ERR_ARG, "null argument");
+    auto &t = m->tab;
+    if (n_partitions == 0 || partition >= n_partitions) return finish(TYCHO_ERR_ARG, "bad partition");
+    for (uint64_t i = 0; i < t.n_cells * 4; ++i)
+        if (t.adj_cell[i] == tycho::kNone && adj_rank[i] != tycho::kNone && adj_rank[i] >= n_partitions)
+            return finish(TYCHO_ERR_ARG, "adjacent partition out of range");
+    t.partition = partition;
+    t.n_partitions = n_partitions;
+    t.adj_rank.assign(adj_rank, adj_rank + t.n_cells * 4);
+    t.side_gid.assign(side_gid, side_gid + t.n_sides);
+    return TYCHO_OK;
+}
+
 int tycho_mesh_side_tables(const tycho_mesh *m, uint64_t *side, uint64_t *adj_rank, uint64_t *side_gid)
 {
     if (!m) return finish(TYCHO_ERR_ARG, "null mesh");
