@@ -151,3 +151,9 @@ class OraclePartition:
         n = float(np.abs(self.psi).sum())
         self.prev = self.psi.copy()
         return d, n
+
+    def get_bound(self):
+        return self.pb.copy()
+
+    def set_bound(self, pb):
+        self.pb = np.ascontiguousarray(pb, np.float64).reshape(self.pb.shape).copy()

@@ -12,8 +12,9 @@ incoming psi on faces toward other partitions from psiBound
     bit for bit;
   - the device CommSides (side_pack / side_unpack) leaves psiBound
     bit-identical to the host restatement (tests/helpers.OraclePartition);
-  - the PBJ drivers over the GPU partitions take the oracle partitions'
-    iterations to the same phi, which is the single-partition solution;
+  - the PBJ and Schur drivers over the GPU partitions take the oracle
+    partitions' iterations to the same phi, which is the single-partition
+    solution;
   - the schedules and paths that cannot read ghost rows refuse such a
     sweeper.
 """
@@ -165,13 +166,15 @@ def test_device_exchange_matches_commsides(built, workdir, P):
 
 @pytest.mark.timeout(600)
 def test_pbj_solvers_on_the_gpu_match_the_oracle(built, workdir):
-    from tycho2_b200.partitions import PartitionSet, pbj, pbj_outer, pbj_si
+    from tycho2_b200.partitions import PartitionSet, pbj, pbj_outer, pbj_si, schur, schur_krylov
     from test_partitions import _gather, _single_partition_si
     path, _ = partitions_fixture(workdir, 4)
     ref, it_ref = _single_partition_si(workdir)
     for solver, kw in ((pbj_si, dict(dd_iter_max=400, dd_err_max=1e-12)),
                        (pbj, dict(iter_max=400, err_max=1e-12, dd_iter_max=100, dd_err_max=1e-13)),
-                       (pbj_outer, dict(iter_max=400, err_max=1e-13, dd_iter_max=100, dd_err_max=1e-12))):
+                       (pbj_outer, dict(iter_max=400, err_max=1e-13, dd_iter_max=100, dd_err_max=1e-12)),
+                       (schur, dict(iter_max=400, err_max=1e-12, dd_iter_max=200, dd_err_max=1e-13)),
+                       (schur_krylov, dict(dd_iter_max=400, dd_err_max=1e-13))):
         gpu = PartitionSet(_parts(path, 4, "gpu"))
         ora = PartitionSet(_parts(path, 4, "oracle"))
         rg = solver(gpu, **kw)
@@ -182,7 +185,8 @@ def test_pbj_solvers_on_the_gpu_match_the_oracle(built, workdir):
         # local sweeps; pbj_outer: outer iterations and source iterations of
         # each); the L1 sums run in another order on the device, so a change
         # within rounding of a tolerance may end one iteration apart
-        counts = {pbj_si: lambda r: (r[1],), pbj: lambda r: (r[1], r[3]), pbj_outer: lambda r: (r[1], r[2])}[solver]
+        counts = {pbj_si: lambda r: (r[1],), pbj: lambda r: (r[1], r[3]), pbj_outer: lambda r: (r[1], r[2]),
+                  schur: lambda r: (r[1], r[3]), schur_krylov: lambda r: (r[1],)}[solver]
         if counts(rg) == counts(ro):
             assert bits_equal(phi_g, phi_o), solver.__name__
         else:

@@ -9,9 +9,10 @@ partition):
     2- and a 4-partition Kuhn cube;
   - the oracle's partition-local sweep with psiBound: the hash of its psi
     equals the reference's, bit for bit.
-Then the PBJ drivers (tycho2_b200.partitions) over oracle partitions: one
-process holding both partitions and two gloo ranks holding one each take the
-same iterations to the same phi, which is the single-partition solution.
+Then the PBJ and Schur drivers (tycho2_b200.partitions) over oracle
+partitions reach the single-partition solution, and for PBJ one process
+holding both partitions and two gloo ranks holding one each take the same
+iterations to the same phi.
 """
 import os
 import socket
@@ -138,6 +139,22 @@ def test_pbj_solvers_in_one_process_reach_the_single_partition_solution(built, w
     ps = PartitionSet(_oracle_parts(path, 2))
     phi, outer, its = pbj_outer(ps, iter_max=400, err_max=1e-13, dd_iter_max=100, dd_err_max=1e-12)
     assert outer > 1 and len(its) == outer
+    assert rel_l1(_gather(ps.parts, phi), ref) <= 1e-10
+
+
+@pytest.mark.timeout(300)
+def test_schur_solvers_reach_the_single_partition_solution(built, workdir):
+    from tycho2_b200.partitions import PartitionSet, schur, schur_krylov
+    path, _ = partitions_fixture(workdir, 2)
+    ref, it_ref = _single_partition_si(workdir)
+    ps = PartitionSet(_oracle_parts(path, 2))
+    phi, it, err, sweeps = schur(ps, iter_max=400, err_max=1e-12, dd_iter_max=200, dd_err_max=1e-13)
+    # each sweep is the whole mesh's sweep to the Krylov tolerance
+    assert abs(it - it_ref) <= 1 and sweeps > 2 * it
+    assert rel_l1(_gather(ps.parts, phi), ref) <= 1e-10
+    ps = PartitionSet(_oracle_parts(path, 2))
+    phi, its, rn = schur_krylov(ps, dd_iter_max=400, dd_err_max=1e-13)
+    assert its < it_ref  # one Krylov solve of the whole problem
     assert rel_l1(_gather(ps.parts, phi), ref) <= 1e-10
 
 

@@ -24,6 +24,11 @@ the same operations to the solvers below:
   pbj_outer  SweeperPBJOuter::solve src/SweeperPBJ.cc:59-141 (source
              iteration to errMax with the boundary values fixed, then
              commSides, until psi changes by at most ddErrMax)
+  schur      SweeperSchur::solve    src/SweeperSchur.cc:196-326 (source
+             iteration whose every sweep solves for the boundary values
+             by GMRES)
+  schur_krylov SweeperSchurKrylov::solve src/SweeperSchur.cc:487-604 (one
+             GMRES over the boundary values and phi together)
 
 Iteration counts and convergence follow the reference's tests; the L1 sums
 run on the device, in another order than the reference's loops, so a
@@ -93,6 +98,13 @@ class GpuPartition:
 
     def psi_change(self):
         return self.sw.psi_change()
+
+    def get_bound(self):
+        """psiBound (PsiBoundData layout, host)."""
+        return self.sw.get_psi_bound()
+
+    def set_bound(self, pb):
+        self.sw.set_psi_bound(pb)
 
 
 class PartitionSet:
@@ -306,6 +318,148 @@ def pbj_outer(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10
         ps.exchange()
         outer += 1
     return phi_new, outer, its
+
+
+def _dot(ps, u, v):
+    """Inner product of two distributed vectors (lists of host arrays, one
+    per local partition) over every partition."""
+    return ps.allsum([sum(float(np.dot(a.reshape(-1), b.reshape(-1))) for a, b in zip(u, v))])[0]
+
+
+def _gmres(ps, op, b, x, rtol, iter_max, restart=30):
+    """Restarted GMRES on distributed host vectors (lists of arrays, one per
+    local partition): op(x) -> A x, b the right-hand side, x the initial
+    guess (updated in place); classical Gram-Schmidt twice, Givens
+    rotations, the true residual at each restart, stop when ||r|| <= rtol
+    ||b||.  The reference's KrylovSolver is PETSc's KSPGMRES with these
+    tolerances (src/KrylovSolver.cc:97-101); PETSc is absent, so the
+    iterates are this method's.  Returns (iterations, residual norm)."""
+    bnorm = np.sqrt(_dot(ps, b, b))
+    its = 0
+
+    def residual():
+        ax = op(x)
+        return [bi - ai for bi, ai in zip(b, ax)]
+
+    r = residual()
+    beta = np.sqrt(_dot(ps, r, r))
+    while its < iter_max and beta > rtol * bnorm:
+        V = [[ri / beta for ri in r]]
+        H = np.zeros((restart + 1, restart))
+        cs, sn, g = np.zeros(restart), np.zeros(restart), np.zeros(restart + 1)
+        g[0] = beta
+        k = 0
+        while k < restart and its < iter_max:
+            w = op(V[k])
+            for _ in range(2):
+                h = [_dot(ps, w, V[j]) for j in range(k + 1)]
+                for j in range(k + 1):
+                    H[j, k] += h[j]
+                    w = [wi - h[j] * vj for wi, vj in zip(w, V[j])]
+            hn = np.sqrt(_dot(ps, w, w))
+            H[k + 1, k] = hn
+            for j in range(k):
+                h0, h1 = H[j, k], H[j + 1, k]
+                H[j, k], H[j + 1, k] = cs[j] * h0 + sn[j] * h1, -sn[j] * h0 + cs[j] * h1
+            den = np.hypot(H[k, k], hn)
+            cs[k], sn[k] = (H[k, k] / den, hn / den) if den > 0 else (1.0, 0.0)
+            H[k, k] = den
+            g[k + 1], g[k] = -sn[k] * g[k], cs[k] * g[k]
+            its += 1
+            k += 1
+            V.append([wi / hn for wi in w] if hn > 0 else w)
+            if abs(g[k]) <= rtol * bnorm or hn == 0:
+                break
+        y = np.linalg.solve(np.triu(H[:k, :k]), g[:k]) if k else np.zeros(0)
+        for j in range(k):
+            for xi, vj in zip(x, V[j]):
+                xi += y[j] * vj
+        r = residual()
+        beta = np.sqrt(_dot(ps, r, r))
+    return its, beta
+
+
+def _sweep_exchange(ps, bounds, phi_in, with_fixed, phi_out):
+    """Util::sweepLocal on every partition with the given psiBound, then
+    CommSides: returns the boundary values after the exchange."""
+    for part, pb in zip(ps.local, bounds):
+        part.set_bound(pb)
+    for part, a, o in zip(ps.local, phi_in, phi_out):
+        part.apply(a, o, with_fixed)
+    ps.exchange()
+    return [part.get_bound() for part in ps.local]
+
+
+def schur(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10):
+    """SweeperSchur::solve with source iteration (src/SweeperSchur.cc:
+    196-326): every sweep of SourceIteration::fixedPoint solves for the
+    incoming partition-boundary psi by Krylov,
+      (I - W L_I^-1 L_B) psi_B = W L_I^-1 q,
+    with the last sweep's psi_B as initial guess (the right-hand side: one
+    local sweep of the total source with zero boundary values, then the
+    exchange), then sweeps each partition with the solved values.  The
+    Krylov vectors are the partitions' psiBound arrays on the host.
+    Returns (phi per local partition, source iterations, last change,
+    local sweeps)."""
+    phi_new = [p.phi_zeros() for p in ps.local]
+    phi_old = [p.phi_zeros() for p in ps.local]
+    tmp = [p.phi_zeros() for p in ps.local]
+    prev = [np.zeros_like(p.get_bound()) for p in ps.local]
+    it, err, sweeps = 0, 1.0, 0
+
+    def op(x):
+        y = _sweep_exchange(ps, x, [None] * len(x), False, tmp)
+        return [xi - yi for xi, yi in zip(x, y)]
+
+    while it < iter_max and err > err_max:
+        for a, b in zip(phi_old, phi_new):
+            a.copy_(b)
+        rhs = _sweep_exchange(ps, [np.zeros_like(x) for x in prev], phi_old, True, tmp)
+        x = [pv.copy() for pv in prev]
+        its, _ = _gmres(ps, op, rhs, x, dd_err_max, dd_iter_max)
+        for part, xi in zip(ps.local, x):
+            part.set_bound(xi)
+        for part, a, o in zip(ps.local, phi_old, phi_new):
+            part.apply(a, o, True)
+        prev = x
+        sweeps += 2 + its
+        d, m = ps.allsum(_l1(ps.local, phi_new, phi_old))
+        err = d / m if m > 0 else 0.0
+        it += 1
+    return phi_new, it, err, sweeps
+
+
+def schur_krylov(ps, dd_iter_max=100, dd_err_max=1e-10):
+    """SweeperSchurKrylov::solve (src/SweeperSchur.cc:487-604): one Krylov
+    solve for the incoming partition-boundary psi and phi together,
+      (I - W L_I^-1 L_B) psi_B - W L_I^-1 M S phi  = W L_I^-1 Q
+      -D L_I^-1 L_B psi_B + (I - D L_I^-1 M S) phi = D L_I^-1 Q,
+    from zero, then one local sweep of Q + M S phi with the solved boundary
+    values.  Returns (phi per local partition, Krylov iterations, residual
+    norm)."""
+    import torch
+    n = len(ps.local)
+    tmp = [p.phi_zeros() for p in ps.local]
+
+    def to_dev(a, like):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(like.device).reshape(like.shape)
+
+    def op(x):
+        xb, xp = x[:n], x[n:]
+        yb = _sweep_exchange(ps, xb, [to_dev(a, t) for a, t in zip(xp, tmp)], False, tmp)
+        yp = [t.cpu().numpy().copy() for t in tmp]
+        return [a - b for a, b in zip(x, yb + yp)]
+
+    rb = _sweep_exchange(ps, [np.zeros_like(p.get_bound()) for p in ps.local], [None] * n, True, tmp)
+    rhs = rb + [t.cpu().numpy().copy() for t in tmp]
+    x = [np.zeros_like(a) for a in rhs]
+    its, rn = _gmres(ps, op, rhs, x, dd_err_max, dd_iter_max)
+    phi = [p.phi_zeros() for p in ps.local]
+    for part, b in zip(ps.local, x[:n]):
+        part.set_bound(b)
+    for part, a, o in zip(ps.local, x[n:], phi):
+        part.apply(to_dev(a, o), o, True)
+    return phi, its, rn
 
 
 def gather_phi(parts, phis):
