@@ -144,7 +144,7 @@ def test_pbj_solvers_in_one_process_reach_the_single_partition_solution(built, w
 
 @pytest.mark.timeout(300)
 def test_schur_solvers_reach_the_single_partition_solution(built, workdir):
-    from tycho2_b200.partitions import PartitionSet, schur, schur_krylov
+    from tycho2_b200.partitions import PartitionSet, schur, schur_krylov, schur_outer
     path, _ = partitions_fixture(workdir, 2)
     ref, it_ref = _single_partition_si(workdir)
     ps = PartitionSet(_oracle_parts(path, 2))
@@ -155,6 +155,10 @@ def test_schur_solvers_reach_the_single_partition_solution(built, workdir):
     ps = PartitionSet(_oracle_parts(path, 2))
     phi, its, rn = schur_krylov(ps, dd_iter_max=400, dd_err_max=1e-13)
     assert its < it_ref  # one Krylov solve of the whole problem
+    assert rel_l1(_gather(ps.parts, phi), ref) <= 1e-10
+    ps = PartitionSet(_oracle_parts(path, 2))
+    phi, its, rn, (i1, iop, i3) = schur_outer(ps, iter_max=400, err_max=1e-13, dd_iter_max=100, dd_err_max=1e-12)
+    assert len(iop) >= its and i1 > 1 and i3 >= 1
     assert rel_l1(_gather(ps.parts, phi), ref) <= 1e-10
 
 

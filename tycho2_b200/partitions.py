@@ -27,6 +27,9 @@ the same operations to the solvers below:
   schur      SweeperSchur::solve    src/SweeperSchur.cc:196-326 (source
              iteration whose every sweep solves for the boundary values
              by GMRES)
+  schur_outer SweeperSchurOuter::solve src/SweeperSchur.cc:326-470 (GMRES
+             on the boundary values, a whole source iteration in every
+             operator application)
   schur_krylov SweeperSchurKrylov::solve src/SweeperSchur.cc:487-604 (one
              GMRES over the boundary values and phi together)
 
@@ -341,7 +344,9 @@ def _gmres(ps, op, b, x, rtol, iter_max, restart=30):
         ax = op(x)
         return [bi - ai for bi, ai in zip(b, ax)]
 
-    r = residual()
+    # a zero initial guess needs no operator application (as KSPSolve)
+    zero = ps.allsum([float(sum(np.abs(xi).sum() for xi in x))])[0] == 0.0
+    r = [bi.copy() for bi in b] if zero else residual()
     beta = np.sqrt(_dot(ps, r, r))
     while its < iter_max and beta > rtol * bnorm:
         V = [[ri / beta for ri in r]]
@@ -427,6 +432,55 @@ def schur(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10):
         err = d / m if m > 0 else 0.0
         it += 1
     return phi_new, it, err, sweeps
+
+
+def schur_outer(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10):
+    """SweeperSchurOuter::solve with source iteration (src/SweeperSchur.cc:
+    326-470): GMRES from zero on the incoming boundary values,
+      (I - W (L_I - M S D)^-1 L_B) psi_B = W (L_I - M S D)^-1 Q,
+    where every operator application is a whole source iteration
+    (SourceIteration::fixedPoint from the current psi, zero source, the
+    given boundary values) followed by the exchange; the right-hand side is
+    the source iteration of Q with zero boundary values, the answer the
+    source iteration of Q with the solved ones.  Returns (phi per local
+    partition, Krylov iterations, residual norm, source iterations: the
+    right-hand side's, each operator application's, the last one's)."""
+    phi = [p.phi_zeros() for p in ps.local]
+
+    def fixed_point(with_fixed):
+        # from phi = psiToPhi(psi) of the last sweep, as fixedPoint starts
+        it, err = 0, 1.0
+        while it < iter_max and err > err_max:
+            old = [t.clone() for t in phi]
+            for part, a, o in zip(ps.local, old, phi):
+                part.apply(a, o, with_fixed)
+            d, m = ps.allsum(_l1(ps.local, phi, old))
+            err = d / m if m > 0 else 0.0
+            it += 1
+        return it
+
+    for part in ps.local:
+        part.set_bound(np.zeros_like(part.get_bound()))
+    its_rhs = fixed_point(True)
+    ps.exchange()
+    rhs = [part.get_bound() for part in ps.local]
+    for t in phi:  # psi = 0
+        t.zero_()
+    its_op = []
+
+    def op(x):
+        for part, xi in zip(ps.local, x):
+            part.set_bound(xi)
+        its_op.append(fixed_point(False))
+        ps.exchange()
+        return [xi - part.get_bound() for part, xi in zip(ps.local, x)]
+
+    x = [np.zeros_like(b) for b in rhs]
+    its, rn = _gmres(ps, op, rhs, x, dd_err_max, dd_iter_max)
+    for part, xi in zip(ps.local, x):
+        part.set_bound(xi)
+    its_end = fixed_point(True)
+    return phi, its, rn, (its_rhs, its_op, its_end)
 
 
 def schur_krylov(ps, dd_iter_max=100, dd_err_max=1e-10):
