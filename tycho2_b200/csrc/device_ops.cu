@@ -139,6 +139,58 @@ multi_dot_kernel(const double *__restrict__ w, const double *__restrict__ V, siz
     }
 }
 
+// The same inner products on 16-byte pairs (n even, 16-byte aligned
+// vectors): each thread issues U x (K + 1) pair loads before its FMAs, so
+// that the few-vector passes of an Arnoldi step keep enough loads in
+// flight to stream at HBM rate.  Per thread: the pairs it visits in
+// grid-stride order, the first element of each pair before the second.
+template <int K, int U>
+__global__ void __launch_bounds__(256)
+multi_dot2_kernel(const double2 *__restrict__ w, const double2 *__restrict__ V, size_t ld2, int k, int j0,
+                  uint64_t n2, double *__restrict__ partials)
+{
+    double acc[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc[j] = 0.0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n2; i0 += stride * U) {
+        double2 wv[U], v[U][K];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint64_t i = i0 + u * stride;
+            if (i < n2) {
+                wv[u] = w[i];
+#pragma unroll
+                for (int j = 0; j < K; ++j)
+                    if (j0 + j < k) v[u][j] = V[(size_t)(j0 + j) * ld2 + i];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (i0 + u * stride >= n2) break;
+#pragma unroll
+            for (int j = 0; j < K; ++j)
+                if (j0 + j < k) {
+                    acc[j] = __fma_rn(wv[u].x, v[u][j].x, acc[j]);
+                    acc[j] = __fma_rn(wv[u].y, v[u][j].y, acc[j]);
+                }
+        }
+    }
+    __shared__ double sh[8][K];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const double v = warp_sum(acc[j]);
+        if (lane == 0) sh[warp][j] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < K && j0 + (int)threadIdx.x < k) {
+        double s = 0.0;
+        for (int q = 0; q < 8; ++q) s += sh[q][threadIdx.x];
+        partials[(size_t)blockIdx.x * 64 + j0 + threadIdx.x] = s;
+    }
+}
+
 __global__ void l1_kernel(const double *__restrict__ x, const double *__restrict__ y, uint64_t n,
                           double *__restrict__ partials)
 {
@@ -190,6 +242,30 @@ __global__ void multi_axpy_kernel(double *__restrict__ w, const double *__restri
     if (i >= n) return;
     double s = w[i];
     for (int j = 0; j < k; ++j) s = __fma_rn(-h[j], V[(size_t)j * ld + i], s);
+    w[i] = s;
+}
+
+// The same update on 16-byte pairs, eight basis vectors' loads issued
+// before their FMAs (the same operations in the same order per element).
+__global__ void multi_axpy2_kernel(double2 *__restrict__ w, const double2 *__restrict__ V, size_t ld2,
+                                   const double *__restrict__ h, int k, uint64_t n2)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n2) return;
+    double2 s = w[i];
+    for (int j0 = 0; j0 < k; j0 += 8) {
+        double2 v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (j0 + j < k) v[j] = V[(size_t)(j0 + j) * ld2 + i];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (j0 + j < k) {
+                const double hj = h[j0 + j];
+                s.x = __fma_rn(-hj, v[j].x, s.x);
+                s.y = __fma_rn(-hj, v[j].y, s.y);
+            }
+    }
     w[i] = s;
 }
 
@@ -257,7 +333,7 @@ cudaError_t launch_bump_epoch(uint32_t *epoch, cudaStream_t s)
 
 cudaError_t reducer_init(Reducer &r, cudaStream_t s)
 {
-    cudaError_t e = dev_malloc(&r.partials, sizeof(double) * kReduceBlocks * 64, s);
+    cudaError_t e = dev_malloc(&r.partials, sizeof(double) * std::max(kReduceBlocks, kDotBlocks) * 64, s);
     if (e == cudaSuccess) e = dev_malloc(&r.result, sizeof(double) * kReduceSlots, s);
     if (e == cudaSuccess) e = cudaMallocHost(&r.host, sizeof(double) * kReduceSlots);
     if (e == cudaSuccess) std::memset(r.host, 0, sizeof(double) * kReduceSlots);
@@ -272,13 +348,42 @@ void reducer_free(Reducer &r, cudaStream_t s)
     r = Reducer();
 }
 
+// k inner products <w, V_j> into per-block partials: pairs of doubles when
+// the vectors allow it, in passes of at most 8 basis vectors.
+static int launch_multi_dot(const double *w, const double *V, size_t ld, int k, uint64_t n, double *partials,
+                            cudaStream_t s)
+{
+    const bool pairs = n % 2 == 0 && ld % 2 == 0 && (reinterpret_cast<uintptr_t>(w) & 15u) == 0 &&
+                       (reinterpret_cast<uintptr_t>(V) & 15u) == 0;
+    if (!pairs) {
+        for (int j0 = 0; j0 < k; j0 += 16)
+            multi_dot_kernel<16><<<kReduceBlocks, 256, 0, s>>>(w, V, ld, k, j0, n, partials);
+        return kReduceBlocks;
+    }
+    const double2 *w2 = reinterpret_cast<const double2 *>(w);
+    const double2 *V2 = reinterpret_cast<const double2 *>(V);
+    for (int j0 = 0; j0 < k;) {
+        const int rem = k - j0;
+        if (rem <= 2) {
+            multi_dot2_kernel<2, 4><<<kDotBlocks, 256, 0, s>>>(w2, V2, ld / 2, k, j0, n / 2, partials);
+            j0 += 2;
+        } else if (rem <= 4) {
+            multi_dot2_kernel<4, 2><<<kDotBlocks, 256, 0, s>>>(w2, V2, ld / 2, k, j0, n / 2, partials);
+            j0 += 4;
+        } else {
+            multi_dot2_kernel<8, 1><<<kDotBlocks, 256, 0, s>>>(w2, V2, ld / 2, k, j0, n / 2, partials);
+            j0 += 8;
+        }
+    }
+    return kDotBlocks;
+}
+
 cudaError_t multi_dot_dev(const double *w, const double *V, size_t ld, int k, uint64_t n, Reducer &r, double *dst,
                           cudaStream_t s)
 {
     if (k < 1 || k > 64) return cudaErrorInvalidValue;
-    for (int j0 = 0; j0 < k; j0 += 16)
-        multi_dot_kernel<16><<<kReduceBlocks, 256, 0, s>>>(w, V, ld, k, j0, n, r.partials);
-    reduce_partials_kernel<<<1, 64, 0, s>>>(r.partials, kReduceBlocks, k, dst);
+    const int nb = launch_multi_dot(w, V, ld, k, n, r.partials, s);
+    reduce_partials_kernel<<<1, 64, 0, s>>>(r.partials, nb, k, dst);
     return cudaGetLastError();
 }
 
@@ -299,9 +404,8 @@ cudaError_t multi_dot(const double *w, const double *V, size_t ld, int k, uint64
                       cudaStream_t s)
 {
     if (k < 1 || k > 64) return cudaErrorInvalidValue;
-    for (int j0 = 0; j0 < k; j0 += 16)
-        multi_dot_kernel<16><<<kReduceBlocks, 256, 0, s>>>(w, V, ld, k, j0, n, r.partials);
-    reduce_partials_kernel<<<1, 64, 0, s>>>(r.partials, kReduceBlocks, k, r.result);
+    const int nb = launch_multi_dot(w, V, ld, k, n, r.partials, s);
+    reduce_partials_kernel<<<1, 64, 0, s>>>(r.partials, nb, k, r.result);
     cudaError_t e = cudaMemcpyAsync(r.host, r.result, sizeof(double) * k, cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return e;
     return cudaStreamSynchronize(s);
@@ -320,7 +424,13 @@ cudaError_t multi_axpy(double *w, const double *V, size_t ld, const double *h, i
                        cudaStream_t s)
 {
     if (n == 0 || k == 0) return cudaSuccess;
-    multi_axpy_kernel<<<blocks_for(n), 256, 0, s>>>(w, V, ld, h, k, n);
+    if (n % 2 == 0 && ld % 2 == 0 && (reinterpret_cast<uintptr_t>(w) & 15u) == 0 &&
+        (reinterpret_cast<uintptr_t>(V) & 15u) == 0)
+        multi_axpy2_kernel<<<blocks_for(n / 2), 256, 0, s>>>(reinterpret_cast<double2 *>(w),
+                                                             reinterpret_cast<const double2 *>(V), ld / 2, h, k,
+                                                             n / 2);
+    else
+        multi_axpy_kernel<<<blocks_for(n), 256, 0, s>>>(w, V, ld, h, k, n);
     return cudaGetLastError();
 }
 

@@ -31,6 +31,7 @@ cudaError_t launch_bump_epoch(uint32_t *epoch, cudaStream_t s);
 // Deterministic reductions: a fixed grid writes per-block partials that one
 // block sums in a fixed order, so results do not depend on scheduling.
 constexpr int kReduceBlocks = 592;  // 4 per SM on 148 SMs
+constexpr int kDotBlocks = 444;     // inner products on pairs: 3 per SM (74-80 registers)
 constexpr int kReduceSlots = 256;   // result / host doubles
 struct Reducer {
     double *partials = nullptr;  // kReduceBlocks * 64
