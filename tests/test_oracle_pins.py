@@ -130,3 +130,39 @@ def test_oracle_psi_writer_format(built, workdir):
     hdr = np.frombuffer(raw[32:64], np.uint64)
     assert list(hdr) == [1, 208, 32, 1]
     assert np.array_equal(np.frombuffer(raw[64:], np.float64), psi.ravel())
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "sweep.x")),
+                    reason="reference build not present")
+def test_problem_checks_match_the_reference_printout(built, workdir):
+    """Problem::hatL2Error and Util::diffBetweenGroups as the reference's
+    main prints them after gold's solve (src/Main.cc:340-344), against
+    tycho2_b200.problems.hat_l2_error / diff_between_groups of that psi."""
+    import re
+    import tycho2_b200 as ty
+    from tycho2_b200 import problems
+    mesh, _ = cube208(workdir)
+    d = os.path.join(str(workdir), "checks")
+    os.makedirs(d, exist_ok=True)
+    deck = os.path.join(d, "gold.deck")
+    with open(deck, "w") as f:
+        f.write("snOrder 8\niterMax 100\nerrMax 1e-10\nmaxCellsPerStep 100\nintraAngleP 3\n"
+                "interAngleP 1\nnGroups 2\nsigmaT1 10\nsigmaS1 5\nsigmaT2 10\nsigmaS2 5\n"
+                "OutputFile true\nOutputFilename out.psi\nSourceIteration true\n"
+                "MPIType TychoTwoSided\nDD_IterMax 100\nDD_ErrMax 1e-10\n"
+                "SweepType TraverseGraph\nGaussElim NoPivot\n")
+    r = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "sweep.x"),
+                        os.path.join(str(workdir), "cube-208.pmesh"), deck],
+                       cwd=d, env=dict(os.environ, OMP_NUM_THREADS="2"), check=True,
+                       capture_output=True, text=True)
+    l2 = float(re.search(r"L2 Relative Error: (\S+)", r.stdout).group(1))
+    dg = float(re.search(r"Diff between groups: (\S+)", r.stdout).group(1))
+    psi = np.fromfile(os.path.join(d, "out.psi"))[8:].reshape(208, 128, 4, 2)
+    assert abs(problems.hat_l2_error(mesh, psi) - l2) <= 1e-6 * l2
+    assert abs(problems.diff_between_groups(psi) - dg) <= 1e-6 * max(dg, 1e-300)
+    # groups with equal cross sections and sources: identical psi
+    assert problems.diff_between_groups(psi) == 0.0 and dg == 0.0
+    # a psi whose groups differ
+    psi2 = psi.copy()
+    psi2[..., 1] *= 1.5
+    assert problems.diff_between_groups(psi2) > 0.0

@@ -2,7 +2,8 @@
 and the benchmark workloads.
 
 hat_source / hat_l2_error restate Problem::hatSource / hatL2Error
-(src/Problem.cc:47-134) for meshes on [0,100]^3.  The benchmark family
+(src/Problem.cc:47-134) for meshes on [0,100]^3; diff_between_groups the
+reference's group-consistency check (src/Util.cc:55-79).  The benchmark family
 (`workload`) extends the reference's two-material problem with per-cell
 lognormal sigma_t, a lower-triangular downscatter matrix and a box source,
 all drawn from seeded generators; q is the angular source density, the
@@ -36,6 +37,18 @@ def hat_l2_error(mesh, psi):
     val = psi.mean(axis=2)  # (c, a, g)
     diff = val - act[:, None, None]
     return float(np.sqrt((diff ** 2).sum() / (val ** 2).sum()))
+
+
+def diff_between_groups(psi):
+    """Util::diffBetweenGroups (src/Util.cc:55-79): the largest |psi_g -
+    psi_0| over groups g >= 1, cells, angles and vertices, relative to the
+    largest |psi_0| (0 when every group carries the same psi, as the
+    reference's within-group problems do).  psi: PsiData layout (c, a, 4, G)."""
+    p = np.asarray(psi)
+    p0 = p[..., 0]
+    max_entry = float(np.abs(p0).max())
+    max_diff = float(np.abs(p[..., 1:] - p0[..., None]).max()) if p.shape[-1] > 1 else 0.0
+    return max_diff / max_entry
 
 
 def downscatter_matrix(n_groups, ratio):
