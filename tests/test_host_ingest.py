@@ -190,3 +190,18 @@ def test_zero_volume_cell_is_rejected(built, workdir):
     with pytest.raises(TychoError) as e:
         ty.TychoMesh.read_smesh(path)
     assert e.value.status == 3
+
+
+def test_face_vertex_numbering_must_round_trip(built):
+    """TychoMesh's constructor insists that cellToFaceVrtx and
+    faceToCellVrtx invert each other (src/TychoMesh.cc:225-240); a mesh whose
+    face 0 lists one vertex twice is rejected."""
+    import tycho2_b200 as ty
+    m = ty.TychoMesh.kuhn_cube(1, 0.0, 0, 1.0)
+    t = m.tables()
+    f2c = t["face_to_cell"].copy()
+    f2c[0, 0] = [1, 1, 3]  # vertex 2 of face 0 missing
+    with pytest.raises(ty.TychoError, match="round-trip"):
+        ty.TychoMesh.from_arrays(t["cell_nodes"], t["coords"], t["adj_cell"], f2c)
+    ok = ty.TychoMesh.from_arrays(t["cell_nodes"], t["coords"], t["adj_cell"], t["face_to_cell"])
+    assert ok.n_cells == m.n_cells

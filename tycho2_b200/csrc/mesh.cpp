@@ -390,6 +390,26 @@ int build_tables(const MeshRecords &m, MeshTables &t, std::string &err)
 int finish_tables(MeshTables &t, std::string &err)
 {
     const uint64_t nc = t.n_cells;
+    // cellToFaceVrtx and faceToCellVrtx invert each other on every face
+    // (the reference's check, src/TychoMesh.cc:225-240)
+    for (uint64_t c = 0; c < nc; ++c)
+        for (int f = 0; f < 4; ++f) {
+            for (int cv = 0; cv < 4; ++cv) {
+                if (cv == f) continue;
+                const uint64_t fv = t.cell_to_face[(c * 4 + f) * 4 + cv];
+                if (fv >= 3 || t.face_to_cell[(c * 4 + f) * 3 + fv] != (uint64_t)cv) {
+                    err = "face-vertex numbering of cell " + std::to_string(c) + " does not round-trip";
+                    return kErrFormat;
+                }
+            }
+            for (int fv = 0; fv < 3; ++fv) {
+                const uint64_t cv = t.face_to_cell[(c * 4 + f) * 3 + fv];
+                if (cv >= 4 || t.cell_to_face[(c * 4 + f) * 4 + cv] != (uint64_t)fv) {
+                    err = "face-vertex numbering of cell " + std::to_string(c) + " does not round-trip";
+                    return kErrFormat;
+                }
+            }
+        }
     // Geometry with the reference's operation order (src/TychoMesh.cc:67-187).
     t.volume.resize(nc); t.area.resize(nc * 4); t.normal.resize(nc * 12);
     for (uint64_t c = 0; c < nc; ++c) {
