@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(256) batch_psi_to_phi_kernel(const BatchSlot *
         const Real *psi = (const Real *)s.psi;
         if (s.G >= 8) {
             for (uint64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x)
-                s.phi_out[i] = psi_to_phi_elem(psi, s.w, i, s.A, s.G);
+                s.phi_out[i] = psi_to_phi_elem8(psi, s.w, i, s.A, s.G);
             return;
         }
         for (uint64_t i = i0 + 4 * threadIdx.x; i < i1; i += 4 * blockDim.x) {

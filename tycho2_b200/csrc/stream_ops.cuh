@@ -92,6 +92,31 @@ __device__ __forceinline__ double psi_to_phi_elem(const Real *__restrict__ psi, 
     return s;
 }
 
+// The same sum with eight angles' loads issued before their products are
+// added (in the same order, so the same bits): for grid-stride loops over
+// many elements per thread (the batched passes), which would otherwise
+// wait one load latency per angle.
+template <typename Real>
+__device__ __forceinline__ double psi_to_phi_elem8(const Real *__restrict__ psi, const double *__restrict__ w,
+                                                   uint64_t i, uint32_t A, uint32_t G)
+{
+    const uint64_t row = (uint64_t)4 * G;
+    const uint64_t c = i / row;
+    const uint64_t vg = i - c * row;
+    const Real *p = psi + c * A * row + vg;
+    double s = 0.0;
+    uint32_t a = 0;
+    for (; a + 8 <= A; a += 8) {
+        Real v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = p[(size_t)(a + k) * row];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s += (double)v[k] * w[a + k];
+    }
+    for (; a < A; ++a) s += (double)p[(size_t)a * row] * w[a];
+    return s;
+}
+
 // The same for the four elements i .. i+3 (i a multiple of 4: they lie in one
 // cell's row and are contiguous in psi for every angle): one 16-byte (FP32)
 // or two 16-byte (FP64) loads per angle, eight angles in flight, and for
