@@ -63,7 +63,7 @@ def parse():
     p.add_argument("--no-serve", action="store_true", help="skip the served-solves leg")
     p.add_argument("--no-parity", action="store_true",
                    help="skip the oracle checks of the benchmarked solves (run after the timed legs)")
-    p.add_argument("--serve-requests", type=int, default=200, help="requests per arrival rate")
+    p.add_argument("--serve-requests", type=int, default=400, help="requests per arrival rate")
     p.add_argument("--serve-rates", default="20,50,100,200",
                    help="Poisson arrival rates (requests per second), comma-separated")
     p.add_argument("--shape", default="default",
