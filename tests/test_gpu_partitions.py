@@ -167,6 +167,10 @@ def test_device_exchange_matches_commsides(built, workdir, P):
 @pytest.mark.timeout(600)
 def test_pbj_solvers_on_the_gpu_match_the_oracle(built, workdir):
     from tycho2_b200.partitions import PartitionSet, pbj, pbj_outer, pbj_si, schur, schur_krylov, schur_outer
+
+    def pbj_krylov(ps, **kw):
+        return pbj(ps, method="krylov", **kw)
+
     from test_partitions import _gather, _single_partition_si
     path, _ = partitions_fixture(workdir, 4)
     ref, it_ref = _single_partition_si(workdir)
@@ -175,7 +179,8 @@ def test_pbj_solvers_on_the_gpu_match_the_oracle(built, workdir):
                        (pbj_outer, dict(iter_max=400, err_max=1e-13, dd_iter_max=100, dd_err_max=1e-12)),
                        (schur, dict(iter_max=400, err_max=1e-12, dd_iter_max=200, dd_err_max=1e-13)),
                        (schur_krylov, dict(dd_iter_max=400, dd_err_max=1e-13)),
-                       (schur_outer, dict(iter_max=400, err_max=1e-13, dd_iter_max=100, dd_err_max=1e-12))):
+                       (schur_outer, dict(iter_max=400, err_max=1e-13, dd_iter_max=100, dd_err_max=1e-12)),
+                       (pbj_krylov, dict(iter_max=200, err_max=1e-12, dd_iter_max=200, dd_err_max=1e-13))):
         gpu = PartitionSet(_parts(path, 4, "gpu"))
         ora = PartitionSet(_parts(path, 4, "oracle"))
         rg = solver(gpu, **kw)
@@ -188,7 +193,8 @@ def test_pbj_solvers_on_the_gpu_match_the_oracle(built, workdir):
         # within rounding of a tolerance may end one iteration apart
         counts = {pbj_si: lambda r: (r[1],), pbj: lambda r: (r[1], r[3]), pbj_outer: lambda r: (r[1], r[2]),
                   schur: lambda r: (r[1], r[3]), schur_krylov: lambda r: (r[1],),
-                  schur_outer: lambda r: (r[1], r[3][0], tuple(r[3][1]), r[3][2])}[solver]
+                  schur_outer: lambda r: (r[1], r[3][0], tuple(r[3][1]), r[3][2]),
+                  pbj_krylov: lambda r: (r[1], r[3])}[solver]
         if counts(rg) == counts(ro):
             assert bits_equal(phi_g, phi_o), solver.__name__
         else:

@@ -217,3 +217,29 @@ def test_pbj_over_two_gloo_ranks_matches_one_process(built, workdir):
         assert np.array_equal(gid, ps.parts[r].gid)
         assert it_si == it and bits_equal(p_si, phi[r].numpy())
         assert it_pbj == it2 and sw_pbj == sweeps2 and bits_equal(p_pbj, phi2[r].numpy())
+
+
+@pytest.mark.timeout(300)
+def test_krylov_forms_reach_the_single_partition_solution(built, workdir):
+    """SourceIteration::krylov over the PBJ, PBJOuter and Schur sweeps
+    (deck key SourceIteration false)."""
+    from tycho2_b200.partitions import PartitionSet, pbj, pbj_outer, schur, source_krylov
+    path, _ = partitions_fixture(workdir, 2)
+    ref, it_ref = _single_partition_si(workdir)
+    ps = PartitionSet(_oracle_parts(path, 2))
+    phi, its, rn, sweeps = pbj(ps, iter_max=200, err_max=1e-12, dd_iter_max=200, dd_err_max=1e-13,
+                               method="krylov")
+    assert its < it_ref and sweeps > its
+    assert rel_l1(_gather(ps.parts, phi), ref) <= 1e-10
+    ps = PartitionSet(_oracle_parts(path, 2))
+    phi, its, rn, sweeps = schur(ps, iter_max=200, err_max=1e-12, dd_iter_max=200, dd_err_max=1e-13,
+                                 method="krylov")
+    assert its < it_ref
+    assert rel_l1(_gather(ps.parts, phi), ref) <= 1e-10
+    ps = PartitionSet(_oracle_parts(path, 2))
+    phi, outer, its = pbj_outer(ps, iter_max=200, err_max=1e-13, dd_iter_max=200, dd_err_max=1e-12,
+                                method="krylov")
+    assert outer > 1 and all(k > 0 for k in its)
+    assert rel_l1(_gather(ps.parts, phi), ref) <= 1e-10
+    with pytest.raises(ValueError):
+        source_krylov(ps, "traverse")

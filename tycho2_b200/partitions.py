@@ -32,6 +32,8 @@ the same operations to the solvers below:
              operator application)
   schur_krylov SweeperSchurKrylov::solve src/SweeperSchur.cc:487-604 (one
              GMRES over the boundary values and phi together)
+  source_krylov SourceIteration::krylov over the PBJ, PBJOuter or Schur
+             sweep (the solvers' deck key SourceIteration false)
 
 Iteration counts and convergence follow the reference's tests; the L1 sums
 run on the device, in another order than the reference's loops, so a
@@ -261,14 +263,14 @@ def pbj_si(ps, dd_iter_max=100, dd_err_max=1e-10):
     return phi0, it, err
 
 
-def _pbj_sweep(ps, phi_old, phi_out, dd_iter_max, dd_err_max):
+def _pbj_sweep(ps, phi_old, phi_out, dd_iter_max, dd_err_max, with_fixed=True):
     """SweeperPBJ::sweep: sweepLocal until psi changes by less than
     dd_err_max (L1, relative), exchanging after every sweep that has not
     converged.  Returns the number of local sweeps."""
     it = 1
     while it < dd_iter_max:
         for p, a, b in zip(ps.local, phi_old, phi_out):
-            p.apply(a, b, True)
+            p.apply(a, b, with_fixed)
         d, m = ps.allsum([sum(v) for v in zip(*[p.psi_change() for p in ps.local])])
         if m > 0 and d / m < dd_err_max:
             break
@@ -277,10 +279,17 @@ def _pbj_sweep(ps, phi_old, phi_out, dd_iter_max, dd_err_max):
     return it
 
 
-def pbj(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10):
+def pbj(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10, method="si"):
     """SweeperPBJ::solve with source iteration (SourceIteration::fixedPoint,
-    src/SourceIteration.cc:127-207, over SweeperPBJ::sweep).  Returns (phi
-    per local partition, source iterations, last change, local sweeps)."""
+    src/SourceIteration.cc:127-207, over SweeperPBJ::sweep), or with
+    method "krylov" SourceIteration::krylov over the same sweep
+    (source_krylov).  Returns (phi per local partition, source iterations
+    or Krylov iterations, last change or residual norm, local sweeps)."""
+    if method == "krylov":
+        counter = _SweepCounter(ps)
+        phi, its, rn = source_krylov(counter, "pbj", iter_max, err_max, dd_iter_max=dd_iter_max,
+                                     dd_err_max=dd_err_max)
+        return phi, its, rn, counter.sweeps
     phi_new = [p.phi_zeros() for p in ps.local]
     phi_old = [p.phi_zeros() for p in ps.local]
     it, err, sweeps = 0, 1.0, 0
@@ -294,17 +303,30 @@ def pbj(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10):
     return phi_new, it, err, sweeps
 
 
-def pbj_outer(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10):
-    """SweeperPBJOuter::solve with source iteration: each outer iteration
-    runs SourceIteration::fixedPoint to err_max from the current psi with
-    the boundary values fixed, then tests the L1 change of psi against
-    dd_err_max and exchanges.  Returns (phi per local partition, outer
-    iterations, source iterations per outer iteration)."""
+def pbj_outer(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10, method="si"):
+    """SweeperPBJOuter::solve: each outer iteration solves the partitions'
+    problems with the boundary values fixed -- SourceIteration::fixedPoint
+    to err_max from the current psi, or with method "krylov"
+    SourceIteration::krylov (source_krylov, "pbj_outer") -- then tests the
+    L1 change of psi against dd_err_max and exchanges.  Returns (phi per
+    local partition, outer iterations, inner iterations per outer
+    iteration)."""
     phi_new = [p.phi_zeros() for p in ps.local]
     phi_old = [p.phi_zeros() for p in ps.local]
     its = []
     outer = 1
     while outer < dd_iter_max:
+        if method == "krylov":
+            phi, k, _ = source_krylov(ps, "pbj_outer", iter_max, err_max)
+            for a, b in zip(phi_new, phi):
+                a.copy_(b)
+            its.append(k)
+            d, m = ps.allsum([sum(v) for v in zip(*[p.psi_change() for p in ps.local])])
+            if m > 0 and d / m < dd_err_max:
+                break
+            ps.exchange()
+            outer += 1
+            continue
         it, err = 0, 1.0
         while it < iter_max and err > err_max:
             for a, b in zip(phi_old, phi_new):
@@ -324,13 +346,18 @@ def pbj_outer(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10
 
 
 def _dot(ps, u, v):
-    """Inner product of two distributed vectors (lists of host arrays, one
-    per local partition) over every partition."""
-    return ps.allsum([sum(float(np.dot(a.reshape(-1), b.reshape(-1))) for a, b in zip(u, v))])[0]
+    """Inner product of two distributed vectors (lists of arrays -- numpy on
+    the host or torch tensors -- one per local partition) over every
+    partition."""
+    return ps.allsum([sum(float((a.reshape(-1) * b.reshape(-1)).sum()) for a, b in zip(u, v))])[0]
+
+
+def _copy(a):
+    return a.clone() if hasattr(a, "clone") else a.copy()
 
 
 def _gmres(ps, op, b, x, rtol, iter_max, restart=30):
-    """Restarted GMRES on distributed host vectors (lists of arrays, one per
+    """Restarted GMRES on distributed vectors (lists of arrays, one per
     local partition): op(x) -> A x, b the right-hand side, x the initial
     guess (updated in place); classical Gram-Schmidt twice, Givens
     rotations, the true residual at each restart, stop when ||r|| <= rtol
@@ -345,8 +372,8 @@ def _gmres(ps, op, b, x, rtol, iter_max, restart=30):
         return [bi - ai for bi, ai in zip(b, ax)]
 
     # a zero initial guess needs no operator application (as KSPSolve)
-    zero = ps.allsum([float(sum(np.abs(xi).sum() for xi in x))])[0] == 0.0
-    r = [bi.copy() for bi in b] if zero else residual()
+    zero = ps.allsum([float(sum(float(abs(xi).sum()) for xi in x))])[0] == 0.0
+    r = [_copy(bi) for bi in b] if zero else residual()
     beta = np.sqrt(_dot(ps, r, r))
     while its < iter_max and beta > rtol * bnorm:
         V = [[ri / beta for ri in r]]
@@ -395,7 +422,7 @@ def _sweep_exchange(ps, bounds, phi_in, with_fixed, phi_out):
     return [part.get_bound() for part in ps.local]
 
 
-def schur(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10):
+def schur(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10, method="si"):
     """SweeperSchur::solve with source iteration (src/SweeperSchur.cc:
     196-326): every sweep of SourceIteration::fixedPoint solves for the
     incoming partition-boundary psi by Krylov,
@@ -405,33 +432,55 @@ def schur(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10):
     exchange), then sweeps each partition with the solved values.  The
     Krylov vectors are the partitions' psiBound arrays on the host.
     Returns (phi per local partition, source iterations, last change,
+    local sweeps); with method "krylov" SourceIteration::krylov over the
+    same sweep (source_krylov): (phi, Krylov iterations, residual norm,
     local sweeps)."""
+    if method == "krylov":
+        counter = _SweepCounter(ps)
+        phi, its, rn = source_krylov(counter, "schur", iter_max, err_max, dd_iter_max=dd_iter_max,
+                                     dd_err_max=dd_err_max)
+        return phi, its, rn, counter.sweeps
     phi_new = [p.phi_zeros() for p in ps.local]
     phi_old = [p.phi_zeros() for p in ps.local]
-    tmp = [p.phi_zeros() for p in ps.local]
-    prev = [np.zeros_like(p.get_bound()) for p in ps.local]
-    it, err, sweeps = 0, 1.0, 0
-
-    def op(x):
-        y = _sweep_exchange(ps, x, [None] * len(x), False, tmp)
-        return [xi - yi for xi, yi in zip(x, y)]
-
+    state = _SchurState(ps)
+    it, err = 0, 1.0
     while it < iter_max and err > err_max:
         for a, b in zip(phi_old, phi_new):
             a.copy_(b)
-        rhs = _sweep_exchange(ps, [np.zeros_like(x) for x in prev], phi_old, True, tmp)
-        x = [pv.copy() for pv in prev]
-        its, _ = _gmres(ps, op, rhs, x, dd_err_max, dd_iter_max)
-        for part, xi in zip(ps.local, x):
-            part.set_bound(xi)
-        for part, a, o in zip(ps.local, phi_old, phi_new):
-            part.apply(a, o, True)
-        prev = x
-        sweeps += 2 + its
+        state.sweep(phi_old, True, phi_new, dd_iter_max, dd_err_max)
         d, m = ps.allsum(_l1(ps.local, phi_new, phi_old))
         err = d / m if m > 0 else 0.0
         it += 1
-    return phi_new, it, err, sweeps
+    return phi_new, it, err, state.sweeps
+
+
+class _SchurState:
+    """SweeperSchur::sweep (src/SweeperSchur.cc:246-323) with its
+    c_psiBoundPrev: the Krylov solve for the incoming boundary values from
+    the last solve's values, then one local sweep with them."""
+
+    def __init__(self, ps):
+        self.ps = ps
+        self.prev = [np.zeros_like(p.get_bound()) for p in ps.local]
+        self.tmp = [p.phi_zeros() for p in ps.local]
+        self.sweeps = 0
+
+    def sweep(self, phi_in, with_fixed, phi_out, dd_iter_max, dd_err_max):
+        ps, tmp = self.ps, self.tmp
+
+        def op(x):
+            y = _sweep_exchange(ps, x, [None] * len(x), False, tmp)
+            return [xi - yi for xi, yi in zip(x, y)]
+
+        rhs = _sweep_exchange(ps, [np.zeros_like(x) for x in self.prev], phi_in, with_fixed, tmp)
+        x = [pv.copy() for pv in self.prev]
+        its, _ = _gmres(ps, op, rhs, x, dd_err_max, dd_iter_max)
+        for part, xi in zip(ps.local, x):
+            part.set_bound(xi)
+        for part, a, o in zip(ps.local, phi_in, phi_out):
+            part.apply(a, o, with_fixed)
+        self.prev = x
+        self.sweeps += 2 + its
 
 
 def schur_outer(ps, iter_max=100, err_max=1e-10, dd_iter_max=100, dd_err_max=1e-10):
@@ -513,6 +562,86 @@ def schur_krylov(ps, dd_iter_max=100, dd_err_max=1e-10):
         part.set_bound(b)
     for part, a, o in zip(ps.local, x[n:], phi):
         part.apply(to_dev(a, o), o, True)
+    return phi, its, rn
+
+
+class _SweepCounter:
+    """The same partitions, counting local sweeps (one per apply of every
+    partition)."""
+
+    def __init__(self, ps):
+        self._ps = ps
+        self.sweeps = 0
+        self.local = [_CountingPart(p, self) for p in ps.local]
+
+    def exchange(self):
+        self._ps.exchange()
+
+    def allsum(self, values):
+        return self._ps.allsum(values)
+
+
+class _CountingPart:
+    def __init__(self, part, counter):
+        self._p, self._c = part, counter
+
+    def apply(self, a, b, with_fixed):
+        if self._p is self._c.local[0]._p:
+            self._c.sweeps += 1
+        self._p.apply(a, b, with_fixed)
+
+    def __getattr__(self, name):
+        return getattr(self._p, name)
+
+
+def source_krylov(ps, sweeper="pbj", iter_max=100, err_max=1e-10, restart=30, dd_iter_max=100,
+                  dd_err_max=1e-10):
+    """SourceIteration::krylov (src/SourceIteration.cc:216-285) over the
+    partitions: GMRES on (I - D L^-1 M S) phi = D L^-1 Q, where L^-1 is the
+    named sweeper's sweep (src/SweeperPBJ.cc, src/SweeperSchur.cc):
+      "pbj"        SweeperPBJ::sweep -- sweepLocal and exchange until psi
+                   settles (the boundary values carry over between sweeps)
+      "pbj_outer"  SweeperPBJOuter::sweep -- one sweepLocal; the operator's
+                   sweeps take zero boundary values (lhsOperator passes
+                   zeroPsiBound, src/SourceIteration.cc:81-103), the others
+                   the values held, which this solver never exchanges
+      "schur"      SweeperSchur::sweep -- the Krylov solve for the boundary
+                   values, then sweepLocal
+    then psi = L^-1 (M S phi + Q).  Returns (phi per local partition,
+    iterations, residual norm)."""
+    n = len(ps.local)
+    state = _SchurState(ps) if sweeper == "schur" else None
+    if sweeper not in ("pbj", "pbj_outer", "schur"):
+        raise ValueError("sweeper must be 'pbj', 'pbj_outer' or 'schur'")
+
+    def sweep(phi_in, with_fixed, zero_bound, phi_out):
+        if sweeper == "pbj":
+            _pbj_sweep(ps, phi_in, phi_out, dd_iter_max, dd_err_max, with_fixed)
+        elif sweeper == "schur":
+            state.sweep(phi_in, with_fixed, phi_out, dd_iter_max, dd_err_max)
+        else:
+            keep = [p.get_bound() for p in ps.local] if zero_bound else None
+            if keep is not None:
+                for p, k in zip(ps.local, keep):
+                    p.set_bound(np.zeros_like(k))
+            for p, a, o in zip(ps.local, phi_in, phi_out):
+                p.apply(a, o, with_fixed)
+            if keep is not None:
+                for p, k in zip(ps.local, keep):
+                    p.set_bound(k)
+
+    tmp = [p.phi_zeros() for p in ps.local]
+    b = [p.phi_zeros() for p in ps.local]
+    sweep([None] * n, True, False, b)
+
+    def op(x):
+        sweep(x, False, True, tmp)
+        return [xi - ti for xi, ti in zip(x, tmp)]
+
+    x = [p.phi_zeros() for p in ps.local]
+    its, rn = _gmres(ps, op, b, x, err_max, iter_max, restart)
+    phi = [p.phi_zeros() for p in ps.local]
+    sweep(x, True, False, phi)
     return phi, its, rn
 
 
