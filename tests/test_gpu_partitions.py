@@ -195,7 +195,12 @@ def test_pbj_solvers_on_the_gpu_match_the_oracle(built, workdir):
                   schur: lambda r: (r[1], r[3]), schur_krylov: lambda r: (r[1],),
                   schur_outer: lambda r: (r[1], r[3][0], tuple(r[3][1]), r[3][2]),
                   pbj_krylov: lambda r: (r[1], r[3])}[solver]
-        if counts(rg) == counts(ro):
+        if solver is pbj_krylov:
+            # GMRES on phi: its inner products are summed on the device for
+            # GPU partitions and on the host for the oracle's, so the iterates
+            # agree to rounding, not bit for bit
+            assert abs(rg[1] - ro[1]) <= 1 and rel_l1(phi_g, phi_o) <= 1e-11, solver.__name__
+        elif counts(rg) == counts(ro):
             assert bits_equal(phi_g, phi_o), solver.__name__
         else:
             assert abs(rg[1] - ro[1]) <= 1, (solver.__name__, counts(rg), counts(ro))
