@@ -263,3 +263,54 @@ def test_reference_adapter_sweep_local(built, workdir):
         assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
         psi = np.fromfile(files[3])
         assert psi_hash(psi) == int(ref["p%d_%d_psi_hash" % (P, p)][0]), p
+
+
+def _dist_worker(rank, world, port, path, out):
+    import datetime
+    import sys
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world),
+                      RANK=str(rank), LOCAL_RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import torch.distributed as dist
+    from tycho2_b200.partitions import DistributedPartitions, pbj_si
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        part = _parts(path, world, "gpu")[rank]
+        phi, it, err = pbj_si(DistributedPartitions(part), dd_iter_max=400, dd_err_max=1e-12)
+        out.put((rank, phi[0].cpu().numpy().copy(), it))
+        part.sw.close()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(600)
+def test_distributed_partitions_two_processes(built, workdir):
+    """Two processes, one partition each, on the one GPU: their device
+    sweeps never wait on each other (the packets go through gloo on the
+    host between sweeps); they take the one-process GPU partition set's
+    iterations to the same phi, bit for bit."""
+    import socket
+    import torch.multiprocessing as mp
+    from tycho2_b200.partitions import PartitionSet, pbj_si
+    path, _ = partitions_fixture(workdir, 2)
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_dist_worker, args=(r, 2, port, path, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = {}
+    for _ in range(2):
+        r = q.get(timeout=500)
+        got[r[0]] = r[1:]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    ps = PartitionSet(_parts(path, 2, "gpu"))
+    phi, it, err = pbj_si(ps, dd_iter_max=400, dd_err_max=1e-12)
+    for r in range(2):
+        assert got[r][1] == it and bits_equal(got[r][0], phi[r].cpu().numpy()), r
+    ps.close()
