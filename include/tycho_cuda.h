@@ -93,6 +93,9 @@ int tycho_mesh_read_pmesh_partition(const char *path, uint64_t partition, tycho_
    partition (any pointer may be NULL). */
 int tycho_mesh_partition_info(const tycho_mesh *mesh, uint64_t *partition, uint64_t *n_partitions,
                               uint64_t *n_bound_sides);
+/* Material index of each cell [n] (TychoMesh::getCellMaterial; 1 for meshes
+   made from arrays). */
+int tycho_mesh_cell_material(const tycho_mesh *mesh, uint64_t *material);
 /* For a mesh made from a reference TychoMesh's arrays (tycho_mesh_from_arrays)
    on one MPI rank of a multi-partition run: the rank, the number of ranks,
    adj_rank [n*4] (getAdjRank, UINT64_MAX = BAD_RANK on the mesh boundary)
@@ -268,6 +271,9 @@ int tycho_sweeper_solve(tycho_sweeper *sw, const tycho_solve_opts *opts, double 
 /* Writes the resident psi in the reference's .psi format
    (PsiData::writeToFile, src/PsiData.cc:62-106). */
 int tycho_sweeper_write_psi(tycho_sweeper *sw, const char *path);
+/* The resident psi of the last FP64 sweep, solve or operator application
+   into host memory (PsiData layout, this sweeper's cells and directions). */
+int tycho_sweeper_read_psi(tycho_sweeper *sw, double *psi);
 
 /* Schedule facts: levels (max over angles), items (cells x angles) and the
    number of incoming interior faces summed over items. */

@@ -69,6 +69,8 @@ SIGNATURES = {
     "tycho_mesh_partition_info": (C.c_int, [_P, _U64P, _U64P, _U64P]),
     "tycho_mesh_side_tables": (C.c_int, [_P, _P, _P, _P]),
     "tycho_mesh_set_partition": (C.c_int, [_P, C.c_uint64, C.c_uint64, _P, _P]),
+    "tycho_mesh_cell_material": (C.c_int, [_P, _P]),
+    "tycho_sweeper_read_psi": (C.c_int, [_P, _P]),
     "tycho_mesh_kuhn_cube": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, C.c_double, _PP]),
     "tycho_mesh_from_arrays": (C.c_int, [C.c_uint64, C.c_uint64, _P, _P, _P, _P, _P, _PP]),
     "tycho_mesh_write_smesh": (C.c_int, [_P, C.c_char_p]),

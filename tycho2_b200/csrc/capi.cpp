@@ -154,6 +154,15 @@ int tycho_mesh_partition_info(const tycho_mesh *m, uint64_t *partition, uint64_t
     return TYCHO_OK;
 }
 
+int tycho_mesh_cell_material(const tycho_mesh *m, uint64_t *material)
+{
+    if (!m || !material) return finish(TYCHO_ERR_ARG, "null argument");
+    const auto &t = m->tab;
+    if (t.cell_material.size() != t.n_cells) return finish(TYCHO_ERR_MISSING, "mesh has no material indices");
+    std::memcpy(material, t.cell_material.data(), sizeof(uint64_t) * t.n_cells);
+    return TYCHO_OK;
+}
+
 int tycho_mesh_set_partition(tycho_mesh *m, uint64_t partition, uint64_t n_partitions, const uint64_t *adj_rank,
                              const uint64_t *side_gid)
 {
@@ -428,6 +437,13 @@ int tycho_sweeper_solve(tycho_sweeper *h, const tycho_solve_opts *opts, double *
         }
         return finish(s, err);
     });
+}
+
+int tycho_sweeper_read_psi(tycho_sweeper *h, double *psi)
+{
+    if (!h || !psi) return finish(TYCHO_ERR_ARG, "null argument");
+    std::string err;
+    return guarded([&] { return finish(h->sw.read_psi(psi, err), err); });
 }
 
 int tycho_sweeper_write_psi(tycho_sweeper *h, const char *path)

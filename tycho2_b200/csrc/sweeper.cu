@@ -1557,6 +1557,16 @@ int Sweeper::solve(const SolveOptions &o, double *phi_out, double *psi_out, Solv
     return status;
 }
 
+int Sweeper::read_psi(double *psi, std::string &err)
+{
+    if (!psi) { err = "psi is required"; return kErrArg; }
+    if (last_psi_prec_ != 0) { err = "no FP64 psi resident (run a solve or an FP64 sweep first)"; return kErrMissing; }
+    TY_CUDA(cudaSetDevice(device_));
+    TY_CUDA(cudaMemcpyAsync(psi, d_psi_, sizeof(double) * psi_size(), cudaMemcpyDeviceToHost, stream_));
+    TY_CUDA(cudaStreamSynchronize(stream_));
+    return kOk;
+}
+
 int Sweeper::write_psi(const std::string &path, std::string &err)
 {
     if (last_psi_prec_ != 0) { err = "no FP64 psi resident (run a solve or an FP64 sweep first)"; return kErrMissing; }

@@ -76,6 +76,8 @@ public:
     int solve(const SolveOptions &o, double *phi_out, double *psi_out, SolveStats &st,
               std::string &err);
     int write_psi(const std::string &path, std::string &err);
+    // The resident FP64 psi (the last FP64 sweep's) into host memory, PsiData layout.
+    int read_psi(double *psi, std::string &err);
     int time_sweeps(int precision, int n, bool flush_l2, double *ms, std::string &err);
     // vg: record variant's groups per vector access (0 = widest dividing G).
     int configure(int prec, int schedule, int variant, int knob, std::string &err, int vg = 0, int streams = 1);

@@ -44,6 +44,12 @@ class TychoMesh:
             check(lib().tycho_mesh_read_pmesh_partition(str(path).encode(), int(partition), C.byref(h)))
         return cls(h.value)
 
+    def cell_material(self):
+        """TychoMesh::getCellMaterial of every cell."""
+        m = np.empty(self.n_cells, np.uint64)
+        check(lib().tycho_mesh_cell_material(self._h, ptr(m)))
+        return m
+
     def side_tables(self):
         """(side (c,4), adj_rank (c,4), side_gid (n_sides)): TychoMesh::getSide,
         getAdjRank and getLGSide; UINT64_MAX where the reference has
@@ -391,6 +397,12 @@ class SweeperCuda:
         stream = torch.cuda.current_stream(src.device)
         check(lib().tycho_sweeper_side_unpack(self._h, int(q), C.c_void_p(src.data_ptr()),
                                               C.c_void_p(stream.cuda_stream)))
+
+    def read_psi(self):
+        """The resident FP64 psi (PsiData layout) on the host."""
+        psi = np.empty(self.psi_shape)
+        check(lib().tycho_sweeper_read_psi(self._h, ptr(psi)))
+        return psi
 
     def psi_change(self):
         """(L1 of psi - psi_prev, L1 of psi) over the resident FP64 psi, then
