@@ -87,3 +87,34 @@ def test_pipelined_traversal_is_refused_on_partitions(built, workdir):
                        stdout=subprocess.DEVNULL)
     with pytest.raises(ValueError, match="pipelined"):
         run(pm, _deck(d, "refused", SweepType="TraverseGraph"))
+
+
+@pytest.mark.skipif(not os.path.exists(PARTITION_COLUMNS), reason="reference's PartitionColumns not built")
+@pytest.mark.timeout(600)
+def test_two_ranks_under_torchrun(built, workdir):
+    """torchrun with two ranks, one partition each (gloo, both on this GPU:
+    their sweeps never wait on each other): the PBJSI deck writes the same
+    .psi as all partitions in one process."""
+    import io
+    import sys
+    from tycho2_b200.run import run
+    d = str(workdir)
+    pm = os.path.join(d, "cube208_p2.pmesh")
+    if not os.path.exists(pm):
+        subprocess.run([PARTITION_COLUMNS, "2", "1", os.path.join(GOLDEN, "cube-208.smesh"), pm], check=True,
+                       stdout=subprocess.DEVNULL)
+    run(pm, _deck(d, "one_proc", SweepType="PBJSI"), out=io.StringIO())
+    deck = _deck(d, "two_ranks", SweepType="PBJSI")
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    r = subprocess.run(["timeout", "-k", "30", "500", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+                        "--nproc-per-node", "2", "--master-addr", "127.0.0.1", "--master-port", str(port),
+                        "-m", "tycho2_b200.run", pm, deck, "--backend", "gloo"],
+                       cwd=ROOT, capture_output=True, text=True, timeout=560)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-3000:]
+    assert "L2 Relative Error:" in r.stdout
+    a = np.fromfile(os.path.join(d, "one_proc.psi"))
+    b = np.fromfile(os.path.join(d, "two_ranks.psi"))
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))

@@ -224,12 +224,15 @@ def main(argv=None):
     ap.add_argument("deck")
     ap.add_argument("--devices", default=None, help="comma-separated CUDA devices for the partitions "
                                                      "of one process (default: all visible)")
+    ap.add_argument("--backend", default="nccl", choices=["nccl", "gloo"],
+                    help="torch.distributed backend under torchrun (gloo: packets through host memory)")
     a = ap.parse_args(argv)
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        dist.init_process_group("nccl")
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")) % max(1, torch.cuda.device_count()))
+        dist.init_process_group(a.backend, timeout=datetime.timedelta(seconds=300))
     devs = [int(x) for x in a.devices.split(",")] if a.devices else None
     try:
         res = run(a.pmesh, a.deck, devs)
