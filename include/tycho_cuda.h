@@ -13,6 +13,10 @@
  *                          (PhiData, src/PsiData.hh:363-370)
  *   per-face tables        [cell][face][...] row-major, face k opposite
  *                          cell vertex k (src/TychoMeshIO.cc:128-145)
+ *   psiBound               ((side*A + angle)*3 + face vertex)*G + group
+ *                          (PsiBoundData, src/PsiData.hh:253-262): the
+ *                          incoming psi of one partition's faces toward
+ *                          other partitions
  *
  * Every entry point returns a tycho_status; tycho_last_error() gives the
  * message of the calling thread's last failure.  The reference aborts on
