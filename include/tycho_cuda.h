@@ -450,7 +450,8 @@ int tycho_sweeper_side_link(tycho_sweeper *sw, uint64_t q, uint64_t n, const uin
 int tycho_sweeper_side_unpack(tycho_sweeper *sw, uint64_t q, const double *src, void *stream);
 /* SweeperPBJ's convergence measure (src/SweeperPBJ.cc:181-195): L1 norms of
    psi - psi_prev and of psi over the resident FP64 psi, then psi_prev = psi
-   (psi_prev starts at zero). */
+   (psi_prev starts at zero: a psi-sized FP64 copy on the device, allocated
+   by the first call). */
 int tycho_sweeper_psi_change(tycho_sweeper *sw, double *diff, double *norm);
 
 /* Device timing of n back-to-back operator applications
