@@ -103,7 +103,7 @@ cudaError_t launch_direct_subset(const LevelArgs &p, const void *rec, const uint
                                  uint64_t end, cudaStream_t s);
 // Compact records (64 B per item for float, 96 B for double): the inputs of
 // each item's matrix, from which the direct kernels rebuild its factors.
-constexpr size_t compact_record_bytes(bool fp32) { return fp32 ? 64 : 96; }
+constexpr size_t compact_record_bytes(bool fp32) { return fp32 ? 64 : 112; }
 template <typename Real>
 cudaError_t launch_compact_records(const LevelArgs &p, uint64_t n, void *rec, cudaStream_t s);
 // Persistent levels: one cooperative launch, a bounded grid barrier between

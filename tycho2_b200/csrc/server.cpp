@@ -24,7 +24,7 @@ uint64_t footprint_bytes(uint64_t n_cells, int sn_order, int n_groups, bool fp32
     uint64_t b = items * 4 * G * 8;                 // psi (FP64-sized; the FP32 sweep shares it)
     b += items * (32 + (fp32 ? 16 : 0));            // per-item face terms
     b += items * (4 + 4);                           // item list, completion epochs
-    b += items * (compact ? 96 + (fp32 ? 64 : 0) : 256 + (fp32 ? 128 : 0));  // records
+    b += items * (compact ? 112 + (fp32 ? 64 : 0) : 256 + (fp32 ? 128 : 0));  // records
     b += n_cells * (16 + 4 + 24 + 12 + 8 + 8 + 8);  // adjacency, maps, cell terms, sigma, levels
     b += phi * (7 + (fp32 ? 4 : 0));                // phi, iso, r, tmp, (FP32 iso, batch r/d/k)
     return b + (b >> 5) + (8ull << 20);             // allocator rounding

@@ -69,9 +69,12 @@ __device__ __forceinline__ Real over12(Real x)
     else return x / 12.0;
 }
 
+// recip (nullable): the NoPivot pivots' reciprocals 1/M00, 1/a11, 1/b22,
+// computed by this function before (the FP64 compact records carry them),
+// used instead of dividing again.
 template <typename Real>
 __device__ __forceinline__ void item_lu(ItemFactor<Real> &F, Real d1, Real d2, const bool (&out)[4],
-                                        uint32_t kind = kSolveNoPivot);
+                                        uint32_t kind = kSolveNoPivot, const Real *recip = nullptr);
 
 template <typename Real>
 __device__ __forceinline__ void item_setup(const LevelArgs &p, uint64_t it, uint32_t ca, ItemFactor<Real> &F)
@@ -252,7 +255,8 @@ __device__ __forceinline__ void factor16(const ItemFactor<Real> &F, uint32_t kin
 // volume terms d1 = sigma_t V/20, d2 = 2 sigma_t V/20 (out[f]: face f is
 // outgoing), and its LU factors.
 template <typename Real>
-__device__ __forceinline__ void item_lu(ItemFactor<Real> &F, Real d1, Real d2, const bool (&out)[4], uint32_t kind)
+__device__ __forceinline__ void item_lu(ItemFactor<Real> &F, Real d1, Real d2, const bool (&out)[4], uint32_t kind,
+                                        const Real *recip)
 {
     // Streaming + collision (volume integrals), then outgoing-face terms in
     // increasing face order.
@@ -290,19 +294,19 @@ __device__ __forceinline__ void item_lu(ItemFactor<Real> &F, Real d1, Real d2, c
     }
     // LU without pivoting: the elimination steps of gaussElim4 NoPivot that
     // touch only the matrix.
-    F.r0 = div_ref(Real(1), M[0][0]);
+    F.r0 = recip ? recip[0] : div_ref(Real(1), M[0][0]);
     F.u01 = M[0][1] * F.r0; F.u02 = M[0][2] * F.r0; F.u03 = M[0][3] * F.r0;
     F.l1 = M[1][0]; F.l2 = M[2][0]; F.l3 = M[3][0];
     const Real a11 = M[1][1] - F.u01 * F.l1, a12 = M[1][2] - F.u02 * F.l1, a13 = M[1][3] - F.u03 * F.l1;
     const Real a21 = M[2][1] - F.u01 * F.l2, a22 = M[2][2] - F.u02 * F.l2, a23 = M[2][3] - F.u03 * F.l2;
     const Real a31 = M[3][1] - F.u01 * F.l3, a32 = M[3][2] - F.u02 * F.l3, a33 = M[3][3] - F.u03 * F.l3;
     F.a21 = a21; F.a31 = a31;
-    F.r1 = div_ref(Real(1), a11);
+    F.r1 = recip ? recip[1] : div_ref(Real(1), a11);
     F.u12 = a12 * F.r1; F.u13 = a13 * F.r1;
     const Real b22 = a22 - F.u12 * a21, b23 = a23 - F.u13 * a21;
     F.b32 = a32 - F.u12 * a31;
     const Real b33 = a33 - F.u13 * a31;
-    F.r2 = div_ref(Real(1), b22);
+    F.r2 = recip ? recip[2] : div_ref(Real(1), b22);
     F.u23 = b23 * F.r2;
     F.c33 = b33 - F.u23 * F.b32;
 }

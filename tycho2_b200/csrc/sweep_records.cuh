@@ -73,20 +73,26 @@ __global__ void item_record_kernel(const LevelArgs p, uint64_t n, ItemRecord<Rea
     out[it] = r;
 }
 
-// Compact record (64 B float, 96 B double): the inputs of the item's matrix
+// Compact record (64 B float, 112 B double): the inputs of the item's matrix
 // instead of its factors -- t1[f] = A_f/12 (f[0..3]), vs20 = V/20 (f[4]),
 // d1 = sigma_t V/20 (f[5]), d2 = 2 sigma_t V/20 (f[6]) -- and the same
 // topology words as ItemRecord.  The loader rebuilds the LU factors with
 // item_lu (the arithmetic of item_setup: t2 = 2 t1 exactly, a face is
-// outgoing iff t1 > 0), so FP64 results stay bit-identical.
+// outgoing iff t1 > 0), so FP64 results stay bit-identical.  The FP64 record
+// also carries the NoPivot pivots' reciprocals (f[7..9], computed by the
+// same item_lu when the record is built): an IEEE FP64 division is a long
+// dependent sequence, and three of them per task sat on the rebuild's chain.
+template <typename Real>
+constexpr int kCompactF = sizeof(Real) == 8 ? 10 : 7;
+
 template <typename Real>
 struct alignas(16) CompactRecord {
-    Real f[7];
+    Real f[kCompactF<Real>];
     uint32_t u[7];
-    uint32_t pad[(sizeof(Real) == 8 ? 24 : 16) - 7 * (sizeof(Real) / 4) - 7];
+    uint32_t pad[(sizeof(Real) == 8 ? 28 : 16) - kCompactF<Real> * (sizeof(Real) / 4) - 7];
 };
 static_assert(sizeof(CompactRecord<float>) == 64, "float compact record is 64 bytes");
-static_assert(sizeof(CompactRecord<double>) == 96, "double compact record is 96 bytes");
+static_assert(sizeof(CompactRecord<double>) == 112, "double compact record is 112 bytes");
 
 template <typename Real>
 __global__ void compact_record_kernel(const LevelArgs p, uint64_t n, CompactRecord<Real> *out)
@@ -96,7 +102,7 @@ __global__ void compact_record_kernel(const LevelArgs p, uint64_t n, CompactReco
     const uint32_t ca = p.items[it];
     CompactRecord<Real> r;
     if (ca == kSentinel) {
-        for (int i = 0; i < 7; ++i) r.f[i] = Real(0);
+        for (int i = 0; i < kCompactF<Real>; ++i) r.f[i] = Real(0);
         r.u[0] = kSentinel; r.u[1] = 0; r.u[2] = 0;
         for (int f = 0; f < 4; ++f) r.u[3 + f] = kNoRow;
     } else {
@@ -107,6 +113,12 @@ __global__ void compact_record_kernel(const LevelArgs p, uint64_t n, CompactReco
         r.f[4] = F.vs20;
         r.f[5] = ck[1];
         r.f[6] = ck[2];
+        if constexpr (kCompactF<Real> == 10) {
+            const bool np = p.solver == kSolveNoPivot;  // the other solvers factor without them
+            r.f[7] = np ? F.r0 : Real(0);
+            r.f[8] = np ? F.r1 : Real(0);
+            r.f[9] = np ? F.r2 : Real(0);
+        }
         r.u[0] = F.c; r.u[1] = ca; r.u[2] = F.nmap;
         for (int f = 0; f < 4; ++f) r.u[3 + f] = F.adj[f] < 0 ? kNoRow : (uint32_t)F.adj[f] * p.A + F.a;
     }
@@ -227,7 +239,8 @@ __device__ __forceinline__ void load_record(const CompactRecord<Real> *__restric
 #pragma unroll
     for (int i = 0; i < N; ++i) v[i] = __ldg(s + i);
     const Real *fr = reinterpret_cast<const Real *>(v);
-    const uint32_t *ur = reinterpret_cast<const uint32_t *>(reinterpret_cast<const char *>(v) + 7 * sizeof(Real));
+    const uint32_t *ur =
+        reinterpret_cast<const uint32_t *>(reinterpret_cast<const char *>(v) + kCompactF<Real> * sizeof(Real));
 #pragma unroll
     for (int k = 0; k < 7; ++k) r.uv[k] = ur[k];
     r.uv[7] = 0;
@@ -240,7 +253,8 @@ __device__ __forceinline__ void load_record(const CompactRecord<Real> *__restric
         F.t2[f] = Real(2) * fr[f];
         out[f] = fr[f] > Real(0);
     }
-    item_lu(F, fr[5], fr[6], out, kind);
+    if constexpr (kCompactF<Real> == 10) item_lu(F, fr[5], fr[6], out, kind, kind == kSolveNoPivot ? fr + 7 : nullptr);
+    else item_lu(F, fr[5], fr[6], out, kind);
 #pragma unroll
     for (int f = 0; f < 4; ++f) r.fv[f] = F.t1[f];
     r.fv[4] = fr[4];
