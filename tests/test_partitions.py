@@ -192,10 +192,17 @@ def _worker(rank, world, port, path, out):
 
 
 @pytest.mark.timeout(300)
-def test_pbj_over_two_gloo_ranks_matches_one_process(built, workdir):
+@pytest.mark.parametrize("world", [2, 4])
+def test_pbj_over_gloo_ranks_matches_one_process(built, workdir, world):
+    """One partition per gloo rank (2 ranks: one neighbour each; 4: two
+    each, exchanged in increasing neighbour order, which no pair of ranks
+    can deadlock).  With two ranks the all-reduced sums are the one
+    process's, bit for bit; with four, gloo may add the ranks' partial sums
+    in another order, so a change within rounding of the tolerance may end
+    one iteration apart (then phi agrees to the tolerance)."""
     from tycho2_b200.partitions import PartitionSet, pbj, pbj_si
-    path, _ = partitions_fixture(workdir, 2)
-    world, port = 2, _free_port()
+    path, _ = partitions_fixture(workdir, world)
+    port = _free_port()
     ctx = mp.get_context("spawn")
     qu = ctx.Queue()
     procs = [ctx.Process(target=_worker, args=(r, world, port, path, qu)) for r in range(world)]
@@ -208,15 +215,21 @@ def test_pbj_over_two_gloo_ranks_matches_one_process(built, workdir):
     for pr in procs:
         pr.join(timeout=30)
         assert pr.exitcode == 0
-    ps = PartitionSet(_oracle_parts(path, 2))
+    ps = PartitionSet(_oracle_parts(path, world))
     phi, it, err = pbj_si(ps, dd_iter_max=400, dd_err_max=1e-12)
-    ps2 = PartitionSet(_oracle_parts(path, 2))
+    ps2 = PartitionSet(_oracle_parts(path, world))
     phi2, it2, err2, sweeps2 = pbj(ps2, iter_max=400, err_max=1e-12, dd_iter_max=100, dd_err_max=1e-13)
     for r in range(world):
         gid, p_si, it_si, err_si, p_pbj, it_pbj, sw_pbj = got[r]
         assert np.array_equal(gid, ps.parts[r].gid)
-        assert it_si == it and bits_equal(p_si, phi[r].numpy())
-        assert it_pbj == it2 and sw_pbj == sweeps2 and bits_equal(p_pbj, phi2[r].numpy())
+        if world == 2 or it_si == it:
+            assert it_si == it and bits_equal(p_si, phi[r].numpy())
+        else:
+            assert abs(it_si - it) <= 1 and rel_l1(p_si, phi[r].numpy()) <= 1e-11
+        if world == 2 or (it_pbj, sw_pbj) == (it2, sweeps2):
+            assert it_pbj == it2 and sw_pbj == sweeps2 and bits_equal(p_pbj, phi2[r].numpy())
+        else:
+            assert abs(it_pbj - it2) <= 1 and rel_l1(p_pbj, phi2[r].numpy()) <= 1e-11
 
 
 @pytest.mark.timeout(300)
