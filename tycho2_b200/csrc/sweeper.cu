@@ -1129,14 +1129,14 @@ int Sweeper::sweep_host_chunked(const double *source, double *psi, int K, std::s
     const int nt = std::max(1, omp_get_max_threads() / (stage_in && stage_out ? 2 : 1));
     // rows [r0, r1) of the chunk's columns [off, off + width) to or from a
     // packed staging buffer
-    // the pack writes a reused 64 MiB staging buffer: plain stores (the
-    // streaming form was 8% slower there, host-only test of this row
-    // pattern); the unpack writes the caller's psi once: streaming stores
-    // (3x faster in the same test)
     auto pack = [&](char *dst, const char *src, size_t off, size_t width, uint64_t r0, uint64_t r1) {
-#pragma omp parallel for num_threads(nt) schedule(static)
-        for (int64_t r = (int64_t)r0; r < (int64_t)r1; ++r)
-            std::memcpy(dst + (size_t)(r - r0) * width, src + (size_t)r * row + off, width);
+#pragma omp parallel num_threads(nt)
+        {
+#pragma omp for schedule(static)
+            for (int64_t r = (int64_t)r0; r < (int64_t)r1; ++r)
+                copy_row(dst + (size_t)(r - r0) * width, src + (size_t)r * row + off, width);
+            stream_fence();
+        }
     };
     auto unpack = [&](char *dst, const char *src, size_t off, size_t width, uint64_t r0, uint64_t r1) {
 #pragma omp parallel num_threads(nt)
