@@ -218,13 +218,19 @@ __device__ __forceinline__ void batch_direct_chunk(const BatchSeg *segs, uint32_
     const uint32_t itl = gpv == 1u ? task : __umulhi(task, p.vmagic);
     const uint32_t g = (task - itl * gpv) * VG;
     RegRecord<Real> R;
-    load_record((const CompactRecord<Real> *)sg.rec + itl, R, ANY ? p.solver : (uint32_t)kSolveNoPivot);
+    // FP64 NoPivot: the LU is rebuilt after the upwind loads are issued, in
+    // their latency (at 128 registers this also removes the kernel's spills;
+    // the FP32 body measured the same either way and keeps it before).
+    constexpr bool kLate = !ANY && sizeof(Real) == 8;
+    if constexpr (kLate) load_compact_raw((const CompactRecord<Real> *)sg.rec + itl, R);
+    else load_record((const CompactRecord<Real> *)sg.rec + itl, R, ANY ? p.solver : (uint32_t)kSolveNoPivot);
     const bool live = R.u(0) != kSentinel;
     PairIn<Real, VG> in;
     if (live) pair_load_source<Real, VG>(p, R, g, in);
     wait();
     if (live) {
         pair_load_upwind<Real, VG, L2_ONLY>(p, R, g, in);
+        if constexpr (kLate) compact_factor_nopivot(R);
         pair_solve_store_any<Real, VG, RegRecord<Real>, ANY>(p, R, g, in);
     }
 }

@@ -265,6 +265,50 @@ __device__ __forceinline__ void load_record(const CompactRecord<Real> *__restric
     r.uv[7] = F.perm;
 }
 
+// A compact record into registers without its factors: the face terms
+// (fv[0..3]), the volume source factor (fv[4]), the volume terms d1, d2 in
+// fv[5], fv[6] (FP64: the three NoPivot reciprocals in fv[7..9]) and the
+// integer words; compact_factor_nopivot rebuilds the NoPivot LU later, once
+// the task's upwind loads are in flight.
+template <typename Real>
+__device__ __forceinline__ void load_compact_raw(const CompactRecord<Real> *__restrict__ src, RegRecord<Real> &r)
+{
+    constexpr int N = sizeof(CompactRecord<Real>) / 16;
+    uint4 v[N];
+    const uint4 *s = reinterpret_cast<const uint4 *>(src);
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = __ldg(s + i);
+    const Real *fr = reinterpret_cast<const Real *>(v);
+    const uint32_t *ur =
+        reinterpret_cast<const uint32_t *>(reinterpret_cast<const char *>(v) + kCompactF<Real> * sizeof(Real));
+#pragma unroll
+    for (int k = 0; k < 7; ++k) r.uv[k] = ur[k];
+    r.uv[7] = 0;
+#pragma unroll
+    for (int k = 0; k < kCompactF<Real>; ++k) r.fv[k] = fr[k];
+}
+
+template <typename Real>
+__device__ __forceinline__ void compact_factor_nopivot(RegRecord<Real> &r)
+{
+    ItemFactor<Real> F;
+    bool out[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        F.t1[f] = r.fv[f];
+        F.t2[f] = Real(2) * r.fv[f];
+        out[f] = r.fv[f] > Real(0);
+    }
+    Real recip[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) recip[k] = kCompactF<Real> == 10 ? r.fv[7 + k] : Real(0);
+    item_lu(F, r.fv[5], r.fv[6], out, (uint32_t)kSolveNoPivot, kCompactF<Real> == 10 ? recip : nullptr);
+    Real f16[16];
+    factor16(F, (uint32_t)kSolveNoPivot, f16);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) r.fv[5 + i] = f16[i];
+}
+
 // All the inputs of one (item, VG groups) task, loaded before any arithmetic.
 template <typename Real, int VG>
 struct PairIn {
@@ -773,8 +817,15 @@ sweep_direct_slot_kernel(const LevelArgs p, const Rec *__restrict__ rec, const u
     bool live = it < end;
     RegRecord<float> R;
     PairIn<float, VG> in;  // sources only
+    // Compact records: the LU is rebuilt after the upwind loads are issued,
+    // in their latency, not before the wait on the previous level -- except
+    // at 14 blocks per SM (73 registers), where that order spills more and
+    // measured slower.  The face-indexed direct kernel keeps it before: its
+    // four upwind rows leave it no registers (FP64 measured 5% slower).
+    constexpr bool kLate = std::is_same<Rec, CompactRecord<float>>::value && MINB <= 12;
     if (live) {
-        load_record(rec + it, R, (uint32_t)kSolveNoPivot);
+        if constexpr (kLate) load_compact_raw(rec + it, R);
+        else load_record(rec + it, R, (uint32_t)kSolveNoPivot);
         live = R.u(0) != kSentinel;
     }
     if (live) {
@@ -785,6 +836,7 @@ sweep_direct_slot_kernel(const LevelArgs p, const Rec *__restrict__ rec, const u
     if (!live) return;
     SlotIn<VG> sl;
     slot_load_upwind<VG>(p, R, g, sl);
+    if constexpr (kLate) compact_factor_nopivot(R);
     slot_solve_store_f32x2<VG>(p, R, g, in.q, sl);
 }
 
