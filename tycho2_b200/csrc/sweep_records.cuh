@@ -788,8 +788,15 @@ sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const 
     bool live = it < end;
     RegRecord<Real> R;
     PairIn<Real, VG> in;
+    // Compact NoPivot records without a register cap (MINB 1): the LU is
+    // rebuilt after the upwind loads are issued, in their latency.  Under a
+    // cap the four face-indexed upwind rows leave it no registers there and
+    // it stays before the wait (FP64 at 102 registers measured 5% slower
+    // the other way).
+    constexpr bool kLate = std::is_same<Rec, CompactRecord<Real>>::value && !ANY && MINB == 1;
     if (live) {
-        load_record(rec + it, R, ANY ? p.solver : (uint32_t)kSolveNoPivot);
+        if constexpr (kLate) load_compact_raw(rec + it, R);
+        else load_record(rec + it, R, ANY ? p.solver : (uint32_t)kSolveNoPivot);
         live = R.u(0) != kSentinel;
     }
     if (live) {
@@ -799,6 +806,7 @@ sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const 
     pdl_wait_prerequisites();
     if (!live) return;
     pair_load_upwind<Real, VG, false>(p, R, g, in);
+    if constexpr (kLate) compact_factor_nopivot(R);
     if constexpr (kPairedF32<Real, VG, ANY>) pair_solve_store_f32x2<VG, RegRecord<Real>, true>(p, R, g, in);
     else pair_solve_store_any<Real, VG, RegRecord<Real>, ANY>(p, R, g, in);
 }
@@ -820,8 +828,7 @@ sweep_direct_slot_kernel(const LevelArgs p, const Rec *__restrict__ rec, const u
     // Compact records: the LU is rebuilt after the upwind loads are issued,
     // in their latency, not before the wait on the previous level -- except
     // at 14 blocks per SM (73 registers), where that order spills more and
-    // measured slower.  The face-indexed direct kernel keeps it before: its
-    // four upwind rows leave it no registers (FP64 measured 5% slower).
+    // measured slower.
     constexpr bool kLate = std::is_same<Rec, CompactRecord<float>>::value && MINB <= 12;
     if (live) {
         if constexpr (kLate) load_compact_raw(rec + it, R);
