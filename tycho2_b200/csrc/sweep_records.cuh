@@ -812,7 +812,8 @@ sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const 
 }
 
 // The FP32 direct kernel with slotted upwind rows (even vector widths).
-template <int VG, int BS, typename Rec, int MINB>
+// PF: the launch is several resident waves deep (record prefetch, below).
+template <int VG, int BS, typename Rec, int MINB, bool PF = false>
 __global__ void __launch_bounds__(BS, MINB)
 sweep_direct_slot_kernel(const LevelArgs p, const Rec *__restrict__ rec, const uint64_t begin, const uint64_t end)
 {
@@ -830,6 +831,23 @@ sweep_direct_slot_kernel(const LevelArgs p, const Rec *__restrict__ rec, const u
     // at 14 blocks per SM (73 registers), where that order spills more and
     // measured slower.
     constexpr bool kLate = std::is_same<Rec, CompactRecord<float>>::value && MINB <= 12;
+    // In a launch several resident waves deep, the task half a resident wave
+    // ahead starts in a later wave, after this level's first blocks are
+    // gone; its record is prefetched into L2 now, so that its own record load
+    // (the head of its dependent chain) hits L2 instead of HBM.
+    if constexpr (PF) {
+        uint32_t nsm;
+        asm("mov.u32 %0, %%nsmid;" : "=r"(nsm));
+        const uint32_t t2 = t + nsm * (uint32_t)(MINB * BS / 2);
+        const uint32_t itl2 = gpv == 1u ? t2 : __umulhi(t2, p.vmagic);
+        const uint64_t it2 = begin + itl2;
+        if (it2 < end) {
+            const char *r2 = reinterpret_cast<const char *>(rec + it2);
+            // the item's gpv tasks share its 32-byte sectors
+            for (uint32_t sct = t2 - itl2 * gpv; sct * 32u < sizeof(Rec); sct += gpv)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(r2 + sct * 32u));
+        }
+    }
     if (live) {
         if constexpr (kLate) load_compact_raw(rec + it, R);
         else load_record(rec + it, R, (uint32_t)kSolveNoPivot);
@@ -1179,25 +1197,29 @@ static const void *direct_any_fn(int vg)
 }
 
 template <typename Real, typename Rec, int BS, int MINB>
-static const void *direct_slot_fn(int vg)
+static const void *direct_slot_fn(int vg, bool pf)
 {
     if constexpr (sizeof(Real) == 4) {
-        if (vg == 2) return (const void *)sweep_direct_slot_kernel<2, BS, Rec, MINB>;
-        if (vg == 4) return (const void *)sweep_direct_slot_kernel<4, BS, Rec, MINB>;
+        if (vg == 2)
+            return pf ? (const void *)sweep_direct_slot_kernel<2, BS, Rec, MINB, true>
+                      : (const void *)sweep_direct_slot_kernel<2, BS, Rec, MINB>;
+        if (vg == 4)
+            return pf ? (const void *)sweep_direct_slot_kernel<4, BS, Rec, MINB, true>
+                      : (const void *)sweep_direct_slot_kernel<4, BS, Rec, MINB>;
     }
     return nullptr;
 }
 
 template <typename Real, typename Rec>
-static const void *direct_fn(int knob, int vg, uint32_t solver)
+static const void *direct_fn(int knob, int vg, uint32_t solver, bool pf = false)
 {
     // Original and the Cramer solvers: one 128-thread kernel per vector width
     if (solver != kSolveNoPivot) return knob == 128 ? direct_any_fn<Real, Rec>(vg) : nullptr;
     switch (knob) {
     // slotted upwind rows: 64 threads with <= 102 / 85 / 73 registers
-    case -196: return direct_slot_fn<Real, Rec, 64, 10>(vg);
-    case -180: return direct_slot_fn<Real, Rec, 64, 12>(vg);
-    case -172: return direct_slot_fn<Real, Rec, 64, 14>(vg);
+    case -196: return direct_slot_fn<Real, Rec, 64, 10>(vg, pf);
+    case -180: return direct_slot_fn<Real, Rec, 64, 12>(vg, pf);
+    case -172: return direct_slot_fn<Real, Rec, 64, 14>(vg, pf);
     case 64: return direct_fn_vg<Real, 64, Rec, 1>(vg);
     case 128: return direct_fn_vg<Real, 128, Rec, 1>(vg);
     case 256: return direct_fn_vg<Real, 256, Rec, 1>(vg);
@@ -1215,6 +1237,20 @@ static const void *direct_fn(int knob, int vg, uint32_t solver)
 // -196 / -180 / -172: the FP32 kernel with slotted upwind rows, 64 threads
 // with at most 102 / 85 / 73 registers); compact picks the compact record
 // format.
+// Streaming multiprocessors of the current device (cached per device).
+inline int device_sm_count()
+{
+    static int cache[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (!cache[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+
 inline int direct_block_threads(int knob)
 {
     switch (knob) {
@@ -1231,8 +1267,12 @@ cudaError_t launch_direct_level(int knob, const LevelArgs &p, const void *rec, u
     if (end <= begin) return cudaSuccess;
     const uint64_t tasks = (end - begin) * (p.G / p.vg);
     if (tasks >= (1ull << 26)) return cudaErrorInvalidValue;
-    const void *fn = compact ? direct_fn<Real, CompactRecord<Real>>(knob, (int)p.vg, p.solver)
-                             : direct_fn<Real, ItemRecord<Real>>(knob, (int)p.vg, p.solver);
+    // Slotted kernels (10 / 12 / 14 blocks per SM): the record prefetch half
+    // a resident wave ahead in launches at least two waves deep.
+    const int slot_blocks = knob == -196 ? 10 : knob == -180 ? 12 : knob == -172 ? 14 : 0;
+    const bool pf = slot_blocks && tasks >= (uint64_t)device_sm_count() * slot_blocks * bs * 2;
+    const void *fn = compact ? direct_fn<Real, CompactRecord<Real>>(knob, (int)p.vg, p.solver, pf)
+                             : direct_fn<Real, ItemRecord<Real>>(knob, (int)p.vg, p.solver, pf);
     if (!fn) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)((tasks + bs - 1) / bs));
