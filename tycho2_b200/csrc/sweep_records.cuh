@@ -768,6 +768,28 @@ sweep_record_level_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict_
     record_pairs<Real, IPW, VG, false>(p, tiles[w], lane);
 }
 
+// Record prefetch of a deep launch (PF kernels): the task half a resident
+// wave ahead (blocks of BS threads, MINB per SM) starts in a later wave,
+// after this level's first blocks are gone; its record is prefetched into
+// L2 now, so that its own record load (the head of its dependent chain)
+// hits L2 instead of HBM.  The gpv tasks of an item share its 32-byte
+// sectors.
+template <typename Rec, int BS, int MINB>
+__device__ __forceinline__ void prefetch_record_ahead(const Rec *__restrict__ rec, uint32_t t, uint32_t gpv,
+                                                      uint32_t vmagic, uint64_t begin, uint64_t end)
+{
+    uint32_t nsm;
+    asm("mov.u32 %0, %%nsmid;" : "=r"(nsm));
+    const uint32_t t2 = t + nsm * (uint32_t)(MINB * BS / 2);
+    const uint32_t itl2 = gpv == 1u ? t2 : __umulhi(t2, vmagic);
+    const uint64_t it2 = begin + itl2;
+    if (it2 < end) {
+        const char *r2 = reinterpret_cast<const char *>(rec + it2);
+        for (uint32_t sct = t2 - itl2 * gpv; sct * 32u < sizeof(Rec); sct += gpv)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(r2 + sct * 32u));
+    }
+}
+
 // Direct variant (level schedule only): one thread per (item, VG groups)
 // task with the item's record loaded straight into registers -- the lanes of
 // one item read the same 128/256 bytes and L1 serves the repeats -- and its
@@ -775,7 +797,7 @@ sweep_record_level_kernel(const LevelArgs p, const ItemRecord<Real> *__restrict_
 // are read after it.  No shared memory.  Tasks of a level: item t / (G/VG),
 // groups VG * (t % (G/VG)) and on (the host keeps a level's task count
 // below 2^26 so that the multiply-high division is exact).
-template <typename Real, int VG, int BS, typename Rec, int MINB = 1, bool ANY = false>
+template <typename Real, int VG, int BS, typename Rec, int MINB = 1, bool ANY = false, bool PF = false>
 __global__ void __launch_bounds__(BS, MINB)
 sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const uint64_t begin, const uint64_t end)
 {
@@ -794,6 +816,7 @@ sweep_direct_level_kernel(const LevelArgs p, const Rec *__restrict__ rec, const 
     // it stays before the wait (FP64 at 102 registers measured 5% slower
     // the other way).
     constexpr bool kLate = std::is_same<Rec, CompactRecord<Real>>::value && !ANY && MINB == 1;
+    if constexpr (PF) prefetch_record_ahead<Rec, BS, MINB>(rec, t, gpv, p.vmagic, begin, end);
     if (live) {
         if constexpr (kLate) load_compact_raw(rec + it, R);
         else load_record(rec + it, R, ANY ? p.solver : (uint32_t)kSolveNoPivot);
@@ -831,23 +854,7 @@ sweep_direct_slot_kernel(const LevelArgs p, const Rec *__restrict__ rec, const u
     // at 14 blocks per SM (73 registers), where that order spills more and
     // measured slower.
     constexpr bool kLate = std::is_same<Rec, CompactRecord<float>>::value && MINB <= 12;
-    // In a launch several resident waves deep, the task half a resident wave
-    // ahead starts in a later wave, after this level's first blocks are
-    // gone; its record is prefetched into L2 now, so that its own record load
-    // (the head of its dependent chain) hits L2 instead of HBM.
-    if constexpr (PF) {
-        uint32_t nsm;
-        asm("mov.u32 %0, %%nsmid;" : "=r"(nsm));
-        const uint32_t t2 = t + nsm * (uint32_t)(MINB * BS / 2);
-        const uint32_t itl2 = gpv == 1u ? t2 : __umulhi(t2, p.vmagic);
-        const uint64_t it2 = begin + itl2;
-        if (it2 < end) {
-            const char *r2 = reinterpret_cast<const char *>(rec + it2);
-            // the item's gpv tasks share its 32-byte sectors
-            for (uint32_t sct = t2 - itl2 * gpv; sct * 32u < sizeof(Rec); sct += gpv)
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(r2 + sct * 32u));
-        }
-    }
+    if constexpr (PF) prefetch_record_ahead<Rec, BS, MINB>(rec, t, gpv, p.vmagic, begin, end);
     if (live) {
         if constexpr (kLate) load_compact_raw(rec + it, R);
         else load_record(rec + it, R, (uint32_t)kSolveNoPivot);
@@ -1167,8 +1174,14 @@ cudaError_t launch_item_records(const LevelArgs &p, uint64_t n, void *out, cudaS
 }
 
 template <typename Real, int BS, typename Rec, int MINB>
-static const void *direct_fn_vg(int vg)
+static const void *direct_fn_vg(int vg, bool pf = false)
 {
+    if constexpr (MINB == 10) {  // -96: the record prefetch of deep launches
+        if (pf && vg == 1) return (const void *)sweep_direct_level_kernel<Real, 1, BS, Rec, MINB, false, true>;
+        if (pf && vg == 2) return (const void *)sweep_direct_level_kernel<Real, 2, BS, Rec, MINB, false, true>;
+        if constexpr (sizeof(Real) == 4)
+            if (pf && vg == 4) return (const void *)sweep_direct_level_kernel<Real, 4, BS, Rec, MINB, false, true>;
+    }
     switch (vg) {
     case 8:  // two 4-group halves per task (FP32)
         if constexpr (sizeof(Real) == 4 && MINB == 1) return (const void *)sweep_direct2_level_kernel<Real, 4, BS, Rec>;
@@ -1224,7 +1237,7 @@ static const void *direct_fn(int knob, int vg, uint32_t solver, bool pf = false)
     case 128: return direct_fn_vg<Real, 128, Rec, 1>(vg);
     case 256: return direct_fn_vg<Real, 256, Rec, 1>(vg);
     case -64: return direct_fn_vg<Real, 64, Rec, 16>(vg);   // <= 64 registers
-    case -96: return direct_fn_vg<Real, 64, Rec, 10>(vg);   // <= 102 registers
+    case -96: return direct_fn_vg<Real, 64, Rec, 10>(vg, pf);  // <= 102 registers
     case -80: return direct_fn_vg<Real, 64, Rec, 12>(vg);   // <= 85 registers
     case -128: return direct_fn_vg<Real, 128, Rec, 8>(vg);  // <= 64 registers
     default: return nullptr;
@@ -1267,10 +1280,10 @@ cudaError_t launch_direct_level(int knob, const LevelArgs &p, const void *rec, u
     if (end <= begin) return cudaSuccess;
     const uint64_t tasks = (end - begin) * (p.G / p.vg);
     if (tasks >= (1ull << 26)) return cudaErrorInvalidValue;
-    // Slotted kernels (10 / 12 / 14 blocks per SM): the record prefetch half
-    // a resident wave ahead in launches at least two waves deep.
-    const int slot_blocks = knob == -196 ? 10 : knob == -180 ? 12 : knob == -172 ? 14 : 0;
-    const bool pf = slot_blocks && tasks >= (uint64_t)device_sm_count() * slot_blocks * bs * 2;
+    // Slotted kernels (10 / 12 / 14 blocks per SM) and -96 (10): the record
+    // prefetch half a resident wave ahead in launches at least two waves deep.
+    const int pf_blocks = knob == -196 || knob == -96 ? 10 : knob == -180 ? 12 : knob == -172 ? 14 : 0;
+    const bool pf = pf_blocks && tasks >= (uint64_t)device_sm_count() * pf_blocks * bs * 2;
     const void *fn = compact ? direct_fn<Real, CompactRecord<Real>>(knob, (int)p.vg, p.solver, pf)
                              : direct_fn<Real, ItemRecord<Real>>(knob, (int)p.vg, p.solver, pf);
     if (!fn) return cudaErrorInvalidValue;
