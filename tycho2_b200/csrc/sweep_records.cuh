@@ -1283,7 +1283,8 @@ cudaError_t launch_direct_level(int knob, const LevelArgs &p, const void *rec, u
     // Slotted kernels (10 / 12 / 14 blocks per SM) and -96 (10): the record
     // prefetch half a resident wave ahead in launches at least two waves deep.
     const int pf_blocks = knob == -196 || knob == -96 ? 10 : knob == -180 ? 12 : knob == -172 ? 14 : 0;
-    const bool pf = pf_blocks && tasks >= (uint64_t)device_sm_count() * pf_blocks * bs * 2;
+    const uint64_t sms = (uint64_t)device_sm_count();
+    const bool pf = pf_blocks && sms && tasks >= sms * pf_blocks * bs * 2;
     const void *fn = compact ? direct_fn<Real, CompactRecord<Real>>(knob, (int)p.vg, p.solver, pf)
                              : direct_fn<Real, ItemRecord<Real>>(knob, (int)p.vg, p.solver, pf);
     if (!fn) return cudaErrorInvalidValue;
