@@ -14,7 +14,6 @@ sigma_t, downscatter rows summing to 0.6 sigma_t, q = 1 in the central 1/8.
   1e-8 of it.
 """
 import os
-import subprocess
 import sys
 
 import numpy as np

@@ -7,8 +7,6 @@ no CPU fallback for the sweep.
 import ctypes as C
 import os
 
-import numpy as np
-
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libtycho_b200.so")
 
